@@ -1,0 +1,221 @@
+"""Synthetic scene generators for the benchmark and test workloads.
+
+Each generator writes a scene in the reference's XML format plus the OBJ meshes it
+references, so that the GPU integrators and the CPU oracle consume the same files.
+All randomness is seeded; the same arguments always produce the same bytes.
+
+Workloads (sizes as named by the benchmark configurations):
+  cornell      -- Cornell box, 256x256, 16 spp, path, max depth 8
+  traversal    -- 1M random triangles + 16M random rays (arrays, no XML)
+  microfacet   -- 1024x1024, 64 spp, path depth 16: ground quad plus a 64x64 grid of
+                  displaced icospheres (1280 triangles each) with plastic / rough
+                  conductor / rough glass, lit by 8 spherical emitters
+  volumetric   -- the Cornell box at 512x512, 64 spp, volpath depth 32, filled with a
+                  homogeneous medium (index-material boundary) plus a glass sphere
+                  holding a second medium
+"""
+import os
+
+import numpy as np
+
+# ------------------------------------------------------------------ OBJ writers
+
+
+def _fmt(x):
+    return "%.9g" % float(x)
+
+
+def write_plane_obj(path):
+    """Unit quad [-0.5, 0.5]^2 in the xz plane, normal +y, with texture coordinates."""
+    with open(path, "w") as f:
+        f.write("v -0.5 0 -0.5\nv 0.5 0 -0.5\nv 0.5 0 0.5\nv -0.5 0 0.5\n")
+        f.write("vt 0 1\nvt 1 1\nvt 1 0\nvt 0 0\n")
+        f.write("vn 0 1 0\n")
+        f.write("f 1/1/1 4/4/1 3/3/1\nf 1/1/1 3/3/1 2/2/1\n")
+
+
+def write_cube_obj(path):
+    """Unit cube [-0.5, 0.5]^3, 12 triangles, flat outward normals, per-face uvs."""
+    corners = np.array([[x, y, z] for z in (-0.5, 0.5) for y in (-0.5, 0.5) for x in (-0.5, 0.5)])
+    faces = [  # (corner indices counter-clockwise seen from outside, normal)
+        ((0, 2, 3, 1), (0, 0, -1)), ((4, 5, 7, 6), (0, 0, 1)),
+        ((0, 4, 6, 2), (-1, 0, 0)), ((1, 3, 7, 5), (1, 0, 0)),
+        ((0, 1, 5, 4), (0, -1, 0)), ((2, 6, 7, 3), (0, 1, 0)),
+    ]
+    with open(path, "w") as f:
+        for c in corners:
+            f.write("v %s %s %s\n" % tuple(_fmt(v) for v in c))
+        f.write("vt 0 0\nvt 1 0\nvt 1 1\nvt 0 1\n")
+        for _, n in faces:
+            f.write("vn %d %d %d\n" % n)
+        for k, (q, _) in enumerate(faces):
+            a, b, c, d = (i + 1 for i in q)
+            n = k + 1
+            f.write("f %d/1/%d %d/2/%d %d/3/%d\n" % (a, n, b, n, c, n))
+            f.write("f %d/1/%d %d/3/%d %d/4/%d\n" % (a, n, c, n, d, n))
+
+
+def write_mesh_obj(path, verts, faces, normals=None):
+    """Indexed triangle mesh; per-vertex normals when given."""
+    lines = ["v %s %s %s" % (_fmt(v[0]), _fmt(v[1]), _fmt(v[2])) for v in verts]
+    if normals is not None:
+        lines += ["vn %s %s %s" % (_fmt(n[0]), _fmt(n[1]), _fmt(n[2])) for n in normals]
+        lines += ["f %d//%d %d//%d %d//%d" % (a + 1, a + 1, b + 1, b + 1, c + 1, c + 1) for a, b, c in faces]
+    else:
+        lines += ["f %d %d %d" % (a + 1, b + 1, c + 1) for a, b, c in faces]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+# ------------------------------------------------------------------ XML helpers
+
+
+def _transform(steps, name="toWorld"):
+    """steps: list of ("scale", (x,y,z)) / ("rotate", (axis, angle)) / ("translate", (x,y,z))."""
+    out = ['<transform name="%s">' % name]
+    for kind, v in steps:
+        if kind == "scale":
+            out.append('<scale x="%s" y="%s" z="%s"/>' % tuple(_fmt(a) for a in v))
+        elif kind == "rotate":
+            axis, ang = v
+            out.append('<rotate axis="%s %s %s" angle="%s"/>' % (*(_fmt(a) for a in axis), _fmt(ang)))
+        elif kind == "translate":
+            out.append('<translate x="%s" y="%s" z="%s"/>' % tuple(_fmt(a) for a in v))
+    out.append("</transform>")
+    return "\n".join(out)
+
+
+def _color(name, c):
+    return '<color name="%s" value="%s %s %s"/>' % (name, _fmt(c[0]), _fmt(c[1]), _fmt(c[2]))
+
+
+def _camera(origin, target, fov, w, h, up=(0, 1, 0)):
+    return "\n".join([
+        '<camera type="perspective">',
+        '<transform name="toWorld"><lookat origin="%s, %s, %s" target="%s, %s, %s" up="%s, %s, %s"/></transform>'
+        % tuple(_fmt(v) for v in (*origin, *target, *up)),
+        '<float name="fov" value="%s"/>' % _fmt(fov),
+        '<integer name="width" value="%d"/>' % w,
+        '<integer name="height" value="%d"/>' % h,
+        '<filter type="box"/>',
+        "</camera>",
+    ])
+
+
+def _medium(name, sigma_a, sigma_s, g):
+    return "\n".join([
+        '<medium type="homogeneous" name="%s">' % name,
+        _color("sigma_a", sigma_a), _color("sigma_s", sigma_s),
+        '<float name="g" value="%s"/>' % _fmt(g),
+        "</medium>",
+    ])
+
+
+# ------------------------------------------------------------------ Cornell box
+
+
+def _cornell_body(light_y=0.998):
+    gray, red, green = (0.75, 0.75, 0.75), (0.63, 0.065, 0.05), (0.14, 0.45, 0.09)
+    walls = [
+        ([("scale", (2, 1, 2)), ("translate", (0, -1, 0))], gray),                               # floor
+        ([("scale", (2, 1, 2)), ("rotate", ((1, 0, 0), 180)), ("translate", (0, 1, 0))], gray),  # ceiling
+        ([("scale", (2, 1, 2)), ("rotate", ((1, 0, 0), 90)), ("translate", (0, 0, -1))], gray),  # back
+        ([("scale", (2, 1, 2)), ("rotate", ((0, 0, 1), -90)), ("translate", (-1, 0, 0))], red),  # left
+        ([("scale", (2, 1, 2)), ("rotate", ((0, 0, 1), 90)), ("translate", (1, 0, 0))], green),  # right
+    ]
+    out = []
+    for k, (tr, alb) in enumerate(walls):
+        shape = '<shape type="mesh" id="plane"><string name="filename" value="plane.obj"/></shape>' if k == 0 else '<ref id="plane"/>'
+        out += ["<primitive>", _transform(tr), shape, '<material type="matte">', _color("albedo", alb), "</material>", "</primitive>"]
+    boxes = [
+        ([("scale", (0.6, 0.6, 0.6)), ("rotate", ((0, 1, 0), 18)), ("translate", (0.35, -0.7, 0.3))]),
+        ([("scale", (0.6, 1.2, 0.6)), ("rotate", ((0, 1, 0), -15)), ("translate", (-0.35, -0.4, -0.3))]),
+    ]
+    for k, tr in enumerate(boxes):
+        shape = '<shape type="mesh" id="cube"><string name="filename" value="cube.obj"/></shape>' if k == 0 else '<ref id="cube"/>'
+        out += ["<primitive>", _transform(tr), shape, '<material type="matte">', _color("albedo", gray), "</material>", "</primitive>"]
+    out += [
+        "<primitive>",
+        _transform([("scale", (0.5, 1, 0.4)), ("rotate", ((1, 0, 0), 180)), ("translate", (0, light_y, 0))]),
+        '<ref id="plane"/>',
+        '<material type="matte">', _color("albedo", (0, 0, 0)), "</material>",
+        '<emitter type="area">', _color("radiance", (17, 12, 4)), "</emitter>",
+        "</primitive>",
+    ]
+    return out
+
+
+def cornell(out_dir, width=256, height=256, spp=16, max_depth=8, integrator="path_gpu"):
+    """Writes the Cornell-box scene; returns the XML path."""
+    os.makedirs(out_dir, exist_ok=True)
+    write_plane_obj(os.path.join(out_dir, "plane.obj"))
+    write_cube_obj(os.path.join(out_dir, "cube.obj"))
+    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height),
+           '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
+           '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
+    xml += _cornell_body()
+    xml.append("</scene>")
+    path = os.path.join(out_dir, "cornell.xml")
+    with open(path, "w") as f:
+        f.write("\n".join(xml) + "\n")
+    return path
+
+
+def volumetric(out_dir, width=512, height=512, spp=64, max_depth=32, integrator="volpath_gpu"):
+    """Cornell box filled with a homogeneous medium plus a glass sphere with its own
+    interior medium; returns the XML path."""
+    os.makedirs(out_dir, exist_ok=True)
+    write_plane_obj(os.path.join(out_dir, "plane.obj"))
+    write_cube_obj(os.path.join(out_dir, "cube.obj"))
+    box_med = ((0.05, 0.05, 0.05), (0.5, 0.5, 0.5), 0.6)
+    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height),
+           '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
+           '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
+    xml += _cornell_body(light_y=0.99)
+    # medium boundary: a box inset to +-0.995, index material (null BSDF)
+    xml += ["<primitive>", _transform([("scale", (1.99, 1.99, 1.99))]), '<ref id="cube"/>',
+            '<material type="index">', _medium("inside", *box_med), "</material>", "</primitive>"]
+    # glass sphere resting on the short box, interior medium, outside = box medium
+    xml += ["<primitive>", _transform([("translate", (0.35, -0.05, 0.3))]),
+            '<shape type="sphere"><float name="radius" value="0.35"/></shape>',
+            '<material type="glass"><float name="eta" value="1.5"/><float name="roughness" value="0"/>',
+            _medium("inside", (0.1, 0.1, 0.1), (2.0, 2.0, 2.0), -0.3),
+            _medium("outside", *box_med),
+            "</material>", "</primitive>"]
+    xml.append("</scene>")
+    path = os.path.join(out_dir, "volumetric.xml")
+    with open(path, "w") as f:
+        f.write("\n".join(xml) + "\n")
+    return path
+
+
+# ------------------------------------------------------------------ traversal micro-benchmark
+
+
+def random_triangles(n=1 << 20, seed=1):
+    """Triangle soup: centroids uniform in [0,1]^3, vertices = centroid + N(0, 0.01^2)
+    per axis. Returns float32 [n, 3, 3]."""
+    rng = np.random.default_rng(seed)
+    c = rng.random((n, 1, 3), dtype=np.float64)
+    e = rng.normal(0.0, 0.01, size=(n, 3, 3))
+    return (c + e).astype(np.float32)
+
+
+def random_rays(n=1 << 24, seed=1):
+    """Rays with origins uniform in [-0.5, 1.5]^3 and directions uniform on the sphere
+    (z = 1 - 2u, phi = 2 pi v); tmin = 1e-4, tmax = inf. Returns float32 [n, 8]
+    laid out (ox, oy, oz, tmin, dx, dy, dz, tmax)."""
+    rng = np.random.default_rng(seed + 1000)
+    o = rng.uniform(-0.5, 1.5, size=(n, 3))
+    u = rng.random(n)
+    v = rng.random(n)
+    z = 1.0 - 2.0 * u
+    r = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    phi = 2.0 * np.pi * v
+    d = np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=1)
+    out = np.empty((n, 8), np.float32)
+    out[:, 0:3] = o
+    out[:, 3] = 1e-4
+    out[:, 4:7] = d
+    out[:, 7] = np.inf
+    return out

@@ -1,0 +1,482 @@
+// Oracle (test infrastructure only): plugin objects of the reference (materials,
+// textures, media, emitters, camera, film, filters, scene) and the name registry,
+// restated on the CPU.
+#include "oscene.h"
+#include <iostream>
+
+namespace orc {
+
+const char* classTypeName(ClassType t) {
+    switch (t) {
+        case EScene: return "scene"; case EPrimitive: return "primitive"; case EShape: return "shape";
+        case ECamera: return "camera"; case EIntegrator: return "integrator"; case ESampler: return "sampler";
+        case ETexture: return "texture"; case EMaterial: return "material"; case EEmitter: return "emitter";
+        case EFilter: return "filter"; case EMedium: return "medium";
+    }
+    return "unknown";
+}
+
+// ---------------------------------------------------------------- textures
+// constant.h:9-32
+template <typename T>
+struct ConstantTexture : Texture<T> {
+    T value;
+    explicit ConstantTexture(const PropertyList& p) {
+        if constexpr (std::is_same_v<T, float>) value = p.getFloat("value", 1.0f);
+        else value = p.getColor("value", Color(1.0f));
+    }
+    T evaluate(const SurfaceInteraction&) const override { return value; }
+};
+// checkerboard.h:20-48
+template <typename T>
+struct CheckerTexture : Texture<T> {
+    T v1, v2;
+    Vec2 scale, delta;
+    explicit CheckerTexture(const PropertyList& p) {
+        if constexpr (std::is_same_v<T, float>) { v1 = p.getFloat("value1", 1.0f); v2 = p.getFloat("value2", 0.0f); }
+        else { v1 = p.getColor("value1", Color(1.0f)); v2 = p.getColor("value2", Color(0.0f)); }
+        scale = p.getVector2("scale", Vec2(1.0f, 1.0f));
+        delta = p.getPoint2("delta", Vec2(0.0f, 0.0f));
+    }
+    T evaluate(const SurfaceInteraction& si) const override {
+        Vec2 uv = si.uv;
+        uv.x /= scale.x; uv.y /= scale.y;
+        uv.x -= delta.x; uv.y -= delta.y;
+        int s = (int)std::floor(uv.x), t = (int)std::floor(uv.y);
+        return ((s + t) % 2 == 0) ? v1 : v2;
+    }
+};
+
+template <typename T>
+static std::shared_ptr<Texture<T>> constTex(const T& v) {
+    PropertyList p;
+    if constexpr (std::is_same_v<T, float>) p.f["value"] = v; else p.c["value"] = v;
+    return std::make_shared<ConstantTexture<T>>(p);
+}
+// matte.cpp:33-43, area.cpp:31-43: the "missing texture" magenta checkerboard
+static std::shared_ptr<ColorTexture> missingTex() {
+    PropertyList p;
+    p.c["value1"] = Color(0.0f);
+    p.c["value2"] = Color(1.0f, 0.0f, 1.0f);
+    p.v2["scale"] = Vec2(0.1f, 0.1f);
+    return std::make_shared<CheckerTexture<Color>>(p);
+}
+
+// ---------------------------------------------------------------- materials
+// material.h:36-59
+void Material::addChild(ObjectPtr child) {
+    if (child->classType() == EMedium && child->name == "inside") {
+        if (inside) throw std::runtime_error("Material: inside medium already defined!");
+        inside = std::static_pointer_cast<Medium>(child);
+    } else if (child->classType() == EMedium && child->name == "outside") {
+        if (outside) throw std::runtime_error("Material: outside medium already defined!");
+        outside = std::static_pointer_cast<Medium>(child);
+    } else {
+        throw std::runtime_error("Material: cannot add specified child (" + child->name + ")!");
+    }
+}
+
+template <typename T>
+static void setTex(std::shared_ptr<Texture<T>>& slot, ObjectPtr child) {
+    slot = std::static_pointer_cast<Texture<T>>(child);
+}
+
+// matte.cpp:7-53
+struct Matte : Material {
+    std::shared_ptr<ColorTexture> albedo;
+    explicit Matte(const PropertyList& p) { if (p.hasColor("albedo")) albedo = constTex(p.getColor("albedo")); }
+    void addChild(ObjectPtr c) override {
+        if (c->classType() != ETexture) throw std::runtime_error("Matte: cannot add specified child!");
+        if (c->name == "albedo") { if (albedo) throw std::runtime_error("Matte: there's already an albedo defined!"); setTex(albedo, c); }
+        else Material::addChild(c);
+    }
+    void activate() override { if (!albedo) albedo = missingTex(); }
+    void computeScatteringFunctions(SurfaceInteraction& si, Arena& a) const override {
+        si.bsdf = a.create<BSDF>(si.n, si.dpdu);
+        si.bsdf->add(a.create<Lambertian>(albedo->evaluate(si)));
+    }
+};
+// plastic.cpp:8-91
+struct Plastic : Material {
+    std::shared_ptr<ColorTexture> Kd, Ks;
+    std::shared_ptr<FloatTexture> rough, eta;
+    explicit Plastic(const PropertyList& p) {
+        if (p.hasColor("Kd")) Kd = constTex(p.getColor("Kd"));
+        if (p.hasColor("Ks")) Ks = constTex(p.getColor("Ks"));
+        if (p.hasFloat("roughness")) rough = constTex(p.getFloat("roughness"));
+        if (p.hasFloat("eta")) eta = constTex(p.getFloat("eta"));
+    }
+    void addChild(ObjectPtr c) override {
+        if (c->classType() != ETexture) return;
+        if (c->name == "Kd") setTex(Kd, c); else if (c->name == "Ks") setTex(Ks, c);
+        else if (c->name == "roughness") setTex(rough, c); else if (c->name == "eta") setTex(eta, c);
+        else Material::addChild(c);
+    }
+    void activate() override {
+        if (!Kd) Kd = constTex(Color(0.25f));
+        if (!Ks) Ks = constTex(Color(0.25f));
+        if (!rough) rough = constTex(0.1f);
+        if (!eta) eta = constTex(1.5f);
+    }
+    void computeScatteringFunctions(SurfaceInteraction& si, Arena& a) const override {
+        Color kd = Kd->evaluate(si), ks = Ks->evaluate(si);
+        float r = rough->evaluate(si), e = eta->evaluate(si);
+        si.bsdf = a.create<BSDF>(si.n, si.dpdu);
+        if (r == 0.0f) si.bsdf->add(a.create<SmoothPlastic>(kd, ks, e));
+        else si.bsdf->add(a.create<RoughPlastic>(kd, ks, e, a.create<TrowbridgeReitz>(roughnessToAlpha(r))));
+    }
+};
+// conductor.cpp:9-120
+struct Conductor : Material {
+    std::shared_ptr<ColorTexture> R, eta, k;
+    std::shared_ptr<FloatTexture> rough;
+    explicit Conductor(const PropertyList& p) {
+        if (p.hasColor("R")) R = constTex(p.getColor("R"));
+        if (p.hasColor("eta")) eta = constTex(p.getColor("eta"));
+        if (p.hasColor("k")) k = constTex(p.getColor("k"));
+        if (p.hasFloat("roughness")) rough = constTex(p.getFloat("roughness"));
+    }
+    void addChild(ObjectPtr c) override {
+        if (c->classType() != ETexture) throw std::runtime_error("Conductor: cannot add specified child!");
+        if (c->name == "R") setTex(R, c); else if (c->name == "eta") setTex(eta, c);
+        else if (c->name == "k") setTex(k, c); else if (c->name == "roughness") setTex(rough, c);
+        else Material::addChild(c);
+    }
+    void activate() override {
+        if (!R) R = constTex(Color(1.0f));
+        if (!eta) eta = constTex(Color(1.0f));
+        if (!k) k = constTex(Color(1.0f));
+        if (!rough) rough = constTex(0.0f);
+    }
+    void computeScatteringFunctions(SurfaceInteraction& si, Arena& a) const override {
+        Color r = R->evaluate(si), e = eta->evaluate(si), kk = k->evaluate(si);
+        float ro = rough->evaluate(si);
+        si.bsdf = a.create<BSDF>(si.n, si.dpdu);
+        Fresnel* fr = a.create<FresnelConductor>(Color(1.0f), e, kk);
+        if (ro == 0.0f) si.bsdf->add(a.create<SpecularReflection>(r, fr));
+        else si.bsdf->add(a.create<MicrofacetReflection>(r, a.create<TrowbridgeReitz>(roughnessToAlpha(ro)), fr));
+    }
+};
+// glass.cpp:8-115
+struct Glass : Material {
+    std::shared_ptr<ColorTexture> R, T;
+    std::shared_ptr<FloatTexture> rough, eta;
+    explicit Glass(const PropertyList& p) {
+        if (p.hasColor("R")) R = constTex(p.getColor("R"));
+        if (p.hasColor("T")) T = constTex(p.getColor("T"));
+        if (p.hasFloat("roughness")) rough = constTex(p.getFloat("roughness"));
+        if (p.hasFloat("eta")) eta = constTex(p.getFloat("eta"));
+    }
+    void addChild(ObjectPtr c) override {
+        if (c->name == "R") setTex(R, c); else if (c->name == "T") setTex(T, c);
+        else if (c->name == "roughness") setTex(rough, c); else if (c->name == "eta") setTex(eta, c);
+        else Material::addChild(c);
+    }
+    void activate() override {
+        if (!R) R = constTex(Color(1.0f));
+        if (!T) T = constTex(Color(1.0f));
+        if (!rough) rough = constTex(0.0f);
+        if (!eta) eta = constTex(1.5f);
+    }
+    void computeScatteringFunctions(SurfaceInteraction& si, Arena& a) const override {
+        applyMediums(si);
+        Color r = R->evaluate(si), t = T->evaluate(si);
+        float e = eta->evaluate(si), ro = rough->evaluate(si);
+        si.bsdf = a.create<BSDF>(si.n, si.dpdu);
+        if (ro == 0.0f) si.bsdf->add(a.create<FresnelSpecular>(r, t, 1.0f, e));
+        else si.bsdf->add(a.create<MicrofacetFresnel>(r, t, 1.0f, e, a.create<TrowbridgeReitz>(roughnessToAlpha(ro))));
+    }
+};
+// index.cpp:6-16 (null BSDF: a pass-through medium boundary)
+struct IndexMaterial : Material {
+    explicit IndexMaterial(const PropertyList&) {}
+    void computeScatteringFunctions(SurfaceInteraction& si, Arena&) const override {
+        applyMediums(si);
+        si.bsdf = nullptr;
+    }
+};
+
+// ---------------------------------------------------------------- media
+// homogeneous.cpp:14-20
+HomogeneousMedium::HomogeneousMedium(const PropertyList& p) {
+    sigma_a = p.getColor("sigma_a", Color(0.1f));
+    sigma_s = p.getColor("sigma_s", Color(0.1f));
+    g = p.getFloat("g", 0.0f);
+    sigma_t = sigma_a + sigma_s;
+}
+// homogeneous.cpp:22-30
+Color HomogeneousMedium::Tr(const Ray& ray) const {
+    if (std::isinf(ray.tMax)) return Color(0.0f);
+    return Color(std::exp(-sigma_t.r * ray.tMax), std::exp(-sigma_t.g * ray.tMax), std::exp(-sigma_t.b * ray.tMax));
+}
+// homogeneous.cpp:32-63
+Color HomogeneousMedium::sample(const Ray& ray, Sampler& s, Arena& a, MediumInteraction& mi) const {
+    float u0 = s.next1D();
+    float u1 = s.next1D();
+    return sampleU(ray, u0, u1, a, mi);
+}
+Color HomogeneousMedium::sampleU(const Ray& ray, float u0, float u1, Arena& a, MediumInteraction& mi) const {
+    int channel = std::min((int)(u0 * 3.0f), 2);
+    float dist = -std::log(1.0f - u1) / sigma_t[channel];
+    float t = std::min(dist, ray.tMax);
+    bool sampledMedium = t < ray.tMax;
+    Color Trv(std::exp(-sigma_t.r * t), std::exp(-sigma_t.g * t), std::exp(-sigma_t.b * t));
+    Color pc = sampledMedium ? (sigma_t * Trv) : Trv;
+    float pdf = (pc.r + pc.g + pc.b) / 3.0f;
+    if (pdf == 0.0f) return Color(0.0f);
+    if (sampledMedium) {
+        mi.p = ray.o + ray.d * t;
+        mi.wo = -ray.d;
+        mi.medium = this;
+        mi.phase = a.create<HGPhase>(g);
+        mi.sigma_a = sigma_a;
+        mi.sigma_s = sigma_s;
+    }
+    return Trv / pdf;
+}
+
+// ---------------------------------------------------------------- emitters
+// area.cpp:7-119
+struct AreaLight : Emitter {
+    std::shared_ptr<ColorTexture> radiance;
+    explicit AreaLight(const PropertyList& p) { if (p.hasColor("radiance")) radiance = constTex(p.getColor("radiance")); }
+    void addChild(ObjectPtr c) override {
+        if (c->classType() != ETexture) throw std::runtime_error("AreaLight: cannot add specified child!");
+        if (c->name == "radiance") { if (radiance) throw std::runtime_error("AreaLight: radiance already defined!"); setTex(radiance, c); }
+    }
+    void activate() override { if (!radiance) radiance = missingTex(); }
+    // area.cpp:45-49
+    Color eval(const SurfaceInteraction& si, const Vec3& w) const override {
+        if (Dot(si.n, w) > 0.0f) return radiance->evaluate(si);
+        return Color(0.0f);
+    }
+    // area.cpp:51-88 (pdf is left unwritten on the early return, as in the reference)
+    Color sample(const SurfaceInteraction& ref, const Vec2& u, SurfaceInteraction& info, float& pdf, Ray& sr) const override {
+        SurfaceInteraction local;
+        const Transform& tw = prim->toWorld;
+        float areaPdf = prim->shape->sampleSurface(ref.p, u, local);
+        info.p = tw.point(local.p);
+        info.n = Normalize(tw.normal(local.n));
+        info.uv = local.uv;
+        info.time = ref.time;
+        Frame fr = Frame::fromNormal(local.n);
+        Vec3 t1 = tw.vector(fr.x), t2 = tw.vector(fr.y);
+        float areaScale = Cross(t1, t2).length();
+        if (areaScale > 0.0f) areaPdf /= areaScale;
+        sr.o = ref.p;
+        sr.d = Normalize(info.p - ref.p);
+        sr.tMin = Epsilon;
+        sr.tMax = (info.p - ref.p).length() - Epsilon;
+        sr.time = ref.time;
+        float dist = (ref.p - info.p).lengthSquared();
+        Vec3 wi = sr.d;
+        float cosTheta = Dot(info.n, -wi);
+        if (areaPdf <= Epsilon || cosTheta <= Epsilon) return Color(0.0f);
+        float anglePdf = areaPdf * dist / cosTheta;
+        pdf = anglePdf;
+        return eval(info, Normalize(ref.p - info.p)) / pdf;
+    }
+    // area.cpp:90-119
+    float pdf(const SurfaceInteraction& ref, const SurfaceInteraction& info) const override {
+        SurfaceInteraction local;
+        const Transform tw = prim->toWorld;
+        const Transform tl = tw.inverse();
+        local.p = tl.point(info.p);
+        local.n = tl.normal(info.n);
+        local.uv = info.uv;
+        float areaPdf = prim->shape->pdfSurface(tl.point(ref.p), local);
+        Frame fr = Frame::fromNormal(local.n);
+        Vec3 t1 = tw.vector(fr.x), t2 = tw.vector(fr.y);
+        float areaScale = Cross(t1, t2).length();
+        if (areaScale > 0.0f) areaPdf /= areaScale;
+        float dist = (ref.p - info.p).lengthSquared();
+        Vec3 wi = Normalize(info.p - ref.p);
+        float cosTheta = Dot(info.n, -wi);
+        if (areaPdf <= Epsilon || cosTheta <= Epsilon) return 0.0f;
+        return areaPdf * dist / cosTheta;
+    }
+};
+
+// ---------------------------------------------------------------- filters, film, camera
+// filter.h:20-32
+struct BoxFilter : Filter {
+    explicit BoxFilter(const PropertyList&) { radius = Vec2(0.5f, 0.5f); }
+    float evaluate(const Vec2& p) const override {
+        return (std::abs(p.x) <= radius.x && std::abs(p.y) <= radius.y) ? 1.0f : 0.0f;
+    }
+};
+// filter.h:34-54
+struct GaussianFilter : Filter {
+    float alpha, expX, expY;
+    explicit GaussianFilter(const PropertyList& p) {
+        radius = p.getVector2("radius", Vec2(2.0f, 2.0f));
+        alpha = p.getFloat("alpha", 2.0f);
+        expX = std::exp(-alpha * radius.x * radius.x);
+        expY = std::exp(-alpha * radius.y * radius.y);
+    }
+    float evaluate(const Vec2& p) const override {
+        float gx = std::max(0.0f, std::exp(-alpha * p.x * p.x) - expX);
+        float gy = std::max(0.0f, std::exp(-alpha * p.y * p.y) - expY);
+        return gx * gy;
+    }
+};
+
+Film::Film(int w, int h, std::shared_ptr<Filter> f) : width(w), height(h), filter(f), sum((size_t)w * h * 7) {
+    if (!filter) filter = std::make_shared<GaussianFilter>(PropertyList());   // film.cpp:29
+    clear();
+}
+void Film::clear() { for (auto& a : sum) a.store(0.0f, std::memory_order_relaxed); }
+static inline void atomicAddF(std::atomic<float>& t, float v) {
+    float cur = t.load(std::memory_order_relaxed);
+    while (!t.compare_exchange_weak(cur, cur + v, std::memory_order_release, std::memory_order_relaxed)) {}
+}
+// film.h:26-69 (radiance channel only)
+void Film::addSample(const Vec2& pFilm, const Color& L) {
+    if (L.hasNaNs()) return;
+    Vec2 r = filter->radius;
+    int x0 = std::max(0, (int)std::ceil(pFilm.x - r.x - 0.5f));
+    int x1 = std::min(width - 1, (int)std::floor(pFilm.x + r.x - 0.5f));
+    int y0 = std::max(0, (int)std::ceil(pFilm.y - r.y - 0.5f));
+    int y1 = std::min(height - 1, (int)std::floor(pFilm.y + r.y - 0.5f));
+    for (int py = y0; py <= y1; ++py) {
+        for (int px = x0; px <= x1; ++px) {
+            Vec2 off(pFilm.x - (px + 0.5f), pFilm.y - (py + 0.5f));
+            float w = filter->evaluate(off);
+            if (w > 0.0f) {
+                std::atomic<float>* a = &sum[((size_t)py * width + px) * 7];
+                atomicAddF(a[0], L.r * w);
+                atomicAddF(a[1], L.g * w);
+                atomicAddF(a[2], L.b * w);
+                atomicAddF(a[3], w);
+                atomicAddF(a[4], L.r * L.r * w);
+                atomicAddF(a[5], L.g * L.g * w);
+                atomicAddF(a[6], L.b * L.b * w);
+            }
+        }
+    }
+}
+
+// camera.h:30-52, perspective.cpp:9-12
+Camera::Camera(const PropertyList& p) {
+    toWorld = p.getTransform("toWorld", Transform());
+    if (p.hasTransform("toWorldEnd") && !(p.getTransform("toWorldEnd") == toWorld))
+        throw std::runtime_error("Camera: animated transforms are not supported by this restatement");
+    width = p.getInteger("width", 1280);
+    height = p.getInteger("height", 720);
+    fov = p.getFloat("fov", 45.0f);
+    scale = std::tan((Pi / 180.f) * (fov * 0.5f));
+}
+void Camera::addChild(ObjectPtr c) {
+    if (c->classType() == EFilter) {
+        if (filterObj) throw std::runtime_error("Camera: cannot define multiple films!");
+        filterObj = std::static_pointer_cast<Filter>(c);
+    }
+}
+// perspective.cpp:15-32
+Ray Camera::shootRay(const Vec2& pFilm, float time) const {
+    float x = (2.0f * pFilm.x - 1.0f) * aspect() * scale;
+    float y = (2.0f * pFilm.y - 1.0f) * scale;
+    Vec3 dir = Normalize(Vec3(x, y, -1.0f));
+    Ray rc(Vec3(0, 0, 0), dir);
+    Ray r = toWorld.ray(rc);
+    r.time = time;
+    return r;
+}
+
+// ---------------------------------------------------------------- primitive, scene
+// primitive.cpp:7-46
+Primitive::Primitive(const PropertyList& p) {
+    toWorld = p.getTransform("toWorld", Transform());
+    if (p.hasTransform("toWorldEnd") && !(p.getTransform("toWorldEnd") == toWorld))
+        throw std::runtime_error("Primitive: animated transforms are not supported by this restatement");
+}
+void Primitive::addChild(ObjectPtr c) {
+    if (c->classType() == EShape) {
+        if (shape) throw std::runtime_error("Primitive: shape already registered!");
+        shape = std::static_pointer_cast<Shape>(c);
+    } else if (c->classType() == EMaterial) {
+        if (material) throw std::runtime_error("Primitive: material already registered!");
+        material = std::static_pointer_cast<Material>(c);
+    } else if (c->classType() == EEmitter) {
+        if (emitter) throw std::runtime_error("Primitive: emitter already registered!");
+        emitter = std::static_pointer_cast<Emitter>(c);
+        emitter->prim = this;
+    } else {
+        throw std::runtime_error("Primitive: invalid child class! Expected Shape.");
+    }
+}
+void Primitive::activate() {
+    if (!shape) throw std::runtime_error("Primitive: defined without a Shape!");
+    if (!material) {
+        auto m = std::make_shared<Matte>(PropertyList());
+        m->activate();
+        material = m;
+    }
+}
+
+// scene.cpp:9-44
+void Scene::addChild(ObjectPtr c) {
+    switch (c->classType()) {
+        case EPrimitive: {
+            auto p = std::static_pointer_cast<Primitive>(c);
+            p->originalIndex = (int)prims.size();
+            prims.push_back(p);
+            if (p->emitter) emitters.push_back(p->emitter);
+            break;
+        }
+        case ECamera:
+            if (camera) throw std::runtime_error("Scene: cannot add multiple cameras!");
+            camera = std::static_pointer_cast<Camera>(c);
+            break;
+        case EIntegrator:
+            if (integrator) throw std::runtime_error("Scene: cannot add multiple integrators!");
+            integrator = std::static_pointer_cast<IntegratorObj>(c);
+            break;
+        case ESampler:
+            if (sampler) throw std::runtime_error("Scene: cannot add multiple samplers!");
+            sampler = std::static_pointer_cast<SamplerObj>(c);
+            break;
+        case EEmitter:
+            throw std::runtime_error("Scene: only area emitters attached to primitives are supported");
+        default:
+            throw std::runtime_error("Scene: cannot add specified child!");
+    }
+}
+// scene.cpp:46-62
+void Scene::activate() {
+    if (!camera) throw std::runtime_error("Scene: no camera specified!");
+    if (!integrator) throw std::runtime_error("Scene: no integrator specified!");
+    if (!sampler) throw std::runtime_error("Scene: no sampler specified!");
+    buildTLAS();
+}
+
+// ---------------------------------------------------------------- registry
+// factory.cpp:17-22 with the class names registered across the reference's plugins
+std::unique_ptr<Object> createInstance(const std::string& t, const PropertyList& p) {
+    if (t == "scene") return std::make_unique<Scene>(p);
+    if (t == "primitive") return std::make_unique<Primitive>(p);
+    if (t == "mesh") return std::make_unique<Mesh>(p);
+    if (t == "sphere") return std::make_unique<Sphere>(p);
+    if (t == "cube") return std::make_unique<Cube>(p);
+    if (t == "matte") return std::make_unique<Matte>(p);
+    if (t == "plastic") return std::make_unique<Plastic>(p);
+    if (t == "conductor") return std::make_unique<Conductor>(p);
+    if (t == "glass") return std::make_unique<Glass>(p);
+    if (t == "index") return std::make_unique<IndexMaterial>(p);
+    if (t == "homogeneous") return std::make_unique<HomogeneousMedium>(p);
+    if (t == "area") return std::make_unique<AreaLight>(p);
+    if (t == "perspective") return std::make_unique<Camera>(p);
+    if (t == "box") return std::make_unique<BoxFilter>(p);
+    if (t == "gaussian") return std::make_unique<GaussianFilter>(p);
+    if (t == "independent") return std::make_unique<SamplerObj>(p);
+    // the GPU drop-ins share the CPU integrators' algorithm
+    if (t == "path" || t == "path_gpu") return std::make_unique<IntegratorObj>(0, p);
+    if (t == "volpath" || t == "volpath_gpu") return std::make_unique<IntegratorObj>(1, p);
+    if (t == "constant_color") return std::make_unique<ConstantTexture<Color>>(p);
+    if (t == "constant_float") return std::make_unique<ConstantTexture<float>>(p);
+    if (t == "checkerboard_color") return std::make_unique<CheckerTexture<Color>>(p);
+    if (t == "checkerboard_float") return std::make_unique<CheckerTexture<float>>(p);
+    throw std::runtime_error("Cannot instantiate object: class '" + t + "' is not registered!");
+}
+
+}  // namespace orc
