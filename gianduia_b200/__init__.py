@@ -1,0 +1,229 @@
+"""gianduia_b200: B200-native radiance path (BVH4 traversal + path/volpath wavefront
+integrators) for Gianduia scenes.
+
+Python binding of the C ABI in include/gnd_gpu.h (libgianduia_b200.so, built in-tree by
+gianduia_b200/build.py). The compute path is the CUDA library only: when no CUDA device
+is usable the GPU calls fail with GpuUnavailable; nothing falls back to the CPU.
+"""
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+from . import build as _build
+
+__all__ = ["lib", "HostScene", "GpuContext", "GndError", "GpuUnavailable", "RAY_DTYPE", "HIT_DTYPE"]
+
+GND_OK = 0
+GND_ERR_NO_DEVICE = 9
+_STATUS = {1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "device check failed",
+           5: "timeout", 6: "parse error", 7: "cancelled", 8: "over HBM budget", 9: "no CUDA device"}
+
+RAY_DTYPE = np.dtype([("o", np.float32, 3), ("tmin", np.float32), ("d", np.float32, 3), ("tmax", np.float32)])
+HIT_DTYPE = np.dtype([("t", np.float32), ("u", np.float32), ("v", np.float32), ("inst", np.int32), ("prim", np.int32)])
+
+
+class GndError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s (status %d: %s)" % (msg, status, _STATUS.get(status, "?")))
+        self.status = status
+
+
+class GpuUnavailable(GndError):
+    pass
+
+
+_lib = None
+_lock = threading.Lock()
+_vp = ctypes.c_void_p
+
+
+def lib():
+    """Loads libgianduia_b200.so (building it first when the sources changed)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            path = _build.build()
+            L = ctypes.CDLL(path)
+            L.gnd_last_error.restype = ctypes.c_char_p
+            L.gnd_version.restype = ctypes.c_char_p
+            for name, args in {
+                "gnd_host_load_xml": [ctypes.c_char_p, ctypes.POINTER(_vp)],
+                "gnd_host_from_triangles": [_vp, ctypes.c_int64, ctypes.POINTER(_vp)],
+                "gnd_host_scene_desc": [_vp, ctypes.POINTER(_vp)],
+                "gnd_host_free": [_vp],
+                "gnd_gpu_create": [ctypes.c_int, ctypes.POINTER(_vp)],
+                "gnd_gpu_destroy": [_vp],
+                "gnd_gpu_scene_upload": [_vp, _vp, ctypes.POINTER(ctypes.c_uint64)],
+                "gnd_gpu_scene_free": [_vp, ctypes.c_uint64],
+                "gnd_gpu_scene_bytes": [_vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)],
+                "gnd_gpu_trace_closest": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp],
+                "gnd_gpu_trace_any": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp],
+                "gnd_gpu_trace_closest_dev": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp, _vp],
+                "gnd_gpu_trace_any_dev": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp, _vp],
+                "gnd_gpu_trace_count_dev": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp, _vp, _vp],
+            }.items():
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = ctypes.c_int32
+            _lib = L
+    return _lib
+
+
+def _check(status, what):
+    if status != GND_OK:
+        msg = "%s: %s" % (what, lib().gnd_last_error().decode(errors="replace"))
+        if status == GND_ERR_NO_DEVICE:
+            raise GpuUnavailable(status, msg)
+        raise GndError(status, msg)
+
+
+class SceneDesc(ctypes.Structure):
+    """Mirror of gnd_scene_desc (read-only view of the render settings)."""
+    _fields_ = [
+        ("nodes", _vp), ("num_nodes", ctypes.c_int64), ("tris", _vp), ("tri_attrs", _vp), ("num_tris", ctypes.c_int64),
+        ("inst_trav", _vp), ("inst_shade", _vp), ("num_instances", ctypes.c_int32), ("tlas_root", ctypes.c_uint32),
+        ("tlas_list", _vp), ("tlas_list_len", ctypes.c_int64), ("materials", _vp), ("num_materials", ctypes.c_int32),
+        ("num_emitters", ctypes.c_int32), ("emitters", _vp), ("media", _vp), ("num_media", ctypes.c_int32),
+        ("num_meshes", ctypes.c_int32), ("meshes", _vp), ("cdf", _vp), ("cdf_len", ctypes.c_int64),
+        ("orig_to_leaf", _vp), ("orig_to_leaf_len", ctypes.c_int64), ("camera", _vp),
+        ("width", ctypes.c_int32), ("height", ctypes.c_int32), ("spp", ctypes.c_int32), ("max_depth", ctypes.c_int32),
+        ("integrator", ctypes.c_int32), ("filter", ctypes.c_int32), ("filter_radius", ctypes.c_float * 2),
+        ("filter_alpha", ctypes.c_float), ("pad", ctypes.c_int32),
+    ]
+
+
+class HostScene:
+    """A scene parsed, BVH-built and flattened by the host framework (no GPU needed)."""
+
+    def __init__(self, handle):
+        self._h = _vp(handle)
+        d = _vp()
+        _check(lib().gnd_host_scene_desc(self._h, ctypes.byref(d)), "gnd_host_scene_desc")
+        self._desc_ptr = d
+        self.desc = SceneDesc.from_address(d.value)
+
+    @staticmethod
+    def load_xml(path):
+        h = _vp()
+        _check(lib().gnd_host_load_xml(os.fsencode(path), ctypes.byref(h)), "gnd_host_load_xml(%s)" % path)
+        return HostScene(h.value)
+
+    @staticmethod
+    def from_triangles(tris):
+        tris = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1, 9)
+        h = _vp()
+        _check(lib().gnd_host_from_triangles(tris.ctypes.data, tris.shape[0], ctypes.byref(h)), "gnd_host_from_triangles")
+        return HostScene(h.value)
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().gnd_host_free(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def width(self):
+        return self.desc.width
+
+    @property
+    def height(self):
+        return self.desc.height
+
+    @property
+    def spp(self):
+        return self.desc.spp
+
+    def nodes(self):
+        """The flattened BVH4 nodes as a structured numpy view (copy)."""
+        dt = np.dtype([("lo_hi", np.float32, (6, 4)), ("child", np.uint32, 4), ("pad", np.uint32, 4)])
+        n = self.desc.num_nodes
+        buf = (ctypes.c_char * (n * 128)).from_address(self.desc.nodes)
+        return np.frombuffer(bytes(buf), dtype=dt)
+
+    def tris(self):
+        n = self.desc.num_tris
+        buf = (ctypes.c_char * (n * 48)).from_address(self.desc.tris)
+        return np.frombuffer(bytes(buf), dtype=np.float32).reshape(n, 12)
+
+    def tlas_list(self):
+        n = self.desc.tlas_list_len
+        return np.ctypeslib.as_array((ctypes.c_uint32 * n).from_address(self.desc.tlas_list)).copy() if n else np.zeros(0, np.uint32)
+
+    def inst_trav(self):
+        n = self.desc.num_instances
+        buf = (ctypes.c_char * (n * 64)).from_address(self.desc.inst_trav)
+        return np.frombuffer(bytes(buf), dtype=np.uint32).reshape(n, 16)
+
+
+def as_rays(arr):
+    """(n, 8) float32 (ox, oy, oz, tmin, dx, dy, dz, tmax) -> contiguous gnd_ray array."""
+    a = np.ascontiguousarray(arr, dtype=np.float32).reshape(-1, 8)
+    return a
+
+
+class GpuContext:
+    """One CUDA device (gnd_gpu_create). Raises GpuUnavailable without a usable B200."""
+
+    def __init__(self, device=0):
+        self._h = _vp()
+        _check(lib().gnd_gpu_create(device, ctypes.byref(self._h)), "gnd_gpu_create")
+        self._scenes = {}
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().gnd_gpu_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def upload(self, host_scene):
+        sid = ctypes.c_uint64()
+        _check(lib().gnd_gpu_scene_upload(self._h, host_scene._desc_ptr, ctypes.byref(sid)), "gnd_gpu_scene_upload")
+        self._scenes[sid.value] = host_scene
+        return sid.value
+
+    def free_scene(self, sid):
+        _check(lib().gnd_gpu_scene_free(self._h, sid), "gnd_gpu_scene_free")
+        self._scenes.pop(sid, None)
+
+    def scene_bytes(self, sid):
+        b = ctypes.c_uint64()
+        _check(lib().gnd_gpu_scene_bytes(self._h, sid, ctypes.byref(b)), "gnd_gpu_scene_bytes")
+        return b.value
+
+    def trace_closest(self, sid, rays):
+        r = as_rays(rays)
+        hits = np.zeros(r.shape[0], HIT_DTYPE)
+        _check(lib().gnd_gpu_trace_closest(self._h, sid, r.ctypes.data, r.shape[0], hits.ctypes.data), "gnd_gpu_trace_closest")
+        return hits
+
+    def trace_any(self, sid, rays):
+        r = as_rays(rays)
+        occ = np.zeros(r.shape[0], np.uint8)
+        _check(lib().gnd_gpu_trace_any(self._h, sid, r.ctypes.data, r.shape[0], occ.ctypes.data), "gnd_gpu_trace_any")
+        return occ.astype(bool)
+
+    # device-pointer variants (pointers as ints, e.g. torch tensor.data_ptr())
+    def trace_closest_dev(self, sid, d_rays, n, d_hits, stream=0):
+        _check(lib().gnd_gpu_trace_closest_dev(self._h, sid, d_rays, n, d_hits, stream or None), "gnd_gpu_trace_closest_dev")
+
+    def trace_any_dev(self, sid, d_rays, n, d_occ, stream=0):
+        _check(lib().gnd_gpu_trace_any_dev(self._h, sid, d_rays, n, d_occ, stream or None), "gnd_gpu_trace_any_dev")
+
+    def trace_count_dev(self, sid, d_rays, n, d_nodes, d_tris, stream=0):
+        _check(lib().gnd_gpu_trace_count_dev(self._h, sid, d_rays, n, d_nodes, d_tris, stream or None), "gnd_gpu_trace_count_dev")

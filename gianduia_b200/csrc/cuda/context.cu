@@ -1,0 +1,185 @@
+// Contexts and resident scenes: gnd_gpu_create/destroy, gnd_gpu_scene_upload/free.
+#include <cstring>
+
+#include "runtime.h"
+#include "wavefront.h"
+
+namespace gnd {
+
+namespace {
+thread_local std::string t_lastError = "no error";
+}
+void setLastError(const std::string& m) { t_lastError = m; }
+const std::string& lastError() { return t_lastError; }
+
+Context::~Context() {
+    if (device >= 0) cudaSetDevice(device);
+    wave.reset();
+    scenes.clear();
+    errWord.release();
+    rayScratch.release();
+    hitScratch.release();
+    if (stream) cudaStreamDestroy(stream);
+}
+
+void Context::checkKernelErrors(const char* what) {
+    uint32_t w = 0;
+    GND_CUDA(cudaMemcpyAsync(&w, errWord.ptr, 4, cudaMemcpyDeviceToHost, stream));
+    GND_CUDA(cudaStreamSynchronize(stream));
+    if (w) {
+        GND_CUDA(cudaMemsetAsync(errWord.ptr, 0, 4, stream));
+        std::string m = std::string(what) + ": device check failed (";
+        if (w & 1) m += " traversal-stack-overflow";
+        if (w & 2) m += " traversal-iteration-limit";
+        if (w & 4) m += " bad-node-reference";
+        if (w & 8) m += " path-queue-overflow";
+        if (w & 16) m += " path-iteration-limit";
+        m += " )";
+        throw Error(GND_ERR_DEVICE_CHECK, m);
+    }
+}
+
+Context* ctxOf(gnd_gpu_ctx* c) {
+    if (!c) throw Error(GND_ERR_INVALID, "null context");
+    return reinterpret_cast<Context*>(c);
+}
+
+namespace {
+template <typename T>
+const T* upload(DeviceScene& ds, cudaStream_t st, const void* src, size_t count) {
+    size_t bytes = count * sizeof(T);
+    ds.bufs.emplace_back(bytes > 0 ? bytes : 16);
+    if (bytes) GND_CUDA(cudaMemcpyAsync(ds.bufs.back().ptr, src, bytes, cudaMemcpyHostToDevice, st));
+    ds.bytes += ds.bufs.back().bytes;
+    return ds.bufs.back().as<T>();
+}
+}  // namespace
+
+}  // namespace gnd
+
+using namespace gnd;
+
+extern "C" {
+
+const char* gnd_last_error(void) { return lastError().c_str(); }
+const char* gnd_version(void) { return "gianduia_b200 1.0 (sm_100a)"; }
+
+gnd_status gnd_gpu_create(int device, gnd_gpu_ctx** out) {
+    return guarded([&]() {
+        if (!out) throw Error(GND_ERR_INVALID, "null output pointer");
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess || n == 0)
+            throw Error(GND_ERR_NO_DEVICE, std::string("no CUDA device available: ") + cudaGetErrorString(e));
+        if (device < 0 || device >= n) throw Error(GND_ERR_INVALID, "device ordinal out of range");
+        auto c = std::make_unique<Context>();
+        c->device = device;
+        c->bind();
+        cudaDeviceProp prop;
+        GND_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10)
+            throw Error(GND_ERR_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100 (this build targets sm_100a)");
+        c->numSMs = prop.multiProcessorCount;
+        GND_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->errWord.alloc(16);
+        GND_CUDA(cudaMemset(c->errWord.ptr, 0, 16));
+        *out = reinterpret_cast<gnd_gpu_ctx*>(c.release());
+    });
+}
+
+gnd_status gnd_gpu_destroy(gnd_gpu_ctx* ctx) {
+    return guarded([&]() { delete ctxOf(ctx); });
+}
+
+gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_scene_id* out) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (!d || !out) throw Error(GND_ERR_INVALID, "null scene description");
+        if (d->num_instances < 0 || d->num_nodes < 0 || d->num_tris < 0) throw Error(GND_ERR_INVALID, "negative sizes");
+        if (d->num_tris >= (int64_t)kLeafFirstMask) throw Error(GND_ERR_INVALID, "too many triangles");
+        // host-side validation of every reference stored in the tree (a corrupted index
+        // is refused here rather than read out of bounds on the device)
+        const Node4* nodes = reinterpret_cast<const Node4*>(d->nodes);
+        for (int64_t i = 0; i < d->num_nodes; ++i) {
+            for (int k = 0; k < 4; ++k) {
+                uint32_t r = nodes[i].child[k];
+                if (r == kEmpty) continue;
+                if (!isLeaf(r)) {
+                    if ((int64_t)r >= d->num_nodes) throw Error(GND_ERR_INVALID, "node reference out of range");
+                } else if ((int64_t)(leafFirst(r) + leafCount(r)) > std::max<int64_t>(d->num_tris, d->tlas_list_len)) {
+                    throw Error(GND_ERR_INVALID, "leaf range out of range");
+                }
+            }
+        }
+        if (d->tlas_root != kEmpty && (int64_t)d->tlas_root >= d->num_nodes) throw Error(GND_ERR_INVALID, "bad top-level root");
+        for (int64_t i = 0; i < d->tlas_list_len; ++i)
+            if ((int64_t)d->tlas_list[i] >= d->num_instances) throw Error(GND_ERR_INVALID, "instance list out of range");
+        const InstTrav* it = reinterpret_cast<const InstTrav*>(d->inst_trav);
+        const InstShade* is = reinterpret_cast<const InstShade*>(d->inst_shade);
+        for (int i = 0; i < d->num_instances; ++i) {
+            if (it[i].kind == kShapeMesh && it[i].blasRoot != kEmpty && (int64_t)it[i].blasRoot >= d->num_nodes)
+                throw Error(GND_ERR_INVALID, "instance root out of range");
+            if (is[i].material < 0 || is[i].material >= d->num_materials) throw Error(GND_ERR_INVALID, "instance material out of range");
+            if (is[i].emitter >= d->num_emitters) throw Error(GND_ERR_INVALID, "instance emitter out of range");
+            if (is[i].mediumIn >= d->num_media || is[i].mediumOut >= d->num_media) throw Error(GND_ERR_INVALID, "instance medium out of range");
+        }
+        c->bind();
+        std::lock_guard<std::mutex> lk(c->mu);
+        auto ds = std::make_unique<DeviceScene>();
+        SceneView& v = ds->view;
+        v.nodes = upload<Node4>(*ds, c->stream, d->nodes, d->num_nodes);
+        v.tris = upload<Tri>(*ds, c->stream, d->tris, d->num_tris);
+        v.attrs = upload<TriAttr>(*ds, c->stream, d->tri_attrs, d->num_tris);
+        v.instT = upload<InstTrav>(*ds, c->stream, d->inst_trav, d->num_instances);
+        v.instS = upload<InstShade>(*ds, c->stream, d->inst_shade, d->num_instances);
+        v.tlasList = upload<uint32_t>(*ds, c->stream, d->tlas_list, d->tlas_list_len);
+        v.materials = upload<Material>(*ds, c->stream, d->materials, d->num_materials);
+        v.emitters = upload<Emitter>(*ds, c->stream, d->emitters, d->num_emitters);
+        v.media = upload<Medium>(*ds, c->stream, d->media, d->num_media);
+        v.meshes = upload<MeshRec>(*ds, c->stream, d->meshes, d->num_meshes);
+        v.cdf = upload<float>(*ds, c->stream, d->cdf, d->cdf_len);
+        v.origToLeaf = upload<uint32_t>(*ds, c->stream, d->orig_to_leaf, d->orig_to_leaf_len);
+        v.tlasRoot = d->tlas_root;
+        v.numEmitters = d->num_emitters;
+        v.numInstances = d->num_instances;
+        if (d->camera) std::memcpy(&v.camera, d->camera, sizeof(Camera));
+        // null-BSDF mask per instance
+        std::vector<uint8_t> mask(std::max(1, d->num_instances), 0);
+        const Material* mats = reinterpret_cast<const Material*>(d->materials);
+        for (int i = 0; i < d->num_instances; ++i)
+            if (mats[is[i].material].type == kMatIndex) { mask[i] = 1; ds->hasNullMaterials = true; }
+        ds->nullMask.alloc(mask.size());
+        GND_CUDA(cudaMemcpyAsync(ds->nullMask.ptr, mask.data(), mask.size(), cudaMemcpyHostToDevice, c->stream));
+        ds->viewDev.alloc(sizeof(SceneView));
+        GND_CUDA(cudaMemcpyAsync(ds->viewDev.ptr, &v, sizeof(SceneView), cudaMemcpyHostToDevice, c->stream));
+        GND_CUDA(cudaStreamSynchronize(c->stream));
+        ds->bytes += ds->nullMask.bytes + ds->viewDev.bytes;
+        ds->width = d->width; ds->height = d->height; ds->spp = d->spp; ds->maxDepth = d->max_depth;
+        ds->integrator = d->integrator; ds->filter = d->filter;
+        ds->filterRadius[0] = d->filter_radius[0]; ds->filterRadius[1] = d->filter_radius[1];
+        ds->filterAlpha = d->filter_alpha;
+        ds->numMaterials = d->num_materials;
+        uint64_t id = c->nextScene++;
+        c->scenes[id] = std::move(ds);
+        *out = id;
+    });
+}
+
+gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctxh, gnd_scene_id id) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        c->bind();
+        std::lock_guard<std::mutex> lk(c->mu);
+        if (!c->scenes.erase(id)) throw Error(GND_ERR_INVALID, "unknown scene id");
+    });
+}
+
+gnd_status gnd_gpu_scene_bytes(gnd_gpu_ctx* ctxh, gnd_scene_id id, uint64_t* bytes) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        std::lock_guard<std::mutex> lk(c->mu);
+        *bytes = c->scene(id).bytes;
+    });
+}
+
+}  // extern "C"

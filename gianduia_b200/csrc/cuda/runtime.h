@@ -1,0 +1,125 @@
+// Device runtime: contexts, resident scenes, status/error plumbing shared by the
+// C-ABI entry points.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "gnd/layout.h"
+#include "gnd_gpu.h"
+
+namespace gnd {
+
+// Error carrying a gnd_status; converted to a status code at the ABI.
+struct Error : std::runtime_error {
+    gnd_status code;
+    Error(gnd_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void setLastError(const std::string& msg);
+const std::string& lastError();
+
+#define GND_CUDA(call)                                                                                     \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) {                                                                           \
+            if (e_ == cudaErrorMemoryAllocation)                                                           \
+                throw ::gnd::Error(GND_ERR_OOM, std::string("out of device memory: ") + #call);            \
+            throw ::gnd::Error(GND_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));          \
+        }                                                                                                  \
+    } while (0)
+
+// Runs an ABI body, mapping exceptions to a status.
+template <typename F>
+gnd_status guarded(F&& f) {
+    try {
+        f();
+        return GND_OK;
+    } catch (const Error& e) {
+        setLastError(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        setLastError("host allocation failed");
+        return GND_ERR_OOM;
+    } catch (const std::exception& e) {
+        setLastError(e.what());
+        return GND_ERR_INVALID;
+    }
+}
+
+// A device allocation with RAII ownership.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t n) { alloc(n); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); ptr = o.ptr; bytes = o.bytes; o.ptr = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(size_t n) {
+        release();
+        if (n == 0) return;
+        GND_CUDA(cudaMalloc(&ptr, n));
+        bytes = n;
+    }
+    void ensure(size_t n) { if (n > bytes) alloc(n); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <typename T>
+    T* as() const { return reinterpret_cast<T*>(ptr); }
+};
+
+// A scene resident in HBM.
+struct DeviceScene {
+    std::vector<DevBuf> bufs;
+    SceneView view{};
+    DevBuf nullMask;          // per instance: 1 when the material has no BSDF (index)
+    DevBuf viewDev;           // SceneView copy in device memory
+    uint64_t bytes = 0;
+    int width = 0, height = 0, spp = 1, maxDepth = 1000, integrator = 0, filter = 0;
+    float filterRadius[2] = {0.5f, 0.5f}, filterAlpha = 2.f;
+    bool hasNullMaterials = false;
+    int numMaterials = 0;
+};
+
+class Wavefront;
+
+struct Context {
+    int device = 0;
+    int numSMs = 148;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::map<uint64_t, std::unique_ptr<DeviceScene>> scenes;
+    uint64_t nextScene = 1;
+    DevBuf errWord;           // device error bitmask written by kernels
+    DevBuf rayScratch, hitScratch;
+    std::unique_ptr<Wavefront> wave;
+    volatile bool cancel = false;
+    ~Context();
+    DeviceScene& scene(uint64_t id) {
+        auto it = scenes.find(id);
+        if (it == scenes.end()) throw Error(GND_ERR_INVALID, "unknown scene id " + std::to_string(id));
+        return *it->second;
+    }
+    void bind() { GND_CUDA(cudaSetDevice(device)); }
+    // Reads and clears the kernel error word; throws on a tripped device check.
+    void checkKernelErrors(const char* what);
+};
+
+Context* ctxOf(gnd_gpu_ctx* c);
+
+}  // namespace gnd

@@ -1,0 +1,142 @@
+// Ray-batch queries: gnd_gpu_trace_closest / _any / _count (Scene::rayIntersect for a
+// batch). One thread per ray, persistent grid sized to the SM count.
+#include "runtime.h"
+#include "traverse.cuh"
+
+namespace gnd {
+
+constexpr int kTraceBlock = 128;
+
+template <bool ANY, bool COUNT>
+__global__ void __launch_bounds__(kTraceBlock) traceKernel(SceneView s, const gnd_ray* __restrict__ rays, int64_t n,
+                                                           gnd_hit* __restrict__ hits, uint8_t* __restrict__ occ,
+                                                           uint32_t* __restrict__ nodesOut, uint32_t* __restrict__ trisOut,
+                                                           uint32_t* errWord) {
+    __shared__ uint32_t stack[kStackSize * kTraceBlock];
+    uint32_t* stk = stack + threadIdx.x;
+    int err = 0;
+    for (int64_t i = (int64_t)blockIdx.x * kTraceBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kTraceBlock) {
+        float4 a = __ldg(reinterpret_cast<const float4*>(rays + i));
+        float4 b = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
+        TRay r;
+        r.o = v3(a.x, a.y, a.z);
+        r.tmin = a.w;
+        r.d = v3(b.x, b.y, b.z);
+        r.tmax = b.w;
+        THit h;
+        TraceCounters cnt{0, 0};
+        err |= traceRay<kTraceBlock, ANY, false, COUNT>(s, r, h, stk, &cnt, nullptr);
+        if (COUNT) {
+            nodesOut[i] = cnt.nodes;
+            trisOut[i] = cnt.tris;
+        } else if (ANY) {
+            occ[i] = h.inst >= 0 ? 1 : 0;
+        } else {
+            gnd_hit o;
+            o.t = h.t;
+            o.u = h.u;
+            o.v = h.v;
+            o.inst = h.inst;
+            o.prim = (h.inst >= 0 && h.slot != 0xFFFFFFFFu) ? (int32_t)__ldg(&s.tris[h.slot].prim) : -1;
+            hits[i] = o;
+        }
+    }
+    if (err) atomicOr(errWord, (uint32_t)err);
+}
+
+namespace {
+int traceGrid(Context* c, int64_t n) {
+    int64_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
+    int64_t cap = (int64_t)c->numSMs * 16;
+    return (int)std::max<int64_t>(1, std::min(blocks, cap));
+}
+
+void launchTrace(Context* c, DeviceScene& ds, const gnd_ray* dr, int64_t n, gnd_hit* dh, uint8_t* docc,
+                 uint32_t* dn, uint32_t* dt, cudaStream_t st) {
+    if (n <= 0) return;
+    int g = traceGrid(c, n);
+    uint32_t* ew = c->errWord.as<uint32_t>();
+    if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(ds.view, dr, n, nullptr, nullptr, dn, dt, ew);
+    else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(ds.view, dr, n, nullptr, docc, nullptr, nullptr, ew);
+    else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(ds.view, dr, n, dh, nullptr, nullptr, nullptr, ew);
+    GND_CUDA(cudaGetLastError());
+}
+
+// Host-buffer variant: copies in, traces, copies out (pinned staging is the caller's
+// concern; pageable memory works, at lower copy bandwidth).
+void traceHost(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_ray* rays, int64_t n, gnd_hit* hits, uint8_t* occ) {
+    Context* c = ctxOf(ctxh);
+    if (n < 0 || (n > 0 && (!rays || (!hits && !occ)))) throw Error(GND_ERR_INVALID, "bad ray batch arguments");
+    c->bind();
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceScene& ds = c->scene(id);
+    if (n == 0) return;
+    size_t outBytes = hits ? sizeof(gnd_hit) * (size_t)n : (size_t)n;
+    c->rayScratch.ensure(sizeof(gnd_ray) * (size_t)n);
+    c->hitScratch.ensure(outBytes);
+    GND_CUDA(cudaMemcpyAsync(c->rayScratch.ptr, rays, sizeof(gnd_ray) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    launchTrace(c, ds, c->rayScratch.as<gnd_ray>(), n, hits ? c->hitScratch.as<gnd_hit>() : nullptr,
+                hits ? nullptr : c->hitScratch.as<uint8_t>(), nullptr, nullptr, c->stream);
+    GND_CUDA(cudaMemcpyAsync(hits ? (void*)hits : (void*)occ, c->hitScratch.ptr, outBytes, cudaMemcpyDeviceToHost, c->stream));
+    GND_CUDA(cudaStreamSynchronize(c->stream));
+    c->checkKernelErrors("trace");
+}
+}  // namespace
+
+}  // namespace gnd
+
+using namespace gnd;
+
+extern "C" {
+
+gnd_status gnd_gpu_trace_closest(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* rays, int64_t n, gnd_hit* hits) {
+    return guarded([&]() {
+        if (!hits && n > 0) throw Error(GND_ERR_INVALID, "null hit buffer");
+        traceHost(ctx, scene, rays, n, hits, nullptr);
+    });
+}
+
+gnd_status gnd_gpu_trace_any(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* rays, int64_t n, uint8_t* occluded) {
+    return guarded([&]() {
+        if (!occluded && n > 0) throw Error(GND_ERR_INVALID, "null output buffer");
+        traceHost(ctx, scene, rays, n, nullptr, occluded);
+    });
+}
+
+gnd_status gnd_gpu_trace_closest_dev(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_ray* d_rays, int64_t n, gnd_hit* d_hits,
+                                     void* stream) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (n < 0 || (n > 0 && (!d_rays || !d_hits))) throw Error(GND_ERR_INVALID, "bad ray batch arguments");
+        c->bind();
+        std::lock_guard<std::mutex> lk(c->mu);
+        cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+        launchTrace(c, c->scene(id), d_rays, n, d_hits, nullptr, nullptr, nullptr, st);
+    });
+}
+
+gnd_status gnd_gpu_trace_any_dev(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_ray* d_rays, int64_t n, uint8_t* d_occ,
+                                 void* stream) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (n < 0 || (n > 0 && (!d_rays || !d_occ))) throw Error(GND_ERR_INVALID, "bad ray batch arguments");
+        c->bind();
+        std::lock_guard<std::mutex> lk(c->mu);
+        cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+        launchTrace(c, c->scene(id), d_rays, n, nullptr, d_occ, nullptr, nullptr, st);
+    });
+}
+
+gnd_status gnd_gpu_trace_count_dev(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_ray* d_rays, int64_t n, uint32_t* d_nodes,
+                                   uint32_t* d_tris, void* stream) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (n < 0 || (n > 0 && (!d_rays || !d_nodes || !d_tris))) throw Error(GND_ERR_INVALID, "bad ray batch arguments");
+        c->bind();
+        std::lock_guard<std::mutex> lk(c->mu);
+        cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+        launchTrace(c, c->scene(id), d_rays, n, nullptr, nullptr, d_nodes, d_tris, st);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,758 @@
+// Host scene framework: matrices, the plugin registry and the scene objects, and the
+// flattening of a scene into the device layout (BLAS per unique mesh, TLAS over the
+// primitives, material / emitter / medium tables, area CDFs, camera).
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <unordered_map>
+
+#include "hscene.h"
+
+namespace gndh {
+
+// ---------------------------------------------------------------- matrices
+Mat4 Mat4::identity() {
+    Mat4 m;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) m.c[i][j] = (i == j) ? 1.f : 0.f;
+    return m;
+}
+void Mat4::mulVec(const float v[4], float out[4]) const {
+    for (int r = 0; r < 4; ++r) {
+        float add0 = c[0][r] * v[0] + c[1][r] * v[1];
+        float add1 = c[2][r] * v[2] + c[3][r] * v[3];
+        out[r] = add0 + add1;
+    }
+}
+Mat4 Mat4::operator*(const Mat4& b) const {
+    Mat4 m;
+    for (int col = 0; col < 4; ++col) mulVec(b.c[col], m.c[col]);
+    return m;
+}
+Mat4 Mat4::transpose() const {
+    Mat4 m;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) m.c[i][j] = c[j][i];
+    return m;
+}
+bool Mat4::operator==(const Mat4& o) const { return std::memcmp(c, o.c, sizeof(c)) == 0; }
+gnd::Xf34 Mat4::toXf34() const {
+    gnd::Xf34 x;
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 4; ++k) x.r[r][k] = c[k][r];
+    return x;
+}
+Mat4 inverse(const Mat4& mm) {
+    float a[4][4], inv[4][4];
+    for (int r = 0; r < 4; ++r)
+        for (int k = 0; k < 4; ++k) a[r][k] = mm.c[k][r];
+    for (int r = 0; r < 4; ++r) {
+        for (int k = 0; k < 4; ++k) {
+            float s[3][3];
+            int si = 0;
+            for (int i = 0; i < 4; ++i) {
+                if (i == k) continue;
+                int sj = 0;
+                for (int j = 0; j < 4; ++j) {
+                    if (j == r) continue;
+                    s[si][sj++] = a[i][j];
+                }
+                ++si;
+            }
+            float d3 = s[0][0] * (s[1][1] * s[2][2] - s[1][2] * s[2][1]) - s[0][1] * (s[1][0] * s[2][2] - s[1][2] * s[2][0]) +
+                       s[0][2] * (s[1][0] * s[2][1] - s[1][1] * s[2][0]);
+            inv[r][k] = ((r + k) & 1) ? -d3 : d3;
+        }
+    }
+    float det = a[0][0] * inv[0][0] + a[0][1] * inv[1][0] + a[0][2] * inv[2][0] + a[0][3] * inv[3][0];
+    float invDet = 1.0f / det;
+    Mat4 out;
+    for (int r = 0; r < 4; ++r)
+        for (int k = 0; k < 4; ++k) out.c[k][r] = inv[r][k] * invDet;
+    return out;
+}
+V3 Transform::point(V3 p) const {
+    float in[4] = {p.x, p.y, p.z, 1.f}, o[4];
+    m.mulVec(in, o);
+    if (o[3] == 1.0f) return gnd::v3(o[0], o[1], o[2]);
+    return gnd::v3(o[0] / o[3], o[1] / o[3], o[2] / o[3]);
+}
+V3 Transform::vector(V3 v) const {
+    float in[4] = {v.x, v.y, v.z, 0.f}, o[4];
+    m.mulVec(in, o);
+    return gnd::v3(o[0], o[1], o[2]);
+}
+Transform Transform::translate(V3 d) {
+    Mat4 a = Mat4::identity(), b = Mat4::identity();
+    a.c[3][0] = d.x; a.c[3][1] = d.y; a.c[3][2] = d.z;
+    b.c[3][0] = -d.x; b.c[3][1] = -d.y; b.c[3][2] = -d.z;
+    return Transform(a, b);
+}
+Transform Transform::scale(float x, float y, float z) {
+    Mat4 a = Mat4::identity(), b = Mat4::identity();
+    a.c[0][0] = x; a.c[1][1] = y; a.c[2][2] = z;
+    b.c[0][0] = 1.f / x; b.c[1][1] = 1.f / y; b.c[2][2] = 1.f / z;
+    return Transform(a, b);
+}
+// Rodrigues rotation about the normalised axis; inverse = transpose (transform.h:421-426)
+Transform Transform::rotate(float degrees, V3 axis) {
+    float rad = degrees * 0.01745329251994329576923690768489f;
+    float c = std::cos(rad), s = std::sin(rad);
+    V3 ax = gnd::normalize(axis);
+    V3 tp = ax * (1.0f - c);
+    Mat4 m = Mat4::identity();
+    m.c[0][0] = c + tp.x * ax.x;
+    m.c[0][1] = tp.x * ax.y + s * ax.z;
+    m.c[0][2] = tp.x * ax.z - s * ax.y;
+    m.c[1][0] = tp.y * ax.x - s * ax.z;
+    m.c[1][1] = c + tp.y * ax.y;
+    m.c[1][2] = tp.y * ax.z + s * ax.x;
+    m.c[2][0] = tp.z * ax.x + s * ax.y;
+    m.c[2][1] = tp.z * ax.y - s * ax.x;
+    m.c[2][2] = c + tp.z * ax.z;
+    return Transform(m, m.transpose());
+}
+// Right-handed view matrix; camera-to-world is its inverse (transform.h:428-431)
+Transform Transform::lookAt(V3 pos, V3 target, V3 up) {
+    V3 f = gnd::normalize(target - pos);
+    V3 s = gnd::normalize(gnd::cross(f, up));
+    V3 u = gnd::cross(s, f);
+    Mat4 v = Mat4::identity();
+    v.c[0][0] = s.x; v.c[1][0] = s.y; v.c[2][0] = s.z;
+    v.c[0][1] = u.x; v.c[1][1] = u.y; v.c[2][1] = u.z;
+    v.c[0][2] = -f.x; v.c[1][2] = -f.y; v.c[2][2] = -f.z;
+    v.c[3][0] = -gnd::dot(s, pos); v.c[3][1] = -gnd::dot(u, pos); v.c[3][2] = gnd::dot(f, pos);
+    return Transform(gndh::inverse(v), v);
+}
+
+// ---------------------------------------------------------------- registry
+const char* classTypeToString(EClassType t) {
+    switch (t) {
+        case EScene: return "scene";
+        case EPrimitive: return "primitive";
+        case EShape: return "shape";
+        case ECamera: return "camera";
+        case EIntegrator: return "integrator";
+        case ESampler: return "sampler";
+        case ETexture: return "texture";
+        case EMaterial: return "material";
+        case EEmitter: return "emitter";
+        case EFilter: return "filter";
+        case EMedium: return "medium";
+    }
+    return "unknown";
+}
+GndFactory* GndFactory::getInstance() {
+    static GndFactory f;
+    return &f;
+}
+void GndFactory::registerClass(const std::string& name, const ObjectFactory& f) { m_ctors[name] = f; }
+std::unique_ptr<GndObject> GndFactory::createInstance(const std::string& name, const PropertyList& props) {
+    auto it = m_ctors.find(name);
+    if (it == m_ctors.end()) throw std::runtime_error("Cannot instantiate object: class '" + name + "' is not registered!");
+    return it->second(props);
+}
+
+// ---------------------------------------------------------------- textures
+namespace {
+gnd::ColorTex constColor(V3 v) {
+    gnd::ColorTex t{};
+    t.kind = 0;
+    t.v1[0] = v.x; t.v1[1] = v.y; t.v1[2] = v.z;
+    t.scale[0] = t.scale[1] = 1.f;
+    return t;
+}
+// matte.cpp:33-43, area.cpp:31-43: the magenta "missing texture" checkerboard
+gnd::ColorTex missingTexture() {
+    gnd::ColorTex t{};
+    t.kind = 1;
+    t.v1[0] = t.v1[1] = t.v1[2] = 0.f;
+    t.v2[0] = 1.f; t.v2[1] = 0.f; t.v2[2] = 1.f;
+    t.scale[0] = t.scale[1] = 0.1f;
+    return t;
+}
+}  // namespace
+
+// constant.h:9-32
+struct ConstantColor : ColorTexture {
+    explicit ConstantColor(const PropertyList& p) { rec = constColor(p.getColor("value", gnd::v3s(1.f))); }
+};
+struct ConstantFloat : FloatTexture {
+    explicit ConstantFloat(const PropertyList& p) { value = p.getFloat("value", 1.0f); }
+};
+// checkerboard.h:20-48
+struct CheckerboardColor : ColorTexture {
+    explicit CheckerboardColor(const PropertyList& p) {
+        V3 a = p.getColor("value1", gnd::v3s(1.f)), b = p.getColor("value2", gnd::v3s(0.f));
+        V2 sc = p.getVector2("scale", V2{1.f, 1.f}), de = p.getPoint2("delta", V2{0.f, 0.f});
+        rec.kind = 1;
+        rec.v1[0] = a.x; rec.v1[1] = a.y; rec.v1[2] = a.z;
+        rec.v2[0] = b.x; rec.v2[1] = b.y; rec.v2[2] = b.z;
+        rec.scale[0] = sc.x; rec.scale[1] = sc.y;
+        rec.delta[0] = de.x; rec.delta[1] = de.y;
+    }
+};
+GND_REGISTER_CLASS(ConstantColor, "constant_color")
+GND_REGISTER_CLASS(ConstantFloat, "constant_float")
+GND_REGISTER_CLASS(CheckerboardColor, "checkerboard_color")
+
+// ---------------------------------------------------------------- media
+// homogeneous.cpp:14-20
+struct HomogeneousMediumObj : MediumObj {
+    explicit HomogeneousMediumObj(const PropertyList& p) {
+        V3 a = p.getColor("sigma_a", gnd::v3s(0.1f)), s = p.getColor("sigma_s", gnd::v3s(0.1f));
+        V3 t = a + s;
+        rec.sigA[0] = a.x; rec.sigA[1] = a.y; rec.sigA[2] = a.z;
+        rec.sigS[0] = s.x; rec.sigS[1] = s.y; rec.sigS[2] = s.z;
+        rec.sigT[0] = t.x; rec.sigT[1] = t.y; rec.sigT[2] = t.z;
+        rec.g = p.getFloat("g", 0.0f);
+    }
+};
+GND_REGISTER_CLASS(HomogeneousMediumObj, "homogeneous")
+
+// ---------------------------------------------------------------- materials
+// material.h:36-59 (normal and bump maps are not part of the GPU path)
+void MaterialObj::addChild(std::shared_ptr<GndObject> c) {
+    if (c->getClassType() == EMedium && c->getName() == "inside") {
+        if (inside) throw std::runtime_error("Material: inside medium already defined!");
+        inside = std::static_pointer_cast<MediumObj>(c);
+    } else if (c->getClassType() == EMedium && c->getName() == "outside") {
+        if (outside) throw std::runtime_error("Material: outside medium already defined!");
+        outside = std::static_pointer_cast<MediumObj>(c);
+    } else {
+        throw std::runtime_error("Material: cannot add specified child (" + c->getName() + ")!");
+    }
+}
+
+namespace {
+void setColorSlot(gnd::ColorTex& slot, bool& have, const std::shared_ptr<GndObject>& c) {
+    auto t = std::dynamic_pointer_cast<ColorTexture>(c);
+    if (!t) throw std::runtime_error("Material: texture '" + c->getName() + "' must be a color texture");
+    slot = t->rec;
+    have = true;
+}
+void setFloatSlot(float& slot, bool& have, const std::shared_ptr<GndObject>& c) {
+    auto t = std::dynamic_pointer_cast<FloatTexture>(c);
+    if (!t) throw std::runtime_error("Material: texture '" + c->getName() + "' must be a constant float texture");
+    slot = t->value;
+    have = true;
+}
+}  // namespace
+
+// matte.cpp:7-53
+struct MatteMat : MaterialObj {
+    bool hasA = false;
+    explicit MatteMat(const PropertyList& p) {
+        rec.type = gnd::kMatMatte;
+        if (p.hasColor("albedo")) { rec.a = constColor(p.getColor("albedo", gnd::v3s(0.f))); hasA = true; }
+    }
+    void addChild(std::shared_ptr<GndObject> c) override {
+        if (c->getClassType() != ETexture) return MaterialObj::addChild(c);
+        if (c->getName() == "albedo") {
+            if (hasA) throw std::runtime_error("Matte: there's already an albedo defined!");
+            setColorSlot(rec.a, hasA, c);
+        } else MaterialObj::addChild(c);
+    }
+    void activate() override { if (!hasA) rec.a = missingTexture(); }
+};
+// plastic.cpp:8-91
+struct PlasticMat : MaterialObj {
+    bool hKd = false, hKs = false, hR = false, hE = false;
+    explicit PlasticMat(const PropertyList& p) {
+        rec.type = gnd::kMatPlastic;
+        if (p.hasColor("Kd")) { rec.a = constColor(p.getColor("Kd", gnd::v3s(0.f))); hKd = true; }
+        if (p.hasColor("Ks")) { rec.b = constColor(p.getColor("Ks", gnd::v3s(0.f))); hKs = true; }
+        if (p.hasFloat("roughness")) { rec.roughness = p.getFloat("roughness"); hR = true; }
+        if (p.hasFloat("eta")) { rec.eta = p.getFloat("eta"); hE = true; }
+    }
+    void addChild(std::shared_ptr<GndObject> c) override {
+        if (c->getClassType() != ETexture) return;   // plastic.cpp:30
+        const std::string& n = c->getName();
+        if (n == "Kd") setColorSlot(rec.a, hKd, c);
+        else if (n == "Ks") setColorSlot(rec.b, hKs, c);
+        else if (n == "roughness") setFloatSlot(rec.roughness, hR, c);
+        else if (n == "eta") setFloatSlot(rec.eta, hE, c);
+        else MaterialObj::addChild(c);
+    }
+    void activate() override {
+        if (!hKd) rec.a = constColor(gnd::v3s(0.25f));
+        if (!hKs) rec.b = constColor(gnd::v3s(0.25f));
+        if (!hR) rec.roughness = 0.1f;
+        if (!hE) rec.eta = 1.5f;
+    }
+};
+// conductor.cpp:9-120
+struct ConductorMat : MaterialObj {
+    bool hR = false, hE = false, hK = false, hRo = false;
+    V3 eta{1, 1, 1}, k{1, 1, 1};
+    explicit ConductorMat(const PropertyList& p) {
+        rec.type = gnd::kMatConductor;
+        if (p.hasColor("R")) { rec.a = constColor(p.getColor("R", gnd::v3s(0.f))); hR = true; }
+        if (p.hasColor("eta")) { eta = p.getColor("eta", eta); hE = true; }
+        if (p.hasColor("k")) { k = p.getColor("k", k); hK = true; }
+        if (p.hasFloat("roughness")) { rec.roughness = p.getFloat("roughness"); hRo = true; }
+    }
+    void addChild(std::shared_ptr<GndObject> c) override {
+        if (c->getClassType() != ETexture) throw std::runtime_error("Conductor: cannot add specified child!");
+        const std::string& n = c->getName();
+        if (n == "R") setColorSlot(rec.a, hR, c);
+        else if (n == "roughness") setFloatSlot(rec.roughness, hRo, c);
+        else if (n == "eta" || n == "k") {
+            auto t = std::dynamic_pointer_cast<ColorTexture>(c);
+            if (!t || t->rec.kind != 0) throw std::runtime_error("Conductor: eta/k must be constant colors");
+            V3 v = gnd::v3(t->rec.v1[0], t->rec.v1[1], t->rec.v1[2]);
+            if (n == "eta") { eta = v; hE = true; } else { k = v; hK = true; }
+        } else MaterialObj::addChild(c);
+    }
+    void activate() override {
+        if (!hR) rec.a = constColor(gnd::v3s(1.f));
+        if (!hRo) rec.roughness = 0.f;
+        rec.condEta[0] = eta.x; rec.condEta[1] = eta.y; rec.condEta[2] = eta.z;
+        rec.condK[0] = k.x; rec.condK[1] = k.y; rec.condK[2] = k.z;
+    }
+};
+// glass.cpp:8-115
+struct GlassMat : MaterialObj {
+    bool hR = false, hT = false, hRo = false, hE = false;
+    explicit GlassMat(const PropertyList& p) {
+        rec.type = gnd::kMatGlass;
+        if (p.hasColor("R")) { rec.a = constColor(p.getColor("R", gnd::v3s(0.f))); hR = true; }
+        if (p.hasColor("T")) { rec.b = constColor(p.getColor("T", gnd::v3s(0.f))); hT = true; }
+        if (p.hasFloat("roughness")) { rec.roughness = p.getFloat("roughness"); hRo = true; }
+        if (p.hasFloat("eta")) { rec.eta = p.getFloat("eta"); hE = true; }
+    }
+    void addChild(std::shared_ptr<GndObject> c) override {
+        const std::string& n = c->getName();
+        if (n == "R") setColorSlot(rec.a, hR, c);
+        else if (n == "T") setColorSlot(rec.b, hT, c);
+        else if (n == "roughness") setFloatSlot(rec.roughness, hRo, c);
+        else if (n == "eta") setFloatSlot(rec.eta, hE, c);
+        else MaterialObj::addChild(c);
+    }
+    void activate() override {
+        if (!hR) rec.a = constColor(gnd::v3s(1.f));
+        if (!hT) rec.b = constColor(gnd::v3s(1.f));
+        if (!hRo) rec.roughness = 0.f;
+        if (!hE) rec.eta = 1.5f;
+    }
+};
+// index.cpp:6-16 (null BSDF: medium boundary only)
+struct IndexMat : MaterialObj {
+    explicit IndexMat(const PropertyList&) { rec.type = gnd::kMatIndex; }
+};
+GND_REGISTER_CLASS(MatteMat, "matte")
+GND_REGISTER_CLASS(PlasticMat, "plastic")
+GND_REGISTER_CLASS(ConductorMat, "conductor")
+GND_REGISTER_CLASS(GlassMat, "glass")
+GND_REGISTER_CLASS(IndexMat, "index")
+
+// ---------------------------------------------------------------- emitter
+// area.cpp:7-43
+void EmitterObj::addChild(std::shared_ptr<GndObject> c) {
+    if (c->getClassType() != ETexture) throw std::runtime_error("AreaLight: cannot add specified child!");
+    if (c->getName() == "radiance") {
+        if (hasRadiance) throw std::runtime_error("AreaLight: there's already a radiance value defined!");
+        setColorSlot(radiance, hasRadiance, c);
+    }
+}
+void EmitterObj::activate() { if (!hasRadiance) radiance = missingTexture(); }
+struct AreaLightObj : EmitterObj {
+    explicit AreaLightObj(const PropertyList& p) {
+        if (p.hasColor("radiance")) { radiance = constColor(p.getColor("radiance", gnd::v3s(0.f))); hasRadiance = true; }
+    }
+};
+GND_REGISTER_CLASS(AreaLightObj, "area")
+
+// ---------------------------------------------------------------- shapes
+Bounds ShapeObj::objectBounds() const {
+    Bounds b;
+    if (kind == gnd::kShapeSphere) {
+        b.lo = gnd::v3s(-radius); b.hi = gnd::v3s(radius);
+    } else if (kind == gnd::kShapeCube) {
+        b.lo = -extents; b.hi = extents;
+    } else {
+        for (const V3& p : positions) b.grow(p);
+    }
+    return b;
+}
+void ShapeObj::activate() {
+    if (kind != gnd::kShapeMesh) return;
+    if (!positions.empty()) return;   // geometry supplied in memory
+    if (filename.empty()) throw std::runtime_error("Mesh: filename missing!");
+    loadOBJ(filename, *this);
+    if (positions.empty()) throw std::runtime_error("Mesh: no geometry loaded!");
+}
+struct MeshShape : ShapeObj {
+    explicit MeshShape(const PropertyList& p) { kind = gnd::kShapeMesh; filename = p.getString("filename", ""); }
+};
+struct SphereShape : ShapeObj {
+    explicit SphereShape(const PropertyList& p) { kind = gnd::kShapeSphere; radius = p.getFloat("radius", 1.0f); }
+};
+struct CubeShape : ShapeObj {
+    explicit CubeShape(const PropertyList& p) { kind = gnd::kShapeCube; extents = p.getVector3("extents", gnd::v3s(1.f)); }
+};
+GND_REGISTER_CLASS(MeshShape, "mesh")
+GND_REGISTER_CLASS(SphereShape, "sphere")
+GND_REGISTER_CLASS(CubeShape, "cube")
+
+// ---------------------------------------------------------------- primitive
+// primitive.cpp:7-46 (static transforms: toWorldEnd must equal toWorld)
+PrimitiveObj::PrimitiveObj(const PropertyList& p) {
+    toWorld = p.getTransform("toWorld", Transform());
+    if (p.hasTransform("toWorldEnd") && !(p.getTransform("toWorldEnd", toWorld) == toWorld))
+        throw std::runtime_error("Primitive: animated transforms (toWorldEnd) are not supported by the GPU integrators");
+}
+void PrimitiveObj::addChild(std::shared_ptr<GndObject> c) {
+    switch (c->getClassType()) {
+        case EShape:
+            if (shape) throw std::runtime_error("Primitive: shape already registered!");
+            shape = std::static_pointer_cast<ShapeObj>(c);
+            break;
+        case EMaterial:
+            if (material) throw std::runtime_error("Primitive: material already registered!");
+            material = std::static_pointer_cast<MaterialObj>(c);
+            break;
+        case EEmitter:
+            if (emitter) throw std::runtime_error("Primitive: emitter already registered!");
+            emitter = std::static_pointer_cast<EmitterObj>(c);
+            break;
+        default:
+            throw std::runtime_error("Primitive: invalid child class! Expected Shape.");
+    }
+}
+void PrimitiveObj::activate() {
+    if (!shape) throw std::runtime_error("Primitive: defined without a Shape!");
+    if (!material) {
+        auto m = std::make_shared<MatteMat>(PropertyList());
+        m->activate();
+        material = m;
+    }
+}
+struct PrimitiveReg : PrimitiveObj {
+    explicit PrimitiveReg(const PropertyList& p) : PrimitiveObj(p) {}
+};
+GND_REGISTER_CLASS(PrimitiveReg, "primitive")
+
+// ---------------------------------------------------------------- camera, filters, sampler
+CameraObj::CameraObj(const PropertyList& p) {
+    toWorld = p.getTransform("toWorld", Transform());
+    if (p.hasTransform("toWorldEnd") && !(p.getTransform("toWorldEnd", toWorld) == toWorld))
+        throw std::runtime_error("Camera: animated transforms (toWorldEnd) are not supported by the GPU integrators");
+    width = p.getInteger("width", 1280);
+    height = p.getInteger("height", 720);
+    fov = p.getFloat("fov", 45.0f);
+}
+void CameraObj::addChild(std::shared_ptr<GndObject> c) {
+    if (c->getClassType() == EFilter) {
+        if (filter) throw std::runtime_error("Camera: cannot define multiple films!");
+        filter = std::static_pointer_cast<FilterObj>(c);
+    }
+}
+struct PerspectiveCameraObj : CameraObj {
+    explicit PerspectiveCameraObj(const PropertyList& p) : CameraObj(p) {}
+};
+// filter.h:20-54
+struct BoxFilterObj : FilterObj {
+    explicit BoxFilterObj(const PropertyList&) { type = 0; rx = ry = 0.5f; }
+};
+struct GaussianFilterObj : FilterObj {
+    explicit GaussianFilterObj(const PropertyList& p) {
+        type = 1;
+        V2 r = p.getVector2("radius", V2{2.f, 2.f});
+        rx = r.x; ry = r.y;
+        alpha = p.getFloat("alpha", 2.0f);
+    }
+};
+struct IndependentSamplerObj : SamplerObj {
+    explicit IndependentSamplerObj(const PropertyList& p) : SamplerObj(p) {}
+};
+GND_REGISTER_CLASS(PerspectiveCameraObj, "perspective")
+GND_REGISTER_CLASS(BoxFilterObj, "box")
+GND_REGISTER_CLASS(GaussianFilterObj, "gaussian")
+GND_REGISTER_CLASS(IndependentSamplerObj, "independent")
+struct SceneReg : Scene {
+    explicit SceneReg(const PropertyList& p) : Scene(p) {}
+};
+GND_REGISTER_CLASS(SceneReg, "scene")
+
+// ---------------------------------------------------------------- scene
+// scene.cpp:9-44
+void Scene::addChild(std::shared_ptr<GndObject> c) {
+    switch (c->getClassType()) {
+        case EPrimitive: m_primitives.push_back(std::static_pointer_cast<PrimitiveObj>(c)); break;
+        case ECamera:
+            if (m_camera) throw std::runtime_error("Scene: cannot add multiple cameras!");
+            m_camera = std::static_pointer_cast<CameraObj>(c);
+            break;
+        case EIntegrator:
+            if (m_integrator) throw std::runtime_error("Scene: cannot add multiple integrators!");
+            m_integrator = std::static_pointer_cast<Integrator>(c);
+            break;
+        case ESampler:
+            if (m_sampler) throw std::runtime_error("Scene: cannot add multiple samplers!");
+            m_sampler = std::static_pointer_cast<SamplerObj>(c);
+            break;
+        case EEmitter:
+            throw std::runtime_error("Scene: only area emitters attached to primitives are supported by the GPU integrators");
+        default:
+            throw std::runtime_error("Scene: cannot add specified child!");
+    }
+}
+
+// scene.cpp:46-62
+void Scene::activate() {
+    if (!m_camera) throw std::runtime_error("Scene: no camera specified!");
+    if (!m_integrator) throw std::runtime_error("Scene: no integrator specified!");
+    if (!m_sampler) throw std::runtime_error("Scene: no sampler specified!");
+    build();
+    if (!deferPreprocess) m_integrator->preprocess(this);
+}
+
+namespace {
+
+struct MeshBuild {
+    std::vector<gnd::Node4> nodes;   // node refs relative to this vector
+    uint32_t root = gnd::kEmpty;
+    std::vector<uint32_t> order;     // leaf order -> original triangle
+};
+
+template <typename F>
+void parallelFor(size_t n, F&& f) {
+    unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), (unsigned)n));
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (;;) {
+            size_t i = next.fetch_add(1);
+            if (i >= n) break;
+            f(i);
+        }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+}
+
+// Rebases inner-node references of a locally built node array.
+void appendNodes(std::vector<gnd::Node4>& dst, const std::vector<gnd::Node4>& src) {
+    uint32_t base = (uint32_t)dst.size();
+    for (gnd::Node4 n : src) {
+        for (int i = 0; i < 4; ++i)
+            if (n.child[i] != gnd::kEmpty && !gnd::isLeaf(n.child[i])) n.child[i] += base;
+        dst.push_back(n);
+    }
+}
+
+}  // namespace
+
+void Scene::build() {
+    auto fs = std::make_unique<FlatScene>();
+    // unique meshes, materials, media
+    std::unordered_map<const ShapeObj*, int> meshIdx;
+    std::vector<const ShapeObj*> meshes;
+    std::unordered_map<const MaterialObj*, int> matIdx;
+    std::unordered_map<const MediumObj*, int> medIdx;
+    auto mediumIndex = [&](const std::shared_ptr<MediumObj>& m) -> int {
+        if (!m) return -1;
+        auto it = medIdx.find(m.get());
+        if (it != medIdx.end()) return it->second;
+        int k = (int)fs->media.size();
+        fs->media.push_back(m->rec);
+        medIdx[m.get()] = k;
+        return k;
+    };
+    for (auto& p : m_primitives) {
+        if (p->shape->kind == gnd::kShapeMesh && !meshIdx.count(p->shape.get())) {
+            meshIdx[p->shape.get()] = (int)meshes.size();
+            meshes.push_back(p->shape.get());
+        }
+    }
+    // bottom-level trees, built in parallel per mesh
+    std::vector<MeshBuild> mb(meshes.size());
+    std::vector<uint32_t> triBase(meshes.size() + 1, 0);
+    for (size_t i = 0; i < meshes.size(); ++i) {
+        size_t nt = meshes[i]->numTris();
+        if (triBase[i] + nt >= gnd::kLeafFirstMask) throw std::runtime_error("Scene: too many triangles for the device layout");
+        triBase[i + 1] = triBase[i] + (uint32_t)nt;
+    }
+    int parDepth = meshes.size() == 1 ? 4 : 0;
+    parallelFor(meshes.size(), [&](size_t i) {
+        const ShapeObj& m = *meshes[i];
+        size_t nt = m.numTris();
+        std::vector<Bounds> pb(nt);
+        std::vector<V3> pc(nt);
+        for (size_t t = 0; t < nt; ++t) {
+            Bounds b;
+            b.grow(m.positions[3 * t]); b.grow(m.positions[3 * t + 1]); b.grow(m.positions[3 * t + 2]);
+            pb[t] = b;
+            pc[t] = b.centroid();
+        }
+        BinTree bt = buildSAH(pb, pc, parDepth);
+        mb[i].root = collapseToNode4(bt, triBase[i], pb, mb[i].nodes);
+        mb[i].order = std::move(bt.order);
+    });
+    // top-level tree over primitive world bounds (bvh.cpp:10-36); it goes first
+    size_t np = m_primitives.size();
+    std::vector<Bounds> wb(np);
+    std::vector<V3> wc(np);
+    for (size_t i = 0; i < np; ++i) {
+        wb[i] = m_primitives[i]->shape->objectBounds().transformed(m_primitives[i]->toWorld);
+        wc[i] = wb[i].lo * 0.5f + wb[i].hi * 0.5f;
+    }
+    if (np > 0) {
+        BinTree tl = buildSAH(wb, wc, 0);
+        fs->tlasRoot = collapseToNode4(tl, 0, wb, fs->nodes);
+        fs->tlasList = tl.order;
+    }
+    // concatenate the meshes
+    std::vector<uint32_t> blasRoot(meshes.size());
+    fs->tris.resize(triBase.back());
+    fs->attrs.resize(triBase.back());
+    for (size_t i = 0; i < meshes.size(); ++i) {
+        uint32_t base = (uint32_t)fs->nodes.size();
+        appendNodes(fs->nodes, mb[i].nodes);
+        blasRoot[i] = mb[i].root + base;
+        const ShapeObj& m = *meshes[i];
+        gnd::MeshRec rec{};
+        rec.cdfOffset = (uint32_t)fs->cdf.size();
+        rec.numTris = (uint32_t)m.numTris();
+        rec.origToLeaf = (uint32_t)fs->origToLeaf.size();
+        fs->origToLeaf.resize(fs->origToLeaf.size() + m.numTris());
+        bool hasN = !m.normals.empty(), hasUV = !m.uvs.empty();
+        for (size_t s = 0; s < m.numTris(); ++s) {
+            uint32_t orig = mb[i].order[s];
+            uint32_t slot = triBase[i] + (uint32_t)s;
+            fs->origToLeaf[rec.origToLeaf + orig] = slot;
+            const V3* P = &m.positions[3 * orig];
+            gnd::Tri& t = fs->tris[slot];
+            t.v0x = P[0].x; t.v0y = P[0].y; t.v0z = P[0].z; t.prim = orig;
+            t.v1x = P[1].x; t.v1y = P[1].y; t.v1z = P[1].z; t.pad1 = 0;
+            t.v2x = P[2].x; t.v2y = P[2].y; t.v2z = P[2].z; t.pad2 = 0;
+            gnd::TriAttr& a = fs->attrs[slot];
+            std::memset(&a, 0, sizeof(a));
+            if (hasN) {
+                const V3* N = &m.normals[3 * orig];
+                a.n0x = N[0].x; a.n0y = N[0].y; a.n0z = N[0].z;
+                a.n1x = N[1].x; a.n1y = N[1].y; a.n1z = N[1].z;
+                a.n2x = N[2].x; a.n2y = N[2].y; a.n2z = N[2].z;
+            }
+            if (hasUV) {
+                const V2* U = &m.uvs[3 * orig];
+                a.u0 = U[0].x; a.v0_ = U[0].y; a.u1 = U[1].x; a.v1_ = U[1].y; a.u2 = U[2].x; a.v2_ = U[2].y;
+            }
+            a.flags = (float)((hasN ? 1 : 0) | (hasUV ? 2 : 0));
+        }
+        // area CDF in original triangle order (mesh.cpp:120-145)
+        fs->cdf.push_back(0.0f);
+        float total = 0.0f;
+        for (size_t t = 0; t < m.numTris(); ++t) {
+            V3 e1 = m.positions[3 * t + 1] - m.positions[3 * t];
+            V3 e2 = m.positions[3 * t + 2] - m.positions[3 * t];
+            total += 0.5f * gnd::length(gnd::cross(e1, e2));
+            fs->cdf.push_back(total);
+        }
+        if (total > 0.0f)
+            for (size_t t = 1; t <= m.numTris(); ++t) fs->cdf[rec.cdfOffset + t] /= total;
+        rec.totalArea = total;
+        fs->meshes.push_back(rec);
+    }
+    // instances, materials, emitters
+    for (size_t i = 0; i < np; ++i) {
+        const PrimitiveObj& p = *m_primitives[i];
+        gnd::InstTrav it{};
+        gnd::InstShade is{};
+        it.w2o = p.toWorld.mInv.toXf34();
+        is.o2w = p.toWorld.m.toXf34();
+        it.kind = p.shape->kind;
+        it.blasRoot = gnd::kEmpty;
+        is.meshId = 0xFFFFFFFFu;
+        if (p.shape->kind == gnd::kShapeMesh) {
+            int mi = meshIdx[p.shape.get()];
+            it.blasRoot = blasRoot[mi];
+            is.triBase = triBase[mi];
+            is.meshId = (uint32_t)mi;
+        } else if (p.shape->kind == gnd::kShapeSphere) {
+            it.p0 = p.shape->radius;
+            is.radius = p.shape->radius;
+        } else {
+            it.p0 = p.shape->extents.x;
+            it.p1 = p.shape->extents.y;
+            is.ext[0] = p.shape->extents.x; is.ext[1] = p.shape->extents.y; is.ext[2] = p.shape->extents.z;
+        }
+        const MaterialObj* mat = p.material.get();
+        auto mit = matIdx.find(mat);
+        if (mit == matIdx.end()) {
+            int k = (int)fs->materials.size();
+            fs->materials.push_back(mat->rec);
+            mit = matIdx.emplace(mat, k).first;
+        }
+        is.material = mit->second;
+        // glass / index attach their media (material.h:119-126); others keep none
+        bool attaches = mat->rec.type == gnd::kMatGlass || mat->rec.type == gnd::kMatIndex;
+        is.hasMedia = (attaches && (mat->inside || mat->outside)) ? 1u : 0u;
+        is.mediumIn = is.hasMedia ? mediumIndex(mat->inside) : -1;
+        is.mediumOut = is.hasMedia ? mediumIndex(mat->outside) : -1;
+        is.emitter = -1;
+        if (p.emitter) {
+            gnd::Emitter e{};
+            e.instance = (int32_t)i;
+            e.radiance = p.emitter->radiance;
+            is.emitter = (int32_t)fs->emitters.size();
+            fs->emitters.push_back(e);
+        }
+        fs->instT.push_back(it);
+        fs->instS.push_back(is);
+    }
+    // camera (perspective.cpp:9-12)
+    if (m_camera) {
+        fs->camera.toWorld = m_camera->toWorld.m.toXf34();
+        fs->camera.width = m_camera->width;
+        fs->camera.height = m_camera->height;
+        fs->camera.scale = std::tan((gnd::kPi / 180.f) * (m_camera->fov * 0.5f));
+        fs->camera.aspect = m_camera->width / (float)m_camera->height;
+    }
+    fs->fillDesc();
+    gnd_scene_desc& d = fs->desc;
+    d.width = m_camera ? m_camera->width : 0;
+    d.height = m_camera ? m_camera->height : 0;
+    d.spp = m_sampler ? m_sampler->spp : 1;
+    d.max_depth = m_integrator ? m_integrator->maxDepth : 1000;
+    d.integrator = m_integrator ? m_integrator->kind : 0;
+    auto filt = m_camera ? m_camera->filter : nullptr;
+    d.filter = filt ? filt->type : 1;   // film.cpp:29: Gaussian when no filter is given
+    d.filter_radius[0] = filt ? filt->rx : 2.f;
+    d.filter_radius[1] = filt ? filt->ry : 2.f;
+    d.filter_alpha = filt ? filt->alpha : 2.f;
+    m_flat = std::move(fs);
+}
+
+void FlatScene::fillDesc() {
+    desc.nodes = nodes.data();
+    desc.num_nodes = (int64_t)nodes.size();
+    desc.tris = tris.data();
+    desc.tri_attrs = attrs.data();
+    desc.num_tris = (int64_t)tris.size();
+    desc.inst_trav = instT.data();
+    desc.inst_shade = instS.data();
+    desc.num_instances = (int32_t)instT.size();
+    desc.tlas_root = tlasRoot;
+    desc.tlas_list = tlasList.data();
+    desc.tlas_list_len = (int64_t)tlasList.size();
+    desc.materials = materials.data();
+    desc.num_materials = (int32_t)materials.size();
+    desc.emitters = emitters.data();
+    desc.num_emitters = (int32_t)emitters.size();
+    desc.media = media.data();
+    desc.num_media = (int32_t)media.size();
+    desc.meshes = meshes.data();
+    desc.num_meshes = (int32_t)meshes.size();
+    desc.cdf = cdf.data();
+    desc.cdf_len = (int64_t)cdf.size();
+    desc.orig_to_leaf = origToLeaf.data();
+    desc.orig_to_leaf_len = (int64_t)origToLeaf.size();
+    desc.camera = &camera;
+}
+
+}  // namespace gndh

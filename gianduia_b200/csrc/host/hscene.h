@@ -1,0 +1,313 @@
+// Host scene framework: the reference's plugin object model (GndObject, PropertyList,
+// GND_REGISTER_CLASS, Scene, Primitive, shapes, materials, media, emitters, camera,
+// filters, sampler, Integrator), producing the flattened device layout that the GPU
+// integrators consume.
+#pragma once
+#include <atomic>
+#include <cstdint>
+#include <functional>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "gnd/layout.h"
+#include "gnd/vmath.h"
+#include "gnd_gpu.h"
+
+namespace gndh {
+
+using gnd::V2;
+using gnd::V3;
+
+// ---------------------------------------------------------------- 4x4 matrices
+// Column-major like glm::mat4: c[col][row].
+struct Mat4 {
+    float c[4][4];
+    static Mat4 identity();
+    Mat4 operator*(const Mat4& b) const;
+    void mulVec(const float v[4], float out[4]) const;   // (c0*x + c1*y) + (c2*z + c3*w)
+    Mat4 transpose() const;
+    bool operator==(const Mat4& o) const;
+    gnd::Xf34 toXf34() const;
+};
+Mat4 inverse(const Mat4& m);   // cofactor expansion
+
+// transform.h:299-437: matrix and inverse composed step by step (parser: t = step * t)
+struct Transform {
+    Mat4 m = Mat4::identity(), mInv = Mat4::identity();
+    Transform() = default;
+    Transform(const Mat4& a, const Mat4& b) : m(a), mInv(b) {}
+    Transform inverse() const { return Transform(mInv, m); }
+    Transform operator*(const Transform& t) const { return Transform(m * t.m, t.mInv * mInv); }
+    bool operator==(const Transform& o) const { return m == o.m; }
+    V3 point(V3 p) const;
+    V3 vector(V3 v) const;
+    static Transform translate(V3 d);
+    static Transform scale(float x, float y, float z);
+    static Transform rotate(float degrees, V3 axis);
+    static Transform lookAt(V3 pos, V3 target, V3 up);
+};
+
+struct Bounds {
+    V3 lo{3.402823466e38f, 3.402823466e38f, 3.402823466e38f};
+    V3 hi{-3.402823466e38f, -3.402823466e38f, -3.402823466e38f};
+    void grow(V3 p);
+    void grow(const Bounds& b);
+    V3 centroid() const { return lo * 0.5f + hi * 0.5f; }   // bounds.h:214-216
+    float area() const;                                      // bounds.h:184-187
+    int maxExtent() const;                                   // bounds.h:196-203
+    Bounds transformed(const Transform& t) const;            // transform.h:356-363
+};
+
+// ---------------------------------------------------------------- properties
+// propertyList.h:12-100
+class PropertyList {
+public:
+    void setBoolean(const std::string& k, bool v) { b_[k] = v; }
+    void setInteger(const std::string& k, int v) { i_[k] = v; }
+    void setFloat(const std::string& k, float v) { f_[k] = v; }
+    void setString(const std::string& k, const std::string& v) { s_[k] = v; }
+    void setPoint3(const std::string& k, V3 v) { p3_[k] = v; }
+    void setVector2(const std::string& k, V2 v) { v2_[k] = v; }
+    void setPoint2(const std::string& k, V2 v) { p2_[k] = v; }
+    void setVector3(const std::string& k, V3 v) { v3_[k] = v; }
+    void setColor(const std::string& k, V3 v) { c_[k] = v; }
+    void setTransform(const std::string& k, const Transform& v) { t_[k] = v; }
+    bool hasColor(const std::string& k) const { return c_.count(k) > 0; }
+    bool hasFloat(const std::string& k) const { return f_.count(k) > 0; }
+    bool hasTransform(const std::string& k) const { return t_.count(k) > 0; }
+    bool getBoolean(const std::string& k, bool d = false) const { return get(b_, k, d); }
+    int getInteger(const std::string& k, int d = 0) const { return get(i_, k, d); }
+    float getFloat(const std::string& k, float d = 0.f) const { return get(f_, k, d); }
+    std::string getString(const std::string& k, const std::string& d = "") const { return get(s_, k, d); }
+    V3 getVector3(const std::string& k, V3 d) const { return get(v3_, k, d); }
+    V2 getVector2(const std::string& k, V2 d) const { return get(v2_, k, d); }
+    V2 getPoint2(const std::string& k, V2 d) const { return get(p2_, k, d); }
+    V3 getColor(const std::string& k, V3 d) const { return get(c_, k, d); }
+    Transform getTransform(const std::string& k, const Transform& d) const { return get(t_, k, d); }
+
+private:
+    template <typename M, typename V>
+    static V get(const M& m, const std::string& k, const V& d) {
+        auto it = m.find(k);
+        return it == m.end() ? d : it->second;
+    }
+    std::map<std::string, bool> b_;
+    std::map<std::string, int> i_;
+    std::map<std::string, float> f_;
+    std::map<std::string, std::string> s_;
+    std::map<std::string, V3> p3_, v3_, c_;
+    std::map<std::string, V2> v2_, p2_;
+    std::map<std::string, Transform> t_;
+};
+
+// ---------------------------------------------------------------- object model
+// object.h:11-23
+enum EClassType { EScene, EPrimitive, EShape, ECamera, EIntegrator, ESampler, ETexture, EMaterial, EEmitter, EFilter, EMedium };
+const char* classTypeToString(EClassType t);
+
+class GndObject {
+public:
+    virtual ~GndObject() = default;
+    virtual void addChild(std::shared_ptr<GndObject>) { throw std::runtime_error("GndObject::addChild() not implemented!"); }
+    virtual void activate() {}
+    virtual EClassType getClassType() const = 0;
+    void setName(const std::string& n) { m_name = n; }
+    const std::string& getName() const { return m_name; }
+
+protected:
+    std::string m_name;
+};
+
+// factory.h:9-36
+using ObjectFactory = std::function<std::unique_ptr<GndObject>(const PropertyList&)>;
+class GndFactory {
+public:
+    static GndFactory* getInstance();
+    void registerClass(const std::string& name, const ObjectFactory& f);
+    std::unique_ptr<GndObject> createInstance(const std::string& name, const PropertyList& props);
+    bool has(const std::string& name) const { return m_ctors.count(name) > 0; }
+
+private:
+    std::map<std::string, ObjectFactory> m_ctors;
+};
+#define GND_REGISTER_CLASS(Cls, XmlName)                                                                   \
+    namespace {                                                                                          \
+    struct Cls##_Factory {                                                                               \
+        Cls##_Factory() {                                                                                \
+            ::gndh::GndFactory::getInstance()->registerClass(                                            \
+                XmlName, [](const ::gndh::PropertyList& p) -> std::unique_ptr<::gndh::GndObject> {       \
+                    return std::make_unique<Cls>(p);                                                     \
+                });                                                                                      \
+        }                                                                                                \
+    };                                                                                                   \
+    Cls##_Factory global_##Cls##_Factory;                                                                \
+    }
+
+// Color texture description (constant_color / checkerboard_color).
+struct ColorTexture : GndObject {
+    gnd::ColorTex rec{};
+    EClassType getClassType() const override { return ETexture; }
+};
+struct FloatTexture : GndObject {
+    float value = 1.f;
+    EClassType getClassType() const override { return ETexture; }
+};
+
+struct MediumObj : GndObject {
+    gnd::Medium rec{};
+    EClassType getClassType() const override { return EMedium; }
+};
+
+struct MaterialObj : GndObject {
+    gnd::Material rec{};
+    std::shared_ptr<MediumObj> inside, outside;
+    EClassType getClassType() const override { return EMaterial; }
+    void addChild(std::shared_ptr<GndObject> c) override;
+};
+
+struct EmitterObj : GndObject {
+    gnd::ColorTex radiance{};
+    bool hasRadiance = false;
+    EClassType getClassType() const override { return EEmitter; }
+    void addChild(std::shared_ptr<GndObject> c) override;
+    void activate() override;
+};
+
+// Mesh geometry in the reference's de-indexed form (one vertex per face corner).
+struct ShapeObj : GndObject {
+    uint32_t kind = gnd::kShapeMesh;
+    std::string filename;
+    std::vector<V3> positions, normals;
+    std::vector<V2> uvs;
+    float radius = 1.f;
+    V3 extents{1.f, 1.f, 1.f};
+    int meshId = -1;      // assigned at flattening
+    EClassType getClassType() const override { return EShape; }
+    void activate() override;
+    Bounds objectBounds() const;
+    size_t numTris() const { return positions.size() / 3; }
+};
+
+struct PrimitiveObj : GndObject {
+    Transform toWorld;
+    std::shared_ptr<ShapeObj> shape;
+    std::shared_ptr<MaterialObj> material;
+    std::shared_ptr<EmitterObj> emitter;
+    explicit PrimitiveObj(const PropertyList& p);
+    EClassType getClassType() const override { return EPrimitive; }
+    void addChild(std::shared_ptr<GndObject> c) override;
+    void activate() override;
+};
+
+struct FilterObj : GndObject {
+    int type = 0;   // 0 box, 1 gaussian
+    float rx = 0.5f, ry = 0.5f, alpha = 2.f;
+    EClassType getClassType() const override { return EFilter; }
+};
+
+struct CameraObj : GndObject {
+    Transform toWorld;
+    int width = 1280, height = 720;
+    float fov = 45.f;
+    std::shared_ptr<FilterObj> filter;
+    explicit CameraObj(const PropertyList& p);
+    EClassType getClassType() const override { return ECamera; }
+    void addChild(std::shared_ptr<GndObject> c) override;
+};
+
+struct SamplerObj : GndObject {
+    int spp = 1;
+    explicit SamplerObj(const PropertyList& p) : spp(p.getInteger("spp", 1)) {}
+    EClassType getClassType() const override { return ESampler; }
+};
+
+class Scene;
+
+// integrator.h:18-40: the plugin interface the GPU integrators implement.
+class Integrator : public GndObject {
+public:
+    using RenderCallback = std::function<void(int sampleIndex, const float* film, int width, int height)>;
+    virtual ~Integrator() = default;
+    virtual void render(Scene* scene) = 0;
+    virtual void cancel() { m_stopRequested = true; }
+    virtual void preprocess(Scene*) {}
+    void setCallback(RenderCallback cb) { m_callback = std::move(cb); }
+    EClassType getClassType() const override { return EIntegrator; }
+    int kind = 0;        // 0 path_gpu, 1 volpath_gpu
+    int maxDepth = 1000; // path.cpp:9, volPath.cpp:12
+
+protected:
+    std::atomic<bool> m_stopRequested{false};
+    RenderCallback m_callback;
+};
+
+// Flattened scene: owner of the arrays a gnd_scene_desc points at.
+struct FlatScene {
+    std::vector<gnd::Node4> nodes;
+    std::vector<gnd::Tri> tris;
+    std::vector<gnd::TriAttr> attrs;
+    std::vector<gnd::InstTrav> instT;
+    std::vector<gnd::InstShade> instS;
+    std::vector<uint32_t> tlasList;
+    std::vector<gnd::Material> materials;
+    std::vector<gnd::Emitter> emitters;
+    std::vector<gnd::Medium> media;
+    std::vector<gnd::MeshRec> meshes;
+    std::vector<float> cdf;
+    std::vector<uint32_t> origToLeaf;
+    gnd::Camera camera{};
+    uint32_t tlasRoot = gnd::kEmpty;
+    gnd_scene_desc desc{};
+    void fillDesc();
+};
+
+// scene.cpp:9-75
+class Scene : public GndObject {
+public:
+    explicit Scene(const PropertyList&) {}
+    void addChild(std::shared_ptr<GndObject> c) override;
+    void activate() override;                 // builds and flattens, then integrator->preprocess
+    void build();                             // builds and flattens only
+    EClassType getClassType() const override { return EScene; }
+    void render() { m_integrator->render(this); }
+    std::shared_ptr<CameraObj> getCamera() { return m_camera; }
+    std::shared_ptr<SamplerObj> getSampler() { return m_sampler; }
+    std::shared_ptr<Integrator> getIntegrator() { return m_integrator; }
+    const FlatScene& flat() const { return *m_flat; }
+    bool deferPreprocess = false;
+
+    std::vector<std::shared_ptr<PrimitiveObj>> m_primitives;
+    std::shared_ptr<CameraObj> m_camera;
+    std::shared_ptr<SamplerObj> m_sampler;
+    std::shared_ptr<Integrator> m_integrator;
+    std::unique_ptr<FlatScene> m_flat;
+};
+
+// parser.cpp:220-235
+std::shared_ptr<GndObject> loadFromXML(const std::string& path, bool deferPreprocess);
+// mesh.cpp:148-229
+void loadOBJ(const std::string& path, ShapeObj& mesh);
+
+// ---------------------------------------------------------------- BVH build
+// bvhBuilder.cpp:59-182: binary SAH tree. Returns nodes in depth-first order; leaf ranges
+// index `order` (the permutation of the input primitives, leaf-contiguous).
+struct BinNode {
+    Bounds b;
+    uint32_t offset;     // leaf: first in `order`; interior: right child index
+    uint32_t count;      // 0 for interior
+};
+struct BinTree {
+    std::vector<BinNode> nodes;
+    std::vector<uint32_t> order;
+};
+BinTree buildSAH(const std::vector<Bounds>& primBounds, const std::vector<V3>& centroids, int parallelDepth);
+
+// bvhBuilder.cpp:184-262 + leaf encoding: appends 4-wide nodes to `out`; leaves become
+// references to [leafBase + first, +count). Returns the root node index.
+uint32_t collapseToNode4(const BinTree& t, uint32_t leafBase, const std::vector<Bounds>& primBounds,
+                         std::vector<gnd::Node4>& out);
+
+}  // namespace gndh

@@ -1,0 +1,159 @@
+// Device-resident scene layout (HBM). The host builder writes these records; the
+// kernels read them. All records are plain data, 16-byte aligned, sized in multiples
+// of 16 bytes so they load as float4/uint4.
+#pragma once
+#include <cstdint>
+#include "vmath.h"
+
+namespace gnd {
+
+// ---------------------------------------------------------------- BVH4 node
+// One 4-wide node = 128 bytes = one 128-byte cache line (aligned to 128):
+//   lox, hix, loy, hiy, loz, hiz : float[4] each, child i bounds (empty: +inf/-inf)
+//   child[4]                     : encoded child references (see below)
+//   pad[4]
+// Child reference:
+//   kEmpty                       : no child
+//   bit31 == 0                   : inner node index
+//   bit31 == 1                   : leaf; bits 27..30 = count-1 (1..16), bits 0..26 = first
+//                                  (first triangle for a bottom-level tree, first entry of
+//                                  the instance list for the top-level tree)
+struct alignas(128) Node4 {
+    float lox[4], hix[4], loy[4], hiy[4], loz[4], hiz[4];
+    uint32_t child[4];
+    uint32_t pad[4];
+};
+static_assert(sizeof(Node4) == 128, "Node4 must be 128 bytes");
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr uint32_t kLeafBit = 0x80000000u;
+constexpr int kLeafMax = 16;
+constexpr uint32_t kLeafFirstMask = (1u << 27) - 1;
+
+GND_HD bool isLeaf(uint32_t c) { return (c & kLeafBit) != 0; }
+GND_HD uint32_t leafFirst(uint32_t c) { return c & kLeafFirstMask; }
+GND_HD uint32_t leafCount(uint32_t c) { return ((c >> 27) & 15u) + 1u; }
+GND_HD uint32_t makeLeaf(uint32_t first, uint32_t count) { return kLeafBit | ((count - 1u) << 27) | first; }
+
+// ---------------------------------------------------------------- triangles
+// Leaf-ordered triangle records for traversal: v0.xyz + original triangle index (bits),
+// v1.xyz, v2.xyz. The edges e1 = v1 - v0, e2 = v2 - v0 are formed in the kernel exactly
+// as the reference's 4-lane test forms them (mesh.cpp:264-265).
+struct alignas(16) Tri {
+    float v0x, v0y, v0z; uint32_t prim;
+    float v1x, v1y, v1z; uint32_t pad1;
+    float v2x, v2y, v2z; uint32_t pad2;
+};
+static_assert(sizeof(Tri) == 48, "Tri must be 48 bytes");
+
+// Shading attributes, same leaf order as Tri: normals of the three corners and uvs.
+struct alignas(16) TriAttr {
+    float n0x, n0y, n0z, n1x;
+    float n1y, n1z, n2x, n2y;
+    float n2z, u0, v0_, u1;
+    float v1_, u2, v2_, flags;   // flags: bit0 has normals, bit1 has uvs (as float)
+};
+static_assert(sizeof(TriAttr) == 64, "TriAttr must be 64 bytes");
+
+// ---------------------------------------------------------------- instances
+enum ShapeKind : uint32_t { kShapeMesh = 0, kShapeSphere = 1, kShapeCube = 2 };
+
+// Traversal record (64 bytes): world-to-object 3x4 plus the shape reference.
+struct alignas(16) InstTrav {
+    Xf34 w2o;                 // 48 B
+    uint32_t kind;            // ShapeKind
+    uint32_t blasRoot;        // mesh: root node index
+    float p0, p1;             // sphere: radius; cube: extents x, y (z in InstShade)
+};
+static_assert(sizeof(InstTrav) == 64, "InstTrav must be 64 bytes");
+
+// Shading record (96 bytes).
+struct alignas(16) InstShade {
+    Xf34 o2w;                 // 48 B object-to-world
+    int32_t material;         // material index
+    int32_t emitter;          // emitter index or -1
+    int32_t mediumIn, mediumOut;   // material media (-1: none); only glass/index set them
+    uint32_t triBase;         // first triangle (leaf order) of the mesh
+    uint32_t meshId;          // mesh record index (area CDF)
+    float ext[3];             // cube extents
+    float radius;             // sphere radius
+    uint32_t hasMedia;        // 1 when the material attaches a medium interface
+    uint32_t pad;
+};
+static_assert(sizeof(InstShade) == 96, "InstShade must be 96 bytes");
+
+// Mesh record for emitter sampling: its area CDF and triangles in original order.
+struct alignas(16) MeshRec {
+    uint32_t cdfOffset;       // into the cdf array (numTris + 1 entries)
+    uint32_t numTris;
+    uint32_t origToLeaf;      // offset into the original-order -> leaf-slot map
+    float totalArea;
+};
+
+// ---------------------------------------------------------------- materials
+enum MatType : uint32_t {
+    kMatMatte = 0, kMatPlastic = 1, kMatConductor = 2, kMatGlass = 3, kMatIndex = 4
+};
+// Color texture slot: constant (kind 0) or checkerboard (kind 1, checkerboard.h:36-48)
+struct alignas(16) ColorTex {
+    float v1[3]; uint32_t kind;
+    float v2[3]; float pad;
+    float scale[2], delta[2];
+};
+static_assert(sizeof(ColorTex) == 48, "ColorTex must be 48 bytes");
+
+struct alignas(16) Material {
+    uint32_t type;
+    float roughness;          // plastic/conductor/glass
+    float eta;                // plastic/glass
+    float pad0;
+    ColorTex a;               // matte albedo | plastic Kd | conductor R | glass R
+    ColorTex b;               // plastic Ks | glass T
+    float condEta[3]; float pad1;
+    float condK[3]; float pad2;
+};
+
+// ---------------------------------------------------------------- emitters, media
+struct alignas(16) Emitter {
+    int32_t instance;         // the primitive carrying the area light
+    uint32_t pad[3];
+    ColorTex radiance;
+};
+
+struct alignas(16) Medium {
+    float sigA[3]; float g;
+    float sigS[3]; float pad0;
+    float sigT[3]; float pad1;
+};
+
+// ---------------------------------------------------------------- camera
+struct alignas(16) Camera {
+    Xf34 toWorld;
+    int32_t width, height;
+    float scale, aspect;      // tan(fov/2), width/height
+};
+
+// ---------------------------------------------------------------- scene view
+// Device pointers of one uploaded scene, passed by value to kernels (or read from an
+// array of views when several scenes share one launch).
+struct SceneView {
+    const Node4* nodes;
+    const Tri* tris;
+    const TriAttr* attrs;
+    const InstTrav* instT;
+    const InstShade* instS;
+    const uint32_t* tlasList;     // top-level leaf entries -> instance index
+    const Material* materials;
+    const Emitter* emitters;
+    const Medium* media;
+    const MeshRec* meshes;
+    const float* cdf;
+    const uint32_t* origToLeaf;
+    uint32_t tlasRoot;            // kEmpty when the scene has no primitives
+    int32_t numEmitters;
+    int32_t numInstances;
+    int32_t pad;
+    Camera camera;
+};
+
+}  // namespace gnd

@@ -1,0 +1,152 @@
+/*
+ * gnd_gpu.h -- C ABI of the B200 radiance path (BVH4 traversal + path/volpath
+ * wavefront integrators) for Gianduia-style scenes.
+ *
+ * The library (gianduia_b200/_lib/libgianduia_b200.so) exports two groups:
+ *
+ *  1. gnd_gpu_*  : the device boundary. Plain pointers and sizes; no C++ types.
+ *                  A reference-side integrator plugin binds exactly these.
+ *  2. gnd_host_* : the host scene framework (XML + OBJ loading through the same plugin
+ *                  names as the reference, SAH BVH build, BVH4 collapse, flattening to
+ *                  the device layout) that produces the gnd_scene_desc the device
+ *                  boundary consumes.
+ *
+ * Every function returns a gnd_status (0 = success). On failure the message is
+ * available from gnd_last_error() (thread-local). No C++ exception crosses the ABI.
+ * Calls on one context are serialised internally; contexts are independent.
+ */
+#ifndef GND_GPU_H
+#define GND_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t gnd_status;
+enum {
+    GND_OK = 0,
+    GND_ERR_INVALID = 1,      /* bad argument or handle */
+    GND_ERR_CUDA = 2,         /* CUDA runtime error (message has the CUDA text) */
+    GND_ERR_OOM = 3,          /* device allocation failed */
+    GND_ERR_DEVICE_CHECK = 4, /* a kernel's bounds/stack/iteration check tripped */
+    GND_ERR_TIMEOUT = 5,      /* a bounded wait ran out */
+    GND_ERR_PARSE = 6,        /* scene file could not be loaded */
+    GND_ERR_CANCELLED = 7,    /* render or job cancelled */
+    GND_ERR_BUDGET = 8,       /* admission refused: over the HBM budget */
+    GND_ERR_NO_DEVICE = 9     /* no CUDA device / extension not usable */
+};
+
+/* Message of the last failing call on this thread (never NULL). */
+const char* gnd_last_error(void);
+/* Library version string. */
+const char* gnd_version(void);
+
+/* ------------------------------------------------------------------ rays and hits */
+/* A ray as the reference's Ray (ray.h:12-33): origin, tMin, direction, tMax. */
+typedef struct gnd_ray {
+    float o[3];
+    float tmin;
+    float d[3];
+    float tmax;
+} gnd_ray;
+
+/* Closest hit (the fields SurfaceInteraction gets from Shape::rayIntersect):
+ * t, barycentric u/v (meshes) and the primitive: inst = index of the <primitive> in
+ * scene-file order, prim = triangle index within its mesh (-1 for analytic shapes).
+ * A miss has inst = -1 and t = +inf. */
+typedef struct gnd_hit {
+    float t, u, v;
+    int32_t inst;
+    int32_t prim;
+} gnd_hit;
+
+/* ------------------------------------------------------------------ scene description */
+/* Flattened scene in the device layout (see gianduia_b200/csrc/include/gnd/layout.h for
+ * the record formats). All arrays are host memory owned by the caller; upload copies. */
+typedef struct gnd_scene_desc {
+    const void* nodes;            /* 128-byte BVH4 nodes, top level and every mesh */
+    int64_t num_nodes;
+    const void* tris;             /* 48-byte leaf-ordered triangles */
+    const void* tri_attrs;        /* 64-byte per-triangle shading attributes */
+    int64_t num_tris;
+    const void* inst_trav;        /* 64-byte per-instance traversal records */
+    const void* inst_shade;       /* 96-byte per-instance shading records */
+    int32_t num_instances;
+    uint32_t tlas_root;           /* root node of the top level (0xFFFFFFFF: empty) */
+    const uint32_t* tlas_list;    /* top-level leaf entries -> instance index */
+    int64_t tlas_list_len;
+    const void* materials;        /* material records */
+    int32_t num_materials;
+    int32_t num_emitters;
+    const void* emitters;         /* emitter records */
+    const void* media;            /* homogeneous media */
+    int32_t num_media;
+    int32_t num_meshes;
+    const void* meshes;           /* mesh records (area sampling) */
+    const float* cdf;             /* concatenated per-mesh area CDFs */
+    int64_t cdf_len;
+    const uint32_t* orig_to_leaf; /* per mesh: original triangle -> leaf slot */
+    int64_t orig_to_leaf_len;
+    const void* camera;           /* camera record */
+    /* render settings read from the scene file */
+    int32_t width, height, spp, max_depth;
+    int32_t integrator;           /* 0 path_gpu, 1 volpath_gpu */
+    int32_t filter;               /* 0 box (radius 0.5), 1 gaussian */
+    float filter_radius[2];
+    float filter_alpha;
+    int32_t pad;
+} gnd_scene_desc;
+
+/* ------------------------------------------------------------------ host framework */
+typedef struct gnd_host_scene gnd_host_scene;
+
+/* Parser::loadFromXML + Scene::activate (parser.cpp:220-235, scene.cpp:46-62): parses the
+ * scene file, loads meshes, builds every BVH and flattens them. */
+gnd_status gnd_host_load_xml(const char* path, gnd_host_scene** out);
+/* One mesh primitive with an identity transform from a triangle soup (ntri x 9 floats),
+ * default camera; used for traversal-only workloads. */
+gnd_status gnd_host_from_triangles(const float* tris, int64_t ntri, gnd_host_scene** out);
+gnd_status gnd_host_scene_desc(const gnd_host_scene* s, const gnd_scene_desc** out);
+gnd_status gnd_host_free(gnd_host_scene* s);
+
+/* ------------------------------------------------------------------ device boundary */
+typedef struct gnd_gpu_ctx gnd_gpu_ctx;
+typedef uint64_t gnd_scene_id;
+
+/* One context per GPU (device ordinal). Fails with GND_ERR_NO_DEVICE when no CUDA
+ * device is usable: there is no CPU fallback. */
+gnd_status gnd_gpu_create(int device, gnd_gpu_ctx** out);
+gnd_status gnd_gpu_destroy(gnd_gpu_ctx* ctx);
+
+/* Integrator::preprocess (integrator.h:23, called at scene.cpp:61): copies a flattened
+ * scene to HBM; the scene stays resident until gnd_gpu_scene_free. */
+gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctx, const gnd_scene_desc* desc, gnd_scene_id* out);
+gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctx, gnd_scene_id scene);
+/* Bytes of HBM the scene occupies. */
+gnd_status gnd_gpu_scene_bytes(gnd_gpu_ctx* ctx, gnd_scene_id scene, uint64_t* bytes);
+
+/* Scene::rayIntersect(ray, isect) (scene.cpp:64-66, bvh.cpp:38-66) for n rays in HOST
+ * memory: closest hit per ray, world tMax shrinking as hits are found. */
+gnd_status gnd_gpu_trace_closest(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* rays, int64_t n,
+                                 gnd_hit* hits);
+/* Scene::rayIntersect(ray) (scene.cpp:68-71): occlusion (any hit) per ray, 1/0. */
+gnd_status gnd_gpu_trace_any(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* rays, int64_t n,
+                             uint8_t* occluded);
+/* The same on DEVICE buffers, asynchronous on `stream` (a cudaStream_t, NULL = the
+ * context's stream). */
+gnd_status gnd_gpu_trace_closest_dev(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* d_rays, int64_t n,
+                                     gnd_hit* d_hits, void* stream);
+gnd_status gnd_gpu_trace_any_dev(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* d_rays, int64_t n,
+                                 uint8_t* d_occluded, void* stream);
+/* Per-ray traversal work of the closest-hit kernel (instrumented variant): node visits
+ * and triangle tests, DEVICE buffers. Used for the roofline byte counts. */
+gnd_status gnd_gpu_trace_count_dev(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* d_rays, int64_t n,
+                                   uint32_t* d_nodes, uint32_t* d_tris, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GND_GPU_H */
