@@ -63,6 +63,8 @@ def lib():
                 "gnd_gpu_trace_closest_dev": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp, _vp],
                 "gnd_gpu_trace_any_dev": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp, _vp],
                 "gnd_gpu_trace_count_dev": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp, _vp, _vp],
+                "gnd_gpu_render": [_vp, ctypes.c_uint64, _vp, _vp, _vp],
+                "gnd_gpu_cancel": [_vp],
             }.items():
                 fn = getattr(L, name)
                 fn.argtypes = args
@@ -227,3 +229,60 @@ class GpuContext:
 
     def trace_count_dev(self, sid, d_rays, n, d_nodes, d_tris, stream=0):
         _check(lib().gnd_gpu_trace_count_dev(self._h, sid, d_rays, n, d_nodes, d_tris, stream or None), "gnd_gpu_trace_count_dev")
+
+    def render(self, sid, spp=0, first_pass=0, max_depth=0, integrator=-1, window=None, batched=False, film=None,
+               callback=None, profile=0):
+        """gnd_gpu_render: adds passes [first_pass, first_pass + spp) of the scene into
+        `film` (float32 [H, W, 7]: sum wL rgb, sum w, sum wL^2 rgb). Returns (film, stats)."""
+        hs = self._scenes[sid]
+        W, H = hs.width, hs.height
+        if film is None:
+            film = np.zeros((H, W, 7), np.float32)
+        assert film.dtype == np.float32 and film.shape == (H, W, 7) and film.flags.c_contiguous
+        p = RenderParams()
+        p.spp = spp
+        p.first_pass = first_pass
+        p.max_depth = max_depth
+        p.integrator = integrator
+        if window is not None:
+            p.window[:] = list(window)
+        p.batched = 1 if batched else 0
+        p.profile = profile
+        cb = None
+        if callback is not None:
+            def _cb(user, s, fptr, w, h):
+                arr = np.ctypeslib.as_array(fptr, shape=(h, w, 7)).copy()
+                callback(int(s), arr)
+            cb = PROGRESS_FN(_cb)
+            p.callback = cb
+        st = RenderStats()
+        _check(lib().gnd_gpu_render(self._h, sid, ctypes.byref(p), film.ctypes.data, ctypes.byref(st)), "gnd_gpu_render")
+        return film, dict(paths=st.paths, rays=st.rays, passes=st.passes_done, ms=st.ms, extend_rays=st.extend_rays,
+                          shadow_rays=st.shadow_rays, extend_nodes=st.extend_nodes, extend_tris=st.extend_tris,
+                          extend_ms=st.extend_ms, iterations=st.iterations)
+
+    def cancel(self):
+        _check(lib().gnd_gpu_cancel(self._h), "gnd_gpu_cancel")
+
+
+PROGRESS_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_float), ctypes.c_int32,
+                               ctypes.c_int32)
+
+
+class RenderParams(ctypes.Structure):
+    _fields_ = [("spp", ctypes.c_int32), ("first_pass", ctypes.c_int32), ("max_depth", ctypes.c_int32),
+                ("integrator", ctypes.c_int32), ("window", ctypes.c_int32 * 4), ("batched", ctypes.c_int32),
+                ("profile", ctypes.c_int32), ("callback", PROGRESS_FN), ("user", _vp)]
+
+
+class RenderStats(ctypes.Structure):
+    _fields_ = [("paths", ctypes.c_int64), ("rays", ctypes.c_int64), ("passes_done", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("ms", ctypes.c_double), ("extend_rays", ctypes.c_int64),
+                ("shadow_rays", ctypes.c_int64), ("extend_nodes", ctypes.c_int64), ("extend_tris", ctypes.c_int64),
+                ("extend_ms", ctypes.c_double), ("iterations", ctypes.c_int64)]
+
+
+def resolve(film):
+    """Image = sum(w L) / sum(w) per pixel (film.cpp:50-95)."""
+    w = film[..., 3:4]
+    return np.where(w > 0, film[..., :3] / np.maximum(w, 1e-30), 0.0).astype(np.float32)

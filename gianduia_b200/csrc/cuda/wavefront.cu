@@ -1,9 +1,999 @@
-// Wavefront path-tracing engine.
+// Wavefront path tracer: the reference's `path` (path.cpp:12-181) and `volpath`
+// (volPath.cpp:15-298) Li loops split into per-bounce kernels over a pool of path slots.
+//
+//   raygen  : camera sample per (pass, pixel) work item (integrator.h:92-125)
+//   extend  : closest hit for every active path (two-level BVH4 traversal)
+//   shade   : one bounce (medium sampling, emission with MIS, next-event estimation,
+//             BSDF / phase sampling, Russian roulette); appends a shadow query and the
+//             path to the next active list or to the done list
+//   shadow  : occlusion (path) or transmittance through media and null surfaces
+//             (volpath, volPath.cpp:261-291); adds the NEE contribution
+//   retire  : film splat of finished paths (film.h:26-69) and, in batched mode, refill
+//             of the freed slot with the next work item
+//
+// Every path draws its random numbers from its own PCG32 stream keyed exactly like the
+// reference (pixel + pass * W * H), in one fixed draw order, so a path's result does
+// not depend on which slot, pass or launch carries it. The film is accumulated in
+// 2^-24 fixed point with integer atomics: sums are independent of completion order.
+#include <chrono>
+#include <cstring>
+
+#include "shading.cuh"
+#include "traverse.cuh"
 #include "wavefront.h"
 
 namespace gnd {
 
-Wavefront::Wavefront(Context* c) : ctx_(c) {}
+constexpr int kBlock = 128;
+constexpr float kFixScale = 16777216.0f;   // 2^24
+constexpr float kFixMax = 1e11f;           // per-sample clamp before the fixed-point conversion
+
+// ---------------------------------------------------------------- queue helpers
+__device__ __forceinline__ uint32_t warpAppend(uint32_t* counter, bool pred) {
+    uint32_t active = __activemask();
+    uint32_t mask = __ballot_sync(active, pred);
+    if (!pred) return 0xFFFFFFFFu;
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+
+struct KParams {
+    const JobDev* jobs;
+    PathState* paths;
+    HitRec* hits;
+    uint32_t* listIn;
+    uint32_t* listOut;
+    ShadowRec* shadow;
+    uint32_t* done;
+    uint32_t* cnt;                 // queue counters (kQIn ...)
+    unsigned long long* totals;    // [0] extend rays, [1] shadow queries, [2] paths retired
+    unsigned long long* workNext;  // next work item (batched refill)
+    uint32_t* errWord;
+    uint32_t capacity;
+    int batched;
+};
+
+// ---------------------------------------------------------------- surface interaction
+struct SurfInt {
+    V3 p, n, dpdu;
+    V2 uv;
+};
+
+__device__ __forceinline__ V3 fallbackDpdu(V3 n) {
+    if (fabsf(n.x) > fabsf(n.y)) return divs(v3(-n.z, 0.0f, n.x), sqrtf(n.x * n.x + n.z * n.z));
+    return divs(v3(0.0f, n.z, -n.y), sqrtf(n.y * n.y + n.z * n.z));
+}
+
+__device__ __forceinline__ void sphereUV(SurfInt& si) {
+    float phi = atan2f(si.n.x, si.n.z);
+    if (phi < 0.0f) phi = (float)((double)phi + 2.0 * kPiD);
+    float u = phi * kInv2Pi;
+    float theta = acosf(clampf(si.n.y, -1.0f, 1.0f));
+    si.uv = V2{u, theta * kInvPi};
+    si.dpdu = v3((float)((double)(si.p.z * 2.0f) * kPiD), 0.0f, (float)((double)(-si.p.x * 2.0f) * kPiD));
+}
+
+// Object-space interaction of a mesh triangle (mesh.cpp:328-390).
+__device__ __forceinline__ SurfInt meshInteraction(const SceneView& s, uint32_t slot, float u, float v) {
+    SurfInt si;
+    float4 a = ldg4(&s.tris[slot].v0x), b = ldg4(&s.tris[slot].v1x), c = ldg4(&s.tris[slot].v2x);
+    V3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
+    const TriAttr* at = s.attrs + slot;
+    float4 A0 = ldg4(&at->n0x), A1 = ldg4(&at->n1y), A2 = ldg4(&at->n2z), A3 = ldg4(&at->v1_);
+    uint32_t flags = (uint32_t)A3.w;
+    float w = 1.0f - u - v;
+    si.p = (p0 * w + p1 * u) + p2 * v;
+    if (flags & 1u) {
+        V3 n0 = v3(A0.x, A0.y, A0.z), n1 = v3(A0.w, A1.x, A1.y), n2 = v3(A1.z, A1.w, A2.x);
+        si.n = normalize((n0 * w + n1 * u) + n2 * v);
+    } else {
+        si.n = normalize(cross(p1 - p0, p2 - p0));
+    }
+    if (flags & 2u) {
+        V2 uv0{A2.y, A2.z}, uv1{A2.w, A3.x}, uv2{A3.y, A3.z};
+        si.uv = V2{(uv0.x * w + uv1.x * u) + uv2.x * v, (uv0.y * w + uv1.y * u) + uv2.y * v};
+        V3 dp1 = p1 - p0, dp2 = p2 - p0;
+        V2 duv1{uv1.x - uv0.x, uv1.y - uv0.y}, duv2{uv2.x - uv0.x, uv2.y - uv0.y};
+        float det = duv1.x * duv2.y - duv1.y * duv2.x;
+        V3 dpdu;
+        if (fabsf(det) < 1e-8f) dpdu = fallbackDpdu(si.n);
+        else dpdu = (dp1 * duv2.y - dp2 * duv1.y) * (1.0f / det);
+        si.dpdu = normalize(dpdu - si.n * dot(si.n, dpdu));
+    } else {
+        si.uv = V2{u, v};
+        si.dpdu = normalize(fallbackDpdu(si.n));
+    }
+    return si;
+}
+
+// Primitive::fillInteraction (primitive.cpp:61-72) for the closest hit of world ray (o, d).
+__device__ __forceinline__ SurfInt surfaceInteraction(const SceneView& s, const HitRec& h, V3 o, V3 d) {
+    const InstTrav& it = s.instT[h.inst];
+    const InstShade& is = s.instS[h.inst];
+    uint32_t kind = it.kind;
+    SurfInt si;
+    if (kind == kShapeMesh) {
+        si = meshInteraction(s, h.slot, h.u, h.v);
+    } else {
+        V3 lo = xfPoint(it.w2o, o), ld = xfVector(it.w2o, d);
+        si.p = lo + ld * h.t;
+        if (kind == kShapeSphere) {     // sphere.cpp:41-55
+            si.n = normalize(si.p);
+            sphereUV(si);
+        } else {                        // cube.cpp:48-81
+            V3 ex = v3(is.ext[0], is.ext[1], is.ext[2]);
+            V3 dmin = si.p - (-ex), dmax = ex - si.p;
+            float md = 3.402823466e38f;
+            int axis = 0;
+            float sign = 1.0f;
+            for (int i = 0; i < 3; ++i) {
+                if (comp(dmin, i) < md) { md = comp(dmin, i); axis = i; sign = -1.0f; }
+                if (comp(dmax, i) < md) { md = comp(dmax, i); axis = i; sign = 1.0f; }
+            }
+            si.n = v3s(0.0f);
+            if (axis == 0) si.n.x = sign; else if (axis == 1) si.n.y = sign; else si.n.z = sign;
+            if (axis == 0) {
+                si.uv = V2{(si.p.z - (-ex.z)) / (2.0f * ex.z), (si.p.y - (-ex.y)) / (2.0f * ex.y)};
+                si.dpdu = v3(0.0f, 0.0f, 2.0f * ex.z * sign);
+            } else if (axis == 1) {
+                si.uv = V2{(si.p.x - (-ex.x)) / (2.0f * ex.x), (si.p.z - (-ex.z)) / (2.0f * ex.z)};
+                si.dpdu = v3(2.0f * ex.x * sign, 0.0f, 0.0f);
+            } else {
+                si.uv = V2{(si.p.x - (-ex.x)) / (2.0f * ex.x), (si.p.y - (-ex.y)) / (2.0f * ex.y)};
+                si.dpdu = v3(2.0f * ex.x * sign, 0.0f, 0.0f);
+            }
+        }
+    }
+    si.p = xfPoint(is.o2w, si.p);
+    si.n = normalize(xfNormal(it.w2o, si.n));
+    si.dpdu = normalize(xfVector(is.o2w, si.dpdu));
+    return si;
+}
+
+// ---------------------------------------------------------------- area emitters (area.cpp)
+struct LightSample {
+    V3 p, n;
+    V2 uv;
+    V3 Li;          // eval / pdf
+    float pdf;      // solid angle; left 0 on the early return
+    V3 sd;          // shadow direction
+    float stmax;    // shadow tMax
+};
+
+// Shape::sampleSurface in object space; returns the area pdf.
+__device__ __forceinline__ float sampleShape(const SceneView& s, int inst, V2 u, V3& p, V3& n, V2& uv) {
+    const InstTrav& it = s.instT[inst];
+    const InstShade& is = s.instS[inst];
+    if (it.kind == kShapeMesh) {                         // mesh.cpp:396-434
+        const MeshRec mr = s.meshes[is.meshId];
+        if (mr.totalArea == 0.0f) return 0.0f;
+        const float* cdf = s.cdf + mr.cdfOffset;
+        uint32_t size = mr.numTris + 1;
+        uint32_t lo = 0, hi = size;                      // std::lower_bound
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (cdf[mid] < u.x) lo = mid + 1; else hi = mid;
+        }
+        uint32_t tri = (lo < 1u ? 1u : (lo > size - 1 ? size - 1 : lo)) - 1;
+        float pdfTri = cdf[tri + 1] - cdf[tri];
+        float rx = clampf((u.x - cdf[tri]) / pdfTri, 0.0f, 1.0f);
+        float sq = sqrtf(rx);
+        float bu = 1.0f - sq;
+        float bv = u.y * sq;
+        uint32_t slot = s.origToLeaf[mr.origToLeaf + tri];
+        SurfInt si = meshInteraction(s, slot, bu, bv);
+        p = si.p;
+        n = si.n;
+        uv = si.uv;
+        const TriAttr* at = s.attrs + slot;
+        if (!(((uint32_t)at->flags) & 2u)) uv = V2{0.f, 0.f};
+        return 1.0f / mr.totalArea;
+    }
+    if (it.kind == kShapeSphere) {                       // sphere.cpp:64-81
+        float r = is.radius;
+        V3 res = squareToUniformSphere(u);
+        SurfInt si;
+        si.p = res * r;
+        si.n = normalize(si.p);
+        sphereUV(si);
+        p = si.p; n = si.n; uv = si.uv;
+        return kInv4Pi / (r * r);
+    }
+    // cube.cpp:83-146
+    V3 ex = v3(is.ext[0], is.ext[1], is.ext[2]);
+    float aX = 4.0f * ex.y * ex.z, aY = 4.0f * ex.x * ex.z, aZ = 4.0f * ex.x * ex.y;
+    float total = 2.0f * (aX + aY + aZ);
+    float fp[6] = {aX / total, aX / total, aY / total, aY / total, aZ / total, aZ / total};
+    float ux = u.x;
+    int face = 0;
+    float c = 0.0f;
+    for (int i = 0; i < 6; ++i) {
+        c += fp[i];
+        if (ux < c || i == 5) { face = i; float prev = c - fp[i]; ux = (ux - prev) / fp[i]; break; }
+    }
+    float sign = (face % 2 == 0) ? 1.0f : -1.0f;
+    if (face < 2) {
+        p = v3(ex.x * sign, -ex.y + ux * (2.0f * ex.y), -ex.z + u.y * (2.0f * ex.z));
+        n = v3(sign, 0.0f, 0.0f);
+        uv = V2{(p.z - (-ex.z)) / (2.0f * ex.z), (p.y - (-ex.y)) / (2.0f * ex.y)};
+    } else if (face < 4) {
+        p = v3(-ex.x + ux * (2.0f * ex.x), ex.y * sign, -ex.z + u.y * (2.0f * ex.z));
+        n = v3(0.0f, sign, 0.0f);
+        uv = V2{(p.x - (-ex.x)) / (2.0f * ex.x), (p.z - (-ex.z)) / (2.0f * ex.z)};
+    } else {
+        p = v3(-ex.x + ux * (2.0f * ex.x), -ex.y + u.y * (2.0f * ex.y), ex.z * sign);
+        n = v3(0.0f, 0.0f, sign);
+        uv = V2{(p.x - (-ex.x)) / (2.0f * ex.x), (p.y - (-ex.y)) / (2.0f * ex.y)};
+    }
+    return 1.0f / total;
+}
+
+__device__ __forceinline__ float shapeAreaPdf(const SceneView& s, int inst) {
+    const InstTrav& it = s.instT[inst];
+    const InstShade& is = s.instS[inst];
+    if (it.kind == kShapeMesh) {
+        float ta = s.meshes[is.meshId].totalArea;
+        return ta > 0.0f ? 1.0f / ta : 0.0f;
+    }
+    if (it.kind == kShapeSphere) return kInv4Pi / (is.radius * is.radius);
+    V3 d = v3(is.ext[0], is.ext[1], is.ext[2]) - (-v3(is.ext[0], is.ext[1], is.ext[2]));
+    return 1.0f / (2.0f * (d.x * d.y + d.x * d.z + d.y * d.z));
+}
+
+// AreaLight::eval (area.cpp:45-49)
+__device__ __forceinline__ V3 emitterEval(const Emitter& e, V3 n, V2 uv, V3 w) {
+    if (dot(n, w) > 0.0f) return evalTex(e.radiance, uv);
+    return v3s(0.0f);
+}
+
+// AreaLight::sample (area.cpp:51-88)
+__device__ __forceinline__ void emitterSample(const SceneView& s, int ei, V3 ref, V2 u, LightSample& ls) {
+    const Emitter e = s.emitters[ei];
+    const InstShade& is = s.instS[e.instance];
+    const InstTrav& it = s.instT[e.instance];
+    V3 lp, ln;
+    V2 luv;
+    float areaPdf = sampleShape(s, e.instance, u, lp, ln, luv);
+    ls.p = xfPoint(is.o2w, lp);
+    ls.n = normalize(xfNormal(it.w2o, ln));
+    ls.uv = luv;
+    Frame fr = frameFromNormal(ln);
+    V3 t1 = xfVector(is.o2w, fr.x), t2 = xfVector(is.o2w, fr.y);
+    float areaScale = length(cross(t1, t2));
+    if (areaScale > 0.0f) areaPdf /= areaScale;
+    ls.sd = normalize(ls.p - ref);
+    ls.stmax = length(ls.p - ref) - kEpsilon;
+    float dist = lengthSq(ref - ls.p);
+    float cosTheta = dot(ls.n, -ls.sd);
+    ls.pdf = 0.0f;
+    ls.Li = v3s(0.0f);
+    if (areaPdf <= kEpsilon || cosTheta <= kEpsilon) return;
+    ls.pdf = areaPdf * dist / cosTheta;
+    ls.Li = cdiv(emitterEval(e, ls.n, ls.uv, normalize(ref - ls.p)), ls.pdf);
+}
+
+// AreaLight::pdf (area.cpp:90-119)
+__device__ __forceinline__ float emitterPdf(const SceneView& s, int ei, V3 ref, V3 p, V3 n) {
+    const Emitter e = s.emitters[ei];
+    const InstShade& is = s.instS[e.instance];
+    float areaPdf = shapeAreaPdf(s, e.instance);
+    V3 ln = xfNormal(is.o2w, n);   // toLocal.normal: transpose(mat3(objectToWorld)) * n
+    Frame fr = frameFromNormal(ln);
+    V3 t1 = xfVector(is.o2w, fr.x), t2 = xfVector(is.o2w, fr.y);
+    float areaScale = length(cross(t1, t2));
+    if (areaScale > 0.0f) areaPdf /= areaScale;
+    float dist = lengthSq(ref - p);
+    V3 wi = normalize(p - ref);
+    float cosTheta = dot(n, -wi);
+    if (areaPdf <= kEpsilon || cosTheta <= kEpsilon) return 0.0f;
+    return areaPdf * dist / cosTheta;
+}
+
+// scene.h:28-34
+__device__ __forceinline__ int pickEmitter(int n, float rnd) {
+    int idx = (int)floorf((float)n * rnd);
+    return idx < n - 1 ? idx : n - 1;
+}
+
+// volPath.cpp:293-298
+__device__ __forceinline__ int nextMedium(V3 wo, V3 wi, int cur, V3 n, int mIn, int mOut) {
+    if (dot(wi, n) > 0.0f) return dot(wo, n) > 0.0f ? cur : mOut;
+    return dot(wo, n) > 0.0f ? mIn : cur;
+}
+
+// ---------------------------------------------------------------- path state helpers
+__device__ __forceinline__ void storeRng(PathState& ps, const Rng& r) {
+    ps.rngLo = (uint32_t)r.state;
+    ps.rngHi = (uint32_t)(r.state >> 32);
+}
+__device__ __forceinline__ Rng loadRng(const PathState& ps) {
+    return Rng{((uint64_t)ps.rngHi << 32) | ps.rngLo};
+}
+
+// Work item -> camera sample (integrator.h:88-125) in slot `slot`.
+__device__ __forceinline__ void generatePath(const JobDev& j, uint32_t jobIdx, uint64_t item, PathState& ps) {
+    int ww = j.wx1 - j.wx0;
+    uint64_t npix = (uint64_t)ww * (uint64_t)(j.wy1 - j.wy0);
+    uint32_t pass = (uint32_t)(item / npix) + (uint32_t)j.firstPass;
+    uint32_t pix = (uint32_t)(item % npix);
+    int x = j.wx0 + (int)(pix % (uint32_t)ww), y = j.wy0 + (int)(pix / (uint32_t)ww);
+    uint64_t key = (uint64_t)y * (uint64_t)j.W + (uint64_t)x + (uint64_t)pass * ((uint64_t)j.W * (uint64_t)j.H);
+    Rng r = rngSeed(key);
+    V2 ps2 = next2D(r);
+    float fx = (float)x + ps2.x, fy = (float)y + ps2.y;
+    float cx = fx / (float)j.W, cy = 1.0f - fy / (float)j.H;
+    next2D(r);   // lens sample (pinhole camera: unused)
+    next1D(r);   // chromatic aberration channel (unused without aberration)
+    next1D(r);   // time (static transforms)
+    // perspective.cpp:15-32
+    const Camera& cam = j.view.camera;
+    float px = (2.0f * cx - 1.0f) * cam.aspect * cam.scale;
+    float py = (2.0f * cy - 1.0f) * cam.scale;
+    V3 dir = normalize(v3(px, py, -1.0f));
+    V3 o = v3(cam.origin[0], cam.origin[1], cam.origin[2]);
+    V3 d = xfVector(cam.toWorld, dir);
+    ps.ox = o.x; ps.oy = o.y; ps.oz = o.z; ps.pdfPrev = 1.0f;
+    ps.dx = d.x; ps.dy = d.y; ps.dz = d.z;
+    ps.lastX = o.x; ps.lastY = o.y; ps.lastZ = o.z;
+    ps.tpr = ps.tpg = ps.tpb = 1.0f;
+    ps.Lr = ps.Lg = ps.Lb = 0.0f;
+    storeRng(ps, r);
+    ps.pixel = pix;
+    ps.pass = pass;
+    ps.bounces = 0;
+    ps.vsBounces = 0;
+    ps.medium = -1;                        // camera rays start in vacuum (ray.h:18)
+    ps.flags = 1u | (jobIdx << 8);         // specularBounce = true
+}
+
+// ---------------------------------------------------------------- kernels
+__global__ void kBeginIter(uint32_t* cnt) {
+    cnt[kQOut] = 0;
+    cnt[kQShadow] = 0;
+    cnt[kQDone] = 0;
+}
+
+// Plain mode: pass `pass` of job 0 for every window pixel, slot = pixel index.
+__global__ void __launch_bounds__(kBlock) kRaygenPass(KParams p, uint64_t itemBase, uint32_t n) {
+    const JobDev& j = p.jobs[0];
+    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        PathState ps;
+        generatePath(j, 0, itemBase + i, ps);
+        p.paths[i] = ps;
+        p.listIn[i] = i;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.cnt[kQIn] = n;
+}
+
+// Batched mode: fill slots [0, n) from the shared work counter.
+__global__ void __launch_bounds__(kBlock) kRaygenFill(KParams p, uint32_t n) {
+    const JobDev& j = p.jobs[0];
+    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        uint64_t item = j.workBegin + i;
+        PathState ps;
+        generatePath(j, 0, item, ps);
+        p.paths[i] = ps;
+        p.listIn[i] = i;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        p.cnt[kQIn] = n;
+        *p.workNext = j.workBegin + n;
+    }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kBlock) kExtend(KParams p) {
+    __shared__ uint32_t stack[kStackSize * kBlock];
+    uint32_t* stk = stack + threadIdx.x;
+    const uint32_t n = p.cnt[kQIn];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[0], (unsigned long long)n);
+    int err = 0;
+    TraceCounters cnt{0, 0};
+    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        uint32_t slot = p.listIn[i];
+        const PathState* ps = p.paths + slot;
+        float4 a = *reinterpret_cast<const float4*>(&ps->ox);
+        float4 b = *reinterpret_cast<const float4*>(&ps->dx);
+        uint32_t job = ps->flags >> 8;
+        TRay r;
+        r.o = v3(a.x, a.y, a.z);
+        r.d = v3(b.x, b.y, b.z);
+        r.tmin = kEpsilon;
+        r.tmax = INFINITY;
+        THit h;
+        err |= traceRay<kBlock, false, false, COUNT>(p.jobs[job].view, r, h, stk, &cnt, nullptr);
+        HitRec hr;
+        hr.t = h.t; hr.u = h.u; hr.v = h.v; hr.inst = h.inst; hr.slot = h.slot;
+        hr.pad[0] = hr.pad[1] = hr.pad[2] = 0;
+        p.hits[slot] = hr;
+    }
+    if (COUNT) {
+        unsigned long long nn = cnt.nodes, nt = cnt.tris;
+        for (int o = 16; o > 0; o >>= 1) {
+            nn += __shfl_down_sync(0xffffffffu, nn, o);
+            nt += __shfl_down_sync(0xffffffffu, nt, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&p.totals[3], nn);
+            atomicAdd(&p.totals[4], nt);
+        }
+    }
+    if (err) atomicOr(p.errWord, (uint32_t)err);
+}
+
+// One bounce of path (VOL = false) or volpath (VOL = true).
+template <bool VOL>
+__global__ void __launch_bounds__(kBlock) kShade(KParams p) {
+    const uint32_t n = p.cnt[kQIn];
+    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        uint32_t slot = p.listIn[i];
+        PathState ps = p.paths[slot];
+        const HitRec h = p.hits[slot];
+        const uint32_t jobIdx = ps.flags >> 8;
+        const JobDev& j = p.jobs[jobIdx];
+        const SceneView& s = j.view;
+        Rng rng = loadRng(ps);
+        V3 o = v3(ps.ox, ps.oy, ps.oz), d = v3(ps.dx, ps.dy, ps.dz);
+        V3 tp = v3(ps.tpr, ps.tpg, ps.tpb), L = v3(ps.Lr, ps.Lg, ps.Lb);
+        V3 last = v3(ps.lastX, ps.lastY, ps.lastZ);
+        uint32_t bounces = ps.bounces & 0xFFFFu, nullB = ps.bounces >> 16;
+        uint32_t volB = ps.vsBounces & 0xFFFFu, surfB = ps.vsBounces >> 16;
+        bool specular = (ps.flags & 1u) != 0;
+        float pdfPrev = ps.pdfPrev;
+        int medium = ps.medium;
+        const float nL = (float)s.numEmitters;
+        bool cont = false, terminate = false, emitShadow = false;
+        ShadowRec sr;
+        const bool hit = h.inst >= 0;
+
+        do {
+            if (VOL && medium >= 0) {
+                // medium->sample (homogeneous.cpp:32-63); the ray's tMax is the hit distance
+                const Medium m = s.media[medium];
+                float rtmax = hit ? h.t : INFINITY;
+                float u0 = next1D(rng);
+                float u1 = next1D(rng);
+                int ch = min((int)(u0 * 3.0f), 2);
+                float sig = ch == 0 ? m.sigT[0] : (ch == 1 ? m.sigT[1] : m.sigT[2]);
+                float dist = -logf(1.0f - u1) / sig;
+                float t = fminf_(dist, rtmax);
+                bool sampled = t < rtmax;
+                V3 tr = v3(expf(-m.sigT[0] * t), expf(-m.sigT[1] * t), expf(-m.sigT[2] * t));
+                V3 pc = sampled ? v3(m.sigT[0], m.sigT[1], m.sigT[2]) * tr : tr;
+                float pdf = (pc.x + pc.y + pc.z) / 3.0f;
+                if (pdf == 0.0f) tp = tp * v3s(0.0f);
+                else tp = tp * cdiv(tr, pdf);
+                if (sampled) {
+                    // volumetric scattering event (volPath.cpp:47-112)
+                    V3 mp = o + d * t;
+                    V3 wo = -d;
+                    tp = tp * v3(m.sigS[0], m.sigS[1], m.sigS[2]);
+                    if (isBlack(tp)) { terminate = true; break; }
+                    float lightSelectPdf = 1.0f / nL;
+                    int ei = pickEmitter(s.numEmitters, next1D(rng));
+                    LightSample ls;
+                    emitterSample(s, ei, mp, next2D(rng), ls);
+                    V3 Li = ls.Li * (1.0f / lightSelectPdf);
+                    if (ls.pdf > 1e-6f && !isBlack(Li)) {
+                        V3 wi = normalize(ls.p - mp);
+                        float g = hgClampG(m.g);
+                        float phasePdf = phaseHG(dot(wo, wi), g);
+                        if (phasePdf > 1e-6f) {
+                            float pl = ls.pdf * lightSelectPdf;
+                            float wl = powerHeuristic(pl, phasePdf);
+                            V3 c = ((tp * phasePdf) * Li) * wl;   // Tr applied by the shadow pass
+                            sr.ox = mp.x; sr.oy = mp.y; sr.oz = mp.z; sr.tmax = ls.stmax;
+                            sr.dx = ls.sd.x; sr.dy = ls.sd.y; sr.dz = ls.sd.z; sr.slot = slot;
+                            sr.cr = c.x; sr.cg = c.y; sr.cb = c.z; sr.medium = medium;
+                            sr.lx = ls.p.x; sr.ly = ls.p.y; sr.lz = ls.p.z; sr.pad = 0;
+                            emitShadow = true;
+                        }
+                    }
+                    V3 wi;
+                    pdfPrev = hgSample(hgClampG(m.g), wo, wi, next2D(rng));
+                    specular = false;
+                    last = mp;
+                    o = mp;
+                    d = wi;
+                    if (volB > 6) {
+                        float q = fmaxf_(0.05f, fminf_(luminance(tp), 0.99f));
+                        if (next1D(rng) > q) { terminate = true; break; }
+                        tp = tp * (1.0f / q);
+                    }
+                    bounces++;
+                    volB = min(volB + 1, 0xFFFFu);
+                    cont = true;
+                    break;
+                }
+            }
+            const int curMedium = medium;
+            if (!hit) { terminate = true; break; }
+            SurfInt si = surfaceInteraction(s, h, o, d);
+            const InstShade& is = s.instS[h.inst];
+            const Material mat = s.materials[is.material];
+            Bsdf bsdf;
+            const bool hasBsdf = makeLobe(mat, si.uv, bsdf.lobe);
+            if (is.emitter >= 0) {
+                bool skip = (bounces == 0 && !hasBsdf);
+                if (!skip) {
+                    const Emitter e = s.emitters[is.emitter];
+                    V3 Le = emitterEval(e, si.n, si.uv, -d);
+                    if (!isBlack(Le)) {
+                        float w = 1.0f;
+                        if (!specular) {
+                            float lightPdf = emitterPdf(s, is.emitter, last, si.p, si.n);
+                            float pl = lightPdf * (1.0f / nL);
+                            w = powerHeuristic(pdfPrev, pl);
+                        }
+                        L = L + (tp * Le) * w;
+                    }
+                }
+            }
+            if (!hasBsdf) {
+                // pass-through boundary (path.cpp:87-92, volPath.cpp:171-177)
+                if (nullB++ > 100) { terminate = true; break; }
+                if (VOL) {
+                    medium = is.hasMedia ? (dot(d, si.n) > 0.0f ? is.mediumOut : is.mediumIn) : -1;
+                }
+                o = si.p;
+                cont = true;
+                break;
+            }
+            bsdf.fr = shadingFrame(si.n, si.dpdu);
+            // next event estimation (path.cpp:104-151, volPath.cpp:193-220)
+            float lightSelectPdf = 1.0f / nL;
+            int ei = pickEmitter(s.numEmitters, next1D(rng));
+            LightSample ls;
+            emitterSample(s, ei, si.p, next2D(rng), ls);
+            V3 Li = ls.Li * (1.0f / lightSelectPdf);
+            if (ls.pdf > 1e-6f && !isBlack(Li)) {
+                V3 wi = normalize(ls.p - si.p);
+                float bp = bsdfPdf(bsdf, -d, wi);
+                V3 f = bsdfF(bsdf, -d, wi);
+                if (!isBlack(f) && bp > 1e-6f) {
+                    float pl = ls.pdf * lightSelectPdf;
+                    float wl = powerHeuristic(pl, bp);
+                    V3 c = (((tp * f) * Li) * fabsf(dot(si.n, wi))) * wl;
+                    int smed = -1;
+                    if (VOL) smed = nextMedium(-d, ls.sd, curMedium, si.n, is.hasMedia ? is.mediumIn : -1, is.hasMedia ? is.mediumOut : -1);
+                    sr.ox = si.p.x; sr.oy = si.p.y; sr.oz = si.p.z; sr.tmax = ls.stmax;
+                    sr.dx = ls.sd.x; sr.dy = ls.sd.y; sr.dz = ls.sd.z; sr.slot = slot;
+                    sr.cr = c.x; sr.cg = c.y; sr.cb = c.z; sr.medium = smed;
+                    sr.lx = ls.p.x; sr.ly = ls.p.y; sr.lz = ls.p.z; sr.pad = 0;
+                    emitShadow = true;
+                }
+            }
+            // BSDF sampling (path.cpp:153-172, volPath.cpp:222-245)
+            V2 u2 = next2D(rng);
+            float u1 = next1D(rng);
+            V3 wi;
+            uint32_t type = 0;
+            V3 fcos = bsdfSample(bsdf, -d, wi, u2, u1, pdfPrev, type);
+            if (isBlack(fcos) || pdfPrev <= 1e-6f) { terminate = true; break; }
+            specular = (type & kSpecular) != 0;
+            tp = tp * fcos;
+            if (VOL) {
+                V3 incident = -d;
+                last = si.p;
+                o = si.p;
+                medium = nextMedium(incident, wi, curMedium, si.n, is.hasMedia ? is.mediumIn : -1, is.hasMedia ? is.mediumOut : -1);
+                d = wi;
+                if (surfB > 2) {
+                    float q = fmaxf_(0.05f, fminf_(luminance(tp), 0.99f));
+                    if (next1D(rng) > q) { terminate = true; break; }
+                    tp = tp * (1.0f / q);
+                }
+                surfB = min(surfB + 1, 0xFFFFu);
+            } else {
+                if (bounces > 2) {
+                    float q = fmaxf_(0.05f, fminf_(luminance(tp), 0.99f));
+                    if (next1D(rng) > q) { terminate = true; break; }
+                    tp = tp * (1.0f / q);
+                }
+                last = si.p;
+                o = si.p;
+                d = wi;
+            }
+            bounces++;
+            cont = true;
+        } while (false);
+
+        if (cont && bounces >= (uint32_t)j.maxDepth) { cont = false; terminate = true; }
+        ps.ox = o.x; ps.oy = o.y; ps.oz = o.z; ps.pdfPrev = pdfPrev;
+        ps.dx = d.x; ps.dy = d.y; ps.dz = d.z;
+        ps.tpr = tp.x; ps.tpg = tp.y; ps.tpb = tp.z;
+        ps.Lr = L.x; ps.Lg = L.y; ps.Lb = L.z;
+        ps.lastX = last.x; ps.lastY = last.y; ps.lastZ = last.z;
+        storeRng(ps, rng);
+        ps.bounces = (bounces & 0xFFFFu) | (min(nullB, 0xFFFFu) << 16);
+        ps.vsBounces = (volB & 0xFFFFu) | (surfB << 16);
+        ps.medium = medium;
+        ps.flags = (ps.flags & ~1u) | (specular ? 1u : 0u);
+        p.paths[slot] = ps;
+        uint32_t k = warpAppend(&p.cnt[kQShadow], emitShadow);
+        if (emitShadow) p.shadow[k] = sr;
+        uint32_t c = warpAppend(&p.cnt[kQOut], cont);
+        if (cont) p.listOut[c] = slot;
+        uint32_t dn = warpAppend(&p.cnt[kQDone], terminate);
+        if (terminate) p.done[dn] = slot;
+    }
+}
+
+// Shadow queries. Path: the reference traces closest hits and treats the segment as
+// occluded when the first surface has a BSDF (path.cpp:124-140; a null-BSDF first hit
+// leaves the segment unoccluded because the next segment's tMax is ~0); with no null
+// materials this is a plain any-hit query. Volpath: evaluateTr (volPath.cpp:261-291).
+template <bool VOL>
+__global__ void __launch_bounds__(kBlock) kShadow(KParams p) {
+    __shared__ uint32_t stack[kStackSize * kBlock];
+    uint32_t* stk = stack + threadIdx.x;
+    const uint32_t n = p.cnt[kQShadow];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
+    int err = 0;
+    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        const ShadowRec sr = p.shadow[i];
+        const uint32_t slot = sr.slot;
+        const uint32_t jobIdx = p.paths[slot].flags >> 8;
+        const JobDev& j = p.jobs[jobIdx];
+        const SceneView& s = j.view;
+        TRay r;
+        r.o = v3(sr.ox, sr.oy, sr.oz);
+        r.d = v3(sr.dx, sr.dy, sr.dz);
+        r.tmin = kEpsilon;
+        r.tmax = sr.tmax;
+        V3 c = v3(sr.cr, sr.cg, sr.cb);
+        bool clear;
+        if (!VOL) {
+            THit h;
+            if (j.hasNull) {
+                err |= traceRay<kBlock, false, false, false>(s, r, h, stk, nullptr, nullptr);
+                clear = h.inst < 0 || j.nullMask[h.inst];
+            } else {
+                err |= traceRay<kBlock, true, false, false>(s, r, h, stk, nullptr, nullptr);
+                clear = h.inst < 0;
+            }
+        } else {
+            V3 Tr = v3s(1.0f);
+            int medium = sr.medium;
+            V3 lightP = v3(sr.lx, sr.ly, sr.lz);
+            clear = true;
+            for (int seg = 0; seg < 256; ++seg) {
+                THit h;
+                err |= traceRay<kBlock, false, false, false>(s, r, h, stk, nullptr, nullptr);
+                bool hit = h.inst >= 0;
+                if (medium >= 0) {
+                    float segT = hit ? h.t : r.tmax;
+                    Tr = Tr * mediumTr(s.media[medium], segT);
+                }
+                if (isBlack(Tr)) { clear = false; break; }
+                if (!hit) break;
+                if (!j.nullMask[h.inst]) { clear = false; break; }
+                HitRec hr;
+                hr.t = h.t; hr.u = h.u; hr.v = h.v; hr.inst = h.inst; hr.slot = h.slot;
+                SurfInt si = surfaceInteraction(s, hr, r.o, r.d);
+                const InstShade& is = s.instS[h.inst];
+                medium = is.hasMedia ? (dot(r.d, si.n) > 0.0f ? is.mediumOut : is.mediumIn) : -1;
+                r.o = si.p;
+                r.tmin = kEpsilon;
+                r.tmax = length(si.p - lightP) - kEpsilon;
+                if (seg == 255) { clear = false; err |= 16; }
+            }
+            c = c * Tr;
+        }
+        if (clear) {
+            PathState* ps = p.paths + slot;
+            ps->Lr = ps->Lr + c.x;
+            ps->Lg = ps->Lg + c.y;
+            ps->Lb = ps->Lb + c.z;
+        }
+    }
+    if (err) atomicOr(p.errWord, (uint32_t)err);
+}
+
+__device__ __forceinline__ unsigned long long toFixed(float x) {
+    x = fminf_(fmaxf_(x, 0.0f), kFixMax);
+    return (unsigned long long)__float2ll_rn(x * kFixScale);
+}
+
+// film.h:26-69 splat of one finished sample (NaN/Inf zeroed as integrator.h:137-141).
+__device__ __forceinline__ void filmSplat(const JobDev& j, const PathState& ps) {
+    V3 L = v3(ps.Lr, ps.Lg, ps.Lb);
+    if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = v3s(0.0f);
+    int ww = j.wx1 - j.wx0;
+    int x = j.wx0 + (int)(ps.pixel % (uint32_t)ww), y = j.wy0 + (int)(ps.pixel / (uint32_t)ww);
+    uint64_t key = (uint64_t)y * (uint64_t)j.W + (uint64_t)x + (uint64_t)ps.pass * ((uint64_t)j.W * (uint64_t)j.H);
+    Rng r = rngSeed(key);
+    V2 s2 = next2D(r);
+    float fx = (float)x + s2.x, fy = (float)y + s2.y;
+    int x0 = max(0, (int)ceilf(fx - j.frx - 0.5f));
+    int x1 = min(j.W - 1, (int)floorf(fx + j.frx - 0.5f));
+    int y0 = max(0, (int)ceilf(fy - j.fry - 0.5f));
+    int y1 = min(j.H - 1, (int)floorf(fy + j.fry - 0.5f));
+    for (int py = y0; py <= y1; ++py) {
+        for (int px = x0; px <= x1; ++px) {
+            float ox = fx - ((float)px + 0.5f), oy = fy - ((float)py + 0.5f);
+            float w;
+            if (j.filter == 0) {
+                w = (fabsf(ox) <= j.frx && fabsf(oy) <= j.fry) ? 1.0f : 0.0f;
+            } else {
+                float gx = fmaxf_(0.0f, expf(-j.falpha * ox * ox) - j.fexpX);
+                float gy = fmaxf_(0.0f, expf(-j.falpha * oy * oy) - j.fexpY);
+                w = gx * gy;
+            }
+            if (w > 0.0f) {
+                size_t idx = (size_t)py * (size_t)j.W + (size_t)px;
+                atomicAdd(&j.filmSum[idx * 4 + 0], toFixed(L.x * w));
+                atomicAdd(&j.filmSum[idx * 4 + 1], toFixed(L.y * w));
+                atomicAdd(&j.filmSum[idx * 4 + 2], toFixed(L.z * w));
+                atomicAdd(&j.filmSum[idx * 4 + 3], toFixed(w));
+                atomicAdd(&j.filmSq[idx * 3 + 0], L.x * L.x * w);
+                atomicAdd(&j.filmSq[idx * 3 + 1], L.y * L.y * w);
+                atomicAdd(&j.filmSq[idx * 3 + 2], L.z * L.z * w);
+            }
+        }
+    }
+}
+
+// Finished paths: film splat; in batched mode the slot takes the next work item.
+__global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
+    const uint32_t n = p.cnt[kQDone];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[2], (unsigned long long)n);
+    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        uint32_t slot = p.done[i];
+        PathState ps = p.paths[slot];
+        const uint32_t jobIdx = ps.flags >> 8;
+        const JobDev& j = p.jobs[jobIdx];
+        filmSplat(j, ps);
+        bool refill = false;
+        uint64_t item = 0;
+        if (p.batched) {
+            item = atomicAdd(p.workNext, 1ull);
+            refill = item < j.workEnd;
+            if (refill) {
+                generatePath(j, jobIdx, item, ps);
+                p.paths[slot] = ps;
+            }
+        }
+        uint32_t k = warpAppend(&p.cnt[kQOut], refill);
+        if (refill) p.listOut[k] = slot;
+    }
+}
+
+// ---------------------------------------------------------------- host driver
+Wavefront::Wavefront(Context* c) : ctx_(c) {
+    counters_.alloc(kQCount * sizeof(uint32_t));
+    totals_.alloc(8 * sizeof(unsigned long long));
+    job_.alloc(sizeof(JobDev));
+    workNext_.alloc(sizeof(unsigned long long));
+}
 Wavefront::~Wavefront() = default;
 
+void Wavefront::ensureCapacity(size_t slots) {
+    if (slots <= cap_) return;
+    paths_.alloc(slots * sizeof(PathState));
+    hits_.alloc(slots * sizeof(HitRec));
+    listA_.alloc(slots * sizeof(uint32_t));
+    listB_.alloc(slots * sizeof(uint32_t));
+    shadow_.alloc(slots * sizeof(ShadowRec));
+    done_.alloc(slots * sizeof(uint32_t));
+    cap_ = slots;
+}
+
+Wavefront::Result Wavefront::render(DeviceScene& ds, int spp, int firstPass, int maxDepth, int integrator,
+                                    const int window[4], bool batched, int profile, float* filmHost, gnd_progress_fn cb,
+                                    void* user) {
+    Context* c = ctx_;
+    cudaStream_t st = c->stream;
+    const int W = ds.width, H = ds.height;
+    if (W <= 0 || H <= 0) throw Error(GND_ERR_INVALID, "scene has no camera film size");
+    if (ds.view.numEmitters <= 0) throw Error(GND_ERR_INVALID, "the path integrators need at least one emitter");
+    int wx0 = 0, wy0 = 0, wx1 = W, wy1 = H;
+    if (window && (window[0] | window[1] | window[2] | window[3])) {
+        wx0 = window[0]; wy0 = window[1]; wx1 = window[2]; wy1 = window[3];
+        if (wx0 < 0 || wy0 < 0 || wx1 > W || wy1 > H || wx0 >= wx1 || wy0 >= wy1) throw Error(GND_ERR_INVALID, "bad pixel window");
+    }
+    const uint64_t npix = (uint64_t)(wx1 - wx0) * (uint64_t)(wy1 - wy0);
+    const uint64_t total = npix * (uint64_t)spp;
+    if (npix > (1ull << 31)) throw Error(GND_ERR_INVALID, "window too large");
+    // slot pool: one pass for plain renders, up to ~4M in-flight paths for batched ones
+    size_t slots = batched ? (size_t)std::min<uint64_t>(total, std::max<uint64_t>(npix, 1ull << 22)) : (size_t)npix;
+    ensureCapacity(std::max<size_t>(slots, 1));
+    filmSum_.ensure((size_t)W * H * 4 * sizeof(unsigned long long));
+    filmSq_.ensure((size_t)W * H * 3 * sizeof(float));
+    GND_CUDA(cudaMemsetAsync(filmSum_.ptr, 0, (size_t)W * H * 4 * sizeof(unsigned long long), st));
+    GND_CUDA(cudaMemsetAsync(filmSq_.ptr, 0, (size_t)W * H * 3 * sizeof(float), st));
+    GND_CUDA(cudaMemsetAsync(totals_.ptr, 0, 8 * sizeof(unsigned long long), st));
+
+    JobDev jd{};
+    jd.view = ds.view;
+    jd.nullMask = ds.nullMask.as<uint8_t>();
+    jd.filmSum = filmSum_.as<unsigned long long>();
+    jd.filmSq = filmSq_.as<float>();
+    jd.W = W; jd.H = H; jd.maxDepth = maxDepth; jd.integrator = integrator;
+    jd.wx0 = wx0; jd.wy0 = wy0; jd.wx1 = wx1; jd.wy1 = wy1;
+    jd.filter = ds.filter;
+    jd.frx = ds.filter == 0 ? 0.5f : ds.filterRadius[0];
+    jd.fry = ds.filter == 0 ? 0.5f : ds.filterRadius[1];
+    jd.falpha = ds.filterAlpha;
+    jd.fexpX = std::exp(-jd.falpha * jd.frx * jd.frx);   // filter.h:39-40
+    jd.fexpY = std::exp(-jd.falpha * jd.fry * jd.fry);
+    jd.hasNull = ds.hasNullMaterials ? 1 : 0;
+    jd.firstPass = firstPass;
+    jd.workBegin = 0;
+    jd.workEnd = total;
+    GND_CUDA(cudaMemcpyAsync(job_.ptr, &jd, sizeof(JobDev), cudaMemcpyHostToDevice, st));
+
+    KParams kp{};
+    kp.jobs = job_.as<JobDev>();
+    kp.paths = paths_.as<PathState>();
+    kp.hits = hits_.as<HitRec>();
+    kp.shadow = shadow_.as<ShadowRec>();
+    kp.done = done_.as<uint32_t>();
+    kp.cnt = counters_.as<uint32_t>();
+    kp.totals = totals_.as<unsigned long long>();
+    kp.workNext = workNext_.as<unsigned long long>();
+    kp.errWord = c->errWord.as<uint32_t>();
+    kp.capacity = (uint32_t)cap_;
+    kp.batched = batched ? 1 : 0;
+    uint32_t* lists[2] = {listA_.as<uint32_t>(), listB_.as<uint32_t>()};
+
+    const int grid = c->numSMs * 8;
+    cudaEvent_t e0, e1;
+    GND_CUDA(cudaEventCreate(&e0));
+    GND_CUDA(cudaEventCreate(&e1));
+    GND_CUDA(cudaEventRecord(e0, st));
+    Result res;
+    std::vector<float> passFilm;
+    std::vector<cudaEvent_t> evs;   // extend start/stop pairs when timing
+    auto runLoop = [&](int maxIter) {
+        int cur = 0;
+        uint32_t hostCnt = 1;
+        for (int it = 0; it < maxIter; ++it) {
+            kp.listIn = lists[cur];
+            kp.listOut = lists[cur ^ 1];
+            kBeginIter<<<1, 1, 0, st>>>(kp.cnt);
+            res.iterations++;
+            cudaEvent_t ea = nullptr, eb = nullptr;
+            if (profile & 1) {
+                GND_CUDA(cudaEventCreate(&ea));
+                GND_CUDA(cudaEventCreate(&eb));
+                GND_CUDA(cudaEventRecord(ea, st));
+            }
+            if (profile & 2) kExtend<true><<<grid, kBlock, 0, st>>>(kp);
+            else kExtend<false><<<grid, kBlock, 0, st>>>(kp);
+            if (profile & 1) {
+                GND_CUDA(cudaEventRecord(eb, st));
+                evs.push_back(ea);
+                evs.push_back(eb);
+            }
+            if (integrator == 1) kShade<true><<<grid, kBlock, 0, st>>>(kp);
+            else kShade<false><<<grid, kBlock, 0, st>>>(kp);
+            if (integrator == 1) kShadow<true><<<grid, kBlock, 0, st>>>(kp);
+            else kShadow<false><<<grid, kBlock, 0, st>>>(kp);
+            kRetire<<<grid, kBlock, 0, st>>>(kp);
+            GND_CUDA(cudaGetLastError());
+            // next iteration reads the list just written; move its count into kQIn
+            cudaMemcpyAsync(kp.cnt + kQIn, kp.cnt + kQOut, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+            cur ^= 1;
+            if ((it & 3) == 3 || it < 4) {
+                GND_CUDA(cudaMemcpyAsync(&hostCnt, kp.cnt + kQIn, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                GND_CUDA(cudaStreamSynchronize(st));
+                if (hostCnt == 0) return;
+            }
+        }
+        throw Error(GND_ERR_DEVICE_CHECK, "path iteration limit reached");
+    };
+    const int maxIter = maxDepth * 2 + 512;
+    if (!batched) {
+        for (int s = 0; s < spp; ++s) {
+            if (c->cancel) break;
+            kp.listIn = lists[0];
+            kRaygenPass<<<grid, kBlock, 0, st>>>(kp, (uint64_t)s * npix, (uint32_t)npix);
+            GND_CUDA(cudaGetLastError());
+            runLoop(maxIter);
+            res.passesDone = s + 1;
+            if (cb) {
+                // film so far, as the reference's per-pass resolve + callback
+                passFilm.assign((size_t)W * H * 7, 0.0f);
+                std::vector<unsigned long long> fs((size_t)W * H * 4);
+                std::vector<float> fq((size_t)W * H * 3);
+                GND_CUDA(cudaMemcpyAsync(fs.data(), filmSum_.ptr, fs.size() * 8, cudaMemcpyDeviceToHost, st));
+                GND_CUDA(cudaMemcpyAsync(fq.data(), filmSq_.ptr, fq.size() * 4, cudaMemcpyDeviceToHost, st));
+                GND_CUDA(cudaStreamSynchronize(st));
+                for (size_t q = 0; q < (size_t)W * H; ++q) {
+                    for (int k = 0; k < 4; ++k) passFilm[q * 7 + k] = (float)((double)fs[q * 4 + k] / 16777216.0);
+                    for (int k = 0; k < 3; ++k) passFilm[q * 7 + 4 + k] = fq[q * 3 + k];
+                }
+                cb(user, firstPass + s, passFilm.data(), W, H);
+            }
+        }
+    } else {
+        kp.listIn = lists[0];
+        kRaygenFill<<<grid, kBlock, 0, st>>>(kp, (uint32_t)slots);
+        GND_CUDA(cudaGetLastError());
+        runLoop(maxIter * std::max(1, spp) + 64);
+        res.passesDone = spp;
+    }
+    GND_CUDA(cudaEventRecord(e1, st));
+    unsigned long long tot[8];
+    GND_CUDA(cudaMemcpyAsync(tot, totals_.ptr, sizeof(tot), cudaMemcpyDeviceToHost, st));
+    std::vector<unsigned long long> fs((size_t)W * H * 4);
+    std::vector<float> fq((size_t)W * H * 3);
+    GND_CUDA(cudaMemcpyAsync(fs.data(), filmSum_.ptr, fs.size() * 8, cudaMemcpyDeviceToHost, st));
+    GND_CUDA(cudaMemcpyAsync(fq.data(), filmSq_.ptr, fq.size() * 4, cudaMemcpyDeviceToHost, st));
+    GND_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (size_t k = 0; k + 1 < evs.size(); k += 2) {
+        float em = 0.f;
+        cudaEventElapsedTime(&em, evs[k], evs[k + 1]);
+        res.extendMs += em;
+        cudaEventDestroy(evs[k]);
+        cudaEventDestroy(evs[k + 1]);
+    }
+    c->checkKernelErrors("render");
+    for (size_t q = 0; q < (size_t)W * H; ++q) {
+        for (int k = 0; k < 4; ++k) filmHost[q * 7 + k] += (float)((double)fs[q * 4 + k] / 16777216.0);
+        for (int k = 0; k < 3; ++k) filmHost[q * 7 + 4 + k] += fq[q * 3 + k];
+    }
+    res.paths = (int64_t)tot[2];
+    res.rays = (int64_t)(tot[0] + tot[1]);
+    res.extendRays = (int64_t)tot[0];
+    res.shadowRays = (int64_t)tot[1];
+    res.extendNodes = (int64_t)tot[3];
+    res.extendTris = (int64_t)tot[4];
+    res.ms = ms;
+    return res;
+}
+
 }  // namespace gnd
+
+using namespace gnd;
+
+extern "C" {
+
+gnd_status gnd_gpu_render(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_render_params* prm, float* film, gnd_render_stats* stats) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (!film) throw Error(GND_ERR_INVALID, "null film buffer");
+        c->bind();
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceScene& ds = c->scene(id);
+        gnd_render_params p{};
+        if (prm) p = *prm;
+        int spp = p.spp > 0 ? p.spp : ds.spp;
+        int maxDepth = p.max_depth > 0 ? p.max_depth : ds.maxDepth;
+        int integ = p.integrator >= 0 && prm ? p.integrator : ds.integrator;
+        if (integ != 0 && integ != 1) throw Error(GND_ERR_INVALID, "integrator must be 0 (path_gpu) or 1 (volpath_gpu)");
+        if (maxDepth > 65535) maxDepth = 65535;
+        if (!c->wave) c->wave = std::make_unique<Wavefront>(c);
+        c->cancel = false;
+        Wavefront::Result r = c->wave->render(ds, spp, p.first_pass, maxDepth, integ, p.window, p.batched != 0, p.profile,
+                                              film, p.batched ? nullptr : p.callback, p.user);
+        if (stats) {
+            stats->paths = r.paths;
+            stats->rays = r.rays;
+            stats->passes_done = r.passesDone;
+            stats->ms = r.ms;
+            stats->extend_rays = r.extendRays;
+            stats->shadow_rays = r.shadowRays;
+            stats->extend_nodes = r.extendNodes;
+            stats->extend_tris = r.extendTris;
+            stats->extend_ms = r.extendMs;
+            stats->iterations = r.iterations;
+        }
+        if (c->cancel && r.passesDone < spp) throw Error(GND_ERR_CANCELLED, "render cancelled");
+    });
+}
+
+gnd_status gnd_gpu_cancel(gnd_gpu_ctx* ctxh) {
+    return guarded([&]() { ctxOf(ctxh)->cancel = true; });
+}
+
+}  // extern "C"

@@ -1,16 +1,85 @@
-// Wavefront path-tracing engine (declared here, defined in wavefront.cu).
+// Wavefront path-tracing engine: path state in HBM, per-bounce kernels (extend =
+// closest hit, shade = one bounce of path / volpath, shadow = occlusion or
+// transmittance, retire = film accumulation and slot refill), queues of path slots
+// with warp-aggregated appends.
 #pragma once
+#include <vector>
+
 #include "runtime.h"
 
 namespace gnd {
+
+// Path state, one 96-byte record per slot.
+struct alignas(16) PathState {
+    float ox, oy, oz, pdfPrev;
+    float dx, dy, dz, lastX;
+    float tpr, tpg, tpb, lastY;
+    float Lr, Lg, Lb, lastZ;
+    uint32_t rngLo, rngHi, pixel, pass;   // pixel = index in the job's window
+    uint32_t bounces;                     // bounces | nullBounces << 16
+    uint32_t vsBounces;                   // volumeBounces | surfaceBounces << 16 (saturating)
+    int32_t medium;                       // -1: vacuum
+    uint32_t flags;                       // bit0 specularBounce, bits 8..31 job index
+};
+static_assert(sizeof(PathState) == 96, "PathState must be 96 bytes");
+
+struct alignas(16) HitRec {
+    float t, u, v;
+    int32_t inst;
+    uint32_t slot;
+    uint32_t pad[3];
+};
+
+// Shadow work item: an occlusion (path) or transmittance (volpath) query whose
+// contribution is added to the owning path's radiance when the segment is clear.
+struct alignas(16) ShadowRec {
+    float ox, oy, oz, tmax;
+    float dx, dy, dz;
+    uint32_t slot;
+    float cr, cg, cb;
+    int32_t medium;
+    float lx, ly, lz;
+    uint32_t pad;
+};
+
+// One render job as the kernels see it.
+struct JobDev {
+    SceneView view;
+    const uint8_t* nullMask;
+    unsigned long long* filmSum;   // per pixel: sum wL (r, g, b) and sum w, fixed point 2^-24
+    float* filmSq;                 // per pixel: sum w L^2 (r, g, b)
+    int32_t W, H, maxDepth, integrator;
+    int32_t wx0, wy0, wx1, wy1;    // pixel window
+    int32_t filter;                // 0 box, 1 gaussian
+    float frx, fry, falpha, fexpX, fexpY;
+    int32_t hasNull;
+    int32_t firstPass;
+    uint64_t workBegin, workEnd;   // work items [begin, end): item -> (pass, window pixel)
+};
+
+// Queue counters (device): ints.
+enum QCounter : int { kQIn = 0, kQOut = 1, kQShadow = 2, kQDone = 3, kQCount = 8 };
 
 class Wavefront {
 public:
     explicit Wavefront(Context* c);
     ~Wavefront();
+    // Renders jobs[0] (plain: one pass in flight at a time; batched: all passes share
+    // the slot pool and refill it). Returns paths and rays traced.
+    struct Result {
+        int64_t paths = 0, rays = 0, extendRays = 0, shadowRays = 0, extendNodes = 0, extendTris = 0, iterations = 0;
+        int passesDone = 0;
+        double ms = 0.0, extendMs = 0.0;
+    };
+    Result render(DeviceScene& ds, int spp, int firstPass, int maxDepth, int integrator, const int window[4],
+                  bool batched, int profile, float* filmHost, gnd_progress_fn cb, void* user);
 
 private:
+    void ensureCapacity(size_t slots);
     Context* ctx_;
+    size_t cap_ = 0;
+    DevBuf paths_, hits_, listA_, listB_, shadow_, done_, counters_, totals_, job_, workNext_;
+    DevBuf filmSum_, filmSq_;
 };
 
 }  // namespace gnd

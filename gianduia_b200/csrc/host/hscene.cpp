@@ -712,6 +712,8 @@ void Scene::build() {
         fs->camera.height = m_camera->height;
         fs->camera.scale = std::tan((gnd::kPi / 180.f) * (m_camera->fov * 0.5f));
         fs->camera.aspect = m_camera->width / (float)m_camera->height;
+        V3 org = m_camera->toWorld.point(gnd::v3s(0.0f));
+        fs->camera.origin[0] = org.x; fs->camera.origin[1] = org.y; fs->camera.origin[2] = org.z;
     }
     fs->fillDesc();
     gnd_scene_desc& d = fs->desc;

@@ -128,9 +128,11 @@ struct alignas(16) Medium {
 
 // ---------------------------------------------------------------- camera
 struct alignas(16) Camera {
-    Xf34 toWorld;
+    Xf34 toWorld;             // directions: toWorld(vector)
     int32_t width, height;
     float scale, aspect;      // tan(fov/2), width/height
+    float origin[3];          // toWorld(point(0,0,0)) evaluated on the host with the
+    float pad;                // homogeneous divide of transform.h:330-337
 };
 
 // ---------------------------------------------------------------- scene view

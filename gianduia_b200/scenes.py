@@ -189,6 +189,129 @@ def volumetric(out_dir, width=512, height=512, spp=64, max_depth=32, integrator=
     return path
 
 
+# ------------------------------------------------------------------ microfacet grid
+
+
+def icosphere(subdiv=3):
+    """Unit icosphere: icosahedron with each triangle split in four `subdiv` times
+    (20 * 4^subdiv triangles; 1280 and 642 vertices for subdiv 3)."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7),
+         (9, 8, 1)]
+    verts = [np.array(p, np.float64) / np.linalg.norm(p) for p in v]
+    faces = f
+    for _ in range(subdiv):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return np.array(verts), np.array(faces, np.int64)
+
+
+def value_noise(p, seed, freq=3.0):
+    """Seeded lattice value noise in [-1, 1]: hashed lattice values, trilinear blend with
+    smoothstep weights. p: [n, 3] world positions."""
+    q = p * freq
+    i0 = np.floor(q).astype(np.int64)
+    fr = q - i0
+    w = fr * fr * (3.0 - 2.0 * fr)
+
+    def h(ix, iy, iz):
+        x = (ix * 73856093) ^ (iy * 19349663) ^ (iz * 83492791) ^ (seed * 2654435761)
+        x = (x ^ (x >> 13)) * 1274126177
+        x = x ^ (x >> 16)
+        return ((x & 0xFFFFFF) / float(0xFFFFFF)) * 2.0 - 1.0
+    out = 0.0
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                wx = w[:, 0] if dx else 1 - w[:, 0]
+                wy = w[:, 1] if dy else 1 - w[:, 1]
+                wz = w[:, 2] if dz else 1 - w[:, 2]
+                out = out + wx * wy * wz * h(i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz)
+    return out
+
+
+def microfacet(out_dir, width=1024, height=1024, spp=64, max_depth=16, grid=64, seed=2, integrator="path_gpu"):
+    """Ground quad (matte 0.5) and a grid x grid of displaced icospheres (1280 triangles,
+    radius 0.4, spacing 1.0, radial displacement 0.05 * value noise of the world
+    position), one OBJ and one primitive each; materials uniform over plastic (IOR 1.5,
+    random Kd), rough conductor (Cu-like eta/k) and rough glass (IOR 1.5), GGX alpha
+    uniform in [0.05, 0.5] written as roughness = sqrt(alpha); 8 spherical emitters of
+    radius 0.2 and radiance 50 above the grid. Returns the XML path (files are reused
+    when the directory already holds this exact scene)."""
+    os.makedirs(out_dir, exist_ok=True)
+    path = os.path.join(out_dir, "microfacet.xml")
+    tag = "<!-- microfacet %d %d %d %d %d %d -->" % (width, height, spp, max_depth, grid, seed)
+    if os.path.exists(path):
+        with open(path) as f:
+            if f.readline().strip() == tag:
+                return path
+    rng = np.random.default_rng(seed)
+    write_plane_obj(os.path.join(out_dir, "plane.obj"))
+    verts, faces = icosphere(3)
+    mesh_dir = os.path.join(out_dir, "spheres")
+    os.makedirs(mesh_dir, exist_ok=True)
+    face_lines = "\n".join("f %d %d %d" % (a + 1, b + 1, c + 1) for a, b, c in faces)
+    ext = (grid - 1) * 1.0
+    xml = [tag, "<scene>",
+           _camera((ext / 2, ext * 0.42, -ext * 0.28), (ext / 2, 0.0, ext * 0.55), 55, width, height),
+           '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
+           '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth),
+           "<primitive>",
+           _transform([("scale", (ext + 8, 1, ext + 8)), ("translate", (ext / 2, 0, ext / 2))]),
+           '<shape type="mesh"><string name="filename" value="plane.obj"/></shape>',
+           '<material type="matte">' + _color("albedo", (0.5, 0.5, 0.5)) + "</material>",
+           "</primitive>"]
+    mats = rng.integers(0, 3, grid * grid)
+    alphas = rng.uniform(0.05, 0.5, grid * grid)
+    kds = rng.uniform(0.1, 0.9, (grid * grid, 3))
+    for k in range(grid * grid):
+        gx, gz = k % grid, k // grid
+        center = np.array([gx * 1.0, 0.45, gz * 1.0])
+        world = verts * 0.4 + center
+        disp = 0.05 * value_noise(world, seed)
+        local = verts * (0.4 + disp)[:, None]
+        name = "s%04d.obj" % k
+        with open(os.path.join(mesh_dir, name), "w") as f:
+            f.write("\n".join("v %s %s %s" % (_fmt(a), _fmt(b), _fmt(c)) for a, b, c in local))
+            f.write("\n" + face_lines + "\n")
+        rough = float(np.sqrt(alphas[k]))
+        if mats[k] == 0:
+            m = ('<material type="plastic">' + _color("Kd", kds[k]) +
+                 '<float name="eta" value="1.5"/><float name="roughness" value="%s"/></material>' % _fmt(rough))
+        elif mats[k] == 1:
+            m = ('<material type="conductor">' + _color("eta", (0.27, 0.68, 1.22)) + _color("k", (3.61, 2.63, 2.29)) +
+                 '<float name="roughness" value="%s"/></material>' % _fmt(rough))
+        else:
+            m = '<material type="glass"><float name="eta" value="1.5"/><float name="roughness" value="%s"/></material>' % _fmt(rough)
+        xml += ["<primitive>", _transform([("translate", tuple(center))]),
+                '<shape type="mesh"><string name="filename" value="spheres/%s"/></shape>' % name, m, "</primitive>"]
+    lights = np.column_stack([rng.uniform(4, ext - 4, 8), rng.uniform(2.0, 3.5, 8), rng.uniform(4, ext - 4, 8)])
+    for c in lights:
+        xml += ["<primitive>", _transform([("translate", tuple(c))]),
+                '<shape type="sphere"><float name="radius" value="0.2"/></shape>',
+                '<material type="matte">' + _color("albedo", (0, 0, 0)) + "</material>",
+                '<emitter type="area">' + _color("radiance", (50, 50, 50)) + "</emitter>", "</primitive>"]
+    xml.append("</scene>")
+    with open(path, "w") as f:
+        f.write("\n".join(xml) + "\n")
+    return path
+
+
 # ------------------------------------------------------------------ traversal micro-benchmark
 
 

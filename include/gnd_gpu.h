@@ -146,6 +146,52 @@ gnd_status gnd_gpu_trace_any_dev(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd
 gnd_status gnd_gpu_trace_count_dev(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* d_rays, int64_t n,
                                    uint32_t* d_nodes, uint32_t* d_tris, void* stream);
 
+/* ------------------------------------------------------------------ rendering */
+/* Progress callback, the reference's Integrator::setCallback / notifyUpdate
+ * (integrator.h:25-35, 148-149): called after each completed sample pass with the film
+ * accumulated so far (height x width x 7 floats, see gnd_gpu_render). */
+typedef void (*gnd_progress_fn)(void* user, int32_t sample_index, const float* film, int32_t width, int32_t height);
+
+typedef struct gnd_render_params {
+    int32_t spp;              /* passes (samples per pixel); <= 0: the scene file's value */
+    int32_t first_pass;       /* sample index of the first pass (it keys the seeds) */
+    int32_t max_depth;        /* <= 0: the scene file's value */
+    int32_t integrator;       /* -1: the scene file's; 0 path_gpu; 1 volpath_gpu */
+    int32_t window[4];        /* pixel window x0, y0, x1, y1; all zero: the full image */
+    int32_t batched;          /* 0: one pass in flight at a time (plain); 1: every pass
+                                 shares the path pool, refilled as paths finish */
+    int32_t profile;          /* bit0: time the closest-hit (extend) launches with events;
+                                 bit1: count BVH node visits / triangle tests in extend */
+    gnd_progress_fn callback; /* optional (plain mode only) */
+    void* user;
+} gnd_render_params;
+
+typedef struct gnd_render_stats {
+    int64_t paths;            /* camera samples traced */
+    int64_t rays;             /* closest-hit + shadow queries */
+    int32_t passes_done;
+    int32_t pad;
+    double ms;                /* device time of the render */
+    int64_t extend_rays;      /* closest-hit queries of the extend kernel */
+    int64_t shadow_rays;      /* shadow queries */
+    int64_t extend_nodes;     /* profile bit1: BVH4 node visits in extend */
+    int64_t extend_tris;      /* profile bit1: triangle tests in extend */
+    double extend_ms;         /* profile bit0: summed device time of the extend launches */
+    int64_t iterations;       /* wavefront iterations (bounce steps) */
+} gnd_render_stats;
+
+/* Integrator::render (integrator.h:49-155) for path_gpu / volpath_gpu: renders the
+ * passes [first_pass, first_pass + spp) and ADDS them into `film` (host memory,
+ * height x width x 7 floats per pixel: sum of w*L (r, g, b), sum of w, sum of w*L^2
+ * (r, g, b); the image is sum(w*L) / sum(w)). Per-pixel sample keys, draw order and film
+ * splatting follow the reference render loop. Cancelled renders (gnd_gpu_cancel) stop
+ * after the current pass and return GND_ERR_CANCELLED with the partial film added. */
+gnd_status gnd_gpu_render(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_render_params* params, float* film,
+                          gnd_render_stats* stats);
+/* Integrator::cancel (integrator.h:22): asks a running gnd_gpu_render on this context
+ * to stop after its current pass. Safe to call from another thread. */
+gnd_status gnd_gpu_cancel(gnd_gpu_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -146,7 +146,9 @@ int orc_trace(void* s, const float* rays, int64_t n, int anyhit, int nthreads, f
             bool h = traverseBVH4(sc.nodes4, ray, false, leafFn, &st);
             if (h) {
                 t[i] = bestSi.t; u[i] = bestSi.uv.x; v[i] = bestSi.uv.y;
-                prim[i] = (int32_t)bestSi.primIndex;
+                // triangle index for meshes; analytic shapes have none (-1)
+                bool isMesh = dynamic_cast<const Mesh*>(bestSi.primitive->shape.get()) != nullptr;
+                prim[i] = isMesh ? (int32_t)bestSi.primIndex : -1;
                 inst[i] = bestInst;
             } else {
                 t[i] = Infinity; u[i] = 0; v[i] = 0; prim[i] = -1; inst[i] = -1;

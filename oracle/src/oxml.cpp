@@ -8,6 +8,7 @@
 #include <filesystem>
 #include <fstream>
 #include <sstream>
+#include <thread>
 #include <unordered_map>
 
 namespace orc {
@@ -204,6 +205,7 @@ Vec2 parseVector2(const std::string& value) {
 struct Loader {
     std::string baseDir;
     std::unordered_map<std::string, ObjectPtr> refs;
+    std::vector<std::shared_ptr<Mesh>> deferred;
 
     // parser.cpp:41-218
     ObjectPtr parse(const XNode& node) {
@@ -283,7 +285,10 @@ struct Loader {
                 sp->addChild(c);
             }
         }
-        sp->activate();
+        // Meshes are activated after the whole file is read, in parallel (loading order
+        // does not change any result); every other object activates as it is parsed.
+        if (auto mesh = std::dynamic_pointer_cast<Mesh>(sp)) deferred.push_back(mesh);
+        else if (node.tag != "scene") sp->activate();
         return sp;
     }
 };
@@ -303,7 +308,24 @@ std::shared_ptr<Object> loadSceneXML(const std::string& path) {
     std::error_code ec;
     auto canon = std::filesystem::canonical(path, ec);
     ld.baseDir = (ec ? std::filesystem::path(path) : canon).parent_path().string();
-    return ld.parse(root);
+    ObjectPtr top = ld.parse(root);
+    std::atomic<size_t> next{0};
+    std::vector<std::string> errors(ld.deferred.size());
+    auto work = [&]() {
+        for (;;) {
+            size_t i = next.fetch_add(1);
+            if (i >= ld.deferred.size()) break;
+            try { ld.deferred[i]->activate(); } catch (const std::exception& e) { errors[i] = e.what(); }
+        }
+    };
+    unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+    for (auto& e : errors) if (!e.empty()) throw std::runtime_error(e);
+    if (root.tag == "scene") top->activate();
+    return top;
 }
 
 // ---------------------------------------------------------------- OBJ
