@@ -166,6 +166,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--plain", action="store_true", help="one pass in flight (no refill) for the timed steps")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -202,8 +204,9 @@ def main():
     tris_per_ray = cst["extend_tris"] / max(1, cst["extend_rays"])
     log("extend work: %.2f nodes, %.2f triangles per ray" % (nodes_per_ray, tris_per_ray))
 
+    batched = not args.plain
     for w in range(args.warmup):
-        ctx.render(sid, spp=spp, first_pass=first)
+        ctx.render(sid, spp=spp, first_pass=first, batched=batched)
 
     def barrier():
         torch.cuda.synchronize()
@@ -217,7 +220,7 @@ def main():
     stats = []
     film_acc = None
     for k in range(args.steps):
-        film, st = ctx.render(sid, spp=spp, first_pass=first, profile=1)
+        film, st = ctx.render(sid, spp=spp, first_pass=first, profile=1, batched=batched)
         if dist:
             ft = torch.from_numpy(film).cuda()
             dist.reduce(ft, dst=0)
@@ -241,23 +244,29 @@ def main():
     # e2e through the C ABI with host buffers: scene upload + render + film readback
     e2e_times = []
     film_bytes = npix * (4 * 8 + 3 * 4)
-    for k in range(max(1, args.steps)):
+    for k in range(0 if args.no_e2e else max(1, args.steps)):
         barrier()
         t = time.perf_counter()
         sid2 = ctx.upload(hs)
-        film, st = ctx.render(sid2, spp=spp, first_pass=first)
+        film, st = ctx.render(sid2, spp=spp, first_pass=first, batched=batched)
         if dist:
             ft = torch.from_numpy(film).cuda()
             dist.reduce(ft, dst=0)
         ctx.free_scene(sid2)
         barrier()
         e2e_times.append(time.perf_counter() - t)
-    e2e_el = sum(e2e_times)
+    e2e_el = sum(e2e_times) if e2e_times else float("nan")
     if dist:
         tt = torch.tensor([e2e_el], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_el = float(tt.item())
-    e2e_value = npix * spp * world * len(e2e_times) / e2e_el / 1e6
+    e2e_value = npix * spp * world * len(e2e_times) / e2e_el / 1e6 if e2e_times else None
+    # the other mode on the same scene, for the batched-vs-plain comparison
+    other = []
+    for k in range(min(2, args.steps)):
+        _, st = ctx.render(sid, spp=spp, first_pass=first, batched=not batched)
+        other.append(st["ms"])
+    other_value = npix * spp / (sum(other) / len(other) / 1000.0) / 1e6 if other else None
 
     peaks, peak_kind = measured_peaks()
     bytes_per_ray = nodes_per_ray * 128 + tris_per_ray * 48 + 32 + 32
@@ -275,9 +284,11 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator, gianduia_b200/scenes.py)",
         "config": {"workload": "microfacet 1024x1024, 64 spp, path_gpu depth 16, 5,242,882 tris, 4105 instances, 8 sphere lights",
-                   "parallelism": "spp-sharded" if world > 1 else "single GPU", "mode": "plain (one pass in flight)",
+                   "parallelism": "spp-sharded" if world > 1 else "single GPU",
+                   "mode": "batched (all passes share a refilled pool of path slots)" if batched else "plain (one pass in flight)",
                    "l2": "inputs larger than L2 (scene %.2f GB resident)" % (scene_bytes / 1e9)},
         "mrays_per_s": rays * world / elapsed / 1e6,
+        ("plain_value" if batched else "batched_value"): other_value,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                      "frac": (achieved / peaks["hbm_gbs"]) if achieved else None, "traffic": traffic,
                      "kernel": "kExtend (closest-hit BVH4 traversal)",

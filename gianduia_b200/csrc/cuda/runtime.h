@@ -107,6 +107,17 @@ struct Context {
     uint64_t nextScene = 1;
     DevBuf errWord;           // device error bitmask written by kernels
     DevBuf rayScratch, hitScratch;
+    // Work counters of persistent launches: each launch takes the next entry of a ring of
+    // kFetchRing counters (reset on the launch's stream), so launches on different
+    // streams do not share one.
+    static constexpr int kFetchRing = 1024;
+    DevBuf fetchRing;
+    uint32_t fetchNext = 0;
+    uint32_t* nextFetchCounter() {
+        if (!fetchRing.ptr) fetchRing.alloc(kFetchRing * sizeof(uint32_t));
+        uint32_t k = fetchNext++ % kFetchRing;
+        return fetchRing.as<uint32_t>() + k;
+    }
     std::unique_ptr<Wavefront> wave;
     volatile bool cancel = false;
     ~Context();

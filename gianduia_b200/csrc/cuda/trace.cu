@@ -6,29 +6,36 @@
 namespace gnd {
 
 constexpr int kTraceBlock = 128;
+constexpr int kTraceBlocksPerSM = 8;
 
+// Ray batch source / sink for the persistent traversal loop.
 template <bool ANY, bool COUNT>
-__global__ void __launch_bounds__(kTraceBlock) traceKernel(SceneView s, const gnd_ray* __restrict__ rays, int64_t n,
-                                                           gnd_hit* __restrict__ hits, uint8_t* __restrict__ occ,
-                                                           uint32_t* __restrict__ nodesOut, uint32_t* __restrict__ trisOut,
-                                                           uint32_t* errWord) {
-    __shared__ uint32_t stack[kStackSize * kTraceBlock];
-    uint32_t* stk = stack + threadIdx.x;
-    int err = 0;
-    for (int64_t i = (int64_t)blockIdx.x * kTraceBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kTraceBlock) {
+struct BatchSrc {
+    const SceneView* sv;
+    const gnd_ray* rays;
+    uint32_t n;
+    gnd_hit* hits;
+    uint8_t* occ;
+    uint32_t* nodesOut;
+    uint32_t* trisOut;
+    TraceCounters* cnt;
+    __device__ uint32_t count() const { return n; }
+    __device__ bool load(uint32_t i, TRay& r, const SceneView*& s, const uint8_t*& nm) {
         float4 a = __ldg(reinterpret_cast<const float4*>(rays + i));
         float4 b = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
-        TRay r;
         r.o = v3(a.x, a.y, a.z);
         r.tmin = a.w;
         r.d = v3(b.x, b.y, b.z);
         r.tmax = b.w;
-        THit h;
-        TraceCounters cnt{0, 0};
-        err |= traceRay<kTraceBlock, ANY, false, COUNT>(s, r, h, stk, &cnt, nullptr);
+        s = sv;
+        nm = nullptr;
+        if (COUNT) { cnt->nodes = 0; cnt->tris = 0; }
+        return true;
+    }
+    __device__ void store(uint32_t i, const THit& h) {
         if (COUNT) {
-            nodesOut[i] = cnt.nodes;
-            trisOut[i] = cnt.tris;
+            nodesOut[i] = cnt->nodes;
+            trisOut[i] = cnt->tris;
         } else if (ANY) {
             occ[i] = h.inst >= 0 ? 1 : 0;
         } else {
@@ -37,28 +44,39 @@ __global__ void __launch_bounds__(kTraceBlock) traceKernel(SceneView s, const gn
             o.u = h.u;
             o.v = h.v;
             o.inst = h.inst;
-            o.prim = (h.inst >= 0 && h.slot != 0xFFFFFFFFu) ? (int32_t)__ldg(&s.tris[h.slot].prim) : -1;
+            o.prim = (h.inst >= 0 && h.slot != 0xFFFFFFFFu) ? (int32_t)__ldg(&sv->tris[h.slot].prim) : -1;
             hits[i] = o;
         }
     }
+};
+
+template <bool ANY, bool COUNT>
+__global__ void __launch_bounds__(kTraceBlock, kTraceBlocksPerSM)
+    traceKernel(const SceneView* __restrict__ sv, const gnd_ray* __restrict__ rays, uint32_t n, gnd_hit* __restrict__ hits,
+                uint8_t* __restrict__ occ, uint32_t* __restrict__ nodesOut, uint32_t* __restrict__ trisOut,
+                uint32_t* fetch, uint32_t* errWord) {
+    __shared__ uint32_t stack[kSmemStack * kTraceBlock];
+    TraceCounters cnt{0, 0};
+    BatchSrc<ANY, COUNT> src{sv, rays, n, hits, occ, nodesOut, trisOut, &cnt};
+    int err = persistentTrace<kTraceBlock, ANY, COUNT>(src, fetch, stack, &cnt);
     if (err) atomicOr(errWord, (uint32_t)err);
 }
 
 namespace {
-int traceGrid(Context* c, int64_t n) {
-    int64_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
-    int64_t cap = (int64_t)c->numSMs * 16;
-    return (int)std::max<int64_t>(1, std::min(blocks, cap));
-}
-
 void launchTrace(Context* c, DeviceScene& ds, const gnd_ray* dr, int64_t n, gnd_hit* dh, uint8_t* docc,
                  uint32_t* dn, uint32_t* dt, cudaStream_t st) {
     if (n <= 0) return;
-    int g = traceGrid(c, n);
+    if (n >= (int64_t)0xF0000000LL) throw Error(GND_ERR_INVALID, "ray batch too large (limit 4e9 rays per call)");
+    int64_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
+    int g = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)c->numSMs * kTraceBlocksPerSM));
     uint32_t* ew = c->errWord.as<uint32_t>();
-    if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(ds.view, dr, n, nullptr, nullptr, dn, dt, ew);
-    else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(ds.view, dr, n, nullptr, docc, nullptr, nullptr, ew);
-    else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(ds.view, dr, n, dh, nullptr, nullptr, nullptr, ew);
+    uint32_t* fetch = c->nextFetchCounter();
+    GND_CUDA(cudaMemsetAsync(fetch, 0, sizeof(uint32_t), st));
+    const SceneView* sv = ds.viewDev.as<SceneView>();
+    uint32_t nn = (uint32_t)n;
+    if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, nullptr, dn, dt, fetch, ew);
+    else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew);
+    else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew);
     GND_CUDA(cudaGetLastError());
 }
 

@@ -257,4 +257,253 @@ __device__ __forceinline__ int traceRay(const SceneView& s, const TRay& ray, THi
     return err;
 }
 
+// ---------------------------------------------------------------- persistent traversal
+// The same traversal as traceRay, restated as an incremental per-lane state machine for
+// persistent warps: lanes that finish a ray fetch the next one (warp-aggregated atomic on
+// a per-launch counter), and each round runs a node phase (every lane pops and tests
+// inner nodes until it holds a leaf) followed by a leaf phase (one primitive per step),
+// so the warp executes one code path at a time. The stack keeps its top kSmemStack
+// entries in shared memory and spills deeper entries to a per-lane local array.
+constexpr int kSmemStack = 32;
+constexpr int kLocalStack = 96;
+constexpr int kPStackMax = kSmemStack + kLocalStack;
+
+struct Trav {
+    V3 wo, wd;          // world ray
+    V3 o, d, inv;       // current ray (world, or object space inside a bottom-level tree)
+    float wtmin, tmin, tmax, bestT;
+    int curInst;
+    int sp;
+    uint32_t leaf;      // pending leaf reference, kEmpty when none
+    uint32_t leafK;     // next primitive of the pending leaf
+    THit hit;
+};
+
+template <int BLOCK>
+struct TStack {
+    uint32_t* smem;                 // this lane's column in the block's shared array
+    uint32_t local[kLocalStack];
+    __device__ __forceinline__ void put(int k, uint32_t v) {
+        if (k < kSmemStack) smem[k * BLOCK] = v;
+        else local[k - kSmemStack] = v;
+    }
+    __device__ __forceinline__ uint32_t get(int k) const { return k < kSmemStack ? smem[k * BLOCK] : local[k - kSmemStack]; }
+};
+
+__device__ __forceinline__ void travInit(Trav& t, const SceneView& s, const TRay& ray) {
+    t.wo = ray.o; t.wd = ray.d;
+    t.o = ray.o; t.d = ray.d;
+    t.inv = v3(__frcp_rn(ray.d.x), __frcp_rn(ray.d.y), __frcp_rn(ray.d.z));
+    t.wtmin = ray.tmin; t.tmin = ray.tmin; t.tmax = ray.tmax;
+    t.bestT = 3.402823466e38f;
+    t.curInst = -1;
+    t.leaf = kEmpty;
+    t.leafK = 0;
+    t.hit.t = INFINITY; t.hit.u = t.hit.v = 0.f; t.hit.inst = -1; t.hit.slot = 0xFFFFFFFFu;
+    t.sp = 0;
+}
+
+// Pops one entry: restores the world ray at a sentinel, tests an inner node and pushes its
+// hit children nearest-last, or makes a leaf pending. Returns an error bitmask.
+template <int BLOCK, bool COUNT>
+__device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<BLOCK>& st, TraceCounters* cnt) {
+    uint32_t e = st.get(--t.sp);
+    if (e == kSentinel) {
+        t.o = t.wo; t.d = t.wd;
+        t.inv = v3(__frcp_rn(t.wd.x), __frcp_rn(t.wd.y), __frcp_rn(t.wd.z));
+        t.tmin = t.wtmin;
+        t.curInst = -1;
+        return 0;
+    }
+    if (isLeaf(e)) {
+        t.leaf = e;
+        t.leafK = 0;
+        return 0;
+    }
+    const Node4* nd = s.nodes + e;
+    if (COUNT) cnt->nodes++;
+    float key[4];
+    uint4 ch = ldgu4(nd->child);
+    uint32_t ref[4] = {ch.x, ch.y, ch.z, ch.w};
+    {
+        float4 lx = ldg4(nd->lox), hx = ldg4(nd->hix);
+        float t1[4] = {(lx.x - t.o.x) * t.inv.x, (lx.y - t.o.x) * t.inv.x, (lx.z - t.o.x) * t.inv.x, (lx.w - t.o.x) * t.inv.x};
+        float t2[4] = {(hx.x - t.o.x) * t.inv.x, (hx.y - t.o.x) * t.inv.x, (hx.z - t.o.x) * t.inv.x, (hx.w - t.o.x) * t.inv.x};
+        float tn[4], tf[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { tn[i] = lmin(t1[i], t2[i]); tf[i] = lmax(t1[i], t2[i]); }
+        float4 ly = ldg4(nd->loy), hy = ldg4(nd->hiy);
+        float u1[4] = {(ly.x - t.o.y) * t.inv.y, (ly.y - t.o.y) * t.inv.y, (ly.z - t.o.y) * t.inv.y, (ly.w - t.o.y) * t.inv.y};
+        float u2[4] = {(hy.x - t.o.y) * t.inv.y, (hy.y - t.o.y) * t.inv.y, (hy.z - t.o.y) * t.inv.y, (hy.w - t.o.y) * t.inv.y};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { tn[i] = lmax(tn[i], lmin(u1[i], u2[i])); tf[i] = lmin(tf[i], lmax(u1[i], u2[i])); }
+        float4 lz = ldg4(nd->loz), hz = ldg4(nd->hiz);
+        float w1[4] = {(lz.x - t.o.z) * t.inv.z, (lz.y - t.o.z) * t.inv.z, (lz.z - t.o.z) * t.inv.z, (lz.w - t.o.z) * t.inv.z};
+        float w2[4] = {(hz.x - t.o.z) * t.inv.z, (hz.y - t.o.z) * t.inv.z, (hz.z - t.o.z) * t.inv.z, (hz.w - t.o.z) * t.inv.z};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            // bvhTraversal.h:69-72: max(max(x, y), max(z, tMin)) <= min(min(x, y), min(z, tMax))
+            float a = lmax(tn[i], lmax(lmin(w1[i], w2[i]), t.tmin));
+            float b = lmin(tf[i], lmin(lmax(w1[i], w2[i]), t.tmax));
+            key[i] = (a <= b && ref[i] != kEmpty) ? a : INFINITY;
+        }
+    }
+#define GND_CSWAP(a, b)                                                          \
+    if (key[b] < key[a]) {                                                       \
+        float tk = key[a]; key[a] = key[b]; key[b] = tk;                         \
+        uint32_t tr = ref[a]; ref[a] = ref[b]; ref[b] = tr;                      \
+    }
+    GND_CSWAP(0, 1) GND_CSWAP(2, 3) GND_CSWAP(0, 2) GND_CSWAP(1, 3) GND_CSWAP(1, 2)
+#undef GND_CSWAP
+#pragma unroll
+    for (int i = 3; i >= 0; --i) {
+        if (key[i] != INFINITY) {
+            if (t.sp >= kPStackMax) return kTraceStackOverflow;
+            st.put(t.sp++, ref[i]);
+        }
+    }
+    return 0;
+}
+
+// Processes one primitive of the pending leaf. For ANY, a hit ends the ray (sp = 0).
+template <int BLOCK, bool ANY, bool COUNT>
+__device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<BLOCK>& st, TraceCounters* cnt,
+                                            const uint8_t* nullMask) {
+    uint32_t first = leafFirst(t.leaf), count = leafCount(t.leaf);
+    uint32_t k = t.leafK++;
+    if (t.leafK >= count) t.leaf = kEmpty;
+    if (t.curInst >= 0) {
+        float tt, u, v;
+        uint32_t prim;
+        if (COUNT) cnt->tris++;
+        if (triTest(s.tris + first + k, t.o, t.d, t.tmin, t.tmax, tt, u, v, prim)) {
+            t.tmax = tt;
+            t.bestT = tt;
+            t.hit.t = tt; t.hit.u = u; t.hit.v = v;
+            t.hit.inst = t.curInst;
+            t.hit.slot = first + k;
+            if (ANY) { t.sp = 0; t.leaf = kEmpty; }
+        }
+        return 0;
+    }
+    uint32_t id = __ldg(s.tlasList + first + k);
+    if (nullMask && nullMask[id]) return 0;
+    const InstTrav* it = s.instT + id;
+    float4 r0 = ldg4(&it->w2o.r[0][0]), r1 = ldg4(&it->w2o.r[1][0]), r2 = ldg4(&it->w2o.r[2][0]);
+    float4 meta = ldg4(&it->kind);
+    uint32_t kind = __float_as_uint(meta.x);
+    V3 lo, ld;
+    lo.x = (r0.x * t.wo.x + r0.y * t.wo.y) + (r0.z * t.wo.z + r0.w);
+    lo.y = (r1.x * t.wo.x + r1.y * t.wo.y) + (r1.z * t.wo.z + r1.w);
+    lo.z = (r2.x * t.wo.x + r2.y * t.wo.y) + (r2.z * t.wo.z + r2.w);
+    ld.x = (r0.x * t.wd.x + r0.y * t.wd.y) + (r0.z * t.wd.z + r0.w * 0.0f);
+    ld.y = (r1.x * t.wd.x + r1.y * t.wd.y) + (r1.z * t.wd.z + r1.w * 0.0f);
+    ld.z = (r2.x * t.wd.x + r2.y * t.wd.y) + (r2.z * t.wd.z + r2.w * 0.0f);
+    if (kind == kShapeMesh) {
+        uint32_t root = __float_as_uint(meta.y);
+        if (root == kEmpty) return 0;
+        if (t.leaf != kEmpty) {
+            // the rest of this leaf comes back after the bottom-level tree
+            if (t.sp >= kPStackMax) return kTraceStackOverflow;
+            st.put(t.sp++, makeLeaf(first + k + 1, count - k - 1));
+            t.leaf = kEmpty;
+        }
+        if (t.sp + 2 > kPStackMax) return kTraceStackOverflow;
+        st.put(t.sp++, kSentinel);
+        st.put(t.sp++, root);
+        t.o = lo; t.d = ld;
+        t.inv = v3(__frcp_rn(ld.x), __frcp_rn(ld.y), __frcp_rn(ld.z));
+        t.tmin = kEpsilon;
+        t.curInst = (int)id;
+        return 0;
+    }
+    float th;
+    bool h;
+    if (kind == kShapeSphere) h = sphereTest(meta.z, lo, ld, kEpsilon, t.tmax, th);
+    else h = cubeTest(v3(meta.z, meta.w, __ldg(&s.instS[id].ext[2])), lo, ld, kEpsilon, t.tmax, th);
+    if (h && th < t.bestT) {
+        t.tmax = th;
+        t.bestT = th;
+        t.hit.t = th; t.hit.u = 0.f; t.hit.v = 0.f;
+        t.hit.inst = (int)id;
+        t.hit.slot = 0xFFFFFFFFu;
+        if (ANY) { t.sp = 0; t.leaf = kEmpty; }
+    }
+    return 0;
+}
+
+// Warp-aggregated fetch of the next work index for lanes in `want`.
+__device__ __forceinline__ uint32_t warpFetch(uint32_t* counter, bool want) {
+    uint32_t mask = __ballot_sync(0xffffffffu, want);
+    uint32_t base = 0;
+    int lane = threadIdx.x & 31;
+    if (mask) {
+        int leader = __ffs(mask) - 1;
+        if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, leader);
+    }
+    return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+
+// Persistent traversal loop. Every lane of every warp runs it to the end (the block size
+// is a multiple of 32 and no lane exits early). Src provides:
+//   uint32_t count()                      number of rays
+//   bool load(uint32_t i, TRay&, const SceneView*&, const uint8_t*& nullMask)
+//   void store(uint32_t i, const THit&)   (closest) / store(i, bool) (any)
+template <int BLOCK, bool ANY, bool COUNT, typename Src>
+__device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter, uint32_t* smemStack, TraceCounters* cnt) {
+    TStack<BLOCK> st;
+    st.smem = smemStack + threadIdx.x;
+    Trav t;
+    const SceneView* sv = nullptr;
+    const uint8_t* nm = nullptr;
+    bool active = false;
+    bool drained = false;   // warp-uniform: the counter has passed n
+    uint32_t idx = 0;
+    int err = 0;
+    const uint32_t n = src.count();
+    uint32_t iter = 0;
+    for (;;) {
+        bool idle = !active && !drained;
+        uint32_t got = warpFetch(fetchCounter, idle);
+        if (__any_sync(0xffffffffu, idle && got >= n)) drained = true;
+        if (idle && got < n) {
+            idx = got;
+            TRay r;
+            if (src.load(idx, r, sv, nm)) {
+                travInit(t, *sv, r);
+                if (sv->tlasRoot != kEmpty) { st.put(0, sv->tlasRoot); t.sp = 1; }
+                active = true;
+                iter = 0;
+            } else {
+                src.store(idx, t.hit);   // never reached for valid inputs
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        // node phase
+        for (;;) {
+            bool want = active && t.leaf == kEmpty && t.sp > 0;
+            if (!__any_sync(0xffffffffu, want)) break;
+            if (want) {
+                int e = travNodeStep<BLOCK, COUNT>(t, *sv, st, cnt);
+                if (e || ++iter > kMaxIterations) { err |= e ? e : (int)kTraceIterLimit; t.sp = 0; t.leaf = kEmpty; }
+            }
+        }
+        // leaf phase
+        for (;;) {
+            bool want = active && t.leaf != kEmpty;
+            if (!__any_sync(0xffffffffu, want)) break;
+            if (want) {
+                int e = travLeafStep<BLOCK, ANY, COUNT>(t, *sv, st, cnt, nm);
+                if (e) { err |= e; t.sp = 0; t.leaf = kEmpty; }
+            }
+        }
+        if (active && t.sp == 0 && t.leaf == kEmpty) {
+            src.store(idx, t.hit);
+            active = false;
+        }
+    }
+    return err;
+}
+
 }  // namespace gnd

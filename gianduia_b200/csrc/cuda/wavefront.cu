@@ -355,6 +355,8 @@ __global__ void kBeginIter(uint32_t* cnt) {
     cnt[kQOut] = 0;
     cnt[kQShadow] = 0;
     cnt[kQDone] = 0;
+    cnt[kQFetchA] = 0;
+    cnt[kQFetchB] = 0;
 }
 
 // Plain mode: pass `pass` of job 0 for every window pixel, slot = pixel index.
@@ -385,32 +387,42 @@ __global__ void __launch_bounds__(kBlock) kRaygenFill(KParams p, uint32_t n) {
     }
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(kBlock) kExtend(KParams p) {
-    __shared__ uint32_t stack[kStackSize * kBlock];
-    uint32_t* stk = stack + threadIdx.x;
-    const uint32_t n = p.cnt[kQIn];
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[0], (unsigned long long)n);
-    int err = 0;
-    TraceCounters cnt{0, 0};
-    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
-        uint32_t slot = p.listIn[i];
-        const PathState* ps = p.paths + slot;
+// Closest-hit source/sink over the active list (extend).
+struct ExtendSrc {
+    const KParams* p;
+    uint32_t n;
+    uint32_t slot;
+    __device__ uint32_t count() const { return n; }
+    __device__ bool load(uint32_t i, TRay& r, const SceneView*& sv, const uint8_t*& nm) {
+        slot = p->listIn[i];
+        const PathState* ps = p->paths + slot;
         float4 a = *reinterpret_cast<const float4*>(&ps->ox);
         float4 b = *reinterpret_cast<const float4*>(&ps->dx);
         uint32_t job = ps->flags >> 8;
-        TRay r;
         r.o = v3(a.x, a.y, a.z);
         r.d = v3(b.x, b.y, b.z);
         r.tmin = kEpsilon;
         r.tmax = INFINITY;
-        THit h;
-        err |= traceRay<kBlock, false, false, COUNT>(p.jobs[job].view, r, h, stk, &cnt, nullptr);
+        sv = &p->jobs[job].view;
+        nm = nullptr;
+        return true;
+    }
+    __device__ void store(uint32_t, const THit& h) {
         HitRec hr;
         hr.t = h.t; hr.u = h.u; hr.v = h.v; hr.inst = h.inst; hr.slot = h.slot;
         hr.pad[0] = hr.pad[1] = hr.pad[2] = 0;
-        p.hits[slot] = hr;
+        p->hits[slot] = hr;
     }
+};
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kBlock, 8) kExtend(KParams p) {
+    __shared__ uint32_t stack[kSmemStack * kBlock];
+    const uint32_t n = p.cnt[kQIn];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[0], (unsigned long long)n);
+    TraceCounters cnt{0, 0};
+    ExtendSrc src{&p, n, 0};
+    int err = persistentTrace<kBlock, false, COUNT>(src, p.cnt + kQFetchA, stack, &cnt);
     if (COUNT) {
         unsigned long long nn = cnt.nodes, nt = cnt.tris;
         for (int o = 16; o > 0; o >>= 1) {
@@ -623,10 +635,58 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p) {
     }
 }
 
-// Shadow queries. Path: the reference traces closest hits and treats the segment as
-// occluded when the first surface has a BSDF (path.cpp:124-140; a null-BSDF first hit
-// leaves the segment unoccluded because the next segment's tMax is ~0); with no null
-// materials this is a plain any-hit query. Volpath: evaluateTr (volPath.cpp:261-291).
+// Shadow queries of `path`. The reference traces closest hits and treats the segment as
+// occluded when the first surface has a BSDF (path.cpp:124-140; after a null-BSDF first
+// hit the next segment's tMax is ~0, so the segment counts as clear). ANY = true is the
+// plain any-hit query, exact when no job in the launch has null-BSDF materials; ANY =
+// false is the closest hit plus the material check.
+template <bool ANY>
+struct ShadowSrc {
+    const KParams* p;
+    uint32_t n;
+    uint32_t slot;
+    const uint8_t* nm;
+    __device__ uint32_t count() const { return n; }
+    __device__ bool load(uint32_t i, TRay& r, const SceneView*& sv, const uint8_t*& nmOut) {
+        const ShadowRec* sr = p->shadow + i;
+        float4 a = *reinterpret_cast<const float4*>(&sr->ox);
+        float4 b = *reinterpret_cast<const float4*>(&sr->dx);
+        slot = __float_as_uint(b.w);
+        r.o = v3(a.x, a.y, a.z);
+        r.tmax = a.w;
+        r.d = v3(b.x, b.y, b.z);
+        r.tmin = kEpsilon;
+        const JobDev& j = p->jobs[p->paths[slot].flags >> 8];
+        sv = &j.view;
+        nm = j.nullMask;
+        nmOut = nullptr;
+        return true;
+    }
+    __device__ void store(uint32_t i, const THit& h) {
+        bool clear = h.inst < 0 || (!ANY && nm[h.inst]);
+        if (clear) {
+            const ShadowRec* sr = p->shadow + i;
+            float4 c = *reinterpret_cast<const float4*>(&sr->cr);
+            PathState* ps = p->paths + slot;
+            ps->Lr = ps->Lr + c.x;
+            ps->Lg = ps->Lg + c.y;
+            ps->Lb = ps->Lb + c.z;
+        }
+    }
+};
+
+template <bool ANY>
+__global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p) {
+    __shared__ uint32_t stack[kSmemStack * kBlock];
+    const uint32_t n = p.cnt[kQShadow];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
+    ShadowSrc<ANY> src{&p, n, 0, nullptr};
+    int err = persistentTrace<kBlock, ANY, false>(src, p.cnt + kQFetchB, stack, nullptr);
+    if (err) atomicOr(p.errWord, (uint32_t)err);
+}
+
+// Shadow queries of `volpath`: evaluateTr (volPath.cpp:261-291), a loop of closest hits
+// through null-BSDF boundaries multiplying the transmittance of each medium segment.
 template <bool VOL>
 __global__ void __launch_bounds__(kBlock) kShadow(KParams p) {
     __shared__ uint32_t stack[kStackSize * kBlock];
@@ -873,7 +933,8 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int spp, int firstPass, int
             if (integrator == 1) kShade<true><<<grid, kBlock, 0, st>>>(kp);
             else kShade<false><<<grid, kBlock, 0, st>>>(kp);
             if (integrator == 1) kShadow<true><<<grid, kBlock, 0, st>>>(kp);
-            else kShadow<false><<<grid, kBlock, 0, st>>>(kp);
+            else if (ds.hasNullMaterials) kShadowPath<false><<<grid, kBlock, 0, st>>>(kp);
+            else kShadowPath<true><<<grid, kBlock, 0, st>>>(kp);
             kRetire<<<grid, kBlock, 0, st>>>(kp);
             GND_CUDA(cudaGetLastError());
             // next iteration reads the list just written; move its count into kQIn

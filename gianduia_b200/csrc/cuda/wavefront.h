@@ -58,7 +58,7 @@ struct JobDev {
 };
 
 // Queue counters (device): ints.
-enum QCounter : int { kQIn = 0, kQOut = 1, kQShadow = 2, kQDone = 3, kQCount = 8 };
+enum QCounter : int { kQIn = 0, kQOut = 1, kQShadow = 2, kQDone = 3, kQFetchA = 4, kQFetchB = 5, kQCount = 8 };
 
 class Wavefront {
 public:

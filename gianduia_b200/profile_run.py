@@ -1,0 +1,61 @@
+"""Small fixed workloads for profiler captures (ncu), sized to end in seconds:
+
+  python -m gianduia_b200.profile_run trace     closest-hit batch of the traversal
+                                                micro-benchmark: 2^20 triangles, 2^22 rays
+  python -m gianduia_b200.profile_run render    one 1-spp pass of the 1024x1024
+                                                microfacet render (path_gpu, depth 16)
+  python -m gianduia_b200.profile_run volpath   one 1-spp pass of the 512x512 volumetric
+                                                Cornell box (volpath_gpu, depth 32)
+  python -m gianduia_b200.profile_run all       trace, then render
+"""
+import os
+import sys
+import tempfile
+
+import gianduia_b200 as G
+from gianduia_b200 import scenes
+
+
+def run_trace(ctx):
+    tri = scenes.random_triangles(1 << 20, seed=1)
+    rays = scenes.random_rays(1 << 22, seed=1)
+    sid = ctx.upload(G.HostScene.from_triangles(tri))
+    h = ctx.trace_closest(sid, rays)
+    print("trace: %d of %d rays hit" % (int((h["inst"] >= 0).sum()), rays.shape[0]))
+    ctx.free_scene(sid)
+
+
+def run_render(ctx, batched=False):
+    xml = scenes.microfacet(os.path.join(tempfile.gettempdir(), "gnd_bench_microfacet_r0"), width=1024, height=1024,
+                            spp=64, max_depth=16, grid=64, seed=2)
+    sid = ctx.upload(G.HostScene.load_xml(xml))
+    _, st = ctx.render(sid, spp=1, batched=batched)
+    print("render:", st)
+    ctx.free_scene(sid)
+
+
+def run_volpath(ctx):
+    xml = scenes.volumetric(os.path.join(tempfile.gettempdir(), "gnd_prof_volumetric"), width=512, height=512, spp=64,
+                            max_depth=32)
+    sid = ctx.upload(G.HostScene.load_xml(xml))
+    _, st = ctx.render(sid, spp=1)
+    print("volpath:", st)
+    ctx.free_scene(sid)
+
+
+def main(argv):
+    what = argv[1] if len(argv) > 1 else "all"
+    ctx = G.GpuContext(0)
+    if what in ("trace", "all"):
+        run_trace(ctx)
+    if what in ("render", "all"):
+        run_render(ctx)
+    if what == "batched":
+        run_render(ctx, batched=True)
+    if what == "volpath":
+        run_volpath(ctx)
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main(sys.argv)
