@@ -290,50 +290,58 @@ __device__ __forceinline__ float roughPlasticPdf(const Lobe& l, V3 wo, V3 wi) {
     return ps * pdfSpec + (1.0f - ps) * pdfDiff;
 }
 
+// Lobe kinds a kernel may meet, as a bitmask over Lobe::kind. Kernels specialised to one
+// material class pass its mask so the other lobes' code is not compiled in.
+constexpr uint32_t kLobesAll = 0x7Fu;
+constexpr uint32_t kLobesMatte = 1u << 0;
+constexpr uint32_t kLobesConductor = (1u << 1) | (1u << 3);
+constexpr uint32_t kLobesGlass = (1u << 2) | (1u << 4);
+constexpr uint32_t kLobesPlastic = (1u << 5) | (1u << 6);
+
 // BxDF::f in the local frame
+template <uint32_t M = kLobesAll>
 __device__ __forceinline__ V3 lobeF(const Lobe& l, V3 wo, V3 wi) {
-    switch (l.kind) {
-        case 0: return l.a * kInvPi;                          // reflection.cpp:8-10
-        case 3: return mfReflF(l, wo, wi);
-        case 4: return mfFresF(l, wo, wi);
-        case 5: return smoothPlasticF(l, wo, wi);
-        case 6: return roughPlasticF(l, wo, wi);
-        default: return v3s(0.f);                             // delta lobes
-    }
+    if ((M & (1u << 0)) && l.kind == 0) return l.a * kInvPi;              // reflection.cpp:8-10
+    if ((M & (1u << 3)) && l.kind == 3) return mfReflF(l, wo, wi);
+    if ((M & (1u << 4)) && l.kind == 4) return mfFresF(l, wo, wi);
+    if ((M & (1u << 5)) && l.kind == 5) return smoothPlasticF(l, wo, wi);
+    if ((M & (1u << 6)) && l.kind == 6) return roughPlasticF(l, wo, wi);
+    return v3s(0.f);                                                      // delta lobes
 }
 // BxDF::pdf in the local frame
+template <uint32_t M = kLobesAll>
 __device__ __forceinline__ float lobePdf(const Lobe& l, V3 wo, V3 wi) {
-    switch (l.kind) {
-        case 0: return cosineHemispherePdf(wi);
-        case 3: return mfReflPdf(l, wo, wi);
-        case 4: return mfFresPdf(l, wo, wi);
-        case 5: {                                             // reflection.cpp:286-290
-            if (wo.z < kEpsilon || wi.z < kEpsilon) return 0.0f;
-            float Fo = frDielectric(wo.z, 1.0f, l.eta);
-            return (1.0f - Fo) * cosineHemispherePdf(wi);
-        }
-        case 6: return roughPlasticPdf(l, wo, wi);
-        default: return 0.0f;
+    if ((M & (1u << 0)) && l.kind == 0) return cosineHemispherePdf(wi);
+    if ((M & (1u << 3)) && l.kind == 3) return mfReflPdf(l, wo, wi);
+    if ((M & (1u << 4)) && l.kind == 4) return mfFresPdf(l, wo, wi);
+    if ((M & (1u << 5)) && l.kind == 5) {                                 // reflection.cpp:286-290
+        if (wo.z < kEpsilon || wi.z < kEpsilon) return 0.0f;
+        float Fo = frDielectric(wo.z, 1.0f, l.eta);
+        return (1.0f - Fo) * cosineHemispherePdf(wi);
     }
+    if ((M & (1u << 6)) && l.kind == 6) return roughPlasticPdf(l, wo, wi);
+    return 0.0f;
 }
 // BxDF::sample in the local frame. Returns f; pdf left untouched on the paths where the
 // reference leaves it unwritten (caller initialises it to 0).
+template <uint32_t M = kLobesAll>
 __device__ __forceinline__ V3 lobeSample(const Lobe& l, V3 wo, V3& wi, V2 u, float uc, float& pdf, uint32_t& type) {
-    switch (l.kind) {
-        case 0: {   // reflection.cpp:12-27
+    const uint32_t kind = l.kind;
+    {
+        if ((M & (1u << 0)) && kind == 0) {   // reflection.cpp:12-27
             if (wo.z <= 0.0f) { pdf = 0.0f; return v3s(0.f); }
             wi = squareToCosineHemisphere(u);
             pdf = cosineHemispherePdf(wi);
             type = kRefl | kDiffuse;
             return l.a * kInvPi;
         }
-        case 1: {   // reflection.cpp:40-47
+        if ((M & (1u << 1)) && kind == 1) {   // reflection.cpp:40-47
             wi = v3(-wo.x, -wo.y, wo.z);
             pdf = 1.0f;
             type = kRefl | kSpecular;
             return l.a * condFresnel(l, wo.z);
         }
-        case 2: {   // reflection.cpp:61-93
+        if ((M & (1u << 2)) && kind == 2) {   // reflection.cpp:61-93
             float F = frDielectric(wo.z, 1.0f, l.eta);
             if (u.x < F) {
                 wi = v3(-wo.x, -wo.y, wo.z);
@@ -353,7 +361,7 @@ __device__ __forceinline__ V3 lobeSample(const Lobe& l, V3 wo, V3& wi, V2 u, flo
             float r = etaI / etaT;
             return ((l.b * r) * r) * (1.0f - F);
         }
-        case 3: {   // reflection.cpp:123-138
+        if ((M & (1u << 3)) && kind == 3) {   // reflection.cpp:123-138
             if (fabsf(wo.z) < kEpsilon) { pdf = 0.0f; return v3s(0.f); }
             V3 wh = ggxSampleWh(l.ggx, wo, u);
             float dotO = dot(wo, wh);
@@ -364,7 +372,7 @@ __device__ __forceinline__ V3 lobeSample(const Lobe& l, V3 wo, V3& wi, V2 u, flo
             type = kRefl | kGlossy;
             return mfReflF(l, wo, wi);
         }
-        case 4: {   // reflection.cpp:193-225
+        if ((M & (1u << 4)) && kind == 4) {   // reflection.cpp:193-225
             if (fabsf(wo.z) < kEpsilon) return v3s(0.f);
             bool entering = wo.z > 0.0f;
             float etaI = entering ? 1.0f : l.eta;
@@ -385,7 +393,7 @@ __device__ __forceinline__ V3 lobeSample(const Lobe& l, V3 wo, V3& wi, V2 u, flo
             pdf = mfFresPdf(l, wo, wi);
             return mfFresF(l, wo, wi);
         }
-        case 5: {   // reflection.cpp:266-284
+        if ((M & (1u << 5)) && kind == 5) {   // reflection.cpp:266-284
             if (wo.z < kEpsilon) { pdf = 0.0f; return v3s(0.f); }
             float ps = frDielectric(wo.z, 1.0f, l.eta);
             if (uc < ps) {
@@ -400,7 +408,7 @@ __device__ __forceinline__ V3 lobeSample(const Lobe& l, V3 wo, V3& wi, V2 u, flo
             type = kRefl | kDiffuse;
             return smoothPlasticF(l, wo, wi);
         }
-        default: {  // 6: reflection.cpp:315-335
+        if ((M & (1u << 6)) && kind == 6) {  // reflection.cpp:315-335
             if (wo.z < kEpsilon) { pdf = 0.0f; return v3s(0.f); }
             float ps = frDielectric(wo.z, 1.0f, l.eta);
             if (uc < ps) {
@@ -419,17 +427,22 @@ __device__ __forceinline__ V3 lobeSample(const Lobe& l, V3 wo, V3& wi, V2 u, flo
             return roughPlasticF(l, wo, wi);
         }
     }
+    pdf = 0.0f;
+    return v3s(0.f);
 }
 
 // Material -> lobe at a shading point (matte.cpp:46-53, plastic.cpp:74-91,
 // conductor.cpp:101-120, glass.cpp:98-115). Returns false for the index material.
+template <uint32_t M = kLobesAll>
 __device__ __forceinline__ bool makeLobe(const Material& m, V2 uv, Lobe& l) {
     switch (m.type) {
         case kMatMatte:
+            if (!(M & kLobesMatte)) return false;
             l.kind = 0;
             l.a = evalTex(m.a, uv);
             return true;
         case kMatPlastic:
+            if (!(M & kLobesPlastic)) return false;
             l.a = evalTex(m.a, uv);
             l.b = evalTex(m.b, uv);
             l.eta = m.eta;
@@ -437,6 +450,7 @@ __device__ __forceinline__ bool makeLobe(const Material& m, V2 uv, Lobe& l) {
             else { l.kind = 6; l.ggx = makeGgx(roughnessToAlpha(m.roughness)); }
             return true;
         case kMatConductor:
+            if (!(M & kLobesConductor)) return false;
             l.a = evalTex(m.a, uv);
             l.ceta = v3(m.condEta[0], m.condEta[1], m.condEta[2]);
             l.ck = v3(m.condK[0], m.condK[1], m.condK[2]);
@@ -444,6 +458,7 @@ __device__ __forceinline__ bool makeLobe(const Material& m, V2 uv, Lobe& l) {
             else { l.kind = 3; l.ggx = makeGgx(roughnessToAlpha(m.roughness)); }
             return true;
         case kMatGlass:
+            if (!(M & kLobesGlass)) return false;
             l.a = evalTex(m.a, uv);
             l.b = evalTex(m.b, uv);
             l.eta = m.eta;
@@ -468,26 +483,29 @@ __device__ __forceinline__ Frame shadingFrame(V3 n, V3 dpdu) {
     return f;
 }
 // bsdf.cpp:19-31
+template <uint32_t M = kLobesAll>
 __device__ __forceinline__ V3 bsdfF(const Bsdf& b, V3 woW, V3 wiW) {
     V3 wo = toLocal(b.fr, woW), wi = toLocal(b.fr, wiW);
     if (wo.z == 0.0f) return v3s(0.f);
-    return v3s(0.f) + lobeF(b.lobe, wo, wi);
+    return v3s(0.f) + lobeF<M>(b.lobe, wo, wi);
 }
 // bsdf.cpp:109-136 (one lobe: probability weight 1/1)
+template <uint32_t M = kLobesAll>
 __device__ __forceinline__ float bsdfPdf(const Bsdf& b, V3 woW, V3 wiW) {
     V3 wo = toLocal(b.fr, woW), wi = toLocal(b.fr, wiW);
     if (wo.z == 0.0f) return 0.0f;
-    return 0.0f + (1.0f / 1.0f) * lobePdf(b.lobe, wo, wi);
+    return 0.0f + (1.0f / 1.0f) * lobePdf<M>(b.lobe, wo, wi);
 }
 // bsdf.cpp:33-107 (one lobe; selectedProb = 1). Returns f*|cos|/pdf. When the reference
 // returns early without writing *pdf the value passed in is kept.
+template <uint32_t M = kLobesAll>
 __device__ __forceinline__ V3 bsdfSample(const Bsdf& b, V3 woW, V3& wiW, V2 u, float uc, float& pdfOut, uint32_t& type) {
     V3 wo = toLocal(b.fr, woW);
     if (wo.z == 0.0f) return v3s(0.f);
     V3 wi = v3s(0.f);
     float lp = 0.0f;
     type = 0;
-    V3 f = lobeSample(b.lobe, wo, wi, u, uc, lp, type);
+    V3 f = lobeSample<M>(b.lobe, wo, wi, u, uc, lp, type);
     wiW = toWorld(b.fr, wi);
     if (lp == 0.0f || isBlack(f)) { pdfOut = 0.0f; return v3s(0.f); }
     if (type & kSpecular) {

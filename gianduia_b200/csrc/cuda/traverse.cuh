@@ -470,13 +470,12 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
         if (idle && got < n) {
             idx = got;
             TRay r;
+            // a source may decline an item (it belongs to another kernel of the launch)
             if (src.load(idx, r, sv, nm)) {
                 travInit(t, *sv, r);
                 if (sv->tlasRoot != kEmpty) { st.put(0, sv->tlasRoot); t.sp = 1; }
                 active = true;
                 iter = 0;
-            } else {
-                src.store(idx, t.hit);   // never reached for valid inputs
             }
         }
         if (!__any_sync(0xffffffffu, active)) break;

@@ -27,6 +27,14 @@ namespace gnd {
 constexpr int kBlock = 128;
 constexpr float kFixScale = 16777216.0f;   // 2^24
 constexpr float kFixMax = 1e11f;           // per-sample clamp before the fixed-point conversion
+// Shade classes: integrator (0 path, 1 volpath) x material class. Material classes 0..3
+// follow the material type (matte, plastic, conductor, glass); class 4 holds misses,
+// null-BSDF surfaces and volpath paths inside a medium (which may scatter before
+// reaching the surface), shaded by the kernel built with every lobe.
+constexpr int kMatClasses = 5;
+constexpr int kShadeClasses = 2 * kMatClasses;
+static_assert(kQClass0 + kShadeClasses <= kQCount, "class counters exceed the counter block");
+
 
 // ---------------------------------------------------------------- queue helpers
 __device__ __forceinline__ uint32_t warpAppend(uint32_t* counter, bool pred) {
@@ -51,10 +59,13 @@ struct KParams {
     uint32_t* done;
     uint32_t* cnt;                 // queue counters (kQIn ...)
     unsigned long long* totals;    // [0] extend rays, [1] shadow queries, [2] paths retired
-    unsigned long long* workNext;  // next work item (batched refill)
+    JobCtl* ctl;                   // per job: next work item, retired samples
+    const uint32_t* active;        // active job indices (count in cnt[kQActive])
+    uint32_t* freeIn;              // idle slots waiting for work
+    uint32_t* freeOut;
     uint32_t* errWord;
     uint32_t capacity;
-    int batched;
+    uint32_t iter;                 // iteration number (round-robin start of job grabs)
 };
 
 // ---------------------------------------------------------------- surface interaction
@@ -357,34 +368,8 @@ __global__ void kBeginIter(uint32_t* cnt) {
     cnt[kQDone] = 0;
     cnt[kQFetchA] = 0;
     cnt[kQFetchB] = 0;
-}
-
-// Plain mode: pass `pass` of job 0 for every window pixel, slot = pixel index.
-__global__ void __launch_bounds__(kBlock) kRaygenPass(KParams p, uint64_t itemBase, uint32_t n) {
-    const JobDev& j = p.jobs[0];
-    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
-        PathState ps;
-        generatePath(j, 0, itemBase + i, ps);
-        p.paths[i] = ps;
-        p.listIn[i] = i;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) p.cnt[kQIn] = n;
-}
-
-// Batched mode: fill slots [0, n) from the shared work counter.
-__global__ void __launch_bounds__(kBlock) kRaygenFill(KParams p, uint32_t n) {
-    const JobDev& j = p.jobs[0];
-    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
-        uint64_t item = j.workBegin + i;
-        PathState ps;
-        generatePath(j, 0, item, ps);
-        p.paths[i] = ps;
-        p.listIn[i] = i;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        p.cnt[kQIn] = n;
-        *p.workNext = j.workBegin + n;
-    }
+    cnt[kQFreeOut] = 0;
+    for (int k = 0; k < kShadeClasses; ++k) cnt[kQClass0 + k] = 0;
 }
 
 // Closest-hit source/sink over the active list (extend).
@@ -437,12 +422,47 @@ __global__ void __launch_bounds__(kBlock, 8) kExtend(KParams p) {
     if (err) atomicOr(p.errWord, (uint32_t)err);
 }
 
-// One bounce of path (VOL = false) or volpath (VOL = true).
-template <bool VOL>
-__global__ void __launch_bounds__(kBlock) kShade(KParams p) {
+// Active list -> per-class lists (warp-aggregated appends, one atomic per class per warp).
+__global__ void __launch_bounds__(kBlock) kClassify(KParams p, uint32_t* classLists) {
     const uint32_t n = p.cnt[kQIn];
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * kBlock + (threadIdx.x & ~31u); base < n; base += gridDim.x * kBlock) {
+        const uint32_t i = base + lane;
+        const bool valid = i < n;
+        uint32_t cls = 0xFFFFFFFFu, slot = 0;
+        if (valid) {
+            slot = p.listIn[i];
+            const PathState* ps = p.paths + slot;
+            const uint32_t jobIdx = ps->flags >> 8;
+            const int medium = ps->medium;
+            const JobDev& j = p.jobs[jobIdx];
+            const int inst = p.hits[slot].inst;
+            const uint32_t vol = j.integrator == 1 ? 1u : 0u;
+            uint32_t mc = kMatClasses - 1;
+            if (inst >= 0 && !(vol && medium >= 0)) {
+                uint32_t t = j.view.materials[j.view.instS[inst].material].type;
+                mc = t < (uint32_t)(kMatClasses - 1) ? t : (uint32_t)(kMatClasses - 1);
+            }
+            cls = vol * kMatClasses + mc;
+        }
+        const uint32_t grp = __match_any_sync(0xffffffffu, cls);
+        if (valid) {
+            const int leader = __ffs(grp) - 1;
+            uint32_t b = 0;
+            if ((int)lane == leader) b = atomicAdd(&p.cnt[kQClass0 + cls], (uint32_t)__popc(grp));
+            b = __shfl_sync(grp, b, leader);
+            classLists[(size_t)cls * p.capacity + b + (uint32_t)__popc(grp & ((1u << lane) - 1u))] = slot;
+        }
+    }
+}
+
+// One bounce of path (VOL = false) or volpath (VOL = true) for the slots of one shade
+// class; M is the set of lobes the class can meet (every lobe for class 4).
+template <bool VOL, uint32_t M>
+__global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list, const uint32_t* count) {
+    const uint32_t n = *count;
     for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
-        uint32_t slot = p.listIn[i];
+        uint32_t slot = list[i];
         PathState ps = p.paths[slot];
         const HitRec h = p.hits[slot];
         const uint32_t jobIdx = ps.flags >> 8;
@@ -463,7 +483,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p) {
         const bool hit = h.inst >= 0;
 
         do {
-            if (VOL && medium >= 0) {
+            if (VOL && M == kLobesAll && medium >= 0) {
                 // medium->sample (homogeneous.cpp:32-63); the ray's tMax is the hit distance
                 const Medium m = s.media[medium];
                 float rtmax = hit ? h.t : INFINITY;
@@ -528,7 +548,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p) {
             const InstShade& is = s.instS[h.inst];
             const Material mat = s.materials[is.material];
             Bsdf bsdf;
-            const bool hasBsdf = makeLobe(mat, si.uv, bsdf.lobe);
+            const bool hasBsdf = makeLobe<M>(mat, si.uv, bsdf.lobe);
             if (is.emitter >= 0) {
                 bool skip = (bounces == 0 && !hasBsdf);
                 if (!skip) {
@@ -564,8 +584,8 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p) {
             V3 Li = ls.Li * (1.0f / lightSelectPdf);
             if (ls.pdf > 1e-6f && !isBlack(Li)) {
                 V3 wi = normalize(ls.p - si.p);
-                float bp = bsdfPdf(bsdf, -d, wi);
-                V3 f = bsdfF(bsdf, -d, wi);
+                float bp = bsdfPdf<M>(bsdf, -d, wi);
+                V3 f = bsdfF<M>(bsdf, -d, wi);
                 if (!isBlack(f) && bp > 1e-6f) {
                     float pl = ls.pdf * lightSelectPdf;
                     float wl = powerHeuristic(pl, bp);
@@ -584,7 +604,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p) {
             float u1 = next1D(rng);
             V3 wi;
             uint32_t type = 0;
-            V3 fcos = bsdfSample(bsdf, -d, wi, u2, u1, pdfPrev, type);
+            V3 fcos = bsdfSample<M>(bsdf, -d, wi, u2, u1, pdfPrev, type);
             if (isBlack(fcos) || pdfPrev <= 1e-6f) { terminate = true; break; }
             specular = (type & kSpecular) != 0;
             tp = tp * fcos;
@@ -646,6 +666,7 @@ struct ShadowSrc {
     uint32_t n;
     uint32_t slot;
     const uint8_t* nm;
+    bool mixed;
     __device__ uint32_t count() const { return n; }
     __device__ bool load(uint32_t i, TRay& r, const SceneView*& sv, const uint8_t*& nmOut) {
         const ShadowRec* sr = p->shadow + i;
@@ -657,6 +678,7 @@ struct ShadowSrc {
         r.d = v3(b.x, b.y, b.z);
         r.tmin = kEpsilon;
         const JobDev& j = p->jobs[p->paths[slot].flags >> 8];
+        if (mixed && j.integrator != 0) return false;
         sv = &j.view;
         nm = j.nullMask;
         nmOut = nullptr;
@@ -676,11 +698,11 @@ struct ShadowSrc {
 };
 
 template <bool ANY>
-__global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p) {
+__global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p, bool mixed) {
     __shared__ uint32_t stack[kSmemStack * kBlock];
     const uint32_t n = p.cnt[kQShadow];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
-    ShadowSrc<ANY> src{&p, n, 0, nullptr};
+    ShadowSrc<ANY> src{&p, n, 0, nullptr, mixed};
     int err = persistentTrace<kBlock, ANY, false>(src, p.cnt + kQFetchB, stack, nullptr);
     if (err) atomicOr(p.errWord, (uint32_t)err);
 }
@@ -688,17 +710,18 @@ __global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p) {
 // Shadow queries of `volpath`: evaluateTr (volPath.cpp:261-291), a loop of closest hits
 // through null-BSDF boundaries multiplying the transmittance of each medium segment.
 template <bool VOL>
-__global__ void __launch_bounds__(kBlock) kShadow(KParams p) {
+__global__ void __launch_bounds__(kBlock) kShadow(KParams p, bool mixed) {
     __shared__ uint32_t stack[kStackSize * kBlock];
     uint32_t* stk = stack + threadIdx.x;
     const uint32_t n = p.cnt[kQShadow];
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
+    if (!mixed && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
     int err = 0;
     for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
         const ShadowRec sr = p.shadow[i];
         const uint32_t slot = sr.slot;
         const uint32_t jobIdx = p.paths[slot].flags >> 8;
         const JobDev& j = p.jobs[jobIdx];
+        if (mixed && j.integrator != 1) continue;
         const SceneView& s = j.view;
         TRay r;
         r.o = v3(sr.ox, sr.oy, sr.oz);
@@ -798,39 +821,136 @@ __device__ __forceinline__ void filmSplat(const JobDev& j, const PathState& ps) 
     }
 }
 
-// Finished paths: film splat; in batched mode the slot takes the next work item.
-__global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
-    const uint32_t n = p.cnt[kQDone];
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[2], (unsigned long long)n);
-    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
-        uint32_t slot = p.done[i];
-        PathState ps = p.paths[slot];
-        const uint32_t jobIdx = ps.flags >> 8;
-        const JobDev& j = p.jobs[jobIdx];
-        filmSplat(j, ps);
-        bool refill = false;
-        uint64_t item = 0;
-        if (p.batched) {
-            item = atomicAdd(p.workNext, 1ull);
-            refill = item < j.workEnd;
-            if (refill) {
-                generatePath(j, jobIdx, item, ps);
-                p.paths[slot] = ps;
-            }
+// ---------------------------------------------------------------- retire / refill
+// Lanes in `want` take work items from the active jobs: the warp leader walks the active
+// list from a per-warp round-robin start and takes one contiguous range per job until the
+// warp is served (at most four jobs per grab); lanes left over stay idle this iteration.
+__device__ __forceinline__ bool warpGrab(const KParams& p, bool want, uint32_t& jobOut, uint64_t& itemOut) {
+    const uint32_t full = 0xffffffffu;
+    uint32_t mask = __ballot_sync(full, want);
+    if (!mask) return false;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t sj0 = 0, sj1 = 0, sj2 = 0, sj3 = 0, sc0 = 0, sc1 = 0, sc2 = 0, sc3 = 0;
+    unsigned long long sb0 = 0, sb1 = 0, sb2 = 0, sb3 = 0;
+    if (lane == leader) {
+        const uint32_t na = p.cnt[kQActive];
+        uint32_t remaining = (uint32_t)__popc(mask);
+        const uint32_t start = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5) + p.iter;
+        int ns = 0;
+        for (uint32_t t = 0; t < na && remaining > 0 && ns < 4; ++t) {
+            uint32_t jid = p.active[(start + t) % na];
+            unsigned long long end = p.jobs[jid].workEnd;
+            if (*(volatile unsigned long long*)&p.ctl[jid].next >= end) continue;
+            unsigned long long got = atomicAdd(&p.ctl[jid].next, (unsigned long long)remaining);
+            if (got >= end) continue;
+            uint32_t avail = (uint32_t)min((unsigned long long)remaining, end - got);
+            if (ns == 0) { sj0 = jid; sb0 = got; sc0 = avail; }
+            else if (ns == 1) { sj1 = jid; sb1 = got; sc1 = avail; }
+            else if (ns == 2) { sj2 = jid; sb2 = got; sc2 = avail; }
+            else { sj3 = jid; sb3 = got; sc3 = avail; }
+            ++ns;
+            remaining -= avail;
         }
-        uint32_t k = warpAppend(&p.cnt[kQOut], refill);
-        if (refill) p.listOut[k] = slot;
     }
+    sj0 = __shfl_sync(full, sj0, leader); sc0 = __shfl_sync(full, sc0, leader); sb0 = __shfl_sync(full, sb0, leader);
+    sj1 = __shfl_sync(full, sj1, leader); sc1 = __shfl_sync(full, sc1, leader); sb1 = __shfl_sync(full, sb1, leader);
+    sj2 = __shfl_sync(full, sj2, leader); sc2 = __shfl_sync(full, sc2, leader); sb2 = __shfl_sync(full, sb2, leader);
+    sj3 = __shfl_sync(full, sj3, leader); sc3 = __shfl_sync(full, sc3, leader); sb3 = __shfl_sync(full, sb3, leader);
+    if (!want) return false;
+    uint32_t r = (uint32_t)__popc(mask & ((1u << lane) - 1u));
+    if (r < sc0) { jobOut = sj0; itemOut = sb0 + r; return true; }
+    r -= sc0;
+    if (r < sc1) { jobOut = sj1; itemOut = sb1 + r; return true; }
+    r -= sc1;
+    if (r < sc2) { jobOut = sj2; itemOut = sb2 + r; return true; }
+    r -= sc2;
+    if (r < sc3) { jobOut = sj3; itemOut = sb3 + r; return true; }
+    return false;
+}
+
+// Finished paths (done list): film splat and per-job retired count. Finished and idle
+// slots (free list) then take new work items; slots left without work join the next
+// free list. The loop is warp-uniform (all lanes of a warp iterate together).
+__global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
+    const uint32_t nd = p.cnt[kQDone], nf = p.cnt[kQFree];
+    const uint32_t total = nd + nf;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[2], (unsigned long long)nd);
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * kBlock + (threadIdx.x & ~31u); base < total; base += gridDim.x * kBlock) {
+        const uint32_t i = base + lane;
+        const bool valid = i < total;
+        const bool isDone = i < nd;
+        const uint32_t slot = valid ? (isDone ? p.done[i] : p.freeIn[i - nd]) : 0u;
+        uint32_t jobIdx = 0xFFFFFFFFu;
+        if (valid && isDone) {
+            PathState ps = p.paths[slot];
+            jobIdx = ps.flags >> 8;
+            filmSplat(p.jobs[jobIdx], ps);
+        }
+        const uint32_t grp = __match_any_sync(0xffffffffu, jobIdx);
+        if (jobIdx != 0xFFFFFFFFu && (int)lane == __ffs(grp) - 1)
+            atomicAdd(&p.ctl[jobIdx].retired, (unsigned long long)__popc(grp));
+        uint32_t gj = 0;
+        uint64_t item = 0;
+        const bool got = warpGrab(p, valid, gj, item);
+        if (got) {
+            PathState ps;
+            generatePath(p.jobs[gj], gj, item, ps);
+            p.paths[slot] = ps;
+        }
+        const uint32_t k = warpAppend(&p.cnt[kQOut], got);
+        if (got) p.listOut[k] = slot;
+        const bool idle = valid && !got;
+        const uint32_t f = warpAppend(&p.cnt[kQFreeOut], idle);
+        if (idle) p.freeOut[f] = slot;
+    }
+}
+
+__global__ void kEndIter(uint32_t* cnt) {
+    cnt[kQIn] = cnt[kQOut];
+    cnt[kQFree] = cnt[kQFreeOut];
+}
+
+// Every slot idle: free list = [0, n).
+__global__ void kResetPool(uint32_t* freeList, uint32_t n, uint32_t* cnt) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) freeList[i] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int k = 0; k < kQCount; ++k)
+            if (k != kQActive) cnt[k] = 0;
+        cnt[kQFree] = n;
+    }
+}
+
+// One shade launch per material class of one integrator (empty classes exit at once).
+template <bool VOL>
+static void launchShade(const KParams& kp, uint32_t* classLists, int grid, cudaStream_t st) {
+    const size_t cap = kp.capacity;
+    const int c0 = VOL ? kMatClasses : 0;
+    uint32_t* cnt = kp.cnt + kQClass0 + c0;
+    uint32_t* lists = classLists + (size_t)c0 * cap;
+    static_assert(kMatMatte == 0 && kMatPlastic == 1 && kMatConductor == 2 && kMatGlass == 3,
+                  "material classes follow the material type codes");
+    kShade<VOL, kLobesMatte><<<grid, kBlock, 0, st>>>(kp, lists + 0 * cap, cnt + 0);
+    kShade<VOL, kLobesPlastic><<<grid, kBlock, 0, st>>>(kp, lists + 1 * cap, cnt + 1);
+    kShade<VOL, kLobesConductor><<<grid, kBlock, 0, st>>>(kp, lists + 2 * cap, cnt + 2);
+    kShade<VOL, kLobesGlass><<<grid, kBlock, 0, st>>>(kp, lists + 3 * cap, cnt + 3);
+    kShade<VOL, kLobesAll><<<grid, kBlock, 0, st>>>(kp, lists + 4 * cap, cnt + 4);
 }
 
 // ---------------------------------------------------------------- host driver
 Wavefront::Wavefront(Context* c) : ctx_(c) {
     counters_.alloc(kQCount * sizeof(uint32_t));
+    GND_CUDA(cudaMemset(counters_.ptr, 0, kQCount * sizeof(uint32_t)));
     totals_.alloc(8 * sizeof(unsigned long long));
-    job_.alloc(sizeof(JobDev));
-    workNext_.alloc(sizeof(unsigned long long));
+    jobTab_.alloc(kMaxJobs * sizeof(JobDev));
+    ctl_.alloc(kMaxJobs * sizeof(JobCtl));
+    active_.alloc(kMaxJobs * sizeof(uint32_t));
+    GND_CUDA(cudaMemset(ctl_.ptr, 0, kMaxJobs * sizeof(JobCtl)));
 }
-Wavefront::~Wavefront() = default;
+Wavefront::~Wavefront() {
+    for (cudaEvent_t e : evs_) cudaEventDestroy(e);
+}
 
 void Wavefront::ensureCapacity(size_t slots) {
     if (slots <= cap_) return;
@@ -838,41 +958,73 @@ void Wavefront::ensureCapacity(size_t slots) {
     hits_.alloc(slots * sizeof(HitRec));
     listA_.alloc(slots * sizeof(uint32_t));
     listB_.alloc(slots * sizeof(uint32_t));
+    freeA_.alloc(slots * sizeof(uint32_t));
+    freeB_.alloc(slots * sizeof(uint32_t));
     shadow_.alloc(slots * sizeof(ShadowRec));
     done_.alloc(slots * sizeof(uint32_t));
+    classes_.alloc(slots * kShadeClasses * sizeof(uint32_t));
     cap_ = slots;
 }
 
-Wavefront::Result Wavefront::render(DeviceScene& ds, int spp, int firstPass, int maxDepth, int integrator,
-                                    const int window[4], bool batched, int profile, float* filmHost, gnd_progress_fn cb,
-                                    void* user) {
-    Context* c = ctx_;
-    cudaStream_t st = c->stream;
-    const int W = ds.width, H = ds.height;
-    if (W <= 0 || H <= 0) throw Error(GND_ERR_INVALID, "scene has no camera film size");
+void Wavefront::reset(size_t slots) {
+    ensureCapacity(std::max<size_t>(slots, 1));
+    cudaStream_t st = ctx_->stream;
+    cur_ = 0;
+    kResetPool<<<ctx_->numSMs * 4, 256, 0, st>>>(freeA_.as<uint32_t>(), (uint32_t)slots, counters_.as<uint32_t>());
+    GND_CUDA(cudaGetLastError());
+    GND_CUDA(cudaMemsetAsync(totals_.ptr, 0, 8 * sizeof(unsigned long long), st));
+}
+
+uint64_t Wavefront::jobBytes() const {
+    uint64_t b = 0;
+    for (const HostJob& j : jobs_)
+        if (j.used) b += j.bytes;
+    return b;
+}
+
+void Wavefront::syncActive() {
+    uint32_t ids[kMaxJobs];
+    uint32_t n = 0;
+    for (int j = 0; j < kMaxJobs; ++j)
+        if (jobs_[j].used) ids[n++] = (uint32_t)j;
+    cudaStream_t st = ctx_->stream;
+    if (n) GND_CUDA(cudaMemcpyAsync(active_.ptr, ids, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    GND_CUDA(cudaMemcpyAsync(counters_.as<uint32_t>() + kQActive, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    // the staging arrays are on the stack: wait for the copies before returning
+    GND_CUDA(cudaStreamSynchronize(st));
+    activeDirty_ = false;
+}
+
+int Wavefront::admit(const DeviceScene& ds, int W, int H, int spp, int firstPass, int maxDepth, int integrator,
+                     const int window[4], uint64_t releaseItems) {
+    int j = -1;
+    for (int k = 0; k < kMaxJobs; ++k)
+        if (!jobs_[k].used) { j = k; break; }
+    if (j < 0) throw Error(GND_ERR_BUDGET, "job table full");
+    if (W <= 0 || H <= 0) throw Error(GND_ERR_INVALID, "job has no film size");
     if (ds.view.numEmitters <= 0) throw Error(GND_ERR_INVALID, "the path integrators need at least one emitter");
     int wx0 = 0, wy0 = 0, wx1 = W, wy1 = H;
     if (window && (window[0] | window[1] | window[2] | window[3])) {
         wx0 = window[0]; wy0 = window[1]; wx1 = window[2]; wy1 = window[3];
         if (wx0 < 0 || wy0 < 0 || wx1 > W || wy1 > H || wx0 >= wx1 || wy0 >= wy1) throw Error(GND_ERR_INVALID, "bad pixel window");
     }
-    const uint64_t npix = (uint64_t)(wx1 - wx0) * (uint64_t)(wy1 - wy0);
-    const uint64_t total = npix * (uint64_t)spp;
-    if (npix > (1ull << 31)) throw Error(GND_ERR_INVALID, "window too large");
-    // slot pool: one pass for plain renders, up to ~4M in-flight paths for batched ones
-    size_t slots = batched ? (size_t)std::min<uint64_t>(total, std::max<uint64_t>(npix, 1ull << 22)) : (size_t)npix;
-    ensureCapacity(std::max<size_t>(slots, 1));
-    filmSum_.ensure((size_t)W * H * 4 * sizeof(unsigned long long));
-    filmSq_.ensure((size_t)W * H * 3 * sizeof(float));
-    GND_CUDA(cudaMemsetAsync(filmSum_.ptr, 0, (size_t)W * H * 4 * sizeof(unsigned long long), st));
-    GND_CUDA(cudaMemsetAsync(filmSq_.ptr, 0, (size_t)W * H * 3 * sizeof(float), st));
-    GND_CUDA(cudaMemsetAsync(totals_.ptr, 0, 8 * sizeof(unsigned long long), st));
-
-    JobDev jd{};
+    HostJob& hj = jobs_[j];
+    cudaStream_t st = ctx_->stream;
+    const size_t npixAll = (size_t)W * H;
+    hj.filmSum.alloc(npixAll * 4 * sizeof(unsigned long long));
+    hj.filmSq.alloc(npixAll * 3 * sizeof(float));
+    GND_CUDA(cudaMemsetAsync(hj.filmSum.ptr, 0, npixAll * 4 * sizeof(unsigned long long), st));
+    GND_CUDA(cudaMemsetAsync(hj.filmSq.ptr, 0, npixAll * 3 * sizeof(float), st));
+    hj.bytes = hj.filmSum.bytes + hj.filmSq.bytes;
+    JobDev& jd = hj.dev;
+    jd = JobDev{};
     jd.view = ds.view;
+    jd.view.camera.width = W;
+    jd.view.camera.height = H;
+    jd.view.camera.aspect = W / (float)H;   // perspective.cpp:20 (getAspectRatio)
     jd.nullMask = ds.nullMask.as<uint8_t>();
-    jd.filmSum = filmSum_.as<unsigned long long>();
-    jd.filmSq = filmSq_.as<float>();
+    jd.filmSum = hj.filmSum.as<unsigned long long>();
+    jd.filmSq = hj.filmSq.as<float>();
     jd.W = W; jd.H = H; jd.maxDepth = maxDepth; jd.integrator = integrator;
     jd.wx0 = wx0; jd.wy0 = wy0; jd.wx1 = wx1; jd.wy1 = wy1;
     jd.filter = ds.filter;
@@ -883,126 +1035,225 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int spp, int firstPass, int
     jd.fexpY = std::exp(-jd.falpha * jd.fry * jd.fry);
     jd.hasNull = ds.hasNullMaterials ? 1 : 0;
     jd.firstPass = firstPass;
+    hj.total = (uint64_t)(wx1 - wx0) * (uint64_t)(wy1 - wy0) * (uint64_t)spp;
+    hj.released = std::min<uint64_t>(releaseItems, hj.total);
+    hj.retired = 0;
     jd.workBegin = 0;
-    jd.workEnd = total;
-    GND_CUDA(cudaMemcpyAsync(job_.ptr, &jd, sizeof(JobDev), cudaMemcpyHostToDevice, st));
+    jd.workEnd = hj.released;
+    hj.used = true;
+    GND_CUDA(cudaMemcpyAsync(jobTab_.as<JobDev>() + j, &jd, sizeof(JobDev), cudaMemcpyHostToDevice, st));
+    GND_CUDA(cudaMemsetAsync(ctl_.as<JobCtl>() + j, 0, sizeof(JobCtl), st));
+    syncActive();
+    return j;
+}
 
+void Wavefront::release(int j, uint64_t upTo) {
+    HostJob& hj = jobs_[j];
+    hj.released = std::min(upTo, hj.total);
+    hj.dev.workEnd = hj.released;
+    GND_CUDA(cudaMemcpyAsync(&jobTab_.as<JobDev>()[j].workEnd, &hj.dev.workEnd, sizeof(uint64_t), cudaMemcpyHostToDevice,
+                             ctx_->stream));
+    GND_CUDA(cudaStreamSynchronize(ctx_->stream));
+}
+
+uint64_t Wavefront::retired(int j) {
+    JobCtl c;
+    GND_CUDA(cudaMemcpyAsync(&c, ctl_.as<JobCtl>() + j, sizeof(JobCtl), cudaMemcpyDeviceToHost, ctx_->stream));
+    GND_CUDA(cudaStreamSynchronize(ctx_->stream));
+    jobs_[j].retired = c.retired;
+    return c.retired;
+}
+
+void Wavefront::readRetired(std::vector<uint64_t>& out) {
+    JobCtl c[kMaxJobs];
+    GND_CUDA(cudaMemcpyAsync(c, ctl_.ptr, sizeof(c), cudaMemcpyDeviceToHost, ctx_->stream));
+    GND_CUDA(cudaStreamSynchronize(ctx_->stream));
+    out.resize(kMaxJobs);
+    for (int j = 0; j < kMaxJobs; ++j) {
+        out[j] = c[j].retired;
+        if (jobs_[j].used) jobs_[j].retired = c[j].retired;
+    }
+}
+
+void Wavefront::finish(int j, float* filmHost) {
+    HostJob& hj = jobs_[j];
+    const size_t npix = (size_t)hj.dev.W * hj.dev.H;
+    std::vector<unsigned long long> fs(npix * 4);
+    std::vector<float> fq(npix * 3);
+    GND_CUDA(cudaMemcpyAsync(fs.data(), hj.filmSum.ptr, fs.size() * 8, cudaMemcpyDeviceToHost, ctx_->stream));
+    GND_CUDA(cudaMemcpyAsync(fq.data(), hj.filmSq.ptr, fq.size() * 4, cudaMemcpyDeviceToHost, ctx_->stream));
+    GND_CUDA(cudaStreamSynchronize(ctx_->stream));
+    if (filmHost) {
+        for (size_t q = 0; q < npix; ++q) {
+            for (int k = 0; k < 4; ++k) filmHost[q * 7 + k] += (float)((double)fs[q * 4 + k] / 16777216.0);
+            for (int k = 0; k < 3; ++k) filmHost[q * 7 + 4 + k] += fq[q * 3 + k];
+        }
+    }
+    drop(j);
+}
+
+void Wavefront::drop(int j) {
+    HostJob& hj = jobs_[j];
+    hj.used = false;
+    hj.filmSum.release();
+    hj.filmSq.release();
+    hj.bytes = 0;
+    syncActive();
+}
+
+uint32_t Wavefront::step(int iters, int mix, bool hasNull, int profile, Result& acc) {
+    Context* c = ctx_;
+    cudaStream_t st = c->stream;
+    const int grid = c->numSMs * 8;
     KParams kp{};
-    kp.jobs = job_.as<JobDev>();
+    kp.jobs = jobTab_.as<JobDev>();
     kp.paths = paths_.as<PathState>();
     kp.hits = hits_.as<HitRec>();
     kp.shadow = shadow_.as<ShadowRec>();
     kp.done = done_.as<uint32_t>();
     kp.cnt = counters_.as<uint32_t>();
     kp.totals = totals_.as<unsigned long long>();
-    kp.workNext = workNext_.as<unsigned long long>();
+    kp.ctl = ctl_.as<JobCtl>();
+    kp.active = active_.as<uint32_t>();
     kp.errWord = c->errWord.as<uint32_t>();
     kp.capacity = (uint32_t)cap_;
-    kp.batched = batched ? 1 : 0;
     uint32_t* lists[2] = {listA_.as<uint32_t>(), listB_.as<uint32_t>()};
+    uint32_t* frees[2] = {freeA_.as<uint32_t>(), freeB_.as<uint32_t>()};
+    for (int it = 0; it < iters; ++it) {
+        kp.listIn = lists[cur_];
+        kp.listOut = lists[cur_ ^ 1];
+        kp.freeIn = frees[cur_];
+        kp.freeOut = frees[cur_ ^ 1];
+        kp.iter = iter_++;
+        kBeginIter<<<1, 1, 0, st>>>(kp.cnt);
+        acc.iterations++;
+        cudaEvent_t ea = nullptr, eb = nullptr;
+        if (profile & 1) {
+            GND_CUDA(cudaEventCreate(&ea));
+            GND_CUDA(cudaEventCreate(&eb));
+            GND_CUDA(cudaEventRecord(ea, st));
+        }
+        if (profile & 2) kExtend<true><<<grid, kBlock, 0, st>>>(kp);
+        else kExtend<false><<<grid, kBlock, 0, st>>>(kp);
+        if (profile & 1) {
+            GND_CUDA(cudaEventRecord(eb, st));
+            evs_.push_back(ea);
+            evs_.push_back(eb);
+        }
+        uint32_t* cls = classes_.as<uint32_t>();
+        kClassify<<<grid, kBlock, 0, st>>>(kp, cls);
+        if (mix & 1) launchShade<false>(kp, cls, grid, st);
+        if (mix & 2) launchShade<true>(kp, cls, grid, st);
+        if (mix & 1) {
+            if (hasNull) kShadowPath<false><<<grid, kBlock, 0, st>>>(kp, mix == 3);
+            else kShadowPath<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
+        }
+        if (mix & 2) kShadow<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
+        kRetire<<<grid, kBlock, 0, st>>>(kp);
+        kEndIter<<<1, 1, 0, st>>>(kp.cnt);
+        GND_CUDA(cudaGetLastError());
+        cur_ ^= 1;
+    }
+    uint32_t inflight = 0;
+    GND_CUDA(cudaMemcpyAsync(&inflight, kp.cnt + kQIn, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GND_CUDA(cudaStreamSynchronize(st));
+    return inflight;
+}
 
-    const int grid = c->numSMs * 8;
+Wavefront::Result Wavefront::render(DeviceScene& ds, int spp, int firstPass, int maxDepth, int integrator,
+                                    const int window[4], bool batched, int profile, float* filmHost, gnd_progress_fn cb,
+                                    void* user) {
+    Context* c = ctx_;
+    cudaStream_t st = c->stream;
+    const int W = ds.width, H = ds.height;
+    int wx0 = 0, wy0 = 0, wx1 = W, wy1 = H;
+    if (window && (window[0] | window[1] | window[2] | window[3])) {
+        wx0 = window[0]; wy0 = window[1]; wx1 = window[2]; wy1 = window[3];
+    }
+    const uint64_t npix = (uint64_t)std::max(0, wx1 - wx0) * (uint64_t)std::max(0, wy1 - wy0);
+    const uint64_t total = npix * (uint64_t)std::max(spp, 0);
+    if (npix > (1ull << 31)) throw Error(GND_ERR_INVALID, "window too large");
+    Result res;
+    if (total == 0) return res;
+    // the pool: one pass for plain renders, up to 4M in-flight paths for batched ones
+    const size_t slots = batched ? (size_t)std::min<uint64_t>(total, std::max<uint64_t>(npix, 1ull << 22)) : (size_t)npix;
+    for (int j = 0; j < kMaxJobs; ++j)
+        if (jobs_[j].used) throw Error(GND_ERR_INVALID, "the engine is serving jobs; render through the server");
+    reset(slots);
+    const int j = admit(ds, W, H, spp, firstPass, maxDepth, integrator, window, batched ? total : npix);
+    const int mix = integrator == 1 ? 2 : 1;
     cudaEvent_t e0, e1;
     GND_CUDA(cudaEventCreate(&e0));
     GND_CUDA(cudaEventCreate(&e1));
     GND_CUDA(cudaEventRecord(e0, st));
-    Result res;
-    std::vector<float> passFilm;
-    std::vector<cudaEvent_t> evs;   // extend start/stop pairs when timing
-    auto runLoop = [&](int maxIter) {
-        int cur = 0;
-        uint32_t hostCnt = 1;
-        for (int it = 0; it < maxIter; ++it) {
-            kp.listIn = lists[cur];
-            kp.listOut = lists[cur ^ 1];
-            kBeginIter<<<1, 1, 0, st>>>(kp.cnt);
-            res.iterations++;
-            cudaEvent_t ea = nullptr, eb = nullptr;
-            if (profile & 1) {
-                GND_CUDA(cudaEventCreate(&ea));
-                GND_CUDA(cudaEventCreate(&eb));
-                GND_CUDA(cudaEventRecord(ea, st));
-            }
-            if (profile & 2) kExtend<true><<<grid, kBlock, 0, st>>>(kp);
-            else kExtend<false><<<grid, kBlock, 0, st>>>(kp);
-            if (profile & 1) {
-                GND_CUDA(cudaEventRecord(eb, st));
-                evs.push_back(ea);
-                evs.push_back(eb);
-            }
-            if (integrator == 1) kShade<true><<<grid, kBlock, 0, st>>>(kp);
-            else kShade<false><<<grid, kBlock, 0, st>>>(kp);
-            if (integrator == 1) kShadow<true><<<grid, kBlock, 0, st>>>(kp);
-            else if (ds.hasNullMaterials) kShadowPath<false><<<grid, kBlock, 0, st>>>(kp);
-            else kShadowPath<true><<<grid, kBlock, 0, st>>>(kp);
-            kRetire<<<grid, kBlock, 0, st>>>(kp);
-            GND_CUDA(cudaGetLastError());
-            // next iteration reads the list just written; move its count into kQIn
-            cudaMemcpyAsync(kp.cnt + kQIn, kp.cnt + kQOut, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
-            cur ^= 1;
-            if ((it & 3) == 3 || it < 4) {
-                GND_CUDA(cudaMemcpyAsync(&hostCnt, kp.cnt + kQIn, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-                GND_CUDA(cudaStreamSynchronize(st));
-                if (hostCnt == 0) return;
-            }
-        }
-        throw Error(GND_ERR_DEVICE_CHECK, "path iteration limit reached");
-    };
-    const int maxIter = maxDepth * 2 + 512;
-    if (!batched) {
-        for (int s = 0; s < spp; ++s) {
-            if (c->cancel) break;
-            kp.listIn = lists[0];
-            kRaygenPass<<<grid, kBlock, 0, st>>>(kp, (uint64_t)s * npix, (uint32_t)npix);
-            GND_CUDA(cudaGetLastError());
-            runLoop(maxIter);
-            res.passesDone = s + 1;
-            if (cb) {
-                // film so far, as the reference's per-pass resolve + callback
-                passFilm.assign((size_t)W * H * 7, 0.0f);
-                std::vector<unsigned long long> fs((size_t)W * H * 4);
-                std::vector<float> fq((size_t)W * H * 3);
-                GND_CUDA(cudaMemcpyAsync(fs.data(), filmSum_.ptr, fs.size() * 8, cudaMemcpyDeviceToHost, st));
-                GND_CUDA(cudaMemcpyAsync(fq.data(), filmSq_.ptr, fq.size() * 4, cudaMemcpyDeviceToHost, st));
-                GND_CUDA(cudaStreamSynchronize(st));
-                for (size_t q = 0; q < (size_t)W * H; ++q) {
-                    for (int k = 0; k < 4; ++k) passFilm[q * 7 + k] = (float)((double)fs[q * 4 + k] / 16777216.0);
-                    for (int k = 0; k < 3; ++k) passFilm[q * 7 + 4 + k] = fq[q * 3 + k];
+    int pass = 0;
+    const int itersPerStep = batched ? 4 : 2;
+    const int64_t iterCap = (int64_t)(maxDepth + 110) * (spp + 2) * 4 + 4096;
+    bool cancelled = false;
+    try {
+        for (;;) {
+            uint32_t inflight = step(itersPerStep, mix, ds.hasNullMaterials, profile, res);
+            uint64_t r = retired(j);
+            if (!batched) {
+                while (pass < spp && r >= (uint64_t)(pass + 1) * npix) {
+                    ++pass;
+                    res.passesDone = pass;
+                    if (cb) {
+                        // film so far, as the reference's per-pass resolve + callback
+                        const size_t n = (size_t)W * H;
+                        std::vector<unsigned long long> fs(n * 4);
+                        std::vector<float> fq(n * 3), pf(n * 7);
+                        GND_CUDA(cudaMemcpyAsync(fs.data(), jobs_[j].filmSum.ptr, fs.size() * 8, cudaMemcpyDeviceToHost, st));
+                        GND_CUDA(cudaMemcpyAsync(fq.data(), jobs_[j].filmSq.ptr, fq.size() * 4, cudaMemcpyDeviceToHost, st));
+                        GND_CUDA(cudaStreamSynchronize(st));
+                        for (size_t q = 0; q < n; ++q) {
+                            for (int k = 0; k < 4; ++k) pf[q * 7 + k] = (float)((double)fs[q * 4 + k] / 16777216.0);
+                            for (int k = 0; k < 3; ++k) pf[q * 7 + 4 + k] = fq[q * 3 + k];
+                        }
+                        cb(user, firstPass + pass - 1, pf.data(), W, H);
+                    }
+                    if (pass < spp && !c->cancel) release(j, (uint64_t)(pass + 1) * npix);
                 }
-                cb(user, firstPass + s, passFilm.data(), W, H);
+                if (c->cancel && !cancelled) cancelled = true;
+            } else if (c->cancel && !cancelled) {
+                // stop handing out work; let the paths in flight finish
+                release(j, std::max<uint64_t>(jobs_[j].released, 0));
+                jobs_[j].dev.workEnd = 0;
+                GND_CUDA(cudaMemsetAsync(&jobTab_.as<JobDev>()[j].workEnd, 0, sizeof(uint64_t), st));
+                cancelled = true;
             }
+            if (r >= total && inflight == 0) break;
+            if (cancelled && inflight == 0) break;
+            if (res.iterations > iterCap) throw Error(GND_ERR_DEVICE_CHECK, "path iteration limit reached");
         }
-    } else {
-        kp.listIn = lists[0];
-        kRaygenFill<<<grid, kBlock, 0, st>>>(kp, (uint32_t)slots);
-        GND_CUDA(cudaGetLastError());
-        runLoop(maxIter * std::max(1, spp) + 64);
-        res.passesDone = spp;
+    } catch (...) {
+        drop(j);
+        throw;
     }
+    if (batched) res.passesDone = cancelled ? (int)(retired(j) / std::max<uint64_t>(npix, 1)) : spp;
     GND_CUDA(cudaEventRecord(e1, st));
     unsigned long long tot[8];
     GND_CUDA(cudaMemcpyAsync(tot, totals_.ptr, sizeof(tot), cudaMemcpyDeviceToHost, st));
-    std::vector<unsigned long long> fs((size_t)W * H * 4);
-    std::vector<float> fq((size_t)W * H * 3);
-    GND_CUDA(cudaMemcpyAsync(fs.data(), filmSum_.ptr, fs.size() * 8, cudaMemcpyDeviceToHost, st));
-    GND_CUDA(cudaMemcpyAsync(fq.data(), filmSq_.ptr, fq.size() * 4, cudaMemcpyDeviceToHost, st));
     GND_CUDA(cudaStreamSynchronize(st));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    for (size_t k = 0; k + 1 < evs.size(); k += 2) {
+    for (size_t k = 0; k + 1 < evs_.size(); k += 2) {
         float em = 0.f;
-        cudaEventElapsedTime(&em, evs[k], evs[k + 1]);
+        cudaEventElapsedTime(&em, evs_[k], evs_[k + 1]);
         res.extendMs += em;
-        cudaEventDestroy(evs[k]);
-        cudaEventDestroy(evs[k + 1]);
+        cudaEventDestroy(evs_[k]);
+        cudaEventDestroy(evs_[k + 1]);
     }
-    c->checkKernelErrors("render");
-    for (size_t q = 0; q < (size_t)W * H; ++q) {
-        for (int k = 0; k < 4; ++k) filmHost[q * 7 + k] += (float)((double)fs[q * 4 + k] / 16777216.0);
-        for (int k = 0; k < 3; ++k) filmHost[q * 7 + 4 + k] += fq[q * 3 + k];
+    evs_.clear();
+    try {
+        c->checkKernelErrors("render");
+    } catch (...) {
+        drop(j);
+        throw;
     }
+    finish(j, filmHost);
     res.paths = (int64_t)tot[2];
     res.rays = (int64_t)(tot[0] + tot[1]);
     res.extendRays = (int64_t)tot[0];
@@ -1027,10 +1278,11 @@ gnd_status gnd_gpu_render(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_render_p
         std::lock_guard<std::mutex> lk(c->mu);
         DeviceScene& ds = c->scene(id);
         gnd_render_params p{};
+        p.integrator = -1;
         if (prm) p = *prm;
         int spp = p.spp > 0 ? p.spp : ds.spp;
         int maxDepth = p.max_depth > 0 ? p.max_depth : ds.maxDepth;
-        int integ = p.integrator >= 0 && prm ? p.integrator : ds.integrator;
+        int integ = p.integrator >= 0 ? p.integrator : ds.integrator;
         if (integ != 0 && integ != 1) throw Error(GND_ERR_INVALID, "integrator must be 0 (path_gpu) or 1 (volpath_gpu)");
         if (maxDepth > 65535) maxDepth = 65535;
         if (!c->wave) c->wave = std::make_unique<Wavefront>(c);

@@ -58,28 +58,75 @@ struct JobDev {
 };
 
 // Queue counters (device): ints.
-enum QCounter : int { kQIn = 0, kQOut = 1, kQShadow = 2, kQDone = 3, kQFetchA = 4, kQFetchB = 5, kQCount = 8 };
+enum QCounter : int {
+    kQIn = 0, kQOut = 1, kQShadow = 2, kQDone = 3, kQFetchA = 4, kQFetchB = 5, kQFree = 6, kQFreeOut = 7,
+    kQActive = 8, kQClass0 = 16, kQCount = 32
+};
 
+// Per-job work control on the device.
+struct alignas(16) JobCtl {
+    unsigned long long next;      // next work item to hand out (may run past the end)
+    unsigned long long retired;   // finished samples
+};
+
+constexpr int kMaxJobs = 64;
+
+// Host record of an admitted job.
+struct HostJob {
+    bool used = false;
+    JobDev dev{};
+    uint64_t total = 0;           // work items (samples)
+    uint64_t released = 0;        // work items handed to the device so far (workEnd)
+    uint64_t retired = 0;         // last value read back
+    DevBuf filmSum, filmSq;
+    uint64_t bytes = 0;           // film bytes held in HBM
+};
+
+// The engine: one pool of path slots shared by every admitted job. Each iteration runs
+// extend, shade, shadow and retire on the active list; retire splats finished samples
+// and refills their slots (and idle slots) with work items of the active jobs, taken
+// round-robin in warp-sized grabs.
 class Wavefront {
 public:
     explicit Wavefront(Context* c);
     ~Wavefront();
-    // Renders jobs[0] (plain: one pass in flight at a time; batched: all passes share
-    // the slot pool and refill it). Returns paths and rays traced.
     struct Result {
         int64_t paths = 0, rays = 0, extendRays = 0, shadowRays = 0, extendNodes = 0, extendTris = 0, iterations = 0;
         int passesDone = 0;
         double ms = 0.0, extendMs = 0.0;
     };
+    // One job to completion: plain = one pass in flight (the pool is one pass and each
+    // pass is released when the previous retired), batched = all passes released at once.
     Result render(DeviceScene& ds, int spp, int firstPass, int maxDepth, int integrator, const int window[4],
                   bool batched, int profile, float* filmHost, gnd_progress_fn cb, void* user);
 
+    // ---- engine interface used by render() and by the server
+    void reset(size_t slots);                         // (re)initialise the pool: every slot idle
+    int admit(const DeviceScene& ds, int W, int H, int spp, int firstPass, int maxDepth, int integrator,
+              const int window[4], uint64_t releaseItems);
+    void release(int job, uint64_t upTo);             // hand out work items [.., upTo)
+    void finish(int job, float* filmHost);            // adds the film to filmHost, frees the job
+    void drop(int job);                               // frees the job without reading it
+    // Runs `iters` iterations; returns the number of paths in flight afterwards.
+    uint32_t step(int iters, int integratorMix, bool hasNull, int profile, Result& acc);
+    uint64_t retired(int job);                        // reads the job's retired count (sync)
+    void readRetired(std::vector<uint64_t>& out);     // all jobs (one copy, sync)
+    size_t capacity() const { return cap_; }
+    HostJob& job(int j) { return jobs_[j]; }
+    uint64_t jobBytes() const;
+
 private:
     void ensureCapacity(size_t slots);
+    void syncActive();
     Context* ctx_;
     size_t cap_ = 0;
-    DevBuf paths_, hits_, listA_, listB_, shadow_, done_, counters_, totals_, job_, workNext_;
-    DevBuf filmSum_, filmSq_;
+    int cur_ = 0;
+    uint32_t iter_ = 0;
+    DevBuf paths_, hits_, listA_, listB_, freeA_, freeB_, shadow_, done_, counters_, totals_, classes_;
+    DevBuf jobTab_, ctl_, active_;
+    HostJob jobs_[kMaxJobs];
+    std::vector<cudaEvent_t> evs_;
+    bool activeDirty_ = true;
 };
 
 }  // namespace gnd
