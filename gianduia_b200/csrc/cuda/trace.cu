@@ -1,5 +1,8 @@
 // Ray-batch queries: gnd_gpu_trace_closest / _any / _count (Scene::rayIntersect for a
 // batch). One thread per ray, persistent grid sized to the SM count.
+#include <mutex>
+#include <string>
+
 #include "runtime.h"
 #include "traverse.cuh"
 
@@ -101,6 +104,40 @@ void traceHost(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_ray* rays, int64_t 
 }
 }  // namespace
 
+// ---------------------------------------------------------------- allocation-free variant
+// Fixed device scratch of gnd_gpu_trace_closest_fixed: the persistent grid's fetch
+// counter (first 256 bytes; must be zero when the kernel starts, so every call clears
+// it), then the rays and the hits of one batch of at most kFixedMaxRays rays. It is a
+// module-scope array, one per device, shared by every context and thread of the
+// process on that device: calls that overlap in time on one device race on it.
+constexpr int64_t kFixedMaxRays = GND_TRACE_FIXED_MAX_RAYS;
+constexpr size_t kFixedCounterBytes = 256;
+constexpr size_t kFixedRayBytes = sizeof(gnd_ray) * (size_t)kFixedMaxRays;   // 2 MiB
+constexpr size_t kFixedHitBytes = sizeof(gnd_hit) * (size_t)kFixedMaxRays;   // 1.25 MiB
+static_assert(kFixedRayBytes % 256 == 0 && kFixedHitBytes % 256 == 0, "scratch regions stay 256-byte aligned");
+static __device__ __align__(256) unsigned char gFixedScratch[kFixedCounterBytes + kFixedRayBytes + kFixedHitBytes];
+
+namespace {
+constexpr int kFixedMaxDevices = 64;
+std::mutex gFixedMu;
+void* gFixedAddr[kFixedMaxDevices] = {};
+
+// Device address of gFixedScratch on the current device, looked up once per device. The
+// first lookup may load the module onto the device.
+unsigned char* fixedScratch(int device) {
+    if (device < 0 || device >= kFixedMaxDevices) throw Error(GND_ERR_INVALID, "device index out of range");
+    std::lock_guard<std::mutex> lk(gFixedMu);
+    if (!gFixedAddr[device]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, gFixedScratch);
+        if (e != cudaSuccess || !ptr)
+            throw Error(GND_ERR_CUDA, std::string("cudaGetSymbolAddress(fixed trace scratch): ") + cudaGetErrorString(e));
+        gFixedAddr[device] = ptr;
+    }
+    return static_cast<unsigned char*>(gFixedAddr[device]);
+}
+}  // namespace
+
 }  // namespace gnd
 
 using namespace gnd;
@@ -154,6 +191,39 @@ gnd_status gnd_gpu_trace_count_dev(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd
         std::lock_guard<std::mutex> lk(c->mu);
         cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
         launchTrace(c, c->scene(id), d_rays, n, nullptr, nullptr, d_nodes, d_tris, st);
+    });
+}
+
+// Closest hits of at most 65536 host-memory rays with no device allocation: rays, hits
+// and the fetch counter live in gFixedScratch. No counterpart in the reference.
+gnd_status gnd_gpu_trace_closest_fixed(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_ray* rays, int64_t n,
+                                       gnd_hit* hits) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (n < 0 || (n > 0 && (!rays || !hits))) throw Error(GND_ERR_INVALID, "bad ray batch arguments");
+        if (n > kFixedMaxRays)
+            throw Error(GND_ERR_INVALID, "gnd_gpu_trace_closest_fixed: " + std::to_string(n) +
+                                             " rays exceed the fixed scratch limit of " + std::to_string(kFixedMaxRays) +
+                                             " rays per call");
+        c->bind();
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceScene& ds = c->scene(id);
+        unsigned char* base = fixedScratch(c->device);
+        if (n == 0) return;
+        uint32_t* fetch = reinterpret_cast<uint32_t*>(base);
+        gnd_ray* dr = reinterpret_cast<gnd_ray*>(base + kFixedCounterBytes);
+        gnd_hit* dh = reinterpret_cast<gnd_hit*>(base + kFixedCounterBytes + kFixedRayBytes);
+        cudaStream_t st = c->stream;
+        GND_CUDA(cudaMemcpyAsync(dr, rays, sizeof(gnd_ray) * (size_t)n, cudaMemcpyHostToDevice, st));
+        GND_CUDA(cudaMemsetAsync(fetch, 0, sizeof(uint32_t), st));
+        int64_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
+        int g = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)c->numSMs * kTraceBlocksPerSM));
+        traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(ds.viewDev.as<SceneView>(), dr, (uint32_t)n, dh, nullptr,
+                                                             nullptr, nullptr, fetch, c->errWord.as<uint32_t>());
+        GND_CUDA(cudaGetLastError());
+        GND_CUDA(cudaMemcpyAsync(hits, dh, sizeof(gnd_hit) * (size_t)n, cudaMemcpyDeviceToHost, st));
+        GND_CUDA(cudaStreamSynchronize(st));
+        c->checkKernelErrors("trace_closest_fixed");
     });
 }
 

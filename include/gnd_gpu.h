@@ -145,6 +145,17 @@ gnd_status gnd_gpu_trace_any_dev(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd
  * and triangle tests, DEVICE buffers. Used for the roofline byte counts. */
 gnd_status gnd_gpu_trace_count_dev(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* d_rays, int64_t n,
                                    uint32_t* d_nodes, uint32_t* d_tris, void* stream);
+/* gnd_gpu_trace_closest without any device allocation. No counterpart in the reference.
+ * Rays, hits and the kernel's fetch counter live in a fixed module-scope device array
+ * (3.25 MiB per device), so n may be at most GND_TRACE_FIXED_MAX_RAYS; larger batches
+ * are rejected with GND_ERR_INVALID. Returns after the hits are in `hits` (HOST
+ * memory). The first call on a device looks the array up (cudaGetSymbolAddress), which
+ * may load the module; make that first call before any stream capture begins. The
+ * array is shared by every context of the process on the device: calls that overlap in
+ * time on one device race on it. */
+#define GND_TRACE_FIXED_MAX_RAYS 65536
+gnd_status gnd_gpu_trace_closest_fixed(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* rays, int64_t n,
+                                       gnd_hit* hits);
 
 /* ------------------------------------------------------------------ rendering */
 /* Progress callback, the reference's Integrator::setCallback / notifyUpdate
