@@ -159,6 +159,38 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def serve_leg(ctx, microfacet_sid, n_requests):
+    """The serving stream: requests over {Cornell box, microfacet grid, volumetric Cornell
+    box} with Poisson arrivals at 80% of the job server's measured capacity, served by the
+    job server and, for comparison, one at a time by plain renders in arrival order."""
+    import gianduia_b200 as G
+    from gianduia_b200 import scenes, serving
+    base = os.path.join(tempfile.gettempdir(), "gnd_bench_serve")
+    sids = {"microfacet": microfacet_sid,
+            "cornell": ctx.upload(G.HostScene.load_xml(scenes.cornell(os.path.join(base, "cornell")))),
+            "volumetric": ctx.upload(G.HostScene.load_xml(scenes.volumetric(os.path.join(base, "volumetric"))))}
+    integ = {"microfacet": 0, "cornell": 0, "volumetric": 1}
+    cap_rps, cap_sps = serving.calibrate_capacity(ctx, sids, integ)
+    rate = 0.8 * cap_rps
+    reqs = serving.make_requests(n_requests, seed=4)
+    arrivals = serving.poisson_arrivals(n_requests, rate, seed=4)
+    lat, makespan = serving.run_served(ctx, sids, integ, reqs, arrivals)
+    service = serving.run_plain_service(ctx, sids, integ, reqs)
+    plain_lat = serving.fifo_finish(arrivals, service) - arrivals
+    s, p = serving.latency_stats(lat), serving.latency_stats(plain_lat)
+    total = sum(serving.samples(r) for r in reqs)
+    for k in ("cornell", "volumetric"):
+        ctx.free_scene(sids[k])
+    log("serve: %d requests at %.2f req/s; p50 %.3f s p99 %.3f s (plain one at a time: p50 %.3f s p99 %.3f s)" % (
+        n_requests, rate, s["p50"], s["p99"], p["p50"], p["p99"]))
+    return {"requests": n_requests, "arrivals": "poisson, seed 4", "rate_rps": rate, "capacity_rps": cap_rps,
+            "capacity_mpaths_s": cap_sps / 1e6, "p50_s": s["p50"], "p99_s": s["p99"], "mean_s": s["mean"],
+            "plain_p50_s": p["p50"], "plain_p99_s": p["p99"], "plain_mean_s": p["mean"],
+            "p50_speedup": p["p50"] / s["p50"], "p99_speedup": p["p99"] / s["p99"],
+            "served_mpaths_s": total / makespan / 1e6, "plain_mpaths_s": total / float(service.sum()) / 1e6,
+            "note": "plain time-to-image from measured per-request render times through the FIFO recurrence"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -168,6 +200,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--plain", action="store_true", help="one pass in flight (no refill) for the timed steps")
+    ap.add_argument("--serve-requests", type=int, default=100,
+                    help="requests in the serving stream (the full stream is 2000); 0 skips it")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -277,7 +311,7 @@ def main():
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get("dram_bytes_per_launch")
-    launches_per_step = iters / len(stats) * 5 + spp
+    launches_total = sum(s["launches"] for s in stats)
     line = {
         "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
@@ -296,9 +330,11 @@ def main():
                      "launches": ext_launches, "ms_total": ext_ms, "peak_kind": peak_kind + " (copy bandwidth)"},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": int(scene_bytes),
                 "d2h_bytes_per_step": int(film_bytes)},
-        "gpu_launches": int(launches_per_step * args.steps),
+        "gpu_launches": int(launches_total),
         "clocks": clk,
     }
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        line["serve"] = serve_leg(ctx, sid, args.serve_requests)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(xml)
     if rank == 0:

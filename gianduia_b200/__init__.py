@@ -16,6 +16,10 @@ from . import build as _build
 __all__ = ["lib", "HostScene", "GpuContext", "GndError", "GpuUnavailable", "RAY_DTYPE", "HIT_DTYPE"]
 
 GND_OK = 0
+GND_ERR_INVALID = 1
+GND_ERR_TIMEOUT = 5
+GND_ERR_CANCELLED = 7
+GND_ERR_BUDGET = 8
 GND_ERR_NO_DEVICE = 9
 _STATUS = {1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "device check failed",
            5: "timeout", 6: "parse error", 7: "cancelled", 8: "over HBM budget", 9: "no CUDA device"}
@@ -65,6 +69,12 @@ def lib():
                 "gnd_gpu_trace_count_dev": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp, _vp, _vp],
                 "gnd_gpu_render": [_vp, ctypes.c_uint64, _vp, _vp, _vp],
                 "gnd_gpu_cancel": [_vp],
+                "gnd_gpu_trace_closest_fixed": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp],
+                "gnd_gpu_set_hbm_budget": [_vp, ctypes.c_uint64],
+                "gnd_gpu_serve_submit": [_vp, _vp, ctypes.POINTER(ctypes.c_uint64)],
+                "gnd_gpu_serve_poll": [_vp, ctypes.c_uint64, _vp],
+                "gnd_gpu_serve_wait": [_vp, ctypes.c_uint64, _vp, _vp, ctypes.c_int64],
+                "gnd_gpu_serve_cancel": [_vp, ctypes.c_uint64],
             }.items():
                 fn = getattr(L, name)
                 fn.argtypes = args
@@ -231,11 +241,13 @@ class GpuContext:
         _check(lib().gnd_gpu_trace_count_dev(self._h, sid, d_rays, n, d_nodes, d_tris, stream or None), "gnd_gpu_trace_count_dev")
 
     def render(self, sid, spp=0, first_pass=0, max_depth=0, integrator=-1, window=None, batched=False, film=None,
-               callback=None, profile=0):
+               callback=None, profile=0, width=0, height=0):
         """gnd_gpu_render: adds passes [first_pass, first_pass + spp) of the scene into
-        `film` (float32 [H, W, 7]: sum wL rgb, sum w, sum wL^2 rgb). Returns (film, stats)."""
+        `film` (float32 [H, W, 7]: sum wL rgb, sum w, sum wL^2 rgb). Returns (film, stats).
+        width / height override the scene file's film size."""
         hs = self._scenes[sid]
-        W, H = hs.width, hs.height
+        W = width if width > 0 else hs.width
+        H = height if height > 0 else hs.height
         if film is None:
             film = np.zeros((H, W, 7), np.float32)
         assert film.dtype == np.float32 and film.shape == (H, W, 7) and film.flags.c_contiguous
@@ -248,6 +260,8 @@ class GpuContext:
             p.window[:] = list(window)
         p.batched = 1 if batched else 0
         p.profile = profile
+        p.width = width
+        p.height = height
         cb = None
         if callback is not None:
             def _cb(user, s, fptr, w, h):
@@ -259,10 +273,55 @@ class GpuContext:
         _check(lib().gnd_gpu_render(self._h, sid, ctypes.byref(p), film.ctypes.data, ctypes.byref(st)), "gnd_gpu_render")
         return film, dict(paths=st.paths, rays=st.rays, passes=st.passes_done, ms=st.ms, extend_rays=st.extend_rays,
                           shadow_rays=st.shadow_rays, extend_nodes=st.extend_nodes, extend_tris=st.extend_tris,
-                          extend_ms=st.extend_ms, iterations=st.iterations)
+                          extend_ms=st.extend_ms, iterations=st.iterations, launches=st.launches)
 
     def cancel(self):
         _check(lib().gnd_gpu_cancel(self._h), "gnd_gpu_cancel")
+
+    # ---- serving (gnd_gpu_serve_*)
+    def set_hbm_budget(self, nbytes):
+        _check(lib().gnd_gpu_set_hbm_budget(self._h, int(nbytes)), "gnd_gpu_set_hbm_budget")
+
+    def submit(self, sid, width=0, height=0, spp=0, max_depth=0, integrator=-1, first_pass=0):
+        """Queues a render job; returns its id at once."""
+        d = JobDesc(scene=sid, width=width, height=height, spp=spp, max_depth=max_depth, integrator=integrator,
+                    first_pass=first_pass)
+        jid = ctypes.c_uint64()
+        _check(lib().gnd_gpu_serve_submit(self._h, ctypes.byref(d), ctypes.byref(jid)), "gnd_gpu_serve_submit")
+        w = width if width > 0 else self._scenes[sid].width
+        h = height if height > 0 else self._scenes[sid].height
+        self._jobs = getattr(self, "_jobs", {})
+        self._jobs[jid.value] = (h, w)
+        return jid.value
+
+    def poll(self, jid):
+        st = JobStatus()
+        _check(lib().gnd_gpu_serve_poll(self._h, jid, ctypes.byref(st)), "gnd_gpu_serve_poll")
+        return st.as_dict()
+
+    def wait(self, jid, timeout_ms=-1):
+        """Blocks until the job finishes; returns (film [H, W, 7], status dict). A cancelled
+        or failed job raises GndError; wait_any returns its status code instead."""
+        h, w = self._jobs[jid]
+        film = np.zeros((h, w, 7), np.float32)
+        st = JobStatus()
+        _check(lib().gnd_gpu_serve_wait(self._h, jid, film.ctypes.data, ctypes.byref(st), int(timeout_ms)),
+               "gnd_gpu_serve_wait")
+        del self._jobs[jid]
+        return film, st.as_dict()
+
+    def wait_any(self, jid, timeout_ms=-1):
+        """As wait, but returns (film, status, gnd_status) instead of raising."""
+        h, w = self._jobs[jid]
+        film = np.zeros((h, w, 7), np.float32)
+        st = JobStatus()
+        rc = lib().gnd_gpu_serve_wait(self._h, jid, film.ctypes.data, ctypes.byref(st), int(timeout_ms))
+        if rc != GND_ERR_TIMEOUT:
+            del self._jobs[jid]
+        return film, st.as_dict(), rc
+
+    def cancel_job(self, jid):
+        _check(lib().gnd_gpu_serve_cancel(self._h, jid), "gnd_gpu_serve_cancel")
 
 
 PROGRESS_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_float), ctypes.c_int32,
@@ -272,14 +331,35 @@ PROGRESS_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int32, ctypes.POI
 class RenderParams(ctypes.Structure):
     _fields_ = [("spp", ctypes.c_int32), ("first_pass", ctypes.c_int32), ("max_depth", ctypes.c_int32),
                 ("integrator", ctypes.c_int32), ("window", ctypes.c_int32 * 4), ("batched", ctypes.c_int32),
-                ("profile", ctypes.c_int32), ("callback", PROGRESS_FN), ("user", _vp)]
+                ("profile", ctypes.c_int32), ("callback", PROGRESS_FN), ("user", _vp), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32)]
 
 
 class RenderStats(ctypes.Structure):
     _fields_ = [("paths", ctypes.c_int64), ("rays", ctypes.c_int64), ("passes_done", ctypes.c_int32),
                 ("pad", ctypes.c_int32), ("ms", ctypes.c_double), ("extend_rays", ctypes.c_int64),
                 ("shadow_rays", ctypes.c_int64), ("extend_nodes", ctypes.c_int64), ("extend_tris", ctypes.c_int64),
-                ("extend_ms", ctypes.c_double), ("iterations", ctypes.c_int64)]
+                ("extend_ms", ctypes.c_double), ("iterations", ctypes.c_int64), ("launches", ctypes.c_int64)]
+
+
+class JobDesc(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_uint64), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
+                ("spp", ctypes.c_int32), ("max_depth", ctypes.c_int32), ("integrator", ctypes.c_int32),
+                ("first_pass", ctypes.c_int32)]
+
+
+JOB_STATES = {0: "queued", 1: "running", 2: "done", 3: "cancelled", 4: "failed"}
+
+
+class JobStatus(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("pad", ctypes.c_int32), ("samples_total", ctypes.c_int64),
+                ("samples_done", ctypes.c_int64), ("submit_ms", ctypes.c_double), ("admit_ms", ctypes.c_double),
+                ("done_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return dict(state=JOB_STATES.get(self.state, self.state), samples_total=self.samples_total,
+                    samples_done=self.samples_done, submit_ms=self.submit_ms, admit_ms=self.admit_ms,
+                    done_ms=self.done_ms)
 
 
 def resolve(film):

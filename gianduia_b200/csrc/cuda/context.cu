@@ -1,7 +1,9 @@
 // Contexts and resident scenes: gnd_gpu_create/destroy, gnd_gpu_scene_upload/free.
+#include <cmath>
 #include <cstring>
 
 #include "runtime.h"
+#include "server.h"
 #include "wavefront.h"
 
 namespace gnd {
@@ -14,6 +16,7 @@ const std::string& lastError() { return t_lastError; }
 
 Context::~Context() {
     if (device >= 0) cudaSetDevice(device);
+    server.reset();   // joins the serving thread before the engine goes away
     wave.reset();
     scenes.clear();
     errWord.release();
@@ -100,7 +103,10 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         // host-side validation of every reference stored in the tree (a corrupted index
         // is refused here rather than read out of bounds on the device)
         const Node4* nodes = reinterpret_cast<const Node4*>(d->nodes);
+        bool nanBounds = false;
         for (int64_t i = 0; i < d->num_nodes; ++i) {
+            for (const float* b : {nodes[i].lox, nodes[i].hix, nodes[i].loy, nodes[i].hiy, nodes[i].loz, nodes[i].hiz})
+                for (int k = 0; k < 4; ++k) nanBounds |= std::isnan(b[k]);
             for (int k = 0; k < 4; ++k) {
                 uint32_t r = nodes[i].child[k];
                 if (r == kEmpty) continue;
@@ -124,7 +130,7 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
             if (is[i].mediumIn >= d->num_media || is[i].mediumOut >= d->num_media) throw Error(GND_ERR_INVALID, "instance medium out of range");
         }
         c->bind();
-        std::lock_guard<std::mutex> lk(c->mu);
+        std::lock_guard<FairMutex> lk(c->mu);
         auto ds = std::make_unique<DeviceScene>();
         SceneView& v = ds->view;
         v.nodes = upload<Node4>(*ds, c->stream, d->nodes, d->num_nodes);
@@ -142,6 +148,7 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         v.tlasRoot = d->tlas_root;
         v.numEmitters = d->num_emitters;
         v.numInstances = d->num_instances;
+        v.fastBoxes = nanBounds ? 0 : 1;
         if (d->camera) std::memcpy(&v.camera, d->camera, sizeof(Camera));
         // null-BSDF mask per instance
         std::vector<uint8_t> mask(std::max(1, d->num_instances), 0);
@@ -169,7 +176,11 @@ gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctxh, gnd_scene_id id) {
     return guarded([&]() {
         Context* c = ctxOf(ctxh);
         c->bind();
-        std::lock_guard<std::mutex> lk(c->mu);
+        std::lock_guard<FairMutex> lk(c->mu);
+        auto use = c->sceneUse.find(id);
+        if (use != c->sceneUse.end() && use->second > 0)
+            throw Error(GND_ERR_INVALID, "scene " + std::to_string(id) + " is used by " + std::to_string(use->second) +
+                                             " queued or running job(s)");
         if (!c->scenes.erase(id)) throw Error(GND_ERR_INVALID, "unknown scene id");
     });
 }
@@ -177,7 +188,7 @@ gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctxh, gnd_scene_id id) {
 gnd_status gnd_gpu_scene_bytes(gnd_gpu_ctx* ctxh, gnd_scene_id id, uint64_t* bytes) {
     return guarded([&]() {
         Context* c = ctxOf(ctxh);
-        std::lock_guard<std::mutex> lk(c->mu);
+        std::lock_guard<FairMutex> lk(c->mu);
         *bytes = c->scene(id).bytes;
     });
 }

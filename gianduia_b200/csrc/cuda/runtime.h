@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <condition_variable>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -96,13 +97,36 @@ struct DeviceScene {
     int numMaterials = 0;
 };
 
+// First-come first-served mutex (ticket lock). The serving thread takes the context
+// again right after each round; with a plain std::mutex it can starve API calls (submit,
+// upload, free) that wait for the same context.
+class FairMutex {
+public:
+    void lock() {
+        std::unique_lock<std::mutex> lk(m_);
+        const uint64_t ticket = next_++;
+        cv_.wait(lk, [&]() { return serving_ == ticket; });
+    }
+    void unlock() {
+        std::lock_guard<std::mutex> lk(m_);
+        ++serving_;
+        cv_.notify_all();
+    }
+
+private:
+    std::mutex m_;
+    std::condition_variable cv_;
+    uint64_t next_ = 0, serving_ = 0;
+};
+
 class Wavefront;
+class Server;
 
 struct Context {
     int device = 0;
     int numSMs = 148;
     cudaStream_t stream = nullptr;
-    std::mutex mu;
+    FairMutex mu;   // serialises every use of the context (stream, scenes, engine)
     std::map<uint64_t, std::unique_ptr<DeviceScene>> scenes;
     uint64_t nextScene = 1;
     DevBuf errWord;           // device error bitmask written by kernels
@@ -120,6 +144,13 @@ struct Context {
     }
     std::unique_ptr<Wavefront> wave;
     volatile bool cancel = false;
+    // serving: HBM admission budget (0 = the device's free memory), queued or running
+    // jobs per scene (a scene in use cannot be freed), and the job server (created on
+    // the first submit; serverMu guards its creation)
+    uint64_t hbmBudget = 0;
+    std::map<uint64_t, int> sceneUse;
+    std::mutex serverMu;
+    std::unique_ptr<Server> server;
     ~Context();
     DeviceScene& scene(uint64_t id) {
         auto it = scenes.find(id);

@@ -1,0 +1,74 @@
+// Render-job serving on one context: submitted jobs (scene, film size, spp, depth,
+// integrator) are admitted first-come first-served into the wavefront engine's shared
+// pool of path slots while the job table and the HBM budget allow, and a host thread
+// steps the engine until each job's samples have all retired, then resolves its film to
+// host memory. Freed slots take the oldest admitted job's next samples, so the pool stays
+// full across job boundaries instead of draining at the end of every image.
+#pragma once
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "runtime.h"
+
+namespace gnd {
+
+struct ServeJob {
+    gnd_job_id id = 0;
+    uint64_t scene = 0;
+    int W = 0, H = 0, spp = 0, maxDepth = 0, integ = 0, firstPass = 0;
+    int state = GND_JOB_QUEUED;
+    int slot = -1;                   // engine job index while running
+    uint64_t total = 0, done = 0;
+    uint64_t filmBytes = 0;          // device film bytes while running
+    bool cancelReq = false;
+    int stopRound = -1;              // server round in which hand-out was stopped
+    double tSubmit = 0, tAdmit = 0, tDone = 0;
+    std::vector<float> film;         // H x W x 7 once finished
+    gnd_status status = GND_OK;
+    std::string error;
+};
+
+class Server {
+public:
+    static constexpr size_t kPoolSlots = size_t(1) << 22;   // 4M path slots (~1 GB)
+    static constexpr int kItersPerRound = 4;
+    static constexpr int64_t kStallIters = 20000;           // iterations without a retired sample
+
+    explicit Server(Context* c);
+    ~Server();
+    gnd_job_id submit(const gnd_job_desc& d);
+    void poll(gnd_job_id id, gnd_job_status* st);
+    gnd_status wait(gnd_job_id id, float* film, gnd_job_status* st, int64_t timeoutMs, std::string& err);
+    void cancel(gnd_job_id id);
+    uint64_t bytesInUseLocked() const;                       // caller holds the context mutex
+
+private:
+    void loop();
+    void fillStatus(const ServeJob& j, gnd_job_status* st) const;
+    double nowMs() const;
+    bool fitsLocked(const ServeJob& j) const;                // caller holds the context mutex
+    void finishJob(ServeJob* j, int state);
+    void failRunning(const std::string& why, gnd_status code);
+
+    Context* c_;
+    std::thread thread_;
+    std::mutex m_;                                           // guards the job records below
+    std::condition_variable workCv_, doneCv_;
+    std::deque<gnd_job_id> queue_;
+    std::unordered_map<gnd_job_id, std::unique_ptr<ServeJob>> jobs_;
+    std::vector<ServeJob*> running_;
+    gnd_job_id nextId_ = 1;
+    bool stop_ = false;
+    int round_ = 0;
+    int64_t itersSinceProgress_ = 0;
+    uint64_t lastRetiredSum_ = 0;
+    const std::chrono::steady_clock::time_point t0_;
+};
+
+}  // namespace gnd

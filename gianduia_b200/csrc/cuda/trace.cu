@@ -89,7 +89,7 @@ void traceHost(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_ray* rays, int64_t 
     Context* c = ctxOf(ctxh);
     if (n < 0 || (n > 0 && (!rays || (!hits && !occ)))) throw Error(GND_ERR_INVALID, "bad ray batch arguments");
     c->bind();
-    std::lock_guard<std::mutex> lk(c->mu);
+    std::lock_guard<FairMutex> lk(c->mu);
     DeviceScene& ds = c->scene(id);
     if (n == 0) return;
     size_t outBytes = hits ? sizeof(gnd_hit) * (size_t)n : (size_t)n;
@@ -164,7 +164,7 @@ gnd_status gnd_gpu_trace_closest_dev(gnd_gpu_ctx* ctxh, gnd_scene_id id, const g
         Context* c = ctxOf(ctxh);
         if (n < 0 || (n > 0 && (!d_rays || !d_hits))) throw Error(GND_ERR_INVALID, "bad ray batch arguments");
         c->bind();
-        std::lock_guard<std::mutex> lk(c->mu);
+        std::lock_guard<FairMutex> lk(c->mu);
         cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
         launchTrace(c, c->scene(id), d_rays, n, d_hits, nullptr, nullptr, nullptr, st);
     });
@@ -176,7 +176,7 @@ gnd_status gnd_gpu_trace_any_dev(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_r
         Context* c = ctxOf(ctxh);
         if (n < 0 || (n > 0 && (!d_rays || !d_occ))) throw Error(GND_ERR_INVALID, "bad ray batch arguments");
         c->bind();
-        std::lock_guard<std::mutex> lk(c->mu);
+        std::lock_guard<FairMutex> lk(c->mu);
         cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
         launchTrace(c, c->scene(id), d_rays, n, nullptr, d_occ, nullptr, nullptr, st);
     });
@@ -188,7 +188,7 @@ gnd_status gnd_gpu_trace_count_dev(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd
         Context* c = ctxOf(ctxh);
         if (n < 0 || (n > 0 && (!d_rays || !d_nodes || !d_tris))) throw Error(GND_ERR_INVALID, "bad ray batch arguments");
         c->bind();
-        std::lock_guard<std::mutex> lk(c->mu);
+        std::lock_guard<FairMutex> lk(c->mu);
         cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
         launchTrace(c, c->scene(id), d_rays, n, nullptr, nullptr, d_nodes, d_tris, st);
     });
@@ -206,7 +206,7 @@ gnd_status gnd_gpu_trace_closest_fixed(gnd_gpu_ctx* ctxh, gnd_scene_id id, const
                                              " rays exceed the fixed scratch limit of " + std::to_string(kFixedMaxRays) +
                                              " rays per call");
         c->bind();
-        std::lock_guard<std::mutex> lk(c->mu);
+        std::lock_guard<FairMutex> lk(c->mu);
         DeviceScene& ds = c->scene(id);
         unsigned char* base = fixedScratch(c->device);
         if (n == 0) return;

@@ -15,6 +15,7 @@
 // reference (pixel + pass * W * H), in one fixed draw order, so a path's result does
 // not depend on which slot, pass or launch carries it. The film is accumulated in
 // 2^-24 fixed point with integer atomics: sums are independent of completion order.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 
@@ -66,6 +67,7 @@ struct KParams {
     uint32_t* errWord;
     uint32_t capacity;
     uint32_t iter;                 // iteration number (round-robin start of job grabs)
+    uint32_t fifo;                 // 1: grabs walk the active list from the oldest job
 };
 
 // ---------------------------------------------------------------- surface interaction
@@ -836,7 +838,7 @@ __device__ __forceinline__ bool warpGrab(const KParams& p, bool want, uint32_t& 
     if (lane == leader) {
         const uint32_t na = p.cnt[kQActive];
         uint32_t remaining = (uint32_t)__popc(mask);
-        const uint32_t start = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5) + p.iter;
+        const uint32_t start = p.fifo ? 0u : blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5) + p.iter;
         int ns = 0;
         for (uint32_t t = 0; t < na && remaining > 0 && ns < 4; ++t) {
             uint32_t jid = p.active[(start + t) % na];
@@ -912,6 +914,16 @@ __global__ void kEndIter(uint32_t* cnt) {
     cnt[kQFree] = cnt[kQFreeOut];
 }
 
+// Fixed-point film -> float film [H*W][7] (sum wL rgb, sum w, sum wL^2 rgb).
+__global__ void kFilmResolve(const unsigned long long* __restrict__ sum, const float* __restrict__ sq, float* __restrict__ out,
+                             size_t npix) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npix; q += (size_t)gridDim.x * blockDim.x) {
+        float* o = out + q * 7;
+        for (int k = 0; k < 4; ++k) o[k] = (float)((double)sum[q * 4 + k] * (1.0 / 16777216.0));
+        for (int k = 0; k < 3; ++k) o[4 + k] = sq[q * 3 + k];
+    }
+}
+
 // Every slot idle: free list = [0, n).
 __global__ void kResetPool(uint32_t* freeList, uint32_t n, uint32_t* cnt) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) freeList[i] = i;
@@ -971,6 +983,7 @@ void Wavefront::reset(size_t slots) {
     cudaStream_t st = ctx_->stream;
     cur_ = 0;
     kResetPool<<<ctx_->numSMs * 4, 256, 0, st>>>(freeA_.as<uint32_t>(), (uint32_t)slots, counters_.as<uint32_t>());
+    ++launches_;
     GND_CUDA(cudaGetLastError());
     GND_CUDA(cudaMemsetAsync(totals_.ptr, 0, 8 * sizeof(unsigned long long), st));
 }
@@ -982,11 +995,18 @@ uint64_t Wavefront::jobBytes() const {
     return b;
 }
 
+bool Wavefront::busy() const {
+    for (const HostJob& j : jobs_)
+        if (j.used) return true;
+    return false;
+}
+
 void Wavefront::syncActive() {
     uint32_t ids[kMaxJobs];
     uint32_t n = 0;
     for (int j = 0; j < kMaxJobs; ++j)
         if (jobs_[j].used) ids[n++] = (uint32_t)j;
+    std::sort(ids, ids + n, [&](uint32_t a, uint32_t b) { return jobs_[a].seq < jobs_[b].seq; });
     cudaStream_t st = ctx_->stream;
     if (n) GND_CUDA(cudaMemcpyAsync(active_.ptr, ids, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     GND_CUDA(cudaMemcpyAsync(counters_.as<uint32_t>() + kQActive, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
@@ -1041,6 +1061,7 @@ int Wavefront::admit(const DeviceScene& ds, int W, int H, int spp, int firstPass
     jd.workBegin = 0;
     jd.workEnd = hj.released;
     hj.used = true;
+    hj.seq = seqNext_++;
     GND_CUDA(cudaMemcpyAsync(jobTab_.as<JobDev>() + j, &jd, sizeof(JobDev), cudaMemcpyHostToDevice, st));
     GND_CUDA(cudaMemsetAsync(ctl_.as<JobCtl>() + j, 0, sizeof(JobCtl), st));
     syncActive();
@@ -1073,6 +1094,34 @@ void Wavefront::readRetired(std::vector<uint64_t>& out) {
         out[j] = c[j].retired;
         if (jobs_[j].used) jobs_[j].retired = c[j].retired;
     }
+}
+
+void Wavefront::readCtl(std::vector<JobCtl>& out) {
+    out.resize(kMaxJobs);
+    GND_CUDA(cudaMemcpyAsync(out.data(), ctl_.ptr, kMaxJobs * sizeof(JobCtl), cudaMemcpyDeviceToHost, ctx_->stream));
+    GND_CUDA(cudaStreamSynchronize(ctx_->stream));
+    for (int j = 0; j < kMaxJobs; ++j)
+        if (jobs_[j].used) jobs_[j].retired = out[j].retired;
+}
+
+void Wavefront::stop(int j) {
+    HostJob& hj = jobs_[j];
+    hj.dev.workEnd = 0;
+    GND_CUDA(cudaMemsetAsync(&jobTab_.as<JobDev>()[j].workEnd, 0, sizeof(uint64_t), ctx_->stream));
+}
+
+void Wavefront::resolve(int j, float* filmHost) {
+    HostJob& hj = jobs_[j];
+    const size_t npix = (size_t)hj.dev.W * hj.dev.H;
+    filmOut_.ensure(npix * 7 * sizeof(float));
+    cudaStream_t st = ctx_->stream;
+    int grid = (int)std::min<size_t>((npix + 255) / 256, (size_t)ctx_->numSMs * 8);
+    kFilmResolve<<<std::max(grid, 1), 256, 0, st>>>(hj.filmSum.as<unsigned long long>(), hj.filmSq.as<float>(),
+                                                    filmOut_.as<float>(), npix);
+    ++launches_;
+    GND_CUDA(cudaGetLastError());
+    GND_CUDA(cudaMemcpyAsync(filmHost, filmOut_.ptr, npix * 7 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    GND_CUDA(cudaStreamSynchronize(st));
 }
 
 void Wavefront::finish(int j, float* filmHost) {
@@ -1117,6 +1166,7 @@ uint32_t Wavefront::step(int iters, int mix, bool hasNull, int profile, Result& 
     kp.active = active_.as<uint32_t>();
     kp.errWord = c->errWord.as<uint32_t>();
     kp.capacity = (uint32_t)cap_;
+    kp.fifo = fifo_ ? 1u : 0u;
     uint32_t* lists[2] = {listA_.as<uint32_t>(), listB_.as<uint32_t>()};
     uint32_t* frees[2] = {freeA_.as<uint32_t>(), freeB_.as<uint32_t>()};
     for (int it = 0; it < iters; ++it) {
@@ -1127,6 +1177,7 @@ uint32_t Wavefront::step(int iters, int mix, bool hasNull, int profile, Result& 
         kp.iter = iter_++;
         kBeginIter<<<1, 1, 0, st>>>(kp.cnt);
         acc.iterations++;
+        launches_ += 5 + (mix & 1 ? 6 : 0) + (mix & 2 ? 6 : 0);   // begin, extend, classify, retire, end; 5 shade + 1 shadow per integrator
         cudaEvent_t ea = nullptr, eb = nullptr;
         if (profile & 1) {
             GND_CUDA(cudaEventCreate(&ea));
@@ -1160,12 +1211,11 @@ uint32_t Wavefront::step(int iters, int mix, bool hasNull, int profile, Result& 
     return inflight;
 }
 
-Wavefront::Result Wavefront::render(DeviceScene& ds, int spp, int firstPass, int maxDepth, int integrator,
+Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int firstPass, int maxDepth, int integrator,
                                     const int window[4], bool batched, int profile, float* filmHost, gnd_progress_fn cb,
                                     void* user) {
     Context* c = ctx_;
     cudaStream_t st = c->stream;
-    const int W = ds.width, H = ds.height;
     int wx0 = 0, wy0 = 0, wx1 = W, wy1 = H;
     if (window && (window[0] | window[1] | window[2] | window[3])) {
         wx0 = window[0]; wy0 = window[1]; wx1 = window[2]; wy1 = window[3];
@@ -1179,6 +1229,7 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int spp, int firstPass, int
     const size_t slots = batched ? (size_t)std::min<uint64_t>(total, std::max<uint64_t>(npix, 1ull << 22)) : (size_t)npix;
     for (int j = 0; j < kMaxJobs; ++j)
         if (jobs_[j].used) throw Error(GND_ERR_INVALID, "the engine is serving jobs; render through the server");
+    const uint64_t launches0 = launches_;
     reset(slots);
     const int j = admit(ds, W, H, spp, firstPass, maxDepth, integrator, window, batched ? total : npix);
     const int mix = integrator == 1 ? 2 : 1;
@@ -1261,6 +1312,7 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int spp, int firstPass, int
     res.extendNodes = (int64_t)tot[3];
     res.extendTris = (int64_t)tot[4];
     res.ms = ms;
+    res.launches = (int64_t)(launches_ - launches0);
     return res;
 }
 
@@ -1275,7 +1327,7 @@ gnd_status gnd_gpu_render(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_render_p
         Context* c = ctxOf(ctxh);
         if (!film) throw Error(GND_ERR_INVALID, "null film buffer");
         c->bind();
-        std::lock_guard<std::mutex> lk(c->mu);
+        std::lock_guard<FairMutex> lk(c->mu);
         DeviceScene& ds = c->scene(id);
         gnd_render_params p{};
         p.integrator = -1;
@@ -1287,8 +1339,10 @@ gnd_status gnd_gpu_render(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_render_p
         if (maxDepth > 65535) maxDepth = 65535;
         if (!c->wave) c->wave = std::make_unique<Wavefront>(c);
         c->cancel = false;
-        Wavefront::Result r = c->wave->render(ds, spp, p.first_pass, maxDepth, integ, p.window, p.batched != 0, p.profile,
-                                              film, p.batched ? nullptr : p.callback, p.user);
+        const int W = p.width > 0 ? p.width : ds.width, H = p.height > 0 ? p.height : ds.height;
+        if ((uint64_t)W * (uint64_t)H > (1ull << 31)) throw Error(GND_ERR_INVALID, "film too large");
+        Wavefront::Result r = c->wave->render(ds, W, H, spp, p.first_pass, maxDepth, integ, p.window, p.batched != 0,
+                                              p.profile, film, p.batched ? nullptr : p.callback, p.user);
         if (stats) {
             stats->paths = r.paths;
             stats->rays = r.rays;
@@ -1300,6 +1354,7 @@ gnd_status gnd_gpu_render(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_render_p
             stats->extend_tris = r.extendTris;
             stats->extend_ms = r.extendMs;
             stats->iterations = r.iterations;
+            stats->launches = r.launches;
         }
         if (c->cancel && r.passesDone < spp) throw Error(GND_ERR_CANCELLED, "render cancelled");
     });

@@ -80,6 +80,7 @@ struct HostJob {
     uint64_t retired = 0;         // last value read back
     DevBuf filmSum, filmSq;
     uint64_t bytes = 0;           // film bytes held in HBM
+    uint64_t seq = 0;             // admission order (the FIFO hand-out order)
 };
 
 // The engine: one pool of path slots shared by every admitted job. Each iteration runs
@@ -92,13 +93,14 @@ public:
     ~Wavefront();
     struct Result {
         int64_t paths = 0, rays = 0, extendRays = 0, shadowRays = 0, extendNodes = 0, extendTris = 0, iterations = 0;
+        int64_t launches = 0;         // kernels launched
         int passesDone = 0;
         double ms = 0.0, extendMs = 0.0;
     };
     // One job to completion: plain = one pass in flight (the pool is one pass and each
     // pass is released when the previous retired), batched = all passes released at once.
-    Result render(DeviceScene& ds, int spp, int firstPass, int maxDepth, int integrator, const int window[4],
-                  bool batched, int profile, float* filmHost, gnd_progress_fn cb, void* user);
+    Result render(DeviceScene& ds, int W, int H, int spp, int firstPass, int maxDepth, int integrator,
+                  const int window[4], bool batched, int profile, float* filmHost, gnd_progress_fn cb, void* user);
 
     // ---- engine interface used by render() and by the server
     void reset(size_t slots);                         // (re)initialise the pool: every slot idle
@@ -106,12 +108,24 @@ public:
               const int window[4], uint64_t releaseItems);
     void release(int job, uint64_t upTo);             // hand out work items [.., upTo)
     void finish(int job, float* filmHost);            // adds the film to filmHost, frees the job
+    void resolve(int job, float* filmHost);           // writes the film (H x W x 7 floats) to filmHost
+    void stop(int job);                               // hands out no further work items of the job
     void drop(int job);                               // frees the job without reading it
     // Runs `iters` iterations; returns the number of paths in flight afterwards.
     uint32_t step(int iters, int integratorMix, bool hasNull, int profile, Result& acc);
     uint64_t retired(int job);                        // reads the job's retired count (sync)
     void readRetired(std::vector<uint64_t>& out);     // all jobs (one copy, sync)
+    void readCtl(std::vector<JobCtl>& out);           // all jobs' hand-out and retired counts (sync)
+    // Hand-out order: false = every warp starts at a different active job (even shares),
+    // true = oldest admitted job first (first-come first-served with the pool kept full).
+    void setFifo(bool fifo) { fifo_ = fifo; }
+    bool busy() const;                                // any job admitted
     size_t capacity() const { return cap_; }
+    // Device bytes of one path slot (state, hit, shadow record, lists) and of the pool.
+    static uint64_t slotBytes() {
+        return sizeof(PathState) + sizeof(HitRec) + sizeof(ShadowRec) + 5 * sizeof(uint32_t) + 10 * sizeof(uint32_t);
+    }
+    uint64_t poolBytes() const { return slotBytes() * cap_ + filmOut_.bytes; }
     HostJob& job(int j) { return jobs_[j]; }
     uint64_t jobBytes() const;
 
@@ -123,7 +137,10 @@ private:
     int cur_ = 0;
     uint32_t iter_ = 0;
     DevBuf paths_, hits_, listA_, listB_, freeA_, freeB_, shadow_, done_, counters_, totals_, classes_;
-    DevBuf jobTab_, ctl_, active_;
+    DevBuf jobTab_, ctl_, active_, filmOut_;
+    bool fifo_ = false;
+    uint64_t launches_ = 0;           // kernels launched by the engine so far
+    uint64_t seqNext_ = 0;
     HostJob jobs_[kMaxJobs];
     std::vector<cudaEvent_t> evs_;
     bool activeDirty_ = true;

@@ -4,6 +4,9 @@
                                                 micro-benchmark: 2^20 triangles, 2^22 rays
   python -m gianduia_b200.profile_run render    one 1-spp pass of the 1024x1024
                                                 microfacet render (path_gpu, depth 16)
+  python -m gianduia_b200.profile_run batched [spp]
+                                                the microfacet render in batched mode,
+                                                `spp` passes (default 1) sharing the pool
   python -m gianduia_b200.profile_run volpath   one 1-spp pass of the 512x512 volumetric
                                                 Cornell box (volpath_gpu, depth 32)
   python -m gianduia_b200.profile_run all       trace, then render
@@ -25,11 +28,11 @@ def run_trace(ctx):
     ctx.free_scene(sid)
 
 
-def run_render(ctx, batched=False):
+def run_render(ctx, batched=False, spp=1):
     xml = scenes.microfacet(os.path.join(tempfile.gettempdir(), "gnd_bench_microfacet_r0"), width=1024, height=1024,
                             spp=64, max_depth=16, grid=64, seed=2)
     sid = ctx.upload(G.HostScene.load_xml(xml))
-    _, st = ctx.render(sid, spp=1, batched=batched)
+    _, st = ctx.render(sid, spp=spp, batched=batched)
     print("render:", st)
     ctx.free_scene(sid)
 
@@ -51,7 +54,7 @@ def main(argv):
     if what in ("render", "all"):
         run_render(ctx)
     if what == "batched":
-        run_render(ctx, batched=True)
+        run_render(ctx, batched=True, spp=int(argv[2]) if len(argv) > 2 else 1)
     if what == "volpath":
         run_volpath(ctx)
     ctx.close()

@@ -175,6 +175,8 @@ typedef struct gnd_render_params {
                                  bit1: count BVH node visits / triangle tests in extend */
     gnd_progress_fn callback; /* optional (plain mode only) */
     void* user;
+    int32_t width, height;    /* film size; <= 0: the scene file's (the camera keeps its
+                                 field of view; the aspect ratio follows the film) */
 } gnd_render_params;
 
 typedef struct gnd_render_stats {
@@ -189,6 +191,7 @@ typedef struct gnd_render_stats {
     int64_t extend_tris;      /* profile bit1: triangle tests in extend */
     double extend_ms;         /* profile bit0: summed device time of the extend launches */
     int64_t iterations;       /* wavefront iterations (bounce steps) */
+    int64_t launches;         /* kernels the render launched */
 } gnd_render_stats;
 
 /* Integrator::render (integrator.h:49-155) for path_gpu / volpath_gpu: renders the
@@ -202,6 +205,56 @@ gnd_status gnd_gpu_render(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_render
 /* Integrator::cancel (integrator.h:22): asks a running gnd_gpu_render on this context
  * to stop after its current pass. Safe to call from another thread. */
 gnd_status gnd_gpu_cancel(gnd_gpu_ctx* ctx);
+
+/* ------------------------------------------------------------------ serving */
+/* A stream of render jobs on one context. No counterpart in the reference, whose
+ * Integrator::render renders one scene per call (integrator.h:49-155); each job renders
+ * exactly what gnd_gpu_render renders for the same arguments (same samples, same film
+ * sums), but jobs share one pool of path slots: they are admitted first-come
+ * first-served while the job table (64 running jobs) and the HBM budget allow, and the
+ * slots freed by finishing paths take the oldest running job's next samples. */
+typedef uint64_t gnd_job_id;
+
+typedef struct gnd_job_desc {
+    gnd_scene_id scene;
+    int32_t width, height;    /* film size; <= 0: the scene file's */
+    int32_t spp;              /* <= 0: the scene file's */
+    int32_t max_depth;        /* <= 0: the scene file's */
+    int32_t integrator;       /* -1: the scene file's; 0 path_gpu; 1 volpath_gpu */
+    int32_t first_pass;       /* sample index of the first pass (it keys the seeds) */
+} gnd_job_desc;
+
+enum { GND_JOB_QUEUED = 0, GND_JOB_RUNNING = 1, GND_JOB_DONE = 2, GND_JOB_CANCELLED = 3, GND_JOB_FAILED = 4 };
+
+typedef struct gnd_job_status {
+    int32_t state;            /* GND_JOB_* */
+    int32_t pad;
+    int64_t samples_total;    /* width * height * spp */
+    int64_t samples_done;     /* samples retired into the film */
+    double submit_ms;         /* host steady clock, ms since the server started */
+    double admit_ms;          /* 0 while queued */
+    double done_ms;           /* film resolved into host memory; 0 while unfinished */
+} gnd_job_status;
+
+/* HBM admission budget in bytes for the context (scenes + path pool + films of running
+ * jobs); 0 = no budget beyond the device's free memory. Jobs over budget wait in the
+ * queue; a job that cannot fit even alone is refused at submit with GND_ERR_BUDGET. */
+gnd_status gnd_gpu_set_hbm_budget(gnd_gpu_ctx* ctx, uint64_t bytes);
+/* Queues a job; returns at once with its id. The scene may not be freed while a job
+ * that names it is queued or running (gnd_gpu_scene_free fails with GND_ERR_INVALID). */
+gnd_status gnd_gpu_serve_submit(gnd_gpu_ctx* ctx, const gnd_job_desc* job, gnd_job_id* id);
+/* Current state of a job (does not block). */
+gnd_status gnd_gpu_serve_poll(gnd_gpu_ctx* ctx, gnd_job_id id, gnd_job_status* status);
+/* Blocks until the job has finished, copies its film (height x width x 7 floats, laid
+ * out as gnd_gpu_render's) into `film` (may be NULL) and releases the job id. Returns
+ * GND_ERR_CANCELLED for a cancelled job (with the samples that were retired) and the
+ * job's error for a failed one. timeout_ms < 0 waits without limit; when it runs out the
+ * call returns GND_ERR_TIMEOUT and the job stays valid. */
+gnd_status gnd_gpu_serve_wait(gnd_gpu_ctx* ctx, gnd_job_id id, float* film, gnd_job_status* status,
+                              int64_t timeout_ms);
+/* Asks a job to stop: a queued job is dropped, a running one hands out no further
+ * samples and finishes when its paths in flight have retired. */
+gnd_status gnd_gpu_serve_cancel(gnd_gpu_ctx* ctx, gnd_job_id id);
 
 #ifdef __cplusplus
 }
