@@ -159,6 +159,65 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def traversal_leg(ctx):
+    """The traversal micro-benchmark: 2^20 random triangles (one mesh, the host SAH BVH4),
+    2^24 random rays with tmax = inf, closest hit and any hit on device buffers, timed with
+    CUDA events on the launching stream (median of 5 after 2 warm-ups). Also measures the
+    read bandwidth of L2 (32 MiB buffer) and HBM (4 GiB buffer) for the roofline."""
+    import torch
+    import gianduia_b200 as G
+    from gianduia_b200 import scenes
+    n = 1 << 24
+    tri = scenes.random_triangles(1 << 20, seed=1)
+    rays = scenes.random_rays(n, seed=1)
+    hs = G.HostScene.from_triangles(tri)
+    sid = ctx.upload(hs)
+    dr = torch.from_numpy(rays).cuda()
+    dh = torch.empty((n, 5), dtype=torch.int32, device="cuda")
+    docc = torch.empty(n, dtype=torch.uint8, device="cuda")
+    strm = torch.cuda.Stream()
+    st = strm.cuda_stream
+    out = {"workload": "2^20 random triangles (centroids U[0,1]^3, vertex offsets N(0, 0.01^2)), 2^24 rays "
+                       "(origins U[-0.5,1.5]^3, uniform directions, tmax inf)"}
+    for name, fn in [("closest", lambda: ctx.trace_closest_dev(sid, dr.data_ptr(), n, dh.data_ptr(), st)),
+                     ("any", lambda: ctx.trace_any_dev(sid, dr.data_ptr(), n, docc.data_ptr(), st))]:
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(strm)
+            fn()
+            e1.record(strm)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = float(statistics.median(ts))
+        out[name + "_ms"] = ms
+        out[name + "_mrays_s"] = n / ms / 1e3
+    nodes = torch.zeros(n, dtype=torch.int32, device="cuda")
+    tris = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ctx.trace_count_dev(sid, dr.data_ptr(), n, nodes.data_ptr(), tris.data_ptr(), st)
+    torch.cuda.synchronize()
+    npr, tpr = float(nodes.double().sum()) / n, float(tris.double().sum()) / n
+    bytes_per_ray = npr * 128 + tpr * 48 + 32 + 20
+    achieved = bytes_per_ray * n / (out["closest_ms"] * 1e-3) / 1e9
+    l2 = max(ctx.read_bandwidth(32 << 20, 200), ctx.read_bandwidth(64 << 20, 100))
+    hbm = ctx.read_bandwidth(4 << 30, 3)
+    scene_bytes = ctx.scene_bytes(sid)
+    out.update({"nodes_per_ray": npr, "tris_per_ray": tpr, "bytes_per_ray": bytes_per_ray,
+                "closest_achieved_gbs": achieved, "l2_read_gbs": l2, "hbm_read_gbs": hbm,
+                "scene_bytes": scene_bytes, "frac_of_l2": achieved / l2, "frac_of_hbm": achieved / hbm,
+                "bound": "l2" if scene_bytes < 100e6 else "hbm",
+                "hit_frac": float((dh[:, 3] >= 0).float().mean().item())})
+    ctx.free_scene(sid)
+    del dr, dh, docc, nodes, tris
+    torch.cuda.empty_cache()
+    log("traversal: closest %.0f Mrays/s, any %.0f Mrays/s; %.1f nodes %.1f tris per ray; %.0f GB/s = %.2f of L2 %.0f GB/s" % (
+        out["closest_mrays_s"], out["any_mrays_s"], npr, tpr, achieved, achieved / l2, l2))
+    return out
+
+
 def serve_leg(ctx, microfacet_sid, n_requests):
     """The serving stream: requests over {Cornell box, microfacet grid, volumetric Cornell
     box} with Poisson arrivals at 80% of the job server's measured capacity, served by the
@@ -170,23 +229,30 @@ def serve_leg(ctx, microfacet_sid, n_requests):
             "cornell": ctx.upload(G.HostScene.load_xml(scenes.cornell(os.path.join(base, "cornell")))),
             "volumetric": ctx.upload(G.HostScene.load_xml(scenes.volumetric(os.path.join(base, "volumetric"))))}
     integ = {"microfacet": 0, "cornell": 0, "volumetric": 1}
+    ctx.set_hbm_budget(150 * 10**9)   # the stream's HBM admission budget
     cap_rps, cap_sps = serving.calibrate_capacity(ctx, sids, integ)
     rate = 0.8 * cap_rps
     reqs = serving.make_requests(n_requests, seed=4)
     arrivals = serving.poisson_arrivals(n_requests, rate, seed=4)
+    ctx.serve_policy("fifo")
+    lat_fifo, _ = serving.run_served(ctx, sids, integ, reqs, arrivals)
+    ctx.serve_policy("srpt")
     lat, makespan = serving.run_served(ctx, sids, integ, reqs, arrivals)
     service = serving.run_plain_service(ctx, sids, integ, reqs)
     plain_lat = serving.fifo_finish(arrivals, service) - arrivals
     s, p = serving.latency_stats(lat), serving.latency_stats(plain_lat)
+    f = serving.latency_stats(lat_fifo)
     total = sum(serving.samples(r) for r in reqs)
     for k in ("cornell", "volumetric"):
         ctx.free_scene(sids[k])
     log("serve: %d requests at %.2f req/s; p50 %.3f s p99 %.3f s (plain one at a time: p50 %.3f s p99 %.3f s)" % (
         n_requests, rate, s["p50"], s["p99"], p["p50"], p["p99"]))
-    return {"requests": n_requests, "arrivals": "poisson, seed 4", "rate_rps": rate, "capacity_rps": cap_rps,
+    return {"requests": n_requests, "arrivals": "poisson, seed 4", "policy": "srpt (fewest samples left first)",
+            "rate_rps": rate, "capacity_rps": cap_rps,
             "capacity_mpaths_s": cap_sps / 1e6, "p50_s": s["p50"], "p99_s": s["p99"], "mean_s": s["mean"],
             "plain_p50_s": p["p50"], "plain_p99_s": p["p99"], "plain_mean_s": p["mean"],
             "p50_speedup": p["p50"] / s["p50"], "p99_speedup": p["p99"] / s["p99"],
+            "fifo_p50_s": f["p50"], "fifo_p99_s": f["p99"],
             "served_mpaths_s": total / makespan / 1e6, "plain_mpaths_s": total / float(service.sum()) / 1e6,
             "note": "plain time-to-image from measured per-request render times through the FIFO recurrence"}
 
@@ -200,6 +266,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--plain", action="store_true", help="one pass in flight (no refill) for the timed steps")
+    ap.add_argument("--no-traversal", action="store_true", help="skip the traversal micro-benchmark")
     ap.add_argument("--serve-requests", type=int, default=100,
                     help="requests in the serving stream (the full stream is 2000); 0 skips it")
     args = ap.parse_args()
@@ -228,8 +295,9 @@ def main():
     ctx = G.GpuContext(local)
     sid = ctx.upload(hs)
     scene_bytes = ctx.scene_bytes(sid)
+    from gianduia_b200.sharding import pass_range, reduce_film
     spp = WORKLOAD["spp"]
-    first = rank * spp
+    first, _ = pass_range(rank, world, spp)
     npix = WORKLOAD["width"] * WORKLOAD["height"]
 
     # traversal work of the extend kernel (instrumented run on the same paths)
@@ -256,8 +324,7 @@ def main():
     for k in range(args.steps):
         film, st = ctx.render(sid, spp=spp, first_pass=first, profile=1, batched=batched)
         if dist:
-            ft = torch.from_numpy(film).cuda()
-            dist.reduce(ft, dst=0)
+            reduce_film(torch.from_numpy(film).cuda(), dist)
         stats.append(st)
     barrier()
     wall = time.perf_counter() - t0
@@ -284,8 +351,7 @@ def main():
         sid2 = ctx.upload(hs)
         film, st = ctx.render(sid2, spp=spp, first_pass=first, batched=batched)
         if dist:
-            ft = torch.from_numpy(film).cuda()
-            dist.reduce(ft, dst=0)
+            reduce_film(torch.from_numpy(film).cuda(), dist)
         ctx.free_scene(sid2)
         barrier()
         e2e_times.append(time.perf_counter() - t)
@@ -333,6 +399,8 @@ def main():
         "gpu_launches": int(launches_total),
         "clocks": clk,
     }
+    if rank == 0 and world == 1 and not args.no_traversal:
+        line["traversal"] = traversal_leg(ctx)
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serve"] = serve_leg(ctx, sid, args.serve_requests)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

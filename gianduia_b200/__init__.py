@@ -75,6 +75,8 @@ def lib():
                 "gnd_gpu_serve_poll": [_vp, ctypes.c_uint64, _vp],
                 "gnd_gpu_serve_wait": [_vp, ctypes.c_uint64, _vp, _vp, ctypes.c_int64],
                 "gnd_gpu_serve_cancel": [_vp, ctypes.c_uint64],
+                "gnd_gpu_serve_policy": [_vp, ctypes.c_int32],
+                "gnd_gpu_read_bandwidth": [_vp, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)],
             }.items():
                 fn = getattr(L, name)
                 fn.argtypes = args
@@ -279,6 +281,17 @@ class GpuContext:
         _check(lib().gnd_gpu_cancel(self._h), "gnd_gpu_cancel")
 
     # ---- serving (gnd_gpu_serve_*)
+    def read_bandwidth(self, nbytes, reps):
+        """GB/s of L2-cached 16-byte loads streaming a buffer of nbytes, reps times."""
+        g = ctypes.c_double()
+        _check(lib().gnd_gpu_read_bandwidth(self._h, int(nbytes), int(reps), ctypes.byref(g)), "gnd_gpu_read_bandwidth")
+        return g.value
+
+    def serve_policy(self, policy):
+        """'srpt' (fewest samples left first, the default) or 'fifo' (oldest job first)."""
+        code = {"fifo": 0, "srpt": 1}[policy]
+        _check(lib().gnd_gpu_serve_policy(self._h, code), "gnd_gpu_serve_policy")
+
     def set_hbm_budget(self, nbytes):
         _check(lib().gnd_gpu_set_hbm_budget(self._h, int(nbytes)), "gnd_gpu_set_hbm_budget")
 

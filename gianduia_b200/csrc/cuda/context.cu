@@ -103,10 +103,17 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         // host-side validation of every reference stored in the tree (a corrupted index
         // is refused here rather than read out of bounds on the device)
         const Node4* nodes = reinterpret_cast<const Node4*>(d->nodes);
-        bool nanBounds = false;
+        bool nanBounds = false;   // true: the traversal keeps the exact slab arithmetic
         for (int64_t i = 0; i < d->num_nodes; ++i) {
-            for (const float* b : {nodes[i].lox, nodes[i].hix, nodes[i].loy, nodes[i].hiy, nodes[i].loz, nodes[i].hiz})
-                for (int k = 0; k < 4; ++k) nanBounds |= std::isnan(b[k]);
+            // the fast slab test needs bounds without NaN and lo <= hi on every non-empty child
+            for (int k = 0; k < 4; ++k) {
+                const float lo[3] = {nodes[i].lox[k], nodes[i].loy[k], nodes[i].loz[k]};
+                const float hi[3] = {nodes[i].hix[k], nodes[i].hiy[k], nodes[i].hiz[k]};
+                for (int a = 0; a < 3; ++a) {
+                    nanBounds |= std::isnan(lo[a]) || std::isnan(hi[a]);
+                    if (nodes[i].child[k] != kEmpty) nanBounds |= !(lo[a] <= hi[a]);
+                }
+            }
             for (int k = 0; k < 4; ++k) {
                 uint32_t r = nodes[i].child[k];
                 if (r == kEmpty) continue;

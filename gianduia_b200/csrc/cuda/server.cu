@@ -296,6 +296,18 @@ void Server::loop() {
                     finishJob(j, GND_JOB_DONE);
                 }
             }
+            if (policy_ == GND_SERVE_SRPT) {
+                // hand out the samples of the job with the fewest samples left to hand out
+                std::vector<std::pair<int, uint64_t>> keys;
+                {
+                    std::lock_guard<std::mutex> lk(m_);
+                    for (ServeJob* j : running_) {
+                        const uint64_t handed = std::min<uint64_t>(ctl[j->slot].next, j->total);
+                        keys.emplace_back(j->slot, j->total - handed);
+                    }
+                }
+                wf.setPriorities(keys);
+            }
             if (retiredSum != lastRetiredSum_) {
                 lastRetiredSum_ = retiredSum;
                 itersSinceProgress_ = 0;
@@ -309,6 +321,12 @@ void Server::loop() {
             failRunning(e.what(), GND_ERR_CUDA);
         }
     }
+}
+
+void Server::setPolicy(int policy) {
+    if (policy != GND_SERVE_FIFO && policy != GND_SERVE_SRPT) throw Error(GND_ERR_INVALID, "unknown serving policy");
+    std::lock_guard<std::mutex> lk(m_);
+    policy_ = policy;
 }
 
 Server& serverOf(Context* c) {
@@ -327,6 +345,15 @@ gnd_status gnd_gpu_set_hbm_budget(gnd_gpu_ctx* ctxh, uint64_t bytes) {
         Context* c = ctxOf(ctxh);
         std::lock_guard<FairMutex> lk(c->mu);
         c->hbmBudget = bytes;
+    });
+}
+
+gnd_status gnd_gpu_serve_policy(gnd_gpu_ctx* ctxh, int32_t policy) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        c->bind();
+        std::lock_guard<std::mutex> lk(c->serverMu);
+        serverOf(c).setPolicy(policy);
     });
 }
 

@@ -47,6 +47,7 @@ public:
     gnd_status wait(gnd_job_id id, float* film, gnd_job_status* st, int64_t timeoutMs, std::string& err);
     void cancel(gnd_job_id id);
     uint64_t bytesInUseLocked() const;                       // caller holds the context mutex
+    void setPolicy(int policy);                              // GND_SERVE_*
 
 private:
     void loop();
@@ -66,6 +67,7 @@ private:
     gnd_job_id nextId_ = 1;
     bool stop_ = false;
     int round_ = 0;
+    int policy_ = GND_SERVE_SRPT;
     int64_t itersSinceProgress_ = 0;
     uint64_t lastRetiredSum_ = 0;
     const std::chrono::steady_clock::time_point t0_;

@@ -274,6 +274,8 @@ struct Trav {
     float wtmin, tmin, tmax, bestT;
     int curInst;
     int sp;
+    bool fast, wfast;   // current / world ray: nodeKeysFast applies (see there)
+    uint32_t next;      // entry to visit next without a stack round trip, kEmpty when none
     uint32_t leaf;      // pending leaf reference, kEmpty when none
     uint32_t leafK;     // next primitive of the pending leaf
     THit hit;
@@ -290,27 +292,112 @@ struct TStack {
     __device__ __forceinline__ uint32_t get(int k) const { return k < kSmemStack ? smem[k * BLOCK] : local[k - kSmemStack]; }
 };
 
+// True when (bound - o) * inv cannot be NaN for any finite or infinite node bound: the
+// origin is finite and every inverse direction component is finite and non-zero.
+__device__ __forceinline__ bool slabFinite(const SceneView& s, V3 o, V3 inv) {
+    const bool f = isfinite(o.x) && isfinite(o.y) && isfinite(o.z) && isfinite(inv.x) && isfinite(inv.y) &&
+                   isfinite(inv.z) && inv.x != 0.0f && inv.y != 0.0f && inv.z != 0.0f;
+    return s.fastBoxes && f;
+}
+
 __device__ __forceinline__ void travInit(Trav& t, const SceneView& s, const TRay& ray) {
     t.wo = ray.o; t.wd = ray.d;
     t.o = ray.o; t.d = ray.d;
     t.inv = v3(__frcp_rn(ray.d.x), __frcp_rn(ray.d.y), __frcp_rn(ray.d.z));
+    t.fast = t.wfast = slabFinite(s, t.o, t.inv) && !isnan(ray.tmin) && !isnan(ray.tmax);
     t.wtmin = ray.tmin; t.tmin = ray.tmin; t.tmax = ray.tmax;
     t.bestT = 3.402823466e38f;
     t.curInst = -1;
     t.leaf = kEmpty;
     t.leafK = 0;
+    t.next = kEmpty;
     t.hit.t = INFINITY; t.hit.u = t.hit.v = 0.f; t.hit.inst = -1; t.hit.slot = 0xFFFFFFFFu;
     t.sp = 0;
+}
+
+// Visit-order key of a hit child: the entry distance's bits with the child slot in the
+// two lowest bits, so that unsigned comparison orders children nearest first (distances
+// within 3 ulp fall back to slot order; a negative distance, possible only with a
+// negative tMin, sorts by magnitude). Order affects only which of several hits at
+// exactly equal t is reported, never whether or where a hit is found.
+constexpr uint32_t kMissKey = 0xFFFFFFFFu;
+__device__ __forceinline__ uint32_t packKey(float a, int slot) {
+    return (__float_as_uint(a) & 0x7FFFFFFCu) | (uint32_t)slot;
+}
+
+// Child entry distances of one node for the current ray (bvhTraversal.h:57-72) as visit
+// keys; kMissKey for a missed or empty child. nodeKeysExact is the reference's lane arithmetic with
+// SSE min/max (the second operand when either is NaN), for any ray and any bounds.
+__device__ __forceinline__ void nodeKeysExact(const Node4* nd, const Trav& t, const uint32_t ref[4], uint32_t key[4]) {
+    float4 lx = ldg4(nd->lox), hx = ldg4(nd->hix);
+    float t1[4] = {(lx.x - t.o.x) * t.inv.x, (lx.y - t.o.x) * t.inv.x, (lx.z - t.o.x) * t.inv.x, (lx.w - t.o.x) * t.inv.x};
+    float t2[4] = {(hx.x - t.o.x) * t.inv.x, (hx.y - t.o.x) * t.inv.x, (hx.z - t.o.x) * t.inv.x, (hx.w - t.o.x) * t.inv.x};
+    float tn[4], tf[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { tn[i] = lmin(t1[i], t2[i]); tf[i] = lmax(t1[i], t2[i]); }
+    float4 ly = ldg4(nd->loy), hy = ldg4(nd->hiy);
+    float u1[4] = {(ly.x - t.o.y) * t.inv.y, (ly.y - t.o.y) * t.inv.y, (ly.z - t.o.y) * t.inv.y, (ly.w - t.o.y) * t.inv.y};
+    float u2[4] = {(hy.x - t.o.y) * t.inv.y, (hy.y - t.o.y) * t.inv.y, (hy.z - t.o.y) * t.inv.y, (hy.w - t.o.y) * t.inv.y};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        tn[i] = lmax(tn[i], lmin(u1[i], u2[i]));
+        tf[i] = lmin(tf[i], lmax(u1[i], u2[i]));
+    }
+    float4 lz = ldg4(nd->loz), hz = ldg4(nd->hiz);
+    float w1[4] = {(lz.x - t.o.z) * t.inv.z, (lz.y - t.o.z) * t.inv.z, (lz.z - t.o.z) * t.inv.z, (lz.w - t.o.z) * t.inv.z};
+    float w2[4] = {(hz.x - t.o.z) * t.inv.z, (hz.y - t.o.z) * t.inv.z, (hz.z - t.o.z) * t.inv.z, (hz.w - t.o.z) * t.inv.z};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        // bvhTraversal.h:69-72: max(max(x, y), max(z, tMin)) <= min(min(x, y), min(z, tMax))
+        float a = lmax(tn[i], lmax(lmin(w1[i], w2[i]), t.tmin));
+        float b = lmin(tf[i], lmin(lmax(w1[i], w2[i]), t.tmax));
+        key[i] = (a <= b && ref[i] != kEmpty) ? packKey(a, i) : kMissKey;
+    }
+}
+
+// The same distances with less work, for rays and nodes where it gives the same values
+// (t.fast: finite origin, finite non-zero inverse direction; fastBoxes: no NaN bound and
+// lo <= hi for every non-empty child). Then no slab term is NaN, so min/max are the
+// hardware ones, and because (bound - o) * inv is monotone in the bound, the smaller of
+// the two planes of an axis is the lo plane when inv > 0 and the hi plane when inv < 0:
+// the near and far planes are chosen once per axis from the direction's sign instead of
+// by a min/max per child. Empty children (ref kEmpty) are discarded as before. The
+// result may differ from nodeKeysExact only in the sign of a zero key, which no
+// comparison sees.
+__device__ __forceinline__ void nodeKeysFast(const Node4* nd, const Trav& t, const uint32_t ref[4], uint32_t key[4]) {
+    const bool sx = t.inv.x < 0.0f, sy = t.inv.y < 0.0f, sz = t.inv.z < 0.0f;
+    const float4 nx = ldg4(sx ? nd->hix : nd->lox), fx = ldg4(sx ? nd->lox : nd->hix);
+    const float4 ny = ldg4(sy ? nd->hiy : nd->loy), fy = ldg4(sy ? nd->loy : nd->hiy);
+    const float4 nz = ldg4(sz ? nd->hiz : nd->loz), fz = ldg4(sz ? nd->loz : nd->hiz);
+    const float n0[4] = {nx.x, nx.y, nx.z, nx.w}, f0[4] = {fx.x, fx.y, fx.z, fx.w};
+    const float n1[4] = {ny.x, ny.y, ny.z, ny.w}, f1[4] = {fy.x, fy.y, fy.z, fy.w};
+    const float n2[4] = {nz.x, nz.y, nz.z, nz.w}, f2[4] = {fz.x, fz.y, fz.z, fz.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float tnx = (n0[i] - t.o.x) * t.inv.x, tfx = (f0[i] - t.o.x) * t.inv.x;
+        const float tny = (n1[i] - t.o.y) * t.inv.y, tfy = (f1[i] - t.o.y) * t.inv.y;
+        const float tnz = (n2[i] - t.o.z) * t.inv.z, tfz = (f2[i] - t.o.z) * t.inv.z;
+        const float a = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, t.tmin));
+        const float b = fminf(fminf(tfx, tfy), fminf(tfz, t.tmax));
+        key[i] = (a <= b && ref[i] != kEmpty) ? packKey(a, i) : kMissKey;
+    }
 }
 
 // Pops one entry: restores the world ray at a sentinel, tests an inner node and pushes its
 // hit children nearest-last, or makes a leaf pending. Returns an error bitmask.
 template <int BLOCK, bool COUNT>
 __device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<BLOCK>& st, TraceCounters* cnt) {
-    uint32_t e = st.get(--t.sp);
+    uint32_t e;
+    if (t.next != kEmpty) {
+        e = t.next;
+        t.next = kEmpty;
+    } else {
+        e = st.get(--t.sp);
+    }
     if (e == kSentinel) {
         t.o = t.wo; t.d = t.wd;
         t.inv = v3(__frcp_rn(t.wd.x), __frcp_rn(t.wd.y), __frcp_rn(t.wd.z));
+        t.fast = t.wfast;
         t.tmin = t.wtmin;
         t.curInst = -1;
         return 0;
@@ -322,46 +409,30 @@ __device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<
     }
     const Node4* nd = s.nodes + e;
     if (COUNT) cnt->nodes++;
-    float key[4];
-    uint4 ch = ldgu4(nd->child);
-    uint32_t ref[4] = {ch.x, ch.y, ch.z, ch.w};
+    uint32_t key[4];
     {
-        float4 lx = ldg4(nd->lox), hx = ldg4(nd->hix);
-        float t1[4] = {(lx.x - t.o.x) * t.inv.x, (lx.y - t.o.x) * t.inv.x, (lx.z - t.o.x) * t.inv.x, (lx.w - t.o.x) * t.inv.x};
-        float t2[4] = {(hx.x - t.o.x) * t.inv.x, (hx.y - t.o.x) * t.inv.x, (hx.z - t.o.x) * t.inv.x, (hx.w - t.o.x) * t.inv.x};
-        float tn[4], tf[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) { tn[i] = lmin(t1[i], t2[i]); tf[i] = lmax(t1[i], t2[i]); }
-        float4 ly = ldg4(nd->loy), hy = ldg4(nd->hiy);
-        float u1[4] = {(ly.x - t.o.y) * t.inv.y, (ly.y - t.o.y) * t.inv.y, (ly.z - t.o.y) * t.inv.y, (ly.w - t.o.y) * t.inv.y};
-        float u2[4] = {(hy.x - t.o.y) * t.inv.y, (hy.y - t.o.y) * t.inv.y, (hy.z - t.o.y) * t.inv.y, (hy.w - t.o.y) * t.inv.y};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) { tn[i] = lmax(tn[i], lmin(u1[i], u2[i])); tf[i] = lmin(tf[i], lmax(u1[i], u2[i])); }
-        float4 lz = ldg4(nd->loz), hz = ldg4(nd->hiz);
-        float w1[4] = {(lz.x - t.o.z) * t.inv.z, (lz.y - t.o.z) * t.inv.z, (lz.z - t.o.z) * t.inv.z, (lz.w - t.o.z) * t.inv.z};
-        float w2[4] = {(hz.x - t.o.z) * t.inv.z, (hz.y - t.o.z) * t.inv.z, (hz.z - t.o.z) * t.inv.z, (hz.w - t.o.z) * t.inv.z};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            // bvhTraversal.h:69-72: max(max(x, y), max(z, tMin)) <= min(min(x, y), min(z, tMax))
-            float a = lmax(tn[i], lmax(lmin(w1[i], w2[i]), t.tmin));
-            float b = lmin(tf[i], lmin(lmax(w1[i], w2[i]), t.tmax));
-            key[i] = (a <= b && ref[i] != kEmpty) ? a : INFINITY;
-        }
+        const uint4 ch = ldgu4(nd->child);
+        const uint32_t ref[4] = {ch.x, ch.y, ch.z, ch.w};
+        if (t.fast) nodeKeysFast(nd, t, ref, key);
+        else nodeKeysExact(nd, t, ref, key);
     }
-#define GND_CSWAP(a, b)                                                          \
-    if (key[b] < key[a]) {                                                       \
-        float tk = key[a]; key[a] = key[b]; key[b] = tk;                         \
-        uint32_t tr = ref[a]; ref[a] = ref[b]; ref[b] = tr;                      \
+    // ascending sort network on the packed keys (unsigned min / max)
+#define GND_CSWAP(a, b)                                     \
+    {                                                       \
+        const uint32_t lo = min(key[a], key[b]);            \
+        key[b] = max(key[a], key[b]);                       \
+        key[a] = lo;                                        \
     }
     GND_CSWAP(0, 1) GND_CSWAP(2, 3) GND_CSWAP(0, 2) GND_CSWAP(1, 3) GND_CSWAP(1, 2)
 #undef GND_CSWAP
+    if (key[0] == kMissKey) return 0;
+    const int npush = (key[1] != kMissKey) + (key[2] != kMissKey) + (key[3] != kMissKey);
+    if (t.sp + npush > kPStackMax) return kTraceStackOverflow;
+    // farther children on the stack (farthest deepest), the nearest visited next
 #pragma unroll
-    for (int i = 3; i >= 0; --i) {
-        if (key[i] != INFINITY) {
-            if (t.sp >= kPStackMax) return kTraceStackOverflow;
-            st.put(t.sp++, ref[i]);
-        }
-    }
+    for (int i = 3; i >= 1; --i)
+        if (key[i] != kMissKey) st.put(t.sp++, __ldg(nd->child + (key[i] & 3u)));
+    t.next = __ldg(nd->child + (key[0] & 3u));
     return 0;
 }
 
@@ -382,7 +453,7 @@ __device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<
             t.hit.t = tt; t.hit.u = u; t.hit.v = v;
             t.hit.inst = t.curInst;
             t.hit.slot = first + k;
-            if (ANY) { t.sp = 0; t.leaf = kEmpty; }
+            if (ANY) { t.sp = 0; t.leaf = kEmpty; t.next = kEmpty; }
         }
         return 0;
     }
@@ -408,11 +479,12 @@ __device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<
             st.put(t.sp++, makeLeaf(first + k + 1, count - k - 1));
             t.leaf = kEmpty;
         }
-        if (t.sp + 2 > kPStackMax) return kTraceStackOverflow;
+        if (t.sp + 1 > kPStackMax) return kTraceStackOverflow;
         st.put(t.sp++, kSentinel);
-        st.put(t.sp++, root);
+        t.next = root;   // the bottom-level root is visited next
         t.o = lo; t.d = ld;
         t.inv = v3(__frcp_rn(ld.x), __frcp_rn(ld.y), __frcp_rn(ld.z));
+        t.fast = t.wfast && slabFinite(s, lo, t.inv);
         t.tmin = kEpsilon;
         t.curInst = (int)id;
         return 0;
@@ -427,7 +499,7 @@ __device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<
         t.hit.t = th; t.hit.u = 0.f; t.hit.v = 0.f;
         t.hit.inst = (int)id;
         t.hit.slot = 0xFFFFFFFFu;
-        if (ANY) { t.sp = 0; t.leaf = kEmpty; }
+        if (ANY) { t.sp = 0; t.leaf = kEmpty; t.next = kEmpty; }
     }
     return 0;
 }
@@ -473,7 +545,7 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
             // a source may decline an item (it belongs to another kernel of the launch)
             if (src.load(idx, r, sv, nm)) {
                 travInit(t, *sv, r);
-                if (sv->tlasRoot != kEmpty) { st.put(0, sv->tlasRoot); t.sp = 1; }
+                t.next = sv->tlasRoot;   // kEmpty for a scene without primitives
                 active = true;
                 iter = 0;
             }
@@ -481,11 +553,14 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
         if (!__any_sync(0xffffffffu, active)) break;
         // node phase
         for (;;) {
-            bool want = active && t.leaf == kEmpty && t.sp > 0;
+            bool want = active && t.leaf == kEmpty && (t.next != kEmpty || t.sp > 0);
             if (!__any_sync(0xffffffffu, want)) break;
             if (want) {
                 int e = travNodeStep<BLOCK, COUNT>(t, *sv, st, cnt);
-                if (e || ++iter > kMaxIterations) { err |= e ? e : (int)kTraceIterLimit; t.sp = 0; t.leaf = kEmpty; }
+                if (e || ++iter > kMaxIterations) {
+                    err |= e ? e : (int)kTraceIterLimit;
+                    t.sp = 0; t.leaf = kEmpty; t.next = kEmpty;
+                }
             }
         }
         // leaf phase
@@ -494,10 +569,10 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
             if (!__any_sync(0xffffffffu, want)) break;
             if (want) {
                 int e = travLeafStep<BLOCK, ANY, COUNT>(t, *sv, st, cnt, nm);
-                if (e) { err |= e; t.sp = 0; t.leaf = kEmpty; }
+                if (e) { err |= e; t.sp = 0; t.leaf = kEmpty; t.next = kEmpty; }
             }
         }
-        if (active && t.sp == 0 && t.leaf == kEmpty) {
+        if (active && t.sp == 0 && t.leaf == kEmpty && t.next == kEmpty) {
             src.store(idx, t.hit);
             active = false;
         }

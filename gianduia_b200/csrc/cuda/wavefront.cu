@@ -66,8 +66,7 @@ struct KParams {
     uint32_t* freeOut;
     uint32_t* errWord;
     uint32_t capacity;
-    uint32_t iter;                 // iteration number (round-robin start of job grabs)
-    uint32_t fifo;                 // 1: grabs walk the active list from the oldest job
+    uint32_t fifo;                 // 1: grabs walk the active list from its first job
 };
 
 // ---------------------------------------------------------------- surface interaction
@@ -371,6 +370,7 @@ __global__ void kBeginIter(uint32_t* cnt) {
     cnt[kQFetchA] = 0;
     cnt[kQFetchB] = 0;
     cnt[kQFreeOut] = 0;
+    cnt[kQIter] += 1;   // iteration number: round-robin start of the job grabs
     for (int k = 0; k < kShadeClasses; ++k) cnt[kQClass0 + k] = 0;
 }
 
@@ -838,7 +838,7 @@ __device__ __forceinline__ bool warpGrab(const KParams& p, bool want, uint32_t& 
     if (lane == leader) {
         const uint32_t na = p.cnt[kQActive];
         uint32_t remaining = (uint32_t)__popc(mask);
-        const uint32_t start = p.fifo ? 0u : blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5) + p.iter;
+        const uint32_t start = p.fifo ? 0u : blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5) + p.cnt[kQIter];
         int ns = 0;
         for (uint32_t t = 0; t < na && remaining > 0 && ns < 4; ++t) {
             uint32_t jid = p.active[(start + t) % na];
@@ -959,13 +959,21 @@ Wavefront::Wavefront(Context* c) : ctx_(c) {
     ctl_.alloc(kMaxJobs * sizeof(JobCtl));
     active_.alloc(kMaxJobs * sizeof(uint32_t));
     GND_CUDA(cudaMemset(ctl_.ptr, 0, kMaxJobs * sizeof(JobCtl)));
+    GND_CUDA(cudaMallocHost(&snaps_, 2 * sizeof(Snapshot)));
+    std::memset(snaps_, 0, 2 * sizeof(Snapshot));
+    for (cudaEvent_t& e : snapEv_) GND_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 }
 Wavefront::~Wavefront() {
     for (cudaEvent_t e : evs_) cudaEventDestroy(e);
+    clearGraphs();
+    for (cudaEvent_t e : snapEv_)
+        if (e) cudaEventDestroy(e);
+    if (snaps_) cudaFreeHost(snaps_);
 }
 
 void Wavefront::ensureCapacity(size_t slots) {
     if (slots <= cap_) return;
+    clearGraphs();   // the captured launches hold the old buffers
     paths_.alloc(slots * sizeof(PathState));
     hits_.alloc(slots * sizeof(HitRec));
     listA_.alloc(slots * sizeof(uint32_t));
@@ -995,6 +1003,22 @@ uint64_t Wavefront::jobBytes() const {
     return b;
 }
 
+void Wavefront::setPriorities(const std::vector<std::pair<int, uint64_t>>& keys) {
+    auto order = [&]() {
+        std::vector<int> ids;
+        for (int j = 0; j < kMaxJobs; ++j)
+            if (jobs_[j].used) ids.push_back(j);
+        std::sort(ids.begin(), ids.end(), [&](int a, int b) {
+            return jobs_[a].prio != jobs_[b].prio ? jobs_[a].prio < jobs_[b].prio : jobs_[a].seq < jobs_[b].seq;
+        });
+        return ids;
+    };
+    const std::vector<int> before = order();
+    for (const auto& k : keys)
+        if (k.first >= 0 && k.first < kMaxJobs && jobs_[k.first].used) jobs_[k.first].prio = k.second;
+    if (order() != before) syncActive();
+}
+
 bool Wavefront::busy() const {
     for (const HostJob& j : jobs_)
         if (j.used) return true;
@@ -1006,7 +1030,9 @@ void Wavefront::syncActive() {
     uint32_t n = 0;
     for (int j = 0; j < kMaxJobs; ++j)
         if (jobs_[j].used) ids[n++] = (uint32_t)j;
-    std::sort(ids, ids + n, [&](uint32_t a, uint32_t b) { return jobs_[a].seq < jobs_[b].seq; });
+    std::sort(ids, ids + n, [&](uint32_t a, uint32_t b) {
+        return jobs_[a].prio != jobs_[b].prio ? jobs_[a].prio < jobs_[b].prio : jobs_[a].seq < jobs_[b].seq;
+    });
     cudaStream_t st = ctx_->stream;
     if (n) GND_CUDA(cudaMemcpyAsync(active_.ptr, ids, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     GND_CUDA(cudaMemcpyAsync(counters_.as<uint32_t>() + kQActive, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
@@ -1062,6 +1088,7 @@ int Wavefront::admit(const DeviceScene& ds, int W, int H, int spp, int firstPass
     jd.workEnd = hj.released;
     hj.used = true;
     hj.seq = seqNext_++;
+    hj.prio = hj.seq;
     GND_CUDA(cudaMemcpyAsync(jobTab_.as<JobDev>() + j, &jd, sizeof(JobDev), cudaMemcpyHostToDevice, st));
     GND_CUDA(cudaMemsetAsync(ctl_.as<JobCtl>() + j, 0, sizeof(JobCtl), st));
     syncActive();
@@ -1126,17 +1153,11 @@ void Wavefront::resolve(int j, float* filmHost) {
 
 void Wavefront::finish(int j, float* filmHost) {
     HostJob& hj = jobs_[j];
-    const size_t npix = (size_t)hj.dev.W * hj.dev.H;
-    std::vector<unsigned long long> fs(npix * 4);
-    std::vector<float> fq(npix * 3);
-    GND_CUDA(cudaMemcpyAsync(fs.data(), hj.filmSum.ptr, fs.size() * 8, cudaMemcpyDeviceToHost, ctx_->stream));
-    GND_CUDA(cudaMemcpyAsync(fq.data(), hj.filmSq.ptr, fq.size() * 4, cudaMemcpyDeviceToHost, ctx_->stream));
-    GND_CUDA(cudaStreamSynchronize(ctx_->stream));
+    const size_t n = (size_t)hj.dev.W * hj.dev.H * 7;
     if (filmHost) {
-        for (size_t q = 0; q < npix; ++q) {
-            for (int k = 0; k < 4; ++k) filmHost[q * 7 + k] += (float)((double)fs[q * 4 + k] / 16777216.0);
-            for (int k = 0; k < 3; ++k) filmHost[q * 7 + 4 + k] += fq[q * 3 + k];
-        }
+        std::vector<float> f(n);
+        resolve(j, f.data());
+        for (size_t q = 0; q < n; ++q) filmHost[q] += f[q];
     }
     drop(j);
 }
@@ -1150,10 +1171,86 @@ void Wavefront::drop(int j) {
     syncActive();
 }
 
+void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int profile, cudaStream_t st) {
+    const int grid = ctx_->numSMs * 8;
+    uint32_t* lists[2] = {listA_.as<uint32_t>(), listB_.as<uint32_t>()};
+    uint32_t* frees[2] = {freeA_.as<uint32_t>(), freeB_.as<uint32_t>()};
+    kp.listIn = lists[par];
+    kp.listOut = lists[par ^ 1];
+    kp.freeIn = frees[par];
+    kp.freeOut = frees[par ^ 1];
+    kBeginIter<<<1, 1, 0, st>>>(kp.cnt);
+    cudaEvent_t ea = nullptr, eb = nullptr;
+    if (profile & 1) {
+        GND_CUDA(cudaEventCreate(&ea));
+        GND_CUDA(cudaEventCreate(&eb));
+        GND_CUDA(cudaEventRecord(ea, st));
+    }
+    if (profile & 2) kExtend<true><<<grid, kBlock, 0, st>>>(kp);
+    else kExtend<false><<<grid, kBlock, 0, st>>>(kp);
+    if (profile & 1) {
+        GND_CUDA(cudaEventRecord(eb, st));
+        evs_.push_back(ea);
+        evs_.push_back(eb);
+    }
+    uint32_t* cls = classes_.as<uint32_t>();
+    kClassify<<<grid, kBlock, 0, st>>>(kp, cls);
+    if (mix & 1) launchShade<false>(kp, cls, grid, st);
+    if (mix & 2) launchShade<true>(kp, cls, grid, st);
+    if (mix & 1) {
+        if (hasNull) kShadowPath<false><<<grid, kBlock, 0, st>>>(kp, mix == 3);
+        else kShadowPath<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
+    }
+    if (mix & 2) kShadow<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
+    kRetire<<<grid, kBlock, 0, st>>>(kp);
+    kEndIter<<<1, 1, 0, st>>>(kp.cnt);
+    GND_CUDA(cudaGetLastError());
+}
+
+void Wavefront::clearGraphs() {
+    for (GraphEntry& g : graphs_) cudaGraphExecDestroy(g.exec);
+    graphs_.clear();
+}
+
+cudaGraphExec_t Wavefront::pairGraph(const KParams& kp, int par, int mix, bool hasNull, cudaStream_t st) {
+    const bool fifo = kp.fifo != 0;
+    for (const GraphEntry& g : graphs_)
+        if (g.par == par && g.mix == mix && g.hasNull == hasNull && g.fifo == fifo) return g.exec;
+    cudaGraph_t graph = nullptr;
+    GND_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+        enqueueIteration(kp, par, mix, hasNull, 0, st);
+        enqueueIteration(kp, par ^ 1, mix, hasNull, 0, st);
+    } catch (...) {
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    GND_CUDA(cudaStreamEndCapture(st, &graph));
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) throw Error(GND_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    graphs_.push_back(GraphEntry{par, mix, hasNull, fifo, exec});
+    return exec;
+}
+
 uint32_t Wavefront::step(int iters, int mix, bool hasNull, int profile, Result& acc) {
+    enqueueRound(iters, mix, hasNull, profile, acc, 0);
+    const Snapshot& sn = waitRound(0);
+    for (int j = 0; j < kMaxJobs; ++j)
+        if (jobs_[j].used) jobs_[j].retired = sn.ctl[j].retired;
+    return sn.inflight;
+}
+
+const Wavefront::Snapshot& Wavefront::waitRound(int slot) {
+    GND_CUDA(cudaEventSynchronize(snapEv_[slot]));
+    return snaps_[slot];
+}
+
+void Wavefront::enqueueRound(int iters, int mix, bool hasNull, int profile, Result& acc, int slot) {
     Context* c = ctx_;
     cudaStream_t st = c->stream;
-    const int grid = c->numSMs * 8;
     KParams kp{};
     kp.jobs = jobTab_.as<JobDev>();
     kp.paths = paths_.as<PathState>();
@@ -1167,48 +1264,26 @@ uint32_t Wavefront::step(int iters, int mix, bool hasNull, int profile, Result& 
     kp.errWord = c->errWord.as<uint32_t>();
     kp.capacity = (uint32_t)cap_;
     kp.fifo = fifo_ ? 1u : 0u;
-    uint32_t* lists[2] = {listA_.as<uint32_t>(), listB_.as<uint32_t>()};
-    uint32_t* frees[2] = {freeA_.as<uint32_t>(), freeB_.as<uint32_t>()};
-    for (int it = 0; it < iters; ++it) {
-        kp.listIn = lists[cur_];
-        kp.listOut = lists[cur_ ^ 1];
-        kp.freeIn = frees[cur_];
-        kp.freeOut = frees[cur_ ^ 1];
-        kp.iter = iter_++;
-        kBeginIter<<<1, 1, 0, st>>>(kp.cnt);
-        acc.iterations++;
-        launches_ += 5 + (mix & 1 ? 6 : 0) + (mix & 2 ? 6 : 0);   // begin, extend, classify, retire, end; 5 shade + 1 shadow per integrator
-        cudaEvent_t ea = nullptr, eb = nullptr;
-        if (profile & 1) {
-            GND_CUDA(cudaEventCreate(&ea));
-            GND_CUDA(cudaEventCreate(&eb));
-            GND_CUDA(cudaEventRecord(ea, st));
+    // begin, extend, classify, retire, end; 5 shade kernels + 1 shadow kernel per integrator
+    const int perIter = 5 + (mix & 1 ? 6 : 0) + (mix & 2 ? 6 : 0);
+    int it = 0;
+    while (it < iters) {
+        if (useGraphs_ && profile == 0 && iters - it >= 2) {
+            GND_CUDA(cudaGraphLaunch(pairGraph(kp, cur_, mix, hasNull, st), st));
+            it += 2;
+            acc.iterations += 2;
+            launches_ += 2 * perIter;
+        } else {
+            enqueueIteration(kp, cur_, mix, hasNull, profile, st);
+            cur_ ^= 1;
+            ++it;
+            acc.iterations++;
+            launches_ += perIter;
         }
-        if (profile & 2) kExtend<true><<<grid, kBlock, 0, st>>>(kp);
-        else kExtend<false><<<grid, kBlock, 0, st>>>(kp);
-        if (profile & 1) {
-            GND_CUDA(cudaEventRecord(eb, st));
-            evs_.push_back(ea);
-            evs_.push_back(eb);
-        }
-        uint32_t* cls = classes_.as<uint32_t>();
-        kClassify<<<grid, kBlock, 0, st>>>(kp, cls);
-        if (mix & 1) launchShade<false>(kp, cls, grid, st);
-        if (mix & 2) launchShade<true>(kp, cls, grid, st);
-        if (mix & 1) {
-            if (hasNull) kShadowPath<false><<<grid, kBlock, 0, st>>>(kp, mix == 3);
-            else kShadowPath<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
-        }
-        if (mix & 2) kShadow<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
-        kRetire<<<grid, kBlock, 0, st>>>(kp);
-        kEndIter<<<1, 1, 0, st>>>(kp.cnt);
-        GND_CUDA(cudaGetLastError());
-        cur_ ^= 1;
     }
-    uint32_t inflight = 0;
-    GND_CUDA(cudaMemcpyAsync(&inflight, kp.cnt + kQIn, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    GND_CUDA(cudaStreamSynchronize(st));
-    return inflight;
+    GND_CUDA(cudaMemcpyAsync(&snaps_[slot].inflight, kp.cnt + kQIn, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GND_CUDA(cudaMemcpyAsync(snaps_[slot].ctl, ctl_.ptr, kMaxJobs * sizeof(JobCtl), cudaMemcpyDeviceToHost, st));
+    GND_CUDA(cudaEventRecord(snapEv_[slot], st));
 }
 
 Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int firstPass, int maxDepth, int integrator,
@@ -1238,11 +1313,35 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
     GND_CUDA(cudaEventCreate(&e1));
     GND_CUDA(cudaEventRecord(e0, st));
     int pass = 0;
-    const int itersPerStep = batched ? 4 : 2;
+    const int itersPerStep = 2;
     const int64_t iterCap = (int64_t)(maxDepth + 110) * (spp + 2) * 4 + 4096;
     bool cancelled = false;
     try {
-        for (;;) {
+        if (batched) {
+            // every work item is released: rounds of kRoundIters iterations, one queued
+            // ahead of the one whose counters the host is reading
+            constexpr int kRoundIters = 8;
+            int64_t k = 0, stopAt = -1;
+            enqueueRound(kRoundIters, mix, ds.hasNullMaterials, profile, res, 0);
+            for (;;) {
+                enqueueRound(kRoundIters, mix, ds.hasNullMaterials, profile, res, (int)((k + 1) & 1));
+                const Snapshot& sn = waitRound((int)(k & 1));
+                const uint64_t r = sn.ctl[j].retired;
+                const uint32_t inflight = sn.inflight;
+                if (r >= total && inflight == 0) break;
+                // after a cancel, only rounds queued after the stop show the final state
+                if (cancelled && k > stopAt && inflight == 0) break;
+                if (c->cancel && !cancelled) {
+                    stop(j);            // queued behind round k + 1
+                    stopAt = k + 1;
+                    cancelled = true;
+                }
+                if (res.iterations > iterCap) throw Error(GND_ERR_DEVICE_CHECK, "path iteration limit reached");
+                ++k;
+            }
+            GND_CUDA(cudaStreamSynchronize(st));   // the round queued ahead has nothing left to do
+        }
+        while (!batched) {
             uint32_t inflight = step(itersPerStep, mix, ds.hasNullMaterials, profile, res);
             uint64_t r = retired(j);
             if (!batched) {
@@ -1266,12 +1365,6 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
                     if (pass < spp && !c->cancel) release(j, (uint64_t)(pass + 1) * npix);
                 }
                 if (c->cancel && !cancelled) cancelled = true;
-            } else if (c->cancel && !cancelled) {
-                // stop handing out work; let the paths in flight finish
-                release(j, std::max<uint64_t>(jobs_[j].released, 0));
-                jobs_[j].dev.workEnd = 0;
-                GND_CUDA(cudaMemsetAsync(&jobTab_.as<JobDev>()[j].workEnd, 0, sizeof(uint64_t), st));
-                cancelled = true;
             }
             if (r >= total && inflight == 0) break;
             if (cancelled && inflight == 0) break;

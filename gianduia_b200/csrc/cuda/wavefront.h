@@ -60,7 +60,7 @@ struct JobDev {
 // Queue counters (device): ints.
 enum QCounter : int {
     kQIn = 0, kQOut = 1, kQShadow = 2, kQDone = 3, kQFetchA = 4, kQFetchB = 5, kQFree = 6, kQFreeOut = 7,
-    kQActive = 8, kQClass0 = 16, kQCount = 32
+    kQActive = 8, kQIter = 9, kQClass0 = 16, kQCount = 32
 };
 
 // Per-job work control on the device.
@@ -80,13 +80,16 @@ struct HostJob {
     uint64_t retired = 0;         // last value read back
     DevBuf filmSum, filmSq;
     uint64_t bytes = 0;           // film bytes held in HBM
-    uint64_t seq = 0;             // admission order (the FIFO hand-out order)
+    uint64_t seq = 0;             // admission order
+    uint64_t prio = 0;            // hand-out order key: lower first, ties by admission
 };
 
 // The engine: one pool of path slots shared by every admitted job. Each iteration runs
 // extend, shade, shadow and retire on the active list; retire splats finished samples
 // and refills their slots (and idle slots) with work items of the active jobs, taken
 // round-robin in warp-sized grabs.
+struct KParams;
+
 class Wavefront {
 public:
     explicit Wavefront(Context* c);
@@ -113,13 +116,28 @@ public:
     void drop(int job);                               // frees the job without reading it
     // Runs `iters` iterations; returns the number of paths in flight afterwards.
     uint32_t step(int iters, int integratorMix, bool hasNull, int profile, Result& acc);
+    // Pipelined rounds: enqueueRound queues `iters` iterations followed by an
+    // asynchronous copy of the queue and job counters into pinned snapshot `slot` (0/1);
+    // waitRound blocks until that snapshot has landed. Queueing round k+1 before waiting
+    // for round k keeps the GPU busy while the host reads the counters.
+    struct alignas(16) Snapshot {
+        uint32_t inflight;            // active paths after the round
+        uint32_t pad[3];
+        JobCtl ctl[kMaxJobs];         // per job: work items handed out, samples retired
+    };
+    void enqueueRound(int iters, int integratorMix, bool hasNull, int profile, Result& acc, int slot);
+    const Snapshot& waitRound(int slot);
     uint64_t retired(int job);                        // reads the job's retired count (sync)
     void readRetired(std::vector<uint64_t>& out);     // all jobs (one copy, sync)
     void readCtl(std::vector<JobCtl>& out);           // all jobs' hand-out and retired counts (sync)
     // Hand-out order: false = every warp starts at a different active job (even shares),
     // true = oldest admitted job first (first-come first-served with the pool kept full).
     void setFifo(bool fifo) { fifo_ = fifo; }
+    // Sets the hand-out order keys of the admitted jobs (index -> key) and updates the
+    // device's active list when the order changed.
+    void setPriorities(const std::vector<std::pair<int, uint64_t>>& keys);
     bool busy() const;                                // any job admitted
+    void setGraphs(bool on) { useGraphs_ = on; }      // replay the per-bounce loop as CUDA graphs
     size_t capacity() const { return cap_; }
     // Device bytes of one path slot (state, hit, shadow record, lists) and of the pool.
     static uint64_t slotBytes() {
@@ -132,12 +150,27 @@ public:
 private:
     void ensureCapacity(size_t slots);
     void syncActive();
+    // One wavefront iteration on the stream for the lists of parity `par`.
+    void enqueueIteration(KParams kp, int par, int mix, bool hasNull, int profile, cudaStream_t st);
+    // Executable graph of two iterations (parity restored) for these settings, captured on
+    // first use; the per-iteration state it needs (queue counters, iteration number) is
+    // in device memory, so one capture serves every later replay.
+    cudaGraphExec_t pairGraph(const KParams& kp, int par, int mix, bool hasNull, cudaStream_t st);
+    void clearGraphs();
+    struct GraphEntry {
+        int par, mix;
+        bool hasNull, fifo;
+        cudaGraphExec_t exec;
+    };
+    std::vector<GraphEntry> graphs_;
+    bool useGraphs_ = true;
     Context* ctx_;
     size_t cap_ = 0;
     int cur_ = 0;
-    uint32_t iter_ = 0;
     DevBuf paths_, hits_, listA_, listB_, freeA_, freeB_, shadow_, done_, counters_, totals_, classes_;
     DevBuf jobTab_, ctl_, active_, filmOut_;
+    Snapshot* snaps_ = nullptr;       // pinned host memory, two slots
+    cudaEvent_t snapEv_[2] = {nullptr, nullptr};
     bool fifo_ = false;
     uint64_t launches_ = 0;           // kernels launched by the engine so far
     uint64_t seqNext_ = 0;

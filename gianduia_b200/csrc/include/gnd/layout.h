@@ -154,7 +154,7 @@ struct SceneView {
     uint32_t tlasRoot;            // kEmpty when the scene has no primitives
     int32_t numEmitters;
     int32_t numInstances;
-    int32_t fastBoxes;            // 1: no node bound is NaN (see traverse.cuh, nodeKeys)
+    int32_t fastBoxes;            // 1: bounds allow the fast slab test (traverse.cuh, nodeKeysFast)
     Camera camera;
 };
 

@@ -157,6 +157,12 @@ gnd_status gnd_gpu_trace_count_dev(gnd_gpu_ctx* ctx, gnd_scene_id scene, const g
 gnd_status gnd_gpu_trace_closest_fixed(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* rays, int64_t n,
                                        gnd_hit* hits);
 
+/* Read bandwidth of the device in GB/s: `reps` passes of 16-byte L2-cached loads over
+ * a buffer of `bytes` (allocated and freed by the call). A buffer well inside L2 gives
+ * the L2 bandwidth, one far larger than L2 the HBM bandwidth: the denominators of the
+ * traversal roofline. Diagnostics; no counterpart in the reference. */
+gnd_status gnd_gpu_read_bandwidth(gnd_gpu_ctx* ctx, uint64_t bytes, int32_t reps, double* gbps);
+
 /* ------------------------------------------------------------------ rendering */
 /* Progress callback, the reference's Integrator::setCallback / notifyUpdate
  * (integrator.h:25-35, 148-149): called after each completed sample pass with the film
@@ -240,6 +246,12 @@ typedef struct gnd_job_status {
  * jobs); 0 = no budget beyond the device's free memory. Jobs over budget wait in the
  * queue; a job that cannot fit even alone is refused at submit with GND_ERR_BUDGET. */
 gnd_status gnd_gpu_set_hbm_budget(gnd_gpu_ctx* ctx, uint64_t bytes);
+/* Order in which running jobs' samples are handed to free path slots:
+ * GND_SERVE_SRPT (default): the job with the fewest samples left to hand out first;
+ * GND_SERVE_FIFO: the oldest running job first. Admission is first-come first-served
+ * under both. */
+enum { GND_SERVE_FIFO = 0, GND_SERVE_SRPT = 1 };
+gnd_status gnd_gpu_serve_policy(gnd_gpu_ctx* ctx, int32_t policy);
 /* Queues a job; returns at once with its id. The scene may not be freed while a job
  * that names it is queued or running (gnd_gpu_scene_free fails with GND_ERR_INVALID). */
 gnd_status gnd_gpu_serve_submit(gnd_gpu_ctx* ctx, const gnd_job_desc* job, gnd_job_id* id);

@@ -100,3 +100,16 @@ def test_budget_and_scene_in_use(setup):
     ctx.cancel_job(big)
     ctx.wait_any(big)
     ctx.free_scene(sid)
+
+
+def test_srpt_hands_out_the_smallest_job_first(setup):
+    ctx, cb, _, _ = setup
+    ctx.serve_policy("srpt")
+    big = ctx.submit(cb, width=256, height=256, spp=1024, max_depth=8, integrator=0)   # 67M samples
+    small = ctx.submit(cb, width=16, height=16, spp=1, max_depth=8, integrator=0)
+    _, ss = ctx.wait(small)
+    _, sb = ctx.wait(big)
+    assert ss["state"] == "done" and sb["state"] == "done"
+    assert ss["done_ms"] < sb["done_ms"]
+    # the small job does not wait for the big one's samples: it finishes long before
+    assert (ss["done_ms"] - ss["submit_ms"]) < 0.5 * (sb["done_ms"] - sb["submit_ms"])
