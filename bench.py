@@ -307,8 +307,10 @@ def main():
     log("extend work: %.2f nodes, %.2f triangles per ray" % (nodes_per_ray, tris_per_ray))
 
     batched = not args.plain
+    # one host film buffer for every render of the run (each render adds its sums into it)
+    film = np.zeros((WORKLOAD["height"], WORKLOAD["width"], 7), np.float32)
     for w in range(args.warmup):
-        ctx.render(sid, spp=spp, first_pass=first, batched=batched)
+        ctx.render(sid, spp=spp, first_pass=first, batched=batched, film=film)
 
     def barrier():
         torch.cuda.synchronize()
@@ -320,9 +322,8 @@ def main():
     clocks.start()
     t0 = time.perf_counter()
     stats = []
-    film_acc = None
     for k in range(args.steps):
-        film, st = ctx.render(sid, spp=spp, first_pass=first, profile=1, batched=batched)
+        _, st = ctx.render(sid, spp=spp, first_pass=first, profile=1, batched=batched, film=film)
         if dist:
             reduce_film(torch.from_numpy(film).cuda(), dist)
         stats.append(st)
@@ -344,12 +345,12 @@ def main():
 
     # e2e through the C ABI with host buffers: scene upload + render + film readback
     e2e_times = []
-    film_bytes = npix * (4 * 8 + 3 * 4)
+    film_bytes = npix * 7 * 4   # resolved float film (sum wL rgb, sum w, sum wL^2 rgb) per pixel
     for k in range(0 if args.no_e2e else max(1, args.steps)):
         barrier()
         t = time.perf_counter()
         sid2 = ctx.upload(hs)
-        film, st = ctx.render(sid2, spp=spp, first_pass=first, batched=batched)
+        _, st = ctx.render(sid2, spp=spp, first_pass=first, batched=batched, film=film)
         if dist:
             reduce_film(torch.from_numpy(film).cuda(), dist)
         ctx.free_scene(sid2)
@@ -364,7 +365,7 @@ def main():
     # the other mode on the same scene, for the batched-vs-plain comparison
     other = []
     for k in range(min(2, args.steps)):
-        _, st = ctx.render(sid, spp=spp, first_pass=first, batched=not batched)
+        _, st = ctx.render(sid, spp=spp, first_pass=first, batched=not batched, film=film)
         other.append(st["ms"])
     other_value = npix * spp / (sum(other) / len(other) / 1000.0) / 1e6 if other else None
 

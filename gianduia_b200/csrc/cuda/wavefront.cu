@@ -962,9 +962,30 @@ Wavefront::Wavefront(Context* c) : ctx_(c) {
     GND_CUDA(cudaMallocHost(&snaps_, 2 * sizeof(Snapshot)));
     std::memset(snaps_, 0, 2 * sizeof(Snapshot));
     for (cudaEvent_t& e : snapEv_) GND_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    GND_CUDA(cudaEventCreate(&evStart_));
+    GND_CUDA(cudaEventCreate(&evEnd_));
+}
+
+cudaEvent_t Wavefront::nextEvent() {
+    if (evUsed_ == evPool_.size()) {
+        cudaEvent_t e = nullptr;
+        GND_CUDA(cudaEventCreate(&e));
+        evPool_.push_back(e);
+    }
+    return evPool_[evUsed_++];
+}
+
+uint64_t Wavefront::poolBytes() const {
+    uint64_t b = slotBytes() * cap_ + filmOut_.bytes;
+    for (const HostJob& j : jobs_)
+        if (!j.used) b += j.filmSum.bytes + j.filmSq.bytes;
+    return b;
 }
 Wavefront::~Wavefront() {
-    for (cudaEvent_t e : evs_) cudaEventDestroy(e);
+    for (cudaEvent_t e : evPool_) cudaEventDestroy(e);
+    if (evStart_) cudaEventDestroy(evStart_);
+    if (evEnd_) cudaEventDestroy(evEnd_);
+    if (pinnedFilm_) cudaFreeHost(pinnedFilm_);
     clearGraphs();
     for (cudaEvent_t e : snapEv_)
         if (e) cudaEventDestroy(e);
@@ -1057,11 +1078,12 @@ int Wavefront::admit(const DeviceScene& ds, int W, int H, int spp, int firstPass
     HostJob& hj = jobs_[j];
     cudaStream_t st = ctx_->stream;
     const size_t npixAll = (size_t)W * H;
-    hj.filmSum.alloc(npixAll * 4 * sizeof(unsigned long long));
-    hj.filmSq.alloc(npixAll * 3 * sizeof(float));
+    // film buffers stay allocated between jobs of the slot and are reused when large enough
+    hj.filmSum.ensure(npixAll * 4 * sizeof(unsigned long long));
+    hj.filmSq.ensure(npixAll * 3 * sizeof(float));
     GND_CUDA(cudaMemsetAsync(hj.filmSum.ptr, 0, npixAll * 4 * sizeof(unsigned long long), st));
     GND_CUDA(cudaMemsetAsync(hj.filmSq.ptr, 0, npixAll * 3 * sizeof(float), st));
-    hj.bytes = hj.filmSum.bytes + hj.filmSq.bytes;
+    hj.bytes = npixAll * (4 * sizeof(unsigned long long) + 3 * sizeof(float));
     JobDev& jd = hj.dev;
     jd = JobDev{};
     jd.view = ds.view;
@@ -1137,26 +1159,39 @@ void Wavefront::stop(int j) {
     GND_CUDA(cudaMemsetAsync(&jobTab_.as<JobDev>()[j].workEnd, 0, sizeof(uint64_t), ctx_->stream));
 }
 
-void Wavefront::resolve(int j, float* filmHost) {
+const float* Wavefront::resolvePinned(int j) {
     HostJob& hj = jobs_[j];
     const size_t npix = (size_t)hj.dev.W * hj.dev.H;
-    filmOut_.ensure(npix * 7 * sizeof(float));
+    const size_t bytes = npix * 7 * sizeof(float);
+    filmOut_.ensure(bytes);
+    if (pinnedFilmBytes_ < bytes) {
+        if (pinnedFilm_) GND_CUDA(cudaFreeHost(pinnedFilm_));
+        pinnedFilm_ = nullptr;
+        pinnedFilmBytes_ = 0;
+        GND_CUDA(cudaMallocHost(&pinnedFilm_, bytes));
+        pinnedFilmBytes_ = bytes;
+    }
     cudaStream_t st = ctx_->stream;
     int grid = (int)std::min<size_t>((npix + 255) / 256, (size_t)ctx_->numSMs * 8);
     kFilmResolve<<<std::max(grid, 1), 256, 0, st>>>(hj.filmSum.as<unsigned long long>(), hj.filmSq.as<float>(),
                                                     filmOut_.as<float>(), npix);
     ++launches_;
     GND_CUDA(cudaGetLastError());
-    GND_CUDA(cudaMemcpyAsync(filmHost, filmOut_.ptr, npix * 7 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    GND_CUDA(cudaMemcpyAsync(pinnedFilm_, filmOut_.ptr, bytes, cudaMemcpyDeviceToHost, st));
     GND_CUDA(cudaStreamSynchronize(st));
+    return pinnedFilm_;
+}
+
+void Wavefront::resolve(int j, float* filmHost) {
+    const float* f = resolvePinned(j);
+    std::memcpy(filmHost, f, (size_t)jobs_[j].dev.W * jobs_[j].dev.H * 7 * sizeof(float));
 }
 
 void Wavefront::finish(int j, float* filmHost) {
     HostJob& hj = jobs_[j];
     const size_t n = (size_t)hj.dev.W * hj.dev.H * 7;
     if (filmHost) {
-        std::vector<float> f(n);
-        resolve(j, f.data());
+        const float* f = resolvePinned(j);
         for (size_t q = 0; q < n; ++q) filmHost[q] += f[q];
     }
     drop(j);
@@ -1164,9 +1199,7 @@ void Wavefront::finish(int j, float* filmHost) {
 
 void Wavefront::drop(int j) {
     HostJob& hj = jobs_[j];
-    hj.used = false;
-    hj.filmSum.release();
-    hj.filmSq.release();
+    hj.used = false;   // its film buffers are kept for the next job of the slot
     hj.bytes = 0;
     syncActive();
 }
@@ -1182,8 +1215,8 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
     kBeginIter<<<1, 1, 0, st>>>(kp.cnt);
     cudaEvent_t ea = nullptr, eb = nullptr;
     if (profile & 1) {
-        GND_CUDA(cudaEventCreate(&ea));
-        GND_CUDA(cudaEventCreate(&eb));
+        ea = nextEvent();
+        eb = nextEvent();
         GND_CUDA(cudaEventRecord(ea, st));
     }
     if (profile & 2) kExtend<true><<<grid, kBlock, 0, st>>>(kp);
@@ -1308,9 +1341,7 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
     reset(slots);
     const int j = admit(ds, W, H, spp, firstPass, maxDepth, integrator, window, batched ? total : npix);
     const int mix = integrator == 1 ? 2 : 1;
-    cudaEvent_t e0, e1;
-    GND_CUDA(cudaEventCreate(&e0));
-    GND_CUDA(cudaEventCreate(&e1));
+    cudaEvent_t e0 = evStart_, e1 = evEnd_;
     GND_CUDA(cudaEventRecord(e0, st));
     int pass = 0;
     const int itersPerStep = 2;
@@ -1381,16 +1412,13 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
     GND_CUDA(cudaStreamSynchronize(st));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     for (size_t k = 0; k + 1 < evs_.size(); k += 2) {
         float em = 0.f;
         cudaEventElapsedTime(&em, evs_[k], evs_[k + 1]);
         res.extendMs += em;
-        cudaEventDestroy(evs_[k]);
-        cudaEventDestroy(evs_[k + 1]);
     }
     evs_.clear();
+    evUsed_ = 0;
     try {
         c->checkKernelErrors("render");
     } catch (...) {

@@ -112,6 +112,8 @@ public:
     void release(int job, uint64_t upTo);             // hand out work items [.., upTo)
     void finish(int job, float* filmHost);            // adds the film to filmHost, frees the job
     void resolve(int job, float* filmHost);           // writes the film (H x W x 7 floats) to filmHost
+    // The job's film resolved into pinned host memory (valid until the next call).
+    const float* resolvePinned(int job);
     void stop(int job);                               // hands out no further work items of the job
     void drop(int job);                               // frees the job without reading it
     // Runs `iters` iterations; returns the number of paths in flight afterwards.
@@ -143,7 +145,7 @@ public:
     static uint64_t slotBytes() {
         return sizeof(PathState) + sizeof(HitRec) + sizeof(ShadowRec) + 5 * sizeof(uint32_t) + 10 * sizeof(uint32_t);
     }
-    uint64_t poolBytes() const { return slotBytes() * cap_ + filmOut_.bytes; }
+    uint64_t poolBytes() const;   // path pool + film staging + film buffers kept for reuse
     HostJob& job(int j) { return jobs_[j]; }
     uint64_t jobBytes() const;
 
@@ -175,7 +177,13 @@ private:
     uint64_t launches_ = 0;           // kernels launched by the engine so far
     uint64_t seqNext_ = 0;
     HostJob jobs_[kMaxJobs];
-    std::vector<cudaEvent_t> evs_;
+    std::vector<cudaEvent_t> evs_;    // profile: (start, end) of each extend launch, from evPool_
+    std::vector<cudaEvent_t> evPool_; // timing events created once and reused
+    size_t evUsed_ = 0;
+    cudaEvent_t evStart_ = nullptr, evEnd_ = nullptr;
+    cudaEvent_t nextEvent();
+    float* pinnedFilm_ = nullptr;     // resolve staging (pinned), grown as needed
+    size_t pinnedFilmBytes_ = 0;
     bool activeDirty_ = true;
 };
 
