@@ -234,25 +234,28 @@ def serve_leg(ctx, microfacet_sid, n_requests):
     rate = 0.8 * cap_rps
     reqs = serving.make_requests(n_requests, seed=4)
     arrivals = serving.poisson_arrivals(n_requests, rate, seed=4)
-    ctx.serve_policy("fifo")
-    lat_fifo, _ = serving.run_served(ctx, sids, integ, reqs, arrivals)
-    ctx.serve_policy("srpt")
+    other = {}
+    for pol in ("fifo", "srpt"):
+        ctx.serve_policy(pol)
+        other[pol] = serving.latency_stats(serving.run_served(ctx, sids, integ, reqs, arrivals)[0])
+    ctx.serve_policy("deadline")
     lat, makespan = serving.run_served(ctx, sids, integ, reqs, arrivals)
     service = serving.run_plain_service(ctx, sids, integ, reqs)
     plain_lat = serving.fifo_finish(arrivals, service) - arrivals
     s, p = serving.latency_stats(lat), serving.latency_stats(plain_lat)
-    f = serving.latency_stats(lat_fifo)
     total = sum(serving.samples(r) for r in reqs)
     for k in ("cornell", "volumetric"):
         ctx.free_scene(sids[k])
     log("serve: %d requests at %.2f req/s; p50 %.3f s p99 %.3f s (plain one at a time: p50 %.3f s p99 %.3f s)" % (
         n_requests, rate, s["p50"], s["p99"], p["p50"], p["p99"]))
-    return {"requests": n_requests, "arrivals": "poisson, seed 4", "policy": "srpt (fewest samples left first)",
+    return {"requests": n_requests, "arrivals": "poisson, seed 4",
+            "policy": "deadline (submission + 4x estimated render time, earliest first)",
             "rate_rps": rate, "capacity_rps": cap_rps,
             "capacity_mpaths_s": cap_sps / 1e6, "p50_s": s["p50"], "p99_s": s["p99"], "mean_s": s["mean"],
             "plain_p50_s": p["p50"], "plain_p99_s": p["p99"], "plain_mean_s": p["mean"],
             "p50_speedup": p["p50"] / s["p50"], "p99_speedup": p["p99"] / s["p99"],
-            "fifo_p50_s": f["p50"], "fifo_p99_s": f["p99"],
+            "fifo_p50_s": other["fifo"]["p50"], "fifo_p99_s": other["fifo"]["p99"],
+            "srpt_p50_s": other["srpt"]["p50"], "srpt_p99_s": other["srpt"]["p99"],
             "served_mpaths_s": total / makespan / 1e6, "plain_mpaths_s": total / float(service.sum()) / 1e6,
             "note": "plain time-to-image from measured per-request render times through the FIFO recurrence"}
 
@@ -267,6 +270,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--plain", action="store_true", help="one pass in flight (no refill) for the timed steps")
     ap.add_argument("--no-traversal", action="store_true", help="skip the traversal micro-benchmark")
+    ap.add_argument("--no-autotune", action="store_true", help="render with the default engine settings")
     ap.add_argument("--serve-requests", type=int, default=100,
                     help="requests in the serving stream (the full stream is 2000); 0 skips it")
     args = ap.parse_args()
@@ -307,6 +311,11 @@ def main():
     log("extend work: %.2f nodes, %.2f triangles per ray" % (nodes_per_ray, tris_per_ray))
 
     batched = not args.plain
+    tune = ctx.get_tune(sid)
+    if not args.no_autotune:
+        t = time.time()
+        tune, tune_mp = ctx.autotune(sid, spp=8, budget_ms=5000)
+        log("autotune %.1fs: %s (%.0f Mpaths/s at 8 spp)" % (time.time() - t, tune, tune_mp))
     # one host film buffer for every render of the run (each render adds its sums into it)
     film = np.zeros((WORKLOAD["height"], WORKLOAD["width"], 7), np.float32)
     for w in range(args.warmup):
@@ -343,7 +352,9 @@ def main():
     ext_ms = sum(s["extend_ms"] for s in stats)
     iters = sum(s["iterations"] for s in stats)
 
-    # e2e through the C ABI with host buffers: scene upload + render + film readback
+    # e2e through the C ABI with host buffers: scene upload from pinned host memory +
+    # render + film read-back to host memory
+    hs.pin(True)
     e2e_times = []
     film_bytes = npix * 7 * 4   # resolved float film (sum wL rgb, sum w, sum wL^2 rgb) per pixel
     for k in range(0 if args.no_e2e else max(1, args.steps)):
@@ -356,6 +367,7 @@ def main():
         ctx.free_scene(sid2)
         barrier()
         e2e_times.append(time.perf_counter() - t)
+    hs.pin(False)
     e2e_el = sum(e2e_times) if e2e_times else float("nan")
     if dist:
         tt = torch.tensor([e2e_el], device="cuda", dtype=torch.float64)
@@ -375,9 +387,12 @@ def main():
     achieved = (bytes_per_ray * ext_rays) / (ext_ms / 1000.0) / 1e9 if ext_ms > 0 else None
     traffic = None
     tp = os.path.join(ROOT, "profiles", "extend_traffic.json")
-    if os.path.exists(tp):
+    if os.path.exists(tp) and ext_launches:
+        # DRAM bytes per extend ray from one ncu capture, scaled to this run's average launch
         with open(tp) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+            per_ray = json.load(f).get("dram_bytes_per_ray")
+        if per_ray:
+            traffic = per_ray * ext_rays / ext_launches
     launches_total = sum(s["launches"] for s in stats)
     line = {
         "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
@@ -387,7 +402,8 @@ def main():
         "config": {"workload": "microfacet 1024x1024, 64 spp, path_gpu depth 16, 5,242,882 tris, 4105 instances, 8 sphere lights",
                    "parallelism": "spp-sharded" if world > 1 else "single GPU",
                    "mode": "batched (all passes share a refilled pool of path slots)" if batched else "plain (one pass in flight)",
-                   "l2": "inputs larger than L2 (scene %.2f GB resident)" % (scene_bytes / 1e9)},
+                   "l2": "inputs larger than L2 (scene %.2f GB resident)" % (scene_bytes / 1e9),
+                   "tune": tune},
         "mrays_per_s": rays * world / elapsed / 1e6,
         ("plain_value" if batched else "batched_value"): other_value,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",

@@ -61,6 +61,7 @@ def lib():
                 "gnd_gpu_destroy": [_vp],
                 "gnd_gpu_scene_upload": [_vp, _vp, ctypes.POINTER(ctypes.c_uint64)],
                 "gnd_gpu_scene_free": [_vp, ctypes.c_uint64],
+                "gnd_gpu_host_register": [_vp, ctypes.c_int32],
                 "gnd_gpu_scene_bytes": [_vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)],
                 "gnd_gpu_trace_closest": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp],
                 "gnd_gpu_trace_any": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp],
@@ -77,6 +78,9 @@ def lib():
                 "gnd_gpu_serve_cancel": [_vp, ctypes.c_uint64],
                 "gnd_gpu_serve_policy": [_vp, ctypes.c_int32],
                 "gnd_gpu_read_bandwidth": [_vp, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)],
+                "gnd_gpu_get_tune": [_vp, ctypes.c_uint64, _vp],
+                "gnd_gpu_set_tune": [_vp, ctypes.c_uint64, _vp],
+                "gnd_gpu_autotune": [_vp, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, _vp, ctypes.POINTER(ctypes.c_double)],
             }.items():
                 fn = getattr(L, name)
                 fn.argtypes = args
@@ -131,8 +135,16 @@ class HostScene:
         _check(lib().gnd_host_from_triangles(tris.ctypes.data, tris.shape[0], ctypes.byref(h)), "gnd_host_from_triangles")
         return HostScene(h.value)
 
+    def pin(self, on=True):
+        """Page-locks (or releases) the large host arrays so uploads run at DMA speed."""
+        _check(lib().gnd_gpu_host_register(self._desc_ptr, 1 if on else 0), "gnd_gpu_host_register")
+        self._pinned = bool(on)
+
     def close(self):
         if self._h and self._h.value:
+            if getattr(self, "_pinned", False):
+                lib().gnd_gpu_host_register(self._desc_ptr, 0)
+                self._pinned = False
             lib().gnd_host_free(self._h)
             self._h = _vp()
 
@@ -281,6 +293,27 @@ class GpuContext:
         _check(lib().gnd_gpu_cancel(self._h), "gnd_gpu_cancel")
 
     # ---- serving (gnd_gpu_serve_*)
+    # ---- engine settings (gnd_tune)
+    def get_tune(self, sid):
+        t = Tune()
+        _check(lib().gnd_gpu_get_tune(self._h, sid, ctypes.byref(t)), "gnd_gpu_get_tune")
+        return t.as_dict()
+
+    def set_tune(self, sid, **fields):
+        t = Tune()
+        _check(lib().gnd_gpu_get_tune(self._h, sid, ctypes.byref(t)), "gnd_gpu_get_tune")
+        for k, v in fields.items():
+            setattr(t, k, int(v))
+        _check(lib().gnd_gpu_set_tune(self._h, sid, ctypes.byref(t)), "gnd_gpu_set_tune")
+
+    def autotune(self, sid, spp=8, budget_ms=4000):
+        """Measures engine settings for the scene (gnd_gpu_autotune); returns (settings, Mpaths/s)."""
+        t = Tune()
+        m = ctypes.c_double()
+        _check(lib().gnd_gpu_autotune(self._h, sid, int(spp), int(budget_ms), ctypes.byref(t), ctypes.byref(m)),
+               "gnd_gpu_autotune")
+        return t.as_dict(), m.value
+
     def read_bandwidth(self, nbytes, reps):
         """GB/s of L2-cached 16-byte loads streaming a buffer of nbytes, reps times."""
         g = ctypes.c_double()
@@ -288,8 +321,9 @@ class GpuContext:
         return g.value
 
     def serve_policy(self, policy):
-        """'srpt' (fewest samples left first, the default) or 'fifo' (oldest job first)."""
-        code = {"fifo": 0, "srpt": 1}[policy]
+        """'deadline' (earliest submission + 4x estimated render time first, the default),
+        'srpt' (fewest samples left to hand out first) or 'fifo' (oldest job first)."""
+        code = {"fifo": 0, "srpt": 1, "deadline": 2}[policy]
         _check(lib().gnd_gpu_serve_policy(self._h, code), "gnd_gpu_serve_policy")
 
     def set_hbm_budget(self, nbytes):
@@ -353,6 +387,14 @@ class RenderStats(ctypes.Structure):
                 ("pad", ctypes.c_int32), ("ms", ctypes.c_double), ("extend_rays", ctypes.c_int64),
                 ("shadow_rays", ctypes.c_int64), ("extend_nodes", ctypes.c_int64), ("extend_tris", ctypes.c_int64),
                 ("extend_ms", ctypes.c_double), ("iterations", ctypes.c_int64), ("launches", ctypes.c_int64)]
+
+
+class Tune(ctypes.Structure):
+    _fields_ = [("pool_log2", ctypes.c_int32), ("round_iters", ctypes.c_int32), ("trav_blocks", ctypes.c_int32),
+                ("material_sort", ctypes.c_int32), ("stack_smem", ctypes.c_int32), ("graphs", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
 
 
 class JobDesc(ctypes.Structure):

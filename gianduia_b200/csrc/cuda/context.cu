@@ -192,6 +192,33 @@ gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctxh, gnd_scene_id id) {
     });
 }
 
+// The large arrays of a scene description (BVH nodes, triangles, triangle attributes):
+// each is one heap allocation of its own, so page-locking them never overlaps another
+// registration.
+static void bigArrays(const gnd_scene_desc* d, const void* ptr[3], size_t bytes[3]) {
+    ptr[0] = d->nodes; bytes[0] = (size_t)d->num_nodes * sizeof(Node4);
+    ptr[1] = d->tris; bytes[1] = (size_t)d->num_tris * sizeof(Tri);
+    ptr[2] = d->tri_attrs; bytes[2] = (size_t)d->num_tris * sizeof(TriAttr);
+}
+
+gnd_status gnd_gpu_host_register(const gnd_scene_desc* d, int32_t pin) {
+    return guarded([&]() {
+        if (!d) throw Error(GND_ERR_INVALID, "null scene description");
+        const void* ptr[3];
+        size_t bytes[3];
+        bigArrays(d, ptr, bytes);
+        for (int k = 0; k < 3; ++k) {
+            if (!ptr[k] || bytes[k] == 0) continue;
+            cudaError_t e = pin ? cudaHostRegister(const_cast<void*>(ptr[k]), bytes[k], cudaHostRegisterPortable)
+                                : cudaHostUnregister(const_cast<void*>(ptr[k]));
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                throw Error(GND_ERR_CUDA, std::string(pin ? "cudaHostRegister: " : "cudaHostUnregister: ") + cudaGetErrorString(e));
+            }
+        }
+    });
+}
+
 gnd_status gnd_gpu_scene_bytes(gnd_gpu_ctx* ctxh, gnd_scene_id id, uint64_t* bytes) {
     return guarded([&]() {
         Context* c = ctxOf(ctxh);

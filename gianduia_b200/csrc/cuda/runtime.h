@@ -84,6 +84,21 @@ struct DevBuf {
     T* as() const { return reinterpret_cast<T*>(ptr); }
 };
 
+// Engine settings that change speed, never results (gnd_tune in the C ABI).
+struct Tune {
+    int poolLog2 = 22;        // path slots of a batched render: 2^poolLog2
+    int roundIters = 8;       // wavefront iterations per host round of a batched render
+    int travBlocks = 8;       // persistent traversal blocks (128 threads) per SM
+    int sort = 1;             // 1: classify hits and shade per material class
+    int smem = 32;            // traversal stack entries in shared memory (16 or 32)
+    int graphs = 1;           // replay iteration pairs as CUDA graphs
+    bool operator==(const Tune& o) const {
+        return poolLog2 == o.poolLog2 && roundIters == o.roundIters && travBlocks == o.travBlocks && sort == o.sort &&
+               smem == o.smem && graphs == o.graphs;
+    }
+    bool operator!=(const Tune& o) const { return !(*this == o); }
+};
+
 // A scene resident in HBM.
 struct DeviceScene {
     std::vector<DevBuf> bufs;
@@ -95,6 +110,7 @@ struct DeviceScene {
     float filterRadius[2] = {0.5f, 0.5f}, filterAlpha = 2.f;
     bool hasNullMaterials = false;
     int numMaterials = 0;
+    Tune tune;                // engine settings for renders of this scene
 };
 
 // First-come first-served mutex (ticket lock). The serving thread takes the context
@@ -148,6 +164,7 @@ struct Context {
     // jobs per scene (a scene in use cannot be freed), and the job server (created on
     // the first submit; serverMu guards its creation)
     uint64_t hbmBudget = 0;
+    Tune serveTune;           // engine settings of the serving thread (pool and round size are its own)
     std::map<uint64_t, int> sceneUse;
     std::mutex serverMu;
     std::unique_ptr<Server> server;

@@ -221,6 +221,7 @@ void Server::loop() {
             }
             if (!admit.empty() && !wf.busy()) wf.reset(kPoolSlots);
             wf.setFifo(true);
+            wf.setTune(c_->serveTune);
             for (ServeJob* j : admit) {
                 int slot = -1;
                 std::string why;
@@ -296,14 +297,25 @@ void Server::loop() {
                     finishJob(j, GND_JOB_DONE);
                 }
             }
-            if (policy_ == GND_SERVE_SRPT) {
-                // hand out the samples of the job with the fewest samples left to hand out
+            // sample rate of the server (retired samples per ms of round), for deadlines
+            const double now = nowMs();
+            if (lastRoundMs_ >= 0.0 && retiredSum > lastRetiredSum_ && now > lastRoundMs_)
+                rate_ = 0.9 * rate_ + 0.1 * (double)(retiredSum - lastRetiredSum_) / (now - lastRoundMs_);
+            lastRoundMs_ = now;
+            if (policy_ != GND_SERVE_FIFO) {
                 std::vector<std::pair<int, uint64_t>> keys;
                 {
                     std::lock_guard<std::mutex> lk(m_);
                     for (ServeJob* j : running_) {
-                        const uint64_t handed = std::min<uint64_t>(ctl[j->slot].next, j->total);
-                        keys.emplace_back(j->slot, j->total - handed);
+                        if (policy_ == GND_SERVE_SRPT) {
+                            // the job with the fewest samples left to hand out first
+                            const uint64_t handed = std::min<uint64_t>(ctl[j->slot].next, j->total);
+                            keys.emplace_back(j->slot, j->total - handed);
+                        } else {
+                            // earliest deadline first (microseconds of the server clock)
+                            const double deadline = j->tSubmit + kDeadlineSlack * (double)j->total / std::max(rate_, 1.0);
+                            keys.emplace_back(j->slot, (uint64_t)(deadline * 1000.0));
+                        }
                     }
                 }
                 wf.setPriorities(keys);
@@ -324,7 +336,8 @@ void Server::loop() {
 }
 
 void Server::setPolicy(int policy) {
-    if (policy != GND_SERVE_FIFO && policy != GND_SERVE_SRPT) throw Error(GND_ERR_INVALID, "unknown serving policy");
+    if (policy != GND_SERVE_FIFO && policy != GND_SERVE_SRPT && policy != GND_SERVE_DEADLINE)
+        throw Error(GND_ERR_INVALID, "unknown serving policy");
     std::lock_guard<std::mutex> lk(m_);
     policy_ = policy;
 }

@@ -67,7 +67,10 @@ private:
     gnd_job_id nextId_ = 1;
     bool stop_ = false;
     int round_ = 0;
-    int policy_ = GND_SERVE_SRPT;
+    int policy_ = GND_SERVE_DEADLINE;
+    static constexpr double kDeadlineSlack = 4.0;
+    double rate_ = 1e5;                                      // samples per ms, running estimate
+    double lastRoundMs_ = -1.0;
     int64_t itersSinceProgress_ = 0;
     uint64_t lastRetiredSum_ = 0;
     const std::chrono::steady_clock::time_point t0_;

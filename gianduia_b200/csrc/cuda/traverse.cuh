@@ -262,11 +262,11 @@ __device__ __forceinline__ int traceRay(const SceneView& s, const TRay& ray, THi
 // persistent warps: lanes that finish a ray fetch the next one (warp-aggregated atomic on
 // a per-launch counter), and each round runs a node phase (every lane pops and tests
 // inner nodes until it holds a leaf) followed by a leaf phase (one primitive per step),
-// so the warp executes one code path at a time. The stack keeps its top kSmemStack
-// entries in shared memory and spills deeper entries to a per-lane local array.
+// so the warp executes one code path at a time. Stack entries 0 .. SMEM-1 live in shared
+// memory and deeper ones in a per-lane local array (SMEM is a template parameter, 32 by
+// default), so shallow stacks never leave shared memory.
 constexpr int kSmemStack = 32;
-constexpr int kLocalStack = 96;
-constexpr int kPStackMax = kSmemStack + kLocalStack;
+constexpr int kPStackMax = 128;   // entries per ray, shared + local
 
 struct Trav {
     V3 wo, wd;          // world ray
@@ -281,15 +281,18 @@ struct Trav {
     THit hit;
 };
 
-template <int BLOCK>
+// SMEM: entries kept in shared memory (the block's array holds SMEM * BLOCK words); the
+// remaining kPStackMax - SMEM entries live in a per-lane local array.
+template <int BLOCK, int SMEM = kSmemStack>
 struct TStack {
+    static_assert(SMEM > 0 && SMEM < kPStackMax, "shared part of the stack out of range");
     uint32_t* smem;                 // this lane's column in the block's shared array
-    uint32_t local[kLocalStack];
+    uint32_t local[kPStackMax - SMEM];
     __device__ __forceinline__ void put(int k, uint32_t v) {
-        if (k < kSmemStack) smem[k * BLOCK] = v;
-        else local[k - kSmemStack] = v;
+        if (k < SMEM) smem[k * BLOCK] = v;
+        else local[k - SMEM] = v;
     }
-    __device__ __forceinline__ uint32_t get(int k) const { return k < kSmemStack ? smem[k * BLOCK] : local[k - kSmemStack]; }
+    __device__ __forceinline__ uint32_t get(int k) const { return k < SMEM ? smem[k * BLOCK] : local[k - SMEM]; }
 };
 
 // True when (bound - o) * inv cannot be NaN for any finite or infinite node bound: the
@@ -385,8 +388,8 @@ __device__ __forceinline__ void nodeKeysFast(const Node4* nd, const Trav& t, con
 
 // Pops one entry: restores the world ray at a sentinel, tests an inner node and pushes its
 // hit children nearest-last, or makes a leaf pending. Returns an error bitmask.
-template <int BLOCK, bool COUNT>
-__device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<BLOCK>& st, TraceCounters* cnt) {
+template <int BLOCK, bool COUNT, int SMEM>
+__device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<BLOCK, SMEM>& st, TraceCounters* cnt) {
     uint32_t e;
     if (t.next != kEmpty) {
         e = t.next;
@@ -437,8 +440,8 @@ __device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<
 }
 
 // Processes one primitive of the pending leaf. For ANY, a hit ends the ray (sp = 0).
-template <int BLOCK, bool ANY, bool COUNT>
-__device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<BLOCK>& st, TraceCounters* cnt,
+template <int BLOCK, bool ANY, bool COUNT, int SMEM>
+__device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<BLOCK, SMEM>& st, TraceCounters* cnt,
                                             const uint8_t* nullMask) {
     uint32_t first = leafFirst(t.leaf), count = leafCount(t.leaf);
     uint32_t k = t.leafK++;
@@ -522,9 +525,9 @@ __device__ __forceinline__ uint32_t warpFetch(uint32_t* counter, bool want) {
 //   uint32_t count()                      number of rays
 //   bool load(uint32_t i, TRay&, const SceneView*&, const uint8_t*& nullMask)
 //   void store(uint32_t i, const THit&)   (closest) / store(i, bool) (any)
-template <int BLOCK, bool ANY, bool COUNT, typename Src>
+template <int BLOCK, bool ANY, bool COUNT, int SMEM = kSmemStack, typename Src>
 __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter, uint32_t* smemStack, TraceCounters* cnt) {
-    TStack<BLOCK> st;
+    TStack<BLOCK, SMEM> st;
     st.smem = smemStack + threadIdx.x;
     Trav t;
     const SceneView* sv = nullptr;
@@ -556,7 +559,7 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
             bool want = active && t.leaf == kEmpty && (t.next != kEmpty || t.sp > 0);
             if (!__any_sync(0xffffffffu, want)) break;
             if (want) {
-                int e = travNodeStep<BLOCK, COUNT>(t, *sv, st, cnt);
+                int e = travNodeStep<BLOCK, COUNT, SMEM>(t, *sv, st, cnt);
                 if (e || ++iter > kMaxIterations) {
                     err |= e ? e : (int)kTraceIterLimit;
                     t.sp = 0; t.leaf = kEmpty; t.next = kEmpty;
@@ -568,7 +571,7 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
             bool want = active && t.leaf != kEmpty;
             if (!__any_sync(0xffffffffu, want)) break;
             if (want) {
-                int e = travLeafStep<BLOCK, ANY, COUNT>(t, *sv, st, cnt, nm);
+                int e = travLeafStep<BLOCK, ANY, COUNT, SMEM>(t, *sv, st, cnt, nm);
                 if (e) { err |= e; t.sp = 0; t.leaf = kEmpty; t.next = kEmpty; }
             }
         }

@@ -402,14 +402,14 @@ struct ExtendSrc {
     }
 };
 
-template <bool COUNT>
+template <bool COUNT, int SMEM>
 __global__ void __launch_bounds__(kBlock, 8) kExtend(KParams p) {
-    __shared__ uint32_t stack[kSmemStack * kBlock];
+    __shared__ uint32_t stack[SMEM * kBlock];
     const uint32_t n = p.cnt[kQIn];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[0], (unsigned long long)n);
     TraceCounters cnt{0, 0};
     ExtendSrc src{&p, n, 0};
-    int err = persistentTrace<kBlock, false, COUNT>(src, p.cnt + kQFetchA, stack, &cnt);
+    int err = persistentTrace<kBlock, false, COUNT, SMEM>(src, p.cnt + kQFetchA, stack, &cnt);
     if (COUNT) {
         unsigned long long nn = cnt.nodes, nt = cnt.tris;
         for (int o = 16; o > 0; o >>= 1) {
@@ -699,13 +699,13 @@ struct ShadowSrc {
     }
 };
 
-template <bool ANY>
+template <bool ANY, int SMEM>
 __global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p, bool mixed) {
-    __shared__ uint32_t stack[kSmemStack * kBlock];
+    __shared__ uint32_t stack[SMEM * kBlock];
     const uint32_t n = p.cnt[kQShadow];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
     ShadowSrc<ANY> src{&p, n, 0, nullptr, mixed};
-    int err = persistentTrace<kBlock, ANY, false>(src, p.cnt + kQFetchB, stack, nullptr);
+    int err = persistentTrace<kBlock, ANY, false, SMEM>(src, p.cnt + kQFetchB, stack, nullptr);
     if (err) atomicOr(p.errWord, (uint32_t)err);
 }
 
@@ -1204,8 +1204,32 @@ void Wavefront::drop(int j) {
     syncActive();
 }
 
+// The traversal kernels for one shared-stack size.
+template <int SMEM>
+static void launchTraversal(const KParams& kp, int mix, bool hasNull, bool count, int travGrid, cudaStream_t st,
+                            cudaEvent_t ea, cudaEvent_t eb, int stage) {
+    if (stage == 0) {
+        if (ea) GND_CUDA(cudaEventRecord(ea, st));
+        if (count) kExtend<true, SMEM><<<travGrid, kBlock, 0, st>>>(kp);
+        else kExtend<false, SMEM><<<travGrid, kBlock, 0, st>>>(kp);
+        if (eb) GND_CUDA(cudaEventRecord(eb, st));
+    } else if (mix & 1) {
+        if (hasNull) kShadowPath<false, SMEM><<<travGrid, kBlock, 0, st>>>(kp, mix == 3);
+        else kShadowPath<true, SMEM><<<travGrid, kBlock, 0, st>>>(kp, mix == 3);
+    }
+}
+
+void Wavefront::setTune(const Tune& t) {
+    if (t != tune_) {
+        clearGraphs();
+        tune_ = t;
+    }
+}
+
 void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int profile, cudaStream_t st) {
     const int grid = ctx_->numSMs * 8;
+    const int travGrid = ctx_->numSMs * std::min(std::max(tune_.travBlocks, 1), 8);
+    const bool sort = tune_.sort != 0 || mix == 3;   // an unsorted launch serves one integrator
     uint32_t* lists[2] = {listA_.as<uint32_t>(), listB_.as<uint32_t>()};
     uint32_t* frees[2] = {freeA_.as<uint32_t>(), freeB_.as<uint32_t>()};
     kp.listIn = lists[par];
@@ -1217,23 +1241,24 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
     if (profile & 1) {
         ea = nextEvent();
         eb = nextEvent();
-        GND_CUDA(cudaEventRecord(ea, st));
-    }
-    if (profile & 2) kExtend<true><<<grid, kBlock, 0, st>>>(kp);
-    else kExtend<false><<<grid, kBlock, 0, st>>>(kp);
-    if (profile & 1) {
-        GND_CUDA(cudaEventRecord(eb, st));
         evs_.push_back(ea);
         evs_.push_back(eb);
     }
-    uint32_t* cls = classes_.as<uint32_t>();
-    kClassify<<<grid, kBlock, 0, st>>>(kp, cls);
-    if (mix & 1) launchShade<false>(kp, cls, grid, st);
-    if (mix & 2) launchShade<true>(kp, cls, grid, st);
-    if (mix & 1) {
-        if (hasNull) kShadowPath<false><<<grid, kBlock, 0, st>>>(kp, mix == 3);
-        else kShadowPath<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
+    const bool count = (profile & 2) != 0;
+    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0);
+    else launchTraversal<32>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0);
+    if (sort) {
+        uint32_t* cls = classes_.as<uint32_t>();
+        kClassify<<<grid, kBlock, 0, st>>>(kp, cls);
+        if (mix & 1) launchShade<false>(kp, cls, grid, st);
+        if (mix & 2) launchShade<true>(kp, cls, grid, st);
+    } else if (mix == 2) {
+        kShade<true, kLobesAll><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
+    } else {
+        kShade<false, kLobesAll><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
     }
+    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1);
+    else launchTraversal<32>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1);
     if (mix & 2) kShadow<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
     kRetire<<<grid, kBlock, 0, st>>>(kp);
     kEndIter<<<1, 1, 0, st>>>(kp.cnt);
@@ -1297,11 +1322,14 @@ void Wavefront::enqueueRound(int iters, int mix, bool hasNull, int profile, Resu
     kp.errWord = c->errWord.as<uint32_t>();
     kp.capacity = (uint32_t)cap_;
     kp.fifo = fifo_ ? 1u : 0u;
-    // begin, extend, classify, retire, end; 5 shade kernels + 1 shadow kernel per integrator
-    const int perIter = 5 + (mix & 1 ? 6 : 0) + (mix & 2 ? 6 : 0);
+    // begin, extend, retire, end; classify + 5 shade kernels per integrator when sorting (one
+    // shade kernel otherwise); 1 shadow kernel per integrator
+    const bool sort = tune_.sort != 0 || mix == 3;
+    const int nint = (mix & 1 ? 1 : 0) + (mix & 2 ? 1 : 0);
+    const int perIter = 4 + nint + (sort ? 1 + 5 * nint : 1);
     int it = 0;
     while (it < iters) {
-        if (useGraphs_ && profile == 0 && iters - it >= 2) {
+        if (tune_.graphs && profile == 0 && iters - it >= 2) {
             GND_CUDA(cudaGraphLaunch(pairGraph(kp, cur_, mix, hasNull, st), st));
             it += 2;
             acc.iterations += 2;
@@ -1334,7 +1362,10 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
     Result res;
     if (total == 0) return res;
     // the pool: one pass for plain renders, up to 4M in-flight paths for batched ones
-    const size_t slots = batched ? (size_t)std::min<uint64_t>(total, std::max<uint64_t>(npix, 1ull << 22)) : (size_t)npix;
+    setTune(ds.tune);
+    const int poolLog2 = std::min(std::max(tune_.poolLog2, 16), 26);
+    const size_t slots =
+        batched ? (size_t)std::min<uint64_t>(total, std::max<uint64_t>(npix, 1ull << poolLog2)) : (size_t)npix;
     for (int j = 0; j < kMaxJobs; ++j)
         if (jobs_[j].used) throw Error(GND_ERR_INVALID, "the engine is serving jobs; render through the server");
     const uint64_t launches0 = launches_;
@@ -1351,7 +1382,7 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
         if (batched) {
             // every work item is released: rounds of kRoundIters iterations, one queued
             // ahead of the one whose counters the host is reading
-            constexpr int kRoundIters = 8;
+            const int kRoundIters = std::min(std::max(tune_.roundIters & ~1, 2), 64);
             int64_t k = 0, stopAt = -1;
             enqueueRound(kRoundIters, mix, ds.hasNullMaterials, profile, res, 0);
             for (;;) {
@@ -1478,6 +1509,113 @@ gnd_status gnd_gpu_render(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_render_p
             stats->launches = r.launches;
         }
         if (c->cancel && r.passesDone < spp) throw Error(GND_ERR_CANCELLED, "render cancelled");
+    });
+}
+
+static Tune tuneFromC(const gnd_tune& t) {
+    if (t.pool_log2 < 16 || t.pool_log2 > 26) throw Error(GND_ERR_INVALID, "pool_log2 must be in 16..26");
+    if (t.round_iters < 2 || t.round_iters > 64 || (t.round_iters & 1)) throw Error(GND_ERR_INVALID, "round_iters must be even, 2..64");
+    if (t.trav_blocks < 1 || t.trav_blocks > 8) throw Error(GND_ERR_INVALID, "trav_blocks must be in 1..8");
+    if (t.material_sort != 0 && t.material_sort != 1) throw Error(GND_ERR_INVALID, "material_sort must be 0 or 1");
+    if (t.stack_smem != 16 && t.stack_smem != 32) throw Error(GND_ERR_INVALID, "stack_smem must be 16 or 32");
+    if (t.graphs != 0 && t.graphs != 1) throw Error(GND_ERR_INVALID, "graphs must be 0 or 1");
+    Tune r;
+    r.poolLog2 = t.pool_log2;
+    r.roundIters = t.round_iters;
+    r.travBlocks = t.trav_blocks;
+    r.sort = t.material_sort;
+    r.smem = t.stack_smem;
+    r.graphs = t.graphs;
+    return r;
+}
+
+static gnd_tune tuneToC(const Tune& t) {
+    gnd_tune r;
+    r.pool_log2 = t.poolLog2;
+    r.round_iters = t.roundIters;
+    r.trav_blocks = t.travBlocks;
+    r.material_sort = t.sort;
+    r.stack_smem = t.smem;
+    r.graphs = t.graphs;
+    return r;
+}
+
+gnd_status gnd_gpu_get_tune(gnd_gpu_ctx* ctxh, gnd_scene_id id, gnd_tune* out) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (!out) throw Error(GND_ERR_INVALID, "null tune");
+        std::lock_guard<FairMutex> lk(c->mu);
+        *out = tuneToC(c->scene(id).tune);
+    });
+}
+
+gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_tune* t) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (!t) throw Error(GND_ERR_INVALID, "null tune");
+        const Tune v = tuneFromC(*t);
+        std::lock_guard<FairMutex> lk(c->mu);
+        c->scene(id).tune = v;
+    });
+}
+
+gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t spp, int32_t budgetMs, gnd_tune* best,
+                            double* mpaths) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        c->bind();
+        std::lock_guard<FairMutex> lk(c->mu);
+        DeviceScene& ds = c->scene(id);
+        if (!c->wave) c->wave = std::make_unique<Wavefront>(c);
+        if (spp <= 0) spp = 8;
+        const int maxDepth = std::min(ds.maxDepth, 65535);
+        const auto t0 = std::chrono::steady_clock::now();
+        auto spentMs = [&]() {
+            return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        };
+        // a candidate: one render to capture graphs and size the pool, one timed on the device
+        auto trial = [&](const Tune& t) {
+            ds.tune = t;
+            double v = 0.0;
+            for (int r = 0; r < 2; ++r) {
+                Wavefront::Result res = c->wave->render(ds, ds.width, ds.height, spp, 0, maxDepth, ds.integrator, nullptr,
+                                                        true, 0, nullptr, nullptr, nullptr);
+                if (r == 1 && res.ms > 0.0) v = (double)res.paths / res.ms / 1e3;
+            }
+            c->checkKernelErrors("autotune");
+            return v;
+        };
+        Tune cur = ds.tune;
+        double bestV = trial(cur);
+        struct Knob {
+            int Tune::*field;
+            std::vector<int> values;
+        };
+        const std::vector<Knob> knobs = {
+            {&Tune::travBlocks, {8, 6, 4}}, {&Tune::smem, {32, 16}},          {&Tune::sort, {1, 0}},
+            {&Tune::poolLog2, {22, 21, 23, 20}}, {&Tune::roundIters, {8, 16, 4}}, {&Tune::graphs, {1, 0}},
+        };
+        for (int sweep = 0; sweep < 2; ++sweep) {
+            bool changed = false;
+            for (const Knob& k : knobs) {
+                for (int v : k.values) {
+                    if (spentMs() > budgetMs) break;
+                    if (cur.*(k.field) == v) continue;
+                    Tune t = cur;
+                    t.*(k.field) = v;
+                    const double m = trial(t);
+                    if (m > bestV * 1.02) {
+                        bestV = m;
+                        cur = t;
+                        changed = true;
+                    }
+                }
+            }
+            if (!changed || spentMs() > budgetMs) break;
+        }
+        ds.tune = cur;
+        if (best) *best = tuneToC(cur);
+        if (mpaths) *mpaths = bestV;
     });
 }
 

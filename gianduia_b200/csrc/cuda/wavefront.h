@@ -139,7 +139,10 @@ public:
     // device's active list when the order changed.
     void setPriorities(const std::vector<std::pair<int, uint64_t>>& keys);
     bool busy() const;                                // any job admitted
-    void setGraphs(bool on) { useGraphs_ = on; }      // replay the per-bounce loop as CUDA graphs
+    // Engine settings for the following iterations (graphs captured under other settings
+    // are dropped).
+    void setTune(const Tune& t);
+    const Tune& tune() const { return tune_; }
     size_t capacity() const { return cap_; }
     // Device bytes of one path slot (state, hit, shadow record, lists) and of the pool.
     static uint64_t slotBytes() {
@@ -165,7 +168,7 @@ private:
         cudaGraphExec_t exec;
     };
     std::vector<GraphEntry> graphs_;
-    bool useGraphs_ = true;
+    Tune tune_;
     Context* ctx_;
     size_t cap_ = 0;
     int cur_ = 0;

@@ -125,6 +125,10 @@ gnd_status gnd_gpu_destroy(gnd_gpu_ctx* ctx);
  * scene to HBM; the scene stays resident until gnd_gpu_scene_free. */
 gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctx, const gnd_scene_desc* desc, gnd_scene_id* out);
 gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctx, gnd_scene_id scene);
+/* Page-locks (pin = 1) or releases (pin = 0) the large host arrays of a scene
+ * description (BVH nodes, triangles, triangle attributes) so that gnd_gpu_scene_upload
+ * copies them by DMA at full link speed. Release before the description is freed. */
+gnd_status gnd_gpu_host_register(const gnd_scene_desc* desc, int32_t pin);
 /* Bytes of HBM the scene occupies. */
 gnd_status gnd_gpu_scene_bytes(gnd_gpu_ctx* ctx, gnd_scene_id scene, uint64_t* bytes);
 
@@ -212,6 +216,27 @@ gnd_status gnd_gpu_render(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_render
  * to stop after its current pass. Safe to call from another thread. */
 gnd_status gnd_gpu_cancel(gnd_gpu_ctx* ctx);
 
+/* ------------------------------------------------------------------ tuning */
+/* Engine settings of a scene's renders. They change speed only: every setting renders
+ * the same film sums. No counterpart in the reference. */
+typedef struct gnd_tune {
+    int32_t pool_log2;        /* path slots of a batched render: 2^pool_log2 (16..26) */
+    int32_t round_iters;      /* wavefront iterations per host round, batched (2..64, even) */
+    int32_t trav_blocks;      /* persistent traversal blocks of 128 threads per SM (1..8) */
+    int32_t material_sort;    /* 1: classify hits and shade per material class; 0: one kernel */
+    int32_t stack_smem;       /* traversal stack entries in shared memory: 16 or 32 */
+    int32_t graphs;           /* 1: replay pairs of iterations as CUDA graphs */
+} gnd_tune;
+gnd_status gnd_gpu_get_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_tune* tune);
+gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_tune* tune);
+/* Chooses the settings for a scene by measurement: coordinate descent from the current
+ * settings over every field, each candidate timed on the device with a batched render of
+ * `spp` passes (<= 0: 8) at the scene's film size, depth and integrator, until about
+ * budget_ms of wall time is spent. Keeps a change only when it is at least 2% faster.
+ * Stores the result as the scene's settings; returns it and its Mpaths/s. */
+gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctx, gnd_scene_id scene, int32_t spp, int32_t budget_ms, gnd_tune* best,
+                            double* mpaths_per_s);
+
 /* ------------------------------------------------------------------ serving */
 /* A stream of render jobs on one context. No counterpart in the reference, whose
  * Integrator::render renders one scene per call (integrator.h:49-155); each job renders
@@ -247,10 +272,14 @@ typedef struct gnd_job_status {
  * queue; a job that cannot fit even alone is refused at submit with GND_ERR_BUDGET. */
 gnd_status gnd_gpu_set_hbm_budget(gnd_gpu_ctx* ctx, uint64_t bytes);
 /* Order in which running jobs' samples are handed to free path slots:
- * GND_SERVE_SRPT (default): the job with the fewest samples left to hand out first;
- * GND_SERVE_FIFO: the oldest running job first. Admission is first-come first-served
- * under both. */
-enum { GND_SERVE_FIFO = 0, GND_SERVE_SRPT = 1 };
+ * GND_SERVE_FIFO: the oldest running job first;
+ * GND_SERVE_SRPT: the job with the fewest samples left to hand out first;
+ * GND_SERVE_DEADLINE (default): earliest deadline first, a job's deadline being its
+ *   submission time plus 4x its estimated render time alone (samples / the server's
+ *   measured sample rate): small jobs overtake large ones, but a large job waits at
+ *   most a bounded multiple of its own render time.
+ * Admission is first-come first-served under every policy. */
+enum { GND_SERVE_FIFO = 0, GND_SERVE_SRPT = 1, GND_SERVE_DEADLINE = 2 };
 gnd_status gnd_gpu_serve_policy(gnd_gpu_ctx* ctx, int32_t policy);
 /* Queues a job; returns at once with its id. The scene may not be freed while a job
  * that names it is queued or running (gnd_gpu_scene_free fails with GND_ERR_INVALID). */

@@ -102,9 +102,10 @@ def test_budget_and_scene_in_use(setup):
     ctx.free_scene(sid)
 
 
-def test_srpt_hands_out_the_smallest_job_first(setup):
+@pytest.mark.parametrize("policy", ["srpt", "deadline"])
+def test_small_job_overtakes_a_large_one(setup, policy):
     ctx, cb, _, _ = setup
-    ctx.serve_policy("srpt")
+    ctx.serve_policy(policy)
     big = ctx.submit(cb, width=256, height=256, spp=1024, max_depth=8, integrator=0)   # 67M samples
     small = ctx.submit(cb, width=16, height=16, spp=1, max_depth=8, integrator=0)
     _, ss = ctx.wait(small)
