@@ -391,7 +391,8 @@ class RenderStats(ctypes.Structure):
 
 class Tune(ctypes.Structure):
     _fields_ = [("pool_log2", ctypes.c_int32), ("round_iters", ctypes.c_int32), ("trav_blocks", ctypes.c_int32),
-                ("material_sort", ctypes.c_int32), ("stack_smem", ctypes.c_int32), ("graphs", ctypes.c_int32)]
+                ("material_sort", ctypes.c_int32), ("stack_smem", ctypes.c_int32), ("graphs", ctypes.c_int32),
+                ("sample_film", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}

@@ -92,9 +92,10 @@ struct Tune {
     int sort = 1;             // 1: classify hits and shade per material class
     int smem = 32;            // traversal stack entries in shared memory (16 or 32)
     int graphs = 1;           // replay iteration pairs as CUDA graphs
+    int sampleFilm = 1;       // batched box-filter renders: per-sample records, no film atomics
     bool operator==(const Tune& o) const {
         return poolLog2 == o.poolLog2 && roundIters == o.roundIters && travBlocks == o.travBlocks && sort == o.sort &&
-               smem == o.smem && graphs == o.graphs;
+               smem == o.smem && graphs == o.graphs && sampleFilm == o.sampleFilm;
     }
     bool operator!=(const Tune& o) const { return !(*this == o); }
 };

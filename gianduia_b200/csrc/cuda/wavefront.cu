@@ -823,6 +823,63 @@ __device__ __forceinline__ void filmSplat(const JobDev& j, const PathState& ps) 
     }
 }
 
+// Per-sample film record for the 0.5-radius box filter. A sample at film position
+// (fx, fy) with neither coordinate a whole number adds weight 1 to exactly its own pixel
+// (floor fx, floor fy): that is the one pixel filmSplat's loop bounds and |offset| <= 0.5
+// test select (film.h:26-69). Such a sample is stored as (L.r, L.g, L.b, 1) at its work
+// item and added to the film later by kFilmFromSamples; a sample on a whole coordinate
+// (it also reaches a neighbouring pixel) is splatted with atomics as before.
+__device__ __forceinline__ void sampleRecord(const JobDev& j, const PathState& ps) {
+    const int ww = j.wx1 - j.wx0;
+    const int x = j.wx0 + (int)(ps.pixel % (uint32_t)ww), y = j.wy0 + (int)(ps.pixel / (uint32_t)ww);
+    const uint64_t key = (uint64_t)y * (uint64_t)j.W + (uint64_t)x + (uint64_t)ps.pass * ((uint64_t)j.W * (uint64_t)j.H);
+    Rng r = rngSeed(key);
+    const V2 s2 = next2D(r);
+    const float fx = (float)x + s2.x, fy = (float)y + s2.y;
+    if (fx == floorf(fx) || fy == floorf(fy)) {
+        filmSplat(j, ps);
+        return;
+    }
+    V3 L = v3(ps.Lr, ps.Lg, ps.Lb);
+    if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = v3s(0.0f);
+    const uint64_t npix = (uint64_t)ww * (uint64_t)(j.wy1 - j.wy0);
+    const uint64_t item = (uint64_t)(ps.pass - (uint32_t)j.firstPass) * npix + ps.pixel;
+    j.samples[item] = make_float4(L.x, L.y, L.z, 1.0f);
+}
+
+// Adds the per-sample records of `passes` passes into the job's film: one thread per
+// window pixel, records in pass order. The fixed-point sums equal what filmSplat's atomics
+// add (integer sums do not depend on order); the float sum of wL^2 is taken in pass order.
+// Records never written (samples splatted directly, or not rendered) have w = 0.
+__global__ void kFilmFromSamples(JobDev j, uint32_t passes) {
+    const int ww = j.wx1 - j.wx0;
+    const uint64_t npix = (uint64_t)ww * (uint64_t)(j.wy1 - j.wy0);
+    for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < npix; q += (uint64_t)gridDim.x * blockDim.x) {
+        unsigned long long sr = 0, sg = 0, sb = 0, sw = 0;
+        float qr = 0.0f, qg = 0.0f, qb = 0.0f;
+        for (uint32_t k = 0; k < passes; ++k) {
+            const float4 rec = j.samples[(uint64_t)k * npix + q];
+            if (rec.w == 0.0f) continue;
+            sr += toFixed(rec.x);
+            sg += toFixed(rec.y);
+            sb += toFixed(rec.z);
+            sw += toFixed(1.0f);
+            qr += rec.x * rec.x;
+            qg += rec.y * rec.y;
+            qb += rec.z * rec.z;
+        }
+        const int x = j.wx0 + (int)(q % (uint64_t)ww), y = j.wy0 + (int)(q / (uint64_t)ww);
+        const size_t idx = (size_t)y * (size_t)j.W + (size_t)x;
+        j.filmSum[idx * 4 + 0] += sr;
+        j.filmSum[idx * 4 + 1] += sg;
+        j.filmSum[idx * 4 + 2] += sb;
+        j.filmSum[idx * 4 + 3] += sw;
+        j.filmSq[idx * 3 + 0] += qr;
+        j.filmSq[idx * 3 + 1] += qg;
+        j.filmSq[idx * 3 + 2] += qb;
+    }
+}
+
 // ---------------------------------------------------------------- retire / refill
 // Lanes in `want` take work items from the active jobs: the warp leader walks the active
 // list from a per-warp round-robin start and takes one contiguous range per job until the
@@ -888,7 +945,9 @@ __global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
         if (valid && isDone) {
             PathState ps = p.paths[slot];
             jobIdx = ps.flags >> 8;
-            filmSplat(p.jobs[jobIdx], ps);
+            const JobDev& jd = p.jobs[jobIdx];
+            if (jd.samples) sampleRecord(jd, ps);
+            else filmSplat(jd, ps);
         }
         const uint32_t grp = __match_any_sync(0xffffffffu, jobIdx);
         if (jobIdx != 0xFFFFFFFFu && (int)lane == __ffs(grp) - 1)
@@ -1153,6 +1212,27 @@ void Wavefront::readCtl(std::vector<JobCtl>& out) {
         if (jobs_[j].used) jobs_[j].retired = out[j].retired;
 }
 
+void Wavefront::useSampleRecords(int j, uint64_t items) {
+    cudaStream_t st = ctx_->stream;
+    samples_.ensure(items * sizeof(float4));
+    GND_CUDA(cudaMemsetAsync(samples_.ptr, 0, items * sizeof(float4), st));
+    HostJob& hj = jobs_[j];
+    hj.dev.samples = samples_.as<float4>();
+    // pageable source: the copy is staged before the call returns
+    GND_CUDA(cudaMemcpyAsync(&jobTab_.as<JobDev>()[j].samples, &hj.dev.samples, sizeof(float4*), cudaMemcpyHostToDevice, st));
+}
+
+void Wavefront::filmFromSamples(int j, uint64_t items) {
+    const JobDev& jd = jobs_[j].dev;
+    const uint64_t npix = (uint64_t)(jd.wx1 - jd.wx0) * (uint64_t)(jd.wy1 - jd.wy0);
+    if (!jd.samples || npix == 0) return;
+    const uint32_t passes = (uint32_t)(items / npix);
+    const int grid = (int)std::min<uint64_t>((npix + 255) / 256, (uint64_t)ctx_->numSMs * 16);
+    kFilmFromSamples<<<std::max(grid, 1), 256, 0, ctx_->stream>>>(jd, passes);
+    ++launches_;
+    GND_CUDA(cudaGetLastError());
+}
+
 void Wavefront::stop(int j) {
     HostJob& hj = jobs_[j];
     hj.dev.workEnd = 0;
@@ -1372,6 +1452,17 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
     reset(slots);
     const int j = admit(ds, W, H, spp, firstPass, maxDepth, integrator, window, batched ? total : npix);
     const int mix = integrator == 1 ? 2 : 1;
+    // batched renders with the box filter keep per-sample records instead of film atomics
+    // (at most 2^30 records: 16 GiB)
+    const bool records = batched && tune_.sampleFilm && ds.filter == 0 && total <= (1ull << 30);
+    if (records) {
+        try {
+            useSampleRecords(j, total);
+        } catch (...) {
+            drop(j);
+            throw;
+        }
+    }
     cudaEvent_t e0 = evStart_, e1 = evEnd_;
     GND_CUDA(cudaEventRecord(e0, st));
     int pass = 0;
@@ -1402,6 +1493,7 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
                 ++k;
             }
             GND_CUDA(cudaStreamSynchronize(st));   // the round queued ahead has nothing left to do
+            if (records) filmFromSamples(j, total);
         }
         while (!batched) {
             uint32_t inflight = step(itersPerStep, mix, ds.hasNullMaterials, profile, res);
@@ -1519,6 +1611,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     if (t.material_sort != 0 && t.material_sort != 1) throw Error(GND_ERR_INVALID, "material_sort must be 0 or 1");
     if (t.stack_smem != 16 && t.stack_smem != 32) throw Error(GND_ERR_INVALID, "stack_smem must be 16 or 32");
     if (t.graphs != 0 && t.graphs != 1) throw Error(GND_ERR_INVALID, "graphs must be 0 or 1");
+    if (t.sample_film != 0 && t.sample_film != 1) throw Error(GND_ERR_INVALID, "sample_film must be 0 or 1");
     Tune r;
     r.poolLog2 = t.pool_log2;
     r.roundIters = t.round_iters;
@@ -1526,6 +1619,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     r.sort = t.material_sort;
     r.smem = t.stack_smem;
     r.graphs = t.graphs;
+    r.sampleFilm = t.sample_film;
     return r;
 }
 
@@ -1537,6 +1631,7 @@ static gnd_tune tuneToC(const Tune& t) {
     r.material_sort = t.sort;
     r.stack_smem = t.smem;
     r.graphs = t.graphs;
+    r.sample_film = t.sampleFilm;
     return r;
 }
 
@@ -1594,6 +1689,7 @@ gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t spp, int
         const std::vector<Knob> knobs = {
             {&Tune::travBlocks, {8, 6, 4}}, {&Tune::smem, {32, 16}},          {&Tune::sort, {1, 0}},
             {&Tune::poolLog2, {22, 21, 23, 20}}, {&Tune::roundIters, {8, 16, 4}}, {&Tune::graphs, {1, 0}},
+            {&Tune::sampleFilm, {1, 0}},
         };
         for (int sweep = 0; sweep < 2; ++sweep) {
             bool changed = false;

@@ -55,6 +55,9 @@ struct JobDev {
     int32_t hasNull;
     int32_t firstPass;
     uint64_t workBegin, workEnd;   // work items [begin, end): item -> (pass, window pixel)
+    // Per-sample film records (batched renders with the 0.5-radius box filter), indexed by
+    // work item; null: finished samples are splatted into the film with atomics.
+    float4* samples;
 };
 
 // Queue counters (device): ints.
@@ -132,6 +135,10 @@ public:
     uint64_t retired(int job);                        // reads the job's retired count (sync)
     void readRetired(std::vector<uint64_t>& out);     // all jobs (one copy, sync)
     void readCtl(std::vector<JobCtl>& out);           // all jobs' hand-out and retired counts (sync)
+    // Gives the job a per-sample record buffer for `items` work items (see JobDev::samples);
+    // filmFromSamples() then adds the records into the job's film.
+    void useSampleRecords(int job, uint64_t items);
+    void filmFromSamples(int job, uint64_t items);
     // Hand-out order: false = every warp starts at a different active job (even shares),
     // true = oldest admitted job first (first-come first-served with the pool kept full).
     void setFifo(bool fifo) { fifo_ = fifo; }
@@ -173,7 +180,7 @@ private:
     size_t cap_ = 0;
     int cur_ = 0;
     DevBuf paths_, hits_, listA_, listB_, freeA_, freeB_, shadow_, done_, counters_, totals_, classes_;
-    DevBuf jobTab_, ctl_, active_, filmOut_;
+    DevBuf jobTab_, ctl_, active_, filmOut_, samples_;
     Snapshot* snaps_ = nullptr;       // pinned host memory, two slots
     cudaEvent_t snapEv_[2] = {nullptr, nullptr};
     bool fifo_ = false;

@@ -226,6 +226,9 @@ typedef struct gnd_tune {
     int32_t material_sort;    /* 1: classify hits and shade per material class; 0: one kernel */
     int32_t stack_smem;       /* traversal stack entries in shared memory: 16 or 32 */
     int32_t graphs;           /* 1: replay pairs of iterations as CUDA graphs */
+    int32_t sample_film;      /* 1: batched renders with the box filter write one record per
+                                 sample and build the film from them afterwards (no film
+                                 atomics; needs 16 bytes of HBM per sample); 0: atomics */
 } gnd_tune;
 gnd_status gnd_gpu_get_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_tune* tune);
 gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_tune* tune);

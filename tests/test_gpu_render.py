@@ -127,6 +127,10 @@ def test_window_matches_full_render(ctx, tmp_path):
     assert st["paths"] == 12 * 26 * 2
     assert np.array_equal(win[4:30, 8:20, :4], full[4:30, 8:20, :4])
     assert not win[:4].any() and not win[:, :8].any()
+    # batched (per-sample film records) over the same window: the same sums
+    winb, _ = ctx.render(sid, spp=2, window=(8, 4, 20, 30), batched=True)
+    assert np.array_equal(winb[..., :4], win[..., :4])
+    assert np.allclose(winb[..., 4:], win[..., 4:], rtol=1e-5, atol=1e-6)
 
 
 def test_progress_callback_and_cancel(ctx, tmp_path):
