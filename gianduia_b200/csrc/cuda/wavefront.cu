@@ -50,6 +50,21 @@ __device__ __forceinline__ uint32_t warpAppend(uint32_t* counter, bool pred) {
     return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
 }
 
+// Two appends with one atomic: lanes with `a` take consecutive entries of the counter in
+// the low half of `pair`, lanes with `b` of the one in the high half. Every lane of the
+// warp calls it.
+__device__ __forceinline__ void warpAppend2(unsigned long long* pair, bool a, bool b, uint32_t& ia, uint32_t& ib) {
+    const uint32_t ma = __ballot_sync(0xffffffffu, a), mb = __ballot_sync(0xffffffffu, b);
+    const uint32_t lane = threadIdx.x & 31u;
+    unsigned long long base = 0;
+    if ((ma | mb) && lane == 0)
+        base = atomicAdd(pair, (unsigned long long)__popc(ma) | ((unsigned long long)__popc(mb) << 32));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const uint32_t lt = (1u << lane) - 1u;
+    ia = (uint32_t)base + (uint32_t)__popc(ma & lt);
+    ib = (uint32_t)(base >> 32) + (uint32_t)__popc(mb & lt);
+}
+
 struct KParams {
     const JobDev* jobs;
     PathState* paths;
@@ -363,15 +378,26 @@ __device__ __forceinline__ void generatePath(const JobDev& j, uint32_t jobIdx, u
 }
 
 // ---------------------------------------------------------------- kernels
-__global__ void kBeginIter(uint32_t* cnt) {
+__global__ void kBeginIter(KParams p) {
+    uint32_t* cnt = p.cnt;
     cnt[kQOut] = 0;
     cnt[kQShadow] = 0;
     cnt[kQDone] = 0;
     cnt[kQFetchA] = 0;
     cnt[kQFetchB] = 0;
-    cnt[kQFreeOut] = 0;
     cnt[kQIter] += 1;   // iteration number: round-robin start of the job grabs
     for (int k = 0; k < kShadeClasses; ++k) cnt[kQClass0 + k] = 0;
+    // Whether any active job has work items left to hand out (the hand-out limits change
+    // only between launches). Without work the idle slots are carried over unchanged:
+    // kRetire copies them to the front of the next free list, reserved here.
+    uint32_t work = 0;
+    const uint32_t na = cnt[kQActive];
+    for (uint32_t t = 0; t < na && !work; ++t) {
+        const uint32_t jid = p.active[t];
+        if (p.ctl[jid].next < p.jobs[jid].workEnd) work = 1;
+    }
+    cnt[kQWork] = work;
+    cnt[kQFreeOut] = work ? 0u : cnt[kQFree];
 }
 
 // Closest-hit source/sink over the active list (extend).
@@ -933,8 +959,13 @@ __device__ __forceinline__ bool warpGrab(const KParams& p, bool want, uint32_t& 
 // free list. The loop is warp-uniform (all lanes of a warp iterate together).
 __global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
     const uint32_t nd = p.cnt[kQDone], nf = p.cnt[kQFree];
-    const uint32_t total = nd + nf;
+    const bool work = p.cnt[kQWork] != 0;
+    // with work left, finished and idle slots take work items; without, only finished
+    // paths are retired and the idle slots are copied over
+    const uint32_t total = work ? nd + nf : nd;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[2], (unsigned long long)nd);
+    if (!work)
+        for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < nf; i += gridDim.x * kBlock) p.freeOut[i] = p.freeIn[i];
     const uint32_t lane = threadIdx.x & 31u;
     for (uint32_t base = blockIdx.x * kBlock + (threadIdx.x & ~31u); base < total; base += gridDim.x * kBlock) {
         const uint32_t i = base + lane;
@@ -954,16 +985,17 @@ __global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
             atomicAdd(&p.ctl[jobIdx].retired, (unsigned long long)__popc(grp));
         uint32_t gj = 0;
         uint64_t item = 0;
-        const bool got = warpGrab(p, valid, gj, item);
+        bool got = false;
+        if (work) got = warpGrab(p, valid, gj, item);   // `work` is uniform over the grid
         if (got) {
             PathState ps;
             generatePath(p.jobs[gj], gj, item, ps);
             p.paths[slot] = ps;
         }
-        const uint32_t k = warpAppend(&p.cnt[kQOut], got);
-        if (got) p.listOut[k] = slot;
         const bool idle = valid && !got;
-        const uint32_t f = warpAppend(&p.cnt[kQFreeOut], idle);
+        uint32_t k, f;
+        warpAppend2(reinterpret_cast<unsigned long long*>(p.cnt + kQOut), got, idle, k, f);
+        if (got) p.listOut[k] = slot;
         if (idle) p.freeOut[f] = slot;
     }
 }
@@ -1316,7 +1348,7 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
     kp.listOut = lists[par ^ 1];
     kp.freeIn = frees[par];
     kp.freeOut = frees[par ^ 1];
-    kBeginIter<<<1, 1, 0, st>>>(kp.cnt);
+    kBeginIter<<<1, 1, 0, st>>>(kp);
     cudaEvent_t ea = nullptr, eb = nullptr;
     if (profile & 1) {
         ea = nextEvent();
@@ -1340,7 +1372,7 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
     if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1);
     else launchTraversal<32>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1);
     if (mix & 2) kShadow<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
-    kRetire<<<grid, kBlock, 0, st>>>(kp);
+    kRetire<<<ctx_->numSMs * 12, kBlock, 0, st>>>(kp);   // 12 blocks per SM: its register limit
     kEndIter<<<1, 1, 0, st>>>(kp.cnt);
     GND_CUDA(cudaGetLastError());
 }

@@ -61,10 +61,13 @@ struct JobDev {
 };
 
 // Queue counters (device): ints.
+// kQOut and kQFreeOut are one aligned 64-bit pair (low, high) so that kRetire appends to
+// both lists with a single atomic.
 enum QCounter : int {
-    kQIn = 0, kQOut = 1, kQShadow = 2, kQDone = 3, kQFetchA = 4, kQFetchB = 5, kQFree = 6, kQFreeOut = 7,
-    kQActive = 8, kQIter = 9, kQClass0 = 16, kQCount = 32
+    kQIn = 0, kQShadow = 2, kQDone = 3, kQFetchA = 4, kQFetchB = 5, kQFree = 6,
+    kQActive = 8, kQIter = 9, kQWork = 10, kQOut = 12, kQFreeOut = 13, kQClass0 = 16, kQCount = 32
 };
+static_assert(kQOut % 2 == 0 && kQFreeOut == kQOut + 1, "kQOut / kQFreeOut must form an aligned pair");
 
 // Per-job work control on the device.
 struct alignas(16) JobCtl {
