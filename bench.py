@@ -218,6 +218,35 @@ def traversal_leg(ctx):
     return out
 
 
+def scenes_leg(ctx):
+    """The two other render configurations at their full sizes: Cornell box (path, 256^2,
+    16 spp, depth 8) and volumetric Cornell box (volpath, 512^2, 64 spp, depth 32), batched
+    and plain, each the median of 3 renders after 1 warm-up (host wall time of the call)."""
+    import gianduia_b200 as G
+    from gianduia_b200 import scenes
+    base = os.path.join(tempfile.gettempdir(), "gnd_bench_scenes")
+    out = {}
+    for name, xml in (("cornell", scenes.cornell(os.path.join(base, "cornell"))),
+                      ("volumetric", scenes.volumetric(os.path.join(base, "volumetric")))):
+        hs = G.HostScene.load_xml(xml)
+        sid = ctx.upload(hs)
+        film = np.zeros((hs.height, hs.width, 7), np.float32)
+        rec = {"width": hs.width, "height": hs.height, "spp": hs.spp, "max_depth": hs.desc.max_depth,
+               "integrator": ["path_gpu", "volpath_gpu"][hs.desc.integrator]}
+        for mode in ("batched", "plain"):
+            ts = []
+            for k in range(4):
+                t = time.perf_counter()
+                _, st = ctx.render(sid, batched=(mode == "batched"), film=film)
+                if k:
+                    ts.append(time.perf_counter() - t)
+            rec[mode + "_mpaths_s"] = st["paths"] / statistics.median(ts) / 1e6
+        ctx.free_scene(sid)
+        out[name] = rec
+        log("%s: batched %.1f Mpaths/s, plain %.1f Mpaths/s" % (name, rec["batched_mpaths_s"], rec["plain_mpaths_s"]))
+    return out
+
+
 def serve_leg(ctx, microfacet_sid, n_requests):
     """The serving stream: requests over {Cornell box, microfacet grid, volumetric Cornell
     box} with Poisson arrivals at 80% of the job server's measured capacity, served by the
@@ -271,6 +300,7 @@ def main():
     ap.add_argument("--plain", action="store_true", help="one pass in flight (no refill) for the timed steps")
     ap.add_argument("--no-traversal", action="store_true", help="skip the traversal micro-benchmark")
     ap.add_argument("--no-autotune", action="store_true", help="render with the default engine settings")
+    ap.add_argument("--no-scenes", action="store_true", help="skip the Cornell / volumetric renders")
     ap.add_argument("--serve-requests", type=int, default=100,
                     help="requests in the serving stream (the full stream is 2000); 0 skips it")
     args = ap.parse_args()
@@ -418,6 +448,8 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_traversal:
         line["traversal"] = traversal_leg(ctx)
+    if rank == 0 and world == 1 and not args.no_scenes:
+        line["scenes"] = scenes_leg(ctx)
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serve"] = serve_leg(ctx, sid, args.serve_requests)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

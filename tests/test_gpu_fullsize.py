@@ -1,0 +1,96 @@
+"""Parity at the benchmark configurations' full sizes.
+
+  * microfacet grid (5,242,882 triangles, 4105 instances, 1024 x 1024): one pass on the
+    same per-pixel streams as the CPU oracle (same-stream bar of test_gpu_render), and
+    per-pixel 3-sigma agreement with independent seeds at 256 x 256, 16 spp;
+  * size-independent properties at the full sample counts: the batched engine and the
+    plain engine give bit-identical film sums for the microfacet render (1024^2 x 64 spp)
+    and the volumetric Cornell box (512^2 x 64 spp, depth 32), every sample lands in the
+    film once (total weight = samples, up to the rare samples on a pixel border that the
+    box filter gives to two pixels), and the radiance is finite and non-negative."""
+import os
+
+import numpy as np
+import pytest
+
+import gianduia_b200 as G
+from gianduia_b200 import scenes
+from oracle import pyoracle as O
+from test_gpu_render import image, same_stream_check, sigma_check
+
+pytestmark = [pytest.mark.gpu, pytest.mark.timeout(900)]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = G.GpuContext(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def microfacet_xml(tmp_path_factory):
+    d = str(tmp_path_factory.mktemp("microfacet"))
+    return scenes.microfacet(d, width=1024, height=1024, spp=64, max_depth=16, grid=64, seed=2)
+
+
+def check_film(f, samples, label):
+    assert np.isfinite(f).all(), label
+    assert (f[..., :3] >= 0).all() and (f[..., 4:] >= 0).all(), label
+    w = f[..., 3]
+    assert w.sum() >= samples and w.sum() <= samples * (1 + 1e-4), "%s: total weight %g for %d samples" % (
+        label, w.sum(), samples)
+
+
+def test_microfacet_full_resolution_same_stream(ctx, microfacet_xml):
+    sid = ctx.upload(G.HostScene.load_xml(microfacet_xml))
+    gfilm, st = ctx.render(sid, spp=1, batched=True)
+    ofilm, paths, _ = O.Scene.load(microfacet_xml).render(0, 1, nthreads=0)
+    assert st["paths"] == paths == 1024 * 1024
+    same_stream_check(image(gfilm), image(ofilm), "microfacet 1024^2 x 1")
+    ctx.free_scene(sid)
+
+
+def test_microfacet_statistics(ctx, microfacet_xml, tmp_path):
+    # the same scene file rendered at 256 x 256 (the camera keeps its field of view)
+    small = os.path.join(str(tmp_path), "microfacet_256.xml")
+    with open(microfacet_xml) as f:
+        txt = f.read()
+    with open(small, "w") as f:
+        f.write(txt.replace('name="width" value="1024"', 'name="width" value="256"')
+                   .replace('name="height" value="1024"', 'name="height" value="256"'))
+    assert 'value="256"' in open(small).read()
+    # the OBJ files are referenced relative to the scene file's directory
+    for name in os.listdir(os.path.dirname(microfacet_xml)):
+        src = os.path.join(os.path.dirname(microfacet_xml), name)
+        dst = os.path.join(str(tmp_path), name)
+        if name != os.path.basename(microfacet_xml) and not os.path.exists(dst):
+            os.symlink(src, dst)
+    sid = ctx.upload(G.HostScene.load_xml(small))
+    gfilm, _ = ctx.render(sid, spp=16, first_pass=100000, batched=True)   # independent seeds
+    ofilm, _, _ = O.Scene.load(small).render(0, 16, nthreads=0)
+    sigma_check(gfilm, ofilm, "microfacet-3sigma", limit=0.012)
+    ctx.free_scene(sid)
+
+
+def test_microfacet_full_size_batched_equals_plain(ctx, microfacet_xml):
+    sid = ctx.upload(G.HostScene.load_xml(microfacet_xml))
+    b, sb = ctx.render(sid, spp=64, batched=True)
+    p, sp = ctx.render(sid, spp=64, batched=False)
+    assert sb["paths"] == sp["paths"] == 1024 * 1024 * 64
+    assert np.array_equal(b[..., :4], p[..., :4])
+    assert np.allclose(b[..., 4:], p[..., 4:], rtol=1e-5, atol=1e-6)
+    check_film(b, 1024 * 1024 * 64, "microfacet 1024^2 x 64")
+    ctx.free_scene(sid)
+
+
+def test_volumetric_full_size_batched_equals_plain(ctx, tmp_path):
+    xml = scenes.volumetric(str(tmp_path), width=512, height=512, spp=64, max_depth=32)
+    sid = ctx.upload(G.HostScene.load_xml(xml))
+    b, sb = ctx.render(sid, batched=True)
+    p, sp = ctx.render(sid, batched=False)
+    assert sb["paths"] == sp["paths"] == 512 * 512 * 64
+    assert np.array_equal(b[..., :4], p[..., :4])
+    assert np.allclose(b[..., 4:], p[..., 4:], rtol=1e-5, atol=1e-6)
+    check_film(b, 512 * 512 * 64, "volumetric 512^2 x 64")
+    ctx.free_scene(sid)
