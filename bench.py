@@ -391,12 +391,17 @@ def main():
         barrier()
         t = time.perf_counter()
         sid2 = ctx.upload(hs)
+        ctx.set_tune(sid2, **tune)
+        t_up = time.perf_counter()
         _, st = ctx.render(sid2, spp=spp, first_pass=first, batched=batched, film=film)
         if dist:
             reduce_film(torch.from_numpy(film).cuda(), dist)
+        t_re = time.perf_counter()
         ctx.free_scene(sid2)
         barrier()
         e2e_times.append(time.perf_counter() - t)
+        log("e2e step: upload %.1f ms, render %.1f ms, free %.1f ms" % (
+            (t_up - t) * 1e3, (t_re - t_up) * 1e3, (time.perf_counter() - t_re) * 1e3))
     hs.pin(False)
     e2e_el = sum(e2e_times) if e2e_times else float("nan")
     if dist:

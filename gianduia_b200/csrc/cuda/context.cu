@@ -19,6 +19,9 @@ Context::~Context() {
     server.reset();   // joins the serving thread before the engine goes away
     wave.reset();
     scenes.clear();
+    if (stream) cudaStreamSynchronize(stream);
+    cudaMemPool_t pool = nullptr;
+    if (device >= 0 && cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     errWord.release();
     rayScratch.release();
     hitScratch.release();
@@ -51,7 +54,7 @@ namespace {
 template <typename T>
 const T* upload(DeviceScene& ds, cudaStream_t st, const void* src, size_t count) {
     size_t bytes = count * sizeof(T);
-    ds.bufs.emplace_back(bytes > 0 ? bytes : 16);
+    ds.bufs.emplace_back(bytes > 0 ? bytes : 16, st);
     if (bytes) GND_CUDA(cudaMemcpyAsync(ds.bufs.back().ptr, src, bytes, cudaMemcpyHostToDevice, st));
     ds.bytes += ds.bufs.back().bytes;
     return ds.bufs.back().as<T>();
@@ -84,6 +87,12 @@ gnd_status gnd_gpu_create(int device, gnd_gpu_ctx** out) {
             throw Error(GND_ERR_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100 (this build targets sm_100a)");
         c->numSMs = prop.multiProcessorCount;
         GND_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        // scene arrays come from the default memory pool; keep freed memory in the pool
+        // (a process-local setting) so that scene uploads reuse it
+        cudaMemPool_t pool = nullptr;
+        GND_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t keep = UINT64_MAX;
+        GND_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
         c->errWord.alloc(16);
         GND_CUDA(cudaMemset(c->errWord.ptr, 0, 16));
         *out = reinterpret_cast<gnd_gpu_ctx*>(c.release());
@@ -157,17 +166,23 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         v.numInstances = d->num_instances;
         v.fastBoxes = nanBounds ? 0 : 1;
         if (d->camera) std::memcpy(&v.camera, d->camera, sizeof(Camera));
-        // null-BSDF mask per instance
-        std::vector<uint8_t> mask(std::max(1, d->num_instances), 0);
+        // null-BSDF mask and material type per instance
+        std::vector<uint8_t> mask(std::max(1, d->num_instances), 0), cls(std::max(1, d->num_instances), kMatIndex);
         const Material* mats = reinterpret_cast<const Material*>(d->materials);
-        for (int i = 0; i < d->num_instances; ++i)
-            if (mats[is[i].material].type == kMatIndex) { mask[i] = 1; ds->hasNullMaterials = true; }
+        for (int i = 0; i < d->num_instances; ++i) {
+            const uint32_t t = mats[is[i].material].type;
+            cls[i] = (uint8_t)(t < kMatIndex ? t : kMatIndex);
+            if (t == kMatIndex) { mask[i] = 1; ds->hasNullMaterials = true; }
+        }
         ds->nullMask.alloc(mask.size());
         GND_CUDA(cudaMemcpyAsync(ds->nullMask.ptr, mask.data(), mask.size(), cudaMemcpyHostToDevice, c->stream));
+        ds->instClass.alloc(cls.size());
+        GND_CUDA(cudaMemcpyAsync(ds->instClass.ptr, cls.data(), cls.size(), cudaMemcpyHostToDevice, c->stream));
+        v.instClass = ds->instClass.as<uint8_t>();
         ds->viewDev.alloc(sizeof(SceneView));
         GND_CUDA(cudaMemcpyAsync(ds->viewDev.ptr, &v, sizeof(SceneView), cudaMemcpyHostToDevice, c->stream));
         GND_CUDA(cudaStreamSynchronize(c->stream));
-        ds->bytes += ds->nullMask.bytes + ds->viewDev.bytes;
+        ds->bytes += ds->nullMask.bytes + ds->instClass.bytes + ds->viewDev.bytes;
         ds->width = d->width; ds->height = d->height; ds->spp = d->spp; ds->maxDepth = d->max_depth;
         ds->integrator = d->integrator; ds->filter = d->filter;
         ds->filterRadius[0] = d->filter_radius[0]; ds->filterRadius[1] = d->filter_radius[1];
@@ -188,7 +203,12 @@ gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctxh, gnd_scene_id id) {
         if (use != c->sceneUse.end() && use->second > 0)
             throw Error(GND_ERR_INVALID, "scene " + std::to_string(id) + " is used by " + std::to_string(use->second) +
                                              " queued or running job(s)");
-        if (!c->scenes.erase(id)) throw Error(GND_ERR_INVALID, "unknown scene id");
+        auto it = c->scenes.find(id);
+        if (it == c->scenes.end()) throw Error(GND_ERR_INVALID, "unknown scene id");
+        // work queued on callers' streams (the _dev ray-batch calls) may still read the
+        // scene; the arrays go back to the pool in the order of the context's stream
+        GND_CUDA(cudaDeviceSynchronize());
+        c->scenes.erase(it);
     });
 }
 

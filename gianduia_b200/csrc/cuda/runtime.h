@@ -84,6 +84,39 @@ struct DevBuf {
     T* as() const { return reinterpret_cast<T*>(ptr); }
 };
 
+// A stream-ordered allocation from the device's default memory pool, for scene arrays.
+// The context raises the pool's release threshold, so memory freed here stays mapped in
+// the pool and the next upload reuses it: freeing and uploading scenes does not unmap and
+// map device memory (a plain cudaFree of a large buffer can stall the host for a long,
+// unpredictable time).
+struct PoolBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaStream_t stream = nullptr;
+    PoolBuf() = default;
+    PoolBuf(size_t n, cudaStream_t st) : stream(st) {
+        if (n == 0) return;
+        GND_CUDA(cudaMallocAsync(&ptr, n, st));
+        bytes = n;
+    }
+    PoolBuf(const PoolBuf&) = delete;
+    PoolBuf& operator=(const PoolBuf&) = delete;
+    PoolBuf(PoolBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes), stream(o.stream) { o.ptr = nullptr; o.bytes = 0; }
+    PoolBuf& operator=(PoolBuf&& o) noexcept {
+        if (this != &o) {
+            if (ptr) cudaFreeAsync(ptr, stream);
+            ptr = o.ptr; bytes = o.bytes; stream = o.stream;
+            o.ptr = nullptr; o.bytes = 0;
+        }
+        return *this;
+    }
+    ~PoolBuf() {
+        if (ptr) cudaFreeAsync(ptr, stream);
+    }
+    template <typename T>
+    T* as() const { return reinterpret_cast<T*>(ptr); }
+};
+
 // Engine settings that change speed, never results (gnd_tune in the C ABI).
 struct Tune {
     int poolLog2 = 22;        // path slots of a batched render: 2^poolLog2
@@ -102,9 +135,10 @@ struct Tune {
 
 // A scene resident in HBM.
 struct DeviceScene {
-    std::vector<DevBuf> bufs;
+    std::vector<PoolBuf> bufs;  // the large arrays (pool memory, freed stream-ordered)
     SceneView view{};
     DevBuf nullMask;          // per instance: 1 when the material has no BSDF (index)
+    DevBuf instClass;         // per instance: material type (SceneView::instClass)
     DevBuf viewDev;           // SceneView copy in device memory
     uint64_t bytes = 0;
     int width = 0, height = 0, spp = 1, maxDepth = 1000, integrator = 0, filter = 0;

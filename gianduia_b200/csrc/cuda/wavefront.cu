@@ -401,29 +401,51 @@ __global__ void kBeginIter(KParams p) {
 }
 
 // Closest-hit source/sink over the active list (extend).
+// Shade class of a path after its extend query: integrator (0 path, 1 volpath) x material
+// class. Material classes 0..3 follow the material type (matte, plastic, conductor,
+// glass); class 4 holds misses, null-BSDF surfaces and volpath paths inside a medium
+// (which may scatter before reaching the surface).
+static_assert(kMatIndex == kMatClasses - 1, "the null-BSDF material type is the last material class");
+__device__ __forceinline__ uint32_t shadeClass(const SceneView& s, bool vol, int medium, int inst) {
+    uint32_t mc = kMatClasses - 1;
+    if (inst >= 0 && !(vol && medium >= 0)) mc = __ldg(s.instClass + inst);   // kMatIndex -> class 4
+    return (vol ? (uint32_t)kMatClasses : 0u) + mc;
+}
+
+// Closest-hit source/sink over the active list (extend). The store also records the
+// path's shade class in the hit record, for kClassify.
 struct ExtendSrc {
     const KParams* p;
     uint32_t n;
     uint32_t slot;
+    int32_t medium;
+    bool vol;
+    const SceneView* view;
     __device__ uint32_t count() const { return n; }
     __device__ bool load(uint32_t i, TRay& r, const SceneView*& sv, const uint8_t*& nm) {
         slot = p->listIn[i];
         const PathState* ps = p->paths + slot;
         float4 a = *reinterpret_cast<const float4*>(&ps->ox);
         float4 b = *reinterpret_cast<const float4*>(&ps->dx);
-        uint32_t job = ps->flags >> 8;
+        uint4 c = *reinterpret_cast<const uint4*>(&ps->bounces);   // bounces, vsBounces, medium, flags
+        const uint32_t job = c.w >> 8;
+        const JobDev& jd = p->jobs[job];
+        medium = (int32_t)c.z;
+        vol = jd.integrator == 1;
         r.o = v3(a.x, a.y, a.z);
         r.d = v3(b.x, b.y, b.z);
         r.tmin = kEpsilon;
         r.tmax = INFINITY;
-        sv = &p->jobs[job].view;
+        view = &jd.view;
+        sv = view;
         nm = nullptr;
         return true;
     }
     __device__ void store(uint32_t, const THit& h) {
         HitRec hr;
         hr.t = h.t; hr.u = h.u; hr.v = h.v; hr.inst = h.inst; hr.slot = h.slot;
-        hr.pad[0] = hr.pad[1] = hr.pad[2] = 0;
+        hr.pad[0] = shadeClass(*view, vol, medium, h.inst);
+        hr.pad[1] = hr.pad[2] = 0;
         p->hits[slot] = hr;
     }
 };
@@ -460,18 +482,7 @@ __global__ void __launch_bounds__(kBlock) kClassify(KParams p, uint32_t* classLi
         uint32_t cls = 0xFFFFFFFFu, slot = 0;
         if (valid) {
             slot = p.listIn[i];
-            const PathState* ps = p.paths + slot;
-            const uint32_t jobIdx = ps->flags >> 8;
-            const int medium = ps->medium;
-            const JobDev& j = p.jobs[jobIdx];
-            const int inst = p.hits[slot].inst;
-            const uint32_t vol = j.integrator == 1 ? 1u : 0u;
-            uint32_t mc = kMatClasses - 1;
-            if (inst >= 0 && !(vol && medium >= 0)) {
-                uint32_t t = j.view.materials[j.view.instS[inst].material].type;
-                mc = t < (uint32_t)(kMatClasses - 1) ? t : (uint32_t)(kMatClasses - 1);
-            }
-            cls = vol * kMatClasses + mc;
+            cls = p.hits[slot].pad[0];   // written by the extend store (shadeClass)
         }
         const uint32_t grp = __match_any_sync(0xffffffffu, cls);
         if (valid) {
@@ -1361,7 +1372,7 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
     else launchTraversal<32>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0);
     if (sort) {
         uint32_t* cls = classes_.as<uint32_t>();
-        kClassify<<<grid, kBlock, 0, st>>>(kp, cls);
+        kClassify<<<ctx_->numSMs * 16, kBlock, 0, st>>>(kp, cls);   // latency-bound: a full SM of warps
         if (mix & 1) launchShade<false>(kp, cls, grid, st);
         if (mix & 2) launchShade<true>(kp, cls, grid, st);
     } else if (mix == 2) {

@@ -151,6 +151,7 @@ struct SceneView {
     const MeshRec* meshes;
     const float* cdf;
     const uint32_t* origToLeaf;
+    const uint8_t* instClass;     // per instance: material type, kMatIndex for null-BSDF ones
     uint32_t tlasRoot;            // kEmpty when the scene has no primitives
     int32_t numEmitters;
     int32_t numInstances;
