@@ -77,6 +77,7 @@ def lib():
                 "gnd_gpu_serve_wait": [_vp, ctypes.c_uint64, _vp, _vp, ctypes.c_int64],
                 "gnd_gpu_serve_cancel": [_vp, ctypes.c_uint64],
                 "gnd_gpu_serve_policy": [_vp, ctypes.c_int32],
+                "gnd_gpu_serve_tune": [_vp, _vp],
                 "gnd_gpu_read_bandwidth": [_vp, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)],
                 "gnd_gpu_get_tune": [_vp, ctypes.c_uint64, _vp],
                 "gnd_gpu_set_tune": [_vp, ctypes.c_uint64, _vp],
@@ -326,6 +327,14 @@ class GpuContext:
         code = {"fifo": 0, "srpt": 1, "deadline": 2}[policy]
         _check(lib().gnd_gpu_serve_policy(self._h, code), "gnd_gpu_serve_policy")
 
+    def serve_tune(self, **fields):
+        """Engine settings of the serving thread (the defaults of gnd_tune, updated by fields)."""
+        t = Tune(pool_log2=22, round_iters=8, trav_blocks=8, material_sort=1, stack_smem=32, graphs=1, sample_film=1,
+                 spec_extend=1, spec_shadow=1)
+        for k, v in fields.items():
+            setattr(t, k, int(v))
+        _check(lib().gnd_gpu_serve_tune(self._h, ctypes.byref(t)), "gnd_gpu_serve_tune")
+
     def set_hbm_budget(self, nbytes):
         _check(lib().gnd_gpu_set_hbm_budget(self._h, int(nbytes)), "gnd_gpu_set_hbm_budget")
 
@@ -392,7 +401,7 @@ class RenderStats(ctypes.Structure):
 class Tune(ctypes.Structure):
     _fields_ = [("pool_log2", ctypes.c_int32), ("round_iters", ctypes.c_int32), ("trav_blocks", ctypes.c_int32),
                 ("material_sort", ctypes.c_int32), ("stack_smem", ctypes.c_int32), ("graphs", ctypes.c_int32),
-                ("sample_film", ctypes.c_int32)]
+                ("sample_film", ctypes.c_int32), ("spec_extend", ctypes.c_int32), ("spec_shadow", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}

@@ -525,7 +525,7 @@ __device__ __forceinline__ uint32_t warpFetch(uint32_t* counter, bool want) {
 //   uint32_t count()                      number of rays
 //   bool load(uint32_t i, TRay&, const SceneView*&, const uint8_t*& nullMask)
 //   void store(uint32_t i, const THit&)   (closest) / store(i, bool) (any)
-template <int BLOCK, bool ANY, bool COUNT, int SMEM = kSmemStack, typename Src>
+template <int BLOCK, bool ANY, bool COUNT, int SMEM = kSmemStack, bool SPEC = false, typename Src>
 __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter, uint32_t* smemStack, TraceCounters* cnt) {
     TStack<BLOCK, SMEM> st;
     st.smem = smemStack + threadIdx.x;
@@ -554,9 +554,24 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
             }
         }
         if (!__any_sync(0xffffffffu, active)) break;
-        // node phase
+        // node phase. Without SPEC a lane steps until it holds a leaf. With SPEC every lane
+        // steps until it is blocked: a lane that holds a leaf keeps traversing ahead while
+        // its next entry is an inner node of the same tree, and stops at the next leaf,
+        // sentinel or an empty stack (more lanes busy per step, at the price of visits a
+        // shorter tMax would have culled). Either way whether a lane steps depends only on
+        // its own state, so each ray's sequence of visits, and its result, is the same
+        // whatever the other rays of the warp do.
         for (;;) {
-            bool want = active && t.leaf == kEmpty && (t.next != kEmpty || t.sp > 0);
+            const bool work = t.next != kEmpty || t.sp > 0;
+            bool want = active && work;
+            if (want && t.leaf != kEmpty) {
+                if (!SPEC) {
+                    want = false;
+                } else {
+                    const uint32_t peek = t.next != kEmpty ? t.next : st.get(t.sp - 1);
+                    want = peek != kSentinel && !isLeaf(peek);
+                }
+            }
             if (!__any_sync(0xffffffffu, want)) break;
             if (want) {
                 int e = travNodeStep<BLOCK, COUNT, SMEM>(t, *sv, st, cnt);

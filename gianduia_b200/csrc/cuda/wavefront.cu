@@ -450,14 +450,14 @@ struct ExtendSrc {
     }
 };
 
-template <bool COUNT, int SMEM>
+template <bool COUNT, int SMEM, bool SPEC>
 __global__ void __launch_bounds__(kBlock, 8) kExtend(KParams p) {
     __shared__ uint32_t stack[SMEM * kBlock];
     const uint32_t n = p.cnt[kQIn];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[0], (unsigned long long)n);
     TraceCounters cnt{0, 0};
     ExtendSrc src{&p, n, 0};
-    int err = persistentTrace<kBlock, false, COUNT, SMEM>(src, p.cnt + kQFetchA, stack, &cnt);
+    int err = persistentTrace<kBlock, false, COUNT, SMEM, SPEC>(src, p.cnt + kQFetchA, stack, &cnt);
     if (COUNT) {
         unsigned long long nn = cnt.nodes, nt = cnt.tris;
         for (int o = 16; o > 0; o >>= 1) {
@@ -736,13 +736,13 @@ struct ShadowSrc {
     }
 };
 
-template <bool ANY, int SMEM>
+template <bool ANY, int SMEM, bool SPEC>
 __global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p, bool mixed) {
     __shared__ uint32_t stack[SMEM * kBlock];
     const uint32_t n = p.cnt[kQShadow];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
     ShadowSrc<ANY> src{&p, n, 0, nullptr, mixed};
-    int err = persistentTrace<kBlock, ANY, false, SMEM>(src, p.cnt + kQFetchB, stack, nullptr);
+    int err = persistentTrace<kBlock, ANY, false, SMEM, SPEC>(src, p.cnt + kQFetchB, stack, nullptr);
     if (err) atomicOr(p.errWord, (uint32_t)err);
 }
 
@@ -1327,19 +1327,28 @@ void Wavefront::drop(int j) {
     syncActive();
 }
 
-// The traversal kernels for one shared-stack size.
-template <int SMEM>
+// The traversal kernels for one shared-stack size and speculation setting.
+template <int SMEM, bool SPEC>
 static void launchTraversal(const KParams& kp, int mix, bool hasNull, bool count, int travGrid, cudaStream_t st,
                             cudaEvent_t ea, cudaEvent_t eb, int stage) {
     if (stage == 0) {
         if (ea) GND_CUDA(cudaEventRecord(ea, st));
-        if (count) kExtend<true, SMEM><<<travGrid, kBlock, 0, st>>>(kp);
-        else kExtend<false, SMEM><<<travGrid, kBlock, 0, st>>>(kp);
+        // the instrumented variant counts the visits of plain nearest-first order: the
+        // algorithmic work of a ray, independent of speculation
+        if (count) kExtend<true, SMEM, false><<<travGrid, kBlock, 0, st>>>(kp);
+        else kExtend<false, SMEM, SPEC><<<travGrid, kBlock, 0, st>>>(kp);
         if (eb) GND_CUDA(cudaEventRecord(eb, st));
     } else if (mix & 1) {
-        if (hasNull) kShadowPath<false, SMEM><<<travGrid, kBlock, 0, st>>>(kp, mix == 3);
-        else kShadowPath<true, SMEM><<<travGrid, kBlock, 0, st>>>(kp, mix == 3);
+        if (hasNull) kShadowPath<false, SMEM, SPEC><<<travGrid, kBlock, 0, st>>>(kp, mix == 3);
+        else kShadowPath<true, SMEM, SPEC><<<travGrid, kBlock, 0, st>>>(kp, mix == 3);
     }
+}
+
+template <int SMEM>
+static void launchTraversal(const KParams& kp, int mix, bool hasNull, bool count, int travGrid, cudaStream_t st,
+                            cudaEvent_t ea, cudaEvent_t eb, int stage, bool spec) {
+    if (spec) launchTraversal<SMEM, true>(kp, mix, hasNull, count, travGrid, st, ea, eb, stage);
+    else launchTraversal<SMEM, false>(kp, mix, hasNull, count, travGrid, st, ea, eb, stage);
 }
 
 void Wavefront::setTune(const Tune& t) {
@@ -1368,8 +1377,8 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
         evs_.push_back(eb);
     }
     const bool count = (profile & 2) != 0;
-    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0);
-    else launchTraversal<32>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0);
+    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0);
+    else launchTraversal<32>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0);
     if (sort) {
         uint32_t* cls = classes_.as<uint32_t>();
         kClassify<<<ctx_->numSMs * 16, kBlock, 0, st>>>(kp, cls);   // latency-bound: a full SM of warps
@@ -1380,8 +1389,8 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
     } else {
         kShade<false, kLobesAll><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
     }
-    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1);
-    else launchTraversal<32>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1);
+    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0);
+    else launchTraversal<32>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0);
     if (mix & 2) kShadow<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
     kRetire<<<ctx_->numSMs * 12, kBlock, 0, st>>>(kp);   // 12 blocks per SM: its register limit
     kEndIter<<<1, 1, 0, st>>>(kp.cnt);
@@ -1655,6 +1664,8 @@ static Tune tuneFromC(const gnd_tune& t) {
     if (t.stack_smem != 16 && t.stack_smem != 32) throw Error(GND_ERR_INVALID, "stack_smem must be 16 or 32");
     if (t.graphs != 0 && t.graphs != 1) throw Error(GND_ERR_INVALID, "graphs must be 0 or 1");
     if (t.sample_film != 0 && t.sample_film != 1) throw Error(GND_ERR_INVALID, "sample_film must be 0 or 1");
+    if (t.spec_extend != 0 && t.spec_extend != 1) throw Error(GND_ERR_INVALID, "spec_extend must be 0 or 1");
+    if (t.spec_shadow != 0 && t.spec_shadow != 1) throw Error(GND_ERR_INVALID, "spec_shadow must be 0 or 1");
     Tune r;
     r.poolLog2 = t.pool_log2;
     r.roundIters = t.round_iters;
@@ -1663,6 +1674,8 @@ static Tune tuneFromC(const gnd_tune& t) {
     r.smem = t.stack_smem;
     r.graphs = t.graphs;
     r.sampleFilm = t.sample_film;
+    r.specExtend = t.spec_extend;
+    r.specShadow = t.spec_shadow;
     return r;
 }
 
@@ -1675,6 +1688,8 @@ static gnd_tune tuneToC(const Tune& t) {
     r.stack_smem = t.smem;
     r.graphs = t.graphs;
     r.sample_film = t.sampleFilm;
+    r.spec_extend = t.specExtend;
+    r.spec_shadow = t.specShadow;
     return r;
 }
 
@@ -1694,6 +1709,17 @@ gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_tune* 
         const Tune v = tuneFromC(*t);
         std::lock_guard<FairMutex> lk(c->mu);
         c->scene(id).tune = v;
+    });
+}
+
+gnd_status gnd_gpu_serve_tune(gnd_gpu_ctx* ctxh, const gnd_tune* t) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (!t) throw Error(GND_ERR_INVALID, "null tune");
+        Tune v = tuneFromC(*t);
+        v.sort = 1;   // served jobs of both integrators share launches: always sorted
+        std::lock_guard<FairMutex> lk(c->mu);
+        c->serveTune = v;
     });
 }
 
@@ -1732,7 +1758,7 @@ gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t spp, int
         const std::vector<Knob> knobs = {
             {&Tune::travBlocks, {8, 6, 4}}, {&Tune::smem, {32, 16}},          {&Tune::sort, {1, 0}},
             {&Tune::poolLog2, {22, 21, 23, 20}}, {&Tune::roundIters, {8, 16, 4}}, {&Tune::graphs, {1, 0}},
-            {&Tune::sampleFilm, {1, 0}},
+            {&Tune::sampleFilm, {1, 0}}, {&Tune::specExtend, {1, 0}}, {&Tune::specShadow, {1, 0}},
         };
         for (int sweep = 0; sweep < 2; ++sweep) {
             bool changed = false;

@@ -122,7 +122,9 @@ def run_plain_service(ctx, sids, integrators, reqs):
 
 def calibrate_capacity(ctx, sids, integrators, n=24, seed=40):
     """Requests per second the job server sustains: n requests of the same distribution
-    submitted at once, n / makespan."""
+    submitted at once, n / makespan, timed on a second submission (the first one warms the
+    server up: its path pool, the kernels' first loads and the captured graphs)."""
     reqs = make_requests(n, seed)
+    run_served(ctx, sids, integrators, reqs, np.zeros(n))
     _, makespan = run_served(ctx, sids, integrators, reqs, np.zeros(n))
     return n / makespan, sum(samples(r) for r in reqs) / makespan

@@ -229,6 +229,9 @@ typedef struct gnd_tune {
     int32_t sample_film;      /* 1: batched renders with the box filter write one record per
                                  sample and build the film from them afterwards (no film
                                  atomics; needs 16 bytes of HBM per sample); 0: atomics */
+    int32_t spec_extend;      /* 1: closest-hit traversal lets a ray that holds a leaf keep
+                                 visiting inner nodes until it is blocked (speculative) */
+    int32_t spec_shadow;      /* the same for the shadow (occlusion) traversal */
 } gnd_tune;
 gnd_status gnd_gpu_get_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_tune* tune);
 gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_tune* tune);
@@ -284,6 +287,10 @@ gnd_status gnd_gpu_set_hbm_budget(gnd_gpu_ctx* ctx, uint64_t bytes);
  * Admission is first-come first-served under every policy. */
 enum { GND_SERVE_FIFO = 0, GND_SERVE_SRPT = 1, GND_SERVE_DEADLINE = 2 };
 gnd_status gnd_gpu_serve_policy(gnd_gpu_ctx* ctx, int32_t policy);
+/* Engine settings of the serving thread (gnd_tune; pool_log2 and round_iters are the
+ * server's own, and material_sort is always on because jobs of both integrators share
+ * launches). Like a scene's settings they change speed, never results. */
+gnd_status gnd_gpu_serve_tune(gnd_gpu_ctx* ctx, const gnd_tune* tune);
 /* Queues a job; returns at once with its id. The scene may not be freed while a job
  * that names it is queued or running (gnd_gpu_scene_free fails with GND_ERR_INVALID). */
 gnd_status gnd_gpu_serve_submit(gnd_gpu_ctx* ctx, const gnd_job_desc* job, gnd_job_id* id);
