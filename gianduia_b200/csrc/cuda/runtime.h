@@ -126,8 +126,8 @@ struct Tune {
     int smem = 32;            // traversal stack entries in shared memory (16 or 32)
     int graphs = 1;           // replay iteration pairs as CUDA graphs
     int sampleFilm = 1;       // batched box-filter renders: per-sample records, no film atomics
-    int specExtend = 1;       // speculative node traversal in the extend kernel
-    int specShadow = 1;       // speculative node traversal in the shadow kernel
+    int specExtend = 0;       // speculative node traversal in the extend kernel
+    int specShadow = 0;       // speculative node traversal in the shadow kernel
     bool operator==(const Tune& o) const {
         return poolLog2 == o.poolLog2 && roundIters == o.roundIters && travBlocks == o.travBlocks && sort == o.sort &&
                smem == o.smem && graphs == o.graphs && sampleFilm == o.sampleFilm && specExtend == o.specExtend &&

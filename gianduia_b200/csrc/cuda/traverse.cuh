@@ -476,6 +476,12 @@ __device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<
     if (kind == kShapeMesh) {
         uint32_t root = __float_as_uint(meta.y);
         if (root == kEmpty) return 0;
+        if (t.next != kEmpty) {
+            // an entry found by speculative traversal before this leaf: keep it for later
+            if (t.sp >= kPStackMax) return kTraceStackOverflow;
+            st.put(t.sp++, t.next);
+            t.next = kEmpty;
+        }
         if (t.leaf != kEmpty) {
             // the rest of this leaf comes back after the bottom-level tree
             if (t.sp >= kPStackMax) return kTraceStackOverflow;

@@ -230,7 +230,8 @@ typedef struct gnd_tune {
                                  sample and build the film from them afterwards (no film
                                  atomics; needs 16 bytes of HBM per sample); 0: atomics */
     int32_t spec_extend;      /* 1: closest-hit traversal lets a ray that holds a leaf keep
-                                 visiting inner nodes until it is blocked (speculative) */
+                                 visiting inner nodes until it is blocked (speculative);
+                                 default 0 */
     int32_t spec_shadow;      /* the same for the shadow (occlusion) traversal */
 } gnd_tune;
 gnd_status gnd_gpu_get_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_tune* tune);
