@@ -7,8 +7,10 @@
   python -m gianduia_b200.profile_run batched [spp]
                                                 the microfacet render in batched mode,
                                                 `spp` passes (default 1) sharing the pool
-  python -m gianduia_b200.profile_run volpath   one 1-spp pass of the 512x512 volumetric
-                                                Cornell box (volpath_gpu, depth 32)
+  python -m gianduia_b200.profile_run volpath [spp] [batched]
+                                                the 512x512 volumetric Cornell box
+                                                (volpath_gpu, depth 32), `spp` passes
+                                                (default 1), plain unless `batched`
   python -m gianduia_b200.profile_run all       trace, then render
 """
 import os
@@ -37,11 +39,11 @@ def run_render(ctx, batched=False, spp=1):
     ctx.free_scene(sid)
 
 
-def run_volpath(ctx):
+def run_volpath(ctx, spp=1, batched=False):
     xml = scenes.volumetric(os.path.join(tempfile.gettempdir(), "gnd_prof_volumetric"), width=512, height=512, spp=64,
                             max_depth=32)
     sid = ctx.upload(G.HostScene.load_xml(xml))
-    _, st = ctx.render(sid, spp=1)
+    _, st = ctx.render(sid, spp=spp, batched=batched)
     print("volpath:", st)
     ctx.free_scene(sid)
 
@@ -56,7 +58,7 @@ def main(argv):
     if what == "batched":
         run_render(ctx, batched=True, spp=int(argv[2]) if len(argv) > 2 else 1)
     if what == "volpath":
-        run_volpath(ctx)
+        run_volpath(ctx, spp=int(argv[2]) if len(argv) > 2 else 1, batched=len(argv) > 3 and argv[3] == "batched")
     ctx.close()
 
 

@@ -73,7 +73,7 @@ def test_cornell_same_stream(ctx, tmp_path):
     gfilm, st = ctx.render(sid, spp=4)
     ofilm, paths, rays = O.Scene.load(xml).render(0, 4)
     assert st["paths"] == paths == 64 * 64 * 4
-    same_stream_check(image(gfilm), image(ofilm), "cornell")
+    same_stream_check(image(gfilm), image(ofilm), "cornell", min_frac=0.995)   # measured: 100%
     # weights: one box-filter sample per pixel per pass
     assert np.allclose(gfilm[..., 3], 4.0) and np.allclose(ofilm[..., 3], 4.0)
 
@@ -97,7 +97,7 @@ def test_volumetric_same_stream(ctx, tmp_path):
     sid = ctx.upload(G.HostScene.load_xml(xml))
     gfilm, _ = ctx.render(sid, spp=4)
     ofilm, _, _ = O.Scene.load(xml).render(0, 4)
-    same_stream_check(image(gfilm), image(ofilm), "volumetric", min_frac=0.85)
+    same_stream_check(image(gfilm), image(ofilm), "volumetric", min_frac=0.995)   # measured: 99.96%
 
 
 def test_volumetric_statistics(ctx, tmp_path):
