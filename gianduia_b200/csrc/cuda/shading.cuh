@@ -293,6 +293,7 @@ __device__ __forceinline__ float roughPlasticPdf(const Lobe& l, V3 wo, V3 wi) {
 // Lobe kinds a kernel may meet, as a bitmask over Lobe::kind. Kernels specialised to one
 // material class pass its mask so the other lobes' code is not compiled in.
 constexpr uint32_t kLobesAll = 0x7Fu;
+constexpr uint32_t kLobesNone = 0u;   // the medium-only shade kernel: no surface lobes
 constexpr uint32_t kLobesMatte = 1u << 0;
 constexpr uint32_t kLobesConductor = (1u << 1) | (1u << 3);
 constexpr uint32_t kLobesGlass = (1u << 2) | (1u << 4);

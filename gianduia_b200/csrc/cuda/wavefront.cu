@@ -28,12 +28,15 @@ namespace gnd {
 constexpr int kBlock = 128;
 constexpr float kFixScale = 16777216.0f;   // 2^24
 constexpr float kFixMax = 1e11f;           // per-sample clamp before the fixed-point conversion
-// Shade classes: integrator (0 path, 1 volpath) x material class. Material classes 0..3
-// follow the material type (matte, plastic, conductor, glass); class 4 holds misses,
-// null-BSDF surfaces and volpath paths inside a medium (which may scatter before
-// reaching the surface), shaded by the kernel built with every lobe.
-constexpr int kMatClasses = 5;
-constexpr int kShadeClasses = 2 * kMatClasses;
+// Shade classes: integrator (0 path, 1 volpath) x class. Classes 0..3 follow the
+// material type (matte, plastic, conductor, glass); class 4 holds misses and null-BSDF
+// surfaces and is shaded by the kernel built with every lobe; class 5 (volpath only)
+// holds paths inside a medium, whose medium sampling runs first in its own kernel.
+constexpr int kMatClasses = 5;                       // surface classes 0..4
+constexpr int kMediumClass = 5;
+constexpr int kClassesPerInt = 6;
+constexpr int kShadeClasses = 2 * kClassesPerInt;
+constexpr uint32_t kFlagMediumDone = 2u;             // PathState::flags: medium sampled this bounce
 static_assert(kQClass0 + kShadeClasses <= kQCount, "class counters exceed the counter block");
 
 
@@ -80,6 +83,7 @@ struct KParams {
     uint32_t* freeIn;              // idle slots waiting for work
     uint32_t* freeOut;
     uint32_t* errWord;
+    uint32_t* classLists;          // shade-class lists, `capacity` entries each
     uint32_t capacity;
     uint32_t fifo;                 // 1: grabs walk the active list from its first job
 };
@@ -401,15 +405,15 @@ __global__ void kBeginIter(KParams p) {
 }
 
 // Closest-hit source/sink over the active list (extend).
-// Shade class of a path after its extend query: integrator (0 path, 1 volpath) x material
-// class. Material classes 0..3 follow the material type (matte, plastic, conductor,
-// glass); class 4 holds misses, null-BSDF surfaces and volpath paths inside a medium
-// (which may scatter before reaching the surface).
-static_assert(kMatIndex == kMatClasses - 1, "the null-BSDF material type is the last material class");
+// Shade class of a path after its extend query (see kMatClasses): volpath paths inside a
+// medium go to the medium class, others to their surface's class.
+static_assert(kMatIndex == kMatClasses - 1, "the null-BSDF material type is the last surface class");
+__device__ __forceinline__ uint32_t surfaceClass(const SceneView& s, int inst) {
+    return inst >= 0 ? (uint32_t)__ldg(s.instClass + inst) : (uint32_t)(kMatClasses - 1);   // kMatIndex -> 4
+}
 __device__ __forceinline__ uint32_t shadeClass(const SceneView& s, bool vol, int medium, int inst) {
-    uint32_t mc = kMatClasses - 1;
-    if (inst >= 0 && !(vol && medium >= 0)) mc = __ldg(s.instClass + inst);   // kMatIndex -> class 4
-    return (vol ? (uint32_t)kMatClasses : 0u) + mc;
+    const uint32_t c = (vol && medium >= 0) ? (uint32_t)kMediumClass : surfaceClass(s, inst);
+    return (vol ? (uint32_t)kClassesPerInt : 0u) + c;
 }
 
 // Closest-hit source/sink over the active list (extend). The store also records the
@@ -496,7 +500,10 @@ __global__ void __launch_bounds__(kBlock) kClassify(KParams p, uint32_t* classLi
 }
 
 // One bounce of path (VOL = false) or volpath (VOL = true) for the slots of one shade
-// class; M is the set of lobes the class can meet (every lobe for class 4).
+// class; M is the set of lobes the class can meet (every lobe for class 4). With
+// M = kLobesNone the kernel serves the medium class: it samples the medium, finishes the
+// bounce of paths that scatter in it, and hands each other path on to its surface
+// class (medium sampling marked done) for a surface kernel later in the iteration.
 template <bool VOL, uint32_t M>
 __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list, const uint32_t* count) {
     const uint32_t n = *count;
@@ -517,12 +524,12 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
         float pdfPrev = ps.pdfPrev;
         int medium = ps.medium;
         const float nL = (float)s.numEmitters;
-        bool cont = false, terminate = false, emitShadow = false;
+        bool cont = false, terminate = false, emitShadow = false, handOff = false;
         ShadowRec sr;
         const bool hit = h.inst >= 0;
 
         do {
-            if (VOL && M == kLobesAll && medium >= 0) {
+            if (VOL && (M == kLobesAll || M == kLobesNone) && medium >= 0 && !(ps.flags & kFlagMediumDone)) {
                 // medium->sample (homogeneous.cpp:32-63); the ray's tMax is the hit distance
                 const Medium m = s.media[medium];
                 float rtmax = hit ? h.t : INFINITY;
@@ -580,6 +587,12 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
                     cont = true;
                     break;
                 }
+            }
+            if (M == kLobesNone) {
+                // no scattering: the path reaches its surface (or escapes)
+                if (!hit) terminate = true;
+                else handOff = true;
+                break;
             }
             const int curMedium = medium;
             if (!hit) { terminate = true; break; }
@@ -683,8 +696,21 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
         ps.bounces = (bounces & 0xFFFFu) | (min(nullB, 0xFFFFu) << 16);
         ps.vsBounces = (volB & 0xFFFFu) | (surfB << 16);
         ps.medium = medium;
-        ps.flags = (ps.flags & ~1u) | (specular ? 1u : 0u);
+        ps.flags = (ps.flags & ~(1u | kFlagMediumDone)) | (specular ? 1u : 0u) | (handOff ? kFlagMediumDone : 0u);
         p.paths[slot] = ps;
+        if (M == kLobesNone) {
+            // hand-off to the surface class (warp-aggregated per class)
+            const uint32_t hc = handOff ? (uint32_t)kClassesPerInt + surfaceClass(s, h.inst) : 0xFFFFFFFFu;
+            const uint32_t grp = __match_any_sync(__activemask(), hc);
+            if (handOff) {
+                const int leader = __ffs(grp) - 1;
+                const int lane = threadIdx.x & 31;
+                uint32_t b = 0;
+                if (lane == leader) b = atomicAdd(&p.cnt[kQClass0 + hc], (uint32_t)__popc(grp));
+                b = __shfl_sync(grp, b, leader);
+                p.classLists[(size_t)hc * p.capacity + b + (uint32_t)__popc(grp & ((1u << lane) - 1u))] = slot;
+            }
+        }
         uint32_t k = warpAppend(&p.cnt[kQShadow], emitShadow);
         if (emitShadow) p.shadow[k] = sr;
         uint32_t c = warpAppend(&p.cnt[kQOut], cont);
@@ -1040,11 +1066,13 @@ __global__ void kResetPool(uint32_t* freeList, uint32_t n, uint32_t* cnt) {
 template <bool VOL>
 static void launchShade(const KParams& kp, uint32_t* classLists, int grid, cudaStream_t st) {
     const size_t cap = kp.capacity;
-    const int c0 = VOL ? kMatClasses : 0;
+    const int c0 = VOL ? kClassesPerInt : 0;
     uint32_t* cnt = kp.cnt + kQClass0 + c0;
     uint32_t* lists = classLists + (size_t)c0 * cap;
     static_assert(kMatMatte == 0 && kMatPlastic == 1 && kMatConductor == 2 && kMatGlass == 3,
                   "material classes follow the material type codes");
+    // medium sampling first: its hand-offs join the surface classes shaded below
+    if (VOL) kShade<true, kLobesNone><<<grid, kBlock, 0, st>>>(kp, lists + kMediumClass * cap, cnt + kMediumClass);
     kShade<VOL, kLobesMatte><<<grid, kBlock, 0, st>>>(kp, lists + 0 * cap, cnt + 0);
     kShade<VOL, kLobesPlastic><<<grid, kBlock, 0, st>>>(kp, lists + 1 * cap, cnt + 1);
     kShade<VOL, kLobesConductor><<<grid, kBlock, 0, st>>>(kp, lists + 2 * cap, cnt + 2);
@@ -1453,12 +1481,13 @@ void Wavefront::enqueueRound(int iters, int mix, bool hasNull, int profile, Resu
     kp.active = active_.as<uint32_t>();
     kp.errWord = c->errWord.as<uint32_t>();
     kp.capacity = (uint32_t)cap_;
+    kp.classLists = classes_.as<uint32_t>();
     kp.fifo = fifo_ ? 1u : 0u;
     // begin, extend, retire, end; classify + 5 shade kernels per integrator when sorting (one
     // shade kernel otherwise); 1 shadow kernel per integrator
     const bool sort = tune_.sort != 0 || mix == 3;
     const int nint = (mix & 1 ? 1 : 0) + (mix & 2 ? 1 : 0);
-    const int perIter = 4 + nint + (sort ? 1 + 5 * nint : 1);
+    const int perIter = 4 + nint + (sort ? 1 + 5 * nint + ((mix & 2) ? 1 : 0) : 1);   // + the medium kernel
     int it = 0;
     while (it < iters) {
         if (tune_.graphs && profile == 0 && iters - it >= 2) {
