@@ -202,7 +202,12 @@ struct Context {
     // jobs per scene (a scene in use cannot be freed), and the job server (created on
     // the first submit; serverMu guards its creation)
     uint64_t hbmBudget = 0;
-    Tune serveTune;           // engine settings of the serving thread (pool and round size are its own)
+    Tune serveTune = serveDefaults();   // engine settings of the serving thread (its own pool size)
+    static Tune serveDefaults() {
+        Tune t;
+        t.roundIters = 4;   // short rounds: jobs are admitted and finished between rounds
+        return t;
+    }
     std::map<uint64_t, int> sceneUse;
     std::mutex serverMu;
     std::unique_ptr<Server> server;

@@ -245,6 +245,7 @@ void Server::loop() {
                     continue;
                 }
                 j->slot = slot;
+                j->firstRound = enqRound_;   // the next round queued is the first to include it
                 j->state = GND_JOB_RUNNING;
                 j->tAdmit = nowMs();
                 running_.push_back(j);
@@ -269,13 +270,26 @@ void Server::loop() {
                 mix |= j->integ == 1 ? 2 : 1;
                 if (j->integ == 0 && c_->scene(j->scene).hasNullMaterials) hasNull = true;
             }
+            const int iters = std::min(std::max(c_->serveTune.roundIters & ~1, 2), 64);
+            applyPriorities(run);   // newly admitted jobs take their place before the next round
             Wavefront::Result acc;
-            wf.step(kItersPerRound, mix, hasNull, 0, acc);
-            c_->checkKernelErrors("serve");
-            wf.readCtl(ctl);
-            ++round_;
+            auto enqueue = [&]() {
+                const int slot = inflight_ ? (inflightSlot_ ^ 1) : inflightSlot_;
+                wf.enqueueRound(iters, mix, hasNull, 0, acc, slot);
+                slotRound_[slot] = enqRound_++;
+                inflightSlot_ = slot;
+                inflight_ = true;
+            };
+            if (!inflight_) enqueue();
+            const int readSlot = inflightSlot_;
+            enqueue();   // the next round runs while this one's counters are read
+            const Wavefront::Snapshot& sn = wf.waitRound(readSlot);
+            const int64_t q = slotRound_[readSlot];
+            if (sn.err) c_->checkKernelErrors("serve");
+            std::vector<JobCtl> ctl(sn.ctl, sn.ctl + kMaxJobs);
             uint64_t retiredSum = 0;
             for (ServeJob* j : run) {
+                if (q < j->firstRound) continue;   // a round queued before the job's admission
                 const JobCtl& k = ctl[j->slot];
                 retiredSum += k.retired;
                 bool cancelNow = false;
@@ -285,54 +299,79 @@ void Server::loop() {
                     cancelNow = j->cancelReq && j->stopRound < 0;
                 }
                 if (cancelNow) {
-                    wf.stop(j->slot);   // stream-ordered before the next round's kernels
-                    j->stopRound = round_;
+                    wf.stop(j->slot);        // stream-ordered after the round in flight
+                    j->stopRound = enqRound_;   // rounds from here on see the final hand-out
                     continue;
                 }
-                if (j->stopRound >= 0 && j->stopRound < round_) {
-                    // hand-out stopped a round ago: `next` is final
-                    const uint64_t handed = std::min<uint64_t>(k.next, j->total);
-                    if (k.retired >= handed) finishJob(j, GND_JOB_CANCELLED);
-                } else if (j->stopRound < 0 && k.retired >= j->total) {
+                if (j->stopRound >= 0) {
+                    if (q >= j->stopRound) {
+                        const uint64_t handed = std::min<uint64_t>(k.next, j->total);
+                        if (k.retired >= handed) finishJob(j, GND_JOB_CANCELLED);
+                    }
+                } else if (k.retired >= j->total) {
                     finishJob(j, GND_JOB_DONE);
                 }
             }
             // sample rate of the server (retired samples per ms of round), for deadlines
             const double now = nowMs();
-            if (lastRoundMs_ >= 0.0 && retiredSum > lastRetiredSum_ && now > lastRoundMs_)
-                rate_ = 0.9 * rate_ + 0.1 * (double)(retiredSum - lastRetiredSum_) / (now - lastRoundMs_);
-            lastRoundMs_ = now;
-            if (policy_ != GND_SERVE_FIFO) {
-                std::vector<std::pair<int, uint64_t>> keys;
-                {
-                    std::lock_guard<std::mutex> lk(m_);
-                    for (ServeJob* j : running_) {
-                        if (policy_ == GND_SERVE_SRPT) {
-                            // the job with the fewest samples left to hand out first
-                            const uint64_t handed = std::min<uint64_t>(ctl[j->slot].next, j->total);
-                            keys.emplace_back(j->slot, j->total - handed);
-                        } else {
-                            // earliest deadline first (microseconds of the server clock)
-                            const double deadline = j->tSubmit + kDeadlineSlack * (double)j->total / std::max(rate_, 1.0);
-                            keys.emplace_back(j->slot, (uint64_t)(deadline * 1000.0));
-                        }
-                    }
-                }
-                wf.setPriorities(keys);
+            // from the engine's own count of retired paths over windows of at least 50 ms
+            // (rounds read back to back would give meaningless rates); the count restarts
+            // when the pool is reset, and an idle gap starts a new window
+            if (lastRoundMs_ < 0.0 || sn.retiredAll < lastRetiredAll_ || now - lastRoundMs_ > 500.0) {
+                lastRoundMs_ = now;
+                lastRetiredAll_ = sn.retiredAll;
+            } else if (now - lastRoundMs_ >= 50.0) {
+                rate_ = 0.7 * rate_ + 0.3 * (double)(sn.retiredAll - lastRetiredAll_) / (now - lastRoundMs_);
+                lastRoundMs_ = now;
+                lastRetiredAll_ = sn.retiredAll;
             }
+            lastCtl_ = ctl;
+            lastRound_ = q;
             if (retiredSum != lastRetiredSum_) {
                 lastRetiredSum_ = retiredSum;
                 itersSinceProgress_ = 0;
-            } else if ((itersSinceProgress_ += kItersPerRound) > kStallIters) {
+            } else if ((itersSinceProgress_ += iters) > kStallIters) {
                 failRunning("no sample retired in " + std::to_string(kStallIters) + " iterations", GND_ERR_DEVICE_CHECK);
                 itersSinceProgress_ = 0;
             }
         } catch (const Error& e) {
             failRunning(e.what(), e.code);
+            drainPipeline();
         } catch (const std::exception& e) {
             failRunning(e.what(), GND_ERR_CUDA);
+            drainPipeline();
         }
     }
+}
+
+// Hand-out order of the running jobs for the rounds queued next (FIFO: admission order,
+// set at admission). Counters come from the last snapshot that includes the job; a job
+// admitted since has handed out nothing.
+void Server::applyPriorities(const std::vector<ServeJob*>& run) {
+    if (policy_ == GND_SERVE_FIFO) return;
+    std::vector<std::pair<int, uint64_t>> keys;
+    for (ServeJob* j : run) {
+        if (policy_ == GND_SERVE_SRPT) {
+            // the job with the fewest samples left to hand out first
+            const bool seen = lastRound_ >= j->firstRound && j->slot >= 0 && (size_t)j->slot < lastCtl_.size();
+            const uint64_t handed = seen ? std::min<uint64_t>(lastCtl_[j->slot].next, j->total) : 0;
+            keys.emplace_back(j->slot, j->total - handed);
+        } else {
+            // earliest deadline first (microseconds of the server clock)
+            const double deadline = j->tSubmit + kDeadlineSlack * (double)j->total / std::max(rate_, 1.0);
+            keys.emplace_back(j->slot, (uint64_t)(deadline * 1000.0));
+        }
+    }
+    c_->wave->setPriorities(keys);
+}
+
+// After a failure: wait for whatever is queued (ignoring its errors) and restart the
+// round pipeline.
+void Server::drainPipeline() {
+    cudaStreamSynchronize(c_->stream);
+    cudaGetLastError();
+    inflight_ = false;
+    slotRound_[0] = slotRound_[1] = -1;
 }
 
 void Server::setPolicy(int policy) {

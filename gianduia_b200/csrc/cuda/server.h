@@ -5,6 +5,7 @@
 // host memory. Freed slots take the oldest admitted job's next samples, so the pool stays
 // full across job boundaries instead of draining at the end of every image.
 #pragma once
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -15,6 +16,7 @@
 #include <vector>
 
 #include "runtime.h"
+#include "wavefront.h"
 
 namespace gnd {
 
@@ -27,7 +29,8 @@ struct ServeJob {
     uint64_t total = 0, done = 0;
     uint64_t filmBytes = 0;          // device film bytes while running
     bool cancelReq = false;
-    int stopRound = -1;              // server round in which hand-out was stopped
+    int64_t firstRound = 0;          // first engine round whose counters include the job
+    int64_t stopRound = -1;          // first round queued after its hand-out was stopped
     double tSubmit = 0, tAdmit = 0, tDone = 0;
     std::vector<float> film;         // H x W x 7 once finished
     gnd_status status = GND_OK;
@@ -37,7 +40,6 @@ struct ServeJob {
 class Server {
 public:
     static constexpr size_t kPoolSlots = size_t(1) << 22;   // 4M path slots (~1 GB)
-    static constexpr int kItersPerRound = 4;
     static constexpr int64_t kStallIters = 20000;           // iterations without a retired sample
 
     explicit Server(Context* c);
@@ -56,6 +58,8 @@ private:
     bool fitsLocked(const ServeJob& j) const;                // caller holds the context mutex
     void finishJob(ServeJob* j, int state);
     void failRunning(const std::string& why, gnd_status code);
+    void drainPipeline();
+    void applyPriorities(const std::vector<ServeJob*>& run);   // caller holds the context mutex
 
     Context* c_;
     std::thread thread_;
@@ -66,11 +70,18 @@ private:
     std::vector<ServeJob*> running_;
     gnd_job_id nextId_ = 1;
     bool stop_ = false;
-    int round_ = 0;
-    int policy_ = GND_SERVE_DEADLINE;
+    // Rounds are queued one ahead: round q+1 runs while the host reads round q's counters.
+    int64_t enqRound_ = 0;                                   // index of the next round to queue
+    int64_t slotRound_[2] = {-1, -1};                        // round held by each snapshot slot
+    int inflightSlot_ = 0;
+    bool inflight_ = false;
+    std::vector<JobCtl> lastCtl_;                            // job counters of the last snapshot read
+    int64_t lastRound_ = -1;                                 // its round
+    std::atomic<int> policy_{GND_SERVE_DEADLINE};
     static constexpr double kDeadlineSlack = 4.0;
     double rate_ = 1e5;                                      // samples per ms, running estimate
     double lastRoundMs_ = -1.0;
+    unsigned long long lastRetiredAll_ = 0;
     int64_t itersSinceProgress_ = 0;
     uint64_t lastRetiredSum_ = 0;
     const std::chrono::steady_clock::time_point t0_;

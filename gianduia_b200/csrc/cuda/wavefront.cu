@@ -1504,6 +1504,8 @@ void Wavefront::enqueueRound(int iters, int mix, bool hasNull, int profile, Resu
         }
     }
     GND_CUDA(cudaMemcpyAsync(&snaps_[slot].inflight, kp.cnt + kQIn, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GND_CUDA(cudaMemcpyAsync(&snaps_[slot].err, kp.errWord, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GND_CUDA(cudaMemcpyAsync(&snaps_[slot].retiredAll, kp.totals + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     GND_CUDA(cudaMemcpyAsync(snaps_[slot].ctl, ctl_.ptr, kMaxJobs * sizeof(JobCtl), cudaMemcpyDeviceToHost, st));
     GND_CUDA(cudaEventRecord(snapEv_[slot], st));
 }

@@ -130,7 +130,8 @@ public:
     // for round k keeps the GPU busy while the host reads the counters.
     struct alignas(16) Snapshot {
         uint32_t inflight;            // active paths after the round
-        uint32_t pad[3];
+        uint32_t err;                 // the context's kernel error word after the round
+        unsigned long long retiredAll;   // paths retired by the engine since its pool was reset
         JobCtl ctl[kMaxJobs];         // per job: work items handed out, samples retired
     };
     void enqueueRound(int iters, int integratorMix, bool hasNull, int profile, Result& acc, int slot);
