@@ -26,6 +26,13 @@ _STATUS = {1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4:
 
 RAY_DTYPE = np.dtype([("o", np.float32, 3), ("tmin", np.float32), ("d", np.float32, 3), ("tmax", np.float32)])
 HIT_DTYPE = np.dtype([("t", np.float32), ("u", np.float32), ("v", np.float32), ("inst", np.int32), ("prim", np.int32)])
+# Camera record of a flattened scene (gnd::Camera, 112 bytes): kind 0 pinhole, 1 thin lens
+CAMERA_DTYPE = np.dtype([("to_world", np.float32, (3, 4)), ("width", np.int32), ("height", np.int32),
+                         ("scale", np.float32), ("aspect", np.float32), ("origin", np.float32, 3), ("pad", np.float32),
+                         ("kind", np.int32), ("blades", np.int32), ("lens_radius", np.float32),
+                         ("focal_distance", np.float32), ("k1", np.float32), ("ca_axial", np.float32),
+                         ("ca_lateral", np.float32), ("vignetting", np.int32)])
+assert CAMERA_DTYPE.itemsize == 112
 
 
 class GndError(RuntimeError):
@@ -135,6 +142,12 @@ class HostScene:
         h = _vp()
         _check(lib().gnd_host_from_triangles(tris.ctypes.data, tris.shape[0], ctypes.byref(h)), "gnd_host_from_triangles")
         return HostScene(h.value)
+
+    def camera(self):
+        """The flattened camera record (CAMERA_DTYPE), or None for a scene without one."""
+        if not self.desc.camera:
+            return None
+        return np.frombuffer(ctypes.string_at(self.desc.camera, CAMERA_DTYPE.itemsize), CAMERA_DTYPE)[0]
 
     def pin(self, on=True):
         """Page-locks (or releases) the large host arrays so uploads run at DMA speed."""

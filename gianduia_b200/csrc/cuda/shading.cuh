@@ -58,6 +58,21 @@ __device__ __forceinline__ V2 squareToUniformDisk(V2 s) {
     }
     return V2{r * cosf(theta), r * sinf(theta)};
 }
+// warp.cpp:86-113: a regular polygon with one corner at the top, sampled by picking one of
+// its `blades` triangles around the centre with s.x and a point in it
+__device__ __forceinline__ V2 squareToUniformPolygon(V2 s, int blades) {
+    if (blades < 3) return squareToUniformDisk(s);
+    const float bladeFloat = s.x * (float)blades;
+    const int bladeIdx = min((int)bladeFloat, blades - 1);
+    const float u0 = bladeFloat - (float)bladeIdx, u1 = s.y;
+    const float deltaTheta = 2.0f * kPi / (float)blades;
+    const float offset = kPi / 2.0f;
+    const float theta1 = (float)bladeIdx * deltaTheta + offset;
+    const float theta2 = (float)(bladeIdx + 1) * deltaTheta + offset;
+    const float c1 = cosf(theta1), s1 = sinf(theta1), c2 = cosf(theta2), s2 = sinf(theta2);
+    const float r = sqrtf(u0);
+    return V2{r * ((1.0f - u1) * c1 + u1 * c2), r * ((1.0f - u1) * s1 + u1 * s2)};
+}
 __device__ __forceinline__ V3 squareToUniformSphere(V2 s) {
     // squareToUniformSphereCap(s, -1): theta = acos(1 - 2 s.x), phi = 2 pi s.y (double)
     float theta = acosf(1.0f - (1.0f - (-1.0f)) * s.x);

@@ -345,6 +345,65 @@ __device__ __forceinline__ Rng loadRng(const PathState& ps) {
     return Rng{((uint64_t)ps.rngHi << 32) | ps.rngLo};
 }
 
+// ---------------------------------------------------------------- camera
+// Colour channel of a camera sample (integrator.h:103-121): -1 without chromatic
+// aberration (thinLens.cpp:97-99), else 0/1/2 from the sample's channel number, with the
+// wavelength offset +1/0/-1 the lens equations scale by.
+__device__ __forceinline__ int cameraChannel(const Camera& cam, float chRnd, float& lambda) {
+    lambda = 0.0f;
+    if (cam.kind != kCamThinLens || (cam.caLateral == 0.0f && cam.caAxial == 0.0f)) return -1;
+    if (chRnd < 0.333333f) { lambda = 1.0f; return 0; }
+    if (chRnd < 0.666666f) return 1;
+    lambda = -1.0f;
+    return 2;
+}
+
+// Thin-lens camera ray in camera space (thinLens.cpp:33-91) for the film position (cx, cy)
+// in [0,1]^2: barrel distortion, lateral / axial chromatic aberration, depth of field
+// through a disk or polygon aperture. Returns the ray weight (cos^4 vignetting or 1).
+// The shutter terms only change the sample time, which static transforms ignore.
+__device__ __forceinline__ float thinLensRay(const Camera& cam, float cx, float cy, V2 lens, float lambda,
+                                             V3& o, V3& dir) {
+    const float ndcX = 2.0f * cx - 1.0f, ndcY = 2.0f * cy - 1.0f;
+    const float r2 = ndcX * ndcX + ndcY * ndcY;
+    const float distortion = 1.0f + cam.k1 * r2;
+    const float distX = ndcX * distortion, distY = ndcY * distortion;
+    const float scaleMod = cam.scale * (1.0f + cam.caLateral * lambda);
+    dir = v3(distX * cam.aspect * scaleMod, distY * scaleMod, -1.0f);
+    o = v3s(0.0f);
+    if (cam.lensRadius > 0.0f) {
+        const V2 pl = cam.blades >= 3 ? squareToUniformPolygon(lens, cam.blades) : squareToUniformDisk(lens);
+        const float lx = pl.x * cam.lensRadius, ly = pl.y * cam.lensRadius;
+        const float focalDistMod = cam.focalDistance * (1.0f + cam.caAxial * lambda);
+        const float ft = focalDistMod / fabsf(dir.z);
+        const V3 pFocus = o + dir * ft;
+        o = v3(lx, ly, 0.0f);
+        dir = pFocus - o;
+    }
+    dir = normalize(dir);
+    if (!cam.vignetting) return 1.0f;
+    const float cosTheta = fabsf(dir.z), cos2 = cosTheta * cosTheta;
+    return cos2 * cos2;
+}
+
+// Camera weighting of a finished sample's radiance (integrator.h:130-135): the thin lens's
+// ray weight, then with chromatic aberration only the sample's channel, times 3. `r` is the
+// sample's generator right after the film position draw.
+__device__ __forceinline__ V3 cameraWeigh(const Camera& cam, V3 L, Rng r, float fx, float fy, int W, int H) {
+    const V2 lens = next2D(r);
+    float lambda;
+    const int ch = cameraChannel(cam, next1D(r), lambda);
+    if (cam.vignetting) {
+        V3 o, d;
+        const float w = thinLensRay(cam, fx / (float)W, 1.0f - fy / (float)H, lens, lambda, o, d);
+        L = L * w;
+    }
+    if (ch == 0) return v3(L.x * 3.0f, 0.0f, 0.0f);
+    if (ch == 1) return v3(0.0f, L.y * 3.0f, 0.0f);
+    if (ch == 2) return v3(0.0f, 0.0f, L.z * 3.0f);
+    return L;
+}
+
 // Work item -> camera sample (integrator.h:88-125) in slot `slot`.
 __device__ __forceinline__ void generatePath(const JobDev& j, uint32_t jobIdx, uint64_t item, PathState& ps) {
     int ww = j.wx1 - j.wx0;
@@ -357,16 +416,26 @@ __device__ __forceinline__ void generatePath(const JobDev& j, uint32_t jobIdx, u
     V2 ps2 = next2D(r);
     float fx = (float)x + ps2.x, fy = (float)y + ps2.y;
     float cx = fx / (float)j.W, cy = 1.0f - fy / (float)j.H;
-    next2D(r);   // lens sample (pinhole camera: unused)
-    next1D(r);   // chromatic aberration channel (unused without aberration)
-    next1D(r);   // time (static transforms)
-    // perspective.cpp:15-32
+    const V2 lens = next2D(r);     // lens position
+    const float chRnd = next1D(r); // chromatic aberration channel
+    next1D(r);                     // time (static transforms)
     const Camera& cam = j.view.camera;
-    float px = (2.0f * cx - 1.0f) * cam.aspect * cam.scale;
-    float py = (2.0f * cy - 1.0f) * cam.scale;
-    V3 dir = normalize(v3(px, py, -1.0f));
-    V3 o = v3(cam.origin[0], cam.origin[1], cam.origin[2]);
-    V3 d = xfVector(cam.toWorld, dir);
+    V3 o, d;
+    if (cam.kind == kCamThinLens) {
+        float lambda;
+        cameraChannel(cam, chRnd, lambda);
+        V3 oc, dc;
+        thinLensRay(cam, cx, cy, lens, lambda, oc, dc);
+        o = xfPoint(cam.toWorld, oc);
+        d = xfVector(cam.toWorld, dc);
+    } else {
+        // perspective.cpp:15-32
+        float px = (2.0f * cx - 1.0f) * cam.aspect * cam.scale;
+        float py = (2.0f * cy - 1.0f) * cam.scale;
+        V3 dir = normalize(v3(px, py, -1.0f));
+        o = v3(cam.origin[0], cam.origin[1], cam.origin[2]);
+        d = xfVector(cam.toWorld, dir);
+    }
     ps.ox = o.x; ps.oy = o.y; ps.oz = o.z; ps.pdfPrev = 1.0f;
     ps.dx = d.x; ps.dy = d.y; ps.dz = d.z;
     ps.lastX = o.x; ps.lastY = o.y; ps.lastZ = o.z;
@@ -850,13 +919,14 @@ __device__ __forceinline__ unsigned long long toFixed(float x) {
 // film.h:26-69 splat of one finished sample (NaN/Inf zeroed as integrator.h:137-141).
 __device__ __forceinline__ void filmSplat(const JobDev& j, const PathState& ps) {
     V3 L = v3(ps.Lr, ps.Lg, ps.Lb);
-    if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = v3s(0.0f);
     int ww = j.wx1 - j.wx0;
     int x = j.wx0 + (int)(ps.pixel % (uint32_t)ww), y = j.wy0 + (int)(ps.pixel / (uint32_t)ww);
     uint64_t key = (uint64_t)y * (uint64_t)j.W + (uint64_t)x + (uint64_t)ps.pass * ((uint64_t)j.W * (uint64_t)j.H);
     Rng r = rngSeed(key);
     V2 s2 = next2D(r);
     float fx = (float)x + s2.x, fy = (float)y + s2.y;
+    if (j.view.camera.kind == kCamThinLens) L = cameraWeigh(j.view.camera, L, r, fx, fy, j.W, j.H);
+    if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = v3s(0.0f);
     int x0 = max(0, (int)ceilf(fx - j.frx - 0.5f));
     int x1 = min(j.W - 1, (int)floorf(fx + j.frx - 0.5f));
     int y0 = max(0, (int)ceilf(fy - j.fry - 0.5f));
@@ -904,6 +974,7 @@ __device__ __forceinline__ void sampleRecord(const JobDev& j, const PathState& p
         return;
     }
     V3 L = v3(ps.Lr, ps.Lg, ps.Lb);
+    if (j.view.camera.kind == kCamThinLens) L = cameraWeigh(j.view.camera, L, r, fx, fy, j.W, j.H);
     if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = v3s(0.0f);
     const uint64_t npix = (uint64_t)ww * (uint64_t)(j.wy1 - j.wy0);
     const uint64_t item = (uint64_t)(ps.pass - (uint32_t)j.firstPass) * npix + ps.pixel;

@@ -453,6 +453,23 @@ void CameraObj::addChild(std::shared_ptr<GndObject> c) {
 struct PerspectiveCameraObj : CameraObj {
     explicit PerspectiveCameraObj(const PropertyList& p) : CameraObj(p) {}
 };
+// thinLens.cpp:13-31. The shutter properties only move the sample time, which no static
+// scene reads; they are parsed for the same error behaviour on malformed values.
+struct ThinLensCameraObj : CameraObj {
+    explicit ThinLensCameraObj(const PropertyList& p) : CameraObj(p) {
+        kind = gnd::kCamThinLens;
+        lensRadius = p.getFloat("lens_radius", 0.0f);
+        focalDistance = p.getFloat("focal_distance", 10.0f);
+        k1 = p.getFloat("k1", 0.0f);
+        caAxial = p.getFloat("ca_axial", 0.0f);
+        caLateral = p.getFloat("ca_lateral", 0.0f);
+        vignetting = p.getBoolean("vignetting", false);
+        blades = p.getInteger("blades", 0);
+        (void)p.getBoolean("rolling_shutter", false);
+        (void)p.getFloat("scan_duration", 0.9f);
+        (void)p.getFloat("exposure_duration", 0.1f);
+    }
+};
 // filter.h:20-54
 struct BoxFilterObj : FilterObj {
     explicit BoxFilterObj(const PropertyList&) { type = 0; rx = ry = 0.5f; }
@@ -469,6 +486,7 @@ struct IndependentSamplerObj : SamplerObj {
     explicit IndependentSamplerObj(const PropertyList& p) : SamplerObj(p) {}
 };
 GND_REGISTER_CLASS(PerspectiveCameraObj, "perspective")
+GND_REGISTER_CLASS(ThinLensCameraObj, "thinlens")
 GND_REGISTER_CLASS(BoxFilterObj, "box")
 GND_REGISTER_CLASS(GaussianFilterObj, "gaussian")
 GND_REGISTER_CLASS(IndependentSamplerObj, "independent")
@@ -714,6 +732,14 @@ void Scene::build() {
         fs->camera.aspect = m_camera->width / (float)m_camera->height;
         V3 org = m_camera->toWorld.point(gnd::v3s(0.0f));
         fs->camera.origin[0] = org.x; fs->camera.origin[1] = org.y; fs->camera.origin[2] = org.z;
+        fs->camera.kind = m_camera->kind;
+        fs->camera.blades = m_camera->blades;
+        fs->camera.lensRadius = m_camera->lensRadius;
+        fs->camera.focalDistance = m_camera->focalDistance;
+        fs->camera.k1 = m_camera->k1;
+        fs->camera.caAxial = m_camera->caAxial;
+        fs->camera.caLateral = m_camera->caLateral;
+        fs->camera.vignetting = m_camera->vignetting ? 1 : 0;
     }
     fs->fillDesc();
     gnd_scene_desc& d = fs->desc;

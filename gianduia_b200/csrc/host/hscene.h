@@ -212,6 +212,11 @@ struct CameraObj : GndObject {
     Transform toWorld;
     int width = 1280, height = 720;
     float fov = 45.f;
+    // thin lens (thinLens.cpp:13-31); kind 0 is the pinhole `perspective` camera
+    int kind = 0;
+    float lensRadius = 0.0f, focalDistance = 10.0f, k1 = 0.0f, caAxial = 0.0f, caLateral = 0.0f;
+    bool vignetting = false;
+    int blades = 0;
     std::shared_ptr<FilterObj> filter;
     explicit CameraObj(const PropertyList& p);
     EClassType getClassType() const override { return ECamera; }

@@ -127,13 +127,23 @@ struct alignas(16) Medium {
 };
 
 // ---------------------------------------------------------------- camera
+enum : int32_t { kCamPerspective = 0, kCamThinLens = 1 };
+
 struct alignas(16) Camera {
     Xf34 toWorld;             // directions: toWorld(vector)
     int32_t width, height;
     float scale, aspect;      // tan(fov/2), width/height
     float origin[3];          // toWorld(point(0,0,0)) evaluated on the host with the
     float pad;                // homogeneous divide of transform.h:330-337
+    // thin lens (thinLens.cpp:13-31); unused by the pinhole camera
+    int32_t kind;             // kCamPerspective / kCamThinLens
+    int32_t blades;           // aperture polygon corners; < 3: disk
+    float lensRadius, focalDistance;
+    float k1;                 // barrel distortion
+    float caAxial, caLateral; // chromatic aberration (per colour channel)
+    int32_t vignetting;       // 1: weight cos^4 of the camera-space direction
 };
+static_assert(sizeof(Camera) == 112, "Camera record must stay 112 bytes");
 
 // ---------------------------------------------------------------- scene view
 // Device pointers of one uploaded scene, passed by value to kernels (or read from an

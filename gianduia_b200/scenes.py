@@ -89,14 +89,25 @@ def _color(name, c):
     return '<color name="%s" value="%s %s %s"/>' % (name, _fmt(c[0]), _fmt(c[1]), _fmt(c[2]))
 
 
-def _camera(origin, target, fov, w, h, up=(0, 1, 0)):
+def _camera(origin, target, fov, w, h, up=(0, 1, 0), lens=None):
+    """A pinhole camera, or with `lens` (a dict of thin-lens properties: lens_radius,
+    focal_distance, k1, ca_axial, ca_lateral, vignetting, blades) a thin-lens one."""
+    props = []
+    for k, v in sorted((lens or {}).items()):
+        if isinstance(v, bool):
+            props.append('<boolean name="%s" value="%s"/>' % (k, "true" if v else "false"))
+        elif isinstance(v, int):
+            props.append('<integer name="%s" value="%d"/>' % (k, v))
+        else:
+            props.append('<float name="%s" value="%s"/>' % (k, _fmt(v)))
     return "\n".join([
-        '<camera type="perspective">',
+        '<camera type="%s">' % ("thinlens" if lens is not None else "perspective"),
         '<transform name="toWorld"><lookat origin="%s, %s, %s" target="%s, %s, %s" up="%s, %s, %s"/></transform>'
         % tuple(_fmt(v) for v in (*origin, *target, *up)),
         '<float name="fov" value="%s"/>' % _fmt(fov),
         '<integer name="width" value="%d"/>' % w,
         '<integer name="height" value="%d"/>' % h,
+        *props,
         '<filter type="box"/>',
         "</camera>",
     ])
@@ -145,12 +156,13 @@ def _cornell_body(light_y=0.998):
     return out
 
 
-def cornell(out_dir, width=256, height=256, spp=16, max_depth=8, integrator="path_gpu"):
-    """Writes the Cornell-box scene; returns the XML path."""
+def cornell(out_dir, width=256, height=256, spp=16, max_depth=8, integrator="path_gpu", lens=None):
+    """Writes the Cornell-box scene; returns the XML path. `lens`: thin-lens camera
+    properties (see _camera), else a pinhole camera."""
     os.makedirs(out_dir, exist_ok=True)
     write_plane_obj(os.path.join(out_dir, "plane.obj"))
     write_cube_obj(os.path.join(out_dir, "cube.obj"))
-    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height),
+    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height, lens=lens),
            '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
            '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
     xml += _cornell_body()

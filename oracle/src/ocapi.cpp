@@ -194,9 +194,14 @@ int orc_camera_rays(void* s, int spass, int64_t n, const int32_t* px, const int3
         Vec2 ps = smp.next2D();
         Vec2 pFilm(px[i] + ps.x, py[i] + ps.y);
         Vec2 camFilm(pFilm.x / W, 1.0f - pFilm.y / H);
-        smp.next2D(); smp.next1D();
-        float time = smp.next1D();
-        Ray r = cam.shootRay(camFilm, time);
+        CameraSample cs;
+        cs.pFilm = camFilm;
+        cs.pLens = smp.next2D();
+        const float channelRnd = smp.next1D();
+        if (cam.hasChromaticAberration()) cs.lambdaOffset = channelRnd < 0.333333f ? 1.0f : (channelRnd < 0.666666f ? 0.0f : -1.0f);
+        cs.time = smp.next1D();
+        Ray r;
+        cam.shootRay(cs, &r);
         float* o = rays + i * 8;
         o[0] = r.o.x; o[1] = r.o.y; o[2] = r.o.z; o[3] = r.tMin;
         o[4] = r.d.x; o[5] = r.d.y; o[6] = r.d.z; o[7] = r.tMax;
@@ -283,7 +288,8 @@ int orc_bxdf_sample(int kind, const float* p, const float* wo, const float* u, f
     return 0;
 }
 // Warps: op 0 disk (2 outputs), 1 uniform sphere, 2 uniform hemisphere, 3 cosine hemisphere,
-// 4 cosine-hemisphere pdf of (u[0],u[1],u[2]) -> out[0]
+// 4 cosine-hemisphere pdf of (u[0],u[1],u[2]) -> out[0], 5 polygon with (int)u[2] blades
+// (2 outputs)
 void orc_warp(int op, const float* u, float* out) {
     Vec2 s(u[0], u[1]);
     Vec3 r;
@@ -293,6 +299,7 @@ void orc_warp(int op, const float* u, float* out) {
         case 2: r = warp::squareToUniformHemisphere(s); break;
         case 3: r = warp::squareToCosineHemisphere(s); break;
         case 4: out[0] = warp::squareToCosineHemispherePdf(Vec3(u[0], u[1], u[2])); return;
+        case 5: { Vec2 d = warp::squareToUniformPolygon(s, (int)u[2]); out[0] = d.x; out[1] = d.y; return; }
     }
     out[0] = r.x; out[1] = r.y; out[2] = r.z;
 }
@@ -344,8 +351,11 @@ int orc_bounds_hit(const float* lo, const float* hi, const float* ray, float* ou
 void orc_perspective(float fov, int w, int h, float fx, float fy, float* out) {
     PropertyList pl;
     pl.f["fov"] = fov; pl.i["width"] = w; pl.i["height"] = h;
-    Camera c(pl);
-    Ray r = c.shootRay(Vec2(fx, fy), 0.f);
+    Camera c(pl, 0);
+    CameraSample cs;
+    cs.pFilm = Vec2(fx, fy);
+    Ray r;
+    c.shootRay(cs, &r);
     out[0] = r.o.x; out[1] = r.o.y; out[2] = r.o.z; out[3] = r.d.x; out[4] = r.d.y; out[5] = r.d.z;
 }
 // Homogeneous medium sampling with explicit uniforms (homogeneous.cpp:32-63).

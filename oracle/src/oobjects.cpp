@@ -357,7 +357,7 @@ void Film::addSample(const Vec2& pFilm, const Color& L) {
 }
 
 // camera.h:30-52, perspective.cpp:9-12
-Camera::Camera(const PropertyList& p) {
+Camera::Camera(const PropertyList& p, int k) {
     toWorld = p.getTransform("toWorld", Transform());
     if (p.hasTransform("toWorldEnd") && !(p.getTransform("toWorldEnd") == toWorld))
         throw std::runtime_error("Camera: animated transforms are not supported by this restatement");
@@ -365,6 +365,19 @@ Camera::Camera(const PropertyList& p) {
     height = p.getInteger("height", 720);
     fov = p.getFloat("fov", 45.0f);
     scale = std::tan((Pi / 180.f) * (fov * 0.5f));
+    kind = k;
+    if (kind == 1) {   // thinLens.cpp:13-31
+        lensRadius = p.getFloat("lens_radius", 0.0f);
+        focalDistance = p.getFloat("focal_distance", 10.0f);
+        k1 = p.getFloat("k1", 0.0f);
+        caAxial = p.getFloat("ca_axial", 0.0f);
+        caLateral = p.getFloat("ca_lateral", 0.0f);
+        vignetting = p.getBoolean("vignetting", false);
+        blades = p.getInteger("blades", 0);
+        rollingShutter = p.getBoolean("rolling_shutter", false);
+        scanDuration = p.getFloat("scan_duration", 0.9f);
+        exposureDuration = p.getFloat("exposure_duration", 0.1f);
+    }
 }
 void Camera::addChild(ObjectPtr c) {
     if (c->classType() == EFilter) {
@@ -373,14 +386,54 @@ void Camera::addChild(ObjectPtr c) {
     }
 }
 // perspective.cpp:15-32
-Ray Camera::shootRay(const Vec2& pFilm, float time) const {
-    float x = (2.0f * pFilm.x - 1.0f) * aspect() * scale;
-    float y = (2.0f * pFilm.y - 1.0f) * scale;
-    Vec3 dir = Normalize(Vec3(x, y, -1.0f));
-    Ray rc(Vec3(0, 0, 0), dir);
-    Ray r = toWorld.ray(rc);
-    r.time = time;
-    return r;
+float Camera::shootRay(const CameraSample& s, Ray* ray) const {
+    if (kind == 0) {   // perspective.cpp:15-32
+        float x = (2.0f * s.pFilm.x - 1.0f) * aspect() * scale;
+        float y = (2.0f * s.pFilm.y - 1.0f) * scale;
+        Vec3 dir = Normalize(Vec3(x, y, -1.0f));
+        Ray rc(Vec3(0, 0, 0), dir);
+        *ray = toWorld.ray(rc);
+        ray->time = s.time;
+        return 1.0f;
+    }
+    // thinLens.cpp:33-91: barrel distortion, lateral / axial chromatic aberration, depth
+    // of field through a disk or polygon aperture, vignetting, rolling shutter
+    float ndcX = 2.0f * s.pFilm.x - 1.0f;
+    float ndcY = 2.0f * s.pFilm.y - 1.0f;
+    float r2 = ndcX * ndcX + ndcY * ndcY;
+    float distortion = 1.0f + k1 * r2;
+    float distX = ndcX * distortion;
+    float distY = ndcY * distortion;
+    float scaleMod = scale * (1.0f + caLateral * s.lambdaOffset);
+    float x = distX * aspect() * scaleMod;
+    float y = distY * scaleMod;
+    Vec3 dir(x, y, -1.0f);
+    Vec3 rayOrigin(0.0f, 0.0f, 0.0f);
+    if (lensRadius > 0.0f) {
+        Vec2 pl = blades >= 3 ? warp::squareToUniformPolygon(s.pLens, blades) : warp::squareToUniformDisk(s.pLens);
+        Vec2 pLens(pl.x * lensRadius, pl.y * lensRadius);
+        float focalDistMod = focalDistance * (1.0f + caAxial * s.lambdaOffset);
+        float ft = focalDistMod / std::abs(dir.z);
+        Vec3 pFocus = rayOrigin + dir * ft;
+        rayOrigin = Vec3(pLens.x, pLens.y, 0.0f);
+        dir = pFocus - rayOrigin;
+    }
+    dir = Normalize(dir);
+    float weight = 1.0f;
+    if (vignetting) {
+        float cosTheta = std::abs(dir.z);
+        float cos2 = cosTheta * cosTheta;
+        weight = cos2 * cos2;
+    }
+    float finalTime = s.time;
+    if (rollingShutter) {
+        float scanline = 1.0f - s.pFilm.y;
+        finalTime = scanline * scanDuration + (s.time * exposureDuration);
+    }
+    Ray rc(rayOrigin, dir);
+    *ray = toWorld.ray(rc);
+    ray->time = finalTime;
+    return weight;
 }
 
 // ---------------------------------------------------------------- primitive, scene
@@ -465,7 +518,8 @@ std::unique_ptr<Object> createInstance(const std::string& t, const PropertyList&
     if (t == "index") return std::make_unique<IndexMaterial>(p);
     if (t == "homogeneous") return std::make_unique<HomogeneousMedium>(p);
     if (t == "area") return std::make_unique<AreaLight>(p);
-    if (t == "perspective") return std::make_unique<Camera>(p);
+    if (t == "perspective") return std::make_unique<Camera>(p, 0);
+    if (t == "thinlens") return std::make_unique<Camera>(p, 1);
     if (t == "box") return std::make_unique<BoxFilter>(p);
     if (t == "gaussian") return std::make_unique<GaussianFilter>(p);
     if (t == "independent") return std::make_unique<SamplerObj>(p);

@@ -308,12 +308,36 @@ RenderStats renderPasses(const Scene& scene, Film& film, int s0, int s1, int x0,
                     Vec2 ps = smp.next2D();
                     Vec2 pFilm(x + ps.x, y + ps.y);
                     Vec2 camFilm(pFilm.x / W, 1.0f - pFilm.y / H);
-                    smp.next2D();                 // lens sample (pinhole: unused)
-                    smp.next1D();                 // chromatic-aberration channel (unused)
-                    float time = smp.next1D();
-                    Ray ray = cam.shootRay(camFilm, time);
-                    Color L = kind == 0 ? LiPath(scene, ray, smp, arena, maxDepth, st)
-                                        : LiVolPath(scene, ray, smp, arena, maxDepth, st);
+                    CameraSample cs;
+                    cs.pFilm = camFilm;
+                    cs.pLens = smp.next2D();
+                    // integrator.h:103-121: one colour channel per sample under chromatic aberration
+                    float channelRnd = smp.next1D();
+                    int channel;
+                    if (!cam.hasChromaticAberration()) {
+                        channel = -1;
+                        cs.lambdaOffset = 0.0f;
+                    } else if (channelRnd < 0.333333f) {
+                        channel = 0;
+                        cs.lambdaOffset = 1.0f;
+                    } else if (channelRnd < 0.666666f) {
+                        channel = 1;
+                        cs.lambdaOffset = 0.0f;
+                    } else {
+                        channel = 2;
+                        cs.lambdaOffset = -1.0f;
+                    }
+                    cs.time = smp.next1D();
+                    Ray ray;
+                    float rayWeight = cam.shootRay(cs, &ray);
+                    Color raw = kind == 0 ? LiPath(scene, ray, smp, arena, maxDepth, st)
+                                          : LiVolPath(scene, ray, smp, arena, maxDepth, st);
+                    raw = raw * rayWeight;
+                    Color L(0.0f);
+                    if (channel == -1) L = raw;
+                    else if (channel == 0) L.r = raw.r * 3.0f;
+                    else if (channel == 1) L.g = raw.g * 3.0f;
+                    else L.b = raw.b * 3.0f;
                     if (L.hasNaNs()) L = Color(0.0f);
                     film.addSample(pFilm, L);
                     st.paths++;

@@ -61,6 +61,25 @@ inline Vec2 squareToUniformDisk(const Vec2& s) {
     }
     return Vec2(r * std::cos(theta), r * std::sin(theta));
 }
+// warp.cpp:86-113: uniform point in a regular polygon with `blades` corners (one corner
+// at the top), sampled as one of its triangles around the centre
+inline Vec2 squareToUniformPolygon(const Vec2& s, int blades) {
+    if (blades < 3) return squareToUniformDisk(s);
+    float bladeFloat = s.x * blades;
+    int bladeIdx = std::min(static_cast<int>(bladeFloat), blades - 1);
+    float u0 = bladeFloat - bladeIdx;
+    float u1 = s.y;
+    float deltaTheta = 2.0f * Pi / blades;
+    float theta1 = bladeIdx * deltaTheta;
+    float theta2 = (bladeIdx + 1) * deltaTheta;
+    float offset = Pi / 2.0f;
+    theta1 += offset;
+    theta2 += offset;
+    Vec2 v1(std::cos(theta1), std::sin(theta1));
+    Vec2 v2(std::cos(theta2), std::sin(theta2));
+    float r = std::sqrt(u0);
+    return Vec2(r * ((1.0f - u1) * v1.x + u1 * v2.x), r * ((1.0f - u1) * v1.y + u1 * v2.y));
+}
 // warp.cpp:35-44
 inline Vec3 squareToUniformSphereCap(const Vec2& s, float cosThetaMax) {
     float theta = std::acos(1 - (1 - cosThetaMax) * s.x);

@@ -268,17 +268,30 @@ struct Film {
     void clear();
 };
 
+// camera.h CameraSample
+struct CameraSample {
+    Vec2 pFilm, pLens;
+    float lambdaOffset = 0.0f, time = 0.0f;
+};
+
 struct Camera : Object {
     Transform toWorld;
     int width, height;
     float fov, scale;
+    // thinLens.cpp:13-31 (kind 1); kind 0 is the pinhole `perspective` camera
+    int kind = 0;
+    float lensRadius = 0.0f, focalDistance = 10.0f, k1 = 0.0f, caAxial = 0.0f, caLateral = 0.0f;
+    bool vignetting = false, rollingShutter = false;
+    int blades = 0;
+    float scanDuration = 0.9f, exposureDuration = 0.1f;
     std::shared_ptr<Filter> filterObj;
-    explicit Camera(const PropertyList& p);
+    Camera(const PropertyList& p, int kind);
     ClassType classType() const override { return ECamera; }
     void addChild(ObjectPtr child) override;
     float aspect() const { return width / (float)height; }
-    // perspective.cpp:15-32
-    Ray shootRay(const Vec2& pFilm, float time) const;
+    bool hasChromaticAberration() const { return kind == 1 && (caLateral != 0.0f || caAxial != 0.0f); }
+    // perspective.cpp:15-32 / thinLens.cpp:33-91; returns the ray weight
+    float shootRay(const CameraSample& s, Ray* ray) const;
 };
 
 struct SamplerObj : Object {
