@@ -218,6 +218,87 @@ def traversal_leg(ctx):
     return out
 
 
+def device_bvh_leg(ctx, xml, host_sid, host_load_s, tune):
+    """Mesh trees built on the GPU at upload against the host SAH build, on the bench
+    scene (4105 meshes, 5.2M triangles) and on the traversal workload (one mesh of 2^20
+    triangles): host load time without the mesh builds, upload wall time and the device
+    build time (CUDA events), and the traversal / render speed through each tree."""
+    import torch
+    import gianduia_b200 as G
+    from gianduia_b200 import scenes
+    out = {}
+    t = time.perf_counter()
+    hd = G.HostScene.load_xml(xml, device_blas=True)
+    out["host_load_s"] = time.perf_counter() - t
+    out["host_load_sah_s"] = host_load_s
+    hd.pin(True)
+    ups, builds = [], []
+    for k in range(4):
+        t = time.perf_counter()
+        sid = ctx.upload(hd)
+        up = time.perf_counter() - t
+        info = ctx.scene_info(sid)
+        if k:
+            ups.append(up)
+            builds.append(info["build_ms"])
+        if k < 3:
+            ctx.free_scene(sid)
+    hd.pin(False)
+    out["upload_ms"] = 1e3 * statistics.median(ups)
+    out["build_ms"] = statistics.median(builds)
+    out["nodes"] = info["num_nodes"]
+    ctx.set_tune(sid, **tune)
+    film = np.zeros((hd.height, hd.width, 7), np.float32)
+    for name, s in (("device_tree", sid), ("host_tree", host_sid)):
+        ctx.render(s, spp=8, batched=True, film=film)
+        ts = []
+        for _ in range(3):
+            _, st = ctx.render(s, spp=16, batched=True, film=film)
+            ts.append(st["ms"])
+        out[name + "_mpaths_s"] = st["paths"] / (statistics.median(ts) / 1e3) / 1e6
+        _, cst = ctx.render(s, spp=2, profile=2)
+        out[name + "_nodes_per_ray"] = cst["extend_nodes"] / max(1, cst["extend_rays"])
+        out[name + "_tris_per_ray"] = cst["extend_tris"] / max(1, cst["extend_rays"])
+    ctx.free_scene(sid)
+    # one large mesh: the traversal workload
+    n = 1 << 22
+    tri = scenes.random_triangles(1 << 20, seed=1)
+    rays = scenes.random_rays(n, seed=1)
+    dr = torch.from_numpy(rays).cuda()
+    dh = torch.empty((n, 5), dtype=torch.int32, device="cuda")
+    strm = torch.cuda.Stream()
+    for name, dev in (("soup_device_tree", True), ("soup_host_tree", False)):
+        t = time.perf_counter()
+        hs = G.HostScene.from_triangles(tri, device_blas=dev)
+        host_s = time.perf_counter() - t
+        t = time.perf_counter()
+        s = ctx.upload(hs)
+        up = time.perf_counter() - t
+        ctx.trace_closest_dev(s, dr.data_ptr(), n, dh.data_ptr(), strm.cuda_stream)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(strm)
+            ctx.trace_closest_dev(s, dr.data_ptr(), n, dh.data_ptr(), strm.cuda_stream)
+            e1.record(strm)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        out[name] = {"host_s": host_s, "upload_ms": up * 1e3, "build_ms": ctx.scene_info(s)["build_ms"],
+                     "closest_mrays_s": n / statistics.median(ts) / 1e3}
+        ctx.free_scene(s)
+        hs.close()
+    del dr, dh
+    torch.cuda.empty_cache()
+    log("device trees: host load %.2fs (SAH %.2fs), upload %.1f ms with a %.1f ms build; render %.0f vs %.0f Mpaths/s "
+        "(%.1f vs %.1f nodes/ray); 2^20-triangle mesh built in %.1f ms, %.0f vs %.0f Mrays/s" % (
+            out["host_load_s"], host_load_s, out["upload_ms"], out["build_ms"], out["device_tree_mpaths_s"],
+            out["host_tree_mpaths_s"], out["device_tree_nodes_per_ray"], out["host_tree_nodes_per_ray"],
+            out["soup_device_tree"]["build_ms"], out["soup_device_tree"]["closest_mrays_s"],
+            out["soup_host_tree"]["closest_mrays_s"]))
+    return out
+
+
 def scenes_leg(ctx):
     """The two other render configurations at their full sizes: Cornell box (path, 256^2,
     16 spp, depth 8) and volumetric Cornell box (volpath, 512^2, 64 spp, depth 32), batched
@@ -301,6 +382,7 @@ def main():
     ap.add_argument("--no-traversal", action="store_true", help="skip the traversal micro-benchmark")
     ap.add_argument("--no-autotune", action="store_true", help="render with the default engine settings")
     ap.add_argument("--no-scenes", action="store_true", help="skip the Cornell / volumetric renders")
+    ap.add_argument("--no-device-bvh", action="store_true", help="skip the device tree build measurements")
     ap.add_argument("--serve-requests", type=int, default=100,
                     help="requests in the serving stream (the full stream is 2000); 0 skips it")
     args = ap.parse_args()
@@ -324,8 +406,9 @@ def main():
     xml = make_scene(rank)
     t = time.time()
     hs = G.HostScene.load_xml(xml)
+    host_load_s = time.time() - t
     log("host load + BVH build %.1fs (%d tris, %d nodes, %d instances)" % (
-        time.time() - t, hs.desc.num_tris, hs.desc.num_nodes, hs.desc.num_instances))
+        host_load_s, hs.desc.num_tris, hs.desc.num_nodes, hs.desc.num_instances))
     ctx = G.GpuContext(local)
     sid = ctx.upload(hs)
     scene_bytes = ctx.scene_bytes(sid)
@@ -455,6 +538,8 @@ def main():
         line["traversal"] = traversal_leg(ctx)
     if rank == 0 and world == 1 and not args.no_scenes:
         line["scenes"] = scenes_leg(ctx)
+    if rank == 0 and world == 1 and not args.no_device_bvh:
+        line["device_bvh"] = device_bvh_leg(ctx, xml, sid, host_load_s, tune)
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serve"] = serve_leg(ctx, sid, args.serve_requests)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

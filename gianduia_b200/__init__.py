@@ -21,6 +21,7 @@ GND_ERR_TIMEOUT = 5
 GND_ERR_CANCELLED = 7
 GND_ERR_BUDGET = 8
 GND_ERR_NO_DEVICE = 9
+GND_HOST_DEVICE_BLAS = 1
 _STATUS = {1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "device check failed",
            5: "timeout", 6: "parse error", 7: "cancelled", 8: "over HBM budget", 9: "no CUDA device"}
 
@@ -33,6 +34,8 @@ CAMERA_DTYPE = np.dtype([("to_world", np.float32, (3, 4)), ("width", np.int32), 
                          ("focal_distance", np.float32), ("k1", np.float32), ("ca_axial", np.float32),
                          ("ca_lateral", np.float32), ("vignetting", np.int32)])
 assert CAMERA_DTYPE.itemsize == 112
+# BVH4 node (gnd::Node4): child bounds as rows lox, hix, loy, hiy, loz, hiz
+NODE_DTYPE = np.dtype([("lo_hi", np.float32, (6, 4)), ("child", np.uint32, 4), ("pad", np.uint32, 4)])
 
 
 class GndError(RuntimeError):
@@ -62,6 +65,10 @@ def lib():
             for name, args in {
                 "gnd_host_load_xml": [ctypes.c_char_p, ctypes.POINTER(_vp)],
                 "gnd_host_from_triangles": [_vp, ctypes.c_int64, ctypes.POINTER(_vp)],
+                "gnd_host_load_xml_ex": [ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(_vp)],
+                "gnd_host_from_triangles_ex": [_vp, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(_vp)],
+                "gnd_gpu_scene_info": [_vp, ctypes.c_uint64, _vp],
+                "gnd_gpu_scene_download": [_vp, ctypes.c_uint64, ctypes.c_int32, _vp, ctypes.c_int64],
                 "gnd_host_scene_desc": [_vp, ctypes.POINTER(_vp)],
                 "gnd_host_free": [_vp],
                 "gnd_gpu_create": [ctypes.c_int, ctypes.POINTER(_vp)],
@@ -105,6 +112,12 @@ def _check(status, what):
         raise GndError(status, msg)
 
 
+class SceneInfo(ctypes.Structure):
+    _fields_ = [("num_nodes", ctypes.c_int64), ("num_tris", ctypes.c_int64), ("num_instances", ctypes.c_int32),
+                ("blas_on_device", ctypes.c_int32), ("fast_boxes", ctypes.c_int32), ("num_meshes", ctypes.c_int32),
+                ("build_ms", ctypes.c_double), ("bytes", ctypes.c_uint64)]
+
+
 class SceneDesc(ctypes.Structure):
     """Mirror of gnd_scene_desc (read-only view of the render settings)."""
     _fields_ = [
@@ -116,7 +129,7 @@ class SceneDesc(ctypes.Structure):
         ("orig_to_leaf", _vp), ("orig_to_leaf_len", ctypes.c_int64), ("camera", _vp),
         ("width", ctypes.c_int32), ("height", ctypes.c_int32), ("spp", ctypes.c_int32), ("max_depth", ctypes.c_int32),
         ("integrator", ctypes.c_int32), ("filter", ctypes.c_int32), ("filter_radius", ctypes.c_float * 2),
-        ("filter_alpha", ctypes.c_float), ("pad", ctypes.c_int32),
+        ("filter_alpha", ctypes.c_float), ("blas_on_device", ctypes.c_int32),
     ]
 
 
@@ -131,16 +144,21 @@ class HostScene:
         self.desc = SceneDesc.from_address(d.value)
 
     @staticmethod
-    def load_xml(path):
+    def load_xml(path, device_blas=False):
+        """Parses and flattens a scene file. device_blas: leave the mesh trees to the GPU
+        (built at upload) instead of the host SAH builder."""
         h = _vp()
-        _check(lib().gnd_host_load_xml(os.fsencode(path), ctypes.byref(h)), "gnd_host_load_xml(%s)" % path)
+        flags = GND_HOST_DEVICE_BLAS if device_blas else 0
+        _check(lib().gnd_host_load_xml_ex(os.fsencode(path), flags, ctypes.byref(h)), "gnd_host_load_xml(%s)" % path)
         return HostScene(h.value)
 
     @staticmethod
-    def from_triangles(tris):
+    def from_triangles(tris, device_blas=False):
         tris = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1, 9)
         h = _vp()
-        _check(lib().gnd_host_from_triangles(tris.ctypes.data, tris.shape[0], ctypes.byref(h)), "gnd_host_from_triangles")
+        flags = GND_HOST_DEVICE_BLAS if device_blas else 0
+        _check(lib().gnd_host_from_triangles_ex(tris.ctypes.data, tris.shape[0], flags, ctypes.byref(h)),
+               "gnd_host_from_triangles")
         return HostScene(h.value)
 
     def camera(self):
@@ -182,7 +200,7 @@ class HostScene:
 
     def nodes(self):
         """The flattened BVH4 nodes as a structured numpy view (copy)."""
-        dt = np.dtype([("lo_hi", np.float32, (6, 4)), ("child", np.uint32, 4), ("pad", np.uint32, 4)])
+        dt = NODE_DTYPE
         n = self.desc.num_nodes
         buf = (ctypes.c_char * (n * 128)).from_address(self.desc.nodes)
         return np.frombuffer(bytes(buf), dtype=dt)
@@ -245,6 +263,27 @@ class GpuContext:
         b = ctypes.c_uint64()
         _check(lib().gnd_gpu_scene_bytes(self._h, sid, ctypes.byref(b)), "gnd_gpu_scene_bytes")
         return b.value
+
+    def scene_info(self, sid):
+        """Sizes and build record of an uploaded scene (gnd_gpu_scene_info) as a dict."""
+        info = SceneInfo()
+        _check(lib().gnd_gpu_scene_info(self._h, sid, ctypes.byref(info)), "gnd_gpu_scene_info")
+        return {k: getattr(info, k) for k, _ in SceneInfo._fields_}
+
+    def download(self, sid, array):
+        """One device array of an uploaded scene (gnd_gpu_scene_download): "nodes",
+        "tris", "tri_attrs", "orig_to_leaf" or "inst_trav", as raw numpy records."""
+        info = self.scene_info(sid)
+        code, dt, n = {
+            "nodes": (0, NODE_DTYPE, info["num_nodes"]),
+            "tris": (1, np.dtype((np.float32, 12)), info["num_tris"]),
+            "tri_attrs": (2, np.dtype((np.float32, 16)), info["num_tris"]),
+            "orig_to_leaf": (3, np.dtype(np.uint32), info["num_tris"]),
+            "inst_trav": (4, np.dtype((np.float32, 16)), info["num_instances"]),
+        }[array]
+        out = np.zeros(n, dt)
+        _check(lib().gnd_gpu_scene_download(self._h, sid, code, out.ctypes.data, out.nbytes), "gnd_gpu_scene_download")
+        return out
 
     def trace_closest(self, sid, rays):
         r = as_rays(rays)

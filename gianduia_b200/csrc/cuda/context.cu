@@ -2,6 +2,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "bvhbuild.h"
 #include "runtime.h"
 #include "server.h"
 #include "wavefront.h"
@@ -134,13 +135,29 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
             }
         }
         if (d->tlas_root != kEmpty && (int64_t)d->tlas_root >= d->num_nodes) throw Error(GND_ERR_INVALID, "bad top-level root");
+        // mesh trees built here: the mesh records must tile the triangles in order
+        const bool deviceBlas = d->blas_on_device != 0;
+        std::vector<uint32_t> meshBase;
+        if (deviceBlas) {
+            if (d->num_meshes < 0 || (d->num_meshes > 0 && !d->meshes)) throw Error(GND_ERR_INVALID, "device tree build needs the mesh records");
+            if (d->orig_to_leaf_len != d->num_tris) throw Error(GND_ERR_INVALID, "device tree build: orig_to_leaf must have one entry per triangle");
+            const MeshRec* mr = reinterpret_cast<const MeshRec*>(d->meshes);
+            meshBase.resize((size_t)d->num_meshes + 1, 0);
+            for (int m = 0; m < d->num_meshes; ++m) {
+                if (mr[m].origToLeaf != meshBase[m]) throw Error(GND_ERR_INVALID, "device tree build: meshes are not contiguous in triangle order");
+                meshBase[m + 1] = meshBase[m] + mr[m].numTris;
+            }
+            if ((int64_t)meshBase.back() != d->num_tris) throw Error(GND_ERR_INVALID, "device tree build: mesh triangle counts do not add up");
+        }
         for (int64_t i = 0; i < d->tlas_list_len; ++i)
             if ((int64_t)d->tlas_list[i] >= d->num_instances) throw Error(GND_ERR_INVALID, "instance list out of range");
         const InstTrav* it = reinterpret_cast<const InstTrav*>(d->inst_trav);
         const InstShade* is = reinterpret_cast<const InstShade*>(d->inst_shade);
         for (int i = 0; i < d->num_instances; ++i) {
-            if (it[i].kind == kShapeMesh && it[i].blasRoot != kEmpty && (int64_t)it[i].blasRoot >= d->num_nodes)
+            if (!deviceBlas && it[i].kind == kShapeMesh && it[i].blasRoot != kEmpty && (int64_t)it[i].blasRoot >= d->num_nodes)
                 throw Error(GND_ERR_INVALID, "instance root out of range");
+            if (deviceBlas && it[i].kind == kShapeMesh && (int64_t)is[i].meshId >= d->num_meshes)
+                throw Error(GND_ERR_INVALID, "instance mesh out of range");
             if (is[i].material < 0 || is[i].material >= d->num_materials) throw Error(GND_ERR_INVALID, "instance material out of range");
             if (is[i].emitter >= d->num_emitters) throw Error(GND_ERR_INVALID, "instance emitter out of range");
             if (is[i].mediumIn >= d->num_media || is[i].mediumOut >= d->num_media) throw Error(GND_ERR_INVALID, "instance medium out of range");
@@ -149,9 +166,19 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         std::lock_guard<FairMutex> lk(c->mu);
         auto ds = std::make_unique<DeviceScene>();
         SceneView& v = ds->view;
-        v.nodes = upload<Node4>(*ds, c->stream, d->nodes, d->num_nodes);
-        v.tris = upload<Tri>(*ds, c->stream, d->tris, d->num_tris);
-        v.attrs = upload<TriAttr>(*ds, c->stream, d->tri_attrs, d->num_tris);
+        PoolBuf rawTris, rawAttrs;   // original order, for the device tree build
+        if (!deviceBlas) {
+            v.nodes = upload<Node4>(*ds, c->stream, d->nodes, d->num_nodes);
+            v.tris = upload<Tri>(*ds, c->stream, d->tris, d->num_tris);
+            v.attrs = upload<TriAttr>(*ds, c->stream, d->tri_attrs, d->num_tris);
+        } else {
+            rawTris = PoolBuf(std::max<size_t>((size_t)d->num_tris * sizeof(Tri), 16), c->stream);
+            rawAttrs = PoolBuf(std::max<size_t>((size_t)d->num_tris * sizeof(TriAttr), 16), c->stream);
+            if (d->num_tris) {
+                GND_CUDA(cudaMemcpyAsync(rawTris.ptr, d->tris, (size_t)d->num_tris * sizeof(Tri), cudaMemcpyHostToDevice, c->stream));
+                GND_CUDA(cudaMemcpyAsync(rawAttrs.ptr, d->tri_attrs, (size_t)d->num_tris * sizeof(TriAttr), cudaMemcpyHostToDevice, c->stream));
+            }
+        }
         v.instT = upload<InstTrav>(*ds, c->stream, d->inst_trav, d->num_instances);
         v.instS = upload<InstShade>(*ds, c->stream, d->inst_shade, d->num_instances);
         v.tlasList = upload<uint32_t>(*ds, c->stream, d->tlas_list, d->tlas_list_len);
@@ -164,6 +191,39 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         v.tlasRoot = d->tlas_root;
         v.numEmitters = d->num_emitters;
         v.numInstances = d->num_instances;
+        ds->numNodes = d->num_nodes;
+        if (deviceBlas) {
+            MeshTreeInput mi{};
+            mi.tlasNodes = nodes;
+            mi.numTlasNodes = (uint32_t)d->num_nodes;
+            mi.meshBase = meshBase.data();
+            mi.numMeshes = d->num_meshes;
+            mi.tris = rawTris.as<Tri>();
+            mi.attrs = rawAttrs.as<TriAttr>();
+            mi.numTris = d->num_tris;
+            mi.instT = const_cast<InstTrav*>(v.instT);
+            mi.instS = v.instS;
+            mi.numInstances = d->num_instances;
+            mi.origToLeaf = const_cast<uint32_t*>(v.origToLeaf);
+            mi.leafMax = c->buildLeafMax;
+            mi.numSMs = c->numSMs;
+            MeshTreeOutput mo = buildMeshTrees(mi, c->stream);
+            nanBounds |= mo.nonFinite;
+            ds->numNodes = mo.numNodes;
+            ds->buildMs = mo.ms;
+            ds->blasOnDevice = true;
+            for (PoolBuf* b : {&mo.nodes, &mo.tris, &mo.attrs}) {
+                ds->bytes += b->bytes;
+                ds->bufs.push_back(std::move(*b));
+            }
+            v.nodes = ds->bufs[ds->bufs.size() - 3].as<Node4>();
+            v.tris = ds->bufs[ds->bufs.size() - 2].as<Tri>();
+            v.attrs = ds->bufs[ds->bufs.size() - 1].as<TriAttr>();
+        }
+        ds->numTris = d->num_tris;
+        ds->origToLeafLen = d->orig_to_leaf_len;
+        ds->numInstances = d->num_instances;
+        ds->numMeshes = d->num_meshes;
         v.fastBoxes = nanBounds ? 0 : 1;
         if (d->camera) std::memcpy(&v.camera, d->camera, sizeof(Camera));
         // null-BSDF mask and material type per instance
@@ -244,6 +304,50 @@ gnd_status gnd_gpu_scene_bytes(gnd_gpu_ctx* ctxh, gnd_scene_id id, uint64_t* byt
         Context* c = ctxOf(ctxh);
         std::lock_guard<FairMutex> lk(c->mu);
         *bytes = c->scene(id).bytes;
+    });
+}
+
+gnd_status gnd_gpu_scene_info(gnd_gpu_ctx* ctxh, gnd_scene_id id, gnd_scene_info* info) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (!info) throw Error(GND_ERR_INVALID, "null output pointer");
+        std::lock_guard<FairMutex> lk(c->mu);
+        const DeviceScene& s = c->scene(id);
+        gnd_scene_info r{};
+        r.num_nodes = s.numNodes;
+        r.num_tris = s.numTris;
+        r.num_instances = s.numInstances;
+        r.blas_on_device = s.blasOnDevice ? 1 : 0;
+        r.fast_boxes = s.view.fastBoxes;
+        r.num_meshes = s.numMeshes;
+        r.build_ms = s.buildMs;
+        r.bytes = s.bytes;
+        *info = r;
+    });
+}
+
+gnd_status gnd_gpu_scene_download(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t array, void* dst, int64_t capacity) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (!dst && capacity > 0) throw Error(GND_ERR_INVALID, "null destination");
+        c->bind();
+        std::lock_guard<FairMutex> lk(c->mu);
+        const DeviceScene& s = c->scene(id);
+        const void* src = nullptr;
+        int64_t bytes = 0;
+        switch (array) {
+            case GND_ARRAY_NODES: src = s.view.nodes; bytes = s.numNodes * (int64_t)sizeof(Node4); break;
+            case GND_ARRAY_TRIS: src = s.view.tris; bytes = s.numTris * (int64_t)sizeof(Tri); break;
+            case GND_ARRAY_TRI_ATTRS: src = s.view.attrs; bytes = s.numTris * (int64_t)sizeof(TriAttr); break;
+            case GND_ARRAY_ORIG_TO_LEAF: src = s.view.origToLeaf; bytes = s.origToLeafLen * 4; break;
+            case GND_ARRAY_INST_TRAV: src = s.view.instT; bytes = s.numInstances * (int64_t)sizeof(InstTrav); break;
+            default: throw Error(GND_ERR_INVALID, "unknown scene array");
+        }
+        if (bytes > capacity) throw Error(GND_ERR_INVALID, "destination too small: the array has " + std::to_string(bytes) + " bytes");
+        if (bytes) {
+            GND_CUDA(cudaMemcpyAsync(dst, src, (size_t)bytes, cudaMemcpyDeviceToHost, c->stream));
+            GND_CUDA(cudaStreamSynchronize(c->stream));
+        }
     });
 }
 

@@ -149,6 +149,11 @@ struct DeviceScene {
     bool hasNullMaterials = false;
     int numMaterials = 0;
     Tune tune;                // engine settings for renders of this scene
+    // array sizes (gnd_gpu_scene_info / gnd_gpu_scene_download)
+    int64_t numNodes = 0, numTris = 0, origToLeafLen = 0;
+    int numInstances = 0, numMeshes = 0;
+    bool blasOnDevice = false;   // mesh trees built on the GPU at upload
+    float buildMs = 0.0f;        // device time of that build
 };
 
 // First-come first-served mutex (ticket lock). The serving thread takes the context
@@ -179,6 +184,7 @@ class Server;
 struct Context {
     int device = 0;
     int numSMs = 148;
+    int buildLeafMax = 4;     // largest leaf of device-built mesh trees
     cudaStream_t stream = nullptr;
     FairMutex mu;   // serialises every use of the context (stream, scenes, engine)
     std::map<uint64_t, std::unique_ptr<DeviceScene>> scenes;

@@ -596,7 +596,13 @@ void Scene::build() {
         triBase[i + 1] = triBase[i] + (uint32_t)nt;
     }
     int parDepth = meshes.size() == 1 ? 4 : 0;
-    parallelFor(meshes.size(), [&](size_t i) {
+    if (deviceBlas) {
+        // the device builds the mesh trees: keep the original order
+        for (size_t i = 0; i < meshes.size(); ++i) {
+            mb[i].order.resize(meshes[i]->numTris());
+            for (size_t t = 0; t < mb[i].order.size(); ++t) mb[i].order[t] = (uint32_t)t;
+        }
+    } else parallelFor(meshes.size(), [&](size_t i) {
         const ShapeObj& m = *meshes[i];
         size_t nt = m.numTris();
         std::vector<Bounds> pb(nt);
@@ -631,7 +637,7 @@ void Scene::build() {
     for (size_t i = 0; i < meshes.size(); ++i) {
         uint32_t base = (uint32_t)fs->nodes.size();
         appendNodes(fs->nodes, mb[i].nodes);
-        blasRoot[i] = mb[i].root + base;
+        blasRoot[i] = mb[i].root == gnd::kEmpty ? gnd::kEmpty : mb[i].root + base;
         const ShapeObj& m = *meshes[i];
         gnd::MeshRec rec{};
         rec.cdfOffset = (uint32_t)fs->cdf.size();
@@ -753,6 +759,7 @@ void Scene::build() {
     d.filter_radius[0] = filt ? filt->rx : 2.f;
     d.filter_radius[1] = filt ? filt->ry : 2.f;
     d.filter_alpha = filt ? filt->alpha : 2.f;
+    d.blas_on_device = deviceBlas ? 1 : 0;
     m_flat = std::move(fs);
 }
 

@@ -283,6 +283,9 @@ public:
     std::shared_ptr<Integrator> getIntegrator() { return m_integrator; }
     const FlatScene& flat() const { return *m_flat; }
     bool deferPreprocess = false;
+    // mesh trees left to the device builder: triangles stay in their original order and
+    // the flattened scene holds only the top-level tree (gnd_scene_desc.blas_on_device)
+    bool deviceBlas = false;
 
     std::vector<std::shared_ptr<PrimitiveObj>> m_primitives;
     std::shared_ptr<CameraObj> m_camera;
@@ -292,7 +295,7 @@ public:
 };
 
 // parser.cpp:220-235
-std::shared_ptr<GndObject> loadFromXML(const std::string& path, bool deferPreprocess);
+std::shared_ptr<GndObject> loadFromXML(const std::string& path, bool deferPreprocess, bool deviceBlas = false);
 // mesh.cpp:148-229
 void loadOBJ(const std::string& path, ShapeObj& mesh);
 

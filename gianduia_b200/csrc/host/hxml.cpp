@@ -223,11 +223,15 @@ public:
                 sp->addChild(parse(*k));
             }
         }
-        if (auto sc = std::dynamic_pointer_cast<Scene>(sp)) sc->deferPreprocess = deferPreprocess;
+        if (auto sc = std::dynamic_pointer_cast<Scene>(sp)) {
+            sc->deferPreprocess = deferPreprocess;
+            sc->deviceBlas = deviceBlas;
+        }
         sp->activate();
         return sp;
     }
     bool deferPreprocess = false;
+    bool deviceBlas = false;
 
 private:
     std::string baseDir_;
@@ -236,7 +240,7 @@ private:
 
 }  // namespace
 
-std::shared_ptr<GndObject> loadFromXML(const std::string& path, bool deferPreprocess) {
+std::shared_ptr<GndObject> loadFromXML(const std::string& path, bool deferPreprocess, bool deviceBlas) {
     std::ifstream f(path, std::ios::binary);
     if (!f) throw std::runtime_error("XML parsing failed: cannot open " + path);
     std::stringstream ss;
@@ -248,6 +252,7 @@ std::shared_ptr<GndObject> loadFromXML(const std::string& path, bool deferPrepro
     std::filesystem::path canon = std::filesystem::canonical(path, ec);
     Loader ld((ec ? std::filesystem::path(path) : canon).parent_path().string());
     ld.deferPreprocess = deferPreprocess;
+    ld.deviceBlas = deviceBlas;
     return ld.parse(root);
 }
 

@@ -97,7 +97,11 @@ typedef struct gnd_scene_desc {
     int32_t filter;               /* 0 box (radius 0.5), 1 gaussian */
     float filter_radius[2];
     float filter_alpha;
-    int32_t pad;
+    /* 1: the mesh trees are left to the device: `nodes` holds only the top-level tree,
+     * tris / tri_attrs / orig_to_leaf are in original triangle order (orig_to_leaf the
+     * identity) and instance blasRoot fields are unset; gnd_gpu_scene_upload builds the
+     * mesh trees on the GPU (gnd_host_load_xml_ex, GND_HOST_DEVICE_BLAS) */
+    int32_t blas_on_device;
 } gnd_scene_desc;
 
 /* ------------------------------------------------------------------ host framework */
@@ -106,6 +110,12 @@ typedef struct gnd_host_scene gnd_host_scene;
 /* Parser::loadFromXML + Scene::activate (parser.cpp:220-235, scene.cpp:46-62): parses the
  * scene file, loads meshes, builds every BVH and flattens them. */
 gnd_status gnd_host_load_xml(const char* path, gnd_host_scene** out);
+/* As gnd_host_load_xml / gnd_host_from_triangles; flags GND_HOST_DEVICE_BLAS: build only
+ * the top-level tree on the host and leave the mesh trees (the SAH build of
+ * bvhBuilder.cpp:59-262) to the device at upload (an LBVH, see gnd_gpu_scene_upload). */
+#define GND_HOST_DEVICE_BLAS 1
+gnd_status gnd_host_load_xml_ex(const char* path, int32_t flags, gnd_host_scene** out);
+gnd_status gnd_host_from_triangles_ex(const float* tris, int64_t ntri, int32_t flags, gnd_host_scene** out);
 /* One mesh primitive with an identity transform from a triangle soup (ntri x 9 floats),
  * default camera; used for traversal-only workloads. */
 gnd_status gnd_host_from_triangles(const float* tris, int64_t ntri, gnd_host_scene** out);
@@ -122,7 +132,12 @@ gnd_status gnd_gpu_create(int device, gnd_gpu_ctx** out);
 gnd_status gnd_gpu_destroy(gnd_gpu_ctx* ctx);
 
 /* Integrator::preprocess (integrator.h:23, called at scene.cpp:61): copies a flattened
- * scene to HBM; the scene stays resident until gnd_gpu_scene_free. */
+ * scene to HBM; the scene stays resident until gnd_gpu_scene_free. With
+ * desc->blas_on_device the mesh trees are built here on the GPU (replacing the host build
+ * of bvhBuilder.cpp:59-262): a linear BVH over 3D Morton codes of the triangle
+ * centroids, leaves chosen by the surface area heuristic, collapsed to the same 4-wide
+ * nodes. Closest hits equal those through a host-built tree except between triangles at
+ * exactly the same distance. */
 gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctx, const gnd_scene_desc* desc, gnd_scene_id* out);
 gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctx, gnd_scene_id scene);
 /* Page-locks (pin = 1) or releases (pin = 0) the large host arrays of a scene
@@ -131,6 +146,30 @@ gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctx, gnd_scene_id scene);
 gnd_status gnd_gpu_host_register(const gnd_scene_desc* desc, int32_t pin);
 /* Bytes of HBM the scene occupies. */
 gnd_status gnd_gpu_scene_bytes(gnd_gpu_ctx* ctx, gnd_scene_id scene, uint64_t* bytes);
+
+/* Sizes and build record of an uploaded scene. */
+typedef struct gnd_scene_info {
+    int64_t num_nodes;          /* BVH4 nodes, the top-level tree first */
+    int64_t num_tris;
+    int32_t num_instances;
+    int32_t blas_on_device;     /* 1: the mesh trees were built on the GPU at upload */
+    int32_t fast_boxes;         /* 1: every node bound is finite (fast slab test) */
+    int32_t num_meshes;
+    double build_ms;            /* device time of the mesh-tree build; 0 when built on the host */
+    uint64_t bytes;             /* device bytes held by the scene */
+} gnd_scene_info;
+gnd_status gnd_gpu_scene_info(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_scene_info* info);
+
+/* Copies one device array of an uploaded scene into host memory `dst` of `capacity`
+ * bytes (GND_ERR_INVALID when the array does not fit): the layout records of
+ * gnd/layout.h. With it a tree built on the GPU can be kept as a host scene
+ * description (blas_on_device 0) and uploaded again without a build. */
+#define GND_ARRAY_NODES 0          /* Node4, 128 bytes each, num_nodes */
+#define GND_ARRAY_TRIS 1           /* Tri, 48 bytes, leaf order */
+#define GND_ARRAY_TRI_ATTRS 2      /* TriAttr, 64 bytes, leaf order */
+#define GND_ARRAY_ORIG_TO_LEAF 3   /* uint32 per triangle: original index -> leaf slot */
+#define GND_ARRAY_INST_TRAV 4      /* InstTrav, 64 bytes, per instance */
+gnd_status gnd_gpu_scene_download(gnd_gpu_ctx* ctx, gnd_scene_id scene, int32_t array, void* dst, int64_t capacity);
 
 /* Scene::rayIntersect(ray, isect) (scene.cpp:64-66, bvh.cpp:38-66) for n rays in HOST
  * memory: closest hit per ray, world tMax shrinking as hits are found. */
