@@ -467,31 +467,40 @@ def main():
 
     # e2e through the C ABI with host buffers: scene upload from pinned host memory +
     # render + film read-back to host memory
-    hs.pin(True)
-    e2e_times = []
     film_bytes = npix * 7 * 4   # resolved float film (sum wL rgb, sum w, sum wL^2 rgb) per pixel
-    for k in range(0 if args.no_e2e else max(1, args.steps)):
-        barrier()
-        t = time.perf_counter()
-        sid2 = ctx.upload(hs)
-        ctx.set_tune(sid2, **tune)
-        t_up = time.perf_counter()
-        _, st = ctx.render(sid2, spp=spp, first_pass=first, batched=batched, film=film)
+
+    def e2e_run(hscene, label):
+        hscene.pin(True)
+        times = []
+        for k in range(0 if args.no_e2e else max(1, args.steps)):
+            barrier()
+            t = time.perf_counter()
+            sid2 = ctx.upload(hscene)
+            ctx.set_tune(sid2, **tune)
+            t_up = time.perf_counter()
+            _, st = ctx.render(sid2, spp=spp, first_pass=first, batched=batched, film=film)
+            if dist:
+                reduce_film(torch.from_numpy(film).cuda(), dist)
+            t_re = time.perf_counter()
+            ctx.free_scene(sid2)
+            barrier()
+            times.append(time.perf_counter() - t)
+            log("e2e step (%s): upload %.1f ms, render %.1f ms, free %.1f ms" % (
+                label, (t_up - t) * 1e3, (t_re - t_up) * 1e3, (time.perf_counter() - t_re) * 1e3))
+        hscene.pin(False)
+        el = sum(times) if times else float("nan")
         if dist:
-            reduce_film(torch.from_numpy(film).cuda(), dist)
-        t_re = time.perf_counter()
-        ctx.free_scene(sid2)
-        barrier()
-        e2e_times.append(time.perf_counter() - t)
-        log("e2e step: upload %.1f ms, render %.1f ms, free %.1f ms" % (
-            (t_up - t) * 1e3, (t_re - t_up) * 1e3, (time.perf_counter() - t_re) * 1e3))
-    hs.pin(False)
-    e2e_el = sum(e2e_times) if e2e_times else float("nan")
-    if dist:
-        tt = torch.tensor([e2e_el], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_el = float(tt.item())
-    e2e_value = npix * spp * world * len(e2e_times) / e2e_el / 1e6 if e2e_times else None
+            tt = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            el = float(tt.item())
+        return npix * spp * world * len(times) / el / 1e6 if times else None
+
+    e2e_value = e2e_run(hs, "host-built trees")
+    e2e_dev = None
+    if not args.no_device_bvh and not args.no_e2e:
+        hd = G.HostScene.load_xml(xml, device_blas=True)
+        e2e_dev = e2e_run(hd, "trees built at upload")
+        hd.close()
     # the other mode on the same scene, for the batched-vs-plain comparison
     other = []
     for k in range(min(2, args.steps)):
@@ -531,6 +540,8 @@ def main():
                      "launches": ext_launches, "ms_total": ext_ms, "peak_kind": peak_kind + " (copy bandwidth)"},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": int(scene_bytes),
                 "d2h_bytes_per_step": int(film_bytes)},
+        "e2e_device_trees": None if e2e_dev is None else {
+            "value": e2e_dev, "unit": "Mpaths/s", "note": "mesh trees built on the GPU inside each timed upload"},
         "gpu_launches": int(launches_total),
         "clocks": clk,
     }

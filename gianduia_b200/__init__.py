@@ -68,6 +68,7 @@ def lib():
                 "gnd_host_load_xml_ex": [ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(_vp)],
                 "gnd_host_from_triangles_ex": [_vp, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(_vp)],
                 "gnd_gpu_scene_info": [_vp, ctypes.c_uint64, _vp],
+                "gnd_gpu_set_build_leaf_max": [_vp, ctypes.c_int32],
                 "gnd_gpu_scene_download": [_vp, ctypes.c_uint64, ctypes.c_int32, _vp, ctypes.c_int64],
                 "gnd_host_scene_desc": [_vp, ctypes.POINTER(_vp)],
                 "gnd_host_free": [_vp],
@@ -263,6 +264,10 @@ class GpuContext:
         b = ctypes.c_uint64()
         _check(lib().gnd_gpu_scene_bytes(self._h, sid, ctypes.byref(b)), "gnd_gpu_scene_bytes")
         return b.value
+
+    def set_build_leaf_max(self, leaf_max):
+        """Largest leaf of mesh trees built on the GPU by later uploads (1..16)."""
+        _check(lib().gnd_gpu_set_build_leaf_max(self._h, leaf_max), "gnd_gpu_set_build_leaf_max")
 
     def scene_info(self, sid):
         """Sizes and build record of an uploaded scene (gnd_gpu_scene_info) as a dict."""

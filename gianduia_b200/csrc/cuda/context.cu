@@ -52,6 +52,35 @@ Context* ctxOf(gnd_gpu_ctx* c) {
 }
 
 namespace {
+constexpr uint32_t kNodeBadRef = 1u, kNodeBadLeaf = 2u, kNodeSlowBounds = 4u;
+
+// Checks every node of an uploaded tree: inner references below n, leaf ranges below
+// leafLimit (triangles or top-level entries), and whether the bounds allow the fast slab
+// test (no NaN, lo <= hi on every non-empty child).
+__global__ void kValidateNodes(const Node4* __restrict__ nodes, int64_t n, int64_t leafLimit, uint32_t* flags) {
+    uint32_t f = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const Node4& nd = nodes[i];
+        for (int k = 0; k < 4; ++k) {
+            const float lo[3] = {nd.lox[k], nd.loy[k], nd.loz[k]};
+            const float hi[3] = {nd.hix[k], nd.hiy[k], nd.hiz[k]};
+            const uint32_t r = nd.child[k];
+            for (int a = 0; a < 3; ++a) {
+                if (isnan(lo[a]) || isnan(hi[a])) f |= kNodeSlowBounds;
+                if (r != kEmpty && !(lo[a] <= hi[a])) f |= kNodeSlowBounds;
+            }
+            if (r == kEmpty) continue;
+            if (!isLeaf(r)) {
+                if ((int64_t)r >= n) f |= kNodeBadRef;
+            } else if ((int64_t)(leafFirst(r) + leafCount(r)) > leafLimit) {
+                f |= kNodeBadLeaf;
+            }
+        }
+    }
+    f = __reduce_or_sync(0xffffffffu, f);
+    if (f && (threadIdx.x & 31) == 0) atomicOr(flags, f);
+}
+
 template <typename T>
 const T* upload(DeviceScene& ds, cudaStream_t st, const void* src, size_t count) {
     size_t bytes = count * sizeof(T);
@@ -112,28 +141,11 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         if (d->num_tris >= (int64_t)kLeafFirstMask) throw Error(GND_ERR_INVALID, "too many triangles");
         // host-side validation of every reference stored in the tree (a corrupted index
         // is refused here rather than read out of bounds on the device)
+        // The node references and bounds are checked on the device after the upload
+        // (kValidateNodes), before any kernel follows them.
         const Node4* nodes = reinterpret_cast<const Node4*>(d->nodes);
+        if (d->num_nodes > 0 && !nodes) throw Error(GND_ERR_INVALID, "null node array");
         bool nanBounds = false;   // true: the traversal keeps the exact slab arithmetic
-        for (int64_t i = 0; i < d->num_nodes; ++i) {
-            // the fast slab test needs bounds without NaN and lo <= hi on every non-empty child
-            for (int k = 0; k < 4; ++k) {
-                const float lo[3] = {nodes[i].lox[k], nodes[i].loy[k], nodes[i].loz[k]};
-                const float hi[3] = {nodes[i].hix[k], nodes[i].hiy[k], nodes[i].hiz[k]};
-                for (int a = 0; a < 3; ++a) {
-                    nanBounds |= std::isnan(lo[a]) || std::isnan(hi[a]);
-                    if (nodes[i].child[k] != kEmpty) nanBounds |= !(lo[a] <= hi[a]);
-                }
-            }
-            for (int k = 0; k < 4; ++k) {
-                uint32_t r = nodes[i].child[k];
-                if (r == kEmpty) continue;
-                if (!isLeaf(r)) {
-                    if ((int64_t)r >= d->num_nodes) throw Error(GND_ERR_INVALID, "node reference out of range");
-                } else if ((int64_t)(leafFirst(r) + leafCount(r)) > std::max<int64_t>(d->num_tris, d->tlas_list_len)) {
-                    throw Error(GND_ERR_INVALID, "leaf range out of range");
-                }
-            }
-        }
         if (d->tlas_root != kEmpty && (int64_t)d->tlas_root >= d->num_nodes) throw Error(GND_ERR_INVALID, "bad top-level root");
         // mesh trees built here: the mesh records must tile the triangles in order
         const bool deviceBlas = d->blas_on_device != 0;
@@ -224,6 +236,21 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         ds->origToLeafLen = d->orig_to_leaf_len;
         ds->numInstances = d->num_instances;
         ds->numMeshes = d->num_meshes;
+        // every node reference in range; bounds fit for the fast slab test
+        PoolBuf vflags(16, c->stream);
+        GND_CUDA(cudaMemsetAsync(vflags.ptr, 0, 16, c->stream));
+        if (ds->numNodes > 0) {
+            const unsigned grid = (unsigned)std::min<int64_t>((ds->numNodes + 255) / 256, (int64_t)c->numSMs * 8);
+            kValidateNodes<<<grid, 256, 0, c->stream>>>(v.nodes, ds->numNodes, std::max<int64_t>(d->num_tris, d->tlas_list_len),
+                                                        vflags.as<uint32_t>());
+            GND_CUDA(cudaGetLastError());
+        }
+        uint32_t vf = 0;
+        GND_CUDA(cudaMemcpyAsync(&vf, vflags.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
+        GND_CUDA(cudaStreamSynchronize(c->stream));
+        if (vf & kNodeBadRef) throw Error(GND_ERR_INVALID, "node reference out of range");
+        if (vf & kNodeBadLeaf) throw Error(GND_ERR_INVALID, "leaf range out of range");
+        nanBounds |= (vf & kNodeSlowBounds) != 0;
         v.fastBoxes = nanBounds ? 0 : 1;
         if (d->camera) std::memcpy(&v.camera, d->camera, sizeof(Camera));
         // null-BSDF mask and material type per instance
@@ -304,6 +331,15 @@ gnd_status gnd_gpu_scene_bytes(gnd_gpu_ctx* ctxh, gnd_scene_id id, uint64_t* byt
         Context* c = ctxOf(ctxh);
         std::lock_guard<FairMutex> lk(c->mu);
         *bytes = c->scene(id).bytes;
+    });
+}
+
+gnd_status gnd_gpu_set_build_leaf_max(gnd_gpu_ctx* ctxh, int32_t leafMax) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (leafMax < 1 || leafMax > kLeafMax) throw Error(GND_ERR_INVALID, "leaf size out of range (1..16)");
+        std::lock_guard<FairMutex> lk(c->mu);
+        c->buildLeafMax = leafMax;
     });
 }
 

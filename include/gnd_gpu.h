@@ -140,6 +140,10 @@ gnd_status gnd_gpu_destroy(gnd_gpu_ctx* ctx);
  * exactly the same distance. */
 gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctx, const gnd_scene_desc* desc, gnd_scene_id* out);
 gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctx, gnd_scene_id scene);
+/* Largest leaf (1..16 triangles, default 4) of the mesh trees that later uploads build on
+ * the GPU; a subtree up to that size becomes a leaf where the surface area heuristic
+ * prefers it. Changes the tree, and so which triangle wins an exact-distance tie. */
+gnd_status gnd_gpu_set_build_leaf_max(gnd_gpu_ctx* ctx, int32_t leaf_max);
 /* Page-locks (pin = 1) or releases (pin = 0) the large host arrays of a scene
  * description (BVH nodes, triangles, triangle attributes) so that gnd_gpu_scene_upload
  * copies them by DMA at full link speed. Release before the description is freed. */

@@ -161,3 +161,22 @@ def test_download_checks_capacity(ctx):
     st = G.lib().gnd_gpu_scene_download(ctx._h, sid, 3, buf.ctypes.data, buf.nbytes)
     assert st == G.GND_ERR_INVALID and b"too small" in G.lib().gnd_last_error()
     ctx.free_scene(sid)
+
+
+def test_upload_rejects_bad_node_references(ctx):
+    """A scene description whose tree points outside its arrays is refused at upload
+    (checked on the device before any kernel follows a reference)."""
+    import ctypes
+    tri = scenes.random_triangles(512, seed=6)
+    for corrupt, msg in (("inner", b"node reference out of range"), ("leaf", b"leaf range out of range")):
+        hs = G.HostScene.from_triangles(tri)
+        n = hs.desc.num_nodes
+        child = (ctypes.c_uint32 * 4).from_address(hs.desc.nodes + (n - 1) * 128 + 96)
+        if corrupt == "inner":
+            child[0] = n + 5
+        else:
+            child[0] = 0x80000000 | (3 << 27) | (hs.desc.num_tris - 2)   # 4 triangles from the last but one
+        with pytest.raises(G.GndError) as ei:
+            ctx.upload(hs)
+        assert ei.value.status == G.GND_ERR_INVALID and msg in G.lib().gnd_last_error()
+        hs.close()
