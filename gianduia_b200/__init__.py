@@ -69,6 +69,10 @@ def lib():
                 "gnd_host_from_triangles_ex": [_vp, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(_vp)],
                 "gnd_gpu_scene_info": [_vp, ctypes.c_uint64, _vp],
                 "gnd_gpu_set_build_leaf_max": [_vp, ctypes.c_int32],
+                "gnd_gpu_post": [_vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp],
+                "gnd_gpu_post_dev": [_vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp, _vp],
+                "gnd_image_write_png": [ctypes.c_char_p, _vp, ctypes.c_int32, ctypes.c_int32],
+                "gnd_image_write_exr": [ctypes.c_char_p, _vp, ctypes.c_int32, ctypes.c_int32],
                 "gnd_gpu_scene_download": [_vp, ctypes.c_uint64, ctypes.c_int32, _vp, ctypes.c_int64],
                 "gnd_host_scene_desc": [_vp, ctypes.POINTER(_vp)],
                 "gnd_host_free": [_vp],
@@ -111,6 +115,34 @@ def _check(status, what):
         if status == GND_ERR_NO_DEVICE:
             raise GpuUnavailable(status, msg)
         raise GndError(status, msg)
+
+
+class PostParams(ctypes.Structure):
+    _fields_ = [("tonemapper", ctypes.c_int32), ("exposure", ctypes.c_float), ("bloom", ctypes.c_int32),
+                ("bloom_threshold", ctypes.c_float), ("bloom_radius", ctypes.c_float),
+                ("bloom_intensity", ctypes.c_float), ("bloom_mips", ctypes.c_int32), ("output", ctypes.c_int32)]
+
+
+TONEMAPPERS = {"linear": 0, "reinhard": 1, "uncharted2": 2, "aces": 3, "khronos_pbr": 4, "agx": 5, "agx_punchy": 6}
+
+
+def post_params(tonemapper=0, exposure=0.0, bloom=False, threshold=1.0, radius=1.0, intensity=0.04, mips=6, output=0):
+    """gnd_post_params with the reference PostProcessor's defaults."""
+    if isinstance(tonemapper, str):
+        tonemapper = TONEMAPPERS[tonemapper]
+    return PostParams(tonemapper, exposure, 1 if bloom else 0, threshold, radius, intensity, mips, output)
+
+
+def write_png(path, rgb8):
+    """Film::savePNG's file: an 8-bit RGB image [h, w, 3]."""
+    a = np.ascontiguousarray(rgb8, dtype=np.uint8)
+    _check(lib().gnd_image_write_png(os.fsencode(path), a.ctypes.data, a.shape[1], a.shape[0]), "gnd_image_write_png")
+
+
+def write_exr(path, rgb):
+    """Film::saveEXR's file: a float RGB image [h, w, 3]."""
+    a = np.ascontiguousarray(rgb, dtype=np.float32)
+    _check(lib().gnd_image_write_exr(os.fsencode(path), a.ctypes.data, a.shape[1], a.shape[0]), "gnd_image_write_exr")
 
 
 class SceneInfo(ctypes.Structure):
@@ -268,6 +300,20 @@ class GpuContext:
     def set_build_leaf_max(self, leaf_max):
         """Largest leaf of mesh trees built on the GPU by later uploads (1..16)."""
         _check(lib().gnd_gpu_set_build_leaf_max(self._h, leaf_max), "gnd_gpu_set_build_leaf_max")
+
+    def post(self, rgb, want_hdr=True, want_rgb8=True, **params):
+        """Post-processing of a linear image [h, w, 3] on the GPU (gnd_gpu_post): returns
+        (tonemapped float image or None, 8-bit image or None). Keyword arguments as
+        post_params."""
+        a = np.ascontiguousarray(rgb, dtype=np.float32)
+        h, w = a.shape[:2]
+        hdr = np.zeros((h, w, 3), np.float32) if want_hdr else None
+        out8 = np.zeros((h, w, 3), np.uint8) if want_rgb8 else None
+        p = post_params(**params)
+        _check(lib().gnd_gpu_post(self._h, a.ctypes.data, w, h, ctypes.byref(p),
+                                  hdr.ctypes.data if hdr is not None else None,
+                                  out8.ctypes.data if out8 is not None else None), "gnd_gpu_post")
+        return hdr, out8
 
     def scene_info(self, sid):
         """Sizes and build record of an uploaded scene (gnd_gpu_scene_info) as a dict."""

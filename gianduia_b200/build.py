@@ -93,7 +93,7 @@ def build(force=False, verbose_ptxas=False, quiet=True):
             if log:
                 logs.append(log)
     tmp = LIB + ".tmp"
-    cmd = [NVCC, "-shared", "-ccbin", CXX, "-Xcompiler", "-fPIC", "-o", tmp] + objs + ["-cudart", "static", "-lpthread"]
+    cmd = [NVCC, "-shared", "-ccbin", CXX, "-Xcompiler", "-fPIC", "-o", tmp] + objs + ["-cudart", "static", "-lpthread", "-lz"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed: %s\n%s\n%s" % (" ".join(cmd), r.stdout, r.stderr))

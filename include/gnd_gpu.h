@@ -210,6 +210,38 @@ gnd_status gnd_gpu_trace_closest_fixed(gnd_gpu_ctx* ctx, gnd_scene_id scene, con
  * traversal roofline. Diagnostics; no counterpart in the reference. */
 gnd_status gnd_gpu_read_bandwidth(gnd_gpu_ctx* ctx, uint64_t bytes, int32_t reps, double* gbps);
 
+/* ------------------------------------------------------------------ image outputs */
+/* The reference's post-processing (PostProcessor::render, postProcessor.cpp:148-235, and
+ * its shaders tonemap.frag, bloom_*.frag, gammaCorrect.frag) and the 8-bit conversion of
+ * Film::savePNG (film.cpp:154-171), run as CUDA kernels on a linear RGB image
+ * (width x height x 3 floats, row-major) instead of through OpenGL. Defaults of
+ * PostProcessor: tonemapper 0, exposure 0, bloom off, threshold 1, radius 1, intensity
+ * 0.04, 6 mips. */
+typedef struct gnd_post_params {
+    int32_t tonemapper;       /* 0 linear, 1 Reinhard, 2 Uncharted 2, 3 ACES, 4 Khronos PBR
+                                 neutral, 5 AgX, 6 AgX punchy (TonemapOperator) */
+    float exposure;           /* stops: colour *= exp2(exposure) */
+    int32_t bloom;            /* 1: bloom pyramid added before the exposure */
+    float bloom_threshold;    /* prefilter: keep texels whose brightest channel exceeds it */
+    float bloom_radius;       /* upsample tent radius in source texels */
+    float bloom_intensity;    /* weight of the bloom in the sum */
+    int32_t bloom_mips;       /* pyramid levels used, 1..6 */
+    int32_t output;           /* 8-bit conversion: 0 Film::savePNG (sRGB, x255 + 0.5,
+                                 truncate), 1 display pass (gammaCorrect.frag, rounded) */
+} gnd_post_params;
+/* Host buffers: `rgb` in; `hdr` (tonemapped floats, w x h x 3) and `rgb8` (w x h x 3
+ * bytes) out, each optional (NULL). */
+gnd_status gnd_gpu_post(gnd_gpu_ctx* ctx, const float* rgb, int32_t width, int32_t height,
+                        const gnd_post_params* params, float* hdr, uint8_t* rgb8);
+/* The same on device buffers, enqueued on `stream` (cudaStream_t; 0 = legacy stream). */
+gnd_status gnd_gpu_post_dev(gnd_gpu_ctx* ctx, const float* d_rgb, int32_t width, int32_t height,
+                            const gnd_post_params* params, float* d_hdr, uint8_t* d_rgb8, void* stream);
+/* Film::savePNG / Film::saveEXR (film.cpp:154-195) as files: an 8-bit RGB PNG (zlib
+ * compressed) and a 32-bit float RGB OpenEXR image (scanline, uncompressed; channels
+ * B, G, R as the format orders them). */
+gnd_status gnd_image_write_png(const char* path, const uint8_t* rgb8, int32_t width, int32_t height);
+gnd_status gnd_image_write_exr(const char* path, const float* rgb, int32_t width, int32_t height);
+
 /* ------------------------------------------------------------------ rendering */
 /* Progress callback, the reference's Integrator::setCallback / notifyUpdate
  * (integrator.h:25-35, 148-149): called after each completed sample pass with the film

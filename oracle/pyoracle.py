@@ -64,6 +64,11 @@ def lib():
             L.orc_medium_sample.argtypes = [_f32p, _f32p]
             L.orc_hg.restype = ctypes.c_float
             L.orc_hg.argtypes = [ctypes.c_int, ctypes.c_float, _f32p, _f32p, _f32p]
+            L.orc_post.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                   ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                   _f32p, ctypes.c_void_p]
+            L.orc_round_half.restype = ctypes.c_float
+            L.orc_round_half.argtypes = [ctypes.c_float]
             _lib = L
     return _lib
 
@@ -254,3 +259,20 @@ def hg(op, g, wo, x):
     out = np.zeros(3, np.float32)
     v = lib().orc_hg(op, g, _fp(f32(wo)), _fp(f32(x)), _fp(out))
     return (float(v), out) if op == 1 else float(v)
+
+
+# ------------------------------------------------------------------ post-processing
+def post(rgb, tonemapper=0, exposure=0.0, bloom=False, threshold=1.0, radius=1.0, intensity=0.04, mips=6, output=0):
+    """Post-processing of a linear image [h, w, 3] (tonemap.frag, bloom_*.frag,
+    gammaCorrect.frag, Film::savePNG): returns (tonemapped float image, 8-bit image)."""
+    rgb = np.ascontiguousarray(rgb, dtype=np.float32)
+    h, w = rgb.shape[:2]
+    hdr = np.zeros((h, w, 3), np.float32)
+    out8 = np.zeros((h, w, 3), np.uint8)
+    lib().orc_post(_fp(rgb), w, h, tonemapper, exposure, 1 if bloom else 0, threshold, radius, intensity, mips, output,
+                   _fp(hdr), out8.ctypes.data)
+    return hdr, out8
+
+
+def round_half(x):
+    return float(lib().orc_round_half(x))
