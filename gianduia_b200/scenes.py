@@ -15,6 +15,7 @@ Workloads (sizes as named by the benchmark configurations):
                   holding a second medium
 """
 import os
+import struct
 
 import numpy as np
 
@@ -319,6 +320,110 @@ def microfacet(out_dir, width=1024, height=1024, spp=64, max_depth=16, grid=64, 
                 '<material type="matte">' + _color("albedo", (0, 0, 0)) + "</material>",
                 '<emitter type="area">' + _color("radiance", (50, 50, 50)) + "</emitter>", "</primitive>"]
     xml.append("</scene>")
+    with open(path, "w") as f:
+        f.write("\n".join(xml) + "\n")
+    return path
+
+
+# ------------------------------------------------------------------ light sources
+
+
+def write_env_exr(path, width=64, height=32, sun=(0.3, 0.3), sun_size=0.04, sun_radiance=60.0):
+    """Latitude-longitude environment image (column u = phi / 2 pi, row v = theta / pi,
+    theta measured from +z): a sky gradient with a small bright disc (the sun) centred
+    at (u, v) = `sun`. Written as an uncompressed float RGB OpenEXR file (the layout of
+    gnd_image_write_exr) so that scene generation needs no compiled code."""
+    v, u = np.mgrid[0:height, 0:width].astype(np.float64)
+    u = (u + 0.5) / width
+    v = (v + 0.5) / height
+    sky = np.stack([0.2 + 0.3 * (1 - v), 0.3 + 0.4 * (1 - v), 0.5 + 0.5 * (1 - v)], axis=-1)
+    du = np.minimum(np.abs(u - sun[0]), 1 - np.abs(u - sun[0]))
+    disc = (du ** 2 + (v - sun[1]) ** 2) < sun_size ** 2
+    img = np.where(disc[..., None], sun_radiance * np.array([1.0, 0.9, 0.7]), sky).astype(np.float32)
+    header = bytearray(struct.pack("<II", 20000630, 2))
+
+    def attr(name, typ, value):
+        header.extend(name.encode() + b"\0" + typ.encode() + b"\0" + struct.pack("<i", len(value)) + value)
+
+    attr("channels", "chlist", b"".join(c + b"\0" + struct.pack("<iBBBBii", 2, 0, 0, 0, 0, 1, 1) for c in (b"B", b"G", b"R")) + b"\0")
+    attr("compression", "compression", b"\0")
+    box = struct.pack("<iiii", 0, 0, width - 1, height - 1)
+    attr("dataWindow", "box2i", box)
+    attr("displayWindow", "box2i", box)
+    attr("lineOrder", "lineOrder", b"\0")
+    attr("pixelAspectRatio", "float", struct.pack("<f", 1.0))
+    attr("screenWindowCenter", "v2f", struct.pack("<ff", 0.0, 0.0))
+    attr("screenWindowWidth", "float", struct.pack("<f", 1.0))
+    header.extend(b"\0")
+    line = 8 + width * 12
+    table = b"".join(struct.pack("<Q", len(header) + 8 * height + y * line) for y in range(height))
+    blocks = b"".join(struct.pack("<ii", y, width * 12) + img[y, :, ::-1].T.astype("<f4").tobytes() for y in range(height))
+    with open(path, "wb") as f:
+        f.write(bytes(header) + table + blocks)
+    return img
+
+
+def _emitter(kind, props):
+    out = ['<emitter type="%s">' % kind]
+    for k, v in props.items():
+        if isinstance(v, str):
+            out.append('<string name="%s" value="%s"/>' % (k, v))
+        elif np.ndim(v) == 0:
+            out.append('<float name="%s" value="%s"/>' % (k, _fmt(v)))
+        elif k == "position":
+            out.append('<point name="%s" value="%s, %s, %s"/>' % ((k,) + tuple(_fmt(x) for x in v)))
+        elif k == "direction":
+            out.append('<vector name="%s" value="%s, %s, %s"/>' % ((k,) + tuple(_fmt(x) for x in v)))
+        else:
+            out.append(_color(k, v))
+    out.append("</emitter>")
+    return "\n".join(out)
+
+
+LIGHTS = {
+    "point": ("point", {"position": (0.6, 1.6, 0.9), "power": (60.0, 55.0, 45.0)}),
+    "spot": ("spot", {"position": (-0.8, 2.0, 1.0), "direction": (0.35, -1.0, -0.45), "power": (150.0, 150.0, 150.0),
+                      "spot_size": 50.0, "blend": 0.3}),
+    "directional": ("directional", {"direction": (-0.4, -1.0, -0.3), "irradiance": (1.5, 1.4, 1.2)}),
+}
+
+
+def lights(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gpu", emitters=("point",), env=False,
+           area=False, media=False):
+    """An open scene: a ground quad and three spheres (matte, plastic, glass) under the
+    given light sources: names from LIGHTS (point, spot, directional), an environment map
+    (env=True, write_env_exr) and/or a small area light (area=True); standalone emitters
+    come after the primitives in the file. media=True fills the glass sphere with a
+    homogeneous medium (for volpath). Returns the XML path."""
+    os.makedirs(out_dir, exist_ok=True)
+    write_plane_obj(os.path.join(out_dir, "plane.obj"))
+    xml = ["<scene>", _camera((0.0, 1.2, 4.0), (0.0, 0.3, 0.0), 40, width, height),
+           '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
+           '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
+    xml += ["<primitive>", _transform([("scale", (4, 1, 4))]),
+            '<shape type="mesh"><string name="filename" value="plane.obj"/></shape>',
+            '<material type="matte">' + _color("albedo", (0.6, 0.6, 0.6)) + "</material>", "</primitive>"]
+    spheres = [((-0.9, 0.45, 0.0), '<material type="matte">' + _color("albedo", (0.8, 0.3, 0.2)) + "</material>"),
+               ((0.0, 0.45, -0.4), '<material type="plastic">' + _color("Kd", (0.2, 0.4, 0.8)) +
+                '<float name="eta" value="1.5"/><float name="roughness" value="0.3"/></material>'),
+               ((0.9, 0.45, 0.2), '<material type="glass"><float name="eta" value="1.5"/>' +
+                (_medium("inside", (0.05, 0.05, 0.05), (0.6, 0.5, 0.4), 0.3) if media else "") + "</material>")]
+    for c, m in spheres:
+        xml += ["<primitive>", _transform([("translate", c)]),
+                '<shape type="sphere"><float name="radius" value="0.45"/></shape>', m, "</primitive>"]
+    if area:
+        xml += ["<primitive>", _transform([("translate", (0.0, 2.5, 0.5))]),
+                '<shape type="sphere"><float name="radius" value="0.15"/></shape>',
+                '<material type="matte">' + _color("albedo", (0, 0, 0)) + "</material>",
+                '<emitter type="area">' + _color("radiance", (30, 30, 30)) + "</emitter>", "</primitive>"]
+    for name in emitters:
+        kind, props = LIGHTS[name]
+        xml.append(_emitter(kind, props))
+    if env:
+        write_env_exr(os.path.join(out_dir, "sky.exr"))
+        xml.append(_emitter("environment", {"filename": "sky.exr", "strength": 1.0}))
+    xml.append("</scene>")
+    path = os.path.join(out_dir, "lights.xml")
     with open(path, "w") as f:
         f.write("\n".join(xml) + "\n")
     return path

@@ -67,6 +67,12 @@ def lib():
             L.orc_post.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int,
                                    _f32p, ctypes.c_void_p]
+            L.orc_env_load.restype = ctypes.c_void_p
+            L.orc_env_load.argtypes = [ctypes.c_char_p, ctypes.c_float]
+            L.orc_env_free.argtypes = [ctypes.c_void_p]
+            L.orc_env_sample.argtypes = [ctypes.c_void_p, ctypes.c_int, _f32p, _f32p, _f32p, _f32p]
+            L.orc_env_pdf.argtypes = [ctypes.c_void_p, ctypes.c_int, _f32p, _f32p]
+            L.orc_env_eval.argtypes = [ctypes.c_void_p, ctypes.c_int, _f32p, _f32p]
             L.orc_round_half.restype = ctypes.c_float
             L.orc_round_half.argtypes = [ctypes.c_float]
             _lib = L
@@ -276,3 +282,36 @@ def post(rgb, tonemapper=0, exposure=0.0, bloom=False, threshold=1.0, radius=1.0
 
 def round_half(x):
     return float(lib().orc_round_half(x))
+
+
+class EnvMap:
+    """The oracle's environment emitter (environment.cpp) loaded from an OpenEXR file."""
+
+    def __init__(self, path, strength=1.0):
+        self.h = lib().orc_env_load(os.fsencode(path), strength)
+        if not self.h:
+            raise RuntimeError("cannot load environment map %s" % path)
+
+    def sample(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float32).reshape(-1, 2)
+        n = u.shape[0]
+        d, p, L = np.zeros((n, 3), np.float32), np.zeros(n, np.float32), np.zeros((n, 3), np.float32)
+        lib().orc_env_sample(self.h, n, _fp(u), _fp(d), _fp(p), _fp(L))
+        return d, p, L
+
+    def pdf(self, dirs):
+        d = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, 3)
+        p = np.zeros(d.shape[0], np.float32)
+        lib().orc_env_pdf(self.h, d.shape[0], _fp(d), _fp(p))
+        return p
+
+    def eval(self, dirs):
+        d = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, 3)
+        L = np.zeros((d.shape[0], 3), np.float32)
+        lib().orc_env_eval(self.h, d.shape[0], _fp(d), _fp(L))
+        return L
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_env_free(self.h)
+            self.h = None

@@ -2,7 +2,13 @@
 // textures, media, emitters, camera, film, filters, scene) and the name registry,
 // restated on the CPU.
 #include "oscene.h"
+#include <algorithm>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
 #include <iostream>
+#include <iterator>
+#include <limits>
 
 namespace orc {
 
@@ -297,6 +303,292 @@ struct AreaLight : Emitter {
     }
 };
 
+// pointlight.cpp:9-35
+struct PointLight : Emitter {
+    Vec3 position;
+    Color power;
+    explicit PointLight(const PropertyList& p)
+        : position(PropertyList::get(p.p3, std::string("position"), Vec3(0.0f, 0.0f, 0.0f))), power(p.getColor("power", Color(10.0f))) {}
+    bool isDelta() const override { return true; }
+    Color eval(const SurfaceInteraction&, const Vec3&) const override { return Color(0.0f); }
+    Color sample(const SurfaceInteraction& ref, const Vec2&, SurfaceInteraction& info, float& pdf, Ray& sr) const override {
+        Color I = power * Inv4Pi;
+        float squaredDist = (position - ref.p).lengthSquared();
+        info.p = position;
+        pdf = 1.0f;
+        sr.o = ref.p;
+        sr.d = Normalize(info.p - ref.p);
+        sr.tMin = Epsilon;
+        sr.tMax = (info.p - ref.p).length() - Epsilon;
+        sr.time = info.time;
+        return I / squaredDist;
+    }
+    float pdf(const SurfaceInteraction&, const SurfaceInteraction&) const override { return 0.0f; }
+};
+
+// spotlight.cpp:9-64
+struct SpotLight : Emitter {
+    Vec3 position, direction;
+    Color power;
+    float cosTotalWidth, cosFalloffStart;
+    explicit SpotLight(const PropertyList& p) {
+        position = PropertyList::get(p.p3, std::string("position"), Vec3(0.0f, 0.0f, 0.0f));
+        direction = Normalize(p.getVector3("direction", Vec3(0.0f, 0.0f, -1.0f)));
+        power = p.getColor("power", Color(10.0f));
+        float spotSize = p.getFloat("spot_size", 45.0f);
+        float blend = p.getFloat("blend", 0.15f);
+        float halfAngle = spotSize * 0.5f;
+        float innerAngle = halfAngle * (1.0f - blend);
+        cosTotalWidth = std::cos((Pi / 180.f) * halfAngle);
+        cosFalloffStart = std::cos((Pi / 180.f) * innerAngle);
+    }
+    bool isDelta() const override { return true; }
+    Color eval(const SurfaceInteraction&, const Vec3&) const override { return Color(0.0f); }
+    Color sample(const SurfaceInteraction& ref, const Vec2&, SurfaceInteraction& info, float& pdf, Ray& sr) const override {
+        Vec3 wi = Normalize(position - ref.p);
+        float dist = (position - ref.p).length();
+        float squaredDist = dist * dist;
+        info.p = position;
+        pdf = 1.0f;
+        sr.o = ref.p;
+        sr.d = wi;
+        sr.tMin = Epsilon;
+        sr.tMax = dist - Epsilon;
+        sr.time = ref.time;
+        float cosTheta = Dot(-wi, direction);
+        if (cosTheta <= cosTotalWidth) return Color(0.0f);
+        float falloff = 1.0f;
+        if (cosTheta < cosFalloffStart) {
+            float t = (cosTheta - cosTotalWidth) / (cosFalloffStart - cosTotalWidth);
+            falloff = (t * t) * (3.0f - 2.0f * t);
+        }
+        Color I = power * Inv4Pi;
+        return (I * falloff) / squaredDist;
+    }
+    float pdf(const SurfaceInteraction&, const SurfaceInteraction&) const override { return 0.0f; }
+};
+
+// directional.cpp:9-38
+struct DirectionalLight : Emitter {
+    Vec3 direction;   // towards the light
+    Color irradiance;
+    explicit DirectionalLight(const PropertyList& p) {
+        direction = -Normalize(p.getVector3("direction", Vec3(0.0f, -1.0f, 0.0f)));
+        irradiance = p.getColor("irradiance", Color(1.0f));
+    }
+    bool isDelta() const override { return true; }
+    Color eval(const SurfaceInteraction&, const Vec3&) const override { return Color(0.0f); }
+    Color sample(const SurfaceInteraction& ref, const Vec2&, SurfaceInteraction& info, float& pdf, Ray& sr) const override {
+        Vec3 wi = direction;
+        info.p = ref.p + wi * 1e5f;
+        info.time = ref.time;
+        pdf = 1.0f;
+        sr.o = ref.p;
+        sr.d = wi;
+        sr.tMin = Epsilon;
+        sr.tMax = std::numeric_limits<float>::max();
+        sr.time = ref.time;
+        return irradiance;
+    }
+    float pdf(const SurfaceInteraction&, const SurfaceInteraction&) const override { return 0.0f; }
+};
+
+// distribution.cpp:6-81
+struct Distribution1D {
+    std::vector<float> func, cdf;
+    float funcInt = 0.0f;
+    Distribution1D(const float* f, int n) : func(f, f + n), cdf(n + 1) {
+        cdf[0] = 0.0f;
+        for (int i = 1; i < n + 1; ++i) cdf[i] = cdf[i - 1] + func[i - 1] / n;
+        funcInt = cdf[n];
+        if (funcInt == 0.0f) {
+            for (int i = 1; i < n + 1; ++i) cdf[i] = float(i) / float(n);
+        } else {
+            for (int i = 1; i < n + 1; ++i) cdf[i] /= funcInt;
+        }
+    }
+    int count() const { return (int)func.size(); }
+    float sampleContinuous(float u, float* pdf, int* off = nullptr) const {
+        auto it = std::upper_bound(cdf.begin(), cdf.end(), u);
+        int offset = std::clamp<int>((int)std::distance(cdf.begin(), it) - 1, 0, (int)cdf.size() - 2);
+        if (off) *off = offset;
+        float du = u - cdf[offset];
+        if ((cdf[offset + 1] - cdf[offset]) > 0.0f) du /= (cdf[offset + 1] - cdf[offset]);
+        if (pdf) *pdf = (funcInt > 0.0f) ? func[offset] / funcInt : 0.0f;
+        return (offset + du) / count();
+    }
+};
+struct Distribution2D {
+    std::vector<Distribution1D> cond;
+    std::unique_ptr<Distribution1D> marginal;
+    Distribution2D(const float* data, int nu, int nv) {
+        cond.reserve(nv);
+        for (int v = 0; v < nv; ++v) cond.emplace_back(&data[v * nu], nu);
+        std::vector<float> m;
+        for (int v = 0; v < nv; ++v) m.push_back(cond[v].funcInt);
+        marginal = std::make_unique<Distribution1D>(m.data(), nv);
+    }
+    Vec2 sampleContinuous(const Vec2& u, float* pdf) const {
+        float pdfs[2];
+        int v;
+        float d1 = marginal->sampleContinuous(u.y, &pdfs[1], &v);
+        float d0 = cond[v].sampleContinuous(u.x, &pdfs[0]);
+        *pdf = pdfs[0] * pdfs[1];
+        return Vec2(d0, d1);
+    }
+    float pdf(const Vec2& p) const {
+        int iu = std::clamp<int>((int)(p.x * cond[0].count()), 0, cond[0].count() - 1);
+        int iv = std::clamp<int>((int)(p.y * marginal->count()), 0, marginal->count() - 1);
+        return cond[iv].func[iu] / marginal->funcInt;
+    }
+};
+
+// constants.h:80-98
+static Vec2 sphericalCoordinates(const Vec3& w) {
+    Vec2 r(std::acos(std::clamp(w.z, -1.0f, 1.0f)), std::atan2(w.y, w.x));
+    if (r.y < 0.0f) r.y += 2.0f * Pi;
+    return r;
+}
+static Vec3 sphericalDirection(const Vec2& p) {
+    float cosTheta = std::cos(p.x), sinTheta = std::sin(p.x), cosPhi = std::cos(p.y), sinPhi = std::sin(p.y);
+    return Vec3(sinTheta * cosPhi, sinTheta * sinPhi, cosTheta);
+}
+
+// Uncompressed scanline OpenEXR (the images the tests write), channels R, G, B as FLOAT
+// or HALF; the reference reads any file through OpenEXR (image2d.h:100-135).
+static float halfToFloat(uint16_t h) {
+    const uint32_t sign = (uint32_t)(h >> 15) << 31;
+    const uint32_t e = (h >> 10) & 31, m = h & 1023;
+    float v;
+    if (e == 0) v = std::ldexp((float)m, -24);
+    else if (e == 31) v = m ? std::numeric_limits<float>::quiet_NaN() : std::numeric_limits<float>::infinity();
+    else v = std::ldexp((float)(m | 1024), (int)e - 25);
+    return sign ? -v : v;
+}
+static void loadEXR(const std::string& path, int& w, int& h, std::vector<Color>& px) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) throw std::runtime_error("EnvMap: cannot open " + path);
+    std::vector<uint8_t> d((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    auto rd32 = [&](size_t at) { int32_t v; std::memcpy(&v, &d.at(at + 3) - 3, 4); return v; };
+    if (d.size() < 8 || rd32(0) != 20000630) throw std::runtime_error("EnvMap: not an OpenEXR file");
+    size_t pos = 8;
+    auto cstr = [&](size_t& at) { std::string s; while (d.at(at)) s += (char)d[at++]; ++at; return s; };
+    std::vector<std::pair<std::string, int>> chans;
+    int comp = -1, x0 = 0, y0 = 0, x1 = -1, y1 = -1;
+    while (d.at(pos)) {
+        std::string name = cstr(pos), type = cstr(pos);
+        int32_t n = rd32(pos);
+        size_t at = pos + 4;
+        if (name == "channels") {
+            size_t q = at;
+            while (d.at(q)) { std::string c = cstr(q); chans.push_back({c, rd32(q)}); q += 16; }
+        } else if (name == "compression") {
+            comp = d.at(at);
+        } else if (name == "dataWindow") {
+            x0 = rd32(at); y0 = rd32(at + 4); x1 = rd32(at + 8); y1 = rd32(at + 12);
+        }
+        pos = at + n;
+    }
+    ++pos;
+    if (comp != 0) throw std::runtime_error("EnvMap: only uncompressed OpenEXR files are read here");
+    w = x1 - x0 + 1;
+    h = y1 - y0 + 1;
+    if (w <= 0 || h <= 0) throw std::runtime_error("EnvMap: empty image");
+    px.assign((size_t)w * h, Color(0.0f));
+    size_t lineBytes = 0;
+    for (auto& c : chans) lineBytes += (size_t)w * (c.second == 1 ? 2 : 4);
+    for (int line = 0; line < h; ++line) {
+        uint64_t off;
+        std::memcpy(&off, &d.at(pos + 8 * (size_t)line), 8);
+        const int y = rd32(off) - y0;
+        size_t at = off + 8;
+        for (auto& c : chans) {
+            const int k = c.first == "R" ? 0 : c.first == "G" ? 1 : c.first == "B" ? 2 : -1;
+            const size_t sz = c.second == 1 ? 2 : 4;
+            for (int x = 0; x < w; ++x, at += sz) {
+                if (k < 0 || y < 0 || y >= h) continue;
+                float v;
+                if (sz == 4) std::memcpy(&v, &d.at(at), 4);
+                else { uint16_t hv; std::memcpy(&hv, &d.at(at), 2); v = halfToFloat(hv); }
+                (k == 0 ? px[(size_t)y * w + x].r : k == 1 ? px[(size_t)y * w + x].g : px[(size_t)y * w + x].b) = v;
+            }
+        }
+        (void)lineBytes;
+    }
+}
+
+// environment.cpp:13-129
+struct EnvironmentMap : Emitter {
+    std::string relPath, baseDir;
+    float strength;
+    int width = 0, height = 0;
+    std::vector<Color> bitmap;
+    std::unique_ptr<Distribution2D> distribution;
+    explicit EnvironmentMap(const PropertyList& p) : relPath(p.getString("filename")), strength(p.getFloat("strength", 1.0f)) {}
+    void setBaseDir(const std::string& d) override { baseDir = d; }
+    void activate() override {
+        std::filesystem::path abs = std::filesystem::path(relPath).is_relative() ? std::filesystem::path(baseDir) / relPath : std::filesystem::path(relPath);
+        if (!std::filesystem::is_regular_file(abs)) throw std::runtime_error("EnvMap: Invalid environment map path.");
+        if (abs.extension() != ".exr") throw std::runtime_error("EnvMap: Invalid environment map extension.");
+        loadEXR(abs.string(), width, height, bitmap);
+        // buildPDFs (environment.cpp:111-124)
+        std::vector<float> img((size_t)width * height);
+        for (int i = 0; i < height; i++) {
+            float sinTheta = (float)std::sin(M_PI * (i + 0.5f) / height);
+            for (int j = 0; j < width; j++) img[(size_t)i * width + j] = bitmap[(size_t)i * width + j].luminance() * sinTheta;
+        }
+        distribution = std::make_unique<Distribution2D>(img.data(), width, height);
+    }
+    bool isInfiniteAreaLight() const override { return true; }
+    // film.cpp:126-151
+    Color pixelBilinear(float u, float v) const {
+        float x = u * width - 0.5f, y = v * height - 0.5f;
+        int x0 = (int)std::floor(x), y0 = (int)std::floor(y);
+        float dx = x - x0, dy = y - y0;
+        int px0 = (x0 % width + width) % width;
+        int px1 = (px0 + 1) % width;
+        int py0 = std::clamp(y0, 0, height - 1), py1 = std::clamp(y0 + 1, 0, height - 1);
+        Color c00 = bitmap[(size_t)py0 * width + px0], c10 = bitmap[(size_t)py0 * width + px1];
+        Color c01 = bitmap[(size_t)py1 * width + px0], c11 = bitmap[(size_t)py1 * width + px1];
+        Color c0 = c00 * (1.0f - dx) + c10 * dx;
+        Color c1 = c01 * (1.0f - dx) + c11 * dx;
+        return c0 * (1.0f - dy) + c1 * dy;
+    }
+    Color eval(const SurfaceInteraction&, const Vec3& w) const override {
+        Vec2 sph = sphericalCoordinates(w);
+        float u = (float)(sph.y * M_1_PI * 0.5f);
+        float v = (float)(sph.x * M_1_PI);
+        return strength * pixelBilinear(u, v);
+    }
+    Color sample(const SurfaceInteraction& ref, const Vec2& u, SurfaceInteraction& info, float& pdf, Ray& sr) const override {
+        float mapPdf;
+        Vec2 uv = distribution->sampleContinuous(u, &mapPdf);
+        if (mapPdf == 0.0f) { pdf = 0.0f; return Color(0.0f); }
+        float theta = (float)(uv.y * M_PI);
+        float phi = (float)(uv.x * 2.0f * M_PI);
+        Vec3 wi = sphericalDirection(Vec2(theta, phi));
+        info.p = ref.p + wi * 1e5f;
+        info.n = -wi;
+        info.time = ref.time;
+        sr = Ray(ref.p, wi);
+        sr.time = ref.time;
+        float sinTheta = std::sin(theta);
+        if (sinTheta <= 0.0f) { pdf = 0.0f; return Color(0.0f); }
+        pdf = (float)(mapPdf / (2.0f * M_PI * M_PI * sinTheta));
+        return eval(info, wi) / pdf;
+    }
+    float pdf(const SurfaceInteraction& ref, const SurfaceInteraction& info) const override {
+        Vec3 wi = Normalize(info.p - ref.p);
+        Vec2 sph = sphericalCoordinates(wi);
+        float sinTheta = std::sin(sph.x);
+        if (sinTheta <= 0.0f) return 0.0f;
+        float u = (float)(sph.y * M_1_PI * 0.5f);
+        float v = (float)(sph.x * M_1_PI);
+        float mapPdf = distribution->pdf(Vec2(u, v));
+        return (float)(mapPdf / (2.0f * M_PI * M_PI * sinTheta));
+    }
+};
+
 // ---------------------------------------------------------------- filters, film, camera
 // filter.h:20-32
 struct BoxFilter : Filter {
@@ -489,8 +781,13 @@ void Scene::addChild(ObjectPtr c) {
             if (sampler) throw std::runtime_error("Scene: cannot add multiple samplers!");
             sampler = std::static_pointer_cast<SamplerObj>(c);
             break;
-        case EEmitter:
-            throw std::runtime_error("Scene: only area emitters attached to primitives are supported");
+        case EEmitter:   // scene.cpp:33-40
+            emitters.push_back(std::static_pointer_cast<Emitter>(c));
+            if (emitters.back()->isInfiniteAreaLight()) {
+                if (envMap) throw std::runtime_error("Scene: cannot add multiple infinite area lights!");
+                envMap = emitters.back();
+            }
+            break;
         default:
             throw std::runtime_error("Scene: cannot add specified child!");
     }
@@ -518,6 +815,10 @@ std::unique_ptr<Object> createInstance(const std::string& t, const PropertyList&
     if (t == "index") return std::make_unique<IndexMaterial>(p);
     if (t == "homogeneous") return std::make_unique<HomogeneousMedium>(p);
     if (t == "area") return std::make_unique<AreaLight>(p);
+    if (t == "point") return std::make_unique<PointLight>(p);
+    if (t == "spot") return std::make_unique<SpotLight>(p);
+    if (t == "directional") return std::make_unique<DirectionalLight>(p);
+    if (t == "environment") return std::make_unique<EnvironmentMap>(p);
     if (t == "perspective") return std::make_unique<Camera>(p, 0);
     if (t == "thinlens") return std::make_unique<Camera>(p, 1);
     if (t == "box") return std::make_unique<BoxFilter>(p);
@@ -534,3 +835,53 @@ std::unique_ptr<Object> createInstance(const std::string& t, const PropertyList&
 }
 
 }  // namespace orc
+
+// ---------------------------------------------------------------- environment-map probes
+// Direct calls into the environment emitter for the sampling tests (the reference's
+// environment_test.cpp design): load, sample, pdf, eval; the reference point is the
+// origin and the light point lies 1e5 along the direction, as in its integrators.
+extern "C" {
+void* orc_env_load(const char* path, float strength) {
+    orc::PropertyList p;
+    p.s["filename"] = path;
+    p.f["strength"] = strength;
+    auto* e = new orc::EnvironmentMap(p);
+    try {
+        e->activate();
+    } catch (...) {
+        delete e;
+        return nullptr;
+    }
+    return e;
+}
+void orc_env_free(void* e) { delete static_cast<orc::EnvironmentMap*>(e); }
+void orc_env_sample(void* h, int n, const float* u, float* dir, float* pdf, float* L) {
+    auto* e = static_cast<orc::EnvironmentMap*>(h);
+    for (int i = 0; i < n; ++i) {
+        orc::SurfaceInteraction ref, info;
+        orc::Ray sr;
+        float p = 0.0f;
+        orc::Color c = e->sample(ref, orc::Vec2(u[2 * i], u[2 * i + 1]), info, p, sr);
+        orc::Vec3 w = orc::Normalize(info.p - ref.p);
+        dir[3 * i] = w.x; dir[3 * i + 1] = w.y; dir[3 * i + 2] = w.z;
+        pdf[i] = p;
+        L[3 * i] = c.r; L[3 * i + 1] = c.g; L[3 * i + 2] = c.b;
+    }
+}
+void orc_env_pdf(void* h, int n, const float* dir, float* pdf) {
+    auto* e = static_cast<orc::EnvironmentMap*>(h);
+    for (int i = 0; i < n; ++i) {
+        orc::SurfaceInteraction ref, info;
+        orc::Vec3 w(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+        info.p = ref.p + w * 1e5f;
+        pdf[i] = e->pdf(ref, info);
+    }
+}
+void orc_env_eval(void* h, int n, const float* dir, float* L) {
+    auto* e = static_cast<orc::EnvironmentMap*>(h);
+    for (int i = 0; i < n; ++i) {
+        orc::Color c = e->eval(orc::SurfaceInteraction(), orc::Vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
+        L[3 * i] = c.r; L[3 * i + 1] = c.g; L[3 * i + 2] = c.b;
+    }
+}
+}

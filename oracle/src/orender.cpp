@@ -12,7 +12,26 @@ static inline float powerHeuristic(int nf, float fPdf, int ng, float gPdf) {
     return denom > 0.0f ? (f * f) / denom : 0.0f;
 }
 
-// path.cpp:12-181 (environment lights and AOVs are not part of this restatement)
+// Environment light seen by an escaping ray (path.cpp:42-55, volPath.cpp:124-141): MIS
+// against the environment's pdf, which the reference evaluates from the origin
+// (a default SurfaceInteraction) towards r.o + 1e5 r.d.
+static bool envMiss(const Scene& scene, const Ray& r, bool specularBounce, float pdfPrev, float nL, Color& Le, float& w) {
+    if (!scene.envMap) return false;
+    Le = scene.envMap->eval(SurfaceInteraction(), r.d);
+    if (Le.isBlack()) return false;
+    w = 1.0f;
+    if (!specularBounce) {
+        SurfaceInteraction envIsect;
+        envIsect.p = r.o + r.d * 1e5f;
+        envIsect.n = -r.d;
+        float envPdf = scene.envMap->pdf(SurfaceInteraction(), envIsect);
+        float pEnv = envPdf * (1.0f / nL);
+        w = powerHeuristic(1, pdfPrev, 1, pEnv);
+    }
+    return true;
+}
+
+// path.cpp:12-181 (AOVs are not part of this restatement)
 Color LiPath(const Scene& scene, const Ray& primary, Sampler& sampler, Arena& arena, int maxDepth, RenderStats& st) {
     Color L(0.0f), tp(1.0f);
     Ray r = primary;
@@ -25,7 +44,12 @@ Color LiPath(const Scene& scene, const Ray& primary, Sampler& sampler, Arena& ar
         SurfaceInteraction isect;
         st.rays++;
         bool hit = scene.rayIntersect(r, isect);
-        if (!hit) break;
+        if (!hit) {
+            Color Le;
+            float w;
+            if (envMiss(scene, r, specularBounce, pdfPrev, nL, Le, w)) L += tp * Le * w;
+            break;
+        }
         isect.primitive->material->computeScatteringFunctions(isect, arena);
         if (isect.primitive->emitter) {
             const Emitter* em = isect.primitive->emitter.get();
@@ -205,7 +229,12 @@ Color LiVolPath(const Scene& scene, const Ray& primary, Sampler& sampler, Arena&
             continue;
         }
         const Medium* curMedium = r.medium;
-        if (!hitSurface) break;
+        if (!hitSurface) {
+            Color Le;
+            float w;
+            if (envMiss(scene, r, specularBounce, pdfPrev, nL, Le, w)) L += tp * Le * w;
+            break;
+        }
         isect.primitive->material->computeScatteringFunctions(isect, arena);
         if (isect.primitive->emitter) {
             const Emitter* em = isect.primitive->emitter.get();

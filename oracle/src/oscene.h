@@ -52,6 +52,8 @@ struct Object {
     virtual void addChild(std::shared_ptr<Object>) { throw std::runtime_error("addChild() not implemented!"); }
     virtual void activate() {}
     virtual ClassType classType() const = 0;
+    // directory of the scene file, for objects that read files (FileResolver::resolve)
+    virtual void setBaseDir(const std::string&) {}
 };
 using ObjectPtr = std::shared_ptr<Object>;
 
@@ -230,7 +232,8 @@ struct Emitter : Object {
     virtual Color eval(const SurfaceInteraction& si, const Vec3& w) const = 0;
     virtual Color sample(const SurfaceInteraction& ref, const Vec2& u, SurfaceInteraction& info, float& pdf, Ray& shadowRay) const = 0;
     virtual float pdf(const SurfaceInteraction& ref, const SurfaceInteraction& info) const = 0;
-    bool isDelta() const { return false; }
+    virtual bool isDelta() const { return false; }             // emitter.h: EMITTER_DELTA
+    virtual bool isInfiniteAreaLight() const { return false; }  // environment.cpp:93
 };
 
 // ---------------------------------------------------------------- primitive
@@ -311,7 +314,8 @@ struct IntegratorObj : Object {
 // scene.cpp:9-71, bvh.cpp:10-66
 struct Scene : Object {
     std::vector<std::shared_ptr<Primitive>> prims;   // reordered by the TLAS build
-    std::vector<std::shared_ptr<Emitter>> emitters;
+    std::vector<std::shared_ptr<Emitter>> emitters;  // scene-file order (scene.cpp:9-43)
+    std::shared_ptr<Emitter> envMap;
     std::shared_ptr<Camera> camera;
     std::shared_ptr<SamplerObj> sampler;
     std::shared_ptr<IntegratorObj> integrator;

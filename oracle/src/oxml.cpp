@@ -276,6 +276,7 @@ struct Loader {
             if (!mesh->filename.empty() && std::filesystem::path(mesh->filename).is_relative())
                 mesh->filename = (std::filesystem::path(baseDir) / mesh->filename).string();
         }
+        sp->setBaseDir(baseDir);
         for (const XNode* k : kids) {
             if (k->tag == "ref") {
                 std::string rid = k->attr("id") ? k->attr("id") : "";
