@@ -73,6 +73,8 @@ def lib():
                 "gnd_gpu_post_dev": [_vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp, _vp],
                 "gnd_image_write_png": [ctypes.c_char_p, _vp, ctypes.c_int32, ctypes.c_int32],
                 "gnd_image_write_exr": [ctypes.c_char_p, _vp, ctypes.c_int32, ctypes.c_int32],
+                "gnd_image_read_exr": [ctypes.c_char_p, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32),
+                                       ctypes.POINTER(ctypes.c_int32)],
                 "gnd_gpu_scene_download": [_vp, ctypes.c_uint64, ctypes.c_int32, _vp, ctypes.c_int64],
                 "gnd_host_scene_desc": [_vp, ctypes.POINTER(_vp)],
                 "gnd_host_free": [_vp],
@@ -145,6 +147,16 @@ def write_exr(path, rgb):
     _check(lib().gnd_image_write_exr(os.fsencode(path), a.ctypes.data, a.shape[1], a.shape[0]), "gnd_image_write_exr")
 
 
+def read_exr(path):
+    """A scanline OpenEXR image (compression none, ZIPS or ZIP) as float RGB [h, w, 3]."""
+    w, h = ctypes.c_int32(), ctypes.c_int32()
+    _check(lib().gnd_image_read_exr(os.fsencode(path), None, 0, ctypes.byref(w), ctypes.byref(h)), "gnd_image_read_exr")
+    out = np.zeros((h.value, w.value, 3), np.float32)
+    _check(lib().gnd_image_read_exr(os.fsencode(path), out.ctypes.data, out.nbytes, ctypes.byref(w), ctypes.byref(h)),
+           "gnd_image_read_exr")
+    return out
+
+
 class SceneInfo(ctypes.Structure):
     _fields_ = [("num_nodes", ctypes.c_int64), ("num_tris", ctypes.c_int64), ("num_instances", ctypes.c_int32),
                 ("blas_on_device", ctypes.c_int32), ("fast_boxes", ctypes.c_int32), ("num_meshes", ctypes.c_int32),
@@ -163,6 +175,9 @@ class SceneDesc(ctypes.Structure):
         ("width", ctypes.c_int32), ("height", ctypes.c_int32), ("spp", ctypes.c_int32), ("max_depth", ctypes.c_int32),
         ("integrator", ctypes.c_int32), ("filter", ctypes.c_int32), ("filter_radius", ctypes.c_float * 2),
         ("filter_alpha", ctypes.c_float), ("blas_on_device", ctypes.c_int32),
+        ("env_emitter", ctypes.c_int32), ("env_width", ctypes.c_int32), ("env_height", ctypes.c_int32),
+        ("env_marginal_integral", ctypes.c_float), ("env_strength", ctypes.c_float), ("pad2", ctypes.c_int32),
+        ("env_texels", _vp), ("env_dist", _vp),
     ]
 
 

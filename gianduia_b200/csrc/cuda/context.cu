@@ -172,7 +172,16 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
                 throw Error(GND_ERR_INVALID, "instance mesh out of range");
             if (is[i].material < 0 || is[i].material >= d->num_materials) throw Error(GND_ERR_INVALID, "instance material out of range");
             if (is[i].emitter >= d->num_emitters) throw Error(GND_ERR_INVALID, "instance emitter out of range");
+            if (is[i].emitter >= 0 && reinterpret_cast<const Emitter*>(d->emitters)[is[i].emitter].type != kEmitArea)
+                throw Error(GND_ERR_INVALID, "instance emitter is not an area light");
             if (is[i].mediumIn >= d->num_media || is[i].mediumOut >= d->num_media) throw Error(GND_ERR_INVALID, "instance medium out of range");
+        }
+        const Emitter* ems = reinterpret_cast<const Emitter*>(d->emitters);
+        for (int k = 0; k < d->num_emitters; ++k) {
+            if (ems[k].type < kEmitArea || ems[k].type > kEmitEnv) throw Error(GND_ERR_INVALID, "unknown emitter type");
+            if (ems[k].type == kEmitArea && (ems[k].instance < 0 || ems[k].instance >= d->num_instances))
+                throw Error(GND_ERR_INVALID, "area emitter instance out of range");
+            if (ems[k].type == kEmitEnv && k != d->env_emitter) throw Error(GND_ERR_INVALID, "environment emitter without its map");
         }
         c->bind();
         std::lock_guard<FairMutex> lk(c->mu);
@@ -200,6 +209,28 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         v.meshes = upload<MeshRec>(*ds, c->stream, d->meshes, d->num_meshes);
         v.cdf = upload<float>(*ds, c->stream, d->cdf, d->cdf_len);
         v.origToLeaf = upload<uint32_t>(*ds, c->stream, d->orig_to_leaf, d->orig_to_leaf_len);
+        // environment map (texels + the sampling tables of distribution.cpp)
+        v.env = EnvView{};
+        v.env.emitter = -1;
+        if (d->env_emitter >= 0) {
+            const int64_t w = d->env_width, h = d->env_height;
+            const Emitter* ems = reinterpret_cast<const Emitter*>(d->emitters);
+            if (d->env_emitter >= d->num_emitters || ems[d->env_emitter].type != kEmitEnv || w <= 0 || h <= 0 ||
+                w * h > ((int64_t)1 << 28) || !d->env_texels || !d->env_dist)
+                throw Error(GND_ERR_INVALID, "bad environment map description");
+            v.env.texels = upload<float>(*ds, c->stream, d->env_texels, (size_t)(w * h * 3));
+            const float* dist = upload<float>(*ds, c->stream, d->env_dist, (size_t)(h + (h + 1) + h * w + h * (w + 1) + h));
+            v.env.margFunc = dist;
+            v.env.margCdf = dist + h;
+            v.env.condFunc = dist + h + (h + 1);
+            v.env.condCdf = v.env.condFunc + h * w;
+            v.env.condInt = v.env.condCdf + h * (w + 1);
+            v.env.width = (int32_t)w;
+            v.env.height = (int32_t)h;
+            v.env.margInt = d->env_marginal_integral;
+            v.env.strength = d->env_strength;
+            v.env.emitter = d->env_emitter;
+        }
         v.tlasRoot = d->tlas_root;
         v.numEmitters = d->num_emitters;
         v.numInstances = d->num_instances;

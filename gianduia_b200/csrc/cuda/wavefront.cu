@@ -16,6 +16,7 @@
 // not depend on which slot, pass or launch carries it. The film is accumulated in
 // 2^-24 fixed point with integer atomics: sums are independent of completion order.
 #include <algorithm>
+#include <cfloat>
 #include <chrono>
 #include <cstring>
 
@@ -193,6 +194,7 @@ struct LightSample {
     float pdf;      // solid angle; left 0 on the early return
     V3 sd;          // shadow direction
     float stmax;    // shadow tMax
+    bool delta;     // point / spot / directional: no MIS against the BSDF (emitter.h)
 };
 
 // Shape::sampleSurface in object space; returns the area pdf.
@@ -281,9 +283,170 @@ __device__ __forceinline__ V3 emitterEval(const Emitter& e, V3 n, V2 uv, V3 w) {
     return v3s(0.0f);
 }
 
-// AreaLight::sample (area.cpp:51-88)
+// ---------------------------------------------------------------- environment map
+// SphericalCoordinates (constants.h:80-85): (theta from +z, phi in [0, 2 pi))
+__device__ __forceinline__ V2 sphericalCoordinates(V3 w) {
+    const float z = w.z < -1.0f ? -1.0f : (1.0f < w.z ? 1.0f : w.z);   // std::clamp
+    V2 r{acosf(z), atan2f(w.y, w.x)};
+    if (r.y < 0.0f) r.y += 2.0f * kPi;
+    return r;
+}
+// (u, v) of a direction in the lat-long image: phi / 2 pi and theta / pi, evaluated in
+// double as the reference's float * M_1_PI expressions are (environment.cpp:31-35)
+__device__ __forceinline__ V2 envUV(V2 sph) {
+    constexpr double kInvPiD = 0.318309886183790671538;
+    return V2{(float)((double)sph.y * kInvPiD * 0.5), (float)((double)sph.x * kInvPiD)};
+}
+// Film::getPixelBilinear (film.cpp:126-151): azimuth wraps, polar angle clamps
+__device__ __forceinline__ V3 envTexel(const EnvView& e, int x, int y) {
+    const float* t = e.texels + 3 * ((size_t)y * e.width + x);
+    return v3(__ldg(t), __ldg(t + 1), __ldg(t + 2));
+}
+__device__ __forceinline__ V3 envBilinear(const EnvView& e, float u, float v) {
+    const float x = u * (float)e.width - 0.5f, y = v * (float)e.height - 0.5f;
+    const int x0 = (int)floorf(x), y0 = (int)floorf(y);
+    const float dx = x - (float)x0, dy = y - (float)y0;
+    const int px0 = (x0 % e.width + e.width) % e.width;
+    const int px1 = (px0 + 1) % e.width;
+    const int py0 = min(max(y0, 0), e.height - 1), py1 = min(max(y0 + 1, 0), e.height - 1);
+    const V3 c0 = envTexel(e, px0, py0) * (1.0f - dx) + envTexel(e, px1, py0) * dx;
+    const V3 c1 = envTexel(e, px0, py1) * (1.0f - dx) + envTexel(e, px1, py1) * dx;
+    return c0 * (1.0f - dy) + c1 * dy;
+}
+// EnvironmentMap::eval (environment.cpp:29-37)
+__device__ __forceinline__ V3 envEval(const EnvView& e, V3 w) {
+    const V2 uv = envUV(sphericalCoordinates(w));
+    return envBilinear(e, uv.x, uv.y) * e.strength;
+}
+// Distribution1D::SampleContinuous (distribution.cpp:21-35)
+__device__ __forceinline__ float dist1DSample(const float* func, const float* cdf, int n, float funcInt, float u, float& pdf,
+                                              int& off) {
+    int lo = 0, hi = n + 1;   // std::upper_bound over cdf[0..n]
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (!(u < __ldg(cdf + mid))) lo = mid + 1;
+        else hi = mid;
+    }
+    off = min(max(lo - 1, 0), n - 1);
+    float du = u - __ldg(cdf + off);
+    if ((__ldg(cdf + off + 1) - __ldg(cdf + off)) > 0.0f) du /= (__ldg(cdf + off + 1) - __ldg(cdf + off));
+    pdf = (funcInt > 0.0f) ? __ldg(func + off) / funcInt : 0.0f;
+    return ((float)off + du) / (float)n;
+}
+// EnvironmentMap::pdf (environment.cpp:75-89) for the unit direction wi from the
+// reference point; Distribution2D::Pdf (distribution.cpp:76-80)
+__device__ __forceinline__ float envPdf(const EnvView& e, V3 wi) {
+    const V2 sph = sphericalCoordinates(wi);
+    const float sinTheta = sinf(sph.x);
+    if (sinTheta <= 0.0f) return 0.0f;
+    const V2 uv = envUV(sph);
+    const int iu = min(max((int)(uv.x * (float)e.width), 0), e.width - 1);
+    const int iv = min(max((int)(uv.y * (float)e.height), 0), e.height - 1);
+    const float mapPdf = __ldg(e.condFunc + (size_t)iv * e.width + iu) / e.margInt;
+    return (float)((double)mapPdf / (2.0 * kPiD * kPiD * (double)sinTheta));
+}
+// EnvironmentMap::sample (environment.cpp:39-73)
+__device__ __noinline__ void envSample(const EnvView& e, V3 ref, V2 u, LightSample& ls) {
+    ls.pdf = 0.0f;
+    ls.Li = v3s(0.0f);
+    ls.delta = false;
+    float pdf0, pdf1;
+    int v, off0;
+    const float d1 = dist1DSample(e.margFunc, e.margCdf, e.height, e.margInt, u.y, pdf1, v);
+    const float d0 = dist1DSample(e.condFunc + (size_t)v * e.width, e.condCdf + (size_t)v * (e.width + 1), e.width,
+                                  __ldg(e.condInt + v), u.x, pdf0, off0);
+    const float mapPdf = pdf0 * pdf1;
+    if (mapPdf == 0.0f) return;
+    const float theta = (float)((double)d1 * kPiD);
+    const float phi = (float)((double)(d0 * 2.0f) * kPiD);
+    const float cosTheta = cosf(theta), sinT = sinf(theta), cosPhi = cosf(phi), sinPhi = sinf(phi);
+    const V3 wi = v3(sinT * cosPhi, sinT * sinPhi, cosTheta);   // SphericalDirection (constants.h:87-98)
+    ls.p = ref + wi * 1e5f;
+    ls.n = -wi;
+    ls.uv = V2{0.0f, 0.0f};
+    ls.sd = wi;
+    ls.stmax = INFINITY;
+    const float sinTheta = sinf(theta);
+    if (sinTheta <= 0.0f) return;
+    ls.pdf = (float)((double)mapPdf / (2.0 * kPiD * kPiD * (double)sinTheta));
+    ls.Li = cdiv(envEval(e, wi), ls.pdf);
+}
+
+// ---------------------------------------------------------------- delta emitters
+// PointLight::sample (pointlight.cpp:18-31), SpotLight::sample (spotlight.cpp:30-60),
+// DirectionalLight::sample (directional.cpp:18-34)
+__device__ __noinline__ void deltaSample(const Emitter& e, V3 ref, LightSample& ls) {
+    ls.delta = true;
+    ls.pdf = 1.0f;
+    ls.n = v3s(0.0f);
+    ls.uv = V2{0.0f, 0.0f};
+    const V3 col = v3(e.color[0], e.color[1], e.color[2]);
+    if (e.type == kEmitDirectional) {
+        const V3 wi = v3(e.dir[0], e.dir[1], e.dir[2]);
+        ls.p = ref + wi * 1e5f;
+        ls.sd = wi;
+        ls.stmax = FLT_MAX;
+        ls.Li = col;
+        return;
+    }
+    const V3 pos = v3(e.pos[0], e.pos[1], e.pos[2]);
+    const V3 I = col * kInv4Pi;
+    ls.p = pos;
+    if (e.type == kEmitPoint) {
+        const float squaredDist = lengthSq(pos - ref);
+        ls.sd = normalize(pos - ref);
+        ls.stmax = length(pos - ref) - kEpsilon;
+        ls.Li = cdiv(I, squaredDist);
+        return;
+    }
+    const V3 wi = normalize(pos - ref);
+    const float dist = length(pos - ref);
+    const float squaredDist = dist * dist;
+    ls.sd = wi;
+    ls.stmax = dist - kEpsilon;
+    const float cosTheta = dot(-wi, v3(e.dir[0], e.dir[1], e.dir[2]));
+    if (cosTheta <= e.cosTotal) {
+        ls.Li = v3s(0.0f);
+        return;
+    }
+    float falloff = 1.0f;
+    if (cosTheta < e.cosFalloff) {
+        const float t = (cosTheta - e.cosTotal) / (e.cosFalloff - e.cosTotal);
+        falloff = (t * t) * (3.0f - 2.0f * t);
+    }
+    ls.Li = cdiv(I * falloff, squaredDist);
+}
+
+// Emitter::sample for emitter ei of the scene's list: area lights below (area.cpp:51-88),
+// the delta lights and the environment above
+__device__ __forceinline__ void areaSample(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls);
 __device__ __forceinline__ void emitterSample(const SceneView& s, int ei, V3 ref, V2 u, LightSample& ls) {
     const Emitter e = s.emitters[ei];
+    if (e.type == kEmitArea) areaSample(s, e, ref, u, ls);
+    else if (e.type == kEmitEnv) envSample(s.env, ref, u, ls);
+    else deltaSample(e, ref, ls);
+}
+
+// Environment light seen by an escaping ray, weighted against the previous bounce's pdf
+// (path.cpp:42-55, volPath.cpp:124-141; the reference evaluates the environment's pdf
+// from the origin towards o + 1e5 d)
+__device__ __noinline__ V3 envMissRadiance(const SceneView& s, V3 o, V3 d, V3 tp, bool specular, float pdfPrev, float nL) {
+    if (s.env.emitter < 0) return v3s(0.0f);
+    const V3 Le = envEval(s.env, d);
+    if (isBlack(Le)) return v3s(0.0f);
+    float w = 1.0f;
+    if (!specular) {
+        const V3 p = o + d * 1e5f;
+        const float ep = envPdf(s.env, normalize(p - v3s(0.0f)));
+        const float pEnv = ep * (1.0f / nL);
+        w = powerHeuristic(pdfPrev, pEnv);
+    }
+    return (tp * Le) * w;
+}
+
+// AreaLight::sample (area.cpp:51-88)
+__device__ __forceinline__ void areaSample(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls) {
+    ls.delta = false;
     const InstShade& is = s.instS[e.instance];
     const InstTrav& it = s.instT[e.instance];
     V3 lp, ln;
@@ -631,7 +794,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
                         float phasePdf = phaseHG(dot(wo, wi), g);
                         if (phasePdf > 1e-6f) {
                             float pl = ls.pdf * lightSelectPdf;
-                            float wl = powerHeuristic(pl, phasePdf);
+                            float wl = powerHeuristic(pl, ls.delta ? 0.0f : phasePdf);
                             V3 c = ((tp * phasePdf) * Li) * wl;   // Tr applied by the shadow pass
                             sr.ox = mp.x; sr.oy = mp.y; sr.oz = mp.z; sr.tmax = ls.stmax;
                             sr.dx = ls.sd.x; sr.dy = ls.sd.y; sr.dz = ls.sd.z; sr.slot = slot;
@@ -659,12 +822,20 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
             }
             if (M == kLobesNone) {
                 // no scattering: the path reaches its surface (or escapes)
-                if (!hit) terminate = true;
-                else handOff = true;
+                if (!hit) {
+                    L = L + envMissRadiance(s, o, d, tp, specular, pdfPrev, nL);
+                    terminate = true;
+                } else {
+                    handOff = true;
+                }
                 break;
             }
             const int curMedium = medium;
-            if (!hit) { terminate = true; break; }
+            if (!hit) {
+                L = L + envMissRadiance(s, o, d, tp, specular, pdfPrev, nL);
+                terminate = true;
+                break;
+            }
             SurfInt si = surfaceInteraction(s, h, o, d);
             const InstShade& is = s.instS[h.inst];
             const Material mat = s.materials[is.material];
@@ -709,7 +880,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
                 V3 f = bsdfF<M>(bsdf, -d, wi);
                 if (!isBlack(f) && bp > 1e-6f) {
                     float pl = ls.pdf * lightSelectPdf;
-                    float wl = powerHeuristic(pl, bp);
+                    float wl = powerHeuristic(pl, ls.delta ? 0.0f : bp);
                     V3 c = (((tp * f) * Li) * fabsf(dot(si.n, wi))) * wl;
                     int smed = -1;
                     if (VOL) smed = nextMedium(-d, ls.sd, curMedium, si.n, is.hasMedia ? is.mediumIn : -1, is.hasMedia ? is.mediumOut : -1);

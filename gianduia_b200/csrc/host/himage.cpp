@@ -1,5 +1,6 @@
 // Image files of Film::savePNG / Film::saveEXR (film.cpp:154-195): an 8-bit RGB PNG and
-// a float RGB OpenEXR image, written without the reference's stb / OpenEXR libraries.
+// a float RGB OpenEXR image, written without the reference's stb / OpenEXR libraries;
+// and the OpenEXR reader of the environment map (image2d.h:100-135).
 //
 // PNG: signature, IHDR (8-bit truecolour), one IDAT holding the zlib stream of the
 // filtered scanlines (filter type 0 on every row), IEND; chunk CRCs from zlib's crc32.
@@ -10,6 +11,7 @@
 // channel order). All integers little endian.
 #include <zlib.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -18,6 +20,7 @@
 #include <vector>
 
 #include "gnd_gpu.h"
+#include "hscene.h"
 
 namespace gnd {
 void setLastError(const std::string& msg);   // thread-local message of gnd_last_error
@@ -65,9 +68,164 @@ void exrAttr(std::vector<uint8_t>& v, const char* name, const char* type, const 
     v.insert(v.end(), value.begin(), value.end());
 }
 
+// IEEE binary16 -> binary32 (exact)
+float halfToFloat(uint16_t h) {
+    const uint32_t sign = (uint32_t)(h >> 15) << 31;
+    const uint32_t e = (h >> 10) & 31u, m = h & 1023u;
+    uint32_t bits;
+    if (e == 0) {
+        if (m == 0) {
+            bits = sign;
+        } else {   // subnormal: normalise
+            int shift = 0;
+            uint32_t mm = m;
+            while (!(mm & 1024u)) { mm <<= 1; ++shift; }
+            bits = sign | ((uint32_t)(127 - 15 + 1 - shift) << 23) | ((mm & 1023u) << 13);
+        }
+    } else if (e == 31) {
+        bits = sign | 0x7f800000u | (m << 13);
+    } else {
+        bits = sign | ((e + 112u) << 23) | (m << 13);
+    }
+    float f;
+    std::memcpy(&f, &bits, 4);
+    return f;
+}
+
 }  // namespace
 
+namespace gndh {
+
+// Scanline OpenEXR: header attributes, line offset table, blocks of 1 (NO, ZIPS) or 16
+// (ZIP) scanlines; a ZIP block is a zlib stream of the block's bytes reordered (the
+// first half holds the even bytes, the second the odd ones) and delta coded.
+void readEXR(const std::string& path, int& width, int& height, std::vector<float>& rgb) {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::runtime_error("EXR: cannot open " + path);
+    std::vector<uint8_t> d;
+    uint8_t buf[65536];
+    size_t n;
+    while ((n = std::fread(buf, 1, sizeof(buf), f)) > 0) d.insert(d.end(), buf, buf + n);
+    std::fclose(f);
+    auto need = [&](size_t at, size_t len) {
+        if (at + len > d.size()) throw std::runtime_error("EXR: truncated file " + path);
+    };
+    auto rd32 = [&](size_t at) { need(at, 4); int32_t v; std::memcpy(&v, &d[at], 4); return v; };
+    auto rd64 = [&](size_t at) { need(at, 8); uint64_t v; std::memcpy(&v, &d[at], 8); return v; };
+    auto cstr = [&](size_t& at) {
+        std::string s;
+        for (;;) { need(at, 1); if (!d[at]) break; s += (char)d[at++]; }
+        ++at;
+        return s;
+    };
+    if (rd32(0) != 20000630) throw std::runtime_error("EXR: not an OpenEXR file: " + path);
+    const int32_t version = rd32(4);
+    if ((version & 0xff) != 2 || (version & 0x1e00)) throw std::runtime_error("EXR: only single-part scanline files are read");
+    struct Chan { std::string name; int type; };
+    std::vector<Chan> chans;
+    int comp = -1, x0 = 0, y0 = 0, x1 = -1, y1 = -1;
+    size_t pos = 8;
+    for (;;) {
+        need(pos, 1);
+        if (!d[pos]) break;
+        std::string name = cstr(pos), type = cstr(pos);
+        const int32_t len = rd32(pos);
+        const size_t at = pos + 4;
+        need(at, (size_t)std::max(len, 0));
+        if (name == "channels") {
+            size_t q = at;
+            while (q < at + len && d[q]) { std::string c = cstr(q); chans.push_back({c, rd32(q)}); q += 16; }
+        } else if (name == "compression") {
+            comp = d[at];
+        } else if (name == "dataWindow") {
+            x0 = rd32(at); y0 = rd32(at + 4); x1 = rd32(at + 8); y1 = rd32(at + 12);
+        }
+        pos = at + (size_t)len;
+    }
+    ++pos;
+    if (comp != 0 && comp != 2 && comp != 3) throw std::runtime_error("EXR: unsupported compression (only none, ZIPS, ZIP)");
+    width = x1 - x0 + 1;
+    height = y1 - y0 + 1;
+    if (width <= 0 || height <= 0 || (int64_t)width * height > ((int64_t)1 << 28)) throw std::runtime_error("EXR: bad data window");
+    for (const Chan& c : chans)
+        if (c.type != 1 && c.type != 2) throw std::runtime_error("EXR: channel " + c.name + " is not HALF or FLOAT");
+    std::sort(chans.begin(), chans.end(), [](const Chan& a, const Chan& b) { return a.name < b.name; });
+    size_t lineBytes = 0;
+    for (const Chan& c : chans) lineBytes += (size_t)width * (c.type == 1 ? 2 : 4);
+    const int linesPerBlock = comp == 3 ? 16 : 1;
+    const int blocks = (height + linesPerBlock - 1) / linesPerBlock;
+    rgb.assign((size_t)width * height * 3, 0.0f);
+    std::vector<uint8_t> raw, tmp;
+    for (int b = 0; b < blocks; ++b) {
+        const uint64_t off = rd64(pos + 8 * (size_t)b);
+        const int yb = rd32(off) - y0;
+        const int32_t size = rd32(off + 4);
+        need(off + 8, (size_t)std::max(size, 0));
+        const int lines = std::min(linesPerBlock, height - yb);
+        if (yb < 0 || lines <= 0) throw std::runtime_error("EXR: block outside the data window");
+        const size_t expect = lineBytes * (size_t)lines;
+        const uint8_t* src = &d[off + 8];
+        if (comp == 0 || (size_t)size == expect) {
+            if ((size_t)size != expect) throw std::runtime_error("EXR: bad block size");
+            raw.assign(src, src + expect);
+        } else {
+            tmp.assign(expect, 0);
+            uLongf outLen = (uLongf)expect;
+            if (uncompress(tmp.data(), &outLen, src, (uLong)size) != Z_OK || outLen != expect)
+                throw std::runtime_error("EXR: corrupt ZIP block");
+            for (size_t i = 1; i < expect; ++i) tmp[i] = (uint8_t)(tmp[i - 1] + tmp[i] - 128);
+            raw.resize(expect);
+            const size_t half = (expect + 1) / 2;
+            for (size_t i = 0; i < expect; ++i) raw[i] = (i & 1) ? tmp[half + i / 2] : tmp[i / 2];
+        }
+        size_t at = 0;
+        for (int l = 0; l < lines; ++l) {
+            const int y = yb + l;
+            for (const Chan& c : chans) {
+                const int k = c.name == "R" ? 0 : c.name == "G" ? 1 : c.name == "B" ? 2 : -1;
+                const size_t sz = c.type == 1 ? 2 : 4;
+                for (int x = 0; x < width; ++x, at += sz) {
+                    if (k < 0) continue;
+                    float v;
+                    if (sz == 4) {
+                        std::memcpy(&v, &raw[at], 4);
+                    } else {
+                        uint16_t hv;
+                        std::memcpy(&hv, &raw[at], 2);
+                        v = halfToFloat(hv);
+                    }
+                    rgb[3 * ((size_t)y * width + x) + k] = v;
+                }
+            }
+        }
+    }
+}
+
+}  // namespace gndh
+
 extern "C" {
+
+gnd_status gnd_image_read_exr(const char* path, float* rgb, int64_t capacity, int32_t* width, int32_t* height) {
+    try {
+        if (!path || !width || !height) throw std::runtime_error("null argument");
+        int w = 0, h = 0;
+        std::vector<float> px;
+        gndh::readEXR(path, w, h, px);
+        *width = w;
+        *height = h;
+        if (rgb) {
+            if ((int64_t)(px.size() * sizeof(float)) > capacity) throw std::runtime_error("destination too small");
+            std::memcpy(rgb, px.data(), px.size() * sizeof(float));
+        }
+        return GND_OK;
+    } catch (const std::bad_alloc&) {
+        gnd::setLastError("host allocation failed");
+        return GND_ERR_OOM;
+    } catch (const std::exception& e) {
+        gnd::setLastError(e.what());
+        return GND_ERR_INVALID;
+    }
+}
 
 gnd_status gnd_image_write_png(const char* path, const uint8_t* rgb8, int32_t w, int32_t h) {
     try {

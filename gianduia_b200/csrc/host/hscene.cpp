@@ -3,7 +3,9 @@
 // primitives, material / emitter / medium tables, area CDFs, camera).
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstring>
+#include <filesystem>
 #include <limits>
 #include <thread>
 #include <unordered_map>
@@ -357,13 +359,91 @@ void EmitterObj::addChild(std::shared_ptr<GndObject> c) {
         setColorSlot(radiance, hasRadiance, c);
     }
 }
-void EmitterObj::activate() { if (!hasRadiance) radiance = missingTexture(); }
+void EmitterObj::activate() {
+    if (type == gnd::kEmitArea && !hasRadiance) radiance = missingTexture();
+    if (type != gnd::kEmitEnv) return;
+    // environment.cpp:15-27 and buildPDFs (environment.cpp:111-124)
+    std::filesystem::path abs = std::filesystem::path(filename);
+    if (abs.is_relative()) abs = std::filesystem::path(baseDir) / abs;
+    if (!std::filesystem::is_regular_file(abs)) throw std::runtime_error("EnvMap: Invalid environment map path.");
+    if (abs.extension() != ".exr") throw std::runtime_error("EnvMap: Invalid environment map extension.");
+    readEXR(abs.string(), envWidth, envHeight, envTexels);
+    const int rows = envHeight, cols = envWidth;
+    std::vector<float> img((size_t)rows * cols);
+    for (int i = 0; i < rows; i++) {
+        const float sinTheta = (float)std::sin(M_PI * (i + 0.5f) / rows);
+        for (int j = 0; j < cols; j++) {
+            const float* t = &envTexels[3 * ((size_t)i * cols + j)];
+            img[(size_t)i * cols + j] = gnd::luminance(gnd::v3(t[0], t[1], t[2])) * sinTheta;
+        }
+    }
+    // distribution.cpp:6-64: one 1D distribution per row, the marginal over row integrals
+    auto build1D = [](const float* f, int n, float* func, float* cdf, float& funcInt) {
+        for (int i = 0; i < n; ++i) func[i] = f[i];
+        cdf[0] = 0.0f;
+        for (int i = 1; i < n + 1; ++i) cdf[i] = cdf[i - 1] + func[i - 1] / n;
+        funcInt = cdf[n];
+        if (funcInt == 0.0f) {
+            for (int i = 1; i < n + 1; ++i) cdf[i] = float(i) / float(n);
+        } else {
+            for (int i = 1; i < n + 1; ++i) cdf[i] /= funcInt;
+        }
+    };
+    const size_t mf = 0, mc = mf + rows, cf = mc + rows + 1, cc = cf + (size_t)rows * cols, ci = cc + (size_t)rows * (cols + 1);
+    envDist.assign(ci + rows, 0.0f);
+    for (int v = 0; v < rows; ++v)
+        build1D(&img[(size_t)v * cols], cols, &envDist[cf + (size_t)v * cols], &envDist[cc + (size_t)v * (cols + 1)], envDist[ci + v]);
+    build1D(&envDist[ci], rows, &envDist[mf], &envDist[mc], envMarginalIntegral);
+}
 struct AreaLightObj : EmitterObj {
     explicit AreaLightObj(const PropertyList& p) {
         if (p.hasColor("radiance")) { radiance = constColor(p.getColor("radiance", gnd::v3s(0.f))); hasRadiance = true; }
     }
 };
+// pointlight.cpp:9-12
+struct PointLightObj : EmitterObj {
+    explicit PointLightObj(const PropertyList& p) {
+        type = gnd::kEmitPoint;
+        position = p.getPoint3("position", gnd::v3s(0.0f));
+        color = p.getColor("power", gnd::v3s(10.0f));
+    }
+};
+// spotlight.cpp:11-24
+struct SpotLightObj : EmitterObj {
+    explicit SpotLightObj(const PropertyList& p) {
+        type = gnd::kEmitSpot;
+        position = p.getPoint3("position", gnd::v3s(0.0f));
+        direction = gnd::normalize(p.getVector3("direction", gnd::v3(0.0f, 0.0f, -1.0f)));
+        color = p.getColor("power", gnd::v3s(10.0f));
+        const float spotSize = p.getFloat("spot_size", 45.0f);
+        const float blend = p.getFloat("blend", 0.15f);
+        const float halfAngle = spotSize * 0.5f;
+        const float innerAngle = halfAngle * (1.0f - blend);
+        cosTotal = std::cos((gnd::kPi / 180.f) * halfAngle);
+        cosFalloff = std::cos((gnd::kPi / 180.f) * innerAngle);
+    }
+};
+// directional.cpp:9-12
+struct DirectionalLightObj : EmitterObj {
+    explicit DirectionalLightObj(const PropertyList& p) {
+        type = gnd::kEmitDirectional;
+        direction = -gnd::normalize(p.getVector3("direction", gnd::v3(0.0f, -1.0f, 0.0f)));
+        color = p.getColor("irradiance", gnd::v3s(1.0f));
+    }
+};
+// environment.cpp:15-27
+struct EnvironmentObj : EmitterObj {
+    explicit EnvironmentObj(const PropertyList& p) {
+        type = gnd::kEmitEnv;
+        filename = p.getString("filename");
+        strength = p.getFloat("strength", 1.0f);
+    }
+};
 GND_REGISTER_CLASS(AreaLightObj, "area")
+GND_REGISTER_CLASS(PointLightObj, "point")
+GND_REGISTER_CLASS(SpotLightObj, "spot")
+GND_REGISTER_CLASS(DirectionalLightObj, "directional")
+GND_REGISTER_CLASS(EnvironmentObj, "environment")
 
 // ---------------------------------------------------------------- shapes
 Bounds ShapeObj::objectBounds() const {
@@ -499,7 +579,12 @@ GND_REGISTER_CLASS(SceneReg, "scene")
 // scene.cpp:9-44
 void Scene::addChild(std::shared_ptr<GndObject> c) {
     switch (c->getClassType()) {
-        case EPrimitive: m_primitives.push_back(std::static_pointer_cast<PrimitiveObj>(c)); break;
+        case EPrimitive: {
+            auto prim = std::static_pointer_cast<PrimitiveObj>(c);
+            if (prim->emitter) m_emitterOrder.push_back(EmitterEntry{(int)m_primitives.size(), nullptr});
+            m_primitives.push_back(prim);
+            break;
+        }
         case ECamera:
             if (m_camera) throw std::runtime_error("Scene: cannot add multiple cameras!");
             m_camera = std::static_pointer_cast<CameraObj>(c);
@@ -512,8 +597,16 @@ void Scene::addChild(std::shared_ptr<GndObject> c) {
             if (m_sampler) throw std::runtime_error("Scene: cannot add multiple samplers!");
             m_sampler = std::static_pointer_cast<SamplerObj>(c);
             break;
-        case EEmitter:
-            throw std::runtime_error("Scene: only area emitters attached to primitives are supported by the GPU integrators");
+        case EEmitter: {   // scene.cpp:33-40
+            auto em = std::static_pointer_cast<EmitterObj>(c);
+            if (em->type == gnd::kEmitArea) throw std::runtime_error("Scene: an area emitter must be attached to a primitive");
+            m_emitterOrder.push_back(EmitterEntry{-1, em});
+            if (em->isInfiniteAreaLight()) {
+                if (m_envMap) throw std::runtime_error("Scene: cannot add multiple infinite area lights!");
+                m_envMap = em;
+            }
+            break;
+        }
         default:
             throw std::runtime_error("Scene: cannot add specified child!");
     }
@@ -682,7 +775,39 @@ void Scene::build() {
         rec.totalArea = total;
         fs->meshes.push_back(rec);
     }
-    // instances, materials, emitters
+    // emitters in scene-file order (scene.cpp:9-43): area lights of primitives and the
+    // standalone point, spot, directional and environment emitters
+    std::vector<int32_t> primEmitter(np, -1);
+    for (const EmitterEntry& en : m_emitterOrder) {
+        gnd::Emitter e{};
+        e.instance = -1;
+        if (en.prim >= 0) {
+            e.type = gnd::kEmitArea;
+            e.instance = en.prim;
+            e.radiance = m_primitives[en.prim]->emitter->radiance;
+            primEmitter[en.prim] = (int32_t)fs->emitters.size();
+        } else {
+            const EmitterObj& o = *en.emitter;
+            e.type = o.type;
+            e.cosTotal = o.cosTotal;
+            e.cosFalloff = o.cosFalloff;
+            e.pos[0] = o.position.x; e.pos[1] = o.position.y; e.pos[2] = o.position.z;
+            e.dir[0] = o.direction.x; e.dir[1] = o.direction.y; e.dir[2] = o.direction.z;
+            e.color[0] = o.color.x; e.color[1] = o.color.y; e.color[2] = o.color.z;
+            e.strength = o.strength;
+            if (o.type == gnd::kEmitEnv) {
+                fs->envEmitter = (int)fs->emitters.size();
+                fs->envWidth = o.envWidth;
+                fs->envHeight = o.envHeight;
+                fs->envTexels = o.envTexels;
+                fs->envDist = o.envDist;
+                fs->envMarginalIntegral = o.envMarginalIntegral;
+                fs->envStrength = o.strength;
+            }
+        }
+        fs->emitters.push_back(e);
+    }
+    // instances, materials
     for (size_t i = 0; i < np; ++i) {
         const PrimitiveObj& p = *m_primitives[i];
         gnd::InstTrav it{};
@@ -718,14 +843,7 @@ void Scene::build() {
         is.hasMedia = (attaches && (mat->inside || mat->outside)) ? 1u : 0u;
         is.mediumIn = is.hasMedia ? mediumIndex(mat->inside) : -1;
         is.mediumOut = is.hasMedia ? mediumIndex(mat->outside) : -1;
-        is.emitter = -1;
-        if (p.emitter) {
-            gnd::Emitter e{};
-            e.instance = (int32_t)i;
-            e.radiance = p.emitter->radiance;
-            is.emitter = (int32_t)fs->emitters.size();
-            fs->emitters.push_back(e);
-        }
+        is.emitter = primEmitter[i];
         fs->instT.push_back(it);
         fs->instS.push_back(is);
     }
@@ -788,6 +906,13 @@ void FlatScene::fillDesc() {
     desc.orig_to_leaf = origToLeaf.data();
     desc.orig_to_leaf_len = (int64_t)origToLeaf.size();
     desc.camera = &camera;
+    desc.env_emitter = envEmitter;
+    desc.env_width = envWidth;
+    desc.env_height = envHeight;
+    desc.env_marginal_integral = envMarginalIntegral;
+    desc.env_strength = envStrength;
+    desc.env_texels = envTexels.empty() ? nullptr : envTexels.data();
+    desc.env_dist = envDist.empty() ? nullptr : envDist.data();
 }
 
 }  // namespace gndh

@@ -86,6 +86,7 @@ public:
     V2 getVector2(const std::string& k, V2 d) const { return get(v2_, k, d); }
     V2 getPoint2(const std::string& k, V2 d) const { return get(p2_, k, d); }
     V3 getColor(const std::string& k, V3 d) const { return get(c_, k, d); }
+    V3 getPoint3(const std::string& k, V3 d) const { return get(p3_, k, d); }
     Transform getTransform(const std::string& k, const Transform& d) const { return get(t_, k, d); }
 
 private:
@@ -114,6 +115,8 @@ public:
     virtual void addChild(std::shared_ptr<GndObject>) { throw std::runtime_error("GndObject::addChild() not implemented!"); }
     virtual void activate() {}
     virtual EClassType getClassType() const = 0;
+    // directory of the scene file, for objects that read files (FileResolver::resolve)
+    virtual void setBaseDir(const std::string&) {}
     void setName(const std::string& n) { m_name = n; }
     const std::string& getName() const { return m_name; }
 
@@ -169,12 +172,28 @@ struct MaterialObj : GndObject {
 };
 
 struct EmitterObj : GndObject {
-    gnd::ColorTex radiance{};
+    int32_t type = gnd::kEmitArea;
+    gnd::ColorTex radiance{};      // area
     bool hasRadiance = false;
+    // point / spot / directional (pointlight.cpp, spotlight.cpp, directional.cpp)
+    V3 position{}, direction{}, color{};
+    float cosTotal = 0.0f, cosFalloff = 0.0f;
+    // environment map (environment.cpp): texels and sampling tables (gnd_scene_desc layout)
+    std::string filename, baseDir;
+    float strength = 1.0f;
+    int envWidth = 0, envHeight = 0;
+    std::vector<float> envTexels, envDist;
+    float envMarginalIntegral = 0.0f;
     EClassType getClassType() const override { return EEmitter; }
     void addChild(std::shared_ptr<GndObject> c) override;
     void activate() override;
+    void setBaseDir(const std::string& d) override { baseDir = d; }
+    bool isInfiniteAreaLight() const { return type == gnd::kEmitEnv; }
 };
+
+// OpenEXR scanline image (NO, ZIPS or ZIP compression; HALF or FLOAT channels): the
+// R, G, B channels as rgb floats, row-major (himage.cpp).
+void readEXR(const std::string& path, int& width, int& height, std::vector<float>& rgb);
 
 // Mesh geometry in the reference's de-indexed form (one vertex per face corner).
 struct ShapeObj : GndObject {
@@ -263,6 +282,9 @@ struct FlatScene {
     std::vector<gnd::MeshRec> meshes;
     std::vector<float> cdf;
     std::vector<uint32_t> origToLeaf;
+    std::vector<float> envTexels, envDist;
+    int envEmitter = -1, envWidth = 0, envHeight = 0;
+    float envMarginalIntegral = 0.0f, envStrength = 1.0f;
     gnd::Camera camera{};
     uint32_t tlasRoot = gnd::kEmpty;
     gnd_scene_desc desc{};
@@ -288,6 +310,14 @@ public:
     bool deviceBlas = false;
 
     std::vector<std::shared_ptr<PrimitiveObj>> m_primitives;
+    // emitters in the order the scene file adds them (scene.cpp:9-43): a primitive's
+    // area light (prim >= 0) or a standalone emitter
+    struct EmitterEntry {
+        int prim;
+        std::shared_ptr<EmitterObj> emitter;
+    };
+    std::vector<EmitterEntry> m_emitterOrder;
+    std::shared_ptr<EmitterObj> m_envMap;
     std::shared_ptr<CameraObj> m_camera;
     std::shared_ptr<SamplerObj> m_sampler;
     std::shared_ptr<Integrator> m_integrator;

@@ -213,6 +213,7 @@ public:
             if (!shape->filename.empty() && std::filesystem::path(shape->filename).is_relative())
                 shape->filename = (std::filesystem::path(baseDir_) / shape->filename).string();
         }
+        sp->setBaseDir(baseDir_);
         for (const XmlNode* k : kids) {
             if (k->tag == "ref") {
                 std::string id = k->attr("id") ? k->attr("id") : "";

@@ -114,10 +114,40 @@ struct alignas(16) Material {
 };
 
 // ---------------------------------------------------------------- emitters, media
+// Emitter kinds: area lights on primitives (area.cpp), the delta lights point, spot and
+// directional (pointlight.cpp, spotlight.cpp, directional.cpp) and the environment map
+// (environment.cpp). The emitter list keeps the scene file's order (scene.cpp:9-43).
+enum EmitterType : int32_t { kEmitArea = 0, kEmitPoint = 1, kEmitSpot = 2, kEmitDirectional = 3, kEmitEnv = 4 };
+
 struct alignas(16) Emitter {
-    int32_t instance;         // the primitive carrying the area light
-    uint32_t pad[3];
-    ColorTex radiance;
+    int32_t instance;         // area: the primitive carrying the light; -1 otherwise
+    int32_t type;             // EmitterType
+    float cosTotal;           // spot: cos of the half width
+    float cosFalloff;         // spot: cos of the angle where the falloff starts
+    ColorTex radiance;        // area radiance
+    float pos[3];             // point / spot position
+    float strength;           // environment strength
+    float dir[3];             // spot axis; directional: unit direction towards the light
+    float pad1;
+    float color[3];           // point / spot power, directional irradiance
+    float pad2;
+};
+static_assert(sizeof(Emitter) == 112, "Emitter must be 112 bytes");
+
+// Environment map for the kernels: texels (rgb, row = polar angle theta from +z, column =
+// azimuth) and the piecewise-constant 2D sampling tables of distribution.cpp (marginal
+// over rows, one conditional per row).
+struct EnvView {
+    const float* texels;
+    const float* margFunc;    // height
+    const float* margCdf;     // height + 1
+    const float* condFunc;    // height x width
+    const float* condCdf;     // height x (width + 1)
+    const float* condInt;     // height
+    int32_t width, height;
+    float margInt, strength;
+    int32_t emitter;          // index in the emitter list; -1: no environment
+    int32_t pad;
 };
 
 struct alignas(16) Medium {
@@ -167,6 +197,7 @@ struct SceneView {
     int32_t numInstances;
     int32_t fastBoxes;            // 1: bounds allow the fast slab test (traverse.cuh, nodeKeysFast)
     Camera camera;
+    EnvView env;
 };
 
 }  // namespace gnd

@@ -102,6 +102,18 @@ typedef struct gnd_scene_desc {
      * identity) and instance blasRoot fields are unset; gnd_gpu_scene_upload builds the
      * mesh trees on the GPU (gnd_host_load_xml_ex, GND_HOST_DEVICE_BLAS) */
     int32_t blas_on_device;
+    /* environment map (environment.cpp), or env_emitter = -1: texels width x height x 3
+     * floats (row = polar angle from +z, column = azimuth), then its sampling tables
+     * (distribution.cpp) in env_dist: marginal func (height), marginal cdf (height + 1),
+     * conditional funcs (height x width), conditional cdfs (height x (width + 1)),
+     * conditional integrals (height) */
+    int32_t env_emitter;          /* index in the emitter list */
+    int32_t env_width, env_height;
+    float env_marginal_integral;
+    float env_strength;
+    int32_t pad2;
+    const float* env_texels;
+    const float* env_dist;
 } gnd_scene_desc;
 
 /* ------------------------------------------------------------------ host framework */
@@ -241,6 +253,11 @@ gnd_status gnd_gpu_post_dev(gnd_gpu_ctx* ctx, const float* d_rgb, int32_t width,
  * B, G, R as the format orders them). */
 gnd_status gnd_image_write_png(const char* path, const uint8_t* rgb8, int32_t width, int32_t height);
 gnd_status gnd_image_write_exr(const char* path, const float* rgb, int32_t width, int32_t height);
+/* Reads a scanline OpenEXR image (compression none, ZIPS or ZIP; HALF or FLOAT channels)
+ * as rgb floats: the reader the environment map uses (image2d.h:100-135). With rgb = NULL
+ * only the size is returned; otherwise `capacity` bytes must hold width x height x 3
+ * floats. */
+gnd_status gnd_image_read_exr(const char* path, float* rgb, int64_t capacity, int32_t* width, int32_t* height);
 
 /* ------------------------------------------------------------------ rendering */
 /* Progress callback, the reference's Integrator::setCallback / notifyUpdate

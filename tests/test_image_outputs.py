@@ -149,3 +149,76 @@ def test_half_rounding_matches_ieee():
     ours = np.array([O.round_half(float(v)) for v in x], np.float32)
     with np.errstate(over="ignore"):
         assert np.array_equal(ours, x.astype(np.float16).astype(np.float32))
+
+
+# ---------------------------------------------------------------- OpenEXR reader
+def exr_bytes(img, compression, half=False, extra_channel=False):
+    """An OpenEXR file written here from the format specification: scanline blocks of 1
+    (none, ZIPS) or 16 (ZIP) lines; ZIP blocks reordered (even bytes, then odd) and delta
+    coded before zlib."""
+    import struct
+    import zlib
+    h, w, _ = img.shape
+    names = [b"A", b"B", b"G", b"R"] if extra_channel else [b"B", b"G", b"R"]
+    ptype = 1 if half else 2
+    hdr = bytearray(struct.pack("<II", 20000630, 2))
+
+    def attr(name, typ, value):
+        hdr.extend(name + b"\0" + typ + b"\0" + struct.pack("<i", len(value)) + value)
+
+    attr(b"channels", b"chlist", b"".join(n + b"\0" + struct.pack("<iBBBBii", ptype, 0, 0, 0, 0, 1, 1) for n in names) + b"\0")
+    attr(b"compression", b"compression", bytes([compression]))
+    box = struct.pack("<iiii", 0, 0, w - 1, h - 1)
+    attr(b"dataWindow", b"box2i", box)
+    attr(b"displayWindow", b"box2i", box)
+    attr(b"lineOrder", b"lineOrder", b"\0")
+    attr(b"pixelAspectRatio", b"float", struct.pack("<f", 1.0))
+    attr(b"screenWindowCenter", b"v2f", struct.pack("<ff", 0, 0))
+    attr(b"screenWindowWidth", b"float", struct.pack("<f", 1.0))
+    hdr.extend(b"\0")
+    dt = "<f2" if half else "<f4"
+    chan = {b"R": 0, b"G": 1, b"B": 2}
+    per = 16 if compression == 3 else 1
+    blocks = []
+    for y0 in range(0, h, per):
+        raw = b""
+        for y in range(y0, min(h, y0 + per)):
+            for n in names:
+                vals = img[y, :, chan[n]] if n in chan else np.full(w, 0.5)
+                raw += vals.astype(dt).tobytes()
+        data = raw
+        if compression in (2, 3):
+            r = np.frombuffer(raw, np.uint8)
+            t = np.concatenate([r[0::2], r[1::2]])
+            d = t.astype(np.int32).copy()
+            d[1:] = (t[1:].astype(np.int32) - t[:-1].astype(np.int32) + 128) & 255
+            data = zlib.compress(d.astype(np.uint8).tobytes())
+        blocks.append(struct.pack("<ii", y0, len(data)) + data)
+    table, off = b"", len(hdr) + 8 * len(blocks)
+    for b in blocks:
+        table += struct.pack("<Q", off)
+        off += len(b)
+    return bytes(hdr) + table + b"".join(blocks)
+
+
+@pytest.mark.parametrize("compression,half,extra", [(0, False, False), (2, False, False), (3, False, True),
+                                                    (3, True, False), (0, True, True)])
+def test_exr_reader(tmp_path, compression, half, extra):
+    rng = np.random.default_rng(compression * 10 + half)
+    img = (rng.random((37, 21, 3)) * 8).astype(np.float32)
+    if half:
+        img = img.astype(np.float16).astype(np.float32)
+    p = tmp_path / "in.exr"
+    p.write_bytes(exr_bytes(img, compression, half, extra))
+    assert np.array_equal(G.read_exr(str(p)), img)
+
+
+def test_exr_reader_round_trip_and_errors(tmp_path):
+    img = np.random.default_rng(5).random((9, 13, 3)).astype(np.float32)
+    G.write_exr(str(tmp_path / "a.exr"), img)
+    assert np.array_equal(G.read_exr(str(tmp_path / "a.exr")), img)
+    (tmp_path / "bad.exr").write_bytes(b"not an exr file at all")
+    with pytest.raises(G.GndError):
+        G.read_exr(str(tmp_path / "bad.exr"))
+    with pytest.raises(G.GndError):
+        G.read_exr(str(tmp_path / "missing.exr"))
