@@ -90,9 +90,10 @@ def _color(name, c):
     return '<color name="%s" value="%s %s %s"/>' % (name, _fmt(c[0]), _fmt(c[1]), _fmt(c[2]))
 
 
-def _camera(origin, target, fov, w, h, up=(0, 1, 0), lens=None):
+def _camera(origin, target, fov, w, h, up=(0, 1, 0), lens=None, end=None):
     """A pinhole camera, or with `lens` (a dict of thin-lens properties: lens_radius,
-    focal_distance, k1, ca_axial, ca_lateral, vignetting, blades) a thin-lens one."""
+    focal_distance, k1, ca_axial, ca_lateral, vignetting, blades) a thin-lens one. `end`:
+    (origin, target) of a toWorldEnd lookat (camera motion over the shutter)."""
     props = []
     for k, v in sorted((lens or {}).items()):
         if isinstance(v, bool):
@@ -105,6 +106,9 @@ def _camera(origin, target, fov, w, h, up=(0, 1, 0), lens=None):
         '<camera type="%s">' % ("thinlens" if lens is not None else "perspective"),
         '<transform name="toWorld"><lookat origin="%s, %s, %s" target="%s, %s, %s" up="%s, %s, %s"/></transform>'
         % tuple(_fmt(v) for v in (*origin, *target, *up)),
+        *([] if end is None else [
+            '<transform name="toWorldEnd"><lookat origin="%s, %s, %s" target="%s, %s, %s" up="%s, %s, %s"/></transform>'
+            % tuple(_fmt(v) for v in (*end[0], *end[1], *up))]),
         '<float name="fov" value="%s"/>' % _fmt(fov),
         '<integer name="width" value="%d"/>' % w,
         '<integer name="height" value="%d"/>' % h,
@@ -320,6 +324,55 @@ def microfacet(out_dir, width=1024, height=1024, spp=64, max_depth=16, grid=64, 
                 '<material type="matte">' + _color("albedo", (0, 0, 0)) + "</material>",
                 '<emitter type="area">' + _color("radiance", (50, 50, 50)) + "</emitter>", "</primitive>"]
     xml.append("</scene>")
+    with open(path, "w") as f:
+        f.write("\n".join(xml) + "\n")
+    return path
+
+
+def motion(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gpu", camera_motion=False, lens=None,
+           light_motion=True):
+    """The Cornell box with motion blur (animated.cpp): the small box slides, the tall box
+    turns 90 degrees about y while it rises and grows, a small emissive sphere moves
+    across the room (light_motion), and with camera_motion the camera pans (toWorldEnd
+    transforms, shutter time [0, 1]). Returns the XML path."""
+    os.makedirs(out_dir, exist_ok=True)
+    write_plane_obj(os.path.join(out_dir, "plane.obj"))
+    write_cube_obj(os.path.join(out_dir, "cube.obj"))
+    end = ((0.3, 0.1, 3.5), (0.1, 0.0, 0.0)) if camera_motion else None
+    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height, lens=lens, end=end),
+           '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
+           '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
+    gray = (0.75, 0.75, 0.75)
+    boxes = [
+        ([("scale", (0.6, 0.6, 0.6)), ("rotate", ((0, 1, 0), 18)), ("translate", (0.35, -0.7, 0.3))],
+         [("scale", (0.6, 0.6, 0.6)), ("rotate", ((0, 1, 0), 18)), ("translate", (0.05, -0.7, 0.45))]),
+        ([("scale", (0.6, 1.2, 0.6)), ("rotate", ((0, 1, 0), -15)), ("translate", (-0.35, -0.4, -0.3))],
+         [("scale", (0.7, 1.3, 0.5)), ("rotate", ((0, 1, 0), 75)), ("translate", (-0.3, -0.3, -0.3))]),
+    ]
+    # the Cornell body lists the walls (5 primitives), two boxes and the light: the boxes
+    # are replaced by animated ones
+    prims, cur = [], []
+    for line in _cornell_body():
+        cur.append(line)
+        if line == "</primitive>":
+            prims.append(cur)
+            cur = []
+    new_boxes = []
+    for i, (a, b) in enumerate(boxes):
+        shape = '<shape type="mesh" id="cube"><string name="filename" value="cube.obj"/></shape>' if i == 0 else '<ref id="cube"/>'
+        new_boxes.append(["<primitive>", _transform(a), _transform(b, name="toWorldEnd"), shape,
+                          '<material type="matte">', _color("albedo", gray), "</material>", "</primitive>"])
+    prims = prims[:5] + new_boxes + prims[7:]
+    for p_ in prims:
+        xml += p_
+    if light_motion:
+        xml += ["<primitive>", _transform([("translate", (-0.6, 0.5, 0.4))]),
+                _transform([("translate", (0.6, 0.2, 0.1))], name="toWorldEnd"),
+                '<shape type="sphere"><float name="radius" value="0.08"/></shape>',
+                '<material type="matte">' + _color("albedo", (0, 0, 0)) + "</material>",
+                '<emitter type="area">' + _color("radiance", (40, 30, 20)) + "</emitter>", "</primitive>"]
+    xml.append("</scene>")
+    path = os.path.join(out_dir, "motion.xml")
     with open(path, "w") as f:
         f.write("\n".join(xml) + "\n")
     return path

@@ -73,6 +73,7 @@ def lib():
             L.orc_env_sample.argtypes = [ctypes.c_void_p, ctypes.c_int, _f32p, _f32p, _f32p, _f32p]
             L.orc_env_pdf.argtypes = [ctypes.c_void_p, ctypes.c_int, _f32p, _f32p]
             L.orc_env_eval.argtypes = [ctypes.c_void_p, ctypes.c_int, _f32p, _f32p]
+            L.orc_motion_interpolate.argtypes = [_f32p, _f32p, ctypes.c_float, _f32p, _f32p]
             L.orc_round_half.restype = ctypes.c_float
             L.orc_round_half.argtypes = [ctypes.c_float]
             _lib = L
@@ -315,3 +316,14 @@ class EnvMap:
         if getattr(self, "h", None):
             lib().orc_env_free(self.h)
             self.h = None
+
+
+def motion_interpolate(a, b, t):
+    """AnimatedTransform::interpolate between 4x4 matrices a (time 0) and b (time 1):
+    returns the 3x4 matrix at time t and its inverse."""
+    a = np.ascontiguousarray(a, np.float32).reshape(4, 4)
+    b = np.ascontiguousarray(b, np.float32).reshape(4, 4)
+    m = np.zeros((3, 4), np.float32)
+    mi = np.zeros((3, 4), np.float32)
+    lib().orc_motion_interpolate(_fp(a), _fp(b), t, _fp(m), _fp(mi))
+    return m, mi

@@ -510,20 +510,21 @@ float Cube::sampleSurface(const Vec3&, const Vec2& s, SurfaceInteraction& info) 
 
 // ---------------------------------------------------------------- primitive, scene BVH
 
-// primitive.cpp:48-59 (static transform: worldToObject is the stored inverse)
+// primitive.cpp:48-59 (worldToObject = the interpolated transform's inverse)
 bool Primitive::rayIntersect(const Ray& rWorld, SurfaceInteraction& si, bool predicate, TraversalStats* st) const {
-    Ray rLocal = toWorld.inverse().ray(rWorld);
+    Ray rLocal = anim.interpolate(rWorld.time).inverse().ray(rWorld);
     if (!shape->rayIntersect(rLocal, si, predicate, st)) return false;
     si.primitive = this;
     return true;
 }
 // primitive.cpp:61-72
 void Primitive::fillInteraction(const Ray& rWorld, SurfaceInteraction& si) const {
-    Ray rLocal = toWorld.inverse().ray(rWorld);
+    const Transform tw = anim.interpolate(rWorld.time);
+    Ray rLocal = tw.inverse().ray(rWorld);
     shape->fillInteraction(rLocal, si);
-    si.p = toWorld.point(si.p);
-    si.n = Normalize(toWorld.normal(si.n));
-    si.dpdu = Normalize(toWorld.vector(si.dpdu));
+    si.p = tw.point(si.p);
+    si.n = Normalize(tw.normal(si.n));
+    si.dpdu = Normalize(tw.vector(si.dpdu));
     si.time = rWorld.time;
 }
 

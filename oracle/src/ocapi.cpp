@@ -385,3 +385,16 @@ float orc_hg(int op, float g, const float* wo, const float* x, float* out) {
 }
 
 }  // extern "C"
+
+// AnimatedTransform::interpolate (animated.cpp:29-47) between two affine matrices given
+// row-major 4x4; out: the interpolated 3x4 matrix and its inverse (row-major).
+extern "C" void orc_motion_interpolate(const float* a, const float* b, float time, float* out, float* outInv) {
+    orc::Mat4 ma, mb;
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) { ma.c[c][r] = a[4 * r + c]; mb.c[c][r] = b[4 * r + c]; }
+    orc::AnimatedTransform at;
+    at.set(orc::Transform(ma, orc::Mat4()), orc::Transform(mb, orc::Mat4()));
+    orc::Transform t = at.interpolate(time);
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) { out[4 * r + c] = t.m.c[c][r]; outInv[4 * r + c] = t.mInv.c[c][r]; }
+}

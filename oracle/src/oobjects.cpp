@@ -259,7 +259,7 @@ struct AreaLight : Emitter {
     // area.cpp:51-88 (pdf is left unwritten on the early return, as in the reference)
     Color sample(const SurfaceInteraction& ref, const Vec2& u, SurfaceInteraction& info, float& pdf, Ray& sr) const override {
         SurfaceInteraction local;
-        const Transform& tw = prim->toWorld;
+        const Transform tw = prim->getToWorld(ref.time);   // area.cpp:54
         float areaPdf = prim->shape->sampleSurface(ref.p, u, local);
         info.p = tw.point(local.p);
         info.n = Normalize(tw.normal(local.n));
@@ -285,7 +285,7 @@ struct AreaLight : Emitter {
     // area.cpp:90-119
     float pdf(const SurfaceInteraction& ref, const SurfaceInteraction& info) const override {
         SurfaceInteraction local;
-        const Transform tw = prim->toWorld;
+        const Transform tw = prim->getToWorld(ref.time);   // area.cpp:92
         const Transform tl = tw.inverse();
         local.p = tl.point(info.p);
         local.n = tl.normal(info.n);
@@ -651,8 +651,7 @@ void Film::addSample(const Vec2& pFilm, const Color& L) {
 // camera.h:30-52, perspective.cpp:9-12
 Camera::Camera(const PropertyList& p, int k) {
     toWorld = p.getTransform("toWorld", Transform());
-    if (p.hasTransform("toWorldEnd") && !(p.getTransform("toWorldEnd") == toWorld))
-        throw std::runtime_error("Camera: animated transforms are not supported by this restatement");
+    anim.set(toWorld, p.getTransform("toWorldEnd", toWorld));   // camera.h:20-25
     width = p.getInteger("width", 1280);
     height = p.getInteger("height", 720);
     fov = p.getFloat("fov", 45.0f);
@@ -684,7 +683,7 @@ float Camera::shootRay(const CameraSample& s, Ray* ray) const {
         float y = (2.0f * s.pFilm.y - 1.0f) * scale;
         Vec3 dir = Normalize(Vec3(x, y, -1.0f));
         Ray rc(Vec3(0, 0, 0), dir);
-        *ray = toWorld.ray(rc);
+        *ray = anim.interpolate(s.time).ray(rc);
         ray->time = s.time;
         return 1.0f;
     }
@@ -723,17 +722,17 @@ float Camera::shootRay(const CameraSample& s, Ray* ray) const {
         finalTime = scanline * scanDuration + (s.time * exposureDuration);
     }
     Ray rc(rayOrigin, dir);
-    *ray = toWorld.ray(rc);
+    *ray = anim.interpolate(finalTime).ray(rc);
     ray->time = finalTime;
     return weight;
 }
 
 // ---------------------------------------------------------------- primitive, scene
 // primitive.cpp:7-46
+// primitive.cpp:6-11
 Primitive::Primitive(const PropertyList& p) {
     toWorld = p.getTransform("toWorld", Transform());
-    if (p.hasTransform("toWorldEnd") && !(p.getTransform("toWorldEnd") == toWorld))
-        throw std::runtime_error("Primitive: animated transforms are not supported by this restatement");
+    anim.set(toWorld, p.getTransform("toWorldEnd", toWorld));
 }
 void Primitive::addChild(ObjectPtr c) {
     if (c->classType() == EShape) {

@@ -3,6 +3,7 @@
 // restated on the CPU. Used only as the checker for the GPU path.
 #pragma once
 #include "omath.h"
+#include "omotion.h"
 #include "osampling.h"
 #include "obsdf.h"
 #include <atomic>
@@ -242,7 +243,8 @@ struct Primitive : Object {
     std::shared_ptr<Shape> shape;
     std::shared_ptr<Material> material;
     std::shared_ptr<Emitter> emitter;
-    Transform toWorld;
+    Transform toWorld;            // the start transform
+    AnimatedTransform anim;       // toWorld -> toWorldEnd over time [0, 1]
     int originalIndex = -1;
     explicit Primitive(const PropertyList& p);
     ClassType classType() const override { return EPrimitive; }
@@ -250,7 +252,8 @@ struct Primitive : Object {
     void activate() override;
     bool rayIntersect(const Ray& rWorld, SurfaceInteraction& si, bool predicate, TraversalStats* st) const;
     void fillInteraction(const Ray& rWorld, SurfaceInteraction& si) const;
-    Bounds3 getWorldBounds() const { return toWorld.bounds(shape->getBounds()); }
+    Bounds3 getWorldBounds() const { return anim.motionBounds(shape->getBounds()); }   // primitive.cpp:74-76
+    Transform getToWorld(float time) const { return anim.interpolate(time); }
 };
 
 // ---------------------------------------------------------------- camera, film
@@ -279,6 +282,7 @@ struct CameraSample {
 
 struct Camera : Object {
     Transform toWorld;
+    AnimatedTransform anim;   // toWorld -> toWorldEnd over the shutter time [0, 1]
     int width, height;
     float fov, scale;
     // thinLens.cpp:13-31 (kind 1); kind 0 is the pinhole `perspective` camera
