@@ -32,8 +32,10 @@ CAMERA_DTYPE = np.dtype([("to_world", np.float32, (3, 4)), ("width", np.int32), 
                          ("scale", np.float32), ("aspect", np.float32), ("origin", np.float32, 3), ("pad", np.float32),
                          ("kind", np.int32), ("blades", np.int32), ("lens_radius", np.float32),
                          ("focal_distance", np.float32), ("k1", np.float32), ("ca_axial", np.float32),
-                         ("ca_lateral", np.float32), ("vignetting", np.int32)])
-assert CAMERA_DTYPE.itemsize == 112
+                         ("ca_lateral", np.float32), ("vignetting", np.int32), ("rolling_shutter", np.int32),
+                         ("scan_duration", np.float32), ("exposure_duration", np.float32), ("animated", np.int32),
+                         ("motion", np.float32, 48)])
+assert CAMERA_DTYPE.itemsize == 320
 # BVH4 node (gnd::Node4): child bounds as rows lox, hix, loy, hiy, loz, hiz
 NODE_DTYPE = np.dtype([("lo_hi", np.float32, (6, 4)), ("child", np.uint32, 4), ("pad", np.uint32, 4)])
 
@@ -177,7 +179,7 @@ class SceneDesc(ctypes.Structure):
         ("filter_alpha", ctypes.c_float), ("blas_on_device", ctypes.c_int32),
         ("env_emitter", ctypes.c_int32), ("env_width", ctypes.c_int32), ("env_height", ctypes.c_int32),
         ("env_marginal_integral", ctypes.c_float), ("env_strength", ctypes.c_float), ("pad2", ctypes.c_int32),
-        ("env_texels", _vp), ("env_dist", _vp),
+        ("env_texels", _vp), ("env_dist", _vp), ("inst_motion", _vp),
     ]
 
 

@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(kBuildBlock) kGather(const uint32_t* __restric
 __global__ void kPatch(InstTrav* instT, const InstShade* __restrict__ instS, int numInstances,
                        const uint32_t* __restrict__ base, int M, uint32_t firstNode) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= numInstances || instT[i].kind != kShapeMesh) return;
+    if (i >= numInstances || (instT[i].kind & ~kInstAnimated) != kShapeMesh) return;
     const uint32_t m = instS[i].meshId;
     instT[i].blasRoot = ((int)m < M && base[m + 1] > base[m]) ? firstNode + m : kEmpty;
 }

@@ -166,12 +166,15 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         const InstTrav* it = reinterpret_cast<const InstTrav*>(d->inst_trav);
         const InstShade* is = reinterpret_cast<const InstShade*>(d->inst_shade);
         for (int i = 0; i < d->num_instances; ++i) {
-            if (!deviceBlas && it[i].kind == kShapeMesh && it[i].blasRoot != kEmpty && (int64_t)it[i].blasRoot >= d->num_nodes)
+            const uint32_t kind = it[i].kind & ~kInstAnimated;
+            if (!deviceBlas && kind == kShapeMesh && it[i].blasRoot != kEmpty && (int64_t)it[i].blasRoot >= d->num_nodes)
                 throw Error(GND_ERR_INVALID, "instance root out of range");
-            if (deviceBlas && it[i].kind == kShapeMesh && (int64_t)is[i].meshId >= d->num_meshes)
+            if (deviceBlas && kind == kShapeMesh && (int64_t)is[i].meshId >= d->num_meshes)
                 throw Error(GND_ERR_INVALID, "instance mesh out of range");
             if (is[i].material < 0 || is[i].material >= d->num_materials) throw Error(GND_ERR_INVALID, "instance material out of range");
             if (is[i].emitter >= d->num_emitters) throw Error(GND_ERR_INVALID, "instance emitter out of range");
+            if ((it[i].kind & kInstAnimated) && !d->inst_motion) throw Error(GND_ERR_INVALID, "animated instance without motion records");
+            if ((it[i].kind & ~kInstAnimated) > kShapeCube) throw Error(GND_ERR_INVALID, "unknown shape kind");
             if (is[i].emitter >= 0 && reinterpret_cast<const Emitter*>(d->emitters)[is[i].emitter].type != kEmitArea)
                 throw Error(GND_ERR_INVALID, "instance emitter is not an area light");
             if (is[i].mediumIn >= d->num_media || is[i].mediumOut >= d->num_media) throw Error(GND_ERR_INVALID, "instance medium out of range");
@@ -209,6 +212,7 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         v.meshes = upload<MeshRec>(*ds, c->stream, d->meshes, d->num_meshes);
         v.cdf = upload<float>(*ds, c->stream, d->cdf, d->cdf_len);
         v.origToLeaf = upload<uint32_t>(*ds, c->stream, d->orig_to_leaf, d->orig_to_leaf_len);
+        v.motion = d->inst_motion ? upload<InstMotion>(*ds, c->stream, d->inst_motion, d->num_instances) : nullptr;
         // environment map (texels + the sampling tables of distribution.cpp)
         v.env = EnvView{};
         v.env.emitter = -1;
@@ -284,6 +288,10 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         nanBounds |= (vf & kNodeSlowBounds) != 0;
         v.fastBoxes = nanBounds ? 0 : 1;
         if (d->camera) std::memcpy(&v.camera, d->camera, sizeof(Camera));
+        // the rarer features select the kernels' EXT variants
+        bool ext = v.motion != nullptr || v.env.emitter >= 0 || v.camera.kind == kCamThinLens || v.camera.animated != 0;
+        for (int k = 0; k < d->num_emitters; ++k) ext = ext || ems[k].type != kEmitArea;
+        v.ext = ext ? 1 : 0;
         // null-BSDF mask and material type per instance
         std::vector<uint8_t> mask(std::max(1, d->num_instances), 0), cls(std::max(1, d->num_instances), kMatIndex);
         const Material* mats = reinterpret_cast<const Material*>(d->materials);

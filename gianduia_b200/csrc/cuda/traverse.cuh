@@ -12,12 +12,14 @@
 // without sorting), so among hits at exactly equal t a different primitive may win.
 #pragma once
 #include "gnd/layout.h"
+#include "gnd/motion.h"
 
 namespace gnd {
 
 struct TRay {
     V3 o, d;
     float tmin, tmax;
+    float time = 0.0f;   // shutter time; moves animated instances (primitive.cpp:48-50)
 };
 
 struct THit {
@@ -108,12 +110,30 @@ __device__ __forceinline__ bool cubeTest(V3 ex, V3 o, V3 d, float tmin, float tm
     return true;
 }
 
+// World-to-object rows of animated instance `id` at `time` (primitive.cpp:49:
+// m_objectToWorld.interpolate(time).inverse()); r0..r2 hold the start transform's rows on
+// entry, which stay for time <= 0. Only the MOTION variants of the traversal call it
+// (scenes with animated instances); rays at time 0 (user ray batches) need none.
+__device__ __forceinline__ void animatedW2ORows(const SceneView& s, uint32_t id, float time, float4& r0, float4& r1, float4& r2) {
+    if (time <= 0.0f) return;
+    Xf34 w;
+    if (time >= 1.0f) {
+        w = s.motion[id].endW2O;
+    } else {
+        Xf34 m;
+        motionCompose(s.motion[id], (time - 0.0f) / (1.0f - 0.0f), m, w);
+    }
+    r0 = make_float4(w.r[0][0], w.r[0][1], w.r[0][2], w.r[0][3]);
+    r1 = make_float4(w.r[1][0], w.r[1][1], w.r[1][2], w.r[1][3]);
+    r2 = make_float4(w.r[2][0], w.r[2][1], w.r[2][2], w.r[2][3]);
+}
+
 // Trace one ray. ANY: stop at the first hit (occlusion query). SKIP_NULL: ignore
 // instances whose material has no BSDF (index material) -- used by the path
 // integrator's shadow rays. COUNT: accumulate node visits and triangle tests.
 // `stk` points at this thread's first stack entry in shared memory; entries are
 // BLOCK apart. Returns an error bitmask (0 on success).
-template <int BLOCK, bool ANY, bool SKIP_NULL, bool COUNT>
+template <int BLOCK, bool ANY, bool SKIP_NULL, bool COUNT, bool MOTION = false>
 __device__ __forceinline__ int traceRay(const SceneView& s, const TRay& ray, THit& hit, uint32_t* stk,
                                         TraceCounters* cnt, const uint8_t* nullMask) {
     hit.t = INFINITY;
@@ -210,6 +230,8 @@ __device__ __forceinline__ int traceRay(const SceneView& s, const TRay& ray, THi
             float4 r0 = ldg4(&it->w2o.r[0][0]), r1 = ldg4(&it->w2o.r[1][0]), r2 = ldg4(&it->w2o.r[2][0]);
             float4 meta = ldg4(&it->kind);
             uint32_t kind = __float_as_uint(meta.x);
+            if (MOTION && (kind & kInstAnimated)) animatedW2ORows(s, id, ray.time, r0, r1, r2);
+            kind &= ~kInstAnimated;
             // primitive.cpp:49-50: rLocal = worldToObject(rWorld), tMin = Epsilon
             V3 lo, ld;
             lo.x = (r0.x * wo.x + r0.y * wo.y) + (r0.z * wo.z + r0.w);
@@ -270,6 +292,7 @@ constexpr int kPStackMax = 128;   // entries per ray, shared + local
 
 struct Trav {
     V3 wo, wd;          // world ray
+    float time;         // shutter time (animated instances)
     V3 o, d, inv;       // current ray (world, or object space inside a bottom-level tree)
     float wtmin, tmin, tmax, bestT;
     int curInst;
@@ -309,6 +332,7 @@ __device__ __forceinline__ void travInit(Trav& t, const SceneView& s, const TRay
     t.inv = v3(__frcp_rn(ray.d.x), __frcp_rn(ray.d.y), __frcp_rn(ray.d.z));
     t.fast = t.wfast = slabFinite(s, t.o, t.inv) && !isnan(ray.tmin) && !isnan(ray.tmax);
     t.wtmin = ray.tmin; t.tmin = ray.tmin; t.tmax = ray.tmax;
+    t.time = ray.time;
     t.bestT = 3.402823466e38f;
     t.curInst = -1;
     t.leaf = kEmpty;
@@ -440,7 +464,7 @@ __device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<
 }
 
 // Processes one primitive of the pending leaf. For ANY, a hit ends the ray (sp = 0).
-template <int BLOCK, bool ANY, bool COUNT, int SMEM>
+template <int BLOCK, bool ANY, bool COUNT, int SMEM, bool MOTION>
 __device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<BLOCK, SMEM>& st, TraceCounters* cnt,
                                             const uint8_t* nullMask) {
     uint32_t first = leafFirst(t.leaf), count = leafCount(t.leaf);
@@ -466,6 +490,8 @@ __device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<
     float4 r0 = ldg4(&it->w2o.r[0][0]), r1 = ldg4(&it->w2o.r[1][0]), r2 = ldg4(&it->w2o.r[2][0]);
     float4 meta = ldg4(&it->kind);
     uint32_t kind = __float_as_uint(meta.x);
+    if (MOTION && (kind & kInstAnimated)) animatedW2ORows(s, id, t.time, r0, r1, r2);
+    kind &= ~kInstAnimated;
     V3 lo, ld;
     lo.x = (r0.x * t.wo.x + r0.y * t.wo.y) + (r0.z * t.wo.z + r0.w);
     lo.y = (r1.x * t.wo.x + r1.y * t.wo.y) + (r1.z * t.wo.z + r1.w);
@@ -531,7 +557,7 @@ __device__ __forceinline__ uint32_t warpFetch(uint32_t* counter, bool want) {
 //   uint32_t count()                      number of rays
 //   bool load(uint32_t i, TRay&, const SceneView*&, const uint8_t*& nullMask)
 //   void store(uint32_t i, const THit&)   (closest) / store(i, bool) (any)
-template <int BLOCK, bool ANY, bool COUNT, int SMEM = kSmemStack, bool SPEC = false, typename Src>
+template <int BLOCK, bool ANY, bool COUNT, int SMEM = kSmemStack, bool SPEC = false, bool MOTION = false, typename Src>
 __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter, uint32_t* smemStack, TraceCounters* cnt) {
     TStack<BLOCK, SMEM> st;
     st.smem = smemStack + threadIdx.x;
@@ -592,7 +618,7 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
             bool want = active && t.leaf != kEmpty;
             if (!__any_sync(0xffffffffu, want)) break;
             if (want) {
-                int e = travLeafStep<BLOCK, ANY, COUNT, SMEM>(t, *sv, st, cnt, nm);
+                int e = travLeafStep<BLOCK, ANY, COUNT, SMEM, MOTION>(t, *sv, st, cnt, nm);
                 if (e) { err |= e; t.sp = 0; t.leaf = kEmpty; t.next = kEmpty; }
             }
         }

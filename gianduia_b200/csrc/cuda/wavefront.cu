@@ -85,6 +85,7 @@ struct KParams {
     uint32_t* freeOut;
     uint32_t* errWord;
     uint32_t* classLists;          // shade-class lists, `capacity` entries each
+    float* slotTime;               // per path slot: the path's shutter time (ray.h: time)
     uint32_t capacity;
     uint32_t fifo;                 // 1: grabs walk the active list from its first job
 };
@@ -142,16 +143,18 @@ __device__ __forceinline__ SurfInt meshInteraction(const SceneView& s, uint32_t 
     return si;
 }
 
-// Primitive::fillInteraction (primitive.cpp:61-72) for the closest hit of world ray (o, d).
-__device__ __forceinline__ SurfInt surfaceInteraction(const SceneView& s, const HitRec& h, V3 o, V3 d) {
+// Primitive::fillInteraction (primitive.cpp:61-72) for the closest hit of world ray (o, d),
+// with the instance's transforms o2w / w2o.
+__device__ __forceinline__ SurfInt surfaceInteractionWith(const SceneView& s, const HitRec& h, V3 o, V3 d, const Xf34& o2w,
+                                                          const Xf34& w2o) {
     const InstTrav& it = s.instT[h.inst];
     const InstShade& is = s.instS[h.inst];
-    uint32_t kind = it.kind;
+    const uint32_t kind = it.kind & ~kInstAnimated;
     SurfInt si;
     if (kind == kShapeMesh) {
         si = meshInteraction(s, h.slot, h.u, h.v);
     } else {
-        V3 lo = xfPoint(it.w2o, o), ld = xfVector(it.w2o, d);
+        V3 lo = xfPoint(w2o, o), ld = xfVector(w2o, d);
         si.p = lo + ld * h.t;
         if (kind == kShapeSphere) {     // sphere.cpp:41-55
             si.n = normalize(si.p);
@@ -180,10 +183,23 @@ __device__ __forceinline__ SurfInt surfaceInteraction(const SceneView& s, const 
             }
         }
     }
-    si.p = xfPoint(is.o2w, si.p);
-    si.n = normalize(xfNormal(it.w2o, si.n));
-    si.dpdu = normalize(xfVector(is.o2w, si.dpdu));
+    si.p = xfPoint(o2w, si.p);
+    si.n = normalize(xfNormal(w2o, si.n));
+    si.dpdu = normalize(xfVector(o2w, si.dpdu));
     return si;
+}
+
+// The same for an animated instance at shutter time `time` (Primitive::getToWorld,
+// primitive.cpp:62 and 82-84). Out of line, so that static scenes keep their registers.
+__device__ __noinline__ SurfInt surfaceInteractionMoving(const SceneView& s, const HitRec& h, V3 o, V3 d, float time) {
+    Xf34 o2w, w2o;
+    motionAt(s.motion[h.inst], s.instS[h.inst].o2w, s.instT[h.inst].w2o, time, o2w, w2o);
+    return surfaceInteractionWith(s, h, o, d, o2w, w2o);
+}
+
+__device__ __forceinline__ SurfInt surfaceInteraction(const SceneView& s, const HitRec& h, V3 o, V3 d, float time) {
+    if (s.instT[h.inst].kind & kInstAnimated) return surfaceInteractionMoving(s, h, o, d, time);
+    return surfaceInteractionWith(s, h, o, d, s.instS[h.inst].o2w, s.instT[h.inst].w2o);
 }
 
 // ---------------------------------------------------------------- area emitters (area.cpp)
@@ -194,6 +210,7 @@ struct LightSample {
     float pdf;      // solid angle; left 0 on the early return
     V3 sd;          // shadow direction
     float stmax;    // shadow tMax
+    float stime;    // shadow ray time (ref.time; a point light's leaves it 0, pointlight.cpp:29)
     bool delta;     // point / spot / directional: no MIS against the BSDF (emitter.h)
 };
 
@@ -201,7 +218,8 @@ struct LightSample {
 __device__ __forceinline__ float sampleShape(const SceneView& s, int inst, V2 u, V3& p, V3& n, V2& uv) {
     const InstTrav& it = s.instT[inst];
     const InstShade& is = s.instS[inst];
-    if (it.kind == kShapeMesh) {                         // mesh.cpp:396-434
+    const uint32_t kind = it.kind & ~kInstAnimated;
+    if (kind == kShapeMesh) {                            // mesh.cpp:396-434
         const MeshRec mr = s.meshes[is.meshId];
         if (mr.totalArea == 0.0f) return 0.0f;
         const float* cdf = s.cdf + mr.cdfOffset;
@@ -226,7 +244,7 @@ __device__ __forceinline__ float sampleShape(const SceneView& s, int inst, V2 u,
         if (!(((uint32_t)at->flags) & 2u)) uv = V2{0.f, 0.f};
         return 1.0f / mr.totalArea;
     }
-    if (it.kind == kShapeSphere) {                       // sphere.cpp:64-81
+    if (kind == kShapeSphere) {                          // sphere.cpp:64-81
         float r = is.radius;
         V3 res = squareToUniformSphere(u);
         SurfInt si;
@@ -268,11 +286,12 @@ __device__ __forceinline__ float sampleShape(const SceneView& s, int inst, V2 u,
 __device__ __forceinline__ float shapeAreaPdf(const SceneView& s, int inst) {
     const InstTrav& it = s.instT[inst];
     const InstShade& is = s.instS[inst];
-    if (it.kind == kShapeMesh) {
+    const uint32_t kind = it.kind & ~kInstAnimated;
+    if (kind == kShapeMesh) {
         float ta = s.meshes[is.meshId].totalArea;
         return ta > 0.0f ? 1.0f / ta : 0.0f;
     }
-    if (it.kind == kShapeSphere) return kInv4Pi / (is.radius * is.radius);
+    if (kind == kShapeSphere) return kInv4Pi / (is.radius * is.radius);
     V3 d = v3(is.ext[0], is.ext[1], is.ext[2]) - (-v3(is.ext[0], is.ext[1], is.ext[2]));
     return 1.0f / (2.0f * (d.x * d.y + d.x * d.z + d.y * d.z));
 }
@@ -346,10 +365,11 @@ __device__ __forceinline__ float envPdf(const EnvView& e, V3 wi) {
     return (float)((double)mapPdf / (2.0 * kPiD * kPiD * (double)sinTheta));
 }
 // EnvironmentMap::sample (environment.cpp:39-73)
-__device__ __noinline__ void envSample(const EnvView& e, V3 ref, V2 u, LightSample& ls) {
+__device__ __noinline__ void envSample(const EnvView& e, V3 ref, V2 u, LightSample& ls, float time) {
     ls.pdf = 0.0f;
     ls.Li = v3s(0.0f);
     ls.delta = false;
+    ls.stime = time;
     float pdf0, pdf1;
     int v, off0;
     const float d1 = dist1DSample(e.margFunc, e.margCdf, e.height, e.margInt, u.y, pdf1, v);
@@ -375,9 +395,10 @@ __device__ __noinline__ void envSample(const EnvView& e, V3 ref, V2 u, LightSamp
 // ---------------------------------------------------------------- delta emitters
 // PointLight::sample (pointlight.cpp:18-31), SpotLight::sample (spotlight.cpp:30-60),
 // DirectionalLight::sample (directional.cpp:18-34)
-__device__ __noinline__ void deltaSample(const Emitter& e, V3 ref, LightSample& ls) {
+__device__ __noinline__ void deltaSample(const Emitter& e, V3 ref, LightSample& ls, float time) {
     ls.delta = true;
     ls.pdf = 1.0f;
+    ls.stime = e.type == kEmitPoint ? 0.0f : time;   // pointlight.cpp:29 uses info.time, never set
     ls.n = v3s(0.0f);
     ls.uv = V2{0.0f, 0.0f};
     const V3 col = v3(e.color[0], e.color[1], e.color[2]);
@@ -419,12 +440,25 @@ __device__ __noinline__ void deltaSample(const Emitter& e, V3 ref, LightSample& 
 
 // Emitter::sample for emitter ei of the scene's list: area lights below (area.cpp:51-88),
 // the delta lights and the environment above
-__device__ __forceinline__ void areaSample(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls);
-__device__ __forceinline__ void emitterSample(const SceneView& s, int ei, V3 ref, V2 u, LightSample& ls) {
+// `time` is the reference point's time (ref.time): the path's for surface next-event
+// estimation, 0 for a volume scattering point (volPath.cpp:61-62 builds a fresh reference)
+__device__ __forceinline__ void areaSample(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls, float time);
+__device__ __forceinline__ void areaSampleWith(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls, float time,
+                                               const Xf34& o2w, const Xf34& w2o);
+__device__ __forceinline__ void emitterSample(const SceneView& s, int ei, V3 ref, V2 u, LightSample& ls, float time) {
     const Emitter e = s.emitters[ei];
-    if (e.type == kEmitArea) areaSample(s, e, ref, u, ls);
-    else if (e.type == kEmitEnv) envSample(s.env, ref, u, ls);
-    else deltaSample(e, ref, ls);
+    if (e.type == kEmitArea) areaSample(s, e, ref, u, ls, time);
+    else if (e.type == kEmitEnv) envSample(s.env, ref, u, ls, time);
+    else deltaSample(e, ref, ls, time);
+}
+template <bool EXT>
+__device__ __forceinline__ void emitterSampleT(const SceneView& s, int ei, V3 ref, V2 u, LightSample& ls, float time) {
+    if (EXT) {
+        emitterSample(s, ei, ref, u, ls, time);
+        return;
+    }
+    const Emitter e = s.emitters[ei];
+    areaSampleWith(s, e, ref, u, ls, time, s.instS[e.instance].o2w, s.instT[e.instance].w2o);
 }
 
 // Environment light seen by an escaping ray, weighted against the previous bounce's pdf
@@ -445,18 +479,18 @@ __device__ __noinline__ V3 envMissRadiance(const SceneView& s, V3 o, V3 d, V3 tp
 }
 
 // AreaLight::sample (area.cpp:51-88)
-__device__ __forceinline__ void areaSample(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls) {
+__device__ __forceinline__ void areaSampleWith(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls, float time,
+                                               const Xf34& o2w, const Xf34& w2o) {
     ls.delta = false;
-    const InstShade& is = s.instS[e.instance];
-    const InstTrav& it = s.instT[e.instance];
+    ls.stime = time;
     V3 lp, ln;
     V2 luv;
     float areaPdf = sampleShape(s, e.instance, u, lp, ln, luv);
-    ls.p = xfPoint(is.o2w, lp);
-    ls.n = normalize(xfNormal(it.w2o, ln));
+    ls.p = xfPoint(o2w, lp);
+    ls.n = normalize(xfNormal(w2o, ln));
     ls.uv = luv;
     Frame fr = frameFromNormal(ln);
-    V3 t1 = xfVector(is.o2w, fr.x), t2 = xfVector(is.o2w, fr.y);
+    V3 t1 = xfVector(o2w, fr.x), t2 = xfVector(o2w, fr.y);
     float areaScale = length(cross(t1, t2));
     if (areaScale > 0.0f) areaPdf /= areaScale;
     ls.sd = normalize(ls.p - ref);
@@ -469,6 +503,23 @@ __device__ __forceinline__ void areaSample(const SceneView& s, const Emitter& e,
     ls.pdf = areaPdf * dist / cosTheta;
     ls.Li = cdiv(emitterEval(e, ls.n, ls.uv, normalize(ref - ls.p)), ls.pdf);
 }
+
+// An animated area light at the reference point's time (m_primitive->getToWorld(ref.time),
+// area.cpp:54); out of line like surfaceInteractionMoving.
+__device__ __noinline__ void areaSampleMoving(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls, float time) {
+    Xf34 o2w, w2o;
+    motionAt(s.motion[e.instance], s.instS[e.instance].o2w, s.instT[e.instance].w2o, time, o2w, w2o);
+    areaSampleWith(s, e, ref, u, ls, time, o2w, w2o);
+}
+
+__device__ __forceinline__ void areaSample(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls, float time) {
+    if (s.instT[e.instance].kind & kInstAnimated) areaSampleMoving(s, e, ref, u, ls, time);
+    else areaSampleWith(s, e, ref, u, ls, time, s.instS[e.instance].o2w, s.instT[e.instance].w2o);
+}
+
+// Emitter sampling in a kernel variant: without EXT every emitter is a static area light.
+template <bool EXT>
+__device__ __forceinline__ void emitterSampleT(const SceneView& s, int ei, V3 ref, V2 u, LightSample& ls, float time);
 
 // AreaLight::pdf (area.cpp:90-119)
 __device__ __forceinline__ float emitterPdf(const SceneView& s, int ei, V3 ref, V3 p, V3 n) {
@@ -567,8 +618,10 @@ __device__ __forceinline__ V3 cameraWeigh(const Camera& cam, V3 L, Rng r, float 
     return L;
 }
 
-// Work item -> camera sample (integrator.h:88-125) in slot `slot`.
-__device__ __forceinline__ void generatePath(const JobDev& j, uint32_t jobIdx, uint64_t item, PathState& ps) {
+// Work item -> camera sample (integrator.h:88-125) in slot `slot`; returns the ray's
+// shutter time, which every ray of the path keeps (ray.h: time; primitive.cpp:71).
+template <bool EXT>
+__device__ __forceinline__ float generatePath(const JobDev& j, uint32_t jobIdx, uint64_t item, PathState& ps) {
     int ww = j.wx1 - j.wx0;
     uint64_t npix = (uint64_t)ww * (uint64_t)(j.wy1 - j.wy0);
     uint32_t pass = (uint32_t)(item / npix) + (uint32_t)j.firstPass;
@@ -581,23 +634,36 @@ __device__ __forceinline__ void generatePath(const JobDev& j, uint32_t jobIdx, u
     float cx = fx / (float)j.W, cy = 1.0f - fy / (float)j.H;
     const V2 lens = next2D(r);     // lens position
     const float chRnd = next1D(r); // chromatic aberration channel
-    next1D(r);                     // time (static transforms)
+    float time = next1D(r);        // shutter time
     const Camera& cam = j.view.camera;
     V3 o, d;
-    if (cam.kind == kCamThinLens) {
+    if (EXT && cam.kind == kCamThinLens) {
         float lambda;
         cameraChannel(cam, chRnd, lambda);
         V3 oc, dc;
         thinLensRay(cam, cx, cy, lens, lambda, oc, dc);
-        o = xfPoint(cam.toWorld, oc);
-        d = xfVector(cam.toWorld, dc);
+        if (cam.rollingShutter) {   // thinLens.cpp:80-85
+            const float scanline = 1.0f - cy;
+            time = scanline * cam.scanDuration + (time * cam.exposureDuration);
+        }
+        Xf34 tw = cam.toWorld, unused;
+        if (cam.animated) motionAt(cam.motion, cam.toWorld, cam.toWorld, time, tw, unused);
+        o = xfPoint(tw, oc);
+        d = xfVector(tw, dc);
     } else {
         // perspective.cpp:15-32
         float px = (2.0f * cx - 1.0f) * cam.aspect * cam.scale;
         float py = (2.0f * cy - 1.0f) * cam.scale;
         V3 dir = normalize(v3(px, py, -1.0f));
-        o = v3(cam.origin[0], cam.origin[1], cam.origin[2]);
-        d = xfVector(cam.toWorld, dir);
+        if (EXT && cam.animated) {
+            Xf34 tw, unused;
+            motionAt(cam.motion, cam.toWorld, cam.toWorld, time, tw, unused);
+            o = xfPoint(tw, v3s(0.0f));
+            d = xfVector(tw, dir);
+        } else {
+            o = v3(cam.origin[0], cam.origin[1], cam.origin[2]);
+            d = xfVector(cam.toWorld, dir);
+        }
     }
     ps.ox = o.x; ps.oy = o.y; ps.oz = o.z; ps.pdfPrev = 1.0f;
     ps.dx = d.x; ps.dy = d.y; ps.dz = d.z;
@@ -611,6 +677,7 @@ __device__ __forceinline__ void generatePath(const JobDev& j, uint32_t jobIdx, u
     ps.vsBounces = 0;
     ps.medium = -1;                        // camera rays start in vacuum (ray.h:18)
     ps.flags = 1u | (jobIdx << 8);         // specularBounce = true
+    return time;
 }
 
 // ---------------------------------------------------------------- kernels
@@ -672,6 +739,7 @@ struct ExtendSrc {
         r.d = v3(b.x, b.y, b.z);
         r.tmin = kEpsilon;
         r.tmax = INFINITY;
+        r.time = p->slotTime[slot];
         view = &jd.view;
         sv = view;
         nm = nullptr;
@@ -686,14 +754,15 @@ struct ExtendSrc {
     }
 };
 
-template <bool COUNT, int SMEM, bool SPEC>
+// MOTION: the scene has animated instances (rays carry their shutter time)
+template <bool COUNT, int SMEM, bool SPEC, bool MOTION = false>
 __global__ void __launch_bounds__(kBlock, 8) kExtend(KParams p) {
     __shared__ uint32_t stack[SMEM * kBlock];
     const uint32_t n = p.cnt[kQIn];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[0], (unsigned long long)n);
     TraceCounters cnt{0, 0};
     ExtendSrc src{&p, n, 0};
-    int err = persistentTrace<kBlock, false, COUNT, SMEM, SPEC>(src, p.cnt + kQFetchA, stack, &cnt);
+    int err = persistentTrace<kBlock, false, COUNT, SMEM, SPEC, MOTION>(src, p.cnt + kQFetchA, stack, &cnt);
     if (COUNT) {
         unsigned long long nn = cnt.nodes, nt = cnt.tris;
         for (int o = 16; o > 0; o >>= 1) {
@@ -736,13 +805,16 @@ __global__ void __launch_bounds__(kBlock) kClassify(KParams p, uint32_t* classLi
 // M = kLobesNone the kernel serves the medium class: it samples the medium, finishes the
 // bounce of paths that scatter in it, and hands each other path on to its surface
 // class (medium sampling marked done) for a surface kernel later in the iteration.
-template <bool VOL, uint32_t M>
+// EXT: some job of the launch uses the rarer features (SceneView::ext); without them the
+// kernel keeps the area-light, static-transform code only.
+template <bool VOL, uint32_t M, bool EXT>
 __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list, const uint32_t* count) {
     const uint32_t n = *count;
     for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
         uint32_t slot = list[i];
         PathState ps = p.paths[slot];
         const HitRec h = p.hits[slot];
+        const float time = EXT ? p.slotTime[slot] : 0.0f;
         const uint32_t jobIdx = ps.flags >> 8;
         const JobDev& j = p.jobs[jobIdx];
         const SceneView& s = j.view;
@@ -786,7 +858,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
                     float lightSelectPdf = 1.0f / nL;
                     int ei = pickEmitter(s.numEmitters, next1D(rng));
                     LightSample ls;
-                    emitterSample(s, ei, mp, next2D(rng), ls);
+                    emitterSampleT<EXT>(s, ei, mp, next2D(rng), ls, 0.0f);
                     V3 Li = ls.Li * (1.0f / lightSelectPdf);
                     if (ls.pdf > 1e-6f && !isBlack(Li)) {
                         V3 wi = normalize(ls.p - mp);
@@ -799,7 +871,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
                             sr.ox = mp.x; sr.oy = mp.y; sr.oz = mp.z; sr.tmax = ls.stmax;
                             sr.dx = ls.sd.x; sr.dy = ls.sd.y; sr.dz = ls.sd.z; sr.slot = slot;
                             sr.cr = c.x; sr.cg = c.y; sr.cb = c.z; sr.medium = medium;
-                            sr.lx = ls.p.x; sr.ly = ls.p.y; sr.lz = ls.p.z; sr.pad = 0;
+                            sr.lx = ls.p.x; sr.ly = ls.p.y; sr.lz = ls.p.z; sr.pad = __float_as_uint(ls.stime);
                             emitShadow = true;
                         }
                     }
@@ -823,7 +895,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
             if (M == kLobesNone) {
                 // no scattering: the path reaches its surface (or escapes)
                 if (!hit) {
-                    L = L + envMissRadiance(s, o, d, tp, specular, pdfPrev, nL);
+                    if (EXT) L = L + envMissRadiance(s, o, d, tp, specular, pdfPrev, nL);
                     terminate = true;
                 } else {
                     handOff = true;
@@ -832,11 +904,12 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
             }
             const int curMedium = medium;
             if (!hit) {
-                L = L + envMissRadiance(s, o, d, tp, specular, pdfPrev, nL);
+                if (EXT) L = L + envMissRadiance(s, o, d, tp, specular, pdfPrev, nL);
                 terminate = true;
                 break;
             }
-            SurfInt si = surfaceInteraction(s, h, o, d);
+            SurfInt si = EXT ? surfaceInteraction(s, h, o, d, time)
+                             : surfaceInteractionWith(s, h, o, d, s.instS[h.inst].o2w, s.instT[h.inst].w2o);
             const InstShade& is = s.instS[h.inst];
             const Material mat = s.materials[is.material];
             Bsdf bsdf;
@@ -872,7 +945,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
             float lightSelectPdf = 1.0f / nL;
             int ei = pickEmitter(s.numEmitters, next1D(rng));
             LightSample ls;
-            emitterSample(s, ei, si.p, next2D(rng), ls);
+            emitterSampleT<EXT>(s, ei, si.p, next2D(rng), ls, time);
             V3 Li = ls.Li * (1.0f / lightSelectPdf);
             if (ls.pdf > 1e-6f && !isBlack(Li)) {
                 V3 wi = normalize(ls.p - si.p);
@@ -887,7 +960,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
                     sr.ox = si.p.x; sr.oy = si.p.y; sr.oz = si.p.z; sr.tmax = ls.stmax;
                     sr.dx = ls.sd.x; sr.dy = ls.sd.y; sr.dz = ls.sd.z; sr.slot = slot;
                     sr.cr = c.x; sr.cg = c.y; sr.cb = c.z; sr.medium = smed;
-                    sr.lx = ls.p.x; sr.ly = ls.p.y; sr.lz = ls.p.z; sr.pad = 0;
+                    sr.lx = ls.p.x; sr.ly = ls.p.y; sr.lz = ls.p.z; sr.pad = __float_as_uint(ls.stime);
                     emitShadow = true;
                 }
             }
@@ -982,6 +1055,7 @@ struct ShadowSrc {
         r.tmax = a.w;
         r.d = v3(b.x, b.y, b.z);
         r.tmin = kEpsilon;
+        r.time = __uint_as_float(sr->pad);
         const JobDev& j = p->jobs[p->paths[slot].flags >> 8];
         if (mixed && j.integrator != 0) return false;
         sv = &j.view;
@@ -1002,19 +1076,19 @@ struct ShadowSrc {
     }
 };
 
-template <bool ANY, int SMEM, bool SPEC>
+template <bool ANY, int SMEM, bool SPEC, bool MOTION = false>
 __global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p, bool mixed) {
     __shared__ uint32_t stack[SMEM * kBlock];
     const uint32_t n = p.cnt[kQShadow];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
     ShadowSrc<ANY> src{&p, n, 0, nullptr, mixed};
-    int err = persistentTrace<kBlock, ANY, false, SMEM, SPEC>(src, p.cnt + kQFetchB, stack, nullptr);
+    int err = persistentTrace<kBlock, ANY, false, SMEM, SPEC, MOTION>(src, p.cnt + kQFetchB, stack, nullptr);
     if (err) atomicOr(p.errWord, (uint32_t)err);
 }
 
 // Shadow queries of `volpath`: evaluateTr (volPath.cpp:261-291), a loop of closest hits
 // through null-BSDF boundaries multiplying the transmittance of each medium segment.
-template <bool VOL>
+template <bool VOL, bool MOTION = false>
 __global__ void __launch_bounds__(kBlock) kShadow(KParams p, bool mixed) {
     __shared__ uint32_t stack[kStackSize * kBlock];
     uint32_t* stk = stack + threadIdx.x;
@@ -1033,15 +1107,16 @@ __global__ void __launch_bounds__(kBlock) kShadow(KParams p, bool mixed) {
         r.d = v3(sr.dx, sr.dy, sr.dz);
         r.tmin = kEpsilon;
         r.tmax = sr.tmax;
+        r.time = __uint_as_float(sr.pad);
         V3 c = v3(sr.cr, sr.cg, sr.cb);
         bool clear;
         if (!VOL) {
             THit h;
             if (j.hasNull) {
-                err |= traceRay<kBlock, false, false, false>(s, r, h, stk, nullptr, nullptr);
+                err |= traceRay<kBlock, false, false, false, MOTION>(s, r, h, stk, nullptr, nullptr);
                 clear = h.inst < 0 || j.nullMask[h.inst];
             } else {
-                err |= traceRay<kBlock, true, false, false>(s, r, h, stk, nullptr, nullptr);
+                err |= traceRay<kBlock, true, false, false, MOTION>(s, r, h, stk, nullptr, nullptr);
                 clear = h.inst < 0;
             }
         } else {
@@ -1051,7 +1126,7 @@ __global__ void __launch_bounds__(kBlock) kShadow(KParams p, bool mixed) {
             clear = true;
             for (int seg = 0; seg < 256; ++seg) {
                 THit h;
-                err |= traceRay<kBlock, false, false, false>(s, r, h, stk, nullptr, nullptr);
+                err |= traceRay<kBlock, false, false, false, MOTION>(s, r, h, stk, nullptr, nullptr);
                 bool hit = h.inst >= 0;
                 if (medium >= 0) {
                     float segT = hit ? h.t : r.tmax;
@@ -1062,7 +1137,8 @@ __global__ void __launch_bounds__(kBlock) kShadow(KParams p, bool mixed) {
                 if (!j.nullMask[h.inst]) { clear = false; break; }
                 HitRec hr;
                 hr.t = h.t; hr.u = h.u; hr.v = h.v; hr.inst = h.inst; hr.slot = h.slot;
-                SurfInt si = surfaceInteraction(s, hr, r.o, r.d);
+                SurfInt si = MOTION ? surfaceInteraction(s, hr, r.o, r.d, r.time)
+                                    : surfaceInteractionWith(s, hr, r.o, r.d, s.instS[h.inst].o2w, s.instT[h.inst].w2o);
                 const InstShade& is = s.instS[h.inst];
                 medium = is.hasMedia ? (dot(r.d, si.n) > 0.0f ? is.mediumOut : is.mediumIn) : -1;
                 r.o = si.p;
@@ -1088,6 +1164,7 @@ __device__ __forceinline__ unsigned long long toFixed(float x) {
 }
 
 // film.h:26-69 splat of one finished sample (NaN/Inf zeroed as integrator.h:137-141).
+template <bool EXT>
 __device__ __forceinline__ void filmSplat(const JobDev& j, const PathState& ps) {
     V3 L = v3(ps.Lr, ps.Lg, ps.Lb);
     int ww = j.wx1 - j.wx0;
@@ -1096,7 +1173,7 @@ __device__ __forceinline__ void filmSplat(const JobDev& j, const PathState& ps) 
     Rng r = rngSeed(key);
     V2 s2 = next2D(r);
     float fx = (float)x + s2.x, fy = (float)y + s2.y;
-    if (j.view.camera.kind == kCamThinLens) L = cameraWeigh(j.view.camera, L, r, fx, fy, j.W, j.H);
+    if (EXT && j.view.camera.kind == kCamThinLens) L = cameraWeigh(j.view.camera, L, r, fx, fy, j.W, j.H);
     if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = v3s(0.0f);
     int x0 = max(0, (int)ceilf(fx - j.frx - 0.5f));
     int x1 = min(j.W - 1, (int)floorf(fx + j.frx - 0.5f));
@@ -1133,6 +1210,7 @@ __device__ __forceinline__ void filmSplat(const JobDev& j, const PathState& ps) 
 // test select (film.h:26-69). Such a sample is stored as (L.r, L.g, L.b, 1) at its work
 // item and added to the film later by kFilmFromSamples; a sample on a whole coordinate
 // (it also reaches a neighbouring pixel) is splatted with atomics as before.
+template <bool EXT>
 __device__ __forceinline__ void sampleRecord(const JobDev& j, const PathState& ps) {
     const int ww = j.wx1 - j.wx0;
     const int x = j.wx0 + (int)(ps.pixel % (uint32_t)ww), y = j.wy0 + (int)(ps.pixel / (uint32_t)ww);
@@ -1141,11 +1219,11 @@ __device__ __forceinline__ void sampleRecord(const JobDev& j, const PathState& p
     const V2 s2 = next2D(r);
     const float fx = (float)x + s2.x, fy = (float)y + s2.y;
     if (fx == floorf(fx) || fy == floorf(fy)) {
-        filmSplat(j, ps);
+        filmSplat<EXT>(j, ps);
         return;
     }
     V3 L = v3(ps.Lr, ps.Lg, ps.Lb);
-    if (j.view.camera.kind == kCamThinLens) L = cameraWeigh(j.view.camera, L, r, fx, fy, j.W, j.H);
+    if (EXT && j.view.camera.kind == kCamThinLens) L = cameraWeigh(j.view.camera, L, r, fx, fy, j.W, j.H);
     if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = v3s(0.0f);
     const uint64_t npix = (uint64_t)ww * (uint64_t)(j.wy1 - j.wy0);
     const uint64_t item = (uint64_t)(ps.pass - (uint32_t)j.firstPass) * npix + ps.pixel;
@@ -1236,6 +1314,7 @@ __device__ __forceinline__ bool warpGrab(const KParams& p, bool want, uint32_t& 
 // Finished paths (done list): film splat and per-job retired count. Finished and idle
 // slots (free list) then take new work items; slots left without work join the next
 // free list. The loop is warp-uniform (all lanes of a warp iterate together).
+template <bool EXT>
 __global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
     const uint32_t nd = p.cnt[kQDone], nf = p.cnt[kQFree];
     const bool work = p.cnt[kQWork] != 0;
@@ -1256,8 +1335,8 @@ __global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
             PathState ps = p.paths[slot];
             jobIdx = ps.flags >> 8;
             const JobDev& jd = p.jobs[jobIdx];
-            if (jd.samples) sampleRecord(jd, ps);
-            else filmSplat(jd, ps);
+            if (jd.samples) sampleRecord<EXT>(jd, ps);
+            else filmSplat<EXT>(jd, ps);
         }
         const uint32_t grp = __match_any_sync(0xffffffffu, jobIdx);
         if (jobIdx != 0xFFFFFFFFu && (int)lane == __ffs(grp) - 1)
@@ -1268,7 +1347,8 @@ __global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
         if (work) got = warpGrab(p, valid, gj, item);   // `work` is uniform over the grid
         if (got) {
             PathState ps;
-            generatePath(p.jobs[gj], gj, item, ps);
+            const float t = generatePath<EXT>(p.jobs[gj], gj, item, ps);
+            if (EXT) p.slotTime[slot] = t;
             p.paths[slot] = ps;
         }
         const bool idle = valid && !got;
@@ -1305,7 +1385,7 @@ __global__ void kResetPool(uint32_t* freeList, uint32_t n, uint32_t* cnt) {
 }
 
 // One shade launch per material class of one integrator (empty classes exit at once).
-template <bool VOL>
+template <bool VOL, bool EXT>
 static void launchShade(const KParams& kp, uint32_t* classLists, int grid, cudaStream_t st) {
     const size_t cap = kp.capacity;
     const int c0 = VOL ? kClassesPerInt : 0;
@@ -1314,12 +1394,12 @@ static void launchShade(const KParams& kp, uint32_t* classLists, int grid, cudaS
     static_assert(kMatMatte == 0 && kMatPlastic == 1 && kMatConductor == 2 && kMatGlass == 3,
                   "material classes follow the material type codes");
     // medium sampling first: its hand-offs join the surface classes shaded below
-    if (VOL) kShade<true, kLobesNone><<<grid, kBlock, 0, st>>>(kp, lists + kMediumClass * cap, cnt + kMediumClass);
-    kShade<VOL, kLobesMatte><<<grid, kBlock, 0, st>>>(kp, lists + 0 * cap, cnt + 0);
-    kShade<VOL, kLobesPlastic><<<grid, kBlock, 0, st>>>(kp, lists + 1 * cap, cnt + 1);
-    kShade<VOL, kLobesConductor><<<grid, kBlock, 0, st>>>(kp, lists + 2 * cap, cnt + 2);
-    kShade<VOL, kLobesGlass><<<grid, kBlock, 0, st>>>(kp, lists + 3 * cap, cnt + 3);
-    kShade<VOL, kLobesAll><<<grid, kBlock, 0, st>>>(kp, lists + 4 * cap, cnt + 4);
+    if (VOL) kShade<true, kLobesNone, EXT><<<grid, kBlock, 0, st>>>(kp, lists + kMediumClass * cap, cnt + kMediumClass);
+    kShade<VOL, kLobesMatte, EXT><<<grid, kBlock, 0, st>>>(kp, lists + 0 * cap, cnt + 0);
+    kShade<VOL, kLobesPlastic, EXT><<<grid, kBlock, 0, st>>>(kp, lists + 1 * cap, cnt + 1);
+    kShade<VOL, kLobesConductor, EXT><<<grid, kBlock, 0, st>>>(kp, lists + 2 * cap, cnt + 2);
+    kShade<VOL, kLobesGlass, EXT><<<grid, kBlock, 0, st>>>(kp, lists + 3 * cap, cnt + 3);
+    kShade<VOL, kLobesAll, EXT><<<grid, kBlock, 0, st>>>(kp, lists + 4 * cap, cnt + 4);
 }
 
 // ---------------------------------------------------------------- host driver
@@ -1368,6 +1448,7 @@ void Wavefront::ensureCapacity(size_t slots) {
     if (slots <= cap_) return;
     clearGraphs();   // the captured launches hold the old buffers
     paths_.alloc(slots * sizeof(PathState));
+    times_.alloc(slots * sizeof(float));
     hits_.alloc(slots * sizeof(HitRec));
     listA_.alloc(slots * sizeof(uint32_t));
     listB_.alloc(slots * sizeof(uint32_t));
@@ -1600,7 +1681,19 @@ void Wavefront::drop(int j) {
 // The traversal kernels for one shared-stack size and speculation setting.
 template <int SMEM, bool SPEC>
 static void launchTraversal(const KParams& kp, int mix, bool hasNull, bool count, int travGrid, cudaStream_t st,
-                            cudaEvent_t ea, cudaEvent_t eb, int stage) {
+                            cudaEvent_t ea, cudaEvent_t eb, int stage, bool motion) {
+    if (motion) {
+        // animated instances: the MOTION kernels (no speculation, no visit counters)
+        if (stage == 0) {
+            if (ea) GND_CUDA(cudaEventRecord(ea, st));
+            kExtend<false, SMEM, false, true><<<travGrid, kBlock, 0, st>>>(kp);
+            if (eb) GND_CUDA(cudaEventRecord(eb, st));
+        } else if (mix & 1) {
+            if (hasNull) kShadowPath<false, SMEM, false, true><<<travGrid, kBlock, 0, st>>>(kp, mix == 3);
+            else kShadowPath<true, SMEM, false, true><<<travGrid, kBlock, 0, st>>>(kp, mix == 3);
+        }
+        return;
+    }
     if (stage == 0) {
         if (ea) GND_CUDA(cudaEventRecord(ea, st));
         // the instrumented variant counts the visits of plain nearest-first order: the
@@ -1616,9 +1709,9 @@ static void launchTraversal(const KParams& kp, int mix, bool hasNull, bool count
 
 template <int SMEM>
 static void launchTraversal(const KParams& kp, int mix, bool hasNull, bool count, int travGrid, cudaStream_t st,
-                            cudaEvent_t ea, cudaEvent_t eb, int stage, bool spec) {
-    if (spec) launchTraversal<SMEM, true>(kp, mix, hasNull, count, travGrid, st, ea, eb, stage);
-    else launchTraversal<SMEM, false>(kp, mix, hasNull, count, travGrid, st, ea, eb, stage);
+                            cudaEvent_t ea, cudaEvent_t eb, int stage, bool spec, bool motion) {
+    if (spec) launchTraversal<SMEM, true>(kp, mix, hasNull, count, travGrid, st, ea, eb, stage, motion);
+    else launchTraversal<SMEM, false>(kp, mix, hasNull, count, travGrid, st, ea, eb, stage, motion);
 }
 
 void Wavefront::setTune(const Tune& t) {
@@ -1647,22 +1740,35 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
         evs_.push_back(eb);
     }
     const bool count = (profile & 2) != 0;
-    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0);
-    else launchTraversal<32>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0);
+    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0, motion_);
+    else launchTraversal<32>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0, motion_);
     if (sort) {
         uint32_t* cls = classes_.as<uint32_t>();
         kClassify<<<ctx_->numSMs * 16, kBlock, 0, st>>>(kp, cls);   // latency-bound: a full SM of warps
-        if (mix & 1) launchShade<false>(kp, cls, grid, st);
-        if (mix & 2) launchShade<true>(kp, cls, grid, st);
+        if (mix & 1) {
+            if (ext_) launchShade<false, true>(kp, cls, grid, st);
+            else launchShade<false, false>(kp, cls, grid, st);
+        }
+        if (mix & 2) {
+            if (ext_) launchShade<true, true>(kp, cls, grid, st);
+            else launchShade<true, false>(kp, cls, grid, st);
+        }
     } else if (mix == 2) {
-        kShade<true, kLobesAll><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
+        if (ext_) kShade<true, kLobesAll, true><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
+        else kShade<true, kLobesAll, false><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
     } else {
-        kShade<false, kLobesAll><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
+        if (ext_) kShade<false, kLobesAll, true><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
+        else kShade<false, kLobesAll, false><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
     }
-    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0);
-    else launchTraversal<32>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0);
-    if (mix & 2) kShadow<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
-    kRetire<<<ctx_->numSMs * 12, kBlock, 0, st>>>(kp);   // 12 blocks per SM: its register limit
+    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0, motion_);
+    else launchTraversal<32>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0, motion_);
+    if (mix & 2) {
+        if (motion_) kShadow<true, true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
+        else kShadow<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
+    }
+    // 12 blocks per SM: its register limit
+    if (ext_) kRetire<true><<<ctx_->numSMs * 12, kBlock, 0, st>>>(kp);
+    else kRetire<false><<<ctx_->numSMs * 12, kBlock, 0, st>>>(kp);
     kEndIter<<<1, 1, 0, st>>>(kp.cnt);
     GND_CUDA(cudaGetLastError());
 }
@@ -1675,7 +1781,8 @@ void Wavefront::clearGraphs() {
 cudaGraphExec_t Wavefront::pairGraph(const KParams& kp, int par, int mix, bool hasNull, cudaStream_t st) {
     const bool fifo = kp.fifo != 0;
     for (const GraphEntry& g : graphs_)
-        if (g.par == par && g.mix == mix && g.hasNull == hasNull && g.fifo == fifo) return g.exec;
+        if (g.par == par && g.mix == mix && g.hasNull == hasNull && g.fifo == fifo && g.motion == motion_ && g.ext == ext_)
+            return g.exec;
     cudaGraph_t graph = nullptr;
     GND_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     try {
@@ -1691,7 +1798,7 @@ cudaGraphExec_t Wavefront::pairGraph(const KParams& kp, int par, int mix, bool h
     cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) throw Error(GND_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-    graphs_.push_back(GraphEntry{par, mix, hasNull, fifo, exec});
+    graphs_.push_back(GraphEntry{par, mix, hasNull, fifo, motion_, ext_, exec});
     return exec;
 }
 
@@ -1711,9 +1818,17 @@ const Wavefront::Snapshot& Wavefront::waitRound(int slot) {
 void Wavefront::enqueueRound(int iters, int mix, bool hasNull, int profile, Result& acc, int slot) {
     Context* c = ctx_;
     cudaStream_t st = c->stream;
+    motion_ = false;   // the traversal variant for animated instances, when a job needs it
+    ext_ = false;      // the shade / retire variants for the rarer features
+    for (int j = 0; j < kMaxJobs; ++j) {
+        if (!jobs_[j].used) continue;
+        if (jobs_[j].dev.view.motion) motion_ = true;
+        if (jobs_[j].dev.view.ext) ext_ = true;
+    }
     KParams kp{};
     kp.jobs = jobTab_.as<JobDev>();
     kp.paths = paths_.as<PathState>();
+    kp.slotTime = times_.as<float>();
     kp.hits = hits_.as<HitRec>();
     kp.shadow = shadow_.as<ShadowRec>();
     kp.done = done_.as<uint32_t>();

@@ -175,15 +175,17 @@ private:
     void clearGraphs();
     struct GraphEntry {
         int par, mix;
-        bool hasNull, fifo;
+        bool hasNull, fifo, motion, ext;
         cudaGraphExec_t exec;
     };
+    bool motion_ = false;   // an admitted job's scene has animated instances (MOTION traversal)
+    bool ext_ = false;      // an admitted job's scene uses the EXT features (SceneView::ext)
     std::vector<GraphEntry> graphs_;
     Tune tune_;
     Context* ctx_;
     size_t cap_ = 0;
     int cur_ = 0;
-    DevBuf paths_, hits_, listA_, listB_, freeA_, freeB_, shadow_, done_, counters_, totals_, classes_;
+    DevBuf paths_, hits_, listA_, listB_, freeA_, freeB_, shadow_, done_, counters_, totals_, classes_, times_;
     DevBuf jobTab_, ctl_, active_, filmOut_, samples_;
     Snapshot* snaps_ = nullptr;       // pinned host memory, two slots
     cudaEvent_t snapEv_[2] = {nullptr, nullptr};

@@ -478,11 +478,31 @@ GND_REGISTER_CLASS(SphereShape, "sphere")
 GND_REGISTER_CLASS(CubeShape, "cube")
 
 // ---------------------------------------------------------------- primitive
-// primitive.cpp:7-46 (static transforms: toWorldEnd must equal toWorld)
+// primitive.cpp:6-11
 PrimitiveObj::PrimitiveObj(const PropertyList& p) {
     toWorld = p.getTransform("toWorld", Transform());
-    if (p.hasTransform("toWorldEnd") && !(p.getTransform("toWorldEnd", toWorld) == toWorld))
-        throw std::runtime_error("Primitive: animated transforms (toWorldEnd) are not supported by the GPU integrators");
+    toWorldEnd = p.getTransform("toWorldEnd", toWorld);
+    animated = !(toWorldEnd == toWorld);
+}
+
+gnd::InstMotion makeMotion(const Transform& a, const Transform& b) {
+    gnd::InstMotion k{};
+    gnd::motionDecompose(a.m.toXf34(), k.t0, k.s0, k.q0);
+    gnd::motionDecompose(b.m.toXf34(), k.t1, k.s1, k.q1);
+    k.endO2W = b.m.toXf34();
+    k.endW2O = b.mInv.toXf34();
+    return k;
+}
+Transform motionMid(const gnd::InstMotion& k) {
+    gnd::Xf34 m, mi;
+    gnd::motionCompose(k, (0.5f - 0.0f) / (1.0f - 0.0f), m, mi);
+    Transform t;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) {
+            t.m.c[c][r] = m.r[r][c];
+            t.mInv.c[c][r] = mi.r[r][c];
+        }
+    return t;
 }
 void PrimitiveObj::addChild(std::shared_ptr<GndObject> c) {
     switch (c->getClassType()) {
@@ -518,8 +538,8 @@ GND_REGISTER_CLASS(PrimitiveReg, "primitive")
 // ---------------------------------------------------------------- camera, filters, sampler
 CameraObj::CameraObj(const PropertyList& p) {
     toWorld = p.getTransform("toWorld", Transform());
-    if (p.hasTransform("toWorldEnd") && !(p.getTransform("toWorldEnd", toWorld) == toWorld))
-        throw std::runtime_error("Camera: animated transforms (toWorldEnd) are not supported by the GPU integrators");
+    toWorldEnd = p.getTransform("toWorldEnd", toWorld);   // camera.h:20-25
+    animated = !(toWorldEnd == toWorld);
     width = p.getInteger("width", 1280);
     height = p.getInteger("height", 720);
     fov = p.getFloat("fov", 45.0f);
@@ -533,8 +553,7 @@ void CameraObj::addChild(std::shared_ptr<GndObject> c) {
 struct PerspectiveCameraObj : CameraObj {
     explicit PerspectiveCameraObj(const PropertyList& p) : CameraObj(p) {}
 };
-// thinLens.cpp:13-31. The shutter properties only move the sample time, which no static
-// scene reads; they are parsed for the same error behaviour on malformed values.
+// thinLens.cpp:13-31
 struct ThinLensCameraObj : CameraObj {
     explicit ThinLensCameraObj(const PropertyList& p) : CameraObj(p) {
         kind = gnd::kCamThinLens;
@@ -545,9 +564,9 @@ struct ThinLensCameraObj : CameraObj {
         caLateral = p.getFloat("ca_lateral", 0.0f);
         vignetting = p.getBoolean("vignetting", false);
         blades = p.getInteger("blades", 0);
-        (void)p.getBoolean("rolling_shutter", false);
-        (void)p.getFloat("scan_duration", 0.9f);
-        (void)p.getFloat("exposure_duration", 0.1f);
+        rollingShutter = p.getBoolean("rolling_shutter", false);
+        scanDuration = p.getFloat("scan_duration", 0.9f);
+        exposureDuration = p.getFloat("exposure_duration", 0.1f);
     }
 };
 // filter.h:20-54
@@ -715,7 +734,13 @@ void Scene::build() {
     std::vector<Bounds> wb(np);
     std::vector<V3> wc(np);
     for (size_t i = 0; i < np; ++i) {
-        wb[i] = m_primitives[i]->shape->objectBounds().transformed(m_primitives[i]->toWorld);
+        const PrimitiveObj& pr = *m_primitives[i];
+        const Bounds ob = pr.shape->objectBounds();
+        wb[i] = ob.transformed(pr.toWorld);
+        if (pr.animated) {   // motionBounds (animated.cpp:49-58): start, end and the middle
+            wb[i].grow(ob.transformed(pr.toWorldEnd));
+            wb[i].grow(ob.transformed(motionMid(makeMotion(pr.toWorld, pr.toWorldEnd))));
+        }
         wc[i] = wb[i].lo * 0.5f + wb[i].hi * 0.5f;
     }
     if (np > 0) {
@@ -815,6 +840,11 @@ void Scene::build() {
         it.w2o = p.toWorld.mInv.toXf34();
         is.o2w = p.toWorld.m.toXf34();
         it.kind = p.shape->kind;
+        if (p.animated) {   // the start matrices above; the motion record for times > 0
+            if (fs->motion.empty()) fs->motion.resize(np);
+            fs->motion[i] = makeMotion(p.toWorld, p.toWorldEnd);
+            it.kind |= gnd::kInstAnimated;
+        }
         it.blasRoot = gnd::kEmpty;
         is.meshId = 0xFFFFFFFFu;
         if (p.shape->kind == gnd::kShapeMesh) {
@@ -864,6 +894,11 @@ void Scene::build() {
         fs->camera.caAxial = m_camera->caAxial;
         fs->camera.caLateral = m_camera->caLateral;
         fs->camera.vignetting = m_camera->vignetting ? 1 : 0;
+        fs->camera.rollingShutter = m_camera->rollingShutter ? 1 : 0;
+        fs->camera.scanDuration = m_camera->scanDuration;
+        fs->camera.exposureDuration = m_camera->exposureDuration;
+        fs->camera.animated = m_camera->animated ? 1 : 0;
+        if (m_camera->animated) fs->camera.motion = makeMotion(m_camera->toWorld, m_camera->toWorldEnd);
     }
     fs->fillDesc();
     gnd_scene_desc& d = fs->desc;
@@ -906,6 +941,7 @@ void FlatScene::fillDesc() {
     desc.orig_to_leaf = origToLeaf.data();
     desc.orig_to_leaf_len = (int64_t)origToLeaf.size();
     desc.camera = &camera;
+    desc.inst_motion = motion.empty() ? nullptr : motion.data();
     desc.env_emitter = envEmitter;
     desc.env_width = envWidth;
     desc.env_height = envHeight;

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "gnd/layout.h"
+#include "gnd/motion.h"
 #include "gnd/vmath.h"
 #include "gnd_gpu.h"
 
@@ -191,6 +192,11 @@ struct EmitterObj : GndObject {
     bool isInfiniteAreaLight() const { return type == gnd::kEmitEnv; }
 };
 
+// Motion record of a transform moving from `a` (time 0) to `b` (time 1): both decomposed
+// (animated.cpp:18-21) and b's matrices; and the transform at time 0.5 (motion bounds).
+gnd::InstMotion makeMotion(const Transform& a, const Transform& b);
+Transform motionMid(const gnd::InstMotion& k);
+
 // OpenEXR scanline image (NO, ZIPS or ZIP compression; HALF or FLOAT channels): the
 // R, G, B channels as rgb floats, row-major (himage.cpp).
 void readEXR(const std::string& path, int& width, int& height, std::vector<float>& rgb);
@@ -212,6 +218,8 @@ struct ShapeObj : GndObject {
 
 struct PrimitiveObj : GndObject {
     Transform toWorld;
+    Transform toWorldEnd;     // primitive.cpp:8: the transform at shutter time 1
+    bool animated = false;    // toWorldEnd differs from toWorld (animated.cpp:16)
     std::shared_ptr<ShapeObj> shape;
     std::shared_ptr<MaterialObj> material;
     std::shared_ptr<EmitterObj> emitter;
@@ -229,6 +237,10 @@ struct FilterObj : GndObject {
 
 struct CameraObj : GndObject {
     Transform toWorld;
+    Transform toWorldEnd;     // camera.h:23
+    bool animated = false;
+    bool rollingShutter = false;                         // thinLens.cpp:28-30
+    float scanDuration = 0.9f, exposureDuration = 0.1f;
     int width = 1280, height = 720;
     float fov = 45.f;
     // thin lens (thinLens.cpp:13-31); kind 0 is the pinhole `perspective` camera
@@ -282,6 +294,7 @@ struct FlatScene {
     std::vector<gnd::MeshRec> meshes;
     std::vector<float> cdf;
     std::vector<uint32_t> origToLeaf;
+    std::vector<gnd::InstMotion> motion;   // per instance when any instance moves, else empty
     std::vector<float> envTexels, envDist;
     int envEmitter = -1, envWidth = 0, envHeight = 0;
     float envMarginalIntegral = 0.0f, envStrength = 1.0f;

@@ -66,6 +66,24 @@ struct alignas(16) InstTrav {
     float p0, p1;             // sphere: radius; cube: extents x, y (z in InstShade)
 };
 static_assert(sizeof(InstTrav) == 64, "InstTrav must be 64 bytes");
+// InstTrav::kind flag: the instance moves (its InstMotion record holds the motion)
+constexpr uint32_t kInstAnimated = 0x80000000u;
+
+// Motion of an animated instance or camera (animated.cpp): translation, rotation
+// quaternion (x, y, z, w) and scale of the start (time 0) and end (time 1) transforms,
+// and the end transform's matrices (used at time >= 1; the start ones are the instance's
+// or camera's own).
+struct alignas(16) InstMotion {
+    float t0[3]; float pad0;
+    float q0[4];
+    float s0[3]; float pad1;
+    float t1[3]; float pad2;
+    float q1[4];
+    float s1[3]; float pad3;
+    Xf34 endO2W;
+    Xf34 endW2O;
+};
+static_assert(sizeof(InstMotion) == 192, "InstMotion must be 192 bytes");
 
 // Shading record (96 bytes).
 struct alignas(16) InstShade {
@@ -172,8 +190,13 @@ struct alignas(16) Camera {
     float k1;                 // barrel distortion
     float caAxial, caLateral; // chromatic aberration (per colour channel)
     int32_t vignetting;       // 1: weight cos^4 of the camera-space direction
+    // shutter (thinLens.cpp:80-85) and motion (camera.h:20-25)
+    int32_t rollingShutter;   // 1: the sample time follows the scanline
+    float scanDuration, exposureDuration;
+    int32_t animated;         // 1: toWorld moves to motion.endO2W over the shutter
+    InstMotion motion;
 };
-static_assert(sizeof(Camera) == 112, "Camera record must stay 112 bytes");
+static_assert(sizeof(Camera) == 320, "Camera record must be 320 bytes");
 
 // ---------------------------------------------------------------- scene view
 // Device pointers of one uploaded scene, passed by value to kernels (or read from an
@@ -192,6 +215,11 @@ struct SceneView {
     const float* cdf;
     const uint32_t* origToLeaf;
     const uint8_t* instClass;     // per instance: material type, kMatIndex for null-BSDF ones
+    const InstMotion* motion;     // per instance, read for instances flagged kInstAnimated
+    int32_t ext;                  // 1: emitters other than area lights, an environment map,
+                                  // animated instances, a thin-lens or moving camera (the
+                                  // kernels' EXT variants handle these)
+    int32_t pad;
     uint32_t tlasRoot;            // kEmpty when the scene has no primitives
     int32_t numEmitters;
     int32_t numInstances;

@@ -114,6 +114,10 @@ typedef struct gnd_scene_desc {
     int32_t pad2;
     const float* env_texels;
     const float* env_dist;
+    /* motion blur (animated.cpp): num_instances motion records (gnd::InstMotion, 192
+     * bytes) when any instance has a toWorldEnd, else NULL; an instance moves when its
+     * traversal record's kind has bit 31 set */
+    const void* inst_motion;
 } gnd_scene_desc;
 
 /* ------------------------------------------------------------------ host framework */
