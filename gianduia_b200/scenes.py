@@ -378,6 +378,135 @@ def motion(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gp
     return path
 
 
+# ------------------------------------------------------------------ textures
+
+
+def write_png(path, img):
+    """A PNG (zlib, filter 0 on every row) from a uint8 or uint16 array [h, w, c], c = 1
+    (grey), 2 (grey + alpha), 3 (RGB) or 4 (RGBA)."""
+    import zlib
+    img = np.asarray(img)
+    if img.ndim == 2:
+        img = img[..., None]
+    h, w, c = img.shape
+    depth = 16 if img.dtype == np.uint16 else 8
+    rows = img.astype(">u2" if depth == 16 else np.uint8)
+    raw = b"".join(b"\0" + rows[y].tobytes() for y in range(h))
+    ctype = {1: 0, 2: 4, 3: 2, 4: 6}[c]
+
+    def chunk(t, body):
+        return struct.pack(">I", len(body)) + t + body + struct.pack(">I", zlib.crc32(t + body) & 0xFFFFFFFF)
+
+    data = b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, depth, ctype, 0, 0, 0))
+    data += chunk(b"IDAT", zlib.compress(raw, 6)) + chunk(b"IEND", b"")
+    with open(path, "wb") as f:
+        f.write(data)
+
+
+def write_exr_float(path, rgb):
+    """An uncompressed scanline OpenEXR file with FLOAT R, G, B channels from [h, w, 3]."""
+    rgb = np.asarray(rgb, np.float32)
+    h, w, _ = rgb.shape
+    header = bytearray(struct.pack("<II", 20000630, 2))
+
+    def attr(name, typ, value):
+        header.extend(name.encode() + b"\0" + typ.encode() + b"\0" + struct.pack("<i", len(value)) + value)
+
+    attr("channels", "chlist", b"".join(c + b"\0" + struct.pack("<iBBBBii", 2, 0, 0, 0, 0, 1, 1) for c in (b"B", b"G", b"R")) + b"\0")
+    attr("compression", "compression", b"\0")
+    box = struct.pack("<iiii", 0, 0, w - 1, h - 1)
+    attr("dataWindow", "box2i", box)
+    attr("displayWindow", "box2i", box)
+    attr("lineOrder", "lineOrder", b"\0")
+    attr("pixelAspectRatio", "float", struct.pack("<f", 1.0))
+    attr("screenWindowCenter", "v2f", struct.pack("<ff", 0.0, 0.0))
+    attr("screenWindowWidth", "float", struct.pack("<f", 1.0))
+    header.extend(b"\0")
+    line = 8 + 12 * w
+    table = b"".join(struct.pack("<Q", len(header) + 8 * h + y * line) for y in range(h))
+    blocks = b"".join(struct.pack("<ii", y, 12 * w) + rgb[y, :, ::-1].T.astype("<f4").tobytes() for y in range(h))
+    with open(path, "wb") as f:
+        f.write(bytes(header) + table + blocks)
+
+
+def _texture(kind, name, props, children=()):
+    out = ['<texture type="%s" name="%s">' % (kind, name)]
+    for k, v in props.items():
+        if isinstance(v, str):
+            out.append('<string name="%s" value="%s"/>' % (k, v))
+        elif isinstance(v, int):
+            out.append('<integer name="%s" value="%d"/>' % (k, v))
+        elif np.ndim(v) == 0:
+            out.append('<float name="%s" value="%s"/>' % (k, _fmt(v)))
+        elif len(v) == 2:
+            out.append('<vector2 name="%s" value="%s, %s"/>' % ((k,) + tuple(_fmt(x) for x in v)))
+        elif k == "axis":
+            out.append('<vector name="%s" value="%s, %s, %s"/>' % ((k,) + tuple(_fmt(x) for x in v)))
+        else:
+            out.append(_color(k, v))
+    out += list(children)
+    out.append("</texture>")
+    return "\n".join(out)
+
+
+def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gpu"):
+    """The Cornell box with the reference's procedural and image textures on its walls and
+    boxes: Perlin turbulence (floor), cellular cracks (back wall), an sRGB PNG with linear
+    filtering (left wall), a float EXR with closest filtering and clamping (right wall),
+    a domain-warped checkerboard (ceiling), marble and wood (boxes). Returns the XML path."""
+    os.makedirs(out_dir, exist_ok=True)
+    write_plane_obj(os.path.join(out_dir, "plane.obj"))
+    write_cube_obj(os.path.join(out_dir, "cube.obj"))
+    rng = np.random.default_rng(7)
+    y, x = np.mgrid[0:24, 0:32]
+    png = np.stack([(x * 8) % 256, (y * 10) % 256, ((x + y) * 5) % 256], axis=-1).astype(np.uint8)
+    write_png(os.path.join(out_dir, "wall.png"), png)
+    write_exr_float(os.path.join(out_dir, "wall.exr"), rng.random((12, 16, 3)) * 0.8 + 0.1)
+    tex = {
+        0: _texture("perlin_color", "albedo", {"value1": (0.2, 0.25, 0.3), "value2": (0.8, 0.75, 0.6), "scale": 0.35, "octaves": 5}),
+        1: _texture("domainWarp_color", "albedo", {"strength": 0.4}, [
+            _texture("checkerboard_color", "base", {"value1": (0.9, 0.9, 0.9), "value2": (0.2, 0.3, 0.6), "scale": (0.25, 0.25)}),
+            _texture("perlin_color", "warp", {"scale": 0.5, "octaves": 3})]),
+        2: _texture("cellular_color", "albedo", {"value1": (0.1, 0.1, 0.1), "value2": (0.85, 0.8, 0.7), "scale": 0.25,
+                                                  "mode": "cracks", "metric": "manhattan"}),
+        3: _texture("image_color", "albedo", {"filename": "wall.png", "interpolation_mode": "linear", "color_space": "sRGB",
+                                               "repeat_mode": "repeat"}),
+        4: _texture("image_color", "albedo", {"filename": "wall.exr", "interpolation_mode": "closest", "repeat_mode": "clamp"}),
+    }
+    walls = [
+        [("scale", (2, 1, 2)), ("translate", (0, -1, 0))],
+        [("scale", (2, 1, 2)), ("rotate", ((1, 0, 0), 180)), ("translate", (0, 1, 0))],
+        [("scale", (2, 1, 2)), ("rotate", ((1, 0, 0), 90)), ("translate", (0, 0, -1))],
+        [("scale", (2, 1, 2)), ("rotate", ((0, 0, 1), -90)), ("translate", (-1, 0, 0))],
+        [("scale", (2, 1, 2)), ("rotate", ((0, 0, 1), 90)), ("translate", (1, 0, 0))],
+    ]
+    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height),
+           '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
+           '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
+    for k, tr in enumerate(walls):
+        shape = '<shape type="mesh" id="plane"><string name="filename" value="plane.obj"/></shape>' if k == 0 else '<ref id="plane"/>'
+        xml += ["<primitive>", _transform(tr), shape, '<material type="matte">', tex[k], "</material>", "</primitive>"]
+    boxes = [
+        ([("scale", (0.6, 0.6, 0.6)), ("rotate", ((0, 1, 0), 18)), ("translate", (0.35, -0.7, 0.3))],
+         _texture("marble_color", "albedo", {"scale": 0.3, "octaves": 4, "vein_freq": 8.0, "turb_scale": 3.0})),
+        ([("scale", (0.6, 1.2, 0.6)), ("rotate", ((0, 1, 0), -15)), ("translate", (-0.35, -0.4, -0.3))],
+         _texture("wood_color", "Kd", {"scale": 0.5, "octaves": 3, "vein_freq": 20.0, "axis": (0.0, 1.0, 0.3)})),
+    ]
+    for k, (tr, t) in enumerate(boxes):
+        shape = '<shape type="mesh" id="cube"><string name="filename" value="cube.obj"/></shape>' if k == 0 else '<ref id="cube"/>'
+        mat = ('<material type="matte">' + t + "</material>") if k == 0 else \
+            ('<material type="plastic">' + t + '<float name="eta" value="1.5"/><float name="roughness" value="0.3"/></material>')
+        xml += ["<primitive>", _transform(tr), shape, mat, "</primitive>"]
+    xml += ["<primitive>",
+            _transform([("scale", (0.5, 1, 0.4)), ("rotate", ((1, 0, 0), 180)), ("translate", (0, 0.998, 0))]),
+            '<ref id="plane"/>', '<material type="matte">', _color("albedo", (0, 0, 0)), "</material>",
+            '<emitter type="area">', _color("radiance", (17, 12, 4)), "</emitter>", "</primitive>", "</scene>"]
+    path = os.path.join(out_dir, "textures.xml")
+    with open(path, "w") as f:
+        f.write("\n".join(xml) + "\n")
+    return path
+
+
 # ------------------------------------------------------------------ light sources
 
 

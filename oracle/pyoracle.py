@@ -76,6 +76,8 @@ def lib():
             L.orc_motion_interpolate.argtypes = [_f32p, _f32p, ctypes.c_float, _f32p, _f32p]
             L.orc_round_half.restype = ctypes.c_float
             L.orc_round_half.argtypes = [ctypes.c_float]
+            L.orc_perlin_perm.argtypes = [ctypes.POINTER(ctypes.c_int32)]
+            L.orc_tex_eval.argtypes = [ctypes.c_char_p, ctypes.c_int64, _f32p, _f32p, ctypes.c_char_p, ctypes.c_int]
             _lib = L
     return _lib
 
@@ -327,3 +329,26 @@ def motion_interpolate(a, b, t):
     mi = np.zeros((3, 4), np.float32)
     lib().orc_motion_interpolate(_fp(a), _fp(b), t, _fp(m), _fp(mi))
     return m, mi
+
+
+def tex_eval(xml_path, p, n=None, dpdu=None, uv=None):
+    """Evaluates the texture that is the root element of `xml_path` at surface points
+    (p, n, dpdu, uv); returns rgb per point (float textures repeat their value)."""
+    p = np.asarray(p, np.float32).reshape(-1, 3)
+    k = p.shape[0]
+    pts = np.zeros((k, 11), np.float32)
+    pts[:, 0:3] = p
+    pts[:, 3:6] = (0, 0, 1) if n is None else np.asarray(n, np.float32).reshape(-1, 3)
+    pts[:, 6:9] = (1, 0, 0) if dpdu is None else np.asarray(dpdu, np.float32).reshape(-1, 3)
+    pts[:, 9:11] = 0 if uv is None else np.asarray(uv, np.float32).reshape(-1, 2)
+    out = np.zeros((k, 3), np.float32)
+    err = ctypes.create_string_buffer(512)
+    if lib().orc_tex_eval(os.fsencode(xml_path), k, _fp(pts), _fp(out), err, 512) != 0:
+        raise RuntimeError(err.value.decode())
+    return out
+
+
+def perlin_perm():
+    out = np.zeros(512, np.int32)
+    lib().orc_perlin_perm(out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    return out

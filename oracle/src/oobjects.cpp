@@ -2,6 +2,7 @@
 // textures, media, emitters, camera, film, filters, scene) and the name registry,
 // restated on the CPU.
 #include "oscene.h"
+#include "otextures.h"
 #include <algorithm>
 #include <cstring>
 #include <filesystem>
@@ -465,7 +466,7 @@ static float halfToFloat(uint16_t h) {
     else v = std::ldexp((float)(m | 1024), (int)e - 25);
     return sign ? -v : v;
 }
-static void loadEXR(const std::string& path, int& w, int& h, std::vector<Color>& px) {
+void loadEXR(const std::string& path, int& w, int& h, std::vector<Color>& px) {
     std::ifstream f(path, std::ios::binary);
     if (!f) throw std::runtime_error("EnvMap: cannot open " + path);
     std::vector<uint8_t> d((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
@@ -830,6 +831,18 @@ std::unique_ptr<Object> createInstance(const std::string& t, const PropertyList&
     if (t == "constant_float") return std::make_unique<ConstantTexture<float>>(p);
     if (t == "checkerboard_color") return std::make_unique<CheckerTexture<Color>>(p);
     if (t == "checkerboard_float") return std::make_unique<CheckerTexture<float>>(p);
+    if (t == "perlin_color") return std::make_unique<PerlinTexture<Color>>(p);
+    if (t == "perlin_float") return std::make_unique<PerlinTexture<float>>(p);
+    if (t == "marble_color") return std::make_unique<MarbleTexture<Color>>(p);
+    if (t == "marble_float") return std::make_unique<MarbleTexture<float>>(p);
+    if (t == "wood_color") return std::make_unique<WoodTexture<Color>>(p);
+    if (t == "wood_float") return std::make_unique<WoodTexture<float>>(p);
+    if (t == "cellular_color") return std::make_unique<CellularTexture<Color>>(p);
+    if (t == "cellular_float") return std::make_unique<CellularTexture<float>>(p);
+    if (t == "domainWarp_color") return std::make_unique<DomainWarpTexture<Color>>(p);
+    if (t == "domainWarp_float") return std::make_unique<DomainWarpTexture<float>>(p);
+    if (t == "image_color") return std::make_unique<ImageTexture<Color>>(p);
+    if (t == "image_float") return std::make_unique<ImageTexture<float>>(p);
     throw std::runtime_error("Cannot instantiate object: class '" + t + "' is not registered!");
 }
 
