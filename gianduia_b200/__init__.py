@@ -180,6 +180,8 @@ class SceneDesc(ctypes.Structure):
         ("env_emitter", ctypes.c_int32), ("env_width", ctypes.c_int32), ("env_height", ctypes.c_int32),
         ("env_marginal_integral", ctypes.c_float), ("env_strength", ctypes.c_float), ("pad2", ctypes.c_int32),
         ("env_texels", _vp), ("env_dist", _vp), ("inst_motion", _vp),
+        ("tex_nodes", _vp), ("num_tex_nodes", ctypes.c_int32), ("pad3", ctypes.c_int32),
+        ("tex_texels", _vp), ("num_tex_texels", ctypes.c_int64),
     ]
 
 

@@ -46,6 +46,48 @@ void Context::checkKernelErrors(const char* what) {
     }
 }
 
+// Texture trees of a scene description: every slot's node, every node's children and
+// texels in range, and warps nested inside warp inputs at most kTexWarpNesting deep (the
+// depth the kernels evaluate).
+namespace {
+int warpNesting(const TexNode* nodes, int64_t n, int64_t node, int depth) {
+    if (depth > kTexWarpNesting) return depth;
+    int need = 0;
+    for (int64_t hop = 0; hop <= n; ++hop) {
+        const TexNode& t = nodes[node];
+        if (t.kind != kTnWarp) return need;
+        need = std::max(need, 1 + warpNesting(nodes, n, t.b, depth + 1));
+        node = t.a;
+    }
+    throw Error(GND_ERR_INVALID, "texture tree has a cycle");
+}
+void validateTextures(const gnd_scene_desc* d) {
+    const int64_t n = d->num_tex_nodes;
+    if (n < 0 || d->num_tex_texels < 0 || (n > 0 && !d->tex_nodes) || (d->num_tex_texels > 0 && !d->tex_texels))
+        throw Error(GND_ERR_INVALID, "bad texture arrays");
+    auto slot = [&](const ColorTex& t) {
+        if (t.kind > kTexNode) throw Error(GND_ERR_INVALID, "unknown color texture kind");
+        if (t.kind == kTexNode && (int64_t)t.node >= n) throw Error(GND_ERR_INVALID, "texture node out of range");
+    };
+    const Material* mats = reinterpret_cast<const Material*>(d->materials);
+    for (int m = 0; m < d->num_materials; ++m) { slot(mats[m].a); slot(mats[m].b); }
+    const Emitter* ems = reinterpret_cast<const Emitter*>(d->emitters);
+    for (int k = 0; k < d->num_emitters; ++k) slot(ems[k].radiance);
+    const TexNode* nodes = reinterpret_cast<const TexNode*>(d->tex_nodes);
+    for (int64_t i = 0; i < n; ++i) {
+        const TexNode& t = nodes[i];
+        if (t.kind < kTnConstant || t.kind > kTnWarp) throw Error(GND_ERR_INVALID, "unknown texture node kind");
+        if (t.kind == kTnWarp && (t.a < 0 || t.a >= n || t.b < 0 || t.b >= n)) throw Error(GND_ERR_INVALID, "warp input out of range");
+        if (t.kind == kTnImage && (t.w <= 0 || t.h <= 0 || t.a < 0 || (int64_t)t.a + (int64_t)t.w * t.h > d->num_tex_texels))
+            throw Error(GND_ERR_INVALID, "image texels out of range");
+        if (t.kind == kTnCellular && ((t.flags >> kTnMetricShift) & 3) > 2) throw Error(GND_ERR_INVALID, "unknown cellular metric");
+    }
+    for (int64_t i = 0; i < n; ++i)
+        if (nodes[i].kind == kTnWarp && warpNesting(nodes, n, i, 0) > kTexWarpNesting)
+            throw Error(GND_ERR_INVALID, "warps nested in warp inputs deeper than supported");
+}
+}  // namespace
+
 Context* ctxOf(gnd_gpu_ctx* c) {
     if (!c) throw Error(GND_ERR_INVALID, "null context");
     return reinterpret_cast<Context*>(c);
@@ -186,6 +228,7 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
                 throw Error(GND_ERR_INVALID, "area emitter instance out of range");
             if (ems[k].type == kEmitEnv && k != d->env_emitter) throw Error(GND_ERR_INVALID, "environment emitter without its map");
         }
+        validateTextures(d);
         c->bind();
         std::lock_guard<FairMutex> lk(c->mu);
         auto ds = std::make_unique<DeviceScene>();
@@ -213,6 +256,9 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         v.cdf = upload<float>(*ds, c->stream, d->cdf, d->cdf_len);
         v.origToLeaf = upload<uint32_t>(*ds, c->stream, d->orig_to_leaf, d->orig_to_leaf_len);
         v.motion = d->inst_motion ? upload<InstMotion>(*ds, c->stream, d->inst_motion, d->num_instances) : nullptr;
+        v.texNodes = upload<TexNode>(*ds, c->stream, d->tex_nodes, d->num_tex_nodes);
+        v.texels = upload<float>(*ds, c->stream, d->tex_texels, (size_t)d->num_tex_texels * 4);
+        v.numTexNodes = d->num_tex_nodes;
         // environment map (texels + the sampling tables of distribution.cpp)
         v.env = EnvView{};
         v.env.emitter = -1;
@@ -289,7 +335,8 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         v.fastBoxes = nanBounds ? 0 : 1;
         if (d->camera) std::memcpy(&v.camera, d->camera, sizeof(Camera));
         // the rarer features select the kernels' EXT variants
-        bool ext = v.motion != nullptr || v.env.emitter >= 0 || v.camera.kind == kCamThinLens || v.camera.animated != 0;
+        bool ext = v.motion != nullptr || v.env.emitter >= 0 || v.camera.kind == kCamThinLens || v.camera.animated != 0 ||
+                   d->num_tex_nodes > 0;
         for (int k = 0; k < d->num_emitters; ++k) ext = ext || ems[k].type != kEmitArea;
         v.ext = ext ? 1 : 0;
         // null-BSDF mask and material type per instance

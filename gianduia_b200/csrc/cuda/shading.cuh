@@ -449,25 +449,26 @@ __device__ __forceinline__ V3 lobeSample(const Lobe& l, V3 wo, V3& wi, V2 u, flo
 
 // Material -> lobe at a shading point (matte.cpp:46-53, plastic.cpp:74-91,
 // conductor.cpp:101-120, glass.cpp:98-115). Returns false for the index material.
-template <uint32_t M = kLobesAll>
-__device__ __forceinline__ bool makeLobe(const Material& m, V2 uv, Lobe& l) {
+// `tex` evaluates a color slot at the point.
+template <uint32_t M, class TexF>
+__device__ __forceinline__ bool makeLobeT(const Material& m, TexF tex, Lobe& l) {
     switch (m.type) {
         case kMatMatte:
             if (!(M & kLobesMatte)) return false;
             l.kind = 0;
-            l.a = evalTex(m.a, uv);
+            l.a = tex(m.a);
             return true;
         case kMatPlastic:
             if (!(M & kLobesPlastic)) return false;
-            l.a = evalTex(m.a, uv);
-            l.b = evalTex(m.b, uv);
+            l.a = tex(m.a);
+            l.b = tex(m.b);
             l.eta = m.eta;
             if (m.roughness == 0.0f) l.kind = 5;
             else { l.kind = 6; l.ggx = makeGgx(roughnessToAlpha(m.roughness)); }
             return true;
         case kMatConductor:
             if (!(M & kLobesConductor)) return false;
-            l.a = evalTex(m.a, uv);
+            l.a = tex(m.a);
             l.ceta = v3(m.condEta[0], m.condEta[1], m.condEta[2]);
             l.ck = v3(m.condK[0], m.condK[1], m.condK[2]);
             if (m.roughness == 0.0f) l.kind = 1;
@@ -475,8 +476,8 @@ __device__ __forceinline__ bool makeLobe(const Material& m, V2 uv, Lobe& l) {
             return true;
         case kMatGlass:
             if (!(M & kLobesGlass)) return false;
-            l.a = evalTex(m.a, uv);
-            l.b = evalTex(m.b, uv);
+            l.a = tex(m.a);
+            l.b = tex(m.b);
             l.eta = m.eta;
             if (m.roughness == 0.0f) l.kind = 2;
             else { l.kind = 4; l.ggx = makeGgx(roughnessToAlpha(m.roughness)); }
@@ -484,6 +485,11 @@ __device__ __forceinline__ bool makeLobe(const Material& m, V2 uv, Lobe& l) {
         default:
             return false;
     }
+}
+
+template <uint32_t M = kLobesAll>
+__device__ __forceinline__ bool makeLobe(const Material& m, V2 uv, Lobe& l) {
+    return makeLobeT<M>(m, [uv](const ColorTex& t) { return evalTex(t, uv); }, l);
 }
 
 // BSDF with one lobe of weight 1 (bsdf.cpp:6-136): world-space evaluation.

@@ -21,6 +21,7 @@
 #include <cstring>
 
 #include "shading.cuh"
+#include "textures.cuh"
 #include "traverse.cuh"
 #include "wavefront.h"
 
@@ -301,6 +302,18 @@ __device__ __forceinline__ V3 emitterEval(const Emitter& e, V3 n, V2 uv, V3 w) {
     if (dot(n, w) > 0.0f) return evalTex(e.radiance, uv);
     return v3s(0.0f);
 }
+// A color slot at a surface point: texture trees in the EXT variants, constant and
+// checkerboard slots everywhere.
+template <bool EXT>
+__device__ __forceinline__ V3 evalColor(const SceneView& s, const ColorTex& t, V3 p, V3 n, V3 dpdu, V2 uv) {
+    if (EXT && t.kind == kTexNode) return evalTexTree(s, t.node, p, n, dpdu, uv);
+    return evalTex(t, uv);
+}
+template <bool EXT>
+__device__ __forceinline__ V3 emitterEvalAt(const SceneView& s, const Emitter& e, V3 p, V3 n, V3 dpdu, V2 uv, V3 w) {
+    if (dot(n, w) > 0.0f) return evalColor<EXT>(s, e.radiance, p, n, dpdu, uv);
+    return v3s(0.0f);
+}
 
 // ---------------------------------------------------------------- environment map
 // SphericalCoordinates (constants.h:80-85): (theta from +z, phi in [0, 2 pi))
@@ -443,6 +456,7 @@ __device__ __noinline__ void deltaSample(const Emitter& e, V3 ref, LightSample& 
 // `time` is the reference point's time (ref.time): the path's for surface next-event
 // estimation, 0 for a volume scattering point (volPath.cpp:61-62 builds a fresh reference)
 __device__ __forceinline__ void areaSample(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls, float time);
+template <bool EXT>
 __device__ __forceinline__ void areaSampleWith(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls, float time,
                                                const Xf34& o2w, const Xf34& w2o);
 __device__ __forceinline__ void emitterSample(const SceneView& s, int ei, V3 ref, V2 u, LightSample& ls, float time) {
@@ -458,7 +472,7 @@ __device__ __forceinline__ void emitterSampleT(const SceneView& s, int ei, V3 re
         return;
     }
     const Emitter e = s.emitters[ei];
-    areaSampleWith(s, e, ref, u, ls, time, s.instS[e.instance].o2w, s.instT[e.instance].w2o);
+    areaSampleWith<false>(s, e, ref, u, ls, time, s.instS[e.instance].o2w, s.instT[e.instance].w2o);
 }
 
 // Environment light seen by an escaping ray, weighted against the previous bounce's pdf
@@ -478,7 +492,8 @@ __device__ __noinline__ V3 envMissRadiance(const SceneView& s, V3 o, V3 d, V3 tp
     return (tp * Le) * w;
 }
 
-// AreaLight::sample (area.cpp:51-88)
+// AreaLight::sample (area.cpp:51-88); the sampled point carries p, n and uv (no dpdu)
+template <bool EXT>
 __device__ __forceinline__ void areaSampleWith(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls, float time,
                                                const Xf34& o2w, const Xf34& w2o) {
     ls.delta = false;
@@ -501,7 +516,7 @@ __device__ __forceinline__ void areaSampleWith(const SceneView& s, const Emitter
     ls.Li = v3s(0.0f);
     if (areaPdf <= kEpsilon || cosTheta <= kEpsilon) return;
     ls.pdf = areaPdf * dist / cosTheta;
-    ls.Li = cdiv(emitterEval(e, ls.n, ls.uv, normalize(ref - ls.p)), ls.pdf);
+    ls.Li = cdiv(emitterEvalAt<EXT>(s, e, ls.p, ls.n, v3s(0.0f), ls.uv, normalize(ref - ls.p)), ls.pdf);
 }
 
 // An animated area light at the reference point's time (m_primitive->getToWorld(ref.time),
@@ -509,12 +524,12 @@ __device__ __forceinline__ void areaSampleWith(const SceneView& s, const Emitter
 __device__ __noinline__ void areaSampleMoving(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls, float time) {
     Xf34 o2w, w2o;
     motionAt(s.motion[e.instance], s.instS[e.instance].o2w, s.instT[e.instance].w2o, time, o2w, w2o);
-    areaSampleWith(s, e, ref, u, ls, time, o2w, w2o);
+    areaSampleWith<true>(s, e, ref, u, ls, time, o2w, w2o);
 }
 
 __device__ __forceinline__ void areaSample(const SceneView& s, const Emitter& e, V3 ref, V2 u, LightSample& ls, float time) {
     if (s.instT[e.instance].kind & kInstAnimated) areaSampleMoving(s, e, ref, u, ls, time);
-    else areaSampleWith(s, e, ref, u, ls, time, s.instS[e.instance].o2w, s.instT[e.instance].w2o);
+    else areaSampleWith<true>(s, e, ref, u, ls, time, s.instS[e.instance].o2w, s.instT[e.instance].w2o);
 }
 
 // Emitter sampling in a kernel variant: without EXT every emitter is a static area light.
@@ -913,12 +928,13 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
             const InstShade& is = s.instS[h.inst];
             const Material mat = s.materials[is.material];
             Bsdf bsdf;
-            const bool hasBsdf = makeLobe<M>(mat, si.uv, bsdf.lobe);
+            const bool hasBsdf = makeLobeT<M>(mat, [&](const ColorTex& t) { return evalColor<EXT>(s, t, si.p, si.n, si.dpdu, si.uv); },
+                                              bsdf.lobe);
             if (is.emitter >= 0) {
                 bool skip = (bounces == 0 && !hasBsdf);
                 if (!skip) {
                     const Emitter e = s.emitters[is.emitter];
-                    V3 Le = emitterEval(e, si.n, si.uv, -d);
+                    V3 Le = emitterEvalAt<EXT>(s, e, si.p, si.n, si.dpdu, si.uv, -d);
                     if (!isBlack(Le)) {
                         float w = 1.0f;
                         if (!specular) {

@@ -12,6 +12,7 @@
 #include <zlib.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -199,6 +200,143 @@ void readEXR(const std::string& path, int& width, int& height, std::vector<float
             }
         }
     }
+}
+
+namespace {
+std::vector<uint8_t> readAll(const std::string& path, const char* what) {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::runtime_error(std::string(what) + ": cannot open " + path);
+    std::vector<uint8_t> d;
+    uint8_t buf[65536];
+    size_t n;
+    while ((n = std::fread(buf, 1, sizeof(buf), f)) > 0) d.insert(d.end(), buf, buf + n);
+    std::fclose(f);
+    return d;
+}
+
+// A float rounded to the nearest binary16 value (ties to even), as Imf::Rgba stores it:
+// 11 significant bits in the normal range, multiples of 2^-24 below 2^-14, infinity from
+// 65520 on.
+float toHalfPrecision(float f) {
+    if (!std::isfinite(f) || f == 0.0f) return f;
+    const float a = std::fabs(f);
+    float r;
+    if (a < 6.103515625e-05f) {
+        r = std::nearbyint(a * 16777216.0f) / 16777216.0f;
+    } else {
+        int e;
+        const float m = std::frexp(a, &e);   // a = m 2^e, m in [0.5, 1)
+        r = std::ldexp(std::nearbyint(std::ldexp(m, 11)), e - 11);
+        if (r > 65504.0f) r = INFINITY;
+    }
+    return f < 0.0f ? -r : r;
+}
+
+// PNG (ISO/IEC 15948): 8- or 16-bit grey, grey + alpha, RGB or RGBA, not interlaced;
+// the IDAT stream inflated, each row's filter (none, sub, up, average, Paeth) undone.
+// 16-bit samples keep their high byte.
+void readPNG(const std::string& path, int& w, int& h, int& channels, std::vector<uint8_t>& px) {
+    const std::vector<uint8_t> d = readAll(path, "TextureCache");
+    const uint8_t magic[8] = {0x89, 0x50, 0x4e, 0x47, 0x0d, 0x0a, 0x1a, 0x0a};
+    if (d.size() < 8 || std::memcmp(d.data(), magic, 8) != 0) throw std::runtime_error("TextureCache: Failed to load image " + path);
+    auto u32 = [&](size_t at) -> uint32_t {
+        if (at + 4 > d.size()) throw std::runtime_error("PNG: truncated file " + path);
+        return (uint32_t)d[at] << 24 | (uint32_t)d[at + 1] << 16 | (uint32_t)d[at + 2] << 8 | (uint32_t)d[at + 3];
+    };
+    int depth = 0, colorType = -1, interlace = 0;
+    bool haveHeader = false;
+    std::vector<uint8_t> stream;
+    for (size_t at = 8;;) {
+        const uint32_t len = u32(at);
+        if ((uint64_t)at + 12 + len > d.size()) throw std::runtime_error("PNG: truncated file " + path);
+        const uint8_t* body = &d[at + 8];
+        const std::string type(reinterpret_cast<const char*>(&d[at + 4]), 4);
+        if (type == "IHDR" && len >= 13) {
+            w = (int)u32(at + 8);
+            h = (int)u32(at + 12);
+            depth = body[8];
+            colorType = body[9];
+            interlace = body[12];
+            haveHeader = true;
+        } else if (type == "IDAT") {
+            stream.insert(stream.end(), body, body + len);
+        } else if (type == "IEND") {
+            break;
+        }
+        at += 12 + (size_t)len;
+    }
+    if (!haveHeader || w <= 0 || h <= 0 || (int64_t)w * h > ((int64_t)1 << 28)) throw std::runtime_error("PNG: bad header in " + path);
+    channels = colorType == 0 ? 1 : colorType == 4 ? 2 : colorType == 2 ? 3 : colorType == 6 ? 4 : 0;
+    if (!channels || interlace || (depth != 8 && depth != 16))
+        throw std::runtime_error("PNG: " + path + ": only 8/16-bit, non-interlaced grey, grey+alpha, RGB or RGBA images");
+    const size_t sampleBytes = (size_t)depth / 8, pixelBytes = (size_t)channels * sampleBytes;
+    const size_t rowBytes = (size_t)w * pixelBytes;
+    std::vector<uint8_t> raw((rowBytes + 1) * (size_t)h);
+    uLongf rawLen = (uLongf)raw.size();
+    if (uncompress(raw.data(), &rawLen, stream.data(), (uLong)stream.size()) != Z_OK || rawLen != raw.size())
+        throw std::runtime_error("PNG: corrupt image data in " + path);
+    std::vector<uint8_t> rows(rowBytes * (size_t)h);
+    for (int y = 0; y < h; ++y) {
+        const uint8_t filter = raw[(size_t)y * (rowBytes + 1)];
+        const uint8_t* src = &raw[(size_t)y * (rowBytes + 1) + 1];
+        uint8_t* dst = &rows[(size_t)y * rowBytes];
+        const uint8_t* up = y > 0 ? dst - rowBytes : nullptr;
+        if (filter > 4) throw std::runtime_error("PNG: bad row filter in " + path);
+        for (size_t i = 0; i < rowBytes; ++i) {
+            const int left = i >= pixelBytes ? dst[i - pixelBytes] : 0;
+            const int above = up ? up[i] : 0;
+            const int corner = (up && i >= pixelBytes) ? up[i - pixelBytes] : 0;
+            int pred = 0;
+            switch (filter) {
+                case 1: pred = left; break;
+                case 2: pred = above; break;
+                case 3: pred = (left + above) >> 1; break;
+                case 4: {
+                    const int est = left + above - corner;
+                    const int dl = std::abs(est - left), da = std::abs(est - above), dc = std::abs(est - corner);
+                    pred = (dl <= da && dl <= dc) ? left : (da <= dc ? above : corner);
+                    break;
+                }
+                default: break;
+            }
+            dst[i] = (uint8_t)(src[i] + pred);
+        }
+    }
+    px.resize((size_t)w * h * channels);
+    for (size_t i = 0; i < px.size(); ++i) px[i] = rows[i * sampleBytes];
+}
+}  // namespace
+
+void readTextureImage(const std::string& path, bool srgb, int& width, int& height, int& channels, std::vector<float>& rgba) {
+    const bool exr = path.size() >= 4 && path.compare(path.size() - 4, 4, ".exr") == 0;
+    if (exr) {
+        std::vector<float> rgb;
+        readEXR(path, width, height, rgb);
+        channels = 4;
+        rgba.assign((size_t)width * height * 4, 1.0f);
+        for (int y = 0; y < height; ++y)
+            for (int x = 0; x < width; ++x) {
+                const float* s = &rgb[3 * ((size_t)y * width + x)];
+                float* o = &rgba[4 * ((size_t)(height - 1 - y) * width + x)];
+                for (int k = 0; k < 3; ++k) o[k] = toHalfPrecision(s[k]);
+            }
+        return;
+    }
+    std::vector<uint8_t> px;
+    readPNG(path, width, height, channels, px);
+    const int c = channels;
+    auto linearize = [](float v) { return v <= 0.04045f ? v / 12.92f : std::pow((v + 0.055f) / 1.055f, 2.4f); };
+    rgba.assign((size_t)width * height * 4, 1.0f);
+    for (int y = 0; y < height; ++y)
+        for (int x = 0; x < width; ++x) {
+            const uint8_t* s = &px[((size_t)(height - 1 - y) * width + x) * c];
+            float* o = &rgba[4 * ((size_t)y * width + x)];
+            for (int k = 0; k < c; ++k) {
+                float v = s[k] / 255.0f;
+                if (srgb && (c <= 3 || k < 3)) v = linearize(v);
+                o[k] = v;
+            }
+        }
 }
 
 }  // namespace gndh

@@ -200,6 +200,196 @@ GND_REGISTER_CLASS(ConstantColor, "constant_color")
 GND_REGISTER_CLASS(ConstantFloat, "constant_float")
 GND_REGISTER_CLASS(CheckerboardColor, "checkerboard_color")
 
+gnd::TexNode ColorTexture::node(TexTables&) const {
+    gnd::TexNode n{};
+    n.kind = rec.kind == gnd::kTexChecker ? gnd::kTnChecker : gnd::kTnConstant;
+    for (int k = 0; k < 3; ++k) { n.v1[k] = rec.v1[k]; n.v2[k] = rec.v2[k]; }
+    n.cscale[0] = rec.scale[0]; n.cscale[1] = rec.scale[1];
+    n.delta[0] = rec.delta[0]; n.delta[1] = rec.delta[1];
+    return n;
+}
+int32_t ColorTexture::flatten(TexTables& t) const {
+    auto it = t.done.find(this);
+    if (it != t.done.end()) return it->second;
+    gnd::TexNode n = node(t);   // flattens the inputs first
+    const int32_t idx = (int32_t)t.nodes.size();
+    t.nodes.push_back(n);
+    t.done.emplace(this, idx);
+    return idx;
+}
+
+namespace {
+// The value1 / value2 pair and p / scale of the procedural color textures
+struct ProceduralColor : ColorTexture {
+    V3 v1{}, v2{};
+    float scale = 1.0f;
+    int octaves = 6;
+    ProceduralColor(const PropertyList& p, V3 d1, V3 d2) {
+        rec.kind = gnd::kTexNode;
+        v1 = p.getColor("value1", d1);
+        v2 = p.getColor("value2", d2);
+        scale = p.getFloat("scale", 1.0f);
+    }
+    gnd::TexNode base(int32_t kind) const {
+        gnd::TexNode n{};
+        n.kind = kind;
+        n.v1[0] = v1.x; n.v1[1] = v1.y; n.v1[2] = v1.z;
+        n.v2[0] = v2.x; n.v2[1] = v2.y; n.v2[2] = v2.z;
+        n.scale = scale;
+        n.octaves = octaves;
+        return n;
+    }
+};
+// perlin.h (texture):15-37: value1 .. value2 by turbulence(p / scale)
+struct PerlinColor : ProceduralColor {
+    explicit PerlinColor(const PropertyList& p) : ProceduralColor(p, gnd::v3s(0.0f), gnd::v3s(1.0f)) {
+        octaves = p.getInteger("octaves", 6);
+    }
+    gnd::TexNode node(TexTables&) const override { return base(gnd::kTnPerlin); }
+};
+// marble.h:15-46 and wood.h:15-46: veins along / around an axis, perturbed by turbulence
+struct VeinColor : ProceduralColor {
+    int32_t kind;
+    float veinFreq, turbScale;
+    V3 axis;
+    VeinColor(const PropertyList& p, int32_t k, V3 d1, V3 d2, float turbDefault) : ProceduralColor(p, d1, d2), kind(k) {
+        octaves = p.getInteger("octaves", 6);
+        veinFreq = p.getFloat("vein_freq", 10.0f);
+        turbScale = p.getFloat("turb_scale", turbDefault);
+        axis = gnd::normalize(p.getVector3("axis", gnd::v3(0.0f, 1.0f, 0.0f)));
+    }
+    gnd::TexNode node(TexTables&) const override {
+        gnd::TexNode n = base(kind);
+        n.veinFreq = veinFreq;
+        n.turbScale = turbScale;
+        n.axis[0] = axis.x; n.axis[1] = axis.y; n.axis[2] = axis.z;
+        return n;
+    }
+};
+struct MarbleColor : VeinColor {
+    explicit MarbleColor(const PropertyList& p) : VeinColor(p, gnd::kTnMarble, gnd::v3s(0.1f), gnd::v3s(0.9f), 5.0f) {}
+};
+struct WoodColor : VeinColor {
+    explicit WoodColor(const PropertyList& p)
+        : VeinColor(p, gnd::kTnWood, gnd::v3(0.6f, 0.4f, 0.2f), gnd::v3(0.3f, 0.15f, 0.05f), 2.0f) {}
+};
+// cellular.h:17-58: Worley F1 (distance) or F2 - F1 (cracks), unknown names fall back
+struct CellularColor : ProceduralColor {
+    int32_t flags = 0;
+    explicit CellularColor(const PropertyList& p) : ProceduralColor(p, gnd::v3s(0.0f), gnd::v3s(1.0f)) {
+        if (p.getString("mode", "distance") == "cracks") flags |= gnd::kTnCracks;
+        const std::string m = p.getString("metric", "euclidean");
+        const int metric = m == "manhattan" ? 1 : (m == "chebyshev" ? 2 : 0);
+        flags |= metric << gnd::kTnMetricShift;
+    }
+    gnd::TexNode node(TexTables&) const override {
+        gnd::TexNode n = base(gnd::kTnCellular);
+        n.flags = flags;
+        return n;
+    }
+};
+// domainWarp.h:13-58: the base texture evaluated at p and uv moved by the warp texture
+struct DomainWarpColor : ColorTexture {
+    float strength;
+    std::shared_ptr<ColorTexture> baseTex, warpTex;
+    explicit DomainWarpColor(const PropertyList& p) : strength(p.getFloat("strength", 1.0f)) { rec.kind = gnd::kTexNode; }
+    void addChild(std::shared_ptr<GndObject> c) override {
+        if (c->getClassType() != ETexture) throw std::runtime_error("WarpTexture: cannot add specified child!");
+        auto t = std::dynamic_pointer_cast<ColorTexture>(c);
+        if (c->getName() == "base") {
+            if (baseTex) throw std::runtime_error("WarpTexture: base texture already defined!");
+            if (!t) throw std::runtime_error("WarpTexture: the base of a color warp must be a color texture");
+            baseTex = t;
+        } else if (c->getName() == "warp") {
+            if (warpTex) throw std::runtime_error("WarpTexture: warp texture already defined!");
+            if (!t) throw std::runtime_error("WarpTexture: the warp input must be a color texture");
+            warpTex = t;
+        }
+    }
+    void activate() override {
+        if (!baseTex) throw std::runtime_error("WarpTexture: missing base texture!");
+        if (!warpTex) throw std::runtime_error("WarpTexture: missing warp texture!");
+    }
+    gnd::TexNode node(TexTables& t) const override {
+        gnd::TexNode n{};
+        n.kind = gnd::kTnWarp;
+        n.strength = strength;
+        n.a = baseTex->flatten(t);
+        n.b = warpTex->flatten(t);
+        return n;
+    }
+};
+// imageTexture.cpp:11-143 with the texels of textureCache.h
+struct ImageColor : ColorTexture {
+    std::string filename, baseDir;
+    bool linear = false, clamp = false, srgb = false;
+    int width = 0, height = 0, channels = 0;
+    std::vector<float> texels;
+    explicit ImageColor(const PropertyList& p) : filename(p.getString("filename")) {
+        rec.kind = gnd::kTexNode;
+        const std::string interp = p.getString("interpolation_mode", "closest");
+        if (interp == "linear") linear = true;
+        else if (interp != "closest") throw std::runtime_error("ImageTexture: Unknown interpolation mode " + interp);
+        const std::string cs = p.getString("color_space", "linear");
+        if (cs == "sRGB") srgb = true;
+        else if (cs != "linear") throw std::runtime_error("ImageTexture: Unknown color space " + cs);
+        const std::string rep = p.getString("repeat_mode", "repeat");
+        if (rep == "clamp") clamp = true;
+        else if (rep != "repeat") throw std::runtime_error("ImageTexture: Unknown repeat mode " + rep);
+    }
+    void setBaseDir(const std::string& d) override { baseDir = d; }
+    void activate() override {
+        std::filesystem::path abs(filename);
+        if (abs.is_relative() && !baseDir.empty()) abs = std::filesystem::path(baseDir) / abs;
+        readTextureImage(abs.string(), srgb, width, height, channels, texels);
+    }
+    gnd::TexNode node(TexTables& t) const override {
+        gnd::TexNode n{};
+        n.kind = gnd::kTnImage;
+        n.flags = (linear ? gnd::kTnLinear : 0) | (clamp ? gnd::kTnClamp : 0);
+        if (t.texels.size() / 4 + (size_t)width * height > (size_t)INT32_MAX)
+            throw std::runtime_error("ImageTexture: image textures larger than 2^31 texels in total");
+        n.a = (int32_t)(t.texels.size() / 4);
+        n.b = channels;
+        n.w = width;
+        n.h = height;
+        // extractValue (imageTexture.cpp:96-100): rgb of 3-4 channel images, the first
+        // channel repeated otherwise
+        for (size_t i = 0; i < (size_t)width * height; ++i) {
+            const float* q = &texels[4 * i];
+            const bool rgb = channels >= 3;
+            t.texels.push_back(q[0]);
+            t.texels.push_back(rgb ? q[1] : q[0]);
+            t.texels.push_back(rgb ? q[2] : q[0]);
+            t.texels.push_back(q[3]);
+        }
+        return n;
+    }
+};
+// The float variants of the procedural and image textures load, but only constant float
+// textures fill a slot of the GPU path (roughness, eta).
+struct NonConstantFloat : FloatTexture {
+    explicit NonConstantFloat(const PropertyList&) { constant = false; }
+};
+}  // namespace
+GND_REGISTER_CLASS(PerlinColor, "perlin_color")
+GND_REGISTER_CLASS(MarbleColor, "marble_color")
+GND_REGISTER_CLASS(WoodColor, "wood_color")
+GND_REGISTER_CLASS(CellularColor, "cellular_color")
+GND_REGISTER_CLASS(DomainWarpColor, "domainWarp_color")
+GND_REGISTER_CLASS(ImageColor, "image_color")
+namespace {
+struct NonConstantFloatNames {
+    NonConstantFloatNames() {
+        for (const char* n : {"checkerboard_float", "perlin_float", "marble_float", "wood_float", "cellular_float",
+                              "domainWarp_float", "image_float"})
+            GndFactory::getInstance()->registerClass(n, [](const PropertyList& p) -> std::unique_ptr<GndObject> {
+                return std::make_unique<NonConstantFloat>(p);
+            });
+    }
+} nonConstantFloatNames;
+}  // namespace
+
 // ---------------------------------------------------------------- media
 // homogeneous.cpp:14-20
 struct HomogeneousMediumObj : MediumObj {
@@ -229,15 +419,16 @@ void MaterialObj::addChild(std::shared_ptr<GndObject> c) {
 }
 
 namespace {
-void setColorSlot(gnd::ColorTex& slot, bool& have, const std::shared_ptr<GndObject>& c) {
+void setColorSlot(gnd::ColorTex& slot, bool& have, const std::shared_ptr<GndObject>& c, std::shared_ptr<ColorTexture>& keep) {
     auto t = std::dynamic_pointer_cast<ColorTexture>(c);
     if (!t) throw std::runtime_error("Material: texture '" + c->getName() + "' must be a color texture");
     slot = t->rec;
+    keep = t;
     have = true;
 }
 void setFloatSlot(float& slot, bool& have, const std::shared_ptr<GndObject>& c) {
     auto t = std::dynamic_pointer_cast<FloatTexture>(c);
-    if (!t) throw std::runtime_error("Material: texture '" + c->getName() + "' must be a constant float texture");
+    if (!t || !t->constant) throw std::runtime_error("Material: texture '" + c->getName() + "' must be a constant float texture");
     slot = t->value;
     have = true;
 }
@@ -254,7 +445,7 @@ struct MatteMat : MaterialObj {
         if (c->getClassType() != ETexture) return MaterialObj::addChild(c);
         if (c->getName() == "albedo") {
             if (hasA) throw std::runtime_error("Matte: there's already an albedo defined!");
-            setColorSlot(rec.a, hasA, c);
+            setColorSlot(rec.a, hasA, c, texA);
         } else MaterialObj::addChild(c);
     }
     void activate() override { if (!hasA) rec.a = missingTexture(); }
@@ -272,8 +463,8 @@ struct PlasticMat : MaterialObj {
     void addChild(std::shared_ptr<GndObject> c) override {
         if (c->getClassType() != ETexture) return;   // plastic.cpp:30
         const std::string& n = c->getName();
-        if (n == "Kd") setColorSlot(rec.a, hKd, c);
-        else if (n == "Ks") setColorSlot(rec.b, hKs, c);
+        if (n == "Kd") setColorSlot(rec.a, hKd, c, texA);
+        else if (n == "Ks") setColorSlot(rec.b, hKs, c, texB);
         else if (n == "roughness") setFloatSlot(rec.roughness, hR, c);
         else if (n == "eta") setFloatSlot(rec.eta, hE, c);
         else MaterialObj::addChild(c);
@@ -299,7 +490,7 @@ struct ConductorMat : MaterialObj {
     void addChild(std::shared_ptr<GndObject> c) override {
         if (c->getClassType() != ETexture) throw std::runtime_error("Conductor: cannot add specified child!");
         const std::string& n = c->getName();
-        if (n == "R") setColorSlot(rec.a, hR, c);
+        if (n == "R") setColorSlot(rec.a, hR, c, texA);
         else if (n == "roughness") setFloatSlot(rec.roughness, hRo, c);
         else if (n == "eta" || n == "k") {
             auto t = std::dynamic_pointer_cast<ColorTexture>(c);
@@ -327,8 +518,8 @@ struct GlassMat : MaterialObj {
     }
     void addChild(std::shared_ptr<GndObject> c) override {
         const std::string& n = c->getName();
-        if (n == "R") setColorSlot(rec.a, hR, c);
-        else if (n == "T") setColorSlot(rec.b, hT, c);
+        if (n == "R") setColorSlot(rec.a, hR, c, texA);
+        else if (n == "T") setColorSlot(rec.b, hT, c, texB);
         else if (n == "roughness") setFloatSlot(rec.roughness, hRo, c);
         else if (n == "eta") setFloatSlot(rec.eta, hE, c);
         else MaterialObj::addChild(c);
@@ -356,7 +547,7 @@ void EmitterObj::addChild(std::shared_ptr<GndObject> c) {
     if (c->getClassType() != ETexture) throw std::runtime_error("AreaLight: cannot add specified child!");
     if (c->getName() == "radiance") {
         if (hasRadiance) throw std::runtime_error("AreaLight: there's already a radiance value defined!");
-        setColorSlot(radiance, hasRadiance, c);
+        setColorSlot(radiance, hasRadiance, c, radianceTex);
     }
 }
 void EmitterObj::activate() {
@@ -809,7 +1000,9 @@ void Scene::build() {
         if (en.prim >= 0) {
             e.type = gnd::kEmitArea;
             e.instance = en.prim;
-            e.radiance = m_primitives[en.prim]->emitter->radiance;
+            const EmitterObj& o = *m_primitives[en.prim]->emitter;
+            e.radiance = o.radiance;
+            if (o.radianceTex && e.radiance.kind == gnd::kTexNode) e.radiance.node = (uint32_t)o.radianceTex->flatten(fs->textures);
             primEmitter[en.prim] = (int32_t)fs->emitters.size();
         } else {
             const EmitterObj& o = *en.emitter;
@@ -864,7 +1057,10 @@ void Scene::build() {
         auto mit = matIdx.find(mat);
         if (mit == matIdx.end()) {
             int k = (int)fs->materials.size();
-            fs->materials.push_back(mat->rec);
+            gnd::Material m = mat->rec;
+            if (mat->texA && m.a.kind == gnd::kTexNode) m.a.node = (uint32_t)mat->texA->flatten(fs->textures);
+            if (mat->texB && m.b.kind == gnd::kTexNode) m.b.node = (uint32_t)mat->texB->flatten(fs->textures);
+            fs->materials.push_back(m);
             mit = matIdx.emplace(mat, k).first;
         }
         is.material = mit->second;
@@ -949,6 +1145,10 @@ void FlatScene::fillDesc() {
     desc.env_strength = envStrength;
     desc.env_texels = envTexels.empty() ? nullptr : envTexels.data();
     desc.env_dist = envDist.empty() ? nullptr : envDist.data();
+    desc.tex_nodes = textures.nodes.empty() ? nullptr : textures.nodes.data();
+    desc.num_tex_nodes = (int32_t)textures.nodes.size();
+    desc.tex_texels = textures.texels.empty() ? nullptr : textures.texels.data();
+    desc.num_tex_texels = (int64_t)(textures.texels.size() / 4);
 }
 
 }  // namespace gndh

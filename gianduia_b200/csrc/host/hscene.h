@@ -150,13 +150,26 @@ private:
     Cls##_Factory global_##Cls##_Factory;                                                                \
     }
 
-// Color texture description (constant_color / checkerboard_color).
+// Texture trees of a scene as the device reads them: nodes, image texels (rgba) and the
+// node of each texture object already flattened.
+struct TexTables {
+    std::vector<gnd::TexNode> nodes;
+    std::vector<float> texels;
+    std::map<const void*, int32_t> done;
+};
+
+// Color texture description: constant_color / checkerboard_color live in the slot itself
+// (rec); the other textures set rec.kind = kTexNode and flatten into a node tree.
 struct ColorTexture : GndObject {
     gnd::ColorTex rec{};
     EClassType getClassType() const override { return ETexture; }
+    // Appends this texture's node (after its inputs') to t and returns its index.
+    int32_t flatten(TexTables& t) const;
+    virtual gnd::TexNode node(TexTables& t) const;   // constant / checker leaf from rec
 };
 struct FloatTexture : GndObject {
     float value = 1.f;
+    bool constant = true;      // false: a procedural or image float texture (not on the GPU path)
     EClassType getClassType() const override { return ETexture; }
 };
 
@@ -167,6 +180,7 @@ struct MediumObj : GndObject {
 
 struct MaterialObj : GndObject {
     gnd::Material rec{};
+    std::shared_ptr<ColorTexture> texA, texB;   // the texture objects of slots a and b
     std::shared_ptr<MediumObj> inside, outside;
     EClassType getClassType() const override { return EMaterial; }
     void addChild(std::shared_ptr<GndObject> c) override;
@@ -175,6 +189,7 @@ struct MaterialObj : GndObject {
 struct EmitterObj : GndObject {
     int32_t type = gnd::kEmitArea;
     gnd::ColorTex radiance{};      // area
+    std::shared_ptr<ColorTexture> radianceTex;
     bool hasRadiance = false;
     // point / spot / directional (pointlight.cpp, spotlight.cpp, directional.cpp)
     V3 position{}, direction{}, color{};
@@ -200,6 +215,12 @@ Transform motionMid(const gnd::InstMotion& k);
 // OpenEXR scanline image (NO, ZIPS or ZIP compression; HALF or FLOAT channels): the
 // R, G, B channels as rgb floats, row-major (himage.cpp).
 void readEXR(const std::string& path, int& width, int& height, std::vector<float>& rgb);
+// TextureCache::load (textureCache.h:23-95): an image texture's texels as rgba floats, row 0
+// the image's bottom row. OpenEXR through half precision (R, G, B; alpha 1); PNG (8 or
+// 16 bit, grey, grey + alpha, RGB, RGBA; 16-bit samples keep their high byte) divided by
+// 255, with the sRGB curve on every channel of 1-3 channel images and on RGB of RGBA ones.
+// `channels` is the file's channel count.
+void readTextureImage(const std::string& path, bool srgb, int& width, int& height, int& channels, std::vector<float>& rgba);
 
 // Mesh geometry in the reference's de-indexed form (one vertex per face corner).
 struct ShapeObj : GndObject {
@@ -296,6 +317,7 @@ struct FlatScene {
     std::vector<uint32_t> origToLeaf;
     std::vector<gnd::InstMotion> motion;   // per instance when any instance moves, else empty
     std::vector<float> envTexels, envDist;
+    TexTables textures;
     int envEmitter = -1, envWidth = 0, envHeight = 0;
     float envMarginalIntegral = 0.0f, envStrength = 1.0f;
     gnd::Camera camera{};

@@ -112,13 +112,44 @@ struct alignas(16) MeshRec {
 enum MatType : uint32_t {
     kMatMatte = 0, kMatPlastic = 1, kMatConductor = 2, kMatGlass = 3, kMatIndex = 4
 };
-// Color texture slot: constant (kind 0) or checkerboard (kind 1, checkerboard.h:36-48)
+// Color texture slot: constant (kind 0), checkerboard (kind 1, checkerboard.h:36-48) or
+// a texture tree (kind kTexNode): node `node` of SceneView::texNodes
+enum : uint32_t { kTexConstant = 0, kTexChecker = 1, kTexNode = 2 };
 struct alignas(16) ColorTex {
     float v1[3]; uint32_t kind;
-    float v2[3]; float pad;
+    float v2[3]; uint32_t node;
     float scale[2], delta[2];
 };
 static_assert(sizeof(ColorTex) == 48, "ColorTex must be 48 bytes");
+
+// Texture tree node: the procedural textures (textures/perlin.h, marble.h, wood.h,
+// cellular.h), image textures (imageTexture.cpp) and the domain warp (domainWarp.h), with
+// constant and checkerboard leaves where a warp's inputs are those.
+enum TexNodeKind : int32_t {
+    kTnConstant = 0, kTnChecker = 1, kTnPerlin = 2, kTnMarble = 3, kTnWood = 4, kTnCellular = 5, kTnImage = 6, kTnWarp = 7
+};
+enum : int32_t {
+    kTnCracks = 1,              // cellular: f2 - f1 instead of f1
+    kTnMetricShift = 1,         // cellular: bits 1-2 = 0 euclidean, 1 manhattan, 2 chebyshev
+    kTnLinear = 1,              // image: bilinear instead of closest texel
+    kTnClamp = 2                // image: clamp instead of repeat
+};
+// Nesting of warps in the `warp` input of a warp: at most this many levels.
+constexpr int kTexWarpNesting = 2;
+struct alignas(16) TexNode {
+    int32_t kind;               // TexNodeKind
+    int32_t octaves;            // perlin / marble / wood
+    float scale;                // perlin / marble / wood / cellular: p / scale
+    float strength;             // warp
+    float v1[3]; float veinFreq;
+    float v2[3]; float turbScale;
+    float axis[3];              // marble / wood (normalised)
+    int32_t flags;              // cellular / image flags above
+    int32_t a, b;               // warp: base node, warp node; image: first texel, channels
+    int32_t w, h;               // image size (texels are rgba floats, row 0 = bottom row)
+    float cscale[2], delta[2];  // checker
+};
+static_assert(sizeof(TexNode) == 96, "TexNode must be 96 bytes");
 
 struct alignas(16) Material {
     uint32_t type;
@@ -216,10 +247,12 @@ struct SceneView {
     const uint32_t* origToLeaf;
     const uint8_t* instClass;     // per instance: material type, kMatIndex for null-BSDF ones
     const InstMotion* motion;     // per instance, read for instances flagged kInstAnimated
+    const TexNode* texNodes;      // texture trees (ColorTex kind kTexNode)
+    const float* texels;          // image texture texels, 4 floats (rgba) each
     int32_t ext;                  // 1: emitters other than area lights, an environment map,
-                                  // animated instances, a thin-lens or moving camera (the
-                                  // kernels' EXT variants handle these)
-    int32_t pad;
+                                  // animated instances, a thin-lens or moving camera, texture
+                                  // trees (the kernels' EXT variants handle these)
+    int32_t numTexNodes;
     uint32_t tlasRoot;            // kEmpty when the scene has no primitives
     int32_t numEmitters;
     int32_t numInstances;

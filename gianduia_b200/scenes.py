@@ -449,11 +449,12 @@ def _texture(kind, name, props, children=()):
     return "\n".join(out)
 
 
-def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gpu"):
+def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gpu", emitter_texture=False):
     """The Cornell box with the reference's procedural and image textures on its walls and
     boxes: Perlin turbulence (floor), cellular cracks (back wall), an sRGB PNG with linear
     filtering (left wall), a float EXR with closest filtering and clamping (right wall),
-    a domain-warped checkerboard (ceiling), marble and wood (boxes). Returns the XML path."""
+    a domain-warped checkerboard (ceiling), marble and wood (boxes); emitter_texture: the
+    area light's radiance is a cellular texture. Returns the XML path."""
     os.makedirs(out_dir, exist_ok=True)
     write_plane_obj(os.path.join(out_dir, "plane.obj"))
     write_cube_obj(os.path.join(out_dir, "cube.obj"))
@@ -500,7 +501,10 @@ def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_
     xml += ["<primitive>",
             _transform([("scale", (0.5, 1, 0.4)), ("rotate", ((1, 0, 0), 180)), ("translate", (0, 0.998, 0))]),
             '<ref id="plane"/>', '<material type="matte">', _color("albedo", (0, 0, 0)), "</material>",
-            '<emitter type="area">', _color("radiance", (17, 12, 4)), "</emitter>", "</primitive>", "</scene>"]
+            '<emitter type="area">',
+            _texture("cellular_color", "radiance", {"value1": (30, 20, 8), "value2": (4, 3, 1), "scale": 0.2})
+            if emitter_texture else _color("radiance", (17, 12, 4)),
+            "</emitter>", "</primitive>", "</scene>"]
     path = os.path.join(out_dir, "textures.xml")
     with open(path, "w") as f:
         f.write("\n".join(xml) + "\n")

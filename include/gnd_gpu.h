@@ -118,6 +118,15 @@ typedef struct gnd_scene_desc {
      * bytes) when any instance has a toWorldEnd, else NULL; an instance moves when its
      * traversal record's kind has bit 31 set */
     const void* inst_motion;
+    /* textures other than constant and checkerboard (textures/perlin.h, marble.h, wood.h,
+     * cellular.h, domainWarp.h, imageTexture.cpp): a color slot of kind 2 evaluates node
+     * `node` of tex_nodes (96-byte gnd::TexNode records); image texels are rgba floats,
+     * num_tex_texels of them, row 0 the image's bottom row */
+    const void* tex_nodes;
+    int32_t num_tex_nodes;
+    int32_t pad3;
+    const float* tex_texels;
+    int64_t num_tex_texels;
 } gnd_scene_desc;
 
 /* ------------------------------------------------------------------ host framework */
