@@ -286,15 +286,22 @@ def device_bvh_leg(ctx, xml, host_sid, host_load_s, tune):
             ts.append(e0.elapsed_time(e1))
         out[name] = {"host_s": host_s, "upload_ms": up * 1e3, "build_ms": ctx.scene_info(s)["build_ms"],
                      "closest_mrays_s": n / statistics.median(ts) / 1e3}
+        if dev:
+            # refit of the same mesh to moved positions (device time of the refit kernels;
+            # the first refit also walks the tree once)
+            moved = tri.reshape(-1, 9) * np.float32(1.01) + np.float32(0.001)
+            first = ctx.refit_mesh(s, 0, moved)
+            out[name]["refit_ms"] = statistics.median([ctx.refit_mesh(s, 0, moved if k % 2 else tri) for k in range(4)])
+            out[name]["first_refit_ms"] = first
         ctx.free_scene(s)
         hs.close()
     del dr, dh
     torch.cuda.empty_cache()
     log("device trees: host load %.2fs (SAH %.2fs), upload %.1f ms with a %.1f ms build; render %.0f vs %.0f Mpaths/s "
-        "(%.1f vs %.1f nodes/ray); 2^20-triangle mesh built in %.1f ms, %.0f vs %.0f Mrays/s" % (
+        "(%.1f vs %.1f nodes/ray); 2^20-triangle mesh built in %.1f ms (refit %.2f ms), %.0f vs %.0f Mrays/s" % (
             out["host_load_s"], host_load_s, out["upload_ms"], out["build_ms"], out["device_tree_mpaths_s"],
             out["host_tree_mpaths_s"], out["device_tree_nodes_per_ray"], out["host_tree_nodes_per_ray"],
-            out["soup_device_tree"]["build_ms"], out["soup_device_tree"]["closest_mrays_s"],
+            out["soup_device_tree"]["build_ms"], out["soup_device_tree"]["refit_ms"], out["soup_device_tree"]["closest_mrays_s"],
             out["soup_host_tree"]["closest_mrays_s"]))
     return out
 

@@ -78,6 +78,7 @@ def lib():
                 "gnd_image_read_exr": [ctypes.c_char_p, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_int32)],
                 "gnd_gpu_scene_download": [_vp, ctypes.c_uint64, ctypes.c_int32, _vp, ctypes.c_int64],
+                "gnd_gpu_scene_refit_mesh": [_vp, ctypes.c_uint64, ctypes.c_int32, _vp, ctypes.c_int64, _vp],
                 "gnd_host_scene_desc": [_vp, ctypes.POINTER(_vp)],
                 "gnd_host_free": [_vp],
                 "gnd_gpu_create": [ctypes.c_int, ctypes.POINTER(_vp)],
@@ -339,6 +340,16 @@ class GpuContext:
         info = SceneInfo()
         _check(lib().gnd_gpu_scene_info(self._h, sid, ctypes.byref(info)), "gnd_gpu_scene_info")
         return {k: getattr(info, k) for k, _ in SceneInfo._fields_}
+
+    def refit_mesh(self, sid, mesh, positions):
+        """New object-space positions (triangles x 9 floats, the mesh's original triangle
+        order) for mesh `mesh`; its tree and the top-level tree are refitted on the GPU
+        (gnd_gpu_scene_refit_mesh). Returns the device time in ms."""
+        pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 9)
+        ms = ctypes.c_float()
+        _check(lib().gnd_gpu_scene_refit_mesh(self._h, sid, mesh, pos.ctypes.data, pos.shape[0], ctypes.byref(ms)),
+               "gnd_gpu_scene_refit_mesh")
+        return ms.value
 
     def download(self, sid, array):
         """One device array of an uploaded scene (gnd_gpu_scene_download): "nodes",

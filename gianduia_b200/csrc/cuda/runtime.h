@@ -137,8 +137,16 @@ struct Tune {
 };
 
 // A scene resident in HBM.
+// The nodes of one tree level by level, for refits (refit.cu): breadth-first node
+// indices, level l at [offsets[l], offsets[l + 1]).
+struct RefitTopo {
+    PoolBuf list;
+    std::vector<int64_t> offsets;
+};
+
 struct DeviceScene {
     std::vector<PoolBuf> bufs;  // the large arrays (pool memory, freed stream-ordered)
+    std::map<uint32_t, RefitTopo> refitTopo;   // per tree root, built by the first refit
     SceneView view{};
     DevBuf nullMask;          // per instance: 1 when the material has no BSDF (index)
     DevBuf instClass;         // per instance: material type (SceneView::instClass)

@@ -200,6 +200,19 @@ gnd_status gnd_gpu_scene_info(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_scene_in
 #define GND_ARRAY_INST_TRAV 4      /* InstTrav, 64 bytes, per instance */
 gnd_status gnd_gpu_scene_download(gnd_gpu_ctx* ctx, gnd_scene_id scene, int32_t array, void* dst, int64_t capacity);
 
+/* BVH refit for a deforming mesh (no counterpart in the reference, whose scenes are
+ * static after Scene::activate; it replaces rebuilding the tree with bvhBuilder.cpp:59-262
+ * for the same triangles): mesh `mesh` of an uploaded scene takes new object-space
+ * positions, num_tris x 9 floats in the mesh's original triangle order (num_tris must
+ * be the mesh's triangle count). Its tree keeps its topology and every box is recomputed
+ * on the GPU, then the instance bounds and the top-level tree; normals and uvs stay as
+ * loaded. Refused for scenes with moving instances and for meshes carrying an area
+ * light. The first refit of a scene walks its trees once (a few synchronous steps);
+ * device_ms (may be NULL) receives the device time of the refit kernels. Must not
+ * overlap a render of the same scene. */
+gnd_status gnd_gpu_scene_refit_mesh(gnd_gpu_ctx* ctx, gnd_scene_id scene, int32_t mesh, const float* positions,
+                                    int64_t num_tris, float* device_ms);
+
 /* Scene::rayIntersect(ray, isect) (scene.cpp:64-66, bvh.cpp:38-66) for n rays in HOST
  * memory: closest hit per ray, world tMax shrinking as hits are found. */
 gnd_status gnd_gpu_trace_closest(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_ray* rays, int64_t n,
