@@ -81,6 +81,10 @@ void validateTextures(const gnd_scene_desc* d) {
         if (t.kind == kTnImage && (t.w <= 0 || t.h <= 0 || t.a < 0 || (int64_t)t.a + (int64_t)t.w * t.h > d->num_tex_texels))
             throw Error(GND_ERR_INVALID, "image texels out of range");
         if (t.kind == kTnCellular && ((t.flags >> kTnMetricShift) & 3) > 2) throw Error(GND_ERR_INVALID, "unknown cellular metric");
+        // beyond ~128 octaves p * 2^i is infinite and every further octave adds NaN; the
+        // bound keeps a shading thread's work finite
+        if ((t.kind == kTnPerlin || t.kind == kTnMarble || t.kind == kTnWood) && t.octaves > kTexMaxOctaves)
+            throw Error(GND_ERR_INVALID, "texture octaves above " + std::to_string(kTexMaxOctaves));
     }
     for (int64_t i = 0; i < n; ++i)
         if (nodes[i].kind == kTnWarp && warpNesting(nodes, n, i, 0) > kTexWarpNesting)

@@ -136,6 +136,8 @@ enum : int32_t {
 };
 // Nesting of warps in the `warp` input of a warp: at most this many levels.
 constexpr int kTexWarpNesting = 2;
+// Octaves of Perlin turbulence a texture may ask for.
+constexpr int kTexMaxOctaves = 64;
 struct alignas(16) TexNode {
     int32_t kind;               // TexNodeKind
     int32_t octaves;            // perlin / marble / wood

@@ -61,3 +61,15 @@ def test_bad_texture_node_rejected(ctx, tmp_path):
     hs.desc.num_tex_nodes = 1
     with pytest.raises(G.GndError):
         ctx.upload(hs)
+
+
+def test_octaves_bounded(ctx, tmp_path):
+    """Perlin turbulence with more than 64 octaves is refused at upload (past ~128 octaves
+    every further one only adds NaN)."""
+    xml = scenes.textures(str(tmp_path), width=16, height=16, spp=1)
+    text = open(xml).read().replace('<integer name="octaves" value="5"/>', '<integer name="octaves" value="65"/>', 1)
+    with open(xml, "w") as f:
+        f.write(text)
+    hs = G.HostScene.load_xml(xml)
+    with pytest.raises(G.GndError, match="octaves"):
+        ctx.upload(hs)
