@@ -449,12 +449,15 @@ def _texture(kind, name, props, children=()):
     return "\n".join(out)
 
 
-def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gpu", emitter_texture=False):
+def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gpu", emitter_texture=False,
+             lens=None, moving=False, point_light=False):
     """The Cornell box with the reference's procedural and image textures on its walls and
     boxes: Perlin turbulence (floor), cellular cracks (back wall), an sRGB PNG with linear
     filtering (left wall), a float EXR with closest filtering and clamping (right wall),
     a domain-warped checkerboard (ceiling), marble and wood (boxes); emitter_texture: the
-    area light's radiance is a cellular texture. Returns the XML path."""
+    area light's radiance is a cellular texture; lens: thin-lens properties (see _camera);
+    moving: the marble box moves over the shutter; point_light: a point light inside the
+    box as well. Returns the XML path."""
     os.makedirs(out_dir, exist_ok=True)
     write_plane_obj(os.path.join(out_dir, "plane.obj"))
     write_cube_obj(os.path.join(out_dir, "cube.obj"))
@@ -481,7 +484,7 @@ def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_
         [("scale", (2, 1, 2)), ("rotate", ((0, 0, 1), -90)), ("translate", (-1, 0, 0))],
         [("scale", (2, 1, 2)), ("rotate", ((0, 0, 1), 90)), ("translate", (1, 0, 0))],
     ]
-    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height),
+    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height, lens=lens),
            '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
            '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
     for k, tr in enumerate(walls):
@@ -497,14 +500,18 @@ def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_
         shape = '<shape type="mesh" id="cube"><string name="filename" value="cube.obj"/></shape>' if k == 0 else '<ref id="cube"/>'
         mat = ('<material type="matte">' + t + "</material>") if k == 0 else \
             ('<material type="plastic">' + t + '<float name="eta" value="1.5"/><float name="roughness" value="0.3"/></material>')
-        xml += ["<primitive>", _transform(tr), shape, mat, "</primitive>"]
+        end = [_transform(tr + [("translate", (0.15, 0.1, 0.0))], name="toWorldEnd")] if moving and k == 0 else []
+        xml += ["<primitive>", _transform(tr)] + end + [shape, mat, "</primitive>"]
     xml += ["<primitive>",
             _transform([("scale", (0.5, 1, 0.4)), ("rotate", ((1, 0, 0), 180)), ("translate", (0, 0.998, 0))]),
             '<ref id="plane"/>', '<material type="matte">', _color("albedo", (0, 0, 0)), "</material>",
             '<emitter type="area">',
             _texture("cellular_color", "radiance", {"value1": (30, 20, 8), "value2": (4, 3, 1), "scale": 0.2})
             if emitter_texture else _color("radiance", (17, 12, 4)),
-            "</emitter>", "</primitive>", "</scene>"]
+            "</emitter>", "</primitive>"]
+    if point_light:
+        xml.append(_emitter("point", {"position": (0.3, 0.6, 0.5), "power": (6.0, 5.0, 4.0)}))
+    xml.append("</scene>")
     path = os.path.join(out_dir, "textures.xml")
     with open(path, "w") as f:
         f.write("\n".join(xml) + "\n")

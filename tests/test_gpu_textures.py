@@ -22,6 +22,10 @@ CASES = {
     "path": dict(),
     "volpath": dict(integrator="volpath_gpu"),
     "textured-light": dict(emitter_texture=True),
+    # every EXT feature at once: textures on moving geometry, seen through a thin lens,
+    # lit by a textured area light and a point light
+    "moving-lens-point": dict(emitter_texture=True, moving=True, point_light=True,
+                              lens={"lens_radius": 0.04, "focal_distance": 3.5}),
 }
 
 
