@@ -411,8 +411,10 @@ __device__ __forceinline__ void nodeKeysFast(const Node4* nd, const Trav& t, con
 }
 
 // Pops one entry: restores the world ray at a sentinel, tests an inner node and pushes its
-// hit children nearest-last, or makes a leaf pending. Returns an error bitmask.
-template <int BLOCK, bool COUNT, int SMEM>
+// hit children nearest-last, or makes a leaf pending. Returns an error bitmask. Without
+// ORDER (any-hit queries, whose answer does not depend on the visit order) the hit
+// children are visited in slot order, which saves the sort.
+template <int BLOCK, bool COUNT, int SMEM, bool ORDER = true>
 __device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<BLOCK, SMEM>& st, TraceCounters* cnt) {
     uint32_t e;
     if (t.next != kEmpty) {
@@ -442,6 +444,20 @@ __device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<
         const uint32_t ref[4] = {ch.x, ch.y, ch.z, ch.w};
         if (t.fast) nodeKeysFast(nd, t, ref, key);
         else nodeKeysExact(nd, t, ref, key);
+    }
+    if (!ORDER) {
+        const int nhit = (key[0] != kMissKey) + (key[1] != kMissKey) + (key[2] != kMissKey) + (key[3] != kMissKey);
+        if (nhit == 0) return 0;
+        if (t.sp + nhit - 1 > kPStackMax) return kTraceStackOverflow;
+        uint32_t pending = kEmpty;
+#pragma unroll
+        for (int i = 3; i >= 0; --i) {
+            if (key[i] == kMissKey) continue;
+            if (pending != kEmpty) st.put(t.sp++, pending);
+            pending = __ldg(nd->child + i);
+        }
+        t.next = pending;
+        return 0;
     }
     // ascending sort network on the packed keys (unsigned min / max)
 #define GND_CSWAP(a, b)                                     \
@@ -557,7 +573,11 @@ __device__ __forceinline__ uint32_t warpFetch(uint32_t* counter, bool want) {
 //   uint32_t count()                      number of rays
 //   bool load(uint32_t i, TRay&, const SceneView*&, const uint8_t*& nullMask)
 //   void store(uint32_t i, const THit&)   (closest) / store(i, bool) (any)
-template <int BLOCK, bool ANY, bool COUNT, int SMEM = kSmemStack, bool SPEC = false, bool MOTION = false, typename Src>
+// SLOT_ORDER_ANY: any-hit queries visit hit children in slot order instead of nearest
+// first (faster for the bounded shadow segments of the path tracer; rays to infinity find
+// an occluder sooner nearest first).
+template <int BLOCK, bool ANY, bool COUNT, int SMEM = kSmemStack, bool SPEC = false, bool MOTION = false,
+          bool SLOT_ORDER_ANY = false, typename Src>
 __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter, uint32_t* smemStack, TraceCounters* cnt) {
     TStack<BLOCK, SMEM> st;
     st.smem = smemStack + threadIdx.x;
@@ -606,7 +626,7 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
             }
             if (!__any_sync(0xffffffffu, want)) break;
             if (want) {
-                int e = travNodeStep<BLOCK, COUNT, SMEM>(t, *sv, st, cnt);
+                int e = travNodeStep<BLOCK, COUNT, SMEM, !(ANY && SLOT_ORDER_ANY)>(t, *sv, st, cnt);
                 if (e || ++iter > kMaxIterations) {
                     err |= e ? e : (int)kTraceIterLimit;
                     t.sp = 0; t.leaf = kEmpty; t.next = kEmpty;

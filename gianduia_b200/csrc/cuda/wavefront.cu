@@ -1098,7 +1098,7 @@ __global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p, bool mixed) 
     const uint32_t n = p.cnt[kQShadow];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
     ShadowSrc<ANY> src{&p, n, 0, nullptr, mixed};
-    int err = persistentTrace<kBlock, ANY, false, SMEM, SPEC, MOTION>(src, p.cnt + kQFetchB, stack, nullptr);
+    int err = persistentTrace<kBlock, ANY, false, SMEM, SPEC, MOTION, true>(src, p.cnt + kQFetchB, stack, nullptr);
     if (err) atomicOr(p.errWord, (uint32_t)err);
 }
 
