@@ -70,7 +70,12 @@ void validateTextures(const gnd_scene_desc* d) {
         if (t.kind == kTexNode && (int64_t)t.node >= n) throw Error(GND_ERR_INVALID, "texture node out of range");
     };
     const Material* mats = reinterpret_cast<const Material*>(d->materials);
-    for (int m = 0; m < d->num_materials; ++m) { slot(mats[m].a); slot(mats[m].b); }
+    for (int m = 0; m < d->num_materials; ++m) {
+        slot(mats[m].a);
+        slot(mats[m].b);
+        for (uint32_t r : {mats[m].roughTex, mats[m].etaTex, mats[m].kTex})
+            if ((int64_t)r > n) throw Error(GND_ERR_INVALID, "material texture node out of range");
+    }
     const Emitter* ems = reinterpret_cast<const Emitter*>(d->emitters);
     for (int k = 0; k < d->num_emitters; ++k) slot(ems[k].radiance);
     const TexNode* nodes = reinterpret_cast<const TexNode*>(d->tex_nodes);

@@ -449,9 +449,12 @@ __device__ __forceinline__ V3 lobeSample(const Lobe& l, V3 wo, V3& wi, V2 u, flo
 
 // Material -> lobe at a shading point (matte.cpp:46-53, plastic.cpp:74-91,
 // conductor.cpp:101-120, glass.cpp:98-115). Returns false for the index material.
-// `tex` evaluates a color slot at the point.
+// `tex` evaluates a color slot at the point; with TexF::kTrees it also evaluates the
+// roughness / eta / k trees (tex.node(root)), else those fields are the constants.
 template <uint32_t M, class TexF>
-__device__ __forceinline__ bool makeLobeT(const Material& m, TexF tex, Lobe& l) {
+__device__ __forceinline__ bool makeLobeT(const Material& m, const TexF& tex, Lobe& l) {
+    float rough = m.roughness;
+    if (TexF::kTrees && m.roughTex) rough = tex.node(m.roughTex - 1).x;
     switch (m.type) {
         case kMatMatte:
             if (!(M & kLobesMatte)) return false;
@@ -462,34 +465,40 @@ __device__ __forceinline__ bool makeLobeT(const Material& m, TexF tex, Lobe& l) 
             if (!(M & kLobesPlastic)) return false;
             l.a = tex(m.a);
             l.b = tex(m.b);
-            l.eta = m.eta;
-            if (m.roughness == 0.0f) l.kind = 5;
-            else { l.kind = 6; l.ggx = makeGgx(roughnessToAlpha(m.roughness)); }
+            l.eta = (TexF::kTrees && m.etaTex) ? tex.node(m.etaTex - 1).x : m.eta;
+            if (rough == 0.0f) l.kind = 5;
+            else { l.kind = 6; l.ggx = makeGgx(roughnessToAlpha(rough)); }
             return true;
         case kMatConductor:
             if (!(M & kLobesConductor)) return false;
             l.a = tex(m.a);
-            l.ceta = v3(m.condEta[0], m.condEta[1], m.condEta[2]);
-            l.ck = v3(m.condK[0], m.condK[1], m.condK[2]);
-            if (m.roughness == 0.0f) l.kind = 1;
-            else { l.kind = 3; l.ggx = makeGgx(roughnessToAlpha(m.roughness)); }
+            l.ceta = (TexF::kTrees && m.etaTex) ? tex.node(m.etaTex - 1) : v3(m.condEta[0], m.condEta[1], m.condEta[2]);
+            l.ck = (TexF::kTrees && m.kTex) ? tex.node(m.kTex - 1) : v3(m.condK[0], m.condK[1], m.condK[2]);
+            if (rough == 0.0f) l.kind = 1;
+            else { l.kind = 3; l.ggx = makeGgx(roughnessToAlpha(rough)); }
             return true;
         case kMatGlass:
             if (!(M & kLobesGlass)) return false;
             l.a = tex(m.a);
             l.b = tex(m.b);
-            l.eta = m.eta;
-            if (m.roughness == 0.0f) l.kind = 2;
-            else { l.kind = 4; l.ggx = makeGgx(roughnessToAlpha(m.roughness)); }
+            l.eta = (TexF::kTrees && m.etaTex) ? tex.node(m.etaTex - 1).x : m.eta;
+            if (rough == 0.0f) l.kind = 2;
+            else { l.kind = 4; l.ggx = makeGgx(roughnessToAlpha(rough)); }
             return true;
         default:
             return false;
     }
 }
-
+// Color slots by uv only (constant and checkerboard), constant roughness / eta / k.
+struct SlotTexUV {
+    static constexpr bool kTrees = false;
+    V2 uv;
+    __device__ __forceinline__ V3 operator()(const ColorTex& t) const { return evalTex(t, uv); }
+    __device__ __forceinline__ V3 node(uint32_t) const { return v3s(0.0f); }
+};
 template <uint32_t M = kLobesAll>
 __device__ __forceinline__ bool makeLobe(const Material& m, V2 uv, Lobe& l) {
-    return makeLobeT<M>(m, [uv](const ColorTex& t) { return evalTex(t, uv); }, l);
+    return makeLobeT<M>(m, SlotTexUV{uv}, l);
 }
 
 // BSDF with one lobe of weight 1 (bsdf.cpp:6-136): world-space evaluation.

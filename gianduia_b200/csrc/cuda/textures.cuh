@@ -90,8 +90,18 @@ __device__ __forceinline__ void worleyNoise(V3 p, int metric, float& f1, float& 
             }
 }
 
-// value1 * (1 - t) + value2 * t
+// std::lerp(a, b, t) as P0811R3 specifies it: exact at t = 0 and t = 1, monotonic,
+// a + t (b - a) unless a and b straddle zero
+__device__ __forceinline__ float stdLerp(float a, float b, float t) {
+    if ((a <= 0.0f && b >= 0.0f) || (a >= 0.0f && b <= 0.0f)) return t * b + (1.0f - t) * a;
+    if (t == 1.0f) return b;
+    const float x = a + t * (b - a);
+    return (t > 1.0f) == (b > a) ? (b < x ? x : b) : (b > x ? x : b);
+}
+// value1 * (1 - t) + value2 * t for color textures; the float perlin / marble / wood
+// textures blend with std::lerp (perlin.h:33, marble.h:42, wood.h:42)
 __device__ __forceinline__ V3 texMix(const TexNode& t, float x) {
+    if (t.flags & kTnFloatLerp) return v3s(stdLerp(t.v1[0], t.v2[0], x));
     return v3(t.v1[0], t.v1[1], t.v1[2]) * (1.0f - x) + v3(t.v2[0], t.v2[1], t.v2[2]) * x;
 }
 

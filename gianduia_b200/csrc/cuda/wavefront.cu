@@ -309,6 +309,15 @@ __device__ __forceinline__ V3 evalColor(const SceneView& s, const ColorTex& t, V
     if (EXT && t.kind == kTexNode) return evalTexTree(s, t.node, p, n, dpdu, uv);
     return evalTex(t, uv);
 }
+// Material slots at a surface point; EXT: with texture trees.
+template <bool EXT>
+struct SlotTexAt {
+    static constexpr bool kTrees = EXT;
+    const SceneView& s;
+    const SurfInt& si;
+    __device__ __forceinline__ V3 operator()(const ColorTex& t) const { return evalColor<EXT>(s, t, si.p, si.n, si.dpdu, si.uv); }
+    __device__ __forceinline__ V3 node(uint32_t root) const { return evalTexTree(s, root, si.p, si.n, si.dpdu, si.uv); }
+};
 template <bool EXT>
 __device__ __forceinline__ V3 emitterEvalAt(const SceneView& s, const Emitter& e, V3 p, V3 n, V3 dpdu, V2 uv, V3 w) {
     if (dot(n, w) > 0.0f) return evalColor<EXT>(s, e.radiance, p, n, dpdu, uv);
@@ -928,8 +937,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
             const InstShade& is = s.instS[h.inst];
             const Material mat = s.materials[is.material];
             Bsdf bsdf;
-            const bool hasBsdf = makeLobeT<M>(mat, [&](const ColorTex& t) { return evalColor<EXT>(s, t, si.p, si.n, si.dpdu, si.uv); },
-                                              bsdf.lobe);
+            const bool hasBsdf = makeLobeT<M>(mat, SlotTexAt<EXT>{s, si}, bsdf.lobe);
             if (is.emitter >= 0) {
                 bool skip = (bounces == 0 && !hasBsdf);
                 if (!skip) {

@@ -182,12 +182,17 @@ struct ConstantColor : ColorTexture {
     explicit ConstantColor(const PropertyList& p) { rec = constColor(p.getColor("value", gnd::v3s(1.f))); }
 };
 struct ConstantFloat : FloatTexture {
-    explicit ConstantFloat(const PropertyList& p) { value = p.getFloat("value", 1.0f); }
+    explicit ConstantFloat(const PropertyList& p) {
+        value = p.getFloat("value", 1.0f);
+        tree = std::make_shared<ColorTexture>();
+        tree->rec = constColor(gnd::v3s(value));
+    }
 };
 // checkerboard.h:20-48
 struct CheckerboardColor : ColorTexture {
-    explicit CheckerboardColor(const PropertyList& p) {
-        V3 a = p.getColor("value1", gnd::v3s(1.f)), b = p.getColor("value2", gnd::v3s(0.f));
+    explicit CheckerboardColor(const PropertyList& p, bool flt = false) {
+        V3 a = flt ? gnd::v3s(p.getFloat("value1", 1.0f)) : p.getColor("value1", gnd::v3s(1.f));
+        V3 b = flt ? gnd::v3s(p.getFloat("value2", 0.0f)) : p.getColor("value2", gnd::v3s(0.f));
         V2 sc = p.getVector2("scale", V2{1.f, 1.f}), de = p.getPoint2("delta", V2{0.f, 0.f});
         rec.kind = 1;
         rec.v1[0] = a.x; rec.v1[1] = a.y; rec.v1[2] = a.z;
@@ -224,15 +229,17 @@ struct ProceduralColor : ColorTexture {
     V3 v1{}, v2{};
     float scale = 1.0f;
     int octaves = 6;
-    ProceduralColor(const PropertyList& p, V3 d1, V3 d2) {
+    bool flt = false;   // float texture: value1 / value2 are floats (default 0 and 1)
+    ProceduralColor(const PropertyList& p, V3 d1, V3 d2, bool isFloat) : flt(isFloat) {
         rec.kind = gnd::kTexNode;
-        v1 = p.getColor("value1", d1);
-        v2 = p.getColor("value2", d2);
+        v1 = flt ? gnd::v3s(p.getFloat("value1", 0.0f)) : p.getColor("value1", d1);
+        v2 = flt ? gnd::v3s(p.getFloat("value2", 1.0f)) : p.getColor("value2", d2);
         scale = p.getFloat("scale", 1.0f);
     }
     gnd::TexNode base(int32_t kind) const {
         gnd::TexNode n{};
         n.kind = kind;
+        if (flt) n.flags = gnd::kTnFloatLerp;
         n.v1[0] = v1.x; n.v1[1] = v1.y; n.v1[2] = v1.z;
         n.v2[0] = v2.x; n.v2[1] = v2.y; n.v2[2] = v2.z;
         n.scale = scale;
@@ -242,7 +249,7 @@ struct ProceduralColor : ColorTexture {
 };
 // perlin.h (texture):15-37: value1 .. value2 by turbulence(p / scale)
 struct PerlinColor : ProceduralColor {
-    explicit PerlinColor(const PropertyList& p) : ProceduralColor(p, gnd::v3s(0.0f), gnd::v3s(1.0f)) {
+    explicit PerlinColor(const PropertyList& p, bool flt = false) : ProceduralColor(p, gnd::v3s(0.0f), gnd::v3s(1.0f), flt) {
         octaves = p.getInteger("octaves", 6);
     }
     gnd::TexNode node(TexTables&) const override { return base(gnd::kTnPerlin); }
@@ -252,7 +259,8 @@ struct VeinColor : ProceduralColor {
     int32_t kind;
     float veinFreq, turbScale;
     V3 axis;
-    VeinColor(const PropertyList& p, int32_t k, V3 d1, V3 d2, float turbDefault) : ProceduralColor(p, d1, d2), kind(k) {
+    VeinColor(const PropertyList& p, int32_t k, V3 d1, V3 d2, float turbDefault, bool flt)
+        : ProceduralColor(p, d1, d2, flt), kind(k) {
         octaves = p.getInteger("octaves", 6);
         veinFreq = p.getFloat("vein_freq", 10.0f);
         turbScale = p.getFloat("turb_scale", turbDefault);
@@ -267,16 +275,17 @@ struct VeinColor : ProceduralColor {
     }
 };
 struct MarbleColor : VeinColor {
-    explicit MarbleColor(const PropertyList& p) : VeinColor(p, gnd::kTnMarble, gnd::v3s(0.1f), gnd::v3s(0.9f), 5.0f) {}
+    explicit MarbleColor(const PropertyList& p, bool flt = false)
+        : VeinColor(p, gnd::kTnMarble, gnd::v3s(0.1f), gnd::v3s(0.9f), 5.0f, flt) {}
 };
 struct WoodColor : VeinColor {
-    explicit WoodColor(const PropertyList& p)
-        : VeinColor(p, gnd::kTnWood, gnd::v3(0.6f, 0.4f, 0.2f), gnd::v3(0.3f, 0.15f, 0.05f), 2.0f) {}
+    explicit WoodColor(const PropertyList& p, bool flt = false)
+        : VeinColor(p, gnd::kTnWood, gnd::v3(0.6f, 0.4f, 0.2f), gnd::v3(0.3f, 0.15f, 0.05f), 2.0f, flt) {}
 };
 // cellular.h:17-58: Worley F1 (distance) or F2 - F1 (cracks), unknown names fall back
 struct CellularColor : ProceduralColor {
     int32_t flags = 0;
-    explicit CellularColor(const PropertyList& p) : ProceduralColor(p, gnd::v3s(0.0f), gnd::v3s(1.0f)) {
+    explicit CellularColor(const PropertyList& p, bool flt = false) : ProceduralColor(p, gnd::v3s(0.0f), gnd::v3s(1.0f), flt) {
         if (p.getString("mode", "distance") == "cracks") flags |= gnd::kTnCracks;
         const std::string m = p.getString("metric", "euclidean");
         const int metric = m == "manhattan" ? 1 : (m == "chebyshev" ? 2 : 0);
@@ -284,7 +293,7 @@ struct CellularColor : ProceduralColor {
     }
     gnd::TexNode node(TexTables&) const override {
         gnd::TexNode n = base(gnd::kTnCellular);
-        n.flags = flags;
+        n.flags = flags;   // Lerp (constants.h:41-44) for both flavours, never std::lerp
         return n;
     }
 };
@@ -292,12 +301,20 @@ struct CellularColor : ProceduralColor {
 struct DomainWarpColor : ColorTexture {
     float strength;
     std::shared_ptr<ColorTexture> baseTex, warpTex;
-    explicit DomainWarpColor(const PropertyList& p) : strength(p.getFloat("strength", 1.0f)) { rec.kind = gnd::kTexNode; }
+    bool flt = false;
+    explicit DomainWarpColor(const PropertyList& p, bool isFloat = false) : strength(p.getFloat("strength", 1.0f)), flt(isFloat) {
+        rec.kind = gnd::kTexNode;
+    }
     void addChild(std::shared_ptr<GndObject> c) override {
         if (c->getClassType() != ETexture) throw std::runtime_error("WarpTexture: cannot add specified child!");
         auto t = std::dynamic_pointer_cast<ColorTexture>(c);
         if (c->getName() == "base") {
             if (baseTex) throw std::runtime_error("WarpTexture: base texture already defined!");
+            if (flt) {
+                auto f = std::dynamic_pointer_cast<FloatTexture>(c);
+                if (!f) throw std::runtime_error("WarpTexture: the base of a float warp must be a float texture");
+                t = f->tree;
+            }
             if (!t) throw std::runtime_error("WarpTexture: the base of a color warp must be a color texture");
             baseTex = t;
         } else if (c->getName() == "warp") {
@@ -325,7 +342,9 @@ struct ImageColor : ColorTexture {
     bool linear = false, clamp = false, srgb = false;
     int width = 0, height = 0, channels = 0;
     std::vector<float> texels;
-    explicit ImageColor(const PropertyList& p) : filename(p.getString("filename")) {
+    // float image textures read the first channel (imageTexture.cpp:93-95), which is the
+    // first texel channel here as well
+    explicit ImageColor(const PropertyList& p, bool = false) : filename(p.getString("filename")) {
         rec.kind = gnd::kTexNode;
         const std::string interp = p.getString("interpolation_mode", "closest");
         if (interp == "linear") linear = true;
@@ -366,11 +385,24 @@ struct ImageColor : ColorTexture {
         return n;
     }
 };
-// The float variants of the procedural and image textures load, but only constant float
-// textures fill a slot of the GPU path (roughness, eta).
-struct NonConstantFloat : FloatTexture {
-    explicit NonConstantFloat(const PropertyList&) { constant = false; }
+// The float variants: the color texture classes built with float values, as a tree.
+template <class C>
+struct TreeFloat : FloatTexture {
+    explicit TreeFloat(const PropertyList& p) {
+        constant = false;
+        tree = std::make_shared<C>(p, true);
+    }
+    void addChild(std::shared_ptr<GndObject> c) override { tree->addChild(c); }
+    void activate() override { tree->activate(); }
+    void setBaseDir(const std::string& d) override { tree->setBaseDir(d); }
 };
+using CheckerboardFloat = TreeFloat<CheckerboardColor>;
+using PerlinFloat = TreeFloat<PerlinColor>;
+using MarbleFloat = TreeFloat<MarbleColor>;
+using WoodFloat = TreeFloat<WoodColor>;
+using CellularFloat = TreeFloat<CellularColor>;
+using DomainWarpFloat = TreeFloat<DomainWarpColor>;
+using ImageFloat = TreeFloat<ImageColor>;
 }  // namespace
 GND_REGISTER_CLASS(PerlinColor, "perlin_color")
 GND_REGISTER_CLASS(MarbleColor, "marble_color")
@@ -378,17 +410,13 @@ GND_REGISTER_CLASS(WoodColor, "wood_color")
 GND_REGISTER_CLASS(CellularColor, "cellular_color")
 GND_REGISTER_CLASS(DomainWarpColor, "domainWarp_color")
 GND_REGISTER_CLASS(ImageColor, "image_color")
-namespace {
-struct NonConstantFloatNames {
-    NonConstantFloatNames() {
-        for (const char* n : {"checkerboard_float", "perlin_float", "marble_float", "wood_float", "cellular_float",
-                              "domainWarp_float", "image_float"})
-            GndFactory::getInstance()->registerClass(n, [](const PropertyList& p) -> std::unique_ptr<GndObject> {
-                return std::make_unique<NonConstantFloat>(p);
-            });
-    }
-} nonConstantFloatNames;
-}  // namespace
+GND_REGISTER_CLASS(CheckerboardFloat, "checkerboard_float")
+GND_REGISTER_CLASS(PerlinFloat, "perlin_float")
+GND_REGISTER_CLASS(MarbleFloat, "marble_float")
+GND_REGISTER_CLASS(WoodFloat, "wood_float")
+GND_REGISTER_CLASS(CellularFloat, "cellular_float")
+GND_REGISTER_CLASS(DomainWarpFloat, "domainWarp_float")
+GND_REGISTER_CLASS(ImageFloat, "image_float")
 
 // ---------------------------------------------------------------- media
 // homogeneous.cpp:14-20
@@ -426,9 +454,14 @@ void setColorSlot(gnd::ColorTex& slot, bool& have, const std::shared_ptr<GndObje
     keep = t;
     have = true;
 }
-void setFloatSlot(float& slot, bool& have, const std::shared_ptr<GndObject>& c) {
+void setFloatSlot(float& slot, bool& have, const std::shared_ptr<GndObject>& c, std::shared_ptr<ColorTexture>& keep) {
     auto t = std::dynamic_pointer_cast<FloatTexture>(c);
-    if (!t || !t->constant) throw std::runtime_error("Material: texture '" + c->getName() + "' must be a constant float texture");
+    if (!t) throw std::runtime_error("Material: texture '" + c->getName() + "' must be a float texture");
+    if (!t->constant) {
+        keep = t->tree;
+        have = true;
+        return;
+    }
     slot = t->value;
     have = true;
 }
@@ -465,8 +498,8 @@ struct PlasticMat : MaterialObj {
         const std::string& n = c->getName();
         if (n == "Kd") setColorSlot(rec.a, hKd, c, texA);
         else if (n == "Ks") setColorSlot(rec.b, hKs, c, texB);
-        else if (n == "roughness") setFloatSlot(rec.roughness, hR, c);
-        else if (n == "eta") setFloatSlot(rec.eta, hE, c);
+        else if (n == "roughness") setFloatSlot(rec.roughness, hR, c, roughTex);
+        else if (n == "eta") setFloatSlot(rec.eta, hE, c, etaTex);
         else MaterialObj::addChild(c);
     }
     void activate() override {
@@ -491,12 +524,17 @@ struct ConductorMat : MaterialObj {
         if (c->getClassType() != ETexture) throw std::runtime_error("Conductor: cannot add specified child!");
         const std::string& n = c->getName();
         if (n == "R") setColorSlot(rec.a, hR, c, texA);
-        else if (n == "roughness") setFloatSlot(rec.roughness, hRo, c);
+        else if (n == "roughness") setFloatSlot(rec.roughness, hRo, c, roughTex);
         else if (n == "eta" || n == "k") {
             auto t = std::dynamic_pointer_cast<ColorTexture>(c);
-            if (!t || t->rec.kind != 0) throw std::runtime_error("Conductor: eta/k must be constant colors");
-            V3 v = gnd::v3(t->rec.v1[0], t->rec.v1[1], t->rec.v1[2]);
-            if (n == "eta") { eta = v; hE = true; } else { k = v; hK = true; }
+            if (!t) throw std::runtime_error("Conductor: eta/k must be color textures");
+            bool& have = n == "eta" ? hE : hK;
+            if (t->rec.kind == gnd::kTexConstant) {
+                (n == "eta" ? eta : k) = gnd::v3(t->rec.v1[0], t->rec.v1[1], t->rec.v1[2]);
+            } else {
+                (n == "eta" ? etaTex : kTex) = t;   // evaluated per shading point
+            }
+            have = true;
         } else MaterialObj::addChild(c);
     }
     void activate() override {
@@ -520,8 +558,8 @@ struct GlassMat : MaterialObj {
         const std::string& n = c->getName();
         if (n == "R") setColorSlot(rec.a, hR, c, texA);
         else if (n == "T") setColorSlot(rec.b, hT, c, texB);
-        else if (n == "roughness") setFloatSlot(rec.roughness, hRo, c);
-        else if (n == "eta") setFloatSlot(rec.eta, hE, c);
+        else if (n == "roughness") setFloatSlot(rec.roughness, hRo, c, roughTex);
+        else if (n == "eta") setFloatSlot(rec.eta, hE, c, etaTex);
         else MaterialObj::addChild(c);
     }
     void activate() override {
@@ -1060,6 +1098,9 @@ void Scene::build() {
             gnd::Material m = mat->rec;
             if (mat->texA && m.a.kind == gnd::kTexNode) m.a.node = (uint32_t)mat->texA->flatten(fs->textures);
             if (mat->texB && m.b.kind == gnd::kTexNode) m.b.node = (uint32_t)mat->texB->flatten(fs->textures);
+            m.roughTex = mat->roughTex ? 1u + (uint32_t)mat->roughTex->flatten(fs->textures) : 0u;
+            m.etaTex = mat->etaTex ? 1u + (uint32_t)mat->etaTex->flatten(fs->textures) : 0u;
+            m.kTex = mat->kTex ? 1u + (uint32_t)mat->kTex->flatten(fs->textures) : 0u;
             fs->materials.push_back(m);
             mit = matIdx.emplace(mat, k).first;
         }

@@ -167,9 +167,13 @@ struct ColorTexture : GndObject {
     int32_t flatten(TexTables& t) const;
     virtual gnd::TexNode node(TexTables& t) const;   // constant / checker leaf from rec
 };
+// Float texture: a constant, or (constant false) a texture tree whose nodes carry the
+// value in every channel. `tree` is set for both, so a float texture can also be a node
+// of another tree (the base of a float domain warp).
 struct FloatTexture : GndObject {
     float value = 1.f;
-    bool constant = true;      // false: a procedural or image float texture (not on the GPU path)
+    bool constant = true;
+    std::shared_ptr<ColorTexture> tree;
     EClassType getClassType() const override { return ETexture; }
 };
 
@@ -181,6 +185,7 @@ struct MediumObj : GndObject {
 struct MaterialObj : GndObject {
     gnd::Material rec{};
     std::shared_ptr<ColorTexture> texA, texB;   // the texture objects of slots a and b
+    std::shared_ptr<ColorTexture> roughTex, etaTex, kTex;   // non-constant roughness / eta / k
     std::shared_ptr<MediumObj> inside, outside;
     EClassType getClassType() const override { return EMaterial; }
     void addChild(std::shared_ptr<GndObject> c) override;

@@ -132,7 +132,8 @@ enum : int32_t {
     kTnCracks = 1,              // cellular: f2 - f1 instead of f1
     kTnMetricShift = 1,         // cellular: bits 1-2 = 0 euclidean, 1 manhattan, 2 chebyshev
     kTnLinear = 1,              // image: bilinear instead of closest texel
-    kTnClamp = 2                // image: clamp instead of repeat
+    kTnClamp = 2,               // image: clamp instead of repeat
+    kTnFloatLerp = 8            // perlin / marble / wood float textures: std::lerp blend
 };
 // Nesting of warps in the `warp` input of a warp: at most this many levels.
 constexpr int kTexWarpNesting = 2;
@@ -153,15 +154,17 @@ struct alignas(16) TexNode {
 };
 static_assert(sizeof(TexNode) == 96, "TexNode must be 96 bytes");
 
+// roughTex / etaTex / kTex: 0 for the constant fields, else 1 + the root node of a texture
+// tree evaluated per shading point (float trees give their value in every channel).
 struct alignas(16) Material {
     uint32_t type;
     float roughness;          // plastic/conductor/glass
     float eta;                // plastic/glass
-    float pad0;
+    uint32_t roughTex;        // roughness tree (plastic/conductor/glass)
     ColorTex a;               // matte albedo | plastic Kd | conductor R | glass R
     ColorTex b;               // plastic Ks | glass T
-    float condEta[3]; float pad1;
-    float condK[3]; float pad2;
+    float condEta[3]; uint32_t etaTex;   // eta tree: float (plastic/glass) or color (conductor)
+    float condK[3]; uint32_t kTex;       // conductor k tree
 };
 
 // ---------------------------------------------------------------- emitters, media

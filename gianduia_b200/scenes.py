@@ -450,14 +450,16 @@ def _texture(kind, name, props, children=()):
 
 
 def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gpu", emitter_texture=False,
-             lens=None, moving=False, point_light=False):
+             lens=None, moving=False, point_light=False, float_textures=False):
     """The Cornell box with the reference's procedural and image textures on its walls and
     boxes: Perlin turbulence (floor), cellular cracks (back wall), an sRGB PNG with linear
     filtering (left wall), a float EXR with closest filtering and clamping (right wall),
     a domain-warped checkerboard (ceiling), marble and wood (boxes); emitter_texture: the
     area light's radiance is a cellular texture; lens: thin-lens properties (see _camera);
     moving: the marble box moves over the shutter; point_light: a point light inside the
-    box as well. Returns the XML path."""
+    box as well; float_textures: the left wall is a rough conductor (image R, cellular eta,
+    wood_float roughness) and the wood box's plastic takes perlin_float roughness and
+    checkerboard_float eta. Returns the XML path."""
     os.makedirs(out_dir, exist_ok=True)
     write_plane_obj(os.path.join(out_dir, "plane.obj"))
     write_cube_obj(os.path.join(out_dir, "cube.obj"))
@@ -489,7 +491,15 @@ def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_
            '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
     for k, tr in enumerate(walls):
         shape = '<shape type="mesh" id="plane"><string name="filename" value="plane.obj"/></shape>' if k == 0 else '<ref id="plane"/>'
-        xml += ["<primitive>", _transform(tr), shape, '<material type="matte">', tex[k], "</material>", "</primitive>"]
+        if float_textures and k == 3:
+            mat = ['<material type="conductor">', tex[k].replace('name="albedo"', 'name="R"', 1),
+                   _texture("cellular_color", "eta", {"value1": (0.2, 0.4, 1.4), "value2": (1.5, 0.9, 0.3), "scale": 0.3}),
+                   _color("k", (3.0, 2.5, 2.2)),
+                   _texture("wood_float", "roughness", {"value1": 0.05, "value2": 0.4, "scale": 0.5, "octaves": 2}),
+                   "</material>"]
+        else:
+            mat = ['<material type="matte">', tex[k], "</material>"]
+        xml += ["<primitive>", _transform(tr), shape] + mat + ["</primitive>"]
     boxes = [
         ([("scale", (0.6, 0.6, 0.6)), ("rotate", ((0, 1, 0), 18)), ("translate", (0.35, -0.7, 0.3))],
          _texture("marble_color", "albedo", {"scale": 0.3, "octaves": 4, "vein_freq": 8.0, "turb_scale": 3.0})),
@@ -499,7 +509,10 @@ def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_
     for k, (tr, t) in enumerate(boxes):
         shape = '<shape type="mesh" id="cube"><string name="filename" value="cube.obj"/></shape>' if k == 0 else '<ref id="cube"/>'
         mat = ('<material type="matte">' + t + "</material>") if k == 0 else \
-            ('<material type="plastic">' + t + '<float name="eta" value="1.5"/><float name="roughness" value="0.3"/></material>')
+            ('<material type="plastic">' + t + (
+                _texture("perlin_float", "roughness", {"value1": 0.05, "value2": 0.5, "scale": 0.4, "octaves": 3}) +
+                _texture("checkerboard_float", "eta", {"value1": 1.3, "value2": 1.7, "scale": (0.2, 0.2)})
+                if float_textures else '<float name="eta" value="1.5"/><float name="roughness" value="0.3"/>') + '</material>')
         end = [_transform(tr + [("translate", (0.15, 0.1, 0.0))], name="toWorldEnd")] if moving and k == 0 else []
         xml += ["<primitive>", _transform(tr)] + end + [shape, mat, "</primitive>"]
     xml += ["<primitive>",

@@ -26,6 +26,9 @@ CASES = {
     # lit by a textured area light and a point light
     "moving-lens-point": dict(emitter_texture=True, moving=True, point_light=True,
                               lens={"lens_radius": 0.04, "focal_distance": 3.5}),
+    # roughness / eta / conductor eta as texture trees
+    "float-textures": dict(float_textures=True),
+    "float-textures-volpath": dict(float_textures=True, integrator="volpath_gpu"),
 }
 
 

@@ -128,14 +128,28 @@ def test_texture_errors(tmp_path, body, msg):
         G.HostScene.load_xml(quad_scene(tmp_path, body))
 
 
-def test_nonconstant_float_texture_refused(tmp_path):
+def test_float_texture_slots(tmp_path):
+    """Float textures in roughness / eta slots become trees (Material.roughTex / etaTex =
+    1 + root node); the float perlin blends with std::lerp (flag 8), the float cellular
+    with Lerp; a constant float stays in the record."""
     d = str(tmp_path)
     scenes.write_plane_obj(os.path.join(d, "plane.obj"))
-    xml = "\n".join(["<scene>", scenes._camera((0, 0, 3), (0, 0, 0), 40, 8, 8), '<sampler type="independent"/>', '<integrator type="path_gpu"/>',
+    xml = "\n".join(["<scene>", scenes._camera((0, 0, 3), (0, 0, 0), 40, 8, 8), '<sampler type="independent"/>',
+                     '<integrator type="path_gpu"/>', "<primitive>",
+                     '<shape type="mesh"><string name="filename" value="plane.obj"/></shape>',
+                     '<material type="plastic">', scenes._texture("perlin_float", "roughness", {"value1": 0.1}),
+                     scenes._texture("cellular_float", "eta", {"value2": 1.8}), "</material>", "</primitive>",
                      "<primitive>", '<shape type="mesh"><string name="filename" value="plane.obj"/></shape>',
-                     '<material type="plastic">', scenes._texture("perlin_float", "roughness", {}), "</material>",
-                     "</primitive>", "</scene>"])
+                     '<material type="glass">', scenes._texture("constant_float", "roughness", {"value": 0.25}),
+                     "</material>", "</primitive>", "</scene>"])
     with open(os.path.join(d, "s.xml"), "w") as f:
         f.write(xml)
-    with pytest.raises(G.GndError, match="constant float"):
-        G.HostScene.load_xml(os.path.join(d, "s.xml"))
+    hs = G.HostScene.load_xml(os.path.join(d, "s.xml"))
+    nodes, _ = tables(hs)
+    mats = np.frombuffer(ctypes.string_at(hs.desc.materials, 144 * hs.desc.num_materials), "<u4").reshape(-1, 36)
+    plastic = mats[mats[:, 0] == 1][0]
+    glass = mats[mats[:, 0] == 3][0]
+    rough, eta = nodes[plastic[3] - 1], nodes[plastic[31] - 1]
+    assert rough["kind"] == 2 and rough["flags"] == 8 and rough["v1"][0] == np.float32(0.1) and rough["v2"][0] == 1.0
+    assert eta["kind"] == 5 and eta["flags"] == 0 and eta["v2"][2] == np.float32(1.8)
+    assert glass[3] == 0 and glass[31] == 0 and glass.view("<f4")[1] == np.float32(0.25)
