@@ -73,7 +73,7 @@ void validateTextures(const gnd_scene_desc* d) {
     for (int m = 0; m < d->num_materials; ++m) {
         slot(mats[m].a);
         slot(mats[m].b);
-        for (uint32_t r : {mats[m].roughTex, mats[m].etaTex, mats[m].kTex})
+        for (uint32_t r : {mats[m].roughTex, mats[m].etaTex, mats[m].kTex, mats[m].normalTex, mats[m].bumpTex})
             if ((int64_t)r > n) throw Error(GND_ERR_INVALID, "material texture node out of range");
     }
     const Emitter* ems = reinterpret_cast<const Emitter*>(d->emitters);

@@ -116,6 +116,8 @@ __device__ __forceinline__ V3 imageTexel(const SceneView& s, const TexNode& t, i
         y = ((y % h) + h) % h;
     }
     const float4 c = __ldg(reinterpret_cast<const float4*>(s.texels) + t.a + (int64_t)y * w + x);
+    if (t.flags & kTnNormal)   // imageTexture.cpp:101-104
+        return t.b >= 3 ? v3(c.x * 2.0f - 1.0f, c.y * 2.0f - 1.0f, c.z * 2.0f - 1.0f) : v3(0.0f, 0.0f, 1.0f);
     return v3(c.x, c.y, c.z);
 }
 // ImageTexture::sampleClosest / sampleLinear (imageTexture.cpp:109-143)

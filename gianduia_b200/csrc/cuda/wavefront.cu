@@ -309,6 +309,36 @@ __device__ __forceinline__ V3 evalColor(const SceneView& s, const ColorTex& t, V
     if (EXT && t.kind == kTexNode) return evalTexTree(s, t.node, p, n, dpdu, uv);
     return evalTex(t, uv);
 }
+// Material::applyNormalOrBump (material.h:71-117): the normal map replaces n by its
+// (x, y, z) in the (dpdu, n x dpdu, n) frame; the bump map tilts dpdu and dpdv by forward
+// differences of the height (steps of 0.001 in p along dpdu / dpdv and in u / v). dpdu is
+// re-orthogonalised against the new n. Everything after it (emission, light pdf, next
+// event cosine, BSDF frame, medium choice) sees the new frame, as in the reference.
+__device__ __noinline__ void applyNormalOrBump(const SceneView& s, const Material& m, SurfInt& si) {
+    if (m.normalTex) {
+        const V3 nm = evalTexTree(s, m.normalTex - 1, si.p, si.n, si.dpdu, si.uv);
+        const V3 dpdv = normalize(cross(si.n, si.dpdu));
+        const V3 pn = (si.dpdu * nm.x + dpdv * nm.y) + si.n * nm.z;
+        si.n = normalize(pn);
+        si.dpdu = normalize(si.dpdu - si.n * dot(si.n, si.dpdu));
+    } else if (m.bumpTex) {
+        const V3 dpdu = si.dpdu;
+        const V3 dpdv = normalize(cross(si.n, dpdu));
+        const float du = 0.001f, dv = 0.001f;
+        const float hBase = evalTexTree(s, m.bumpTex - 1, si.p, si.n, si.dpdu, si.uv).x;
+        const float hDu = evalTexTree(s, m.bumpTex - 1, si.p + dpdu * du, si.n, si.dpdu, V2{si.uv.x + du, si.uv.y}).x;
+        const float hDv = evalTexTree(s, m.bumpTex - 1, si.p + dpdv * dv, si.n, si.dpdu, V2{si.uv.x, si.uv.y + dv}).x;
+        float dhdu = (hDu - hBase) / du;
+        float dhdv = (hDv - hBase) / dv;
+        dhdu *= m.bumpScale;
+        dhdv *= m.bumpScale;
+        const V3 ndu = dpdu + si.n * dhdu;
+        const V3 ndv = dpdv + si.n * dhdv;
+        si.n = normalize(cross(ndu, ndv));
+        si.dpdu = normalize(ndu - si.n * dot(si.n, ndu));
+    }
+}
+
 // Material slots at a surface point; EXT: with texture trees.
 template <bool EXT>
 struct SlotTexAt {
@@ -936,6 +966,7 @@ __global__ void __launch_bounds__(kBlock) kShade(KParams p, const uint32_t* list
                              : surfaceInteractionWith(s, h, o, d, s.instS[h.inst].o2w, s.instT[h.inst].w2o);
             const InstShade& is = s.instS[h.inst];
             const Material mat = s.materials[is.material];
+            if (EXT && (mat.normalTex | mat.bumpTex)) applyNormalOrBump(s, mat, si);
             Bsdf bsdf;
             const bool hasBsdf = makeLobeT<M>(mat, SlotTexAt<EXT>{s, si}, bsdf.lobe);
             if (is.emitter >= 0) {

@@ -344,7 +344,9 @@ struct ImageColor : ColorTexture {
     std::vector<float> texels;
     // float image textures read the first channel (imageTexture.cpp:93-95), which is the
     // first texel channel here as well
-    explicit ImageColor(const PropertyList& p, bool = false) : filename(p.getString("filename")) {
+    bool normal = false;   // image_normal
+    bool isNormalMap() const override { return normal; }
+    explicit ImageColor(const PropertyList& p, bool = false, bool isNormal = false) : filename(p.getString("filename")), normal(isNormal) {
         rec.kind = gnd::kTexNode;
         const std::string interp = p.getString("interpolation_mode", "closest");
         if (interp == "linear") linear = true;
@@ -365,7 +367,7 @@ struct ImageColor : ColorTexture {
     gnd::TexNode node(TexTables& t) const override {
         gnd::TexNode n{};
         n.kind = gnd::kTnImage;
-        n.flags = (linear ? gnd::kTnLinear : 0) | (clamp ? gnd::kTnClamp : 0);
+        n.flags = (linear ? gnd::kTnLinear : 0) | (clamp ? gnd::kTnClamp : 0) | (normal ? gnd::kTnNormal : 0);
         if (t.texels.size() / 4 + (size_t)width * height > (size_t)INT32_MAX)
             throw std::runtime_error("ImageTexture: image textures larger than 2^31 texels in total");
         n.a = (int32_t)(t.texels.size() / 4);
@@ -403,6 +405,10 @@ using WoodFloat = TreeFloat<WoodColor>;
 using CellularFloat = TreeFloat<CellularColor>;
 using DomainWarpFloat = TreeFloat<DomainWarpColor>;
 using ImageFloat = TreeFloat<ImageColor>;
+// imageTexture.cpp:101-104 (ImageTexture<Normal3f>)
+struct ImageNormal : ImageColor {
+    explicit ImageNormal(const PropertyList& p) : ImageColor(p, false, true) {}
+};
 }  // namespace
 GND_REGISTER_CLASS(PerlinColor, "perlin_color")
 GND_REGISTER_CLASS(MarbleColor, "marble_color")
@@ -417,6 +423,7 @@ GND_REGISTER_CLASS(WoodFloat, "wood_float")
 GND_REGISTER_CLASS(CellularFloat, "cellular_float")
 GND_REGISTER_CLASS(DomainWarpFloat, "domainWarp_float")
 GND_REGISTER_CLASS(ImageFloat, "image_float")
+GND_REGISTER_CLASS(ImageNormal, "image_normal")
 
 // ---------------------------------------------------------------- media
 // homogeneous.cpp:14-20
@@ -435,7 +442,17 @@ GND_REGISTER_CLASS(HomogeneousMediumObj, "homogeneous")
 // ---------------------------------------------------------------- materials
 // material.h:36-59 (normal and bump maps are not part of the GPU path)
 void MaterialObj::addChild(std::shared_ptr<GndObject> c) {
-    if (c->getClassType() == EMedium && c->getName() == "inside") {
+    if (c->getClassType() == ETexture && c->getName() == "normal") {
+        if (normalTex) throw std::runtime_error("Material: normal map already defined!");
+        auto t = std::dynamic_pointer_cast<ColorTexture>(c);
+        if (!t || !t->isNormalMap()) throw std::runtime_error("Material: the normal map must be an image_normal texture");
+        normalTex = t;
+    } else if (c->getClassType() == ETexture && c->getName() == "bump") {
+        if (bumpTex) throw std::runtime_error("Material: bump map already defined!");
+        auto f = std::dynamic_pointer_cast<FloatTexture>(c);
+        if (!f) throw std::runtime_error("Material: the bump map must be a float texture");
+        bumpTex = f->tree;
+    } else if (c->getClassType() == EMedium && c->getName() == "inside") {
         if (inside) throw std::runtime_error("Material: inside medium already defined!");
         inside = std::static_pointer_cast<MediumObj>(c);
     } else if (c->getClassType() == EMedium && c->getName() == "outside") {
@@ -472,6 +489,7 @@ struct MatteMat : MaterialObj {
     bool hasA = false;
     explicit MatteMat(const PropertyList& p) {
         rec.type = gnd::kMatMatte;
+        rec.bumpScale = p.getFloat("bump_scale", 1.0f);   // material.h:14
         if (p.hasColor("albedo")) { rec.a = constColor(p.getColor("albedo", gnd::v3s(0.f))); hasA = true; }
     }
     void addChild(std::shared_ptr<GndObject> c) override {
@@ -488,6 +506,7 @@ struct PlasticMat : MaterialObj {
     bool hKd = false, hKs = false, hR = false, hE = false;
     explicit PlasticMat(const PropertyList& p) {
         rec.type = gnd::kMatPlastic;
+        rec.bumpScale = p.getFloat("bump_scale", 1.0f);   // material.h:14
         if (p.hasColor("Kd")) { rec.a = constColor(p.getColor("Kd", gnd::v3s(0.f))); hKd = true; }
         if (p.hasColor("Ks")) { rec.b = constColor(p.getColor("Ks", gnd::v3s(0.f))); hKs = true; }
         if (p.hasFloat("roughness")) { rec.roughness = p.getFloat("roughness"); hR = true; }
@@ -515,6 +534,7 @@ struct ConductorMat : MaterialObj {
     V3 eta{1, 1, 1}, k{1, 1, 1};
     explicit ConductorMat(const PropertyList& p) {
         rec.type = gnd::kMatConductor;
+        rec.bumpScale = p.getFloat("bump_scale", 1.0f);   // material.h:14
         if (p.hasColor("R")) { rec.a = constColor(p.getColor("R", gnd::v3s(0.f))); hR = true; }
         if (p.hasColor("eta")) { eta = p.getColor("eta", eta); hE = true; }
         if (p.hasColor("k")) { k = p.getColor("k", k); hK = true; }
@@ -549,6 +569,7 @@ struct GlassMat : MaterialObj {
     bool hR = false, hT = false, hRo = false, hE = false;
     explicit GlassMat(const PropertyList& p) {
         rec.type = gnd::kMatGlass;
+        rec.bumpScale = p.getFloat("bump_scale", 1.0f);   // material.h:14
         if (p.hasColor("R")) { rec.a = constColor(p.getColor("R", gnd::v3s(0.f))); hR = true; }
         if (p.hasColor("T")) { rec.b = constColor(p.getColor("T", gnd::v3s(0.f))); hT = true; }
         if (p.hasFloat("roughness")) { rec.roughness = p.getFloat("roughness"); hRo = true; }
@@ -571,7 +592,10 @@ struct GlassMat : MaterialObj {
 };
 // index.cpp:6-16 (null BSDF: medium boundary only)
 struct IndexMat : MaterialObj {
-    explicit IndexMat(const PropertyList&) { rec.type = gnd::kMatIndex; }
+    explicit IndexMat(const PropertyList& p) {
+        rec.type = gnd::kMatIndex;
+        rec.bumpScale = p.getFloat("bump_scale", 1.0f);
+    }
 };
 GND_REGISTER_CLASS(MatteMat, "matte")
 GND_REGISTER_CLASS(PlasticMat, "plastic")
@@ -1101,6 +1125,8 @@ void Scene::build() {
             m.roughTex = mat->roughTex ? 1u + (uint32_t)mat->roughTex->flatten(fs->textures) : 0u;
             m.etaTex = mat->etaTex ? 1u + (uint32_t)mat->etaTex->flatten(fs->textures) : 0u;
             m.kTex = mat->kTex ? 1u + (uint32_t)mat->kTex->flatten(fs->textures) : 0u;
+            m.normalTex = mat->normalTex ? 1u + (uint32_t)mat->normalTex->flatten(fs->textures) : 0u;
+            m.bumpTex = (mat->bumpTex && !mat->normalTex) ? 1u + (uint32_t)mat->bumpTex->flatten(fs->textures) : 0u;
             fs->materials.push_back(m);
             mit = matIdx.emplace(mat, k).first;
         }

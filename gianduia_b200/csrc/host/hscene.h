@@ -166,6 +166,7 @@ struct ColorTexture : GndObject {
     // Appends this texture's node (after its inputs') to t and returns its index.
     int32_t flatten(TexTables& t) const;
     virtual gnd::TexNode node(TexTables& t) const;   // constant / checker leaf from rec
+    virtual bool isNormalMap() const { return false; }
 };
 // Float texture: a constant, or (constant false) a texture tree whose nodes carry the
 // value in every channel. `tree` is set for both, so a float texture can also be a node
@@ -186,6 +187,7 @@ struct MaterialObj : GndObject {
     gnd::Material rec{};
     std::shared_ptr<ColorTexture> texA, texB;   // the texture objects of slots a and b
     std::shared_ptr<ColorTexture> roughTex, etaTex, kTex;   // non-constant roughness / eta / k
+    std::shared_ptr<ColorTexture> normalTex, bumpTex;       // normal / bump map trees (material.h:36-44)
     std::shared_ptr<MediumObj> inside, outside;
     EClassType getClassType() const override { return EMaterial; }
     void addChild(std::shared_ptr<GndObject> c) override;

@@ -133,7 +133,8 @@ enum : int32_t {
     kTnMetricShift = 1,         // cellular: bits 1-2 = 0 euclidean, 1 manhattan, 2 chebyshev
     kTnLinear = 1,              // image: bilinear instead of closest texel
     kTnClamp = 2,               // image: clamp instead of repeat
-    kTnFloatLerp = 8            // perlin / marble / wood float textures: std::lerp blend
+    kTnFloatLerp = 8,           // perlin / marble / wood float textures: std::lerp blend
+    kTnNormal = 16              // image_normal: 2 c - 1 of the rgb, (0, 0, 1) below 3 channels
 };
 // Nesting of warps in the `warp` input of a warp: at most this many levels.
 constexpr int kTexWarpNesting = 2;
@@ -165,7 +166,12 @@ struct alignas(16) Material {
     ColorTex b;               // plastic Ks | glass T
     float condEta[3]; uint32_t etaTex;   // eta tree: float (plastic/glass) or color (conductor)
     float condK[3]; uint32_t kTex;       // conductor k tree
+    // normal map (image_normal tree) or bump map (float tree), material.h:71-117
+    uint32_t normalTex, bumpTex;
+    float bumpScale;
+    uint32_t pad;
 };
+static_assert(sizeof(Material) == 160, "Material must be 160 bytes");
 
 // ---------------------------------------------------------------- emitters, media
 // Emitter kinds: area lights on primitives (area.cpp), the delta lights point, spot and

@@ -450,7 +450,7 @@ def _texture(kind, name, props, children=()):
 
 
 def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gpu", emitter_texture=False,
-             lens=None, moving=False, point_light=False, float_textures=False):
+             lens=None, moving=False, point_light=False, float_textures=False, maps=False):
     """The Cornell box with the reference's procedural and image textures on its walls and
     boxes: Perlin turbulence (floor), cellular cracks (back wall), an sRGB PNG with linear
     filtering (left wall), a float EXR with closest filtering and clamping (right wall),
@@ -459,7 +459,8 @@ def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_
     moving: the marble box moves over the shutter; point_light: a point light inside the
     box as well; float_textures: the left wall is a rough conductor (image R, cellular eta,
     wood_float roughness) and the wood box's plastic takes perlin_float roughness and
-    checkerboard_float eta. Returns the XML path."""
+    checkerboard_float eta; maps: a normal map (PNG) on the back wall and a bump map
+    (perlin_float) on the floor. Returns the XML path."""
     os.makedirs(out_dir, exist_ok=True)
     write_plane_obj(os.path.join(out_dir, "plane.obj"))
     write_cube_obj(os.path.join(out_dir, "cube.obj"))
@@ -489,9 +490,20 @@ def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_
     xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height, lens=lens),
            '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
            '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
+    if maps:
+        ny, nx = np.mgrid[0:16, 0:16]
+        tilt = np.stack([np.sin(nx * 0.8) * 0.4, np.cos(ny * 0.6) * 0.3, np.ones((16, 16))], axis=-1)
+        tilt /= np.linalg.norm(tilt, axis=-1, keepdims=True)
+        write_png(os.path.join(out_dir, "normal.png"), np.round((tilt * 0.5 + 0.5) * 255).astype(np.uint8))
+    wall_maps = {
+        0: _texture("perlin_float", "bump", {"scale": 0.15, "octaves": 2}) + '<float name="bump_scale" value="0.04"/>',
+        2: _texture("image_normal", "normal", {"filename": "normal.png", "interpolation_mode": "linear"}),
+    } if maps else {}
     for k, tr in enumerate(walls):
         shape = '<shape type="mesh" id="plane"><string name="filename" value="plane.obj"/></shape>' if k == 0 else '<ref id="plane"/>'
-        if float_textures and k == 3:
+        if k in wall_maps:
+            mat = ['<material type="matte">', tex[k], wall_maps[k], "</material>"]
+        elif float_textures and k == 3:
             mat = ['<material type="conductor">', tex[k].replace('name="albedo"', 'name="R"', 1),
                    _texture("cellular_color", "eta", {"value1": (0.2, 0.4, 1.4), "value2": (1.5, 0.9, 0.3), "scale": 0.3}),
                    _color("k", (3.0, 2.5, 2.2)),

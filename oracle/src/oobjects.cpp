@@ -72,7 +72,13 @@ static std::shared_ptr<ColorTexture> missingTex() {
 // ---------------------------------------------------------------- materials
 // material.h:36-59
 void Material::addChild(ObjectPtr child) {
-    if (child->classType() == EMedium && child->name == "inside") {
+    if (child->classType() == ETexture && child->name == "normal") {
+        if (normalMap) throw std::runtime_error("Material: normal map already defined!");
+        normalMap = std::static_pointer_cast<Texture<Color>>(child);
+    } else if (child->classType() == ETexture && child->name == "bump") {
+        if (bumpMap) throw std::runtime_error("Material: bump map already defined!");
+        bumpMap = std::static_pointer_cast<Texture<float>>(child);
+    } else if (child->classType() == EMedium && child->name == "inside") {
         if (inside) throw std::runtime_error("Material: inside medium already defined!");
         inside = std::static_pointer_cast<Medium>(child);
     } else if (child->classType() == EMedium && child->name == "outside") {
@@ -80,6 +86,42 @@ void Material::addChild(ObjectPtr child) {
         outside = std::static_pointer_cast<Medium>(child);
     } else {
         throw std::runtime_error("Material: cannot add specified child (" + child->name + ")!");
+    }
+}
+
+// material.h:71-117: the normal map replaces n by its (x, y, z) in the (dpdu, n x dpdu, n)
+// frame; the bump map tilts dpdu and dpdv by the height's forward differences (steps of
+// 0.001 along dpdu / dpdv in p and along u / v); dpdu is re-orthogonalised either way.
+void Material::applyNormalOrBump(SurfaceInteraction& si) const {
+    if (normalMap) {
+        Color nm = normalMap->evaluate(si);
+        Vec3 dpdv = Normalize(Cross(si.n, si.dpdu));
+        Vec3 pn = si.dpdu * nm.r + dpdv * nm.g + si.n * nm.b;
+        si.n = Normalize(pn);
+        Vec3 nd = si.dpdu - si.n * Dot(si.n, si.dpdu);
+        si.dpdu = Normalize(nd);
+    } else if (bumpMap) {
+        Vec3 dpdu = si.dpdu;
+        Vec3 dpdv = Normalize(Cross(si.n, dpdu));
+        const float du = 0.001f, dv = 0.001f;
+        float hBase = bumpMap->evaluate(si);
+        SurfaceInteraction sDu = si;
+        sDu.p = si.p + dpdu * du;
+        sDu.uv.x += du;
+        float hDu = bumpMap->evaluate(sDu);
+        SurfaceInteraction sDv = si;
+        sDv.p = si.p + dpdv * dv;
+        sDv.uv.y += dv;
+        float hDv = bumpMap->evaluate(sDv);
+        float dhdu = (hDu - hBase) / du;
+        float dhdv = (hDv - hBase) / dv;
+        dhdu *= bumpScale;
+        dhdv *= bumpScale;
+        Vec3 ndu = dpdu + si.n * dhdu;
+        Vec3 ndv = dpdv + si.n * dhdv;
+        si.n = Normalize(Cross(ndu, ndv));
+        Vec3 proj = ndu - si.n * Dot(si.n, ndu);
+        si.dpdu = Normalize(proj);
     }
 }
 
@@ -91,7 +133,10 @@ static void setTex(std::shared_ptr<Texture<T>>& slot, ObjectPtr child) {
 // matte.cpp:7-53
 struct Matte : Material {
     std::shared_ptr<ColorTexture> albedo;
-    explicit Matte(const PropertyList& p) { if (p.hasColor("albedo")) albedo = constTex(p.getColor("albedo")); }
+    explicit Matte(const PropertyList& p) {
+        bumpScale = p.getFloat("bump_scale", 1.0f);
+        if (p.hasColor("albedo")) albedo = constTex(p.getColor("albedo"));
+    }
     void addChild(ObjectPtr c) override {
         if (c->classType() != ETexture) throw std::runtime_error("Matte: cannot add specified child!");
         if (c->name == "albedo") { if (albedo) throw std::runtime_error("Matte: there's already an albedo defined!"); setTex(albedo, c); }
@@ -99,6 +144,7 @@ struct Matte : Material {
     }
     void activate() override { if (!albedo) albedo = missingTex(); }
     void computeScatteringFunctions(SurfaceInteraction& si, Arena& a) const override {
+        applyNormalOrBump(si);
         si.bsdf = a.create<BSDF>(si.n, si.dpdu);
         si.bsdf->add(a.create<Lambertian>(albedo->evaluate(si)));
     }
@@ -108,6 +154,7 @@ struct Plastic : Material {
     std::shared_ptr<ColorTexture> Kd, Ks;
     std::shared_ptr<FloatTexture> rough, eta;
     explicit Plastic(const PropertyList& p) {
+        bumpScale = p.getFloat("bump_scale", 1.0f);
         if (p.hasColor("Kd")) Kd = constTex(p.getColor("Kd"));
         if (p.hasColor("Ks")) Ks = constTex(p.getColor("Ks"));
         if (p.hasFloat("roughness")) rough = constTex(p.getFloat("roughness"));
@@ -126,6 +173,7 @@ struct Plastic : Material {
         if (!eta) eta = constTex(1.5f);
     }
     void computeScatteringFunctions(SurfaceInteraction& si, Arena& a) const override {
+        applyNormalOrBump(si);
         Color kd = Kd->evaluate(si), ks = Ks->evaluate(si);
         float r = rough->evaluate(si), e = eta->evaluate(si);
         si.bsdf = a.create<BSDF>(si.n, si.dpdu);
@@ -138,6 +186,7 @@ struct Conductor : Material {
     std::shared_ptr<ColorTexture> R, eta, k;
     std::shared_ptr<FloatTexture> rough;
     explicit Conductor(const PropertyList& p) {
+        bumpScale = p.getFloat("bump_scale", 1.0f);
         if (p.hasColor("R")) R = constTex(p.getColor("R"));
         if (p.hasColor("eta")) eta = constTex(p.getColor("eta"));
         if (p.hasColor("k")) k = constTex(p.getColor("k"));
@@ -156,6 +205,7 @@ struct Conductor : Material {
         if (!rough) rough = constTex(0.0f);
     }
     void computeScatteringFunctions(SurfaceInteraction& si, Arena& a) const override {
+        applyNormalOrBump(si);
         Color r = R->evaluate(si), e = eta->evaluate(si), kk = k->evaluate(si);
         float ro = rough->evaluate(si);
         si.bsdf = a.create<BSDF>(si.n, si.dpdu);
@@ -169,6 +219,7 @@ struct Glass : Material {
     std::shared_ptr<ColorTexture> R, T;
     std::shared_ptr<FloatTexture> rough, eta;
     explicit Glass(const PropertyList& p) {
+        bumpScale = p.getFloat("bump_scale", 1.0f);
         if (p.hasColor("R")) R = constTex(p.getColor("R"));
         if (p.hasColor("T")) T = constTex(p.getColor("T"));
         if (p.hasFloat("roughness")) rough = constTex(p.getFloat("roughness"));
@@ -186,6 +237,7 @@ struct Glass : Material {
         if (!eta) eta = constTex(1.5f);
     }
     void computeScatteringFunctions(SurfaceInteraction& si, Arena& a) const override {
+        applyNormalOrBump(si);
         applyMediums(si);
         Color r = R->evaluate(si), t = T->evaluate(si);
         float e = eta->evaluate(si), ro = rough->evaluate(si);
@@ -196,8 +248,9 @@ struct Glass : Material {
 };
 // index.cpp:6-16 (null BSDF: a pass-through medium boundary)
 struct IndexMaterial : Material {
-    explicit IndexMaterial(const PropertyList&) {}
+    explicit IndexMaterial(const PropertyList& p) { bumpScale = p.getFloat("bump_scale", 1.0f); }
     void computeScatteringFunctions(SurfaceInteraction& si, Arena&) const override {
+        applyNormalOrBump(si);
         applyMediums(si);
         si.bsdf = nullptr;
     }
@@ -843,6 +896,11 @@ std::unique_ptr<Object> createInstance(const std::string& t, const PropertyList&
     if (t == "domainWarp_float") return std::make_unique<DomainWarpTexture<float>>(p);
     if (t == "image_color") return std::make_unique<ImageTexture<Color>>(p);
     if (t == "image_float") return std::make_unique<ImageTexture<float>>(p);
+    if (t == "image_normal") {   // ImageTexture<Normal3f>: 2 c - 1 of the rgb, (0, 0, 1) for 1-2 channels
+        auto n = std::make_unique<ImageTexture<Color>>(p);
+        n->normal = true;
+        return n;
+    }
     throw std::runtime_error("Cannot instantiate object: class '" + t + "' is not registered!");
 }
 

@@ -217,9 +217,13 @@ public:
 // ---------------------------------------------------------------- materials
 struct Material : Object {
     std::shared_ptr<Medium> inside, outside;
+    std::shared_ptr<Texture<Color>> normalMap;   // image_normal: (x, y, z) in r, g, b
+    std::shared_ptr<Texture<float>> bumpMap;
+    float bumpScale = 1.0f;                      // material.h:14
     ClassType classType() const override { return EMaterial; }
-    void addChild(ObjectPtr child) override;   // material.h:36-59 (media only; maps unsupported)
+    void addChild(ObjectPtr child) override;   // material.h:36-59
     virtual void computeScatteringFunctions(SurfaceInteraction& si, Arena& a) const = 0;
+    void applyNormalOrBump(SurfaceInteraction& si) const;   // material.h:71-117
     // material.h:119-126
     void applyMediums(SurfaceInteraction& si) const {
         if (inside || outside) si.mediumInterface = MediumInterface{inside.get(), outside.get()};

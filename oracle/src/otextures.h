@@ -187,6 +187,7 @@ template <typename T>
 struct ImageTexture : Texture<T> {
     std::string filename, baseDir;
     bool linear = false, clamp = false, srgb = false;
+    bool normal = false;   // image_normal (imageTexture.cpp:101-104)
     std::shared_ptr<ImageData> img;
     explicit ImageTexture(const PropertyList& p);
     void setBaseDir(const std::string& d) override { baseDir = d; }
@@ -201,6 +202,7 @@ struct ImageTexture : Texture<T> {
         else { x = std::clamp(x, 0, w - 1); y = std::clamp(y, 0, h - 1); }
         const float* ptr = &img->data[(size_t)(y * w + x) * c];
         if constexpr (std::is_same_v<T, float>) return ptr[0];
+        else if (normal) return c >= 3 ? Color(ptr[0] * 2.0f - 1.0f, ptr[1] * 2.0f - 1.0f, ptr[2] * 2.0f - 1.0f) : Color(0.0f, 0.0f, 1.0f);
         else return c >= 3 ? Color(ptr[0], ptr[1], ptr[2]) : Color(ptr[0]);
     }
     T evaluate(const SurfaceInteraction& si) const override {

@@ -29,6 +29,9 @@ CASES = {
     # roughness / eta / conductor eta as texture trees
     "float-textures": dict(float_textures=True),
     "float-textures-volpath": dict(float_textures=True, integrator="volpath_gpu"),
+    # normal map on the back wall, bump map on the floor
+    "normal-bump-maps": dict(maps=True),
+    "normal-bump-maps-volpath": dict(maps=True, integrator="volpath_gpu", float_textures=True),
 }
 
 

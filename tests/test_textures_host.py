@@ -146,10 +146,24 @@ def test_float_texture_slots(tmp_path):
         f.write(xml)
     hs = G.HostScene.load_xml(os.path.join(d, "s.xml"))
     nodes, _ = tables(hs)
-    mats = np.frombuffer(ctypes.string_at(hs.desc.materials, 144 * hs.desc.num_materials), "<u4").reshape(-1, 36)
+    mats = np.frombuffer(ctypes.string_at(hs.desc.materials, 160 * hs.desc.num_materials), "<u4").reshape(-1, 40)
     plastic = mats[mats[:, 0] == 1][0]
     glass = mats[mats[:, 0] == 3][0]
     rough, eta = nodes[plastic[3] - 1], nodes[plastic[31] - 1]
     assert rough["kind"] == 2 and rough["flags"] == 8 and rough["v1"][0] == np.float32(0.1) and rough["v2"][0] == 1.0
     assert eta["kind"] == 5 and eta["flags"] == 0 and eta["v2"][2] == np.float32(1.8)
     assert glass[3] == 0 and glass[31] == 0 and glass.view("<f4")[1] == np.float32(0.25)
+
+
+def test_normal_and_bump_maps_flattened(tmp_path):
+    """material.h:36-44: `normal` (image_normal) and `bump` (a float texture) children and
+    bump_scale land in Material.normalTex / bumpTex / bumpScale; the normal image's node
+    carries flag 16."""
+    hs = G.HostScene.load_xml(scenes.textures(str(tmp_path), width=8, height=8, spp=1, maps=True))
+    nodes, _ = tables(hs)
+    mats = np.frombuffer(ctypes.string_at(hs.desc.materials, 160 * hs.desc.num_materials), "<u4").reshape(-1, 40)
+    normal = mats[mats[:, 36] > 0]
+    bump = mats[mats[:, 37] > 0]
+    assert len(normal) == 1 and len(bump) == 1
+    assert nodes[normal[0, 36] - 1]["kind"] == 6 and nodes[normal[0, 36] - 1]["flags"] & 16
+    assert nodes[bump[0, 37] - 1]["kind"] == 2 and bump[0, 38:39].view("<f4")[0] == np.float32(0.04)
