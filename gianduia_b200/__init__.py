@@ -93,6 +93,8 @@ def lib():
                 "gnd_gpu_trace_any_dev": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp, _vp],
                 "gnd_gpu_trace_count_dev": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp, _vp, _vp],
                 "gnd_gpu_render": [_vp, ctypes.c_uint64, _vp, _vp, _vp],
+                "gnd_gpu_render_fixed": [_vp, ctypes.c_uint64, _vp, _vp, _vp, _vp],
+                "gnd_gpu_counters": [_vp, _vp, ctypes.c_int32],
                 "gnd_gpu_cancel": [_vp],
                 "gnd_gpu_trace_closest_fixed": [_vp, ctypes.c_uint64, _vp, ctypes.c_int64, _vp],
                 "gnd_gpu_set_hbm_budget": [_vp, ctypes.c_uint64],
@@ -388,17 +390,59 @@ class GpuContext:
     def trace_count_dev(self, sid, d_rays, n, d_nodes, d_tris, stream=0):
         _check(lib().gnd_gpu_trace_count_dev(self._h, sid, d_rays, n, d_nodes, d_tris, stream or None), "gnd_gpu_trace_count_dev")
 
+    def _film_size(self, sid, width, height):
+        hs = self._scenes[sid]
+        return (width if width > 0 else hs.width), (height if height > 0 else hs.height)
+
     def render(self, sid, spp=0, first_pass=0, max_depth=0, integrator=-1, window=None, batched=False, film=None,
                callback=None, profile=0, width=0, height=0):
         """gnd_gpu_render: adds passes [first_pass, first_pass + spp) of the scene into
         `film` (float32 [H, W, 7]: sum wL rgb, sum w, sum wL^2 rgb). Returns (film, stats).
         width / height override the scene file's film size."""
-        hs = self._scenes[sid]
-        W = width if width > 0 else hs.width
-        H = height if height > 0 else hs.height
+        W, H = self._film_size(sid, width, height)
         if film is None:
             film = np.zeros((H, W, 7), np.float32)
         assert film.dtype == np.float32 and film.shape == (H, W, 7) and film.flags.c_contiguous
+        p = self._params(spp, first_pass, max_depth, integrator, window, batched, profile, width, height)
+        cb = None
+        if callback is not None:
+            def _cb(user, s, fptr, w, h):
+                arr = np.ctypeslib.as_array(fptr, shape=(h, w, 7)).copy()
+                callback(int(s), arr)
+            cb = PROGRESS_FN(_cb)
+            p.callback = cb
+        st = RenderStats()
+        _check(lib().gnd_gpu_render(self._h, sid, ctypes.byref(p), film.ctypes.data, ctypes.byref(st)), "gnd_gpu_render")
+        return film, st.as_dict()
+
+    def render_fixed(self, sid, spp=0, first_pass=0, max_depth=0, integrator=-1, window=None, batched=False, fsum=None,
+                     fsq=None, profile=0, width=0, height=0):
+        """gnd_gpu_render_fixed: adds the passes into the exact film -- fsum (uint64 [H, W, 4],
+        sum wL rgb and sum w in units of 2^-24) and fsq (float32 [H, W, 3], sum wL^2).
+        Returns (fsum, fsq, stats)."""
+        W, H = self._film_size(sid, width, height)
+        if fsum is None:
+            fsum = np.zeros((H, W, 4), np.uint64)
+        if fsq is None:
+            fsq = np.zeros((H, W, 3), np.float32)
+        assert fsum.dtype == np.uint64 and fsum.shape == (H, W, 4) and fsum.flags.c_contiguous
+        assert fsq.dtype == np.float32 and fsq.shape == (H, W, 3) and fsq.flags.c_contiguous
+        p = self._params(spp, first_pass, max_depth, integrator, window, batched, profile, width, height)
+        st = RenderStats()
+        _check(lib().gnd_gpu_render_fixed(self._h, sid, ctypes.byref(p), fsum.ctypes.data, fsq.ctypes.data,
+                                          ctypes.byref(st)), "gnd_gpu_render_fixed")
+        return fsum, fsq, st.as_dict()
+
+    def counters(self, reset=False):
+        """gnd_gpu_counters: the context's work counters as a dict (`last`: the last render's stats)."""
+        c = Counters()
+        _check(lib().gnd_gpu_counters(self._h, ctypes.byref(c), 1 if reset else 0), "gnd_gpu_counters")
+        d = {name: getattr(c, name) for name, _ in Counters._fields_ if name != "last"}
+        d["last"] = c.last.as_dict()
+        return d
+
+    @staticmethod
+    def _params(spp, first_pass, max_depth, integrator, window, batched, profile, width, height):
         p = RenderParams()
         p.spp = spp
         p.first_pass = first_pass
@@ -410,18 +454,7 @@ class GpuContext:
         p.profile = profile
         p.width = width
         p.height = height
-        cb = None
-        if callback is not None:
-            def _cb(user, s, fptr, w, h):
-                arr = np.ctypeslib.as_array(fptr, shape=(h, w, 7)).copy()
-                callback(int(s), arr)
-            cb = PROGRESS_FN(_cb)
-            p.callback = cb
-        st = RenderStats()
-        _check(lib().gnd_gpu_render(self._h, sid, ctypes.byref(p), film.ctypes.data, ctypes.byref(st)), "gnd_gpu_render")
-        return film, dict(paths=st.paths, rays=st.rays, passes=st.passes_done, ms=st.ms, extend_rays=st.extend_rays,
-                          shadow_rays=st.shadow_rays, extend_nodes=st.extend_nodes, extend_tris=st.extend_tris,
-                          extend_ms=st.extend_ms, iterations=st.iterations, launches=st.launches)
+        return p
 
     def cancel(self):
         _check(lib().gnd_gpu_cancel(self._h), "gnd_gpu_cancel")
@@ -530,6 +563,20 @@ class RenderStats(ctypes.Structure):
                 ("shadow_rays", ctypes.c_int64), ("extend_nodes", ctypes.c_int64), ("extend_tris", ctypes.c_int64),
                 ("extend_ms", ctypes.c_double), ("iterations", ctypes.c_int64), ("launches", ctypes.c_int64)]
 
+    def as_dict(self):
+        return dict(paths=self.paths, rays=self.rays, passes=self.passes_done, ms=self.ms, extend_rays=self.extend_rays,
+                    shadow_rays=self.shadow_rays, extend_nodes=self.extend_nodes, extend_tris=self.extend_tris,
+                    extend_ms=self.extend_ms, iterations=self.iterations, launches=self.launches)
+
+
+class Counters(ctypes.Structure):
+    """gnd_counters"""
+    _fields_ = [("trace_batches", ctypes.c_int64), ("trace_rays", ctypes.c_int64), ("counted_rays", ctypes.c_int64),
+                ("counted_nodes", ctypes.c_int64), ("counted_tris", ctypes.c_int64), ("renders", ctypes.c_int64),
+                ("paths", ctypes.c_int64), ("extend_rays", ctypes.c_int64), ("shadow_rays", ctypes.c_int64),
+                ("extend_nodes", ctypes.c_int64), ("extend_tris", ctypes.c_int64), ("iterations", ctypes.c_int64),
+                ("launches", ctypes.c_int64), ("render_ms", ctypes.c_double), ("last", RenderStats)]
+
 
 class Tune(ctypes.Structure):
     _fields_ = [("pool_log2", ctypes.c_int32), ("round_iters", ctypes.c_int32), ("trav_blocks", ctypes.c_int32),
@@ -564,3 +611,12 @@ def resolve(film):
     """Image = sum(w L) / sum(w) per pixel (film.cpp:50-95)."""
     w = film[..., 3:4]
     return np.where(w > 0, film[..., :3] / np.maximum(w, 1e-30), 0.0).astype(np.float32)
+
+
+def fixed_to_film(fsum, fsq):
+    """The float film [H, W, 7] of an exact film (fsum uint64 [H, W, 4] in units of 2^-24,
+    fsq float32 [H, W, 3]), converted as gnd_gpu_render converts it."""
+    f = np.empty(fsum.shape[:2] + (7,), np.float32)
+    f[..., :4] = (fsum.astype(np.float64) * (1.0 / 16777216.0)).astype(np.float32)
+    f[..., 4:] = fsq
+    return f

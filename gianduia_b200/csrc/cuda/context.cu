@@ -176,12 +176,39 @@ gnd_status gnd_gpu_create(int device, gnd_gpu_ctx** out) {
         GND_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
         c->errWord.alloc(16);
         GND_CUDA(cudaMemset(c->errWord.ptr, 0, 16));
+        c->traceTotals.alloc(kTraceTotals * sizeof(unsigned long long));
+        GND_CUDA(cudaMemset(c->traceTotals.ptr, 0, kTraceTotals * sizeof(unsigned long long)));
         *out = reinterpret_cast<gnd_gpu_ctx*>(c.release());
     });
 }
 
 gnd_status gnd_gpu_destroy(gnd_gpu_ctx* ctx) {
     return guarded([&]() { delete ctxOf(ctx); });
+}
+
+gnd_status gnd_gpu_counters(gnd_gpu_ctx* ctxh, gnd_counters* out, int32_t reset) {
+    return guarded([&]() {
+        Context* c = ctxOf(ctxh);
+        if (!out) throw Error(GND_ERR_INVALID, "null output pointer");
+        c->bind();
+        std::lock_guard<FairMutex> lk(c->mu);
+        // batches may have been queued on the caller's streams: wait for all of them
+        GND_CUDA(cudaDeviceSynchronize());
+        unsigned long long t[kTraceTotals];
+        GND_CUDA(cudaMemcpy(t, c->traceTotals.ptr, sizeof(t), cudaMemcpyDeviceToHost));
+        gnd_counters r = c->counters;
+        r.trace_rays = (int64_t)t[kTraceTotalRays];
+        r.counted_rays = (int64_t)t[kTraceTotalCountedRays];
+        r.counted_nodes = (int64_t)t[kTraceTotalNodes];
+        r.counted_tris = (int64_t)t[kTraceTotalTris];
+        *out = r;
+        if (reset) {
+            GND_CUDA(cudaMemset(c->traceTotals.ptr, 0, sizeof(t)));
+            const gnd_render_stats last = c->counters.last;
+            c->counters = gnd_counters{};
+            c->counters.last = last;
+        }
+    });
 }
 
 gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_scene_id* out) {

@@ -36,6 +36,9 @@ const std::string& lastError();
         }                                                                                                  \
     } while (0)
 
+// Device sums of the trace kernels (Context::traceTotals, unsigned long long each).
+enum TraceTotal : int { kTraceTotalRays = 0, kTraceTotalCountedRays = 1, kTraceTotalNodes = 2, kTraceTotalTris = 3, kTraceTotals = 4 };
+
 // Runs an ABI body, mapping exceptions to a status.
 template <typename F>
 gnd_status guarded(F&& f) {
@@ -199,6 +202,22 @@ struct Context {
     uint64_t nextScene = 1;
     DevBuf errWord;           // device error bitmask written by kernels
     DevBuf rayScratch, hitScratch;
+    // gnd_gpu_counters: device sums of the trace kernels (kTraceTotal*), allocated with
+    // the context, and the host sums of the renders
+    DevBuf traceTotals;
+    gnd_counters counters{};
+    void countRender(const gnd_render_stats& s) {
+        counters.renders += 1;
+        counters.paths += s.paths;
+        counters.extend_rays += s.extend_rays;
+        counters.shadow_rays += s.shadow_rays;
+        counters.extend_nodes += s.extend_nodes;
+        counters.extend_tris += s.extend_tris;
+        counters.iterations += s.iterations;
+        counters.launches += s.launches;
+        counters.render_ms += s.ms;
+        counters.last = s;
+    }
     // Work counters of persistent launches: each launch takes the next entry of a ring of
     // kFetchRing counters (reset on the launch's stream), so launches on different
     // streams do not share one.

@@ -22,6 +22,7 @@ struct BatchSrc {
     uint32_t* nodesOut;
     uint32_t* trisOut;
     TraceCounters* cnt;
+    unsigned long long sumNodes = 0, sumTris = 0;   // COUNT: this lane's rays, for the context totals
     __device__ uint32_t count() const { return n; }
     __device__ bool load(uint32_t i, TRay& r, const SceneView*& s, const uint8_t*& nm) {
         float4 a = __ldg(reinterpret_cast<const float4*>(rays + i));
@@ -39,6 +40,8 @@ struct BatchSrc {
         if (COUNT) {
             nodesOut[i] = cnt->nodes;
             trisOut[i] = cnt->tris;
+            sumNodes += cnt->nodes;
+            sumTris += cnt->tris;
         } else if (ANY) {
             occ[i] = h.inst >= 0 ? 1 : 0;
         } else {
@@ -57,11 +60,26 @@ template <bool ANY, bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock, kTraceBlocksPerSM)
     traceKernel(const SceneView* __restrict__ sv, const gnd_ray* __restrict__ rays, uint32_t n, gnd_hit* __restrict__ hits,
                 uint8_t* __restrict__ occ, uint32_t* __restrict__ nodesOut, uint32_t* __restrict__ trisOut,
-                uint32_t* fetch, uint32_t* errWord) {
+                uint32_t* fetch, uint32_t* errWord, unsigned long long* totals) {
     __shared__ uint32_t stack[kSmemStack * kTraceBlock];
     TraceCounters cnt{0, 0};
     BatchSrc<ANY, COUNT> src{sv, rays, n, hits, occ, nodesOut, trisOut, &cnt};
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&totals[kTraceTotalRays], (unsigned long long)n);
+        if (COUNT) atomicAdd(&totals[kTraceTotalCountedRays], (unsigned long long)n);
+    }
     int err = persistentTrace<kTraceBlock, ANY, COUNT>(src, fetch, stack, &cnt);
+    if (COUNT) {
+        unsigned long long nn = src.sumNodes, nt = src.sumTris;
+        for (int o = 16; o > 0; o >>= 1) {
+            nn += __shfl_down_sync(0xffffffffu, nn, o);
+            nt += __shfl_down_sync(0xffffffffu, nt, o);
+        }
+        if ((threadIdx.x & 31) == 0 && (nn | nt)) {
+            atomicAdd(&totals[kTraceTotalNodes], nn);
+            atomicAdd(&totals[kTraceTotalTris], nt);
+        }
+    }
     if (err) atomicOr(errWord, (uint32_t)err);
 }
 
@@ -77,10 +95,12 @@ void launchTrace(Context* c, DeviceScene& ds, const gnd_ray* dr, int64_t n, gnd_
     GND_CUDA(cudaMemsetAsync(fetch, 0, sizeof(uint32_t), st));
     const SceneView* sv = ds.viewDev.as<SceneView>();
     uint32_t nn = (uint32_t)n;
-    if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, nullptr, dn, dt, fetch, ew);
-    else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew);
-    else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew);
+    unsigned long long* tot = c->traceTotals.as<unsigned long long>();
+    if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, nullptr, dn, dt, fetch, ew, tot);
+    else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew, tot);
+    else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew, tot);
     GND_CUDA(cudaGetLastError());
+    c->counters.trace_batches += 1;
 }
 
 // Host-buffer variant: copies in, traces, copies out (pinned staging is the caller's
@@ -219,8 +239,10 @@ gnd_status gnd_gpu_trace_closest_fixed(gnd_gpu_ctx* ctxh, gnd_scene_id id, const
         int64_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
         int g = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)c->numSMs * kTraceBlocksPerSM));
         traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(ds.viewDev.as<SceneView>(), dr, (uint32_t)n, dh, nullptr,
-                                                             nullptr, nullptr, fetch, c->errWord.as<uint32_t>());
+                                                             nullptr, nullptr, fetch, c->errWord.as<uint32_t>(),
+                                                             c->traceTotals.as<unsigned long long>());
         GND_CUDA(cudaGetLastError());
+        c->counters.trace_batches += 1;
         GND_CUDA(cudaMemcpyAsync(hits, dh, sizeof(gnd_hit) * (size_t)n, cudaMemcpyDeviceToHost, st));
         GND_CUDA(cudaStreamSynchronize(st));
         c->checkKernelErrors("trace_closest_fixed");

@@ -1195,6 +1195,12 @@ __global__ void __launch_bounds__(kBlock) kShadow(KParams p, bool mixed) {
                 SurfInt si = MOTION ? surfaceInteraction(s, hr, r.o, r.d, r.time)
                                     : surfaceInteractionWith(s, hr, r.o, r.d, s.instS[h.inst].o2w, s.instT[h.inst].w2o);
                 const InstShade& is = s.instS[h.inst];
+                // volPath.cpp:277: computeScatteringFunctions applies the material's normal or
+                // bump map before the medium is chosen by the side the ray leaves through
+                if (s.ext) {
+                    const Material& mat = s.materials[is.material];
+                    if (mat.normalTex | mat.bumpTex) applyNormalOrBump(s, mat, si);
+                }
                 medium = is.hasMedia ? (dot(r.d, si.n) > 0.0f ? is.mediumOut : is.mediumIn) : -1;
                 r.o = si.p;
                 r.tmin = kEpsilon;
@@ -1726,6 +1732,21 @@ void Wavefront::finish(int j, float* filmHost) {
     drop(j);
 }
 
+void Wavefront::finishFixed(int j, uint64_t* sum, float* sq) {
+    HostJob& hj = jobs_[j];
+    const size_t npix = (size_t)hj.dev.W * hj.dev.H;
+    std::vector<unsigned long long> fs(npix * 4);
+    std::vector<float> fq(npix * 3);
+    GND_CUDA(cudaMemcpyAsync(fs.data(), hj.filmSum.ptr, fs.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             ctx_->stream));
+    GND_CUDA(cudaMemcpyAsync(fq.data(), hj.filmSq.ptr, fq.size() * sizeof(float), cudaMemcpyDeviceToHost, ctx_->stream));
+    GND_CUDA(cudaStreamSynchronize(ctx_->stream));
+    for (size_t q = 0; q < fs.size(); ++q) sum[q] += fs[q];   // modulo 2^64
+    if (sq)
+        for (size_t q = 0; q < fq.size(); ++q) sq[q] += fq[q];
+    drop(j);
+}
+
 void Wavefront::drop(int j) {
     HostJob& hj = jobs_[j];
     hj.used = false;   // its film buffers are kept for the next job of the slot
@@ -1924,7 +1945,7 @@ void Wavefront::enqueueRound(int iters, int mix, bool hasNull, int profile, Resu
 
 Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int firstPass, int maxDepth, int integrator,
                                     const int window[4], bool batched, int profile, float* filmHost, gnd_progress_fn cb,
-                                    void* user) {
+                                    void* user, uint64_t* fixedSum, float* fixedSq) {
     Context* c = ctx_;
     cudaStream_t st = c->stream;
     int wx0 = 0, wy0 = 0, wx1 = W, wy1 = H;
@@ -2043,7 +2064,8 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
         drop(j);
         throw;
     }
-    finish(j, filmHost);
+    if (fixedSum) finishFixed(j, fixedSum, fixedSq);
+    else finish(j, filmHost);
     res.paths = (int64_t)tot[2];
     res.rays = (int64_t)(tot[0] + tot[1]);
     res.extendRays = (int64_t)tot[0];
@@ -2061,41 +2083,60 @@ using namespace gnd;
 
 extern "C" {
 
+namespace {
+// gnd_gpu_render / gnd_gpu_render_fixed: the film goes to `film` or, in fixed-point form,
+// to `sum` and `sq`.
+void renderCall(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_render_params* prm, float* film, uint64_t* sum, float* sq,
+                gnd_render_stats* stats) {
+    Context* c = ctxOf(ctxh);
+    if (!film && !sum) throw Error(GND_ERR_INVALID, "null film buffer");
+    c->bind();
+    std::lock_guard<FairMutex> lk(c->mu);
+    DeviceScene& ds = c->scene(id);
+    gnd_render_params p{};
+    p.integrator = -1;
+    if (prm) p = *prm;
+    int spp = p.spp > 0 ? p.spp : ds.spp;
+    int maxDepth = p.max_depth > 0 ? p.max_depth : ds.maxDepth;
+    int integ = p.integrator >= 0 ? p.integrator : ds.integrator;
+    if (integ != 0 && integ != 1) throw Error(GND_ERR_INVALID, "integrator must be 0 (path_gpu) or 1 (volpath_gpu)");
+    if (maxDepth > 65535) maxDepth = 65535;
+    if (!c->wave) c->wave = std::make_unique<Wavefront>(c);
+    c->cancel = false;
+    const int W = p.width > 0 ? p.width : ds.width, H = p.height > 0 ? p.height : ds.height;
+    if ((uint64_t)W * (uint64_t)H > (1ull << 31)) throw Error(GND_ERR_INVALID, "film too large");
+    Wavefront::Result r = c->wave->render(ds, W, H, spp, p.first_pass, maxDepth, integ, p.window, p.batched != 0,
+                                          p.profile, film, p.batched ? nullptr : p.callback, p.user, sum, sq);
+    gnd_render_stats rs{};
+    rs.paths = r.paths;
+    rs.rays = r.rays;
+    rs.passes_done = r.passesDone;
+    rs.ms = r.ms;
+    rs.extend_rays = r.extendRays;
+    rs.shadow_rays = r.shadowRays;
+    rs.extend_nodes = r.extendNodes;
+    rs.extend_tris = r.extendTris;
+    rs.extend_ms = r.extendMs;
+    rs.iterations = r.iterations;
+    rs.launches = r.launches;
+    c->countRender(rs);
+    if (stats) *stats = rs;
+    if (c->cancel && r.passesDone < spp) throw Error(GND_ERR_CANCELLED, "render cancelled");
+}
+}  // namespace
+
 gnd_status gnd_gpu_render(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_render_params* prm, float* film, gnd_render_stats* stats) {
     return guarded([&]() {
-        Context* c = ctxOf(ctxh);
         if (!film) throw Error(GND_ERR_INVALID, "null film buffer");
-        c->bind();
-        std::lock_guard<FairMutex> lk(c->mu);
-        DeviceScene& ds = c->scene(id);
-        gnd_render_params p{};
-        p.integrator = -1;
-        if (prm) p = *prm;
-        int spp = p.spp > 0 ? p.spp : ds.spp;
-        int maxDepth = p.max_depth > 0 ? p.max_depth : ds.maxDepth;
-        int integ = p.integrator >= 0 ? p.integrator : ds.integrator;
-        if (integ != 0 && integ != 1) throw Error(GND_ERR_INVALID, "integrator must be 0 (path_gpu) or 1 (volpath_gpu)");
-        if (maxDepth > 65535) maxDepth = 65535;
-        if (!c->wave) c->wave = std::make_unique<Wavefront>(c);
-        c->cancel = false;
-        const int W = p.width > 0 ? p.width : ds.width, H = p.height > 0 ? p.height : ds.height;
-        if ((uint64_t)W * (uint64_t)H > (1ull << 31)) throw Error(GND_ERR_INVALID, "film too large");
-        Wavefront::Result r = c->wave->render(ds, W, H, spp, p.first_pass, maxDepth, integ, p.window, p.batched != 0,
-                                              p.profile, film, p.batched ? nullptr : p.callback, p.user);
-        if (stats) {
-            stats->paths = r.paths;
-            stats->rays = r.rays;
-            stats->passes_done = r.passesDone;
-            stats->ms = r.ms;
-            stats->extend_rays = r.extendRays;
-            stats->shadow_rays = r.shadowRays;
-            stats->extend_nodes = r.extendNodes;
-            stats->extend_tris = r.extendTris;
-            stats->extend_ms = r.extendMs;
-            stats->iterations = r.iterations;
-            stats->launches = r.launches;
-        }
-        if (c->cancel && r.passesDone < spp) throw Error(GND_ERR_CANCELLED, "render cancelled");
+        renderCall(ctxh, id, prm, film, nullptr, nullptr, stats);
+    });
+}
+
+gnd_status gnd_gpu_render_fixed(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_render_params* prm, uint64_t* sum, float* sq,
+                                gnd_render_stats* stats) {
+    return guarded([&]() {
+        if (!sum || !sq) throw Error(GND_ERR_INVALID, "null film buffer");
+        renderCall(ctxh, id, prm, nullptr, sum, sq, stats);
     });
 }
 

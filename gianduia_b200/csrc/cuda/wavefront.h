@@ -108,8 +108,11 @@ public:
     };
     // One job to completion: plain = one pass in flight (the pool is one pass and each
     // pass is released when the previous retired), batched = all passes released at once.
+    // The film is added into filmHost (H x W x 7 floats) or, when fixedSum is given, in its
+    // fixed-point form into fixedSum (H x W x 4 uint64) and fixedSq (H x W x 3 floats).
     Result render(DeviceScene& ds, int W, int H, int spp, int firstPass, int maxDepth, int integrator,
-                  const int window[4], bool batched, int profile, float* filmHost, gnd_progress_fn cb, void* user);
+                  const int window[4], bool batched, int profile, float* filmHost, gnd_progress_fn cb, void* user,
+                  uint64_t* fixedSum = nullptr, float* fixedSq = nullptr);
 
     // ---- engine interface used by render() and by the server
     void reset(size_t slots);                         // (re)initialise the pool: every slot idle
@@ -117,6 +120,8 @@ public:
               const int window[4], uint64_t releaseItems);
     void release(int job, uint64_t upTo);             // hand out work items [.., upTo)
     void finish(int job, float* filmHost);            // adds the film to filmHost, frees the job
+    // adds the job's fixed-point sums into sum (H x W x 4) and sq (H x W x 3), frees the job
+    void finishFixed(int job, uint64_t* sum, float* sq);
     void resolve(int job, float* filmHost);           // writes the film (H x W x 7 floats) to filmHost
     // The job's film resolved into pinned host memory (valid until the next call).
     const float* resolvePinned(int job);

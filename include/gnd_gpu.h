@@ -208,8 +208,10 @@ gnd_status gnd_gpu_scene_download(gnd_gpu_ctx* ctx, gnd_scene_id scene, int32_t 
  * on the GPU, then the instance bounds and the top-level tree; normals and uvs stay as
  * loaded. Refused for scenes with moving instances and for meshes carrying an area
  * light. The first refit of a scene walks its trees once (a few synchronous steps);
- * device_ms (may be NULL) receives the device time of the refit kernels. Must not
- * overlap a render of the same scene. */
+ * device_ms (may be NULL) receives the device time of the refit kernels. Renders of the
+ * context finish before the refit starts (both hold the context and run on its stream);
+ * a scene named by a queued or running served job is refused (GND_ERR_INVALID), and ray
+ * batches the caller queued on its own streams must have finished. */
 gnd_status gnd_gpu_scene_refit_mesh(gnd_gpu_ctx* ctx, gnd_scene_id scene, int32_t mesh, const float* positions,
                                     int64_t num_tris, float* device_ms);
 
@@ -333,6 +335,50 @@ gnd_status gnd_gpu_render(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_render
 /* Integrator::cancel (integrator.h:22): asks a running gnd_gpu_render on this context
  * to stop after its current pass. Safe to call from another thread. */
 gnd_status gnd_gpu_cancel(gnd_gpu_ctx* ctx);
+
+/* gnd_gpu_render with the film in the exact form the device accumulates it. No
+ * counterpart in the reference, whose film holds float sums (film.h:110-124); it serves
+ * callers that add up films of several renders (sample passes sharded over GPUs or
+ * processes) and want the total to equal one render of all the passes bit for bit.
+ * `sum` (height x width x 4 uint64: sum of w*L r, g, b and sum of w, in units of 2^-24)
+ * and `sq` (height x width x 3 floats: sum of w*L^2) are HOST buffers; the render ADDS
+ * into them (the integer sums modulo 2^64). Integer sums do not depend on the order of
+ * the additions, so passes split over any number of calls or ranks give the same `sum`
+ * as one call; `sq` is a float sum and agrees to rounding. Image = sum[0..2] / sum[3]. */
+gnd_status gnd_gpu_render_fixed(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_render_params* params, uint64_t* sum,
+                                float* sq, gnd_render_stats* stats);
+
+/* Work counters of a context (diagnostics; no counterpart in the reference, which keeps
+ * none). Sums since the context was created or the counters were last reset:
+ *   trace_*  the ray batches of gnd_gpu_trace_closest / _any / _count_dev / _closest_fixed
+ *            and their _dev forms (rays queued on another stream are counted once the
+ *            device has run them: the call synchronises the device);
+ *   the node visits and triangle tests of the batches that count them
+ *            (gnd_gpu_trace_count_dev);
+ *   render   gnd_gpu_render / gnd_gpu_render_fixed calls: camera paths, closest-hit and
+ *            shadow queries, wavefront iterations, kernel launches, device time, and the
+ *            extend kernel's node visits and triangle tests for renders that count them
+ *            (gnd_render_params.profile bit1);
+ *   last     the statistics of the last render.
+ * reset != 0 clears the sums after reading them. */
+typedef struct gnd_counters {
+    int64_t trace_batches;    /* batches with at least one ray */
+    int64_t trace_rays;
+    int64_t counted_rays;     /* rays of the counting batches */
+    int64_t counted_nodes;    /* BVH4 node visits of those rays */
+    int64_t counted_tris;     /* triangle tests of those rays */
+    int64_t renders;
+    int64_t paths;
+    int64_t extend_rays;
+    int64_t shadow_rays;
+    int64_t extend_nodes;     /* renders with profile bit1 only */
+    int64_t extend_tris;
+    int64_t iterations;
+    int64_t launches;
+    double render_ms;
+    gnd_render_stats last;
+} gnd_counters;
+gnd_status gnd_gpu_counters(gnd_gpu_ctx* ctx, gnd_counters* out, int32_t reset);
 
 /* ------------------------------------------------------------------ tuning */
 /* Engine settings of a scene's renders. They change speed only: every setting renders

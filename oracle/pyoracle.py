@@ -38,6 +38,8 @@ def lib():
             L.orc_free_scene.argtypes = [ctypes.c_void_p]
             L.orc_scene_info.argtypes = [ctypes.c_void_p, _i32p]
             L.orc_render.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 7 + [_f32p, _u64p, ctypes.c_char_p, ctypes.c_int]
+            L.orc_render_fixed.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 7 + [_u64p, _f32p, _u64p, ctypes.c_char_p,
+                                                                                   ctypes.c_int]
             L.orc_trace.argtypes = [ctypes.c_void_p, _f32p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
                                     _f32p, _f32p, _f32p, _i32p, _i32p, _u32p, _u32p]
             L.orc_trace_interaction.argtypes = [ctypes.c_void_p, _f32p, ctypes.c_int64, ctypes.c_int, _f32p, _i32p]
@@ -135,6 +137,25 @@ class Scene:
         if rc != 0:
             raise RuntimeError(err.value.decode())
         return film, int(stats[0]), int(stats[1])
+
+    def render_fixed(self, s0=0, s1=None, window=None, nthreads=0, fsum=None, fsq=None):
+        """As render with the film in fixed point: returns (fsum uint64 [H, W, 4] -- sum wL
+        rgb and sum w in units of 2^-24 --, fsq float32 [H, W, 3] -- sum wL^2 --, paths, rays),
+        accumulated on top of fsum / fsq when given."""
+        s1 = self.spp if s1 is None else s1
+        x0, y0, x1, y1 = window if window else (0, 0, self.width, self.height)
+        if fsum is None:
+            fsum = np.zeros((self.height, self.width, 4), np.uint64)
+        if fsq is None:
+            fsq = np.zeros((self.height, self.width, 3), np.float32)
+        assert fsum.dtype == np.uint64 and fsum.flags.c_contiguous and fsq.dtype == np.float32 and fsq.flags.c_contiguous
+        stats = np.zeros(2, np.uint64)
+        err = ctypes.create_string_buffer(1024)
+        rc = lib().orc_render_fixed(self.h, s0, s1, x0, y0, x1, y1, nthreads, fsum.ctypes.data_as(_u64p), _fp(fsq),
+                                    stats.ctypes.data_as(_u64p), err, 1024)
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        return fsum, fsq, int(stats[0]), int(stats[1])
 
     def trace(self, rays, anyhit=False, nthreads=0, counters=False):
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)

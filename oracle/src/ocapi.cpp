@@ -106,6 +106,29 @@ int orc_render(void* s, int s0, int s1, int x0, int y0, int x1, int y1, int nthr
     }
 }
 
+// As orc_render with the film in fixed point (Film::enableFixed): fsum receives W*H*4
+// uint64 per pixel (sum wL rgb, sum w; units of 2^-24) and fsq W*H*3 floats (sum wL^2),
+// both accumulated on top of their content (the integer sums modulo 2^64).
+int orc_render_fixed(void* s, int s0, int s1, int x0, int y0, int x1, int y1, int nthreads, uint64_t* fsum, float* fsq,
+                     uint64_t* stats, char* err, int errlen) {
+    try {
+        auto& sc = *((OracleScene*)s)->scene;
+        Film f(sc.camera->width, sc.camera->height, sc.camera->filterObj);
+        f.enableFixed();
+        const size_t npix = (size_t)sc.camera->width * sc.camera->height;
+        RenderStats st = renderPasses(sc, f, s0, s1, x0, y0, x1, y1, nthreads);
+        for (size_t q = 0; q < npix; ++q) {
+            for (int k = 0; k < 4; ++k) fsum[q * 4 + k] += f.fixedSum[q * 4 + k].load(std::memory_order_relaxed);
+            for (int k = 0; k < 3; ++k) fsq[q * 3 + k] += f.sum[q * 7 + 4 + k].load(std::memory_order_relaxed);
+        }
+        if (stats) { stats[0] = st.paths; stats[1] = st.rays; }
+        return 0;
+    } catch (const std::exception& e) {
+        setErr(err, errlen, e.what());
+        return -1;
+    }
+}
+
 // Closest-hit (anyhit=0) or occlusion (anyhit=1) queries against the scene's TLAS.
 // rays: n x 8 floats (ox, oy, oz, tmin, dx, dy, dz, tmax).
 // Outputs (closest): t, u, v (barycentrics from the shape), prim (triangle index or -1),

@@ -671,7 +671,20 @@ Film::Film(int w, int h, std::shared_ptr<Filter> f) : width(w), height(h), filte
     if (!filter) filter = std::make_shared<GaussianFilter>(PropertyList());   // film.cpp:29
     clear();
 }
-void Film::clear() { for (auto& a : sum) a.store(0.0f, std::memory_order_relaxed); }
+void Film::clear() {
+    for (auto& a : sum) a.store(0.0f, std::memory_order_relaxed);
+    for (auto& a : fixedSum) a.store(0, std::memory_order_relaxed);
+}
+void Film::enableFixed() {
+    fixedMode = true;
+    fixedSum = std::vector<std::atomic<uint64_t>>((size_t)width * height * 4);
+    for (auto& a : fixedSum) a.store(0, std::memory_order_relaxed);
+}
+uint64_t toFixed(float x) {
+    x = x > 0.0f ? x : 0.0f;          // NaN -> 0
+    x = x < 1e11f ? x : 1e11f;
+    return (uint64_t)(int64_t)std::nearbyint(x * 16777216.0f);   // default rounding: nearest even
+}
 static inline void atomicAddF(std::atomic<float>& t, float v) {
     float cur = t.load(std::memory_order_relaxed);
     while (!t.compare_exchange_weak(cur, cur + v, std::memory_order_release, std::memory_order_relaxed)) {}
@@ -690,10 +703,18 @@ void Film::addSample(const Vec2& pFilm, const Color& L) {
             float w = filter->evaluate(off);
             if (w > 0.0f) {
                 std::atomic<float>* a = &sum[((size_t)py * width + px) * 7];
-                atomicAddF(a[0], L.r * w);
-                atomicAddF(a[1], L.g * w);
-                atomicAddF(a[2], L.b * w);
-                atomicAddF(a[3], w);
+                if (fixedMode) {
+                    std::atomic<uint64_t>* q = &fixedSum[((size_t)py * width + px) * 4];
+                    q[0].fetch_add(toFixed(L.r * w), std::memory_order_relaxed);
+                    q[1].fetch_add(toFixed(L.g * w), std::memory_order_relaxed);
+                    q[2].fetch_add(toFixed(L.b * w), std::memory_order_relaxed);
+                    q[3].fetch_add(toFixed(w), std::memory_order_relaxed);
+                } else {
+                    atomicAddF(a[0], L.r * w);
+                    atomicAddF(a[1], L.g * w);
+                    atomicAddF(a[2], L.b * w);
+                    atomicAddF(a[3], w);
+                }
                 atomicAddF(a[4], L.r * L.r * w);
                 atomicAddF(a[5], L.g * L.g * w);
                 atomicAddF(a[6], L.b * L.b * w);

@@ -269,14 +269,25 @@ struct Filter : Object {
 
 // film.h:21-136 plus a per-pixel sum of squares (not in the reference) for
 // standard errors in the statistical parity tests.
+//
+// Fixed-point mode (not in the reference): sum wL and sum w are accumulated as 64-bit
+// integers in units of 2^-24, each term clamped to [0, 1e11] and rounded to nearest even
+// before it is added -- the film the GPU keeps. Integer sums do not depend on the order of
+// the additions, so renders of disjoint pass ranges add up to one render of all of them
+// bit for bit (the multi-rank reduction checks this).
 struct Film {
     int width, height;
     std::shared_ptr<Filter> filter;
     std::vector<std::atomic<float>> sum;   // 7 floats per pixel: wL(3), w, wL^2(3)
+    bool fixedMode = false;
+    std::vector<std::atomic<uint64_t>> fixedSum;   // fixedMode: 4 per pixel: wL(3), w
     Film(int w, int h, std::shared_ptr<Filter> f);
+    void enableFixed();
     void addSample(const Vec2& pFilm, const Color& L);
     void clear();
 };
+// One term of the fixed-point film: clamp to [0, 1e11], scale by 2^24, round to nearest even.
+uint64_t toFixed(float x);
 
 // camera.h CameraSample
 struct CameraSample {
