@@ -186,7 +186,9 @@ bool traverseBVH4(const std::vector<BVHNode4>& nodes, const Ray& ray, bool shado
         int ni = stack[--sp];
         const BVHNode4& n = nodes[ni];
         if (st) st->nodes++;
-        int mask = 0;
+        // the four lanes as one straight-line loop over fixed-size arrays, so that the
+        // compiler turns it into 4-wide vector code as the Highway lanes are
+        float tminL[4], tmaxL[4];
         for (int i = 0; i < 4; ++i) {
             float t1x = (n.minX[i] - ox) * ix, t2x = (n.maxX[i] - ox) * ix;
             float tminx = vmin(t1x, t2x), tmaxx = vmax(t1x, t2x);
@@ -194,10 +196,11 @@ bool traverseBVH4(const std::vector<BVHNode4>& nodes, const Ray& ray, bool shado
             float tminy = vmin(t1y, t2y), tmaxy = vmax(t1y, t2y);
             float t1z = (n.minZ[i] - oz) * iz, t2z = (n.maxZ[i] - oz) * iz;
             float tminz = vmin(t1z, t2z), tmaxz = vmax(t1z, t2z);
-            float tmin = vmax(vmax(tminx, tminy), vmax(tminz, tMinR));
-            float tmax = vmin(vmin(tmaxx, tmaxy), vmin(tmaxz, tMaxR));
-            if (tmin <= tmax) mask |= 1 << i;
+            tminL[i] = vmax(vmax(tminx, tminy), vmax(tminz, tMinR));
+            tmaxL[i] = vmin(vmin(tmaxx, tmaxy), vmin(tmaxz, tMaxR));
         }
+        int mask = 0;
+        for (int i = 0; i < 4; ++i) mask |= (tminL[i] <= tmaxL[i] ? 1 : 0) << i;
         if (!mask) continue;
         for (int i = 0; i < 4; ++i) {
             if (!(mask & (1 << i))) continue;
@@ -283,6 +286,38 @@ void Mesh::buildAccel() {
     if (totalArea > 0.0f) for (size_t i = 1; i <= triCount; ++i) cdf[i] /= totalArea;
 }
 
+// mesh.cpp:259-291: Moller-Trumbore on the four lanes of a pack, in the Highway code's
+// operation order. Straight-line lanes (no short-circuit branches) over restrict
+// pointers, so that the compiler emits 4-wide vector code as the Highway lanes do.
+static inline void packTest(const TrianglePack4& pk, float ox, float oy, float oz, float dx, float dy, float dz,
+                            float tMin, float tMax, float* __restrict__ tA, float* __restrict__ uA,
+                            float* __restrict__ vA, int* __restrict__ valid) {
+    const float* __restrict__ v0x = pk.v0x; const float* __restrict__ v0y = pk.v0y; const float* __restrict__ v0z = pk.v0z;
+    const float* __restrict__ v1x = pk.v1x; const float* __restrict__ v1y = pk.v1y; const float* __restrict__ v1z = pk.v1z;
+    const float* __restrict__ v2x = pk.v2x; const float* __restrict__ v2y = pk.v2y; const float* __restrict__ v2z = pk.v2z;
+    for (int l = 0; l < 4; ++l) {
+        float e1x = v1x[l] - v0x[l], e1y = v1y[l] - v0y[l], e1z = v1z[l] - v0z[l];
+        float e2x = v2x[l] - v0x[l], e2y = v2y[l] - v0y[l], e2z = v2z[l] - v0z[l];
+        float px = dy * e2z - dz * e2y;
+        float py = dz * e2x - dx * e2z;
+        float pz = dx * e2y - dy * e2x;
+        float det = (e1x * px + e1y * py) + e1z * pz;
+        int ok = std::abs(det) > 1e-8f;
+        float invDet = 1.0f / det;
+        float tx = ox - v0x[l], ty = oy - v0y[l], tz = oz - v0z[l];
+        float u = ((tx * px + ty * py) + tz * pz) * invDet;
+        ok = ok & (u >= 0.0f) & (u <= 1.0f);
+        float qx = ty * e1z - tz * e1y;
+        float qy = tz * e1x - tx * e1z;
+        float qz = tx * e1y - ty * e1x;
+        float v = ((dx * qx + dy * qy) + dz * qz) * invDet;
+        ok = ok & (v >= 0.0f) & (u + v <= 1.0f);
+        float t = ((e2x * qx + e2y * qy) + e2z * qz) * invDet;
+        ok = ok & (t > tMin) & (t < tMax);
+        tA[l] = t; uA[l] = u; vA[l] = v; valid[l] = ok;
+    }
+}
+
 // mesh.cpp:231-326 (four lanes per pack, same operation order as the Highway code)
 bool Mesh::rayIntersect(const Ray& ray, SurfaceInteraction& si, bool predicate, TraversalStats* st) const {
     const float ox = ray.o.x, oy = ray.o.y, oz = ray.o.z;
@@ -293,29 +328,9 @@ bool Mesh::rayIntersect(const Ray& ray, SurfaceInteraction& si, bool predicate, 
         for (int p = 0; p < count; ++p) {
             const TrianglePack4& pk = packs[offset + p];
             float tA[4], uA[4], vA[4];
-            bool valid[4];
-            for (int l = 0; l < 4; ++l) {
-                if (st) st->tris++;
-                float e1x = pk.v1x[l] - pk.v0x[l], e1y = pk.v1y[l] - pk.v0y[l], e1z = pk.v1z[l] - pk.v0z[l];
-                float e2x = pk.v2x[l] - pk.v0x[l], e2y = pk.v2y[l] - pk.v0y[l], e2z = pk.v2z[l] - pk.v0z[l];
-                float px = dy * e2z - dz * e2y;
-                float py = dz * e2x - dx * e2z;
-                float pz = dx * e2y - dy * e2x;
-                float det = (e1x * px + e1y * py) + e1z * pz;
-                bool ok = std::abs(det) > 1e-8f;
-                float invDet = 1.0f / det;
-                float tx = ox - pk.v0x[l], ty = oy - pk.v0y[l], tz = oz - pk.v0z[l];
-                float u = ((tx * px + ty * py) + tz * pz) * invDet;
-                ok = ok && (u >= 0.0f) && (u <= 1.0f);
-                float qx = ty * e1z - tz * e1y;
-                float qy = tz * e1x - tx * e1z;
-                float qz = tx * e1y - ty * e1x;
-                float v = ((dx * qx + dy * qy) + dz * qz) * invDet;
-                ok = ok && (v >= 0.0f) && (u + v <= 1.0f);
-                float t = ((e2x * qx + e2y * qy) + e2z * qz) * invDet;
-                ok = ok && (t > ray.tMin) && (t < tMaxPack);
-                tA[l] = t; uA[l] = u; vA[l] = v; valid[l] = ok;
-            }
+            int valid[4];
+            if (st) st->tris += 4;
+            packTest(pk, ox, oy, oz, dx, dy, dz, ray.tMin, tMaxPack, tA, uA, vA, valid);
             for (int l = 0; l < 4; ++l) {
                 if (valid[l] && tA[l] < ray.tMax) {
                     if (predicate) return true;
