@@ -890,7 +890,22 @@ void Scene::activate() {
     if (!m_integrator) throw std::runtime_error("Scene: no integrator specified!");
     if (!m_sampler) throw std::runtime_error("Scene: no sampler specified!");
     build();
-    if (!deferPreprocess) m_integrator->preprocess(this);
+    if (!deferPreprocess) {
+        ensureFilm();
+        m_integrator->preprocess(this);
+    }
+}
+
+// camera.h:63-66: the camera's film (its filter travels in the flattened scene). Scenes
+// loaded only for their flattened description (deferPreprocess) get it when first rendered.
+Film* Scene::ensureFilm() {
+    if (!m_camera) throw std::runtime_error("Scene: no camera specified!");
+    if (!m_camera->film) {
+        m_camera->film = std::make_unique<Film>(m_camera->width, m_camera->height);
+        m_camera->film->outputPath = outputPath;
+        m_camera->film->outputName = outputName;
+    }
+    return m_camera->film.get();
 }
 
 namespace {

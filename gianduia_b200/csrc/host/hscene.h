@@ -5,6 +5,7 @@
 #pragma once
 #include <atomic>
 #include <cstdint>
+#include <filesystem>
 #include <functional>
 #include <map>
 #include <memory>
@@ -123,6 +124,24 @@ public:
 
 protected:
     std::string m_name;
+};
+
+// fileResolver.h:11-41: the directory of the scene file being loaded and the name its
+// outputs take (its stem), recorded by loadFromXML as Parser::loadFromXML records them
+// (parser.cpp:220-223) before the scene is built.
+class FileResolver {
+public:
+    static void setBasePath(const std::filesystem::path& p) { basePath() = p; }
+    static void setOutputPath(const std::filesystem::path& p) { outputPath() = p; }
+    static void setOutputName(const std::string& n) { outputName() = n; }
+    static std::filesystem::path getBasePath() { return basePath(); }
+    static std::filesystem::path getOutputPath() { return outputPath(); }
+    static std::string getOutputName() { return outputName(); }
+
+private:
+    static std::filesystem::path& basePath();
+    static std::filesystem::path& outputPath();
+    static std::string& outputName();
 };
 
 // factory.h:9-36
@@ -263,6 +282,37 @@ struct FilterObj : GndObject {
     EClassType getClassType() const override { return EFilter; }
 };
 
+// film.h:21-136: the image a render writes. The GPU integrators fill it from the device's
+// per-pixel sums (sum wL rgb, sum w, sum wL^2 rgb: setSums) and resolve it as
+// film.cpp:50-95 does; savePNG / saveEXR write <outputPath>/<outputName>.png / .exr as
+// film.cpp:154-195 (the scene file's directory and stem, FileResolver).
+class Film {
+public:
+    Film(int width, int height);
+    void clear();
+    // sums: width x height x 7 floats (the layout of gnd_gpu_render's film)
+    void setSums(const float* sums);
+    const std::vector<float>& sums() const { return m_sums; }
+    // radiance = sum wL / sum w per pixel, 0 where no sample has weight
+    void resolve();
+    void setPixel(int x, int y, V3 c) { m_radiance[(size_t)y * m_width + x] = c; }
+    const V3& getPixel(int x, int y) const { return m_radiance[(size_t)y * m_width + x]; }
+    const std::vector<V3>& getRadiance() const { return m_radiance; }
+    int width() const { return m_width; }
+    int height() const { return m_height; }
+    float aspectRatio() const { return (float)m_width / (float)m_height; }
+    void savePNG() const { savePNG(outputName); }
+    void saveEXR() const { saveEXR(outputName); }
+    void savePNG(const std::string& relativeOutPath) const;   // sRGB, x255 + 0.5, clamped, truncated
+    void saveEXR(const std::string& relativeOutPath) const;   // float RGB
+    std::string outputPath = ".", outputName = "output";
+
+private:
+    int m_width, m_height;
+    std::vector<float> m_sums;
+    std::vector<V3> m_radiance;
+};
+
 struct CameraObj : GndObject {
     Transform toWorld;
     Transform toWorldEnd;     // camera.h:23
@@ -277,15 +327,21 @@ struct CameraObj : GndObject {
     bool vignetting = false;
     int blades = 0;
     std::shared_ptr<FilterObj> filter;
+    std::unique_ptr<Film> film;   // camera.h:72: created by Scene::activate
     explicit CameraObj(const PropertyList& p);
     EClassType getClassType() const override { return ECamera; }
     void addChild(std::shared_ptr<GndObject> c) override;
+    // camera.h:32-39
+    Film* getFilm() const { return film.get(); }
+    int getWidth() const { return width; }
+    int getHeight() const { return height; }
 };
 
 struct SamplerObj : GndObject {
     int spp = 1;
     explicit SamplerObj(const PropertyList& p) : spp(p.getInteger("spp", 1)) {}
     EClassType getClassType() const override { return ESampler; }
+    size_t getSampleCount() const { return (size_t)spp; }   // sampler.h:21
 };
 
 class Scene;
@@ -293,7 +349,7 @@ class Scene;
 // integrator.h:18-40: the plugin interface the GPU integrators implement.
 class Integrator : public GndObject {
 public:
-    using RenderCallback = std::function<void(int sampleIndex, const float* film, int width, int height)>;
+    using RenderCallback = std::function<void(int sampleIndex, const Film& film)>;
     virtual ~Integrator() = default;
     virtual void render(Scene* scene) = 0;
     virtual void cancel() { m_stopRequested = true; }
@@ -304,6 +360,10 @@ public:
     int maxDepth = 1000; // path.cpp:9, volPath.cpp:12
 
 protected:
+    // integrator.h:31-35
+    void notifyUpdate(int sampleIndex, const Film& film) {
+        if (m_callback && !m_stopRequested) m_callback(sampleIndex, film);
+    }
     std::atomic<bool> m_stopRequested{false};
     RenderCallback m_callback;
 };
@@ -340,6 +400,7 @@ public:
     void addChild(std::shared_ptr<GndObject> c) override;
     void activate() override;                 // builds and flattens, then integrator->preprocess
     void build();                             // builds and flattens only
+    Film* ensureFilm();                       // the camera's film, created on first use
     EClassType getClassType() const override { return EScene; }
     void render() { m_integrator->render(this); }
     std::shared_ptr<CameraObj> getCamera() { return m_camera; }
@@ -364,6 +425,9 @@ public:
     std::shared_ptr<SamplerObj> m_sampler;
     std::shared_ptr<Integrator> m_integrator;
     std::unique_ptr<FlatScene> m_flat;
+    // FileResolver::getOutputPath / getOutputName (parser.cpp:220-223): the scene file's
+    // directory and stem, where the film's images are written
+    std::string outputPath = ".", outputName = "output";
 };
 
 // parser.cpp:220-235

@@ -1,12 +1,14 @@
 // Scene-file loading: a small XML reader, the reference's element grammar
 // (parser.cpp:41-235: property tags, nested objects, <ref id>, transforms composed as
 // t = step * t) and the OBJ reader for meshes (mesh.cpp:148-229).
+#include <atomic>
 #include <cctype>
 #include <cstdlib>
 #include <cstring>
 #include <filesystem>
 #include <fstream>
 #include <sstream>
+#include <thread>
 #include <unordered_map>
 
 #include "hscene.h"
@@ -209,9 +211,15 @@ public:
             if (refs_.count(id)) throw std::runtime_error("Parsing error: id <" + id + "> already exists.");
             refs_[id] = sp;
         }
+        bool deferred = false;
         if (auto shape = std::dynamic_pointer_cast<ShapeObj>(sp)) {
             if (!shape->filename.empty() && std::filesystem::path(shape->filename).is_relative())
                 shape->filename = (std::filesystem::path(baseDir_) / shape->filename).string();
+            // mesh files are read later, all at once on every host core (loadPending)
+            if (shape->kind == gnd::kShapeMesh && !shape->filename.empty() && shape->positions.empty()) {
+                pending_.push_back(shape);
+                deferred = true;
+            }
         }
         sp->setBaseDir(baseDir_);
         for (const XmlNode* k : kids) {
@@ -227,19 +235,66 @@ public:
         if (auto sc = std::dynamic_pointer_cast<Scene>(sp)) {
             sc->deferPreprocess = deferPreprocess;
             sc->deviceBlas = deviceBlas;
+            sc->outputPath = outputPath;
+            sc->outputName = outputName;
+            loadPending();   // the scene's activate builds the mesh trees
         }
-        sp->activate();
+        if (!deferred) sp->activate();
         return sp;
+    }
+
+    // Reads the deferred mesh files (ShapeObj::activate, mesh.cpp:148-229) on every host
+    // core. Parsing does not look at mesh data, so only the loading order changes; the
+    // first failing file (in scene-file order) is reported.
+    void loadPending() {
+        std::vector<std::shared_ptr<ShapeObj>> todo;
+        todo.swap(pending_);
+        if (todo.empty()) return;
+        std::vector<std::exception_ptr> errs(todo.size());
+        std::atomic<size_t> next{0};
+        auto work = [&]() {
+            for (;;) {
+                const size_t i = next.fetch_add(1);
+                if (i >= todo.size()) break;
+                try {
+                    todo[i]->activate();
+                } catch (...) {
+                    errs[i] = std::current_exception();
+                }
+            }
+        };
+        const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), (unsigned)todo.size()));
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t < nt; ++t) th.emplace_back(work);
+        work();
+        for (auto& t : th) t.join();
+        for (auto& e : errs)
+            if (e) std::rethrow_exception(e);
     }
     bool deferPreprocess = false;
     bool deviceBlas = false;
+    std::string outputPath = ".", outputName = "output";
 
 private:
+    std::vector<std::shared_ptr<ShapeObj>> pending_;   // mesh shapes whose files are not read yet
     std::string baseDir_;
     std::unordered_map<std::string, std::shared_ptr<GndObject>> refs_;
 };
 
 }  // namespace
+
+std::filesystem::path& FileResolver::basePath() {
+    static std::filesystem::path p = std::filesystem::current_path();
+    return p;
+}
+std::filesystem::path& FileResolver::outputPath() {
+    static std::filesystem::path p = std::filesystem::current_path();
+    return p;
+}
+std::string& FileResolver::outputName() {
+    static std::string n = "output";   // fileResolver.cpp: the default output name
+    return n;
+}
 
 std::shared_ptr<GndObject> loadFromXML(const std::string& path, bool deferPreprocess, bool deviceBlas) {
     std::ifstream f(path, std::ios::binary);
@@ -251,10 +306,19 @@ std::shared_ptr<GndObject> loadFromXML(const std::string& path, bool deferPrepro
     XmlNode root = reader.document();
     std::error_code ec;
     std::filesystem::path canon = std::filesystem::canonical(path, ec);
-    Loader ld((ec ? std::filesystem::path(path) : canon).parent_path().string());
+    const std::filesystem::path file = ec ? std::filesystem::path(path) : canon;
+    // parser.cpp:221-223
+    FileResolver::setBasePath(file.parent_path());
+    FileResolver::setOutputPath(file.parent_path());
+    FileResolver::setOutputName(file.stem().string());
+    Loader ld(file.parent_path().string());
     ld.deferPreprocess = deferPreprocess;
     ld.deviceBlas = deviceBlas;
-    return ld.parse(root);
+    ld.outputPath = file.parent_path().string();   // parser.cpp:222-223 (FileResolver)
+    ld.outputName = file.stem().string();
+    auto obj = ld.parse(root);
+    ld.loadPending();   // a root that is not a scene
+    return obj;
 }
 
 // mesh.cpp:148-229 for v / vt / vn / f (polygons split as fans). When the file has no
