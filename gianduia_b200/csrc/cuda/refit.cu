@@ -175,6 +175,12 @@ gnd_status gnd_gpu_scene_refit_mesh(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t 
         std::lock_guard<FairMutex> lk(c->mu);
         DeviceScene& ds = c->scene(id);
         const SceneView& v = ds.view;
+        // Renders hold the context lock and run on its stream, so they finish before the
+        // refit starts; a served job may still be queued or running, and would see the
+        // geometry change between its rounds.
+        auto use = c->sceneUse.find(id);
+        if (use != c->sceneUse.end() && use->second > 0)
+            throw Error(GND_ERR_INVALID, "refit: the scene is used by queued or running jobs");
         if (mesh < 0 || mesh >= ds.numMeshes) throw Error(GND_ERR_INVALID, "refit: mesh index out of range");
         if (v.motion) throw Error(GND_ERR_INVALID, "refit: scenes with moving instances are not refitted");
         MeshRec rec;
@@ -203,9 +209,17 @@ gnd_status gnd_gpu_scene_refit_mesh(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t 
         PoolBuf pos((size_t)num_tris * 9 * sizeof(float), c->stream);
         PoolBuf inst((size_t)std::max(ds.numInstances, 1) * sizeof(Box), c->stream);
         GND_CUDA(cudaMemcpyAsync(pos.ptr, positions, pos.bytes, cudaMemcpyHostToDevice, c->stream));
-        cudaEvent_t e0, e1;
-        GND_CUDA(cudaEventCreate(&e0));
-        GND_CUDA(cudaEventCreate(&e1));
+        // timing events, destroyed on every exit (a failing launch throws)
+        struct Events {
+            cudaEvent_t e[2] = {nullptr, nullptr};
+            ~Events() {
+                for (cudaEvent_t x : e)
+                    if (x) cudaEventDestroy(x);
+            }
+        } ev;
+        GND_CUDA(cudaEventCreate(&ev.e[0]));
+        GND_CUDA(cudaEventCreate(&ev.e[1]));
+        cudaEvent_t e0 = ev.e[0], e1 = ev.e[1];
         GND_CUDA(cudaEventRecord(e0, c->stream));
         Node4* nodes = const_cast<Node4*>(v.nodes);
         kRefitTris<<<gridFor(num_tris, c->numSMs), 256, 0, c->stream>>>(pos.as<float>(), num_tris, v.origToLeaf + rec.origToLeaf,
@@ -227,8 +241,6 @@ gnd_status gnd_gpu_scene_refit_mesh(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t 
         GND_CUDA(cudaEventSynchronize(e1));
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, e0, e1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
         if (device_ms) *device_ms = ms;
     });
 }

@@ -90,10 +90,27 @@ def _color(name, c):
     return '<color name="%s" value="%s %s %s"/>' % (name, _fmt(c[0]), _fmt(c[1]), _fmt(c[2]))
 
 
-def _camera(origin, target, fov, w, h, up=(0, 1, 0), lens=None, end=None):
+def _filter(spec):
+    """The camera's <filter> element: "box" (radius 0.5); "default": none, so the film takes
+    the reference's default Gaussian filter (film.cpp:29; radius 2, alpha 2); "gaussian", or
+    ("gaussian", (rx, ry), alpha), an explicit Gaussian filter (filter.h:34-54)."""
+    if spec == "box":
+        return ['<filter type="box"/>']
+    if spec == "default":
+        return []
+    if spec == "gaussian":
+        return ['<filter type="gaussian"/>']
+    kind, radius, alpha = spec
+    assert kind == "gaussian"
+    return ['<filter type="gaussian">', '<vector2 name="radius" value="%s, %s"/>' % (_fmt(radius[0]), _fmt(radius[1])),
+            '<float name="alpha" value="%s"/>' % _fmt(alpha), "</filter>"]
+
+
+def _camera(origin, target, fov, w, h, up=(0, 1, 0), lens=None, end=None, filter="box"):
     """A pinhole camera, or with `lens` (a dict of thin-lens properties: lens_radius,
     focal_distance, k1, ca_axial, ca_lateral, vignetting, blades) a thin-lens one. `end`:
-    (origin, target) of a toWorldEnd lookat (camera motion over the shutter)."""
+    (origin, target) of a toWorldEnd lookat (camera motion over the shutter). `filter`: see
+    _filter."""
     props = []
     for k, v in sorted((lens or {}).items()):
         if isinstance(v, bool):
@@ -113,7 +130,7 @@ def _camera(origin, target, fov, w, h, up=(0, 1, 0), lens=None, end=None):
         '<integer name="width" value="%d"/>' % w,
         '<integer name="height" value="%d"/>' % h,
         *props,
-        '<filter type="box"/>',
+        *_filter(filter),
         "</camera>",
     ])
 
@@ -161,13 +178,13 @@ def _cornell_body(light_y=0.998):
     return out
 
 
-def cornell(out_dir, width=256, height=256, spp=16, max_depth=8, integrator="path_gpu", lens=None):
+def cornell(out_dir, width=256, height=256, spp=16, max_depth=8, integrator="path_gpu", lens=None, filter="box"):
     """Writes the Cornell-box scene; returns the XML path. `lens`: thin-lens camera
-    properties (see _camera), else a pinhole camera."""
+    properties (see _camera), else a pinhole camera. `filter`: see _filter."""
     os.makedirs(out_dir, exist_ok=True)
     write_plane_obj(os.path.join(out_dir, "plane.obj"))
     write_cube_obj(os.path.join(out_dir, "cube.obj"))
-    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height, lens=lens),
+    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height, lens=lens, filter=filter),
            '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
            '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
     xml += _cornell_body()
@@ -178,14 +195,14 @@ def cornell(out_dir, width=256, height=256, spp=16, max_depth=8, integrator="pat
     return path
 
 
-def volumetric(out_dir, width=512, height=512, spp=64, max_depth=32, integrator="volpath_gpu"):
+def volumetric(out_dir, width=512, height=512, spp=64, max_depth=32, integrator="volpath_gpu", filter="box"):
     """Cornell box filled with a homogeneous medium plus a glass sphere with its own
-    interior medium; returns the XML path."""
+    interior medium; returns the XML path. `filter`: see _filter."""
     os.makedirs(out_dir, exist_ok=True)
     write_plane_obj(os.path.join(out_dir, "plane.obj"))
     write_cube_obj(os.path.join(out_dir, "cube.obj"))
     box_med = ((0.05, 0.05, 0.05), (0.5, 0.5, 0.5), 0.6)
-    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height),
+    xml = ["<scene>", _camera((0, 0, 3.5), (0, 0, 0), 40, width, height, filter=filter),
            '<sampler type="independent"><integer name="spp" value="%d"/></sampler>' % spp,
            '<integrator type="%s"><integer name="maxDepth" value="%d"/></integrator>' % (integrator, max_depth)]
     xml += _cornell_body(light_y=0.99)
@@ -450,7 +467,7 @@ def _texture(kind, name, props, children=()):
 
 
 def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_gpu", emitter_texture=False,
-             lens=None, moving=False, point_light=False, float_textures=False, maps=False):
+             lens=None, moving=False, point_light=False, float_textures=False, maps=False, index_box=False):
     """The Cornell box with the reference's procedural and image textures on its walls and
     boxes: Perlin turbulence (floor), cellular cracks (back wall), an sRGB PNG with linear
     filtering (left wall), a float EXR with closest filtering and clamping (right wall),
@@ -460,7 +477,9 @@ def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_
     box as well; float_textures: the left wall is a rough conductor (image R, cellular eta,
     wood_float roughness) and the wood box's plastic takes perlin_float roughness and
     checkerboard_float eta; maps: a normal map (PNG) on the back wall and a bump map
-    (perlin_float) on the floor. Returns the XML path."""
+    (perlin_float) on the floor; index_box (with maps): a box of `index` material (null
+    BSDF) holding a homogeneous medium, with the normal map on its faces, so that volpath
+    transmittance queries cross normal-mapped boundaries. Returns the XML path."""
     os.makedirs(out_dir, exist_ok=True)
     write_plane_obj(os.path.join(out_dir, "plane.obj"))
     write_cube_obj(os.path.join(out_dir, "cube.obj"))
@@ -527,6 +546,13 @@ def textures(out_dir, width=64, height=64, spp=4, max_depth=8, integrator="path_
                 if float_textures else '<float name="eta" value="1.5"/><float name="roughness" value="0.3"/>') + '</material>')
         end = [_transform(tr + [("translate", (0.15, 0.1, 0.0))], name="toWorldEnd")] if moving and k == 0 else []
         xml += ["<primitive>", _transform(tr)] + end + [shape, mat, "</primitive>"]
+    if index_box:
+        assert maps, "the index box carries the normal map written with maps=True"
+        xml += ["<primitive>", _transform([("scale", (0.7, 0.5, 0.6)), ("rotate", ((0, 1, 0), 30)),
+                                           ("translate", (0.05, 0.3, 0.2))]), '<ref id="cube"/>',
+                '<material type="index">', _medium("inside", (0.2, 0.3, 0.4), (1.5, 1.2, 0.9), 0.3),
+                _texture("image_normal", "normal", {"filename": "normal.png", "interpolation_mode": "linear"}),
+                "</material>", "</primitive>"]
     xml += ["<primitive>",
             _transform([("scale", (0.5, 1, 0.4)), ("rotate", ((1, 0, 0), 180)), ("translate", (0, 0.998, 0))]),
             '<ref id="plane"/>', '<material type="matte">', _color("albedo", (0, 0, 0)), "</material>",

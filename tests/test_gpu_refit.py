@@ -147,3 +147,29 @@ def test_refit_refusals(ctx, tmp_path):
     with pytest.raises(G.GndError, match="moving"):
         ctx.refit_mesh(sid, 0, plane)
     ctx.free_scene(sid)
+
+
+def test_refit_refused_while_jobs_use_the_scene(ctx, tmp_path):
+    """A served job that names the scene (queued or running) blocks a refit, which would
+    change the geometry between the job's rounds; once the job is done the refit runs."""
+    xml = scenes.cornell(str(tmp_path / "c"), width=64, height=64, spp=4)
+    hs = G.HostScene.load_xml(xml)
+    sid = ctx.upload(hs)
+    cube = _cube_triangles(os.path.join(str(tmp_path / "c"), "cube.obj"))
+    box = None   # the cube mesh (12 triangles, no area light)
+    for m in range(ctx.scene_info(sid)["num_meshes"]):
+        try:
+            ctx.refit_mesh(sid, m, cube)
+            box = m
+            break
+        except G.GndError:
+            continue
+    assert box is not None
+    big = ctx.submit(sid, width=256, height=256, spp=2048, max_depth=8, integrator=0)
+    with pytest.raises(G.GndError, match="jobs") as e:
+        ctx.refit_mesh(sid, box, cube)
+    assert e.value.status == G.GND_ERR_INVALID
+    ctx.cancel_job(big)
+    ctx.wait_any(big)
+    ctx.refit_mesh(sid, box, cube)
+    ctx.free_scene(sid)

@@ -32,6 +32,9 @@ CASES = {
     # normal map on the back wall, bump map on the floor
     "normal-bump-maps": dict(maps=True),
     "normal-bump-maps-volpath": dict(maps=True, integrator="volpath_gpu", float_textures=True),
+    # a medium-filled index box with a normal map: the medium a transmittance query enters
+    # follows the perturbed normal (volPath.cpp:277)
+    "index-normal-map-volpath": dict(maps=True, index_box=True, integrator="volpath_gpu"),
 }
 
 
