@@ -6,8 +6,11 @@ path max depth 16, ground quad plus a 64x64 grid of displaced icospheres
 and 8 spherical emitters; synthetic, seeded (gianduia_b200/scenes.py).
 
 Metric: Mpaths/s (camera samples per second, whole job). N GPUs: weak scaling over the
-sample passes -- rank r renders passes [r*64, (r+1)*64) of the same image and the films
-are summed to rank 0 with one NCCL reduce (the sharded render's only exchange).
+sample passes -- rank r renders passes [r*64, (r+1)*64) of the same image and the exact
+films (fixed-point sums of wL and w, plus sum wL^2) are reduced to rank 0 (the sharded
+render's only exchange), where they equal one render of all N*64 passes bit for bit.
+The timed steps run the production path (per-bounce loop replayed as CUDA graphs); the
+roofline's extend-kernel time comes from a separate instrumented render.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -31,6 +34,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Mpaths/s at matched relMSE; serve p50/p99 time-to-image vs plain GPU"
+# how the CPU restatement of the reference (the oracle, also the timed CPU baseline) is built
+CPU_BUILD = ("g++ -O3 -march=x86-64-v3 -ffp-contract=off; 4-lane slab and Moller-Trumbore loops vectorised "
+             "(the reference's Highway lanes); one std::thread per host core over image rows")
+CPU_NOTE = ("a C++ port of the reference's render loop, not the reference binary (its glm / Highway / TBB / "
+            "vcpkg build cannot be compiled here): GPU/CPU ratios are against this port")
 WORKLOAD = dict(width=1024, height=1024, spp=64, max_depth=16, grid=64, seed=2)
 
 
@@ -128,6 +136,7 @@ def cpu_baseline(xml, seconds=12.0):
         s += 1
     cores = os.cpu_count() or 1
     return {"value": paths / el / 1e6, "unit": "Mpaths/s", "cores": cores, "kind": "port",
+            "build": CPU_BUILD, "note": CPU_NOTE,
             "sample": "%d full-image passes (%d paths) of the 1024x1024 microfacet scene" % (s, paths)}
 
 
@@ -153,8 +162,8 @@ def run_reference(args, rank, world):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, gianduia_b200/scenes.py)",
             "config": {"workload": "microfacet 1024x1024 path depth 16, one full-image pass (1,048,576 paths) per step",
                        "l2": "scene (0.7 GB) larger than L2"},
-            "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": cores, "kind": "port",
-                             "sample": "one 1024x1024 pass per step, %d steps" % args.steps},
+            "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": cores, "kind": "port", "build": CPU_BUILD,
+                             "note": CPU_NOTE, "sample": "one 1024x1024 pass per step, %d steps" % args.steps},
             "e2e": {"value": v, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -335,10 +344,13 @@ def scenes_leg(ctx):
     return out
 
 
-def serve_leg(ctx, microfacet_sid, n_requests):
+def serve_leg(ctx, microfacet_sid, n_requests, n_policy=300):
     """The serving stream: requests over {Cornell box, microfacet grid, volumetric Cornell
-    box} with Poisson arrivals at 80% of the job server's measured capacity, served by the
-    job server and, for comparison, one at a time by plain renders in arrival order."""
+    box} with Poisson arrivals at 80% of the job server's capacity, served by the job
+    server and, for comparison, one at a time by plain renders in arrival order.
+    Capacity: 200 requests of the same distribution submitted at once (samples/s), so
+    that the arrival rate offers 0.8 x capacity for the stream's own mean request size.
+    The FIFO and SRPT hand-out policies are compared on the first `n_policy` requests."""
     import gianduia_b200 as G
     from gianduia_b200 import scenes, serving
     base = os.path.join(tempfile.gettempdir(), "gnd_bench_serve")
@@ -347,34 +359,53 @@ def serve_leg(ctx, microfacet_sid, n_requests):
             "volumetric": ctx.upload(G.HostScene.load_xml(scenes.volumetric(os.path.join(base, "volumetric"))))}
     integ = {"microfacet": 0, "cornell": 0, "volumetric": 1}
     ctx.set_hbm_budget(150 * 10**9)   # the stream's HBM admission budget
-    cap_rps, cap_sps = serving.calibrate_capacity(ctx, sids, integ)
-    rate = 0.8 * cap_rps
-    reqs = serving.make_requests(n_requests, seed=4)
-    arrivals = serving.poisson_arrivals(n_requests, rate, seed=4)
-    other = {}
-    for pol in ("fifo", "srpt"):
-        ctx.serve_policy(pol)
-        other[pol] = serving.latency_stats(serving.run_served(ctx, sids, integ, reqs, arrivals)[0])
     ctx.serve_policy("deadline")
+    t = time.perf_counter()
+    cap_rps, cap_sps = serving.calibrate_capacity(ctx, sids, integ, n=200)
+    log("serve: capacity %.1f Mpaths/s (%.2f req/s) from 200 requests at once, %.1fs" % (
+        cap_sps / 1e6, cap_rps, time.perf_counter() - t))
+    reqs = serving.make_requests(n_requests, seed=4)
+    total = sum(serving.samples(r) for r in reqs)
+    rate = 0.8 * cap_sps / (total / n_requests)   # offered load 0.8 for this stream's mean request
+    arrivals = serving.poisson_arrivals(n_requests, rate, seed=4)
+    t = time.perf_counter()
     lat, makespan = serving.run_served(ctx, sids, integ, reqs, arrivals)
-    service = serving.run_plain_service(ctx, sids, integ, reqs)
+    log("serve: %d requests served in %.1fs" % (n_requests, time.perf_counter() - t))
+    other = {}
+    npol = min(n_policy, n_requests)
+    for pol in ("fifo", "srpt", "deadline"):
+        ctx.serve_policy(pol)
+        other[pol] = serving.latency_stats(serving.run_served(ctx, sids, integ, reqs[:npol], arrivals[:npol])[0])
+    ctx.serve_policy("deadline")
+    t = time.perf_counter()
+    service, model = serving.plain_service_model(ctx, sids, integ, reqs)
+    log("serve: plain render-time model over %d (scene, resolution, depth) keys in %.1fs, largest error %s" % (
+        model["keys"], time.perf_counter() - t, model["max_rel_err"]))
     plain_lat = serving.fifo_finish(arrivals, service) - arrivals
     s, p = serving.latency_stats(lat), serving.latency_stats(plain_lat)
-    total = sum(serving.samples(r) for r in reqs)
     for k in ("cornell", "volumetric"):
         ctx.free_scene(sids[k])
     log("serve: %d requests at %.2f req/s; p50 %.3f s p99 %.3f s (plain one at a time: p50 %.3f s p99 %.3f s)" % (
         n_requests, rate, s["p50"], s["p99"], p["p50"], p["p99"]))
+    plain_sps = total / float(service.sum())
     return {"requests": n_requests, "arrivals": "poisson, seed 4",
             "policy": "deadline (submission + 4x estimated render time, earliest first)",
-            "rate_rps": rate, "capacity_rps": cap_rps,
-            "capacity_mpaths_s": cap_sps / 1e6, "p50_s": s["p50"], "p99_s": s["p99"], "mean_s": s["mean"],
+            "rate_rps": rate, "capacity_rps": cap_rps, "capacity_mpaths_s": cap_sps / 1e6,
+            "capacity_from": "200 requests of the stream's distribution submitted at once",
+            "offered_load": rate * (total / n_requests) / cap_sps,
+            "p50_s": s["p50"], "p99_s": s["p99"], "mean_s": s["mean"], "max_s": s["max"],
             "plain_p50_s": p["p50"], "plain_p99_s": p["p99"], "plain_mean_s": p["mean"],
             "p50_speedup": p["p50"] / s["p50"], "p99_speedup": p["p99"] / s["p99"],
+            "served_mpaths_s": total / makespan / 1e6, "makespan_s": makespan,
+            "plain_mpaths_s": plain_sps / 1e6, "capacity_vs_plain": cap_sps / plain_sps,
+            "policies_first_requests": npol,
             "fifo_p50_s": other["fifo"]["p50"], "fifo_p99_s": other["fifo"]["p99"],
             "srpt_p50_s": other["srpt"]["p50"], "srpt_p99_s": other["srpt"]["p99"],
-            "served_mpaths_s": total / makespan / 1e6, "plain_mpaths_s": total / float(service.sum()) / 1e6,
-            "note": "plain time-to-image from measured per-request render times through the FIFO recurrence"}
+            "deadline_p50_s": other["deadline"]["p50"], "deadline_p99_s": other["deadline"]["p99"],
+            "plain_model": model,
+            "note": "plain time-to-image: the FIFO recurrence over plain render times, each the fixed + spp x "
+                    "per-pass time measured for its (scene, resolution, depth) (plain renders run their passes "
+                    "one after another); served_mpaths_s at 80% offered load is bounded by the arrivals"}
 
 
 def main():
@@ -390,8 +421,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="render with the default engine settings")
     ap.add_argument("--no-scenes", action="store_true", help="skip the Cornell / volumetric renders")
     ap.add_argument("--no-device-bvh", action="store_true", help="skip the device tree build measurements")
-    ap.add_argument("--serve-requests", type=int, default=100,
-                    help="requests in the serving stream (the full stream is 2000); 0 skips it")
+    ap.add_argument("--serve-requests", type=int, default=2000,
+                    help="requests in the serving stream (2000: the full stream); 0 skips it")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -419,7 +450,7 @@ def main():
     ctx = G.GpuContext(local)
     sid = ctx.upload(hs)
     scene_bytes = ctx.scene_bytes(sid)
-    from gianduia_b200.sharding import pass_range, reduce_film
+    from gianduia_b200.sharding import as_int64, as_uint64, pass_range, reduce_fixed_film
     spp = WORKLOAD["spp"]
     first, _ = pass_range(rank, world, spp)
     npix = WORKLOAD["width"] * WORKLOAD["height"]
@@ -446,16 +477,28 @@ def main():
         if dist:
             dist.barrier()
 
+    reduced = []
+
+    def step(profile=0):
+        """One full render of this rank's passes; with N > 1 the exact films (fixed-point
+        sums) are reduced to rank 0, which keeps the result."""
+        if not dist:
+            return ctx.render(sid, spp=spp, first_pass=first, profile=profile, batched=batched, film=film)[1]
+        fsum, fsq, st = ctx.render_fixed(sid, spp=spp, first_pass=first, profile=profile, batched=batched)
+        ts, tq = torch.from_numpy(as_int64(fsum)).cuda(), torch.from_numpy(fsq).cuda()
+        reduce_fixed_film(ts, tq, dist)
+        if rank == 0:
+            reduced[:] = [ts, tq]
+        return st
+
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
     t0 = time.perf_counter()
     stats = []
     for k in range(args.steps):
-        _, st = ctx.render(sid, spp=spp, first_pass=first, profile=1, batched=batched, film=film)
-        if dist:
-            reduce_film(torch.from_numpy(film).cuda(), dist)
-        stats.append(st)
+        # the production path: CUDA-graph bounce loop, no per-launch instrumentation
+        stats.append(step())
     barrier()
     wall = time.perf_counter() - t0
     clk = clocks.stop()
@@ -468,13 +511,22 @@ def main():
     paths_total = sum(s["paths"] for s in stats) * world
     value = paths_total / elapsed / 1e6
     rays = sum(s["rays"] for s in stats)
-    ext_rays = sum(s["extend_rays"] for s in stats)
-    ext_ms = sum(s["extend_ms"] for s in stats)
-    iters = sum(s["iterations"] for s in stats)
+    # the roofline's extend time: a separate instrumented render of the same passes, each
+    # extend launch bracketed by CUDA events on the engine's stream (graphs off in it)
+    inst = ctx.render(sid, spp=spp, first_pass=first, profile=1, batched=batched,
+                      film=np.zeros_like(film))[1]
+    ext_rays, ext_ms, iters = inst["extend_rays"], inst["extend_ms"], inst["iterations"]
+    film_check = None
+    if dist and rank == 0 and reduced:
+        fs = as_uint64(reduced[0].cpu().numpy())
+        img = fs[..., :3].astype(np.float64) / np.maximum(fs[..., 3:4].astype(np.float64), 1.0)
+        film_check = {"passes": spp * world, "mean_radiance": float(img.mean()),
+                      "sum_w": int(fs[..., 3].sum(dtype=np.uint64)) / 16777216.0}
 
     # e2e through the C ABI with host buffers: scene upload from pinned host memory +
-    # render + film read-back to host memory
-    film_bytes = npix * 7 * 4   # resolved float film (sum wL rgb, sum w, sum wL^2 rgb) per pixel
+    # render + film read-back to host memory: the resolved float film (sum wL rgb, sum w,
+    # sum wL^2 rgb) per pixel, or with N > 1 the exact film (4 x uint64 + 3 x float)
+    film_bytes = npix * 7 * 4 if not dist else npix * (4 * 8 + 3 * 4)
 
     def e2e_run(hscene, label):
         hscene.pin(True)
@@ -485,9 +537,11 @@ def main():
             sid2 = ctx.upload(hscene)
             ctx.set_tune(sid2, **tune)
             t_up = time.perf_counter()
-            _, st = ctx.render(sid2, spp=spp, first_pass=first, batched=batched, film=film)
             if dist:
-                reduce_film(torch.from_numpy(film).cuda(), dist)
+                fsum, fsq, st = ctx.render_fixed(sid2, spp=spp, first_pass=first, batched=batched)
+                reduce_fixed_film(torch.from_numpy(as_int64(fsum)).cuda(), torch.from_numpy(fsq).cuda(), dist)
+            else:
+                _, st = ctx.render(sid2, spp=spp, first_pass=first, batched=batched, film=film)
             t_re = time.perf_counter()
             ctx.free_scene(sid2)
             barrier()
@@ -537,6 +591,7 @@ def main():
                    "parallelism": "spp-sharded" if world > 1 else "single GPU",
                    "mode": "batched (all passes share a refilled pool of path slots)" if batched else "plain (one pass in flight)",
                    "l2": "inputs larger than L2 (scene %.2f GB resident)" % (scene_bytes / 1e9),
+                   "graphs": "per-bounce loop replayed as CUDA graphs" if tune.get("graphs") else "graphs off",
                    "tune": tune},
         "mrays_per_s": rays * world / elapsed / 1e6,
         ("plain_value" if batched else "batched_value"): other_value,
@@ -544,7 +599,9 @@ def main():
                      "frac": (achieved / peaks["hbm_gbs"]) if achieved else None, "traffic": traffic,
                      "kernel": "kExtend (closest-hit BVH4 traversal)",
                      "bytes_per_ray": bytes_per_ray, "nodes_per_ray": nodes_per_ray, "tris_per_ray": tris_per_ray,
-                     "launches": ext_launches, "ms_total": ext_ms, "peak_kind": peak_kind + " (copy bandwidth)"},
+                     "launches": ext_launches, "ms_total": ext_ms, "peak_kind": peak_kind + " (copy bandwidth)",
+                     "timed_in": "a separate instrumented render of the same %d passes (CUDA events around each "
+                                 "extend launch, graphs off); the headline steps run the CUDA-graph loop" % spp},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": int(scene_bytes),
                 "d2h_bytes_per_step": int(film_bytes)},
         "e2e_device_trees": None if e2e_dev is None else {
@@ -552,6 +609,8 @@ def main():
         "gpu_launches": int(launches_total),
         "clocks": clk,
     }
+    if film_check is not None:
+        line["reduced_film"] = film_check
     if rank == 0 and world == 1 and not args.no_traversal:
         line["traversal"] = traversal_leg(ctx)
     if rank == 0 and world == 1 and not args.no_scenes:

@@ -6,8 +6,12 @@
            its arrival time; jobs share one pool of path slots, oldest job first.
   plain  : one request at a time through gnd_gpu_render (one sample pass in flight),
            first come first served. Its time-to-image follows from each request's
-           measured render time by the single-server FIFO recurrence
-           finish_i = max(arrival_i, finish_{i-1}) + service_i.
+           render time by the single-server FIFO recurrence
+           finish_i = max(arrival_i, finish_{i-1}) + service_i. The render time is
+           measured per request (run_plain_service) or, for long streams, modelled from
+           measured renders (plain_service_model): a plain render runs its passes one
+           after another, so its time is a fixed part plus spp times a per-pass part,
+           both measured for every (scene, resolution, depth) of the stream.
 
 Per request, uniformly: scene, square resolution in {128, 256, 512, 1024}, spp in
 {4, 16, 64}, maximum depth in 8..32. Time-to-image runs from arrival to the finished
@@ -120,11 +124,48 @@ def run_plain_service(ctx, sids, integrators, reqs):
     return out
 
 
-def calibrate_capacity(ctx, sids, integrators, n=24, seed=40):
-    """Requests per second the job server sustains: n requests of the same distribution
-    submitted at once, n / makespan, timed on a second submission (the first one warms the
-    server up: its path pool, the kernels' first loads and the captured graphs)."""
+def _plain_time(ctx, sid, integrator, res, spp, depth):
+    t = time.perf_counter()
+    ctx.render(sid, spp=spp, max_depth=depth, integrator=integrator, width=res, height=res)
+    return time.perf_counter() - t
+
+
+def plain_service_model(ctx, sids, integrators, reqs, check=6):
+    """Plain (one pass in flight) render times of the requests without rendering each one:
+    for every distinct (scene, resolution, depth) of the stream a 1-pass and a 4-pass
+    plain render are timed (host wall time, as run_plain_service), giving
+    time(spp) = fixed + spp * per_pass with per_pass = (t4 - t1) / 3. `check` requests of
+    spp 16 or 64 are also rendered in full and compared with the model.
+    Returns (service times in s, dict with the model's size and its largest relative error)."""
+    keys = sorted({(r["scene"], r["res"], r["max_depth"]) for r in reqs})
+    model = {}
+    for sc, res, depth in keys:
+        sid, integ = sids[sc], integrators[sc]
+        _plain_time(ctx, sid, integ, res, 1, depth)   # warm-up (first use of this film size)
+        t1 = _plain_time(ctx, sid, integ, res, 1, depth)
+        t4 = _plain_time(ctx, sid, integ, res, 4, depth)
+        per = max((t4 - t1) / 3.0, 0.0)
+        model[(sc, res, depth)] = (max(t1 - per, 0.0), per)
+
+    def predict(r):
+        fixed, per = model[(r["scene"], r["res"], r["max_depth"])]
+        return fixed + r["spp"] * per
+
+    svc = np.array([predict(r) for r in reqs])
+    errs = []
+    big = [r for r in reqs if r["spp"] >= 16][:check]
+    for r in big:
+        meas = _plain_time(ctx, sids[r["scene"]], integrators[r["scene"]], r["res"], r["spp"], r["max_depth"])
+        errs.append(abs(predict(r) - meas) / meas)
+    return svc, {"keys": len(keys), "checked": len(errs), "max_rel_err": float(max(errs)) if errs else None}
+
+
+def calibrate_capacity(ctx, sids, integrators, n=200, warm=24, seed=40):
+    """What the job server sustains when saturated: n requests of the stream's
+    distribution submitted at once, timed from the first submission to the last film
+    (after a warm-up submission of `warm` others: the server's path pool, the kernels'
+    first loads and the captured graphs). Returns (requests/s, samples/s)."""
+    run_served(ctx, sids, integrators, make_requests(warm, seed + 1), np.zeros(warm))
     reqs = make_requests(n, seed)
-    run_served(ctx, sids, integrators, reqs, np.zeros(n))
     _, makespan = run_served(ctx, sids, integrators, reqs, np.zeros(n))
     return n / makespan, sum(samples(r) for r in reqs) / makespan

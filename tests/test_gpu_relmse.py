@@ -1,0 +1,74 @@
+"""relMSE gates at the benchmark configurations: the GPU integrators' relMSE against a
+4096-spp CPU render matches the CPU integrator's relMSE at equal spp within 5%.
+
+References (tests/relmse_refs.py): the oracle at 4096 spp over the Cornell box (256^2,
+whole image), a 128^2 window of the volumetric Cornell box (512^2, volpath depth 32, the
+glass sphere and its media) and two 64^2 windows of the microfacet grid (1024^2, depth
+16), cached under baseline/_ref/relmse/ and computed here when absent.
+
+relMSE = mean over the window's pixels and channels of (I - R)^2 / (R^2 + 0.01). Both
+sides render K = 4 images at the configuration's spp with seeds independent of each other
+and of the reference; the mean relMSE of the GPU's images must be within 5% of the
+CPU's. With the CPU's seeds the GPU renders the same sample streams: then the two relMSEs
+agree within 1% (only paths whose branch a last-ulp transcendental difference flipped
+differ)."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import gianduia_b200 as G
+from oracle import pyoracle as O
+import relmse_refs as R
+
+pytestmark = [pytest.mark.gpu, pytest.mark.timeout(1800)]
+
+K = 4
+GPU_SEED0 = 300000     # first passes of the GPU's independent renders
+CPU_SEED0 = 600000     # the CPU's (and the GPU's same-stream renders)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = G.GpuContext(0)
+    yield c
+    c.close()
+
+
+def rel_mse(img, ref):
+    return float(np.mean((img - ref) ** 2 / (ref * ref + 1e-2)))
+
+
+def crop(film, win):
+    x0, y0, x1, y1 = win
+    return G.resolve(film)[y0:y1, x0:x1]
+
+
+@pytest.mark.parametrize("name", ["cornell", "volumetric", "microfacet"])
+def test_relmse_matches_cpu(ctx, name):
+    work = tempfile.mkdtemp(prefix="gnd_relmse_")
+    refs = R.load(name)
+    if refs is None:
+        R.compute(name, work)
+        refs = R.load(name)
+    cfg = R.CONFIGS[name]
+    spp = cfg["kw"]["spp"]
+    xml = R.scene_xml(name, work)
+    sid = ctx.upload(G.HostScene.load_xml(xml))
+    osc = O.Scene.load(xml)
+    for win, ref in zip(cfg["windows"], refs):
+        g_ind, g_same, c = [], [], []
+        for k in range(K):
+            gf, _ = ctx.render(sid, spp=spp, first_pass=GPU_SEED0 + k * spp, window=win, batched=True)
+            g_ind.append(rel_mse(crop(gf, win), ref))
+            gs, _ = ctx.render(sid, spp=spp, first_pass=CPU_SEED0 + k * spp, window=win, batched=True)
+            g_same.append(rel_mse(crop(gs, win), ref))
+            of, _, _ = osc.render(CPU_SEED0 + k * spp, CPU_SEED0 + (k + 1) * spp, window=win)
+            c.append(rel_mse(crop(of, win), ref))
+        rg, rs, rc = float(np.mean(g_ind)), float(np.mean(g_same)), float(np.mean(c))
+        print("%s %s: relMSE gpu %.5g (same streams %.5g), cpu %.5g at %d spp; per render gpu %s cpu %s" % (
+            name, win, rg, rs, rc, spp, np.round(g_ind, 5).tolist(), np.round(c, 5).tolist()))
+        assert abs(rs - rc) <= 0.01 * rc, "%s %s: same-stream relMSE %g vs cpu %g" % (name, win, rs, rc)
+        assert abs(rg - rc) <= 0.05 * rc, "%s %s: relMSE gpu %g vs cpu %g (5%% bar)" % (name, win, rg, rc)
+    ctx.free_scene(sid)

@@ -8,9 +8,11 @@ Three levels:
     last-ulp difference of a transcendental function flipped a branch. Bar: median
     relative difference <= 1e-4 and >= 90% of pixels within 1e-3 relative.
   * statistics: independent seeds; per-pixel means agree within 3 combined standard
-    errors (expected 0.27% outside; the bar is 1%, failures listed).
-  * relMSE against a high-spp oracle image: the GPU's relMSE at equal spp is within 5%
-    of the CPU integrator's (plus the sampling error of the estimate itself).
+    errors. The count of pixel channels beyond that is bounded by its binomial mean plus
+    4 standard deviations at the rate a t distribution gives for standard errors
+    estimated from the render's samples (0.27% as the sample count grows); the worst
+    channels are listed on failure.
+  * relMSE against high-spp oracle images: tests/test_gpu_relmse.py.
 """
 import numpy as np
 import pytest
@@ -18,6 +20,7 @@ import pytest
 import gianduia_b200 as G
 from gianduia_b200 import scenes
 from oracle import pyoracle as O
+from statbounds import binomial_bound, t_tail
 
 pytestmark = pytest.mark.gpu
 
@@ -44,8 +47,11 @@ def same_stream_check(gimg, oimg, label, min_frac=0.90):
     return frac
 
 
-def sigma_check(gfilm, ofilm, label, limit=0.01):
-    """Per-pixel 3-sigma agreement with combined standard errors from sum L and sum L^2."""
+def sigma_check(gfilm, ofilm, label):
+    """Per-pixel 3-sigma agreement of two box-filter films with independent samples, with
+    combined standard errors from sum L and sum L^2 (n samples per pixel each). The count
+    of channels beyond 3 sigma must stay within binomial_bound at the t tail for
+    2 (n - 1) degrees of freedom. Returns (count, channels, bound)."""
     out = []
     for f in (gfilm, ofilm):
         n = np.maximum(f[..., 3:4], 1)
@@ -57,10 +63,17 @@ def sigma_check(gfilm, ofilm, label, limit=0.01):
     z = np.abs(mg - mo) / np.maximum(se, 1e-12)
     valid = se > 1e-9
     beyond = (z > 3) & valid
-    frac = float(beyond.sum()) / max(1, int(valid.sum()))
-    idx = np.argwhere(beyond)[:10].tolist()
-    assert frac <= limit, "%s: %.4f of pixel channels beyond 3 sigma (expected ~0.0027): %s" % (label, frac, idx)
-    return frac
+    nsamp = float(np.median(np.maximum(gfilm[..., 3], 1)))
+    p = t_tail(3.0, max(2.0 * (nsamp - 1.0), 1.0))
+    nvalid = int(valid.sum())
+    bound = binomial_bound(nvalid, p)
+    count = int(beyond.sum())
+    worst = np.argsort(-np.where(valid, z, 0).ravel())[:10]
+    listed = [(tuple(int(v) for v in np.unravel_index(int(i), z.shape)), round(float(z.ravel()[i]), 2)) for i in worst]
+    print("%s: %d of %d channels beyond 3 sigma (bound %d, expected %.1f)" % (label, count, nvalid, bound, nvalid * p))
+    assert count <= bound, "%s: %d of %d pixel channels beyond 3 sigma (bound %d, expected %.1f); worst: %s" % (
+        label, count, nvalid, bound, nvalid * p, listed)
+    return count, nvalid, bound
 
 
 def rel_mse(img, ref):
@@ -78,18 +91,14 @@ def test_cornell_same_stream(ctx, tmp_path):
     assert np.allclose(gfilm[..., 3], 4.0) and np.allclose(ofilm[..., 3], 4.0)
 
 
-def test_cornell_statistics_and_relmse(ctx, tmp_path):
-    W = 48
+def test_cornell_statistics(ctx, tmp_path):
+    W = 64
     xml = scenes.cornell(str(tmp_path), width=W, height=W, spp=32)
     sid = ctx.upload(G.HostScene.load_xml(xml))
     osc = O.Scene.load(xml)
     gfilm, _ = ctx.render(sid, spp=32, first_pass=100000)   # independent seeds
     ofilm, _, _ = osc.render(0, 32)
     sigma_check(gfilm, ofilm, "cornell-3sigma")
-    ref, _, _ = osc.render(200000, 200000 + 2048)
-    refimg = image(ref)
-    rg, ro = rel_mse(image(gfilm), refimg), rel_mse(image(ofilm), refimg)
-    assert abs(rg - ro) <= 0.05 * ro + 0.02 * ro, "relMSE gpu %g vs cpu %g" % (rg, ro)
 
 
 def test_volumetric_same_stream(ctx, tmp_path):
@@ -105,7 +114,7 @@ def test_volumetric_statistics(ctx, tmp_path):
     sid = ctx.upload(G.HostScene.load_xml(xml))
     gfilm, _ = ctx.render(sid, spp=64, first_pass=100000)
     ofilm, _, _ = O.Scene.load(xml).render(0, 64)
-    sigma_check(gfilm, ofilm, "volumetric-3sigma", limit=0.015)
+    sigma_check(gfilm, ofilm, "volumetric-3sigma")
 
 
 def test_batched_equals_plain(ctx, tmp_path):
