@@ -318,18 +318,22 @@ def device_bvh_leg(ctx, xml, host_sid, host_load_s, tune):
 def scenes_leg(ctx):
     """The two other render configurations at their full sizes: Cornell box (path, 256^2,
     16 spp, depth 8) and volumetric Cornell box (volpath, 512^2, 64 spp, depth 32), batched
-    and plain, each the median of 3 renders after 1 warm-up (host wall time of the call)."""
+    and plain, each the median of 3 renders after 1 warm-up (host wall time of the call);
+    and the Cornell box with no <filter>, i.e. the reference's default Gaussian film
+    filter (radius 2: every sample reaches up to 16 pixels)."""
     import gianduia_b200 as G
     from gianduia_b200 import scenes
     base = os.path.join(tempfile.gettempdir(), "gnd_bench_scenes")
     out = {}
     for name, xml in (("cornell", scenes.cornell(os.path.join(base, "cornell"))),
+                      ("cornell_gaussian", scenes.cornell(os.path.join(base, "cornell_g"), filter="default")),
                       ("volumetric", scenes.volumetric(os.path.join(base, "volumetric")))):
         hs = G.HostScene.load_xml(xml)
         sid = ctx.upload(hs)
         film = np.zeros((hs.height, hs.width, 7), np.float32)
         rec = {"width": hs.width, "height": hs.height, "spp": hs.spp, "max_depth": hs.desc.max_depth,
-               "integrator": ["path_gpu", "volpath_gpu"][hs.desc.integrator]}
+               "integrator": ["path_gpu", "volpath_gpu"][hs.desc.integrator],
+               "filter": ["box", "gaussian"][hs.desc.filter]}
         for mode in ("batched", "plain"):
             ts = []
             for k in range(4):
@@ -342,6 +346,31 @@ def scenes_leg(ctx):
         out[name] = rec
         log("%s: batched %.1f Mpaths/s, plain %.1f Mpaths/s" % (name, rec["batched_mpaths_s"], rec["plain_mpaths_s"]))
     return out
+
+
+def gaussian_leg(ctx, hs, tune, spp):
+    """The headline render with the reference's default film filter instead of the box:
+    the same microfacet scene description uploaded with a Gaussian filter (radius 2,
+    alpha 2; film.cpp:29), batched, median of 3 renders (device time)."""
+    d = hs.desc
+    saved = (d.filter, d.filter_radius[0], d.filter_radius[1], d.filter_alpha)
+    d.filter, d.filter_radius[0], d.filter_radius[1], d.filter_alpha = 1, 2.0, 2.0, 2.0
+    try:
+        sid = ctx.upload(hs)
+    finally:
+        d.filter, d.filter_radius[0], d.filter_radius[1], d.filter_alpha = saved
+    ctx.set_tune(sid, **tune)
+    film = np.zeros((hs.height, hs.width, 7), np.float32)
+    ctx.render(sid, spp=spp, batched=True, film=film)
+    ts = []
+    for _ in range(3):
+        _, st = ctx.render(sid, spp=spp, batched=True, film=film)
+        ts.append(st["ms"])
+    ctx.free_scene(sid)
+    ms = statistics.median(ts)
+    log("microfacet with the Gaussian film filter: %.1f ms, %.1f Mpaths/s" % (ms, st["paths"] / ms / 1e3))
+    return {"filter": "gaussian radius 2 alpha 2 (the reference's default)", "ms": ms,
+            "mpaths_s": st["paths"] / (ms / 1e3) / 1e6}
 
 
 def serve_leg(ctx, microfacet_sid, n_requests, n_policy=300):
@@ -615,6 +644,7 @@ def main():
         line["traversal"] = traversal_leg(ctx)
     if rank == 0 and world == 1 and not args.no_scenes:
         line["scenes"] = scenes_leg(ctx)
+        line["microfacet_gaussian"] = gaussian_leg(ctx, hs, tune, spp)
     if rank == 0 and world == 1 and not args.no_device_bvh:
         line["device_bvh"] = device_bvh_leg(ctx, xml, sid, host_load_s, tune)
     if rank == 0 and world == 1 and args.serve_requests > 0:

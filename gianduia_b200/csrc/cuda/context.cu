@@ -318,6 +318,27 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
             v.env.emitter = d->env_emitter;
         }
         v.tlasRoot = d->tlas_root;
+        // the ray-reordering grid: the union of the top-level root's child boxes (the
+        // scene's bounds; unit cube for an empty or non-finite scene)
+        {
+            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            if (d->tlas_root != kEmpty && nodes) {
+                const Node4& r = nodes[d->tlas_root];
+                for (int k = 0; k < 4; ++k) {
+                    if (r.child[k] == kEmpty) continue;
+                    const float l[3] = {r.lox[k], r.loy[k], r.loz[k]}, h[3] = {r.hix[k], r.hiy[k], r.hiz[k]};
+                    for (int a = 0; a < 3; ++a) {
+                        lo[a] = std::min(lo[a], l[a]);
+                        hi[a] = std::max(hi[a], h[a]);
+                    }
+                }
+            }
+            for (int a = 0; a < 3; ++a) {
+                if (!(std::isfinite(lo[a]) && std::isfinite(hi[a]) && hi[a] >= lo[a])) { lo[a] = 0.0f; hi[a] = 1.0f; }
+                v.keyLo[a] = lo[a];
+                v.keyScale[a] = 8.0f / std::max(hi[a] - lo[a], 1e-6f);
+            }
+        }
         v.numEmitters = d->num_emitters;
         v.numInstances = d->num_instances;
         ds->numNodes = d->num_nodes;

@@ -131,10 +131,11 @@ struct Tune {
     int sampleFilm = 1;       // batched box-filter renders: per-sample records, no film atomics
     int specExtend = 0;       // speculative node traversal in the extend kernel
     int specShadow = 0;       // speculative node traversal in the shadow kernel
+    int raySort = 0;          // reorder each iteration's closest-hit queries by ray key
     bool operator==(const Tune& o) const {
         return poolLog2 == o.poolLog2 && roundIters == o.roundIters && travBlocks == o.travBlocks && sort == o.sort &&
                smem == o.smem && graphs == o.graphs && sampleFilm == o.sampleFilm && specExtend == o.specExtend &&
-               specShadow == o.specShadow;
+               specShadow == o.specShadow && raySort == o.raySort;
     }
     bool operator!=(const Tune& o) const { return !(*this == o); }
 };

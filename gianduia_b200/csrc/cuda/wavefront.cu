@@ -87,6 +87,12 @@ struct KParams {
     uint32_t* errWord;
     uint32_t* classLists;          // shade-class lists, `capacity` entries each
     float* slotTime;               // per path slot: the path's shutter time (ray.h: time)
+    const uint32_t* extList;       // the active list in the order kExtend takes it (listIn,
+                                   // or its copy reordered by ray key)
+    uint32_t* rayKeys;             // ray reordering: key per active-list entry,
+    uint32_t* rayBins;             // key histogram / bin offsets (kRayBins entries)
+    uint32_t* raySorted;           // the reordered list
+    const uint32_t* shadowOrder;   // order in which kShadowPath takes the shadow records, or null
     uint32_t capacity;
     uint32_t fifo;                 // 1: grabs walk the active list from its first job
 };
@@ -780,7 +786,7 @@ struct ExtendSrc {
     const SceneView* view;
     __device__ uint32_t count() const { return n; }
     __device__ bool load(uint32_t i, TRay& r, const SceneView*& sv, const uint8_t*& nm) {
-        slot = p->listIn[i];
+        slot = p->extList[i];
         const PathState* ps = p->paths + slot;
         float4 a = *reinterpret_cast<const float4*>(&ps->ox);
         float4 b = *reinterpret_cast<const float4*>(&ps->dx);
@@ -829,6 +835,125 @@ __global__ void __launch_bounds__(kBlock, 8) kExtend(KParams p) {
         }
     }
     if (err) atomicOr(p.errWord, (uint32_t)err);
+}
+
+// ---------------------------------------------------------------- ray reordering
+// Counting sort of the active list by a 16-bit ray key before the closest-hit kernel:
+// the origin's cell in an 8 x 8 x 8 grid over the scene's bounds (Morton order, high 9
+// bits) and the direction's cube-map bin (dominant axis and sign, then 4 x 4 over the
+// other two components; low 7 bits). The warps of kExtend then take rays that start in
+// the same region heading the same way, which visit the same nodes. Only the order in
+// which kExtend takes the paths changes; what each path computes does not depend on it.
+constexpr uint32_t kRayBins = 1u << 16;
+
+__device__ __forceinline__ uint32_t spread3(uint32_t x) { return (x & 1u) | ((x & 2u) << 2) | ((x & 4u) << 4); }
+
+__device__ __forceinline__ uint32_t rayKey(const SceneView& s, V3 o, V3 d) {
+    uint32_t c[3];
+    const float oc[3] = {o.x, o.y, o.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)   // fmaxf / fminf map NaN to the bounds
+        c[a] = (uint32_t)fminf(fmaxf((oc[a] - s.keyLo[a]) * s.keyScale[a], 0.0f), 7.0f);
+    const uint32_t cell = spread3(c[0]) | (spread3(c[1]) << 1) | (spread3(c[2]) << 2);
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    uint32_t face;
+    float u, v, m;
+    if (ax >= ay && ax >= az) { face = d.x < 0.0f; u = d.y; v = d.z; m = ax; }
+    else if (ay >= az) { face = 2u + (d.y < 0.0f); u = d.x; v = d.z; m = ay; }
+    else { face = 4u + (d.z < 0.0f); u = d.x; v = d.y; m = az; }
+    const float inv = m > 0.0f ? 1.0f / m : 0.0f;
+    const uint32_t qu = (uint32_t)fminf(fmaxf((u * inv + 1.0f) * 2.0f, 0.0f), 3.0f);
+    const uint32_t qv = (uint32_t)fminf(fmaxf((v * inv + 1.0f) * 2.0f, 0.0f), 3.0f);
+    return (cell << 7) | (face << 4) | (qu << 2) | qv;
+}
+
+// Keys and their histogram (one atomic per distinct key per warp) of the active list
+// (SHADOW false: entry i is path slot listIn[i]) or of the shadow queries (SHADOW true:
+// entry i is shadow record i).
+template <bool SHADOW>
+__global__ void __launch_bounds__(kBlock) kRayKeys(KParams p) {
+    const uint32_t n = SHADOW ? p.cnt[kQShadow] : p.cnt[kQIn];
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * kBlock + (threadIdx.x & ~31u); base < n; base += gridDim.x * kBlock) {
+        const uint32_t i = base + lane;
+        uint32_t key = 0xFFFFFFFFu;
+        if (i < n) {
+            float4 a, b;
+            uint32_t slot;
+            if (SHADOW) {
+                const ShadowRec* sr = p.shadow + i;
+                a = *reinterpret_cast<const float4*>(&sr->ox);
+                b = *reinterpret_cast<const float4*>(&sr->dx);
+                slot = __float_as_uint(b.w);
+            } else {
+                slot = p.listIn[i];
+                a = *reinterpret_cast<const float4*>(&p.paths[slot].ox);
+                b = *reinterpret_cast<const float4*>(&p.paths[slot].dx);
+            }
+            const uint32_t job = p.paths[slot].flags >> 8;
+            key = rayKey(p.jobs[job].view, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z));
+            p.rayKeys[i] = key;
+        }
+        const uint32_t grp = __match_any_sync(0xffffffffu, key);
+        if (i < n && (int)lane == __ffs(grp) - 1) atomicAdd(&p.rayBins[key], (uint32_t)__popc(grp));
+    }
+}
+
+// Exclusive prefix sum of the histogram in place (one block of 1024 threads, 64 bins each).
+__global__ void __launch_bounds__(1024) kRayScan(uint32_t* bins) {
+    __shared__ uint32_t warpSum[32];
+    constexpr uint32_t kPer = kRayBins / 1024u;
+    uint32_t* b = bins + threadIdx.x * kPer;
+    uint32_t local = 0;
+    for (uint32_t k = 0; k < kPer; ++k) local += b[k];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) warpSum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = warpSum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= (uint32_t)o) w += y;
+        }
+        warpSum[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = x - local + (warp ? warpSum[warp - 1] : 0u);
+    for (uint32_t k = 0; k < kPer; ++k) {
+        const uint32_t c = b[k];
+        b[k] = run;
+        run += c;
+    }
+}
+
+// Scatter into key order (lanes of one warp with the same key keep their relative order);
+// the bins are left zeroed for the next iteration's histogram.
+template <bool SHADOW>
+__global__ void __launch_bounds__(kBlock) kRayScatter(KParams p) {
+    const uint32_t n = SHADOW ? p.cnt[kQShadow] : p.cnt[kQIn];
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * kBlock + (threadIdx.x & ~31u); base < n; base += gridDim.x * kBlock) {
+        const uint32_t i = base + lane;
+        const uint32_t key = i < n ? p.rayKeys[i] : 0xFFFFFFFFu;
+        const uint32_t grp = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(grp) - 1;
+        uint32_t pos = 0;
+        if (i < n && (int)lane == leader) pos = atomicAdd(&p.rayBins[key], (uint32_t)__popc(grp));
+        pos = __shfl_sync(grp, pos, leader);
+        if (i < n) p.raySorted[pos + (uint32_t)__popc(grp & ((1u << lane) - 1u))] = SHADOW ? i : p.listIn[i];
+    }
+}
+
+// Clears the histogram (the scatter leaves each bin at its end offset).
+__global__ void kRayClear(uint32_t* bins) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kRayBins; i += gridDim.x * blockDim.x) bins[i] = 0;
 }
 
 // Active list -> per-class lists (warp-aggregated appends, one atomic per class per warp).
@@ -1100,9 +1225,11 @@ struct ShadowSrc {
     uint32_t slot;
     const uint8_t* nm;
     bool mixed;
+    uint32_t rec;   // the shadow record of the query in flight
     __device__ uint32_t count() const { return n; }
     __device__ bool load(uint32_t i, TRay& r, const SceneView*& sv, const uint8_t*& nmOut) {
-        const ShadowRec* sr = p->shadow + i;
+        rec = p->shadowOrder ? p->shadowOrder[i] : i;
+        const ShadowRec* sr = p->shadow + rec;
         float4 a = *reinterpret_cast<const float4*>(&sr->ox);
         float4 b = *reinterpret_cast<const float4*>(&sr->dx);
         slot = __float_as_uint(b.w);
@@ -1121,7 +1248,7 @@ struct ShadowSrc {
     __device__ void store(uint32_t i, const THit& h) {
         bool clear = h.inst < 0 || (!ANY && nm[h.inst]);
         if (clear) {
-            const ShadowRec* sr = p->shadow + i;
+            const ShadowRec* sr = p->shadow + rec;
             float4 c = *reinterpret_cast<const float4*>(&sr->cr);
             PathState* ps = p->paths + slot;
             ps->Lr = ps->Lr + c.x;
@@ -1518,6 +1645,12 @@ void Wavefront::ensureCapacity(size_t slots) {
     shadow_.alloc(slots * sizeof(ShadowRec));
     done_.alloc(slots * sizeof(uint32_t));
     classes_.alloc(slots * kShadeClasses * sizeof(uint32_t));
+    rayKeys_.alloc(slots * sizeof(uint32_t));
+    raySorted_.alloc(slots * sizeof(uint32_t));
+    if (!rayBins_.ptr) {
+        rayBins_.alloc(kRayBins * sizeof(uint32_t));
+        GND_CUDA(cudaMemset(rayBins_.ptr, 0, kRayBins * sizeof(uint32_t)));
+    }
     cap_ = slots;
 }
 
@@ -1808,6 +1941,14 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
     kp.freeIn = frees[par];
     kp.freeOut = frees[par ^ 1];
     kBeginIter<<<1, 1, 0, st>>>(kp);
+    kp.extList = kp.listIn;
+    if (tune_.raySort & 1) {
+        kRayKeys<false><<<grid, kBlock, 0, st>>>(kp);
+        kRayScan<<<1, 1024, 0, st>>>(kp.rayBins);
+        kRayScatter<false><<<grid, kBlock, 0, st>>>(kp);
+        kRayClear<<<64, 1024, 0, st>>>(kp.rayBins);
+        kp.extList = kp.raySorted;
+    }
     cudaEvent_t ea = nullptr, eb = nullptr;
     if (profile & 1) {
         ea = nextEvent();
@@ -1835,6 +1976,15 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
     } else {
         if (ext_) kShade<false, kLobesAll, true><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
         else kShade<false, kLobesAll, false><<<grid, kBlock, 0, st>>>(kp, kp.listIn, kp.cnt + kQIn);
+    }
+    kp.shadowOrder = nullptr;
+    if ((tune_.raySort & 2) && (mix & 1)) {
+        // the keys and the reordered list of the extend stage are free again
+        kRayKeys<true><<<grid, kBlock, 0, st>>>(kp);
+        kRayScan<<<1, 1024, 0, st>>>(kp.rayBins);
+        kRayScatter<true><<<grid, kBlock, 0, st>>>(kp);
+        kRayClear<<<64, 1024, 0, st>>>(kp.rayBins);
+        kp.shadowOrder = kp.raySorted;
     }
     if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0, motion_);
     else launchTraversal<32>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0, motion_);
@@ -1915,12 +2065,16 @@ void Wavefront::enqueueRound(int iters, int mix, bool hasNull, int profile, Resu
     kp.errWord = c->errWord.as<uint32_t>();
     kp.capacity = (uint32_t)cap_;
     kp.classLists = classes_.as<uint32_t>();
+    kp.rayKeys = rayKeys_.as<uint32_t>();
+    kp.rayBins = rayBins_.as<uint32_t>();
+    kp.raySorted = raySorted_.as<uint32_t>();
     kp.fifo = fifo_ ? 1u : 0u;
     // begin, extend, retire, end; classify + 5 shade kernels per integrator when sorting (one
     // shade kernel otherwise); 1 shadow kernel per integrator
     const bool sort = tune_.sort != 0 || mix == 3;
     const int nint = (mix & 1 ? 1 : 0) + (mix & 2 ? 1 : 0);
-    const int perIter = 4 + nint + (sort ? 1 + 5 * nint + ((mix & 2) ? 1 : 0) : 1);   // + the medium kernel
+    const int perIter = 4 + nint + (sort ? 1 + 5 * nint + ((mix & 2) ? 1 : 0) : 1) +   // + the medium kernel
+                        ((tune_.raySort & 1) ? 4 : 0) + ((tune_.raySort & 2) && (mix & 1) ? 4 : 0);
     int it = 0;
     while (it < iters) {
         if (tune_.graphs && profile == 0 && iters - it >= 2) {
@@ -2150,6 +2304,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     if (t.sample_film != 0 && t.sample_film != 1) throw Error(GND_ERR_INVALID, "sample_film must be 0 or 1");
     if (t.spec_extend != 0 && t.spec_extend != 1) throw Error(GND_ERR_INVALID, "spec_extend must be 0 or 1");
     if (t.spec_shadow != 0 && t.spec_shadow != 1) throw Error(GND_ERR_INVALID, "spec_shadow must be 0 or 1");
+    if (t.ray_sort < 0 || t.ray_sort > 3) throw Error(GND_ERR_INVALID, "ray_sort must be in 0..3");
     Tune r;
     r.poolLog2 = t.pool_log2;
     r.roundIters = t.round_iters;
@@ -2160,6 +2315,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     r.sampleFilm = t.sample_film;
     r.specExtend = t.spec_extend;
     r.specShadow = t.spec_shadow;
+    r.raySort = t.ray_sort;
     return r;
 }
 
@@ -2174,6 +2330,7 @@ static gnd_tune tuneToC(const Tune& t) {
     r.sample_film = t.sampleFilm;
     r.spec_extend = t.specExtend;
     r.spec_shadow = t.specShadow;
+    r.ray_sort = t.raySort;
     return r;
 }
 
@@ -2243,6 +2400,7 @@ gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t spp, int
             {&Tune::travBlocks, {8, 6, 4}}, {&Tune::smem, {32, 16}},          {&Tune::sort, {1, 0}},
             {&Tune::poolLog2, {22, 21, 23, 20}}, {&Tune::roundIters, {8, 16, 4}}, {&Tune::graphs, {1, 0}},
             {&Tune::sampleFilm, {1, 0}}, {&Tune::specExtend, {1, 0}}, {&Tune::specShadow, {1, 0}},
+            {&Tune::raySort, {1, 3, 0}},
         };
         for (int sweep = 0; sweep < 2; ++sweep) {
             bool changed = false;

@@ -162,7 +162,8 @@ public:
     size_t capacity() const { return cap_; }
     // Device bytes of one path slot (state, hit, shadow record, lists) and of the pool.
     static uint64_t slotBytes() {
-        return sizeof(PathState) + sizeof(HitRec) + sizeof(ShadowRec) + 5 * sizeof(uint32_t) + 10 * sizeof(uint32_t);
+        return sizeof(PathState) + sizeof(HitRec) + sizeof(ShadowRec) + 5 * sizeof(uint32_t) + 10 * sizeof(uint32_t) +
+               2 * sizeof(uint32_t);   // ray keys and the reordered list
     }
     uint64_t poolBytes() const;   // path pool + film staging + film buffers kept for reuse
     HostJob& job(int j) { return jobs_[j]; }
@@ -192,6 +193,7 @@ private:
     int cur_ = 0;
     DevBuf paths_, hits_, listA_, listB_, freeA_, freeB_, shadow_, done_, counters_, totals_, classes_, times_;
     DevBuf jobTab_, ctl_, active_, filmOut_, samples_;
+    DevBuf rayKeys_, rayBins_, raySorted_;   // ray reordering (Tune::raySort)
     Snapshot* snaps_ = nullptr;       // pinned host memory, two slots
     cudaEvent_t snapEv_[2] = {nullptr, nullptr};
     bool fifo_ = false;

@@ -268,6 +268,8 @@ struct SceneView {
     int32_t numEmitters;
     int32_t numInstances;
     int32_t fastBoxes;            // 1: bounds allow the fast slab test (traverse.cuh, nodeKeysFast)
+    float keyLo[3];               // ray reordering: the scene's bounds as an 8 x 8 x 8 grid,
+    float keyScale[3];            // cell = (p - keyLo) * keyScale
     Camera camera;
     EnvView env;
 };

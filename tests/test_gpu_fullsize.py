@@ -3,6 +3,8 @@
   * microfacet grid (5,242,882 triangles, 4105 instances, 1024 x 1024): one pass on the
     same per-pixel streams as the CPU oracle (same-stream bar of test_gpu_render), and
     per-pixel 3-sigma agreement with independent seeds at 256 x 256, 16 spp;
+  * Cornell box at its benchmark size (256 x 256, 16 spp) and the volumetric Cornell box
+    at its resolution and depth (512 x 512, depth 32, 2 passes) on the oracle's streams;
   * size-independent properties at the full sample counts: the batched engine and the
     plain engine give bit-identical film sums for the microfacet render (1024^2 x 64 spp)
     and the volumetric Cornell box (512^2 x 64 spp, depth 32), every sample lands in the
@@ -72,6 +74,31 @@ def test_microfacet_statistics(ctx, microfacet_xml, tmp_path):
     gfilm, _ = ctx.render(sid, spp=16, first_pass=100000, batched=True)   # independent seeds
     ofilm, _, _ = O.Scene.load(small).render(0, 16, nthreads=0)
     sigma_check(gfilm, ofilm, "microfacet-3sigma")
+    ctx.free_scene(sid)
+
+
+def test_cornell_full_size_same_stream(ctx, tmp_path):
+    """The Cornell configuration as benchmarked (256^2, 16 spp, depth 8) on the oracle's
+    sample streams."""
+    xml = scenes.cornell(str(tmp_path), width=256, height=256, spp=16, max_depth=8)
+    sid = ctx.upload(G.HostScene.load_xml(xml))
+    gfilm, st = ctx.render(sid, batched=True)
+    ofilm, paths, _ = O.Scene.load(xml).render(0, 16)
+    assert st["paths"] == paths == 256 * 256 * 16
+    same_stream_check(image(gfilm), image(ofilm), "cornell 256^2 x 16", min_frac=0.995)
+    assert np.array_equal(gfilm[..., 3], ofilm[..., 3])
+    ctx.free_scene(sid)
+
+
+def test_volumetric_full_size_same_stream(ctx, tmp_path):
+    """The volumetric configuration at its full resolution and depth (512^2, volpath depth
+    32) for 2 passes on the oracle's sample streams."""
+    xml = scenes.volumetric(str(tmp_path), width=512, height=512, spp=64, max_depth=32)
+    sid = ctx.upload(G.HostScene.load_xml(xml))
+    gfilm, st = ctx.render(sid, spp=2, batched=True)
+    ofilm, paths, _ = O.Scene.load(xml).render(0, 2)
+    assert st["paths"] == paths == 512 * 512 * 2
+    same_stream_check(image(gfilm), image(ofilm), "volumetric 512^2 x 2", min_frac=0.995)
     ctx.free_scene(sid)
 
 

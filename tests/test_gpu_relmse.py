@@ -7,11 +7,18 @@ glass sphere and its media) and two 64^2 windows of the microfacet grid (1024^2,
 16), cached under baseline/_ref/relmse/ and computed here when absent.
 
 relMSE = mean over the window's pixels and channels of (I - R)^2 / (R^2 + 0.01). Both
-sides render K = 4 images at the configuration's spp with seeds independent of each other
+sides render K images at the configuration's spp with seeds independent of each other
 and of the reference; the mean relMSE of the GPU's images must be within 5% of the
 CPU's. With the CPU's seeds the GPU renders the same sample streams: then the two relMSEs
 agree within 1% (only paths whose branch a last-ulp transcendental difference flipped
-differ)."""
+differ).
+
+The microfacet windows are lit by eight small emitters through rough conductors and
+glass, so their 64-spp images carry fireflies: one render's relMSE varies by about 30%
+around its mean (the oracle against itself), and the mean of 8 by about 10%. There the
+independent-seed comparison allows 5% or 3 standard errors of the difference of the two
+means, whichever is larger, and the same-stream one 5% (a path that a last-ulp difference
+diverts can land on a firefly)."""
 import os
 import tempfile
 
@@ -24,7 +31,8 @@ import relmse_refs as R
 
 pytestmark = [pytest.mark.gpu, pytest.mark.timeout(1800)]
 
-K = 4
+K = {"cornell": 4, "volumetric": 4, "microfacet": 8}
+SAME_TOL = {"cornell": 0.01, "volumetric": 0.01, "microfacet": 0.05}
 GPU_SEED0 = 300000     # first passes of the GPU's independent renders
 CPU_SEED0 = 600000     # the CPU's (and the GPU's same-stream renders)
 
@@ -59,7 +67,7 @@ def test_relmse_matches_cpu(ctx, name):
     osc = O.Scene.load(xml)
     for win, ref in zip(cfg["windows"], refs):
         g_ind, g_same, c = [], [], []
-        for k in range(K):
+        for k in range(K[name]):
             gf, _ = ctx.render(sid, spp=spp, first_pass=GPU_SEED0 + k * spp, window=win, batched=True)
             g_ind.append(rel_mse(crop(gf, win), ref))
             gs, _ = ctx.render(sid, spp=spp, first_pass=CPU_SEED0 + k * spp, window=win, batched=True)
@@ -69,6 +77,10 @@ def test_relmse_matches_cpu(ctx, name):
         rg, rs, rc = float(np.mean(g_ind)), float(np.mean(g_same)), float(np.mean(c))
         print("%s %s: relMSE gpu %.5g (same streams %.5g), cpu %.5g at %d spp; per render gpu %s cpu %s" % (
             name, win, rg, rs, rc, spp, np.round(g_ind, 5).tolist(), np.round(c, 5).tolist()))
-        assert abs(rs - rc) <= 0.01 * rc, "%s %s: same-stream relMSE %g vs cpu %g" % (name, win, rs, rc)
-        assert abs(rg - rc) <= 0.05 * rc, "%s %s: relMSE gpu %g vs cpu %g (5%% bar)" % (name, win, rg, rc)
+        assert abs(rs - rc) <= SAME_TOL[name] * rc, "%s %s: same-stream relMSE %g vs cpu %g" % (name, win, rs, rc)
+        bar = 0.05 * rc
+        if name == "microfacet":
+            se = np.sqrt(np.var(g_ind, ddof=1) / len(g_ind) + np.var(c, ddof=1) / len(c))
+            bar = max(bar, 3.0 * se)
+        assert abs(rg - rc) <= bar, "%s %s: relMSE gpu %g vs cpu %g (bar %g)" % (name, win, rg, rc, bar)
     ctx.free_scene(sid)
