@@ -1398,6 +1398,10 @@ __device__ __forceinline__ void filmSplat(const JobDev& j, const PathState& ps) 
 // test select (film.h:26-69). Such a sample is stored as (L.r, L.g, L.b, 1) at its work
 // item and added to the film later by kFilmFromSamples; a sample on a whole coordinate
 // (it also reaches a neighbouring pixel) is splatted with atomics as before.
+//
+// With the Gaussian filter every sample is recorded, with its film position within its
+// pixel (fx - x, fy - y: exact, as fx lies in [x, x + 1]), and kFilmFromSamplesGauss
+// gathers the records of each pixel's neighbourhood.
 template <bool EXT>
 __device__ __forceinline__ void sampleRecord(const JobDev& j, const PathState& ps) {
     const int ww = j.wx1 - j.wx0;
@@ -1406,7 +1410,7 @@ __device__ __forceinline__ void sampleRecord(const JobDev& j, const PathState& p
     Rng r = rngSeed(key);
     const V2 s2 = next2D(r);
     const float fx = (float)x + s2.x, fy = (float)y + s2.y;
-    if (fx == floorf(fx) || fy == floorf(fy)) {
+    if (j.filter == 0 && (fx == floorf(fx) || fy == floorf(fy))) {
         filmSplat<EXT>(j, ps);
         return;
     }
@@ -1416,6 +1420,62 @@ __device__ __forceinline__ void sampleRecord(const JobDev& j, const PathState& p
     const uint64_t npix = (uint64_t)ww * (uint64_t)(j.wy1 - j.wy0);
     const uint64_t item = (uint64_t)(ps.pass - (uint32_t)j.firstPass) * npix + ps.pixel;
     j.samples[item] = make_float4(L.x, L.y, L.z, 1.0f);
+    if (j.filter != 0) j.sampleOff[item] = make_float2(fx - (float)x, fy - (float)y);
+}
+
+// The Gaussian film from per-sample records: one thread per film pixel that the window's
+// samples can reach (the window grown by the filter radius, inside the film). For every
+// recorded sample of the pixels around it, the same test and weight as filmSplat: the
+// pixel must lie in the sample's [ceil(f - r - 0.5), floor(f + r - 0.5)] range on both
+// axes (film.h:37-40), w = max(0, exp(-a dx^2) - e_x) * max(0, exp(-a dy^2) - e_y)
+// (filter.h:43-47), and w > 0. The fixed-point sums equal the atomic splat's; the float
+// sum of wL^2 is taken in a fixed order (source pixel, then pass).
+__global__ void kFilmFromSamplesGauss(JobDev j, uint32_t passes) {
+    const int ww = j.wx1 - j.wx0, wh = j.wy1 - j.wy0;
+    const uint64_t npix = (uint64_t)ww * (uint64_t)wh;
+    const int Rx = (int)ceilf(j.frx) + 1, Ry = (int)ceilf(j.fry) + 1;
+    const int tx0 = max(0, j.wx0 - Rx), tx1 = min(j.W, j.wx1 + Rx);
+    const int ty0 = max(0, j.wy0 - Ry), ty1 = min(j.H, j.wy1 + Ry);
+    const uint64_t tw = (uint64_t)max(tx1 - tx0, 0), nt = tw * (uint64_t)max(ty1 - ty0, 0);
+    for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < nt; q += (uint64_t)gridDim.x * blockDim.x) {
+        const int px = tx0 + (int)(q % tw), py = ty0 + (int)(q / tw);
+        unsigned long long sr = 0, sg = 0, sb = 0, sw = 0;
+        float qr = 0.0f, qg = 0.0f, qb = 0.0f;
+        for (int sy = max(py - Ry, j.wy0); sy <= min(py + Ry, j.wy1 - 1); ++sy) {
+            for (int sx = max(px - Rx, j.wx0); sx <= min(px + Rx, j.wx1 - 1); ++sx) {
+                const uint64_t src = (uint64_t)(sy - j.wy0) * (uint64_t)ww + (uint64_t)(sx - j.wx0);
+                for (uint32_t k = 0; k < passes; ++k) {
+                    const uint64_t item = (uint64_t)k * npix + src;
+                    const float4 rec = j.samples[item];
+                    if (rec.w == 0.0f) continue;
+                    const float2 off = j.sampleOff[item];
+                    const float fx = (float)sx + off.x, fy = (float)sy + off.y;
+                    if (px < max(0, (int)ceilf(fx - j.frx - 0.5f)) || px > min(j.W - 1, (int)floorf(fx + j.frx - 0.5f))) continue;
+                    if (py < max(0, (int)ceilf(fy - j.fry - 0.5f)) || py > min(j.H - 1, (int)floorf(fy + j.fry - 0.5f))) continue;
+                    const float ox = fx - ((float)px + 0.5f), oy = fy - ((float)py + 0.5f);
+                    const float gx = fmaxf_(0.0f, expf(-j.falpha * ox * ox) - j.fexpX);
+                    const float gy = fmaxf_(0.0f, expf(-j.falpha * oy * oy) - j.fexpY);
+                    const float w = gx * gy;
+                    if (!(w > 0.0f)) continue;
+                    sr += toFixed(rec.x * w);
+                    sg += toFixed(rec.y * w);
+                    sb += toFixed(rec.z * w);
+                    sw += toFixed(w);
+                    qr += rec.x * rec.x * w;
+                    qg += rec.y * rec.y * w;
+                    qb += rec.z * rec.z * w;
+                }
+            }
+        }
+        const size_t idx = (size_t)py * (size_t)j.W + (size_t)px;
+        j.filmSum[idx * 4 + 0] += sr;
+        j.filmSum[idx * 4 + 1] += sg;
+        j.filmSum[idx * 4 + 2] += sb;
+        j.filmSum[idx * 4 + 3] += sw;
+        j.filmSq[idx * 3 + 0] += qr;
+        j.filmSq[idx * 3 + 1] += qg;
+        j.filmSq[idx * 3 + 2] += qb;
+    }
 }
 
 // Adds the per-sample records of `passes` passes into the job's film: one thread per
@@ -1806,8 +1866,14 @@ void Wavefront::useSampleRecords(int j, uint64_t items) {
     GND_CUDA(cudaMemsetAsync(samples_.ptr, 0, items * sizeof(float4), st));
     HostJob& hj = jobs_[j];
     hj.dev.samples = samples_.as<float4>();
-    // pageable source: the copy is staged before the call returns
+    hj.dev.sampleOff = nullptr;
+    if (hj.dev.filter != 0) {
+        sampleOff_.ensure(items * sizeof(float2));
+        hj.dev.sampleOff = sampleOff_.as<float2>();
+    }
+    // pageable sources: the copies are staged before the call returns
     GND_CUDA(cudaMemcpyAsync(&jobTab_.as<JobDev>()[j].samples, &hj.dev.samples, sizeof(float4*), cudaMemcpyHostToDevice, st));
+    GND_CUDA(cudaMemcpyAsync(&jobTab_.as<JobDev>()[j].sampleOff, &hj.dev.sampleOff, sizeof(float2*), cudaMemcpyHostToDevice, st));
 }
 
 void Wavefront::filmFromSamples(int j, uint64_t items) {
@@ -1815,6 +1881,13 @@ void Wavefront::filmFromSamples(int j, uint64_t items) {
     const uint64_t npix = (uint64_t)(jd.wx1 - jd.wx0) * (uint64_t)(jd.wy1 - jd.wy0);
     if (!jd.samples || npix == 0) return;
     const uint32_t passes = (uint32_t)(items / npix);
+    if (jd.filter != 0) {
+        const int grid = (int)std::min<uint64_t>(((uint64_t)jd.W * jd.H + 255) / 256, (uint64_t)ctx_->numSMs * 16);
+        kFilmFromSamplesGauss<<<std::max(grid, 1), 256, 0, ctx_->stream>>>(jd, passes);
+        ++launches_;
+        GND_CUDA(cudaGetLastError());
+        return;
+    }
     const int grid = (int)std::min<uint64_t>((npix + 255) / 256, (uint64_t)ctx_->numSMs * 16);
     kFilmFromSamples<<<std::max(grid, 1), 256, 0, ctx_->stream>>>(jd, passes);
     ++launches_;
@@ -2122,9 +2195,9 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
     reset(slots);
     const int j = admit(ds, W, H, spp, firstPass, maxDepth, integrator, window, batched ? total : npix);
     const int mix = integrator == 1 ? 2 : 1;
-    // batched renders with the box filter keep per-sample records instead of film atomics
-    // (at most 2^30 records: 16 GiB)
-    const bool records = batched && tune_.sampleFilm && ds.filter == 0 && total <= (1ull << 30);
+    // batched renders keep per-sample records instead of film atomics (at most 2^30
+    // records: 16 GiB, and 8 GiB more of film positions with the Gaussian filter)
+    const bool records = batched && tune_.sampleFilm && total <= (1ull << 30);
     if (records) {
         try {
             useSampleRecords(j, total);

@@ -55,9 +55,11 @@ struct JobDev {
     int32_t hasNull;
     int32_t firstPass;
     uint64_t workBegin, workEnd;   // work items [begin, end): item -> (pass, window pixel)
-    // Per-sample film records (batched renders with the 0.5-radius box filter), indexed by
-    // work item; null: finished samples are splatted into the film with atomics.
+    // Per-sample film records (batched renders), indexed by work item; null: finished
+    // samples are splatted into the film with atomics. With the Gaussian filter each
+    // record also keeps its film position within its pixel (sampleOff).
     float4* samples;
+    float2* sampleOff;
 };
 
 // Queue counters (device): ints.
@@ -192,7 +194,7 @@ private:
     size_t cap_ = 0;
     int cur_ = 0;
     DevBuf paths_, hits_, listA_, listB_, freeA_, freeB_, shadow_, done_, counters_, totals_, classes_, times_;
-    DevBuf jobTab_, ctl_, active_, filmOut_, samples_;
+    DevBuf jobTab_, ctl_, active_, filmOut_, samples_, sampleOff_;
     DevBuf rayKeys_, rayBins_, raySorted_;   // ray reordering (Tune::raySort)
     Snapshot* snaps_ = nullptr;       // pinned host memory, two slots
     cudaEvent_t snapEv_[2] = {nullptr, nullptr};

@@ -390,9 +390,10 @@ typedef struct gnd_tune {
     int32_t material_sort;    /* 1: classify hits and shade per material class; 0: one kernel */
     int32_t stack_smem;       /* traversal stack entries in shared memory: 16 or 32 */
     int32_t graphs;           /* 1: replay pairs of iterations as CUDA graphs */
-    int32_t sample_film;      /* 1: batched renders with the box filter write one record per
-                                 sample and build the film from them afterwards (no film
-                                 atomics; needs 16 bytes of HBM per sample); 0: atomics */
+    int32_t sample_film;      /* 1: batched renders write one record per sample and build the
+                                 film from them afterwards (no film atomics; 16 bytes of HBM
+                                 per sample, 24 with the Gaussian filter, whose film is then
+                                 gathered per pixel from the records around it); 0: atomics */
     int32_t spec_extend;      /* 1: closest-hit traversal lets a ray that holds a leaf keep
                                  visiting inner nodes until it is blocked (speculative);
                                  default 0 */
