@@ -12,6 +12,9 @@
                                                 (volpath_gpu, depth 32), `spp` passes
                                                 (default 1), plain unless `batched`
   python -m gianduia_b200.profile_run all       trace, then render
+
+Arguments of the form name=value (gnd_tune fields, e.g. ray_sort=3) set the rendered
+scene's engine settings.
 """
 import os
 import sys
@@ -30,35 +33,42 @@ def run_trace(ctx):
     ctx.free_scene(sid)
 
 
-def run_render(ctx, batched=False, spp=1):
+def run_render(ctx, batched=False, spp=1, tune=None):
     xml = scenes.microfacet(os.path.join(tempfile.gettempdir(), "gnd_bench_microfacet_r0"), width=1024, height=1024,
                             spp=64, max_depth=16, grid=64, seed=2)
     sid = ctx.upload(G.HostScene.load_xml(xml))
+    if tune:
+        ctx.set_tune(sid, **tune)
     _, st = ctx.render(sid, spp=spp, batched=batched)
     print("render:", st)
     ctx.free_scene(sid)
 
 
-def run_volpath(ctx, spp=1, batched=False):
+def run_volpath(ctx, spp=1, batched=False, tune=None):
     xml = scenes.volumetric(os.path.join(tempfile.gettempdir(), "gnd_prof_volumetric"), width=512, height=512, spp=64,
                             max_depth=32)
     sid = ctx.upload(G.HostScene.load_xml(xml))
+    if tune:
+        ctx.set_tune(sid, **tune)
     _, st = ctx.render(sid, spp=spp, batched=batched)
     print("volpath:", st)
     ctx.free_scene(sid)
 
 
 def main(argv):
+    tune = {k: int(v) for k, v in (a.split("=", 1) for a in argv[1:] if "=" in a)}
+    argv = [a for a in argv if "=" not in a]
     what = argv[1] if len(argv) > 1 else "all"
     ctx = G.GpuContext(0)
     if what in ("trace", "all"):
         run_trace(ctx)
     if what in ("render", "all"):
-        run_render(ctx)
+        run_render(ctx, tune=tune)
     if what == "batched":
-        run_render(ctx, batched=True, spp=int(argv[2]) if len(argv) > 2 else 1)
+        run_render(ctx, batched=True, spp=int(argv[2]) if len(argv) > 2 else 1, tune=tune)
     if what == "volpath":
-        run_volpath(ctx, spp=int(argv[2]) if len(argv) > 2 else 1, batched=len(argv) > 3 and argv[3] == "batched")
+        run_volpath(ctx, spp=int(argv[2]) if len(argv) > 2 else 1, batched=len(argv) > 3 and argv[3] == "batched",
+                    tune=tune)
     ctx.close()
 
 
