@@ -14,7 +14,8 @@
   python -m gianduia_b200.profile_run all       trace, then render
 
 Arguments of the form name=value (gnd_tune fields, e.g. ray_sort=3) set the rendered
-scene's engine settings.
+scene's engine settings; `gaussian` renders the microfacet scene with the reference's
+default Gaussian film filter (radius 2, alpha 2) instead of its box filter.
 """
 import os
 import sys
@@ -33,10 +34,14 @@ def run_trace(ctx):
     ctx.free_scene(sid)
 
 
-def run_render(ctx, batched=False, spp=1, tune=None):
+def run_render(ctx, batched=False, spp=1, tune=None, gaussian=False):
     xml = scenes.microfacet(os.path.join(tempfile.gettempdir(), "gnd_bench_microfacet_r0"), width=1024, height=1024,
                             spp=64, max_depth=16, grid=64, seed=2)
-    sid = ctx.upload(G.HostScene.load_xml(xml))
+    hs = G.HostScene.load_xml(xml)
+    if gaussian:
+        d = hs.desc
+        d.filter, d.filter_radius[0], d.filter_radius[1], d.filter_alpha = 1, 2.0, 2.0, 2.0
+    sid = ctx.upload(hs)
     if tune:
         ctx.set_tune(sid, **tune)
     _, st = ctx.render(sid, spp=spp, batched=batched)
@@ -57,7 +62,8 @@ def run_volpath(ctx, spp=1, batched=False, tune=None):
 
 def main(argv):
     tune = {k: int(v) for k, v in (a.split("=", 1) for a in argv[1:] if "=" in a)}
-    argv = [a for a in argv if "=" not in a]
+    gaussian = "gaussian" in argv
+    argv = [a for a in argv if "=" not in a and a != "gaussian"]
     what = argv[1] if len(argv) > 1 else "all"
     ctx = G.GpuContext(0)
     if what in ("trace", "all"):
@@ -65,7 +71,7 @@ def main(argv):
     if what in ("render", "all"):
         run_render(ctx, tune=tune)
     if what == "batched":
-        run_render(ctx, batched=True, spp=int(argv[2]) if len(argv) > 2 else 1, tune=tune)
+        run_render(ctx, batched=True, spp=int(argv[2]) if len(argv) > 2 else 1, tune=tune, gaussian=gaussian)
     if what == "volpath":
         run_volpath(ctx, spp=int(argv[2]) if len(argv) > 2 else 1, batched=len(argv) > 3 and argv[3] == "batched",
                     tune=tune)
