@@ -188,8 +188,14 @@ def traversal_leg(ctx):
     st = strm.cuda_stream
     out = {"workload": "2^20 random triangles (centroids U[0,1]^3, vertex offsets N(0, 0.01^2)), 2^24 rays "
                        "(origins U[-0.5,1.5]^3, uniform directions, tmax inf)"}
-    for name, fn in [("closest", lambda: ctx.trace_closest_dev(sid, dr.data_ptr(), n, dh.data_ptr(), st)),
-                     ("any", lambda: ctx.trace_any_dev(sid, dr.data_ptr(), n, docc.data_ptr(), st))]:
+    runs = [("closest", lambda: ctx.trace_closest_dev(sid, dr.data_ptr(), n, dh.data_ptr(), st)),
+            ("any", lambda: ctx.trace_any_dev(sid, dr.data_ptr(), n, docc.data_ptr(), st)),
+            ("closest_key_order", lambda: ctx.trace_closest_dev(sid, dr.data_ptr(), n, dh.data_ptr(), st)),
+            ("any_key_order", lambda: ctx.trace_any_dev(sid, dr.data_ptr(), n, docc.data_ptr(), st))]
+    for name, fn in runs:
+        # the last two: the batch traversed in ray-key order (gnd_tune ray_sort bit 2),
+        # the reordering inside the timed region
+        ctx.set_tune(sid, ray_sort=4 if name.endswith("key_order") else 0)
         for _ in range(2):
             fn()
         torch.cuda.synchronize()
@@ -204,6 +210,7 @@ def traversal_leg(ctx):
         ms = float(statistics.median(ts))
         out[name + "_ms"] = ms
         out[name + "_mrays_s"] = n / ms / 1e3
+    ctx.set_tune(sid, ray_sort=0)
     nodes = torch.zeros(n, dtype=torch.int32, device="cuda")
     tris = torch.zeros(n, dtype=torch.int32, device="cuda")
     ctx.trace_count_dev(sid, dr.data_ptr(), n, nodes.data_ptr(), tris.data_ptr(), st)
@@ -222,8 +229,12 @@ def traversal_leg(ctx):
     ctx.free_scene(sid)
     del dr, dh, docc, nodes, tris
     torch.cuda.empty_cache()
-    log("traversal: closest %.0f Mrays/s, any %.0f Mrays/s; %.1f nodes %.1f tris per ray; %.0f GB/s = %.2f of L2 %.0f GB/s" % (
-        out["closest_mrays_s"], out["any_mrays_s"], npr, tpr, achieved, achieved / l2, l2))
+    out["key_order_closest_achieved_gbs"] = bytes_per_ray * n / (out["closest_key_order_ms"] * 1e-3) / 1e9
+    out["key_order_frac_of_l2"] = out["key_order_closest_achieved_gbs"] / l2
+    log("traversal: closest %.0f Mrays/s (key order %.0f), any %.0f Mrays/s (key order %.0f); %.1f nodes %.1f tris "
+        "per ray; %.0f GB/s = %.2f of L2 %.0f GB/s (key order %.2f)" % (
+            out["closest_mrays_s"], out["closest_key_order_mrays_s"], out["any_mrays_s"], out["any_key_order_mrays_s"],
+            npr, tpr, achieved, achieved / l2, l2, out["key_order_frac_of_l2"]))
     return out
 
 

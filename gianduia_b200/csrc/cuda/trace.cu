@@ -3,6 +3,7 @@
 #include <mutex>
 #include <string>
 
+#include "raysort.cuh"
 #include "runtime.h"
 #include "traverse.cuh"
 
@@ -11,7 +12,9 @@ namespace gnd {
 constexpr int kTraceBlock = 128;
 constexpr int kTraceBlocksPerSM = 8;
 
-// Ray batch source / sink for the persistent traversal loop.
+// Ray batch source / sink for the persistent traversal loop. With `perm` (a batch
+// reordered by ray key) the loop's i-th ray is ray perm[i] of the batch, and its result
+// goes to slot perm[i].
 template <bool ANY, bool COUNT>
 struct BatchSrc {
     const SceneView* sv;
@@ -22,9 +25,11 @@ struct BatchSrc {
     uint32_t* nodesOut;
     uint32_t* trisOut;
     TraceCounters* cnt;
+    const uint32_t* perm;
     unsigned long long sumNodes = 0, sumTris = 0;   // COUNT: this lane's rays, for the context totals
     __device__ uint32_t count() const { return n; }
-    __device__ bool load(uint32_t i, TRay& r, const SceneView*& s, const uint8_t*& nm) {
+    __device__ bool load(uint32_t k, TRay& r, const SceneView*& s, const uint8_t*& nm) {
+        const uint32_t i = perm ? __ldg(perm + k) : k;
         float4 a = __ldg(reinterpret_cast<const float4*>(rays + i));
         float4 b = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
         r.o = v3(a.x, a.y, a.z);
@@ -36,7 +41,8 @@ struct BatchSrc {
         if (COUNT) { cnt->nodes = 0; cnt->tris = 0; }
         return true;
     }
-    __device__ void store(uint32_t i, const THit& h) {
+    __device__ void store(uint32_t k, const THit& h) {
+        const uint32_t i = perm ? __ldg(perm + k) : k;
         if (COUNT) {
             nodesOut[i] = cnt->nodes;
             trisOut[i] = cnt->tris;
@@ -60,10 +66,10 @@ template <bool ANY, bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock, kTraceBlocksPerSM)
     traceKernel(const SceneView* __restrict__ sv, const gnd_ray* __restrict__ rays, uint32_t n, gnd_hit* __restrict__ hits,
                 uint8_t* __restrict__ occ, uint32_t* __restrict__ nodesOut, uint32_t* __restrict__ trisOut,
-                uint32_t* fetch, uint32_t* errWord, unsigned long long* totals) {
+                uint32_t* fetch, uint32_t* errWord, unsigned long long* totals, const uint32_t* __restrict__ perm) {
     __shared__ uint32_t stack[kSmemStack * kTraceBlock];
     TraceCounters cnt{0, 0};
-    BatchSrc<ANY, COUNT> src{sv, rays, n, hits, occ, nodesOut, trisOut, &cnt};
+    BatchSrc<ANY, COUNT> src{sv, rays, n, hits, occ, nodesOut, trisOut, &cnt, perm};
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&totals[kTraceTotalRays], (unsigned long long)n);
         if (COUNT) atomicAdd(&totals[kTraceTotalCountedRays], (unsigned long long)n);
@@ -83,7 +89,44 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceBlocksPerSM)
     if (err) atomicOr(errWord, (uint32_t)err);
 }
 
+// Keys of a ray batch and their histogram (raysort.cuh).
+__global__ void __launch_bounds__(256) kBatchKeys(const SceneView* __restrict__ sv, const gnd_ray* __restrict__ rays,
+                                                  uint32_t n, uint32_t* __restrict__ keys, uint32_t* bins) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + lane;
+        uint32_t key = 0xFFFFFFFFu;
+        if (i < n) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(rays + i));
+            const float4 b = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
+            key = rayKey(*sv, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z));
+            keys[i] = key;
+        }
+        const uint32_t grp = __match_any_sync(0xffffffffu, key);
+        if (i < n && (int)lane == __ffs(grp) - 1) atomicAdd(&bins[key], (uint32_t)__popc(grp));
+    }
+}
+
+// The batch's permutation in key order (rays of one warp with the same key keep their order).
+__global__ void __launch_bounds__(256) kBatchScatter(const uint32_t* __restrict__ keys, uint32_t n, uint32_t* bins,
+                                                     uint32_t* __restrict__ perm) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + lane;
+        const uint32_t key = i < n ? keys[i] : 0xFFFFFFFFu;
+        const uint32_t grp = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(grp) - 1;
+        uint32_t pos = 0;
+        if (i < n && (int)lane == leader) pos = atomicAdd(&bins[key], (uint32_t)__popc(grp));
+        pos = __shfl_sync(grp, pos, leader);
+        if (i < n) perm[pos + (uint32_t)__popc(grp & ((1u << lane) - 1u))] = i;
+    }
+}
+
 namespace {
+// Batches of at least this many rays are reordered when the scene's ray_sort has bit 2.
+constexpr int64_t kBatchSortMin = 1 << 16;
+
 void launchTrace(Context* c, DeviceScene& ds, const gnd_ray* dr, int64_t n, gnd_hit* dh, uint8_t* docc,
                  uint32_t* dn, uint32_t* dt, cudaStream_t st) {
     if (n <= 0) return;
@@ -96,9 +139,25 @@ void launchTrace(Context* c, DeviceScene& ds, const gnd_ray* dr, int64_t n, gnd_
     const SceneView* sv = ds.viewDev.as<SceneView>();
     uint32_t nn = (uint32_t)n;
     unsigned long long* tot = c->traceTotals.as<unsigned long long>();
-    if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, nullptr, dn, dt, fetch, ew, tot);
-    else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew, tot);
-    else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew, tot);
+    // Reordering: scratch from the stream-ordered pool on the batch's own stream, so
+    // batches queued on different streams never share it; freed behind the traversal.
+    PoolBuf keys, perm, bins;
+    const uint32_t* order = nullptr;
+    if ((ds.tune.raySort & 4) && n >= kBatchSortMin) {
+        keys = PoolBuf((size_t)n * sizeof(uint32_t), st);
+        perm = PoolBuf((size_t)n * sizeof(uint32_t), st);
+        bins = PoolBuf(kRayBins * sizeof(uint32_t), st);
+        GND_CUDA(cudaMemsetAsync(bins.ptr, 0, kRayBins * sizeof(uint32_t), st));
+        const int kg = (int)std::min<int64_t>((n + 255) / 256, (int64_t)c->numSMs * 8);
+        kBatchKeys<<<kg, 256, 0, st>>>(sv, dr, nn, keys.as<uint32_t>(), bins.as<uint32_t>());
+        kRayScan<<<1, 1024, 0, st>>>(bins.as<uint32_t>());
+        kBatchScatter<<<kg, 256, 0, st>>>(keys.as<uint32_t>(), nn, bins.as<uint32_t>(), perm.as<uint32_t>());
+        GND_CUDA(cudaGetLastError());
+        order = perm.as<uint32_t>();
+    }
+    if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, nullptr, dn, dt, fetch, ew, tot, order);
+    else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew, tot, order);
+    else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew, tot, order);
     GND_CUDA(cudaGetLastError());
     c->counters.trace_batches += 1;
 }
@@ -240,7 +299,7 @@ gnd_status gnd_gpu_trace_closest_fixed(gnd_gpu_ctx* ctxh, gnd_scene_id id, const
         int g = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)c->numSMs * kTraceBlocksPerSM));
         traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(ds.viewDev.as<SceneView>(), dr, (uint32_t)n, dh, nullptr,
                                                              nullptr, nullptr, fetch, c->errWord.as<uint32_t>(),
-                                                             c->traceTotals.as<unsigned long long>());
+                                                             c->traceTotals.as<unsigned long long>(), nullptr);
         GND_CUDA(cudaGetLastError());
         c->counters.trace_batches += 1;
         GND_CUDA(cudaMemcpyAsync(hits, dh, sizeof(gnd_hit) * (size_t)n, cudaMemcpyDeviceToHost, st));

@@ -20,6 +20,7 @@
 #include <chrono>
 #include <cstring>
 
+#include "raysort.cuh"
 #include "shading.cuh"
 #include "textures.cuh"
 #include "traverse.cuh"
@@ -838,35 +839,9 @@ __global__ void __launch_bounds__(kBlock, 8) kExtend(KParams p) {
 }
 
 // ---------------------------------------------------------------- ray reordering
-// Counting sort of the active list by a 16-bit ray key before the closest-hit kernel:
-// the origin's cell in an 8 x 8 x 8 grid over the scene's bounds (Morton order, high 9
-// bits) and the direction's cube-map bin (dominant axis and sign, then 4 x 4 over the
-// other two components; low 7 bits). The warps of kExtend then take rays that start in
-// the same region heading the same way, which visit the same nodes. Only the order in
-// which kExtend takes the paths changes; what each path computes does not depend on it.
-constexpr uint32_t kRayBins = 1u << 16;
-
-__device__ __forceinline__ uint32_t spread3(uint32_t x) { return (x & 1u) | ((x & 2u) << 2) | ((x & 4u) << 4); }
-
-__device__ __forceinline__ uint32_t rayKey(const SceneView& s, V3 o, V3 d) {
-    uint32_t c[3];
-    const float oc[3] = {o.x, o.y, o.z};
-#pragma unroll
-    for (int a = 0; a < 3; ++a)   // fmaxf / fminf map NaN to the bounds
-        c[a] = (uint32_t)fminf(fmaxf((oc[a] - s.keyLo[a]) * s.keyScale[a], 0.0f), 7.0f);
-    const uint32_t cell = spread3(c[0]) | (spread3(c[1]) << 1) | (spread3(c[2]) << 2);
-    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
-    uint32_t face;
-    float u, v, m;
-    if (ax >= ay && ax >= az) { face = d.x < 0.0f; u = d.y; v = d.z; m = ax; }
-    else if (ay >= az) { face = 2u + (d.y < 0.0f); u = d.x; v = d.z; m = ay; }
-    else { face = 4u + (d.z < 0.0f); u = d.x; v = d.y; m = az; }
-    const float inv = m > 0.0f ? 1.0f / m : 0.0f;
-    const uint32_t qu = (uint32_t)fminf(fmaxf((u * inv + 1.0f) * 2.0f, 0.0f), 3.0f);
-    const uint32_t qv = (uint32_t)fminf(fmaxf((v * inv + 1.0f) * 2.0f, 0.0f), 3.0f);
-    return (cell << 7) | (face << 4) | (qu << 2) | qv;
-}
-
+// Counting sort of the active list (or of the shadow queries) by ray key (raysort.cuh)
+// before the traversal kernel that takes them. Only the order in which the kernel takes
+// the paths changes; what each path computes does not depend on it.
 // Keys and their histogram (one atomic per distinct key per warp) of the active list
 // (SHADOW false: entry i is path slot listIn[i]) or of the shadow queries (SHADOW true:
 // entry i is shadow record i).
@@ -899,40 +874,6 @@ __global__ void __launch_bounds__(kBlock) kRayKeys(KParams p) {
     }
 }
 
-// Exclusive prefix sum of the histogram in place (one block of 1024 threads, 64 bins each).
-__global__ void __launch_bounds__(1024) kRayScan(uint32_t* bins) {
-    __shared__ uint32_t warpSum[32];
-    constexpr uint32_t kPer = kRayBins / 1024u;
-    uint32_t* b = bins + threadIdx.x * kPer;
-    uint32_t local = 0;
-    for (uint32_t k = 0; k < kPer; ++k) local += b[k];
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t x = local;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= (uint32_t)o) x += y;
-    }
-    if (lane == 31) warpSum[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = warpSum[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= (uint32_t)o) w += y;
-        }
-        warpSum[lane] = w;
-    }
-    __syncthreads();
-    uint32_t run = x - local + (warp ? warpSum[warp - 1] : 0u);
-    for (uint32_t k = 0; k < kPer; ++k) {
-        const uint32_t c = b[k];
-        b[k] = run;
-        run += c;
-    }
-}
-
 // Scatter into key order (lanes of one warp with the same key keep their relative order);
 // the bins are left zeroed for the next iteration's histogram.
 template <bool SHADOW>
@@ -951,10 +892,6 @@ __global__ void __launch_bounds__(kBlock) kRayScatter(KParams p) {
     }
 }
 
-// Clears the histogram (the scatter leaves each bin at its end offset).
-__global__ void kRayClear(uint32_t* bins) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kRayBins; i += gridDim.x * blockDim.x) bins[i] = 0;
-}
 
 // Active list -> per-class lists (warp-aggregated appends, one atomic per class per warp).
 __global__ void __launch_bounds__(kBlock) kClassify(KParams p, uint32_t* classLists) {
@@ -2377,7 +2314,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     if (t.sample_film != 0 && t.sample_film != 1) throw Error(GND_ERR_INVALID, "sample_film must be 0 or 1");
     if (t.spec_extend != 0 && t.spec_extend != 1) throw Error(GND_ERR_INVALID, "spec_extend must be 0 or 1");
     if (t.spec_shadow != 0 && t.spec_shadow != 1) throw Error(GND_ERR_INVALID, "spec_shadow must be 0 or 1");
-    if (t.ray_sort < 0 || t.ray_sort > 3) throw Error(GND_ERR_INVALID, "ray_sort must be in 0..3");
+    if (t.ray_sort < 0 || t.ray_sort > 7) throw Error(GND_ERR_INVALID, "ray_sort must be in 0..7");
     Tune r;
     r.poolLog2 = t.pool_log2;
     r.roundIters = t.round_iters;
@@ -2480,9 +2417,11 @@ gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t spp, int
             for (const Knob& k : knobs) {
                 for (int v : k.values) {
                     if (spentMs() > budgetMs) break;
-                    if (cur.*(k.field) == v) continue;
+                    // the render knobs only: ray_sort keeps its ray-batch bit (bit 2)
+                    const int value = k.field == &Tune::raySort ? (v | (cur.raySort & 4)) : v;
+                    if (cur.*(k.field) == value) continue;
                     Tune t = cur;
-                    t.*(k.field) = v;
+                    t.*(k.field) = value;
                     const double m = trial(t);
                     if (m > bestV * 1.02) {
                         bestV = m;

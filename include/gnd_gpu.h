@@ -401,7 +401,10 @@ typedef struct gnd_tune {
     int32_t ray_sort;         /* bit 0: before each closest-hit launch the active paths are
                                  reordered by a ray key (origin cell and direction bin) so
                                  that a warp's rays visit the same nodes; bit 1: the path
-                                 tracer's shadow queries likewise; default 0 */
+                                 tracer's shadow queries likewise; bit 2: ray batches of at
+                                 least 65,536 rays (gnd_gpu_trace_*, except the _fixed
+                                 form) are traversed in key order, results still in input
+                                 order; default 0 */
 } gnd_tune;
 gnd_status gnd_gpu_get_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_tune* tune);
 gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_tune* tune);
