@@ -1370,7 +1370,9 @@ __device__ __forceinline__ void sampleRecord(const JobDev& j, const PathState& p
 __global__ void kFilmFromSamplesGauss(JobDev j, uint32_t passes) {
     const int ww = j.wx1 - j.wx0, wh = j.wy1 - j.wy0;
     const uint64_t npix = (uint64_t)ww * (uint64_t)wh;
-    const int Rx = (int)ceilf(j.frx) + 1, Ry = (int)ceilf(j.fry) + 1;
+    // a sample of pixel sx lies at fx in [sx, sx + 1], so the pixels it reaches satisfy
+    // |px - sx| <= floor(r + 0.5) (the largest bound, floor(fx + r - 0.5), at fx = sx + 1)
+    const int Rx = (int)floorf(j.frx + 0.5f), Ry = (int)floorf(j.fry + 0.5f);
     const int tx0 = max(0, j.wx0 - Rx), tx1 = min(j.W, j.wx1 + Rx);
     const int ty0 = max(0, j.wy0 - Ry), ty1 = min(j.H, j.wy1 + Ry);
     const uint64_t tw = (uint64_t)max(tx1 - tx0, 0), nt = tw * (uint64_t)max(ty1 - ty0, 0);

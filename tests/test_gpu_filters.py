@@ -54,13 +54,23 @@ def test_gaussian_same_stream(ctx, tmp_path, scene, filt):
     ctx.free_scene(sid)
 
 
-def test_gaussian_batched_equals_plain(ctx, tmp_path):
-    xml = scenes.cornell(str(tmp_path), width=40, height=30, spp=6, filter="default")
+@pytest.mark.parametrize("filt", sorted(FILTERS))
+def test_gaussian_batched_equals_plain(ctx, tmp_path, filt):
+    """Batched renders gather the film from per-sample records (kFilmFromSamplesGauss),
+    plain ones splat with atomics: the fixed-point sums must agree bit for bit, also for a
+    pixel window whose samples reach pixels outside it."""
+    xml = scenes.cornell(str(tmp_path), width=40, height=30, spp=6, filter=FILTERS[filt])
     sid = ctx.upload(G.HostScene.load_xml(xml))
     a, _ = ctx.render(sid, spp=6)
     b, _ = ctx.render(sid, spp=6, batched=True)
     assert np.array_equal(a[..., :4], b[..., :4])
     np.testing.assert_allclose(a[..., 4:], b[..., 4:], rtol=1e-5, atol=1e-6)
+    wa, _ = ctx.render(sid, spp=3, window=(7, 5, 23, 19))
+    wb, _ = ctx.render(sid, spp=3, window=(7, 5, 23, 19), batched=True)
+    assert np.array_equal(wa[..., :4], wb[..., :4])
+    assert wa[:3].sum() == 0 and wa[:, :5].sum() == 0 and wa[:, 25:].sum() == 0   # at most 2 pixels past the window
+    if filt == "default":
+        assert wa[4, 6:24, 3].min() > 0   # the row above the window gets weight
     ctx.free_scene(sid)
 
 
