@@ -363,7 +363,8 @@ def cold_request_leg(ctx, xml, spp):
     """Time-to-image of a cold request: from the scene file on disk to the film in host
     memory -- parse and load the 4,105 OBJ files, build (mesh trees on the GPU, or the
     host SAH build), upload, render all passes batched, read the film back -- host wall
-    time, median of 3."""
+    time, median of 3 (the files sit in the OS page cache, as for a server that keeps
+    receiving the same scenes)."""
     import gianduia_b200 as G
     out = {}
     for name, dev in (("device_trees", True), ("host_trees", False)):
