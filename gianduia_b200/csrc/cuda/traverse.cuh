@@ -576,9 +576,13 @@ __device__ __forceinline__ uint32_t warpFetch(uint32_t* counter, bool want) {
 // SLOT_ORDER_ANY: any-hit queries visit hit children in slot order instead of nearest
 // first (faster for the bounded shadow segments of the path tracer; rays to infinity find
 // an occluder sooner nearest first).
+// leafBatch (1..32): the node phase ends as soon as that many lanes hold a leaf (32: when
+// no lane can take another node step); lanes still traversing keep their state and go on
+// in the next round. Only the interleaving of the lanes' steps changes.
 template <int BLOCK, bool ANY, bool COUNT, int SMEM = kSmemStack, bool SPEC = false, bool MOTION = false,
           bool SLOT_ORDER_ANY = false, typename Src>
-__device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter, uint32_t* smemStack, TraceCounters* cnt) {
+__device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter, uint32_t* smemStack, TraceCounters* cnt,
+                                               uint32_t leafBatch = 32) {
     TStack<BLOCK, SMEM> st;
     st.smem = smemStack + threadIdx.x;
     Trav t;
@@ -625,6 +629,8 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
                 }
             }
             if (!__any_sync(0xffffffffu, want)) break;
+            if (leafBatch < 32u && (uint32_t)__popc(__ballot_sync(0xffffffffu, active && t.leaf != kEmpty)) >= leafBatch)
+                break;
             if (want) {
                 int e = travNodeStep<BLOCK, COUNT, SMEM, !(ANY && SLOT_ORDER_ANY)>(t, *sv, st, cnt);
                 if (e || ++iter > kMaxIterations) {

@@ -94,6 +94,7 @@ struct KParams {
     uint32_t* rayBins;             // key histogram / bin offsets (kRayBins entries)
     uint32_t* raySorted;           // the reordered list
     const uint32_t* shadowOrder;   // order in which kShadowPath takes the shadow records, or null
+    uint32_t leafBatch;            // traversal: lanes holding a leaf that end the node phase (1..32)
     uint32_t capacity;
     uint32_t fifo;                 // 1: grabs walk the active list from its first job
 };
@@ -823,7 +824,7 @@ __global__ void __launch_bounds__(kBlock, 8) kExtend(KParams p) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[0], (unsigned long long)n);
     TraceCounters cnt{0, 0};
     ExtendSrc src{&p, n, 0};
-    int err = persistentTrace<kBlock, false, COUNT, SMEM, SPEC, MOTION>(src, p.cnt + kQFetchA, stack, &cnt);
+    int err = persistentTrace<kBlock, false, COUNT, SMEM, SPEC, MOTION>(src, p.cnt + kQFetchA, stack, &cnt, p.leafBatch);
     if (COUNT) {
         unsigned long long nn = cnt.nodes, nt = cnt.tris;
         for (int o = 16; o > 0; o >>= 1) {
@@ -1201,7 +1202,8 @@ __global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p, bool mixed) 
     const uint32_t n = p.cnt[kQShadow];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
     ShadowSrc<ANY> src{&p, n, 0, nullptr, mixed};
-    int err = persistentTrace<kBlock, ANY, false, SMEM, SPEC, MOTION, true>(src, p.cnt + kQFetchB, stack, nullptr);
+    int err = persistentTrace<kBlock, ANY, false, SMEM, SPEC, MOTION, true>(src, p.cnt + kQFetchB, stack, nullptr,
+                                                                            p.leafBatch);
     if (err) atomicOr(p.errWord, (uint32_t)err);
 }
 
@@ -2077,6 +2079,7 @@ void Wavefront::enqueueRound(int iters, int mix, bool hasNull, int profile, Resu
     kp.errWord = c->errWord.as<uint32_t>();
     kp.capacity = (uint32_t)cap_;
     kp.classLists = classes_.as<uint32_t>();
+    kp.leafBatch = (uint32_t)tune_.leafBatch;
     kp.rayKeys = rayKeys_.as<uint32_t>();
     kp.rayBins = rayBins_.as<uint32_t>();
     kp.raySorted = raySorted_.as<uint32_t>();
@@ -2317,6 +2320,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     if (t.spec_extend != 0 && t.spec_extend != 1) throw Error(GND_ERR_INVALID, "spec_extend must be 0 or 1");
     if (t.spec_shadow != 0 && t.spec_shadow != 1) throw Error(GND_ERR_INVALID, "spec_shadow must be 0 or 1");
     if (t.ray_sort < 0 || t.ray_sort > 7) throw Error(GND_ERR_INVALID, "ray_sort must be in 0..7");
+    if (t.leaf_batch < 1 || t.leaf_batch > 32) throw Error(GND_ERR_INVALID, "leaf_batch must be in 1..32");
     Tune r;
     r.poolLog2 = t.pool_log2;
     r.roundIters = t.round_iters;
@@ -2328,6 +2332,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     r.specExtend = t.spec_extend;
     r.specShadow = t.spec_shadow;
     r.raySort = t.ray_sort;
+    r.leafBatch = t.leaf_batch;
     return r;
 }
 
@@ -2343,6 +2348,7 @@ static gnd_tune tuneToC(const Tune& t) {
     r.spec_extend = t.specExtend;
     r.spec_shadow = t.specShadow;
     r.ray_sort = t.raySort;
+    r.leaf_batch = t.leafBatch;
     return r;
 }
 
@@ -2412,7 +2418,7 @@ gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t spp, int
             {&Tune::travBlocks, {8, 6, 4}}, {&Tune::smem, {32, 16}},          {&Tune::sort, {1, 0}},
             {&Tune::poolLog2, {22, 21, 23, 20}}, {&Tune::roundIters, {8, 16, 4}}, {&Tune::graphs, {1, 0}},
             {&Tune::sampleFilm, {1, 0}}, {&Tune::specExtend, {1, 0}}, {&Tune::specShadow, {1, 0}},
-            {&Tune::raySort, {1, 3, 0}},
+            {&Tune::raySort, {1, 3, 0}}, {&Tune::leafBatch, {16, 8, 24, 32}},
         };
         for (int sweep = 0; sweep < 2; ++sweep) {
             bool changed = false;
