@@ -66,7 +66,8 @@ template <bool ANY, bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock, kTraceBlocksPerSM)
     traceKernel(const SceneView* __restrict__ sv, const gnd_ray* __restrict__ rays, uint32_t n, gnd_hit* __restrict__ hits,
                 uint8_t* __restrict__ occ, uint32_t* __restrict__ nodesOut, uint32_t* __restrict__ trisOut,
-                uint32_t* fetch, uint32_t* errWord, unsigned long long* totals, const uint32_t* __restrict__ perm) {
+                uint32_t* fetch, uint32_t* errWord, unsigned long long* totals, const uint32_t* __restrict__ perm,
+                uint32_t leafBatch) {
     __shared__ uint32_t stack[kSmemStack * kTraceBlock];
     TraceCounters cnt{0, 0};
     BatchSrc<ANY, COUNT> src{sv, rays, n, hits, occ, nodesOut, trisOut, &cnt, perm};
@@ -74,7 +75,7 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceBlocksPerSM)
         atomicAdd(&totals[kTraceTotalRays], (unsigned long long)n);
         if (COUNT) atomicAdd(&totals[kTraceTotalCountedRays], (unsigned long long)n);
     }
-    int err = persistentTrace<kTraceBlock, ANY, COUNT>(src, fetch, stack, &cnt);
+    int err = persistentTrace<kTraceBlock, ANY, COUNT>(src, fetch, stack, &cnt, leafBatch);
     if (COUNT) {
         unsigned long long nn = src.sumNodes, nt = src.sumTris;
         for (int o = 16; o > 0; o >>= 1) {
@@ -155,9 +156,10 @@ void launchTrace(Context* c, DeviceScene& ds, const gnd_ray* dr, int64_t n, gnd_
         GND_CUDA(cudaGetLastError());
         order = perm.as<uint32_t>();
     }
-    if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, nullptr, dn, dt, fetch, ew, tot, order);
-    else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew, tot, order);
-    else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew, tot, order);
+    const uint32_t lb = (uint32_t)ds.tune.leafBatch;
+    if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, nullptr, dn, dt, fetch, ew, tot, order, lb);
+    else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew, tot, order, lb);
+    else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew, tot, order, lb);
     GND_CUDA(cudaGetLastError());
     c->counters.trace_batches += 1;
 }
@@ -299,7 +301,7 @@ gnd_status gnd_gpu_trace_closest_fixed(gnd_gpu_ctx* ctxh, gnd_scene_id id, const
         int g = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)c->numSMs * kTraceBlocksPerSM));
         traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(ds.viewDev.as<SceneView>(), dr, (uint32_t)n, dh, nullptr,
                                                              nullptr, nullptr, fetch, c->errWord.as<uint32_t>(),
-                                                             c->traceTotals.as<unsigned long long>(), nullptr);
+                                                             c->traceTotals.as<unsigned long long>(), nullptr, 32u);
         GND_CUDA(cudaGetLastError());
         c->counters.trace_batches += 1;
         GND_CUDA(cudaMemcpyAsync(hits, dh, sizeof(gnd_hit) * (size_t)n, cudaMemcpyDeviceToHost, st));

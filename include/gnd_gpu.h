@@ -405,7 +405,7 @@ typedef struct gnd_tune {
                                  least 65,536 rays (gnd_gpu_trace_*, except the _fixed
                                  form) are traversed in key order, results still in input
                                  order; default 0 */
-    int32_t leaf_batch;       /* path-tracer traversal (1..32): a warp leaves its inner-node
+    int32_t leaf_batch;       /* traversal (1..32; renders and the scene's ray batches): a warp leaves its inner-node
                                  phase for its leaf phase once this many of its rays hold a
                                  leaf; the others resume their traversal afterwards (32:
                                  only when no ray can take another inner-node step, the
