@@ -129,19 +129,16 @@ protected:
 // fileResolver.h:11-41: the directory of the scene file being loaded and the name its
 // outputs take (its stem), recorded by loadFromXML as Parser::loadFromXML records them
 // (parser.cpp:220-223) before the scene is built.
+// Process-wide like the reference's; a mutex makes loads on several threads safe, the
+// values being those of the latest load to set them.
 class FileResolver {
 public:
-    static void setBasePath(const std::filesystem::path& p) { basePath() = p; }
-    static void setOutputPath(const std::filesystem::path& p) { outputPath() = p; }
-    static void setOutputName(const std::string& n) { outputName() = n; }
-    static std::filesystem::path getBasePath() { return basePath(); }
-    static std::filesystem::path getOutputPath() { return outputPath(); }
-    static std::string getOutputName() { return outputName(); }
-
-private:
-    static std::filesystem::path& basePath();
-    static std::filesystem::path& outputPath();
-    static std::string& outputName();
+    static void setBasePath(const std::filesystem::path& p);
+    static void setOutputPath(const std::filesystem::path& p);
+    static void setOutputName(const std::string& n);
+    static std::filesystem::path getBasePath();
+    static std::filesystem::path getOutputPath();
+    static std::string getOutputName();
 };
 
 // factory.h:9-36

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <filesystem>
 #include <fstream>
+#include <mutex>
 #include <sstream>
 #include <thread>
 #include <unordered_map>
@@ -283,17 +284,41 @@ private:
 
 }  // namespace
 
-std::filesystem::path& FileResolver::basePath() {
-    static std::filesystem::path p = std::filesystem::current_path();
-    return p;
+namespace {
+struct ResolverState {
+    std::mutex mu;
+    std::filesystem::path base = std::filesystem::current_path(), output = std::filesystem::current_path();
+    std::string name = "output";   // fileResolver.cpp: the default output name
+};
+ResolverState& resolver() {
+    static ResolverState r;
+    return r;
 }
-std::filesystem::path& FileResolver::outputPath() {
-    static std::filesystem::path p = std::filesystem::current_path();
-    return p;
+}  // namespace
+
+void FileResolver::setBasePath(const std::filesystem::path& p) {
+    std::lock_guard<std::mutex> lk(resolver().mu);
+    resolver().base = p;
 }
-std::string& FileResolver::outputName() {
-    static std::string n = "output";   // fileResolver.cpp: the default output name
-    return n;
+void FileResolver::setOutputPath(const std::filesystem::path& p) {
+    std::lock_guard<std::mutex> lk(resolver().mu);
+    resolver().output = p;
+}
+void FileResolver::setOutputName(const std::string& n) {
+    std::lock_guard<std::mutex> lk(resolver().mu);
+    resolver().name = n;
+}
+std::filesystem::path FileResolver::getBasePath() {
+    std::lock_guard<std::mutex> lk(resolver().mu);
+    return resolver().base;
+}
+std::filesystem::path FileResolver::getOutputPath() {
+    std::lock_guard<std::mutex> lk(resolver().mu);
+    return resolver().output;
+}
+std::string FileResolver::getOutputName() {
+    std::lock_guard<std::mutex> lk(resolver().mu);
+    return resolver().name;
 }
 
 std::shared_ptr<GndObject> loadFromXML(const std::string& path, bool deferPreprocess, bool deviceBlas) {
