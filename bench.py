@@ -188,14 +188,17 @@ def traversal_leg(ctx):
     st = strm.cuda_stream
     out = {"workload": "2^20 random triangles (centroids U[0,1]^3, vertex offsets N(0, 0.01^2)), 2^24 rays "
                        "(origins U[-0.5,1.5]^3, uniform directions, tmax inf)"}
-    runs = [("closest", lambda: ctx.trace_closest_dev(sid, dr.data_ptr(), n, dh.data_ptr(), st)),
-            ("any", lambda: ctx.trace_any_dev(sid, dr.data_ptr(), n, docc.data_ptr(), st)),
-            ("closest_key_order", lambda: ctx.trace_closest_dev(sid, dr.data_ptr(), n, dh.data_ptr(), st)),
-            ("any_key_order", lambda: ctx.trace_any_dev(sid, dr.data_ptr(), n, docc.data_ptr(), st))]
-    for name, fn in runs:
-        # the last two: the batch traversed in ray-key order (gnd_tune ray_sort bit 2),
-        # the reordering inside the timed region
-        ctx.set_tune(sid, ray_sort=4 if name.endswith("key_order") else 0)
+    closest = lambda: ctx.trace_closest_dev(sid, dr.data_ptr(), n, dh.data_ptr(), st)
+    anyhit = lambda: ctx.trace_any_dev(sid, dr.data_ptr(), n, docc.data_ptr(), st)
+    # default settings (trace_leaf_batch 16); the full node phase of every warp
+    # (trace_leaf_batch 32, the earlier default); the batch traversed in ray-key order
+    # (ray_sort bit 2, the reordering inside the timed region)
+    runs = [("closest", closest, {}), ("any", anyhit, {}),
+            ("closest_full_node_phase", closest, {"trace_leaf_batch": 32}),
+            ("any_full_node_phase", anyhit, {"trace_leaf_batch": 32}),
+            ("closest_key_order", closest, {"ray_sort": 4}), ("any_key_order", anyhit, {"ray_sort": 4})]
+    for name, fn, tune_fields in runs:
+        ctx.set_tune(sid, **dict({"ray_sort": 0, "trace_leaf_batch": 16}, **tune_fields))
         for _ in range(2):
             fn()
         torch.cuda.synchronize()
@@ -210,7 +213,7 @@ def traversal_leg(ctx):
         ms = float(statistics.median(ts))
         out[name + "_ms"] = ms
         out[name + "_mrays_s"] = n / ms / 1e3
-    ctx.set_tune(sid, ray_sort=0)
+    ctx.set_tune(sid, ray_sort=0, trace_leaf_batch=16)
     nodes = torch.zeros(n, dtype=torch.int32, device="cuda")
     tris = torch.zeros(n, dtype=torch.int32, device="cuda")
     ctx.trace_count_dev(sid, dr.data_ptr(), n, nodes.data_ptr(), tris.data_ptr(), st)
@@ -231,10 +234,11 @@ def traversal_leg(ctx):
     torch.cuda.empty_cache()
     out["key_order_closest_achieved_gbs"] = bytes_per_ray * n / (out["closest_key_order_ms"] * 1e-3) / 1e9
     out["key_order_frac_of_l2"] = out["key_order_closest_achieved_gbs"] / l2
-    log("traversal: closest %.0f Mrays/s (key order %.0f), any %.0f Mrays/s (key order %.0f); %.1f nodes %.1f tris "
-        "per ray; %.0f GB/s = %.2f of L2 %.0f GB/s (key order %.2f)" % (
-            out["closest_mrays_s"], out["closest_key_order_mrays_s"], out["any_mrays_s"], out["any_key_order_mrays_s"],
-            npr, tpr, achieved, achieved / l2, l2, out["key_order_frac_of_l2"]))
+    log("traversal: closest %.0f Mrays/s (full node phases %.0f, key order %.0f), any %.0f Mrays/s (%.0f, %.0f); "
+        "%.1f nodes %.1f tris per ray; %.0f GB/s = %.2f of L2 %.0f GB/s" % (
+            out["closest_mrays_s"], out["closest_full_node_phase_mrays_s"], out["closest_key_order_mrays_s"],
+            out["any_mrays_s"], out["any_full_node_phase_mrays_s"], out["any_key_order_mrays_s"],
+            npr, tpr, achieved, achieved / l2, l2))
     return out
 
 

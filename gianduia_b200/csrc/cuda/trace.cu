@@ -156,7 +156,7 @@ void launchTrace(Context* c, DeviceScene& ds, const gnd_ray* dr, int64_t n, gnd_
         GND_CUDA(cudaGetLastError());
         order = perm.as<uint32_t>();
     }
-    const uint32_t lb = (uint32_t)ds.tune.leafBatch;
+    const uint32_t lb = (uint32_t)ds.tune.traceLeafBatch;
     if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, nullptr, dn, dt, fetch, ew, tot, order, lb);
     else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew, tot, order, lb);
     else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew, tot, order, lb);

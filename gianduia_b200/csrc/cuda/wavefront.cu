@@ -2321,6 +2321,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     if (t.spec_shadow != 0 && t.spec_shadow != 1) throw Error(GND_ERR_INVALID, "spec_shadow must be 0 or 1");
     if (t.ray_sort < 0 || t.ray_sort > 7) throw Error(GND_ERR_INVALID, "ray_sort must be in 0..7");
     if (t.leaf_batch < 1 || t.leaf_batch > 32) throw Error(GND_ERR_INVALID, "leaf_batch must be in 1..32");
+    if (t.trace_leaf_batch < 1 || t.trace_leaf_batch > 32) throw Error(GND_ERR_INVALID, "trace_leaf_batch must be in 1..32");
     Tune r;
     r.poolLog2 = t.pool_log2;
     r.roundIters = t.round_iters;
@@ -2333,6 +2334,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     r.specShadow = t.spec_shadow;
     r.raySort = t.ray_sort;
     r.leafBatch = t.leaf_batch;
+    r.traceLeafBatch = t.trace_leaf_batch;
     return r;
 }
 
@@ -2349,6 +2351,7 @@ static gnd_tune tuneToC(const Tune& t) {
     r.spec_shadow = t.specShadow;
     r.ray_sort = t.raySort;
     r.leaf_batch = t.leafBatch;
+    r.trace_leaf_batch = t.traceLeafBatch;
     return r;
 }
 

@@ -159,9 +159,11 @@ def test_full_size_traversal_parity(ctx):
 
 
 def test_key_ordered_batches(ctx):
-    """ray_sort bit 2: a batch traversed in ray-key order gives every ray the same result
-    in its own slot (closest hit, occlusion, node and triangle counts) as input order, and
-    matches the oracle; each ray's traversal does not depend on the other rays."""
+    """ray_sort bit 2 and trace_leaf_batch: a batch traversed in ray-key order, or with the
+    warps' node phases cut short at any leaf count, gives every ray the same result in its
+    own slot (closest hit, occlusion, node and triangle counts) as input order with full
+    node phases, and matches the oracle; each ray's traversal does not depend on the other
+    rays."""
     torch = pytest.importorskip("torch")
     tri = scenes.random_triangles(1 << 18, seed=4)
     rays = scenes.random_rays(1 << 20, seed=4)
@@ -169,8 +171,8 @@ def test_key_ordered_batches(ctx):
     sid = ctx.upload(hs)
     try:
         out = {}
-        for rs in (0, 4):
-            ctx.set_tune(sid, ray_sort=rs)
+        for rs, lb in ((0, 32), (4, 16), (0, 1), (4, 7)):
+            ctx.set_tune(sid, ray_sort=rs, trace_leaf_batch=lb)
             closest = ctx.trace_closest(sid, rays)
             occ = ctx.trace_any(sid, rays)
             dr = torch.from_numpy(rays).cuda()
@@ -178,16 +180,18 @@ def test_key_ordered_batches(ctx):
             tris = torch.zeros(rays.shape[0], dtype=torch.int32, device="cuda")
             ctx.trace_count_dev(sid, dr.data_ptr(), rays.shape[0], nodes.data_ptr(), tris.data_ptr())
             torch.cuda.synchronize()
-            out[rs] = (closest, occ, nodes.cpu().numpy(), tris.cpu().numpy())
-        a, b = out[0], out[4]
-        assert a[0].tobytes() == b[0].tobytes()
-        assert np.array_equal(a[1], b[1])
-        assert np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
+            out[(rs, lb)] = (closest, occ, nodes.cpu().numpy(), tris.cpu().numpy())
+        a = out[(0, 32)]
+        for key, b in out.items():
+            assert a[0].tobytes() == b[0].tobytes(), key
+            assert np.array_equal(a[1], b[1]), key
+            assert np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3]), key
+        b = out[(4, 16)]
         sample = rays[::16]
         ref = O.Scene.from_triangles(tri).trace(sample)
         compare_closest(b[0][::16], ref, sample, "key-ordered")
     finally:
-        ctx.set_tune(sid, ray_sort=0)
+        ctx.set_tune(sid, ray_sort=0, trace_leaf_batch=16)
         ctx.free_scene(sid)
 
 
