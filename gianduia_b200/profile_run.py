@@ -25,10 +25,12 @@ import gianduia_b200 as G
 from gianduia_b200 import scenes
 
 
-def run_trace(ctx):
+def run_trace(ctx, tune=None):
     tri = scenes.random_triangles(1 << 20, seed=1)
     rays = scenes.random_rays(1 << 22, seed=1)
     sid = ctx.upload(G.HostScene.from_triangles(tri))
+    if tune:
+        ctx.set_tune(sid, **tune)
     h = ctx.trace_closest(sid, rays)
     print("trace: %d of %d rays hit" % (int((h["inst"] >= 0).sum()), rays.shape[0]))
     ctx.free_scene(sid)
@@ -67,7 +69,7 @@ def main(argv):
     what = argv[1] if len(argv) > 1 else "all"
     ctx = G.GpuContext(0)
     if what in ("trace", "all"):
-        run_trace(ctx)
+        run_trace(ctx, tune=tune)
     if what in ("render", "all"):
         run_render(ctx, tune=tune)
     if what == "batched":
