@@ -190,7 +190,7 @@ def traversal_leg(ctx):
                        "(origins U[-0.5,1.5]^3, uniform directions, tmax inf)"}
     closest = lambda: ctx.trace_closest_dev(sid, dr.data_ptr(), n, dh.data_ptr(), st)
     anyhit = lambda: ctx.trace_any_dev(sid, dr.data_ptr(), n, docc.data_ptr(), st)
-    # default settings (trace_leaf_batch 16); the full node phase of every warp
+    # default settings (trace_leaf_batch 12); the full node phase of every warp
     # (trace_leaf_batch 32, the earlier default); the batch traversed in ray-key order
     # (ray_sort bit 2, the reordering inside the timed region)
     runs = [("closest", closest, {}), ("any", anyhit, {}),
@@ -198,7 +198,7 @@ def traversal_leg(ctx):
             ("any_full_node_phase", anyhit, {"trace_leaf_batch": 32}),
             ("closest_key_order", closest, {"ray_sort": 4}), ("any_key_order", anyhit, {"ray_sort": 4})]
     for name, fn, tune_fields in runs:
-        ctx.set_tune(sid, **dict({"ray_sort": 0, "trace_leaf_batch": 16}, **tune_fields))
+        ctx.set_tune(sid, **dict({"ray_sort": 0, "trace_leaf_batch": 12}, **tune_fields))
         for _ in range(2):
             fn()
         torch.cuda.synchronize()
@@ -213,7 +213,7 @@ def traversal_leg(ctx):
         ms = float(statistics.median(ts))
         out[name + "_ms"] = ms
         out[name + "_mrays_s"] = n / ms / 1e3
-    ctx.set_tune(sid, ray_sort=0, trace_leaf_batch=16)
+    ctx.set_tune(sid, ray_sort=0, trace_leaf_batch=12)
     nodes = torch.zeros(n, dtype=torch.int32, device="cuda")
     tris = torch.zeros(n, dtype=torch.int32, device="cuda")
     ctx.trace_count_dev(sid, dr.data_ptr(), n, nodes.data_ptr(), tris.data_ptr(), st)

@@ -496,7 +496,7 @@ class GpuContext:
     def serve_tune(self, **fields):
         """Engine settings of the serving thread (the defaults of gnd_tune, updated by fields)."""
         t = Tune(pool_log2=22, round_iters=4, trav_blocks=8, material_sort=1, stack_smem=32, graphs=1, sample_film=1,
-                 spec_extend=0, spec_shadow=0, ray_sort=0, leaf_batch=32, trace_leaf_batch=16)
+                 spec_extend=0, spec_shadow=0, ray_sort=0, leaf_batch=32, trace_leaf_batch=12)
         for k, v in fields.items():
             setattr(t, k, int(v))
         _check(lib().gnd_gpu_serve_tune(self._h, ctypes.byref(t)), "gnd_gpu_serve_tune")

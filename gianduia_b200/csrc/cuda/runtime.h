@@ -133,7 +133,7 @@ struct Tune {
     int specShadow = 0;       // speculative node traversal in the shadow kernel
     int raySort = 0;          // reorder each iteration's closest-hit queries by ray key
     int leafBatch = 32;       // render traversal: lanes holding a leaf that end the node phase
-    int traceLeafBatch = 16;  // the same for the scene's ray batches
+    int traceLeafBatch = 12;  // the same for the scene's ray batches
     bool operator==(const Tune& o) const {
         return poolLog2 == o.poolLog2 && roundIters == o.roundIters && travBlocks == o.travBlocks && sort == o.sort &&
                smem == o.smem && graphs == o.graphs && sampleFilm == o.sampleFilm && specExtend == o.specExtend &&

@@ -411,7 +411,7 @@ typedef struct gnd_tune {
                                  only when no ray can take another inner-node step, the
                                  default) */
     int32_t trace_leaf_batch; /* the same for the scene's ray batches (gnd_gpu_trace_*,
-                                 except the _fixed form); default 16 */
+                                 except the _fixed form); default 12 */
 } gnd_tune;
 gnd_status gnd_gpu_get_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_tune* tune);
 gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_tune* tune);

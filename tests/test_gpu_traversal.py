@@ -171,7 +171,7 @@ def test_key_ordered_batches(ctx):
     sid = ctx.upload(hs)
     try:
         out = {}
-        for rs, lb in ((0, 32), (4, 16), (0, 1), (4, 7)):
+        for rs, lb in ((0, 32), (4, 12), (0, 1), (4, 7)):
             ctx.set_tune(sid, ray_sort=rs, trace_leaf_batch=lb)
             closest = ctx.trace_closest(sid, rays)
             occ = ctx.trace_any(sid, rays)
@@ -186,12 +186,12 @@ def test_key_ordered_batches(ctx):
             assert a[0].tobytes() == b[0].tobytes(), key
             assert np.array_equal(a[1], b[1]), key
             assert np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3]), key
-        b = out[(4, 16)]
+        b = out[(4, 12)]
         sample = rays[::16]
         ref = O.Scene.from_triangles(tri).trace(sample)
         compare_closest(b[0][::16], ref, sample, "key-ordered")
     finally:
-        ctx.set_tune(sid, ray_sort=0, trace_leaf_batch=16)
+        ctx.set_tune(sid, ray_sort=0, trace_leaf_batch=12)
         ctx.free_scene(sid)
 
 
