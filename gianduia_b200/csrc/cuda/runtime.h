@@ -132,13 +132,14 @@ struct Tune {
     int specExtend = 0;       // speculative node traversal in the extend kernel
     int specShadow = 0;       // speculative node traversal in the shadow kernel
     int raySort = 0;          // reorder each iteration's closest-hit queries by ray key
-    int leafBatch = 32;       // render traversal: lanes holding a leaf that end the node phase
+    int leafBatch = 32;       // closest-hit traversal of renders: lanes holding a leaf that end the node phase
     int traceLeafBatch = 12;  // the same for the scene's ray batches
+    int shadowLeafBatch = 32; // the same for the path tracer's shadow queries
     bool operator==(const Tune& o) const {
         return poolLog2 == o.poolLog2 && roundIters == o.roundIters && travBlocks == o.travBlocks && sort == o.sort &&
                smem == o.smem && graphs == o.graphs && sampleFilm == o.sampleFilm && specExtend == o.specExtend &&
                specShadow == o.specShadow && raySort == o.raySort && leafBatch == o.leafBatch &&
-               traceLeafBatch == o.traceLeafBatch;
+               traceLeafBatch == o.traceLeafBatch && shadowLeafBatch == o.shadowLeafBatch;
     }
     bool operator!=(const Tune& o) const { return !(*this == o); }
 };

@@ -94,7 +94,8 @@ struct KParams {
     uint32_t* rayBins;             // key histogram / bin offsets (kRayBins entries)
     uint32_t* raySorted;           // the reordered list
     const uint32_t* shadowOrder;   // order in which kShadowPath takes the shadow records, or null
-    uint32_t leafBatch;            // traversal: lanes holding a leaf that end the node phase (1..32)
+    uint32_t leafBatch;            // closest-hit traversal: lanes holding a leaf that end the node phase (1..32)
+    uint32_t shadowLeafBatch;      // the same for the shadow queries
     uint32_t capacity;
     uint32_t fifo;                 // 1: grabs walk the active list from its first job
 };
@@ -1203,7 +1204,7 @@ __global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p, bool mixed) 
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
     ShadowSrc<ANY> src{&p, n, 0, nullptr, mixed};
     int err = persistentTrace<kBlock, ANY, false, SMEM, SPEC, MOTION, true>(src, p.cnt + kQFetchB, stack, nullptr,
-                                                                            p.leafBatch);
+                                                                            p.shadowLeafBatch);
     if (err) atomicOr(p.errWord, (uint32_t)err);
 }
 
@@ -2080,6 +2081,7 @@ void Wavefront::enqueueRound(int iters, int mix, bool hasNull, int profile, Resu
     kp.capacity = (uint32_t)cap_;
     kp.classLists = classes_.as<uint32_t>();
     kp.leafBatch = (uint32_t)tune_.leafBatch;
+    kp.shadowLeafBatch = (uint32_t)tune_.shadowLeafBatch;
     kp.rayKeys = rayKeys_.as<uint32_t>();
     kp.rayBins = rayBins_.as<uint32_t>();
     kp.raySorted = raySorted_.as<uint32_t>();
@@ -2322,6 +2324,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     if (t.ray_sort < 0 || t.ray_sort > 7) throw Error(GND_ERR_INVALID, "ray_sort must be in 0..7");
     if (t.leaf_batch < 1 || t.leaf_batch > 32) throw Error(GND_ERR_INVALID, "leaf_batch must be in 1..32");
     if (t.trace_leaf_batch < 1 || t.trace_leaf_batch > 32) throw Error(GND_ERR_INVALID, "trace_leaf_batch must be in 1..32");
+    if (t.shadow_leaf_batch < 1 || t.shadow_leaf_batch > 32) throw Error(GND_ERR_INVALID, "shadow_leaf_batch must be in 1..32");
     Tune r;
     r.poolLog2 = t.pool_log2;
     r.roundIters = t.round_iters;
@@ -2335,6 +2338,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     r.raySort = t.ray_sort;
     r.leafBatch = t.leaf_batch;
     r.traceLeafBatch = t.trace_leaf_batch;
+    r.shadowLeafBatch = t.shadow_leaf_batch;
     return r;
 }
 
@@ -2352,6 +2356,7 @@ static gnd_tune tuneToC(const Tune& t) {
     r.ray_sort = t.raySort;
     r.leaf_batch = t.leafBatch;
     r.trace_leaf_batch = t.traceLeafBatch;
+    r.shadow_leaf_batch = t.shadowLeafBatch;
     return r;
 }
 
@@ -2421,7 +2426,7 @@ gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t spp, int
             {&Tune::travBlocks, {8, 6, 4}}, {&Tune::smem, {32, 16}},          {&Tune::sort, {1, 0}},
             {&Tune::poolLog2, {22, 21, 23, 20}}, {&Tune::roundIters, {8, 16, 4}}, {&Tune::graphs, {1, 0}},
             {&Tune::sampleFilm, {1, 0}}, {&Tune::specExtend, {1, 0}}, {&Tune::specShadow, {1, 0}},
-            {&Tune::raySort, {1, 3, 0}}, {&Tune::leafBatch, {16, 8, 24, 32}},
+            {&Tune::raySort, {1, 3, 0}}, {&Tune::leafBatch, {16, 8, 24, 32}}, {&Tune::shadowLeafBatch, {16, 8, 24, 32}},
         };
         for (int sweep = 0; sweep < 2; ++sweep) {
             bool changed = false;

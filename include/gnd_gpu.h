@@ -405,13 +405,14 @@ typedef struct gnd_tune {
                                  least 65,536 rays (gnd_gpu_trace_*, except the _fixed
                                  form) are traversed in key order, results still in input
                                  order; default 0 */
-    int32_t leaf_batch;       /* traversal of renders (1..32): a warp leaves its inner-node
-                                 phase for its leaf phase once this many of its rays hold a
-                                 leaf; the others resume their traversal afterwards (32:
-                                 only when no ray can take another inner-node step, the
-                                 default) */
+    int32_t leaf_batch;       /* closest-hit traversal of renders (1..32): a warp leaves its
+                                 inner-node phase for its leaf phase once this many of its
+                                 rays hold a leaf; the others resume their traversal
+                                 afterwards (32: only when no ray can take another
+                                 inner-node step, the default) */
     int32_t trace_leaf_batch; /* the same for the scene's ray batches (gnd_gpu_trace_*,
                                  except the _fixed form); default 12 */
+    int32_t shadow_leaf_batch; /* the same for the path tracer's shadow queries; default 32 */
 } gnd_tune;
 gnd_status gnd_gpu_get_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_tune* tune);
 gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_tune* tune);
