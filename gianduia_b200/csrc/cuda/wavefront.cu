@@ -818,8 +818,10 @@ struct ExtendSrc {
 };
 
 // MOTION: the scene has animated instances (rays carry their shutter time)
-template <bool COUNT, int SMEM, bool SPEC, bool MOTION = false>
-__global__ void __launch_bounds__(kBlock, 8) kExtend(KParams p) {
+// MINB: the blocks per SM the kernel is compiled to fit (8: 64 registers; 9 and 10 trade
+// registers, with some spilled, for more resident warps; gnd_tune trav_blocks)
+template <bool COUNT, int SMEM, bool SPEC, bool MOTION = false, int MINB = 8>
+__global__ void __launch_bounds__(kBlock, MINB) kExtend(KParams p) {
     __shared__ uint32_t stack[SMEM * kBlock];
     const uint32_t n = p.cnt[kQIn];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[0], (unsigned long long)n);
@@ -1197,8 +1199,8 @@ struct ShadowSrc {
     }
 };
 
-template <bool ANY, int SMEM, bool SPEC, bool MOTION = false>
-__global__ void __launch_bounds__(kBlock, 8) kShadowPath(KParams p, bool mixed) {
+template <bool ANY, int SMEM, bool SPEC, bool MOTION = false, int MINB = 8>
+__global__ void __launch_bounds__(kBlock, MINB) kShadowPath(KParams p, bool mixed) {
     __shared__ uint32_t stack[SMEM * kBlock];
     const uint32_t n = p.cnt[kQShadow];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
@@ -1902,10 +1904,32 @@ void Wavefront::drop(int j) {
     syncActive();
 }
 
-// The traversal kernels for one shared-stack size and speculation setting.
+// The plain traversal kernels compiled for MINB blocks per SM.
+template <int SMEM, int MINB>
+static void launchWide(const KParams& kp, int mix, bool hasNull, int travGrid, cudaStream_t st, cudaEvent_t ea,
+                       cudaEvent_t eb, int stage) {
+    if (stage == 0) {
+        if (ea) GND_CUDA(cudaEventRecord(ea, st));
+        kExtend<false, SMEM, false, false, MINB><<<travGrid, kBlock, 0, st>>>(kp);
+        if (eb) GND_CUDA(cudaEventRecord(eb, st));
+    } else if (mix & 1) {
+        if (hasNull) kShadowPath<false, SMEM, false, false, MINB><<<travGrid, kBlock, 0, st>>>(kp, mix == 3);
+        else kShadowPath<true, SMEM, false, false, MINB><<<travGrid, kBlock, 0, st>>>(kp, mix == 3);
+    }
+}
+
+// The traversal kernels for one shared-stack size and speculation setting; bps: blocks
+// per SM (the grid is bps per SM; 9 and 10 select the kernels compiled for them, for
+// static scenes without speculation or visit counting).
 template <int SMEM, bool SPEC>
 static void launchTraversal(const KParams& kp, int mix, bool hasNull, bool count, int travGrid, cudaStream_t st,
-                            cudaEvent_t ea, cudaEvent_t eb, int stage, bool motion) {
+                            cudaEvent_t ea, cudaEvent_t eb, int stage, bool motion, int bps) {
+    if (!motion && !count && !SPEC && bps > 8) {
+        if (bps == 9) launchWide<SMEM, 9>(kp, mix, hasNull, travGrid, st, ea, eb, stage);
+        else launchWide<SMEM, 10>(kp, mix, hasNull, travGrid, st, ea, eb, stage);
+        return;
+    }
+    if (bps > 8) travGrid = travGrid / bps * 8;   // the 64-register kernels fit 8 blocks per SM
     if (motion) {
         // animated instances: the MOTION kernels (no speculation, no visit counters)
         if (stage == 0) {
@@ -1933,9 +1957,9 @@ static void launchTraversal(const KParams& kp, int mix, bool hasNull, bool count
 
 template <int SMEM>
 static void launchTraversal(const KParams& kp, int mix, bool hasNull, bool count, int travGrid, cudaStream_t st,
-                            cudaEvent_t ea, cudaEvent_t eb, int stage, bool spec, bool motion) {
-    if (spec) launchTraversal<SMEM, true>(kp, mix, hasNull, count, travGrid, st, ea, eb, stage, motion);
-    else launchTraversal<SMEM, false>(kp, mix, hasNull, count, travGrid, st, ea, eb, stage, motion);
+                            cudaEvent_t ea, cudaEvent_t eb, int stage, bool spec, bool motion, int bps) {
+    if (spec) launchTraversal<SMEM, true>(kp, mix, hasNull, count, travGrid, st, ea, eb, stage, motion, bps);
+    else launchTraversal<SMEM, false>(kp, mix, hasNull, count, travGrid, st, ea, eb, stage, motion, bps);
 }
 
 void Wavefront::setTune(const Tune& t) {
@@ -1947,7 +1971,8 @@ void Wavefront::setTune(const Tune& t) {
 
 void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int profile, cudaStream_t st) {
     const int grid = ctx_->numSMs * 8;
-    const int travGrid = ctx_->numSMs * std::min(std::max(tune_.travBlocks, 1), 8);
+    const int bps = std::min(std::max(tune_.travBlocks, 1), 10);
+    const int travGrid = ctx_->numSMs * bps;
     const bool sort = tune_.sort != 0 || mix == 3;   // an unsorted launch serves one integrator
     uint32_t* lists[2] = {listA_.as<uint32_t>(), listB_.as<uint32_t>()};
     uint32_t* frees[2] = {freeA_.as<uint32_t>(), freeB_.as<uint32_t>()};
@@ -1972,8 +1997,8 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
         evs_.push_back(eb);
     }
     const bool count = (profile & 2) != 0;
-    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0, motion_);
-    else launchTraversal<32>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0, motion_);
+    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0, motion_, bps);
+    else launchTraversal<32>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0, motion_, bps);
     if (sort) {
         uint32_t* cls = classes_.as<uint32_t>();
         kClassify<<<ctx_->numSMs * 16, kBlock, 0, st>>>(kp, cls);   // latency-bound: a full SM of warps
@@ -2001,8 +2026,8 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
         kRayClear<<<64, 1024, 0, st>>>(kp.rayBins);
         kp.shadowOrder = kp.raySorted;
     }
-    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0, motion_);
-    else launchTraversal<32>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0, motion_);
+    if (tune_.smem == 16) launchTraversal<16>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0, motion_, bps);
+    else launchTraversal<32>(kp, mix, hasNull, false, travGrid, st, nullptr, nullptr, 1, tune_.specShadow != 0, motion_, bps);
     if (mix & 2) {
         if (motion_) kShadow<true, true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
         else kShadow<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
@@ -2314,7 +2339,7 @@ gnd_status gnd_gpu_render_fixed(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_re
 static Tune tuneFromC(const gnd_tune& t) {
     if (t.pool_log2 < 16 || t.pool_log2 > 26) throw Error(GND_ERR_INVALID, "pool_log2 must be in 16..26");
     if (t.round_iters < 2 || t.round_iters > 64 || (t.round_iters & 1)) throw Error(GND_ERR_INVALID, "round_iters must be even, 2..64");
-    if (t.trav_blocks < 1 || t.trav_blocks > 8) throw Error(GND_ERR_INVALID, "trav_blocks must be in 1..8");
+    if (t.trav_blocks < 1 || t.trav_blocks > 10) throw Error(GND_ERR_INVALID, "trav_blocks must be in 1..10");
     if (t.material_sort != 0 && t.material_sort != 1) throw Error(GND_ERR_INVALID, "material_sort must be 0 or 1");
     if (t.stack_smem != 16 && t.stack_smem != 32) throw Error(GND_ERR_INVALID, "stack_smem must be 16 or 32");
     if (t.graphs != 0 && t.graphs != 1) throw Error(GND_ERR_INVALID, "graphs must be 0 or 1");
@@ -2423,7 +2448,7 @@ gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t spp, int
             std::vector<int> values;
         };
         const std::vector<Knob> knobs = {
-            {&Tune::travBlocks, {8, 6, 4}}, {&Tune::smem, {32, 16}},          {&Tune::sort, {1, 0}},
+            {&Tune::travBlocks, {8, 9, 10, 6, 4}}, {&Tune::smem, {32, 16}},          {&Tune::sort, {1, 0}},
             {&Tune::poolLog2, {22, 21, 23, 20}}, {&Tune::roundIters, {8, 16, 4}}, {&Tune::graphs, {1, 0}},
             {&Tune::sampleFilm, {1, 0}}, {&Tune::specExtend, {1, 0}}, {&Tune::specShadow, {1, 0}},
             {&Tune::raySort, {1, 3, 0}}, {&Tune::leafBatch, {16, 8, 24, 32}}, {&Tune::shadowLeafBatch, {16, 8, 24, 32}},

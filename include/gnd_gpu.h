@@ -386,7 +386,9 @@ gnd_status gnd_gpu_counters(gnd_gpu_ctx* ctx, gnd_counters* out, int32_t reset);
 typedef struct gnd_tune {
     int32_t pool_log2;        /* path slots of a batched render: 2^pool_log2 (16..26) */
     int32_t round_iters;      /* wavefront iterations per host round, batched (2..64, even) */
-    int32_t trav_blocks;      /* persistent traversal blocks of 128 threads per SM (1..8) */
+    int32_t trav_blocks;      /* persistent traversal blocks of 128 threads per SM (1..10; 9
+                                 and 10 run the plain closest-hit and shadow kernels
+                                 compiled to fit them, with fewer registers per thread) */
     int32_t material_sort;    /* 1: classify hits and shade per material class; 0: one kernel */
     int32_t stack_smem;       /* traversal stack entries in shared memory: 16 or 32 */
     int32_t graphs;           /* 1: replay pairs of iterations as CUDA graphs */

@@ -18,6 +18,7 @@ VARIANTS = [dict(material_sort=0), dict(stack_smem=16), dict(trav_blocks=4), dic
             dict(ray_sort=1), dict(ray_sort=3), dict(ray_sort=2, graphs=0, pool_log2=16),
             dict(leaf_batch=16), dict(leaf_batch=1, spec_extend=1), dict(leaf_batch=8, stack_smem=16),
             dict(shadow_leaf_batch=12), dict(shadow_leaf_batch=1, spec_shadow=1),
+            dict(trav_blocks=9), dict(trav_blocks=10, leaf_batch=16), dict(trav_blocks=10, spec_extend=1),
             dict(material_sort=0, stack_smem=16, trav_blocks=2, pool_log2=16, round_iters=4, graphs=0)]
 
 
