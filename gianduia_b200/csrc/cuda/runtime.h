@@ -135,11 +135,12 @@ struct Tune {
     int leafBatch = 32;       // closest-hit traversal of renders: lanes holding a leaf that end the node phase
     int traceLeafBatch = 12;  // the same for the scene's ray batches
     int shadowLeafBatch = 32; // the same for the path tracer's shadow queries
+    int traceBlocks = 8;      // persistent blocks per SM of the scene's ray batches
     bool operator==(const Tune& o) const {
         return poolLog2 == o.poolLog2 && roundIters == o.roundIters && travBlocks == o.travBlocks && sort == o.sort &&
                smem == o.smem && graphs == o.graphs && sampleFilm == o.sampleFilm && specExtend == o.specExtend &&
                specShadow == o.specShadow && raySort == o.raySort && leafBatch == o.leafBatch &&
-               traceLeafBatch == o.traceLeafBatch && shadowLeafBatch == o.shadowLeafBatch;
+               traceLeafBatch == o.traceLeafBatch && shadowLeafBatch == o.shadowLeafBatch && traceBlocks == o.traceBlocks;
     }
     bool operator!=(const Tune& o) const { return !(*this == o); }
 };

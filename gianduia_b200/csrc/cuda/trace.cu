@@ -62,8 +62,10 @@ struct BatchSrc {
     }
 };
 
-template <bool ANY, bool COUNT>
-__global__ void __launch_bounds__(kTraceBlock, kTraceBlocksPerSM)
+// MINB: blocks per SM the kernel is compiled to fit (8: 64 registers; 9 and 10 trade
+// registers, some spilled, for more resident warps; gnd_tune trace_blocks).
+template <bool ANY, bool COUNT, int MINB = kTraceBlocksPerSM>
+__global__ void __launch_bounds__(kTraceBlock, MINB)
     traceKernel(const SceneView* __restrict__ sv, const gnd_ray* __restrict__ rays, uint32_t n, gnd_hit* __restrict__ hits,
                 uint8_t* __restrict__ occ, uint32_t* __restrict__ nodesOut, uint32_t* __restrict__ trisOut,
                 uint32_t* fetch, uint32_t* errWord, unsigned long long* totals, const uint32_t* __restrict__ perm,
@@ -133,7 +135,9 @@ void launchTrace(Context* c, DeviceScene& ds, const gnd_ray* dr, int64_t n, gnd_
     if (n <= 0) return;
     if (n >= (int64_t)0xF0000000LL) throw Error(GND_ERR_INVALID, "ray batch too large (limit 4e9 rays per call)");
     int64_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
-    int g = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)c->numSMs * kTraceBlocksPerSM));
+    // the counting kernel always fits 8 blocks per SM
+    const int bps = dn ? kTraceBlocksPerSM : std::min(std::max(ds.tune.traceBlocks, 1), 10);
+    int g = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)c->numSMs * bps));
     uint32_t* ew = c->errWord.as<uint32_t>();
     uint32_t* fetch = c->nextFetchCounter();
     GND_CUDA(cudaMemsetAsync(fetch, 0, sizeof(uint32_t), st));
@@ -158,7 +162,11 @@ void launchTrace(Context* c, DeviceScene& ds, const gnd_ray* dr, int64_t n, gnd_
     }
     const uint32_t lb = (uint32_t)ds.tune.traceLeafBatch;
     if (dn) traceKernel<false, true><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, nullptr, dn, dt, fetch, ew, tot, order, lb);
+    else if (docc && bps == 9) traceKernel<true, false, 9><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew, tot, order, lb);
+    else if (docc && bps == 10) traceKernel<true, false, 10><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew, tot, order, lb);
     else if (docc) traceKernel<true, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, nullptr, docc, nullptr, nullptr, fetch, ew, tot, order, lb);
+    else if (bps == 9) traceKernel<false, false, 9><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew, tot, order, lb);
+    else if (bps == 10) traceKernel<false, false, 10><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew, tot, order, lb);
     else traceKernel<false, false><<<g, kTraceBlock, 0, st>>>(sv, dr, nn, dh, nullptr, nullptr, nullptr, fetch, ew, tot, order, lb);
     GND_CUDA(cudaGetLastError());
     c->counters.trace_batches += 1;

@@ -2350,6 +2350,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     if (t.leaf_batch < 1 || t.leaf_batch > 32) throw Error(GND_ERR_INVALID, "leaf_batch must be in 1..32");
     if (t.trace_leaf_batch < 1 || t.trace_leaf_batch > 32) throw Error(GND_ERR_INVALID, "trace_leaf_batch must be in 1..32");
     if (t.shadow_leaf_batch < 1 || t.shadow_leaf_batch > 32) throw Error(GND_ERR_INVALID, "shadow_leaf_batch must be in 1..32");
+    if (t.trace_blocks < 1 || t.trace_blocks > 10) throw Error(GND_ERR_INVALID, "trace_blocks must be in 1..10");
     Tune r;
     r.poolLog2 = t.pool_log2;
     r.roundIters = t.round_iters;
@@ -2364,6 +2365,7 @@ static Tune tuneFromC(const gnd_tune& t) {
     r.leafBatch = t.leaf_batch;
     r.traceLeafBatch = t.trace_leaf_batch;
     r.shadowLeafBatch = t.shadow_leaf_batch;
+    r.traceBlocks = t.trace_blocks;
     return r;
 }
 
@@ -2382,6 +2384,7 @@ static gnd_tune tuneToC(const Tune& t) {
     r.leaf_batch = t.leafBatch;
     r.trace_leaf_batch = t.traceLeafBatch;
     r.shadow_leaf_batch = t.shadowLeafBatch;
+    r.trace_blocks = t.traceBlocks;
     return r;
 }
 

@@ -415,6 +415,8 @@ typedef struct gnd_tune {
     int32_t trace_leaf_batch; /* the same for the scene's ray batches (gnd_gpu_trace_*,
                                  except the _fixed form); default 12 */
     int32_t shadow_leaf_batch; /* the same for the path tracer's shadow queries; default 32 */
+    int32_t trace_blocks;     /* persistent blocks of 128 threads per SM for the scene's ray
+                                 batches (1..10, as trav_blocks; default 8) */
 } gnd_tune;
 gnd_status gnd_gpu_get_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_tune* tune);
 gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_tune* tune);

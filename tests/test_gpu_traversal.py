@@ -171,8 +171,8 @@ def test_key_ordered_batches(ctx):
     sid = ctx.upload(hs)
     try:
         out = {}
-        for rs, lb in ((0, 32), (4, 12), (0, 1), (4, 7)):
-            ctx.set_tune(sid, ray_sort=rs, trace_leaf_batch=lb)
+        for rs, lb, tb in ((0, 32, 8), (4, 12, 8), (0, 1, 9), (4, 7, 10), (0, 12, 9)):
+            ctx.set_tune(sid, ray_sort=rs, trace_leaf_batch=lb, trace_blocks=tb)
             closest = ctx.trace_closest(sid, rays)
             occ = ctx.trace_any(sid, rays)
             dr = torch.from_numpy(rays).cuda()
@@ -180,18 +180,18 @@ def test_key_ordered_batches(ctx):
             tris = torch.zeros(rays.shape[0], dtype=torch.int32, device="cuda")
             ctx.trace_count_dev(sid, dr.data_ptr(), rays.shape[0], nodes.data_ptr(), tris.data_ptr())
             torch.cuda.synchronize()
-            out[(rs, lb)] = (closest, occ, nodes.cpu().numpy(), tris.cpu().numpy())
-        a = out[(0, 32)]
+            out[(rs, lb, tb)] = (closest, occ, nodes.cpu().numpy(), tris.cpu().numpy())
+        a = out[(0, 32, 8)]
         for key, b in out.items():
             assert a[0].tobytes() == b[0].tobytes(), key
             assert np.array_equal(a[1], b[1]), key
             assert np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3]), key
-        b = out[(4, 12)]
+        b = out[(4, 12, 8)]
         sample = rays[::16]
         ref = O.Scene.from_triangles(tri).trace(sample)
         compare_closest(b[0][::16], ref, sample, "key-ordered")
     finally:
-        ctx.set_tune(sid, ray_sort=0, trace_leaf_batch=12)
+        ctx.set_tune(sid, ray_sort=0, trace_leaf_batch=12, trace_blocks=8)
         ctx.free_scene(sid)
 
 

@@ -12,7 +12,7 @@ pytestmark = [pytest.mark.gpu, pytest.mark.timeout(600)]
 
 DEFAULTS = dict(pool_log2=22, round_iters=8, trav_blocks=8, material_sort=1, stack_smem=32, graphs=1, sample_film=1,
                 spec_extend=0, spec_shadow=0, ray_sort=0, leaf_batch=32, trace_leaf_batch=12,
-                shadow_leaf_batch=32)
+                shadow_leaf_batch=32, trace_blocks=8)
 VARIANTS = [dict(material_sort=0), dict(stack_smem=16), dict(trav_blocks=4), dict(pool_log2=16),
             dict(round_iters=2), dict(graphs=0), dict(sample_film=0), dict(spec_extend=1), dict(spec_shadow=1),
             dict(ray_sort=1), dict(ray_sort=3), dict(ray_sort=2, graphs=0, pool_log2=16),
