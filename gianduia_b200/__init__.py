@@ -497,7 +497,7 @@ class GpuContext:
         """Engine settings of the serving thread (the defaults of gnd_tune, updated by fields)."""
         t = Tune(pool_log2=22, round_iters=4, trav_blocks=8, material_sort=1, stack_smem=32, graphs=1, sample_film=1,
                  spec_extend=0, spec_shadow=0, ray_sort=0, leaf_batch=32, trace_leaf_batch=12,
-                 shadow_leaf_batch=32, trace_blocks=8, top_inline=0)
+                 shadow_leaf_batch=32, trace_blocks=8)
         for k, v in fields.items():
             setattr(t, k, int(v))
         _check(lib().gnd_gpu_serve_tune(self._h, ctypes.byref(t)), "gnd_gpu_serve_tune")
@@ -584,8 +584,7 @@ class Tune(ctypes.Structure):
                 ("material_sort", ctypes.c_int32), ("stack_smem", ctypes.c_int32), ("graphs", ctypes.c_int32),
                 ("sample_film", ctypes.c_int32), ("spec_extend", ctypes.c_int32), ("spec_shadow", ctypes.c_int32),
                 ("ray_sort", ctypes.c_int32), ("leaf_batch", ctypes.c_int32), ("trace_leaf_batch", ctypes.c_int32),
-                ("shadow_leaf_batch", ctypes.c_int32), ("trace_blocks", ctypes.c_int32),
-                ("top_inline", ctypes.c_int32)]
+                ("shadow_leaf_batch", ctypes.c_int32), ("trace_blocks", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}

@@ -136,13 +136,11 @@ struct Tune {
     int traceLeafBatch = 12;  // the same for the scene's ray batches
     int shadowLeafBatch = 32; // the same for the path tracer's shadow queries
     int traceBlocks = 8;      // persistent blocks per SM of the scene's ray batches
-    int topInline = 0;        // traversal: top-level leaves taken in the node phase
     bool operator==(const Tune& o) const {
         return poolLog2 == o.poolLog2 && roundIters == o.roundIters && travBlocks == o.travBlocks && sort == o.sort &&
                smem == o.smem && graphs == o.graphs && sampleFilm == o.sampleFilm && specExtend == o.specExtend &&
                specShadow == o.specShadow && raySort == o.raySort && leafBatch == o.leafBatch &&
-               traceLeafBatch == o.traceLeafBatch && shadowLeafBatch == o.shadowLeafBatch && traceBlocks == o.traceBlocks &&
-               topInline == o.topInline;
+               traceLeafBatch == o.traceLeafBatch && shadowLeafBatch == o.shadowLeafBatch && traceBlocks == o.traceBlocks;
     }
     bool operator!=(const Tune& o) const { return !(*this == o); }
 };

@@ -578,15 +578,11 @@ __device__ __forceinline__ uint32_t warpFetch(uint32_t* counter, bool want) {
 // an occluder sooner nearest first).
 // leafBatch (1..32): the node phase ends as soon as that many lanes hold a leaf (32: when
 // no lane can take another node step); lanes still traversing keep their state and go on
-// in the next round. inlineTop: a lane that reaches a top-level leaf takes that leaf's
-// first primitive right away in the node phase (the step the leaf phase would take next:
-// entering a mesh instance, or testing a sphere or cube) instead of waiting for the leaf
-// phase. Either way only the interleaving of the lanes' steps changes, never a ray's
-// sequence of steps.
+// in the next round. Only the interleaving of the lanes' steps changes.
 template <int BLOCK, bool ANY, bool COUNT, int SMEM = kSmemStack, bool SPEC = false, bool MOTION = false,
           bool SLOT_ORDER_ANY = false, typename Src>
 __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter, uint32_t* smemStack, TraceCounters* cnt,
-                                               uint32_t leafBatch = 32, bool inlineTop = false) {
+                                               uint32_t leafBatch = 32) {
     TStack<BLOCK, SMEM> st;
     st.smem = smemStack + threadIdx.x;
     Trav t;
@@ -637,8 +633,6 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
                 break;
             if (want) {
                 int e = travNodeStep<BLOCK, COUNT, SMEM, !(ANY && SLOT_ORDER_ANY)>(t, *sv, st, cnt);
-                if (!e && inlineTop && t.leaf != kEmpty && t.curInst < 0)
-                    e = travLeafStep<BLOCK, ANY, COUNT, SMEM, MOTION>(t, *sv, st, cnt, nm);
                 if (e || ++iter > kMaxIterations) {
                     err |= e ? e : (int)kTraceIterLimit;
                     t.sp = 0; t.leaf = kEmpty; t.next = kEmpty;

@@ -96,7 +96,6 @@ struct KParams {
     const uint32_t* shadowOrder;   // order in which kShadowPath takes the shadow records, or null
     uint32_t leafBatch;            // closest-hit traversal: lanes holding a leaf that end the node phase (1..32)
     uint32_t shadowLeafBatch;      // the same for the shadow queries
-    uint32_t topInline;            // 1: top-level leaves are taken in the node phase
     uint32_t capacity;
     uint32_t fifo;                 // 1: grabs walk the active list from its first job
 };
@@ -828,8 +827,7 @@ __global__ void __launch_bounds__(kBlock, MINB) kExtend(KParams p) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[0], (unsigned long long)n);
     TraceCounters cnt{0, 0};
     ExtendSrc src{&p, n, 0};
-    int err = persistentTrace<kBlock, false, COUNT, SMEM, SPEC, MOTION>(src, p.cnt + kQFetchA, stack, &cnt, p.leafBatch,
-                                                                         p.topInline != 0);
+    int err = persistentTrace<kBlock, false, COUNT, SMEM, SPEC, MOTION>(src, p.cnt + kQFetchA, stack, &cnt, p.leafBatch);
     if (COUNT) {
         unsigned long long nn = cnt.nodes, nt = cnt.tris;
         for (int o = 16; o > 0; o >>= 1) {
@@ -1208,7 +1206,7 @@ __global__ void __launch_bounds__(kBlock, MINB) kShadowPath(KParams p, bool mixe
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
     ShadowSrc<ANY> src{&p, n, 0, nullptr, mixed};
     int err = persistentTrace<kBlock, ANY, false, SMEM, SPEC, MOTION, true>(src, p.cnt + kQFetchB, stack, nullptr,
-                                                                            p.shadowLeafBatch, p.topInline != 0);
+                                                                            p.shadowLeafBatch);
     if (err) atomicOr(p.errWord, (uint32_t)err);
 }
 
@@ -2109,7 +2107,6 @@ void Wavefront::enqueueRound(int iters, int mix, bool hasNull, int profile, Resu
     kp.classLists = classes_.as<uint32_t>();
     kp.leafBatch = (uint32_t)tune_.leafBatch;
     kp.shadowLeafBatch = (uint32_t)tune_.shadowLeafBatch;
-    kp.topInline = (uint32_t)tune_.topInline;
     kp.rayKeys = rayKeys_.as<uint32_t>();
     kp.rayBins = rayBins_.as<uint32_t>();
     kp.raySorted = raySorted_.as<uint32_t>();
@@ -2354,7 +2351,6 @@ static Tune tuneFromC(const gnd_tune& t) {
     if (t.trace_leaf_batch < 1 || t.trace_leaf_batch > 32) throw Error(GND_ERR_INVALID, "trace_leaf_batch must be in 1..32");
     if (t.shadow_leaf_batch < 1 || t.shadow_leaf_batch > 32) throw Error(GND_ERR_INVALID, "shadow_leaf_batch must be in 1..32");
     if (t.trace_blocks < 1 || t.trace_blocks > 10) throw Error(GND_ERR_INVALID, "trace_blocks must be in 1..10");
-    if (t.top_inline != 0 && t.top_inline != 1) throw Error(GND_ERR_INVALID, "top_inline must be 0 or 1");
     Tune r;
     r.poolLog2 = t.pool_log2;
     r.roundIters = t.round_iters;
@@ -2370,7 +2366,6 @@ static Tune tuneFromC(const gnd_tune& t) {
     r.traceLeafBatch = t.trace_leaf_batch;
     r.shadowLeafBatch = t.shadow_leaf_batch;
     r.traceBlocks = t.trace_blocks;
-    r.topInline = t.top_inline;
     return r;
 }
 
@@ -2390,7 +2385,6 @@ static gnd_tune tuneToC(const Tune& t) {
     r.trace_leaf_batch = t.traceLeafBatch;
     r.shadow_leaf_batch = t.shadowLeafBatch;
     r.trace_blocks = t.traceBlocks;
-    r.top_inline = t.topInline;
     return r;
 }
 
@@ -2461,7 +2455,6 @@ gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t spp, int
             {&Tune::poolLog2, {22, 21, 23, 20}}, {&Tune::roundIters, {8, 16, 4}}, {&Tune::graphs, {1, 0}},
             {&Tune::sampleFilm, {1, 0}}, {&Tune::specExtend, {1, 0}}, {&Tune::specShadow, {1, 0}},
             {&Tune::raySort, {1, 3, 0}}, {&Tune::leafBatch, {16, 8, 24, 32}}, {&Tune::shadowLeafBatch, {16, 8, 24, 32}},
-            {&Tune::topInline, {1, 0}},
         };
         for (int sweep = 0; sweep < 2; ++sweep) {
             bool changed = false;

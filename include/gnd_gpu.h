@@ -417,11 +417,6 @@ typedef struct gnd_tune {
     int32_t shadow_leaf_batch; /* the same for the path tracer's shadow queries; default 32 */
     int32_t trace_blocks;     /* persistent blocks of 128 threads per SM for the scene's ray
                                  batches (1..10, as trav_blocks; default 8) */
-    int32_t top_inline;       /* 1: in the path tracer's traversals a ray that reaches a
-                                 top-level leaf takes its first primitive (entering a mesh
-                                 instance, or testing a sphere or cube) within the warp's
-                                 inner-node phase instead of waiting for its leaf phase;
-                                 default 0 */
 } gnd_tune;
 gnd_status gnd_gpu_get_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, gnd_tune* tune);
 gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_tune* tune);

@@ -12,15 +12,13 @@ pytestmark = [pytest.mark.gpu, pytest.mark.timeout(600)]
 
 DEFAULTS = dict(pool_log2=22, round_iters=8, trav_blocks=8, material_sort=1, stack_smem=32, graphs=1, sample_film=1,
                 spec_extend=0, spec_shadow=0, ray_sort=0, leaf_batch=32, trace_leaf_batch=12,
-                shadow_leaf_batch=32, trace_blocks=8, top_inline=0)
+                shadow_leaf_batch=32, trace_blocks=8)
 VARIANTS = [dict(material_sort=0), dict(stack_smem=16), dict(trav_blocks=4), dict(pool_log2=16),
             dict(round_iters=2), dict(graphs=0), dict(sample_film=0), dict(spec_extend=1), dict(spec_shadow=1),
             dict(ray_sort=1), dict(ray_sort=3), dict(ray_sort=2, graphs=0, pool_log2=16),
             dict(leaf_batch=16), dict(leaf_batch=1, spec_extend=1), dict(leaf_batch=8, stack_smem=16),
             dict(shadow_leaf_batch=12), dict(shadow_leaf_batch=1, spec_shadow=1),
             dict(trav_blocks=9), dict(trav_blocks=10, leaf_batch=16), dict(trav_blocks=10, spec_extend=1),
-            dict(top_inline=1), dict(top_inline=1, leaf_batch=12, shadow_leaf_batch=12),
-            dict(top_inline=1, spec_extend=1, spec_shadow=1),
             dict(material_sort=0, stack_smem=16, trav_blocks=2, pool_log2=16, round_iters=4, graphs=0)]
 
 
