@@ -933,16 +933,6 @@ void parallelFor(size_t n, F&& f) {
     for (auto& t : th) t.join();
 }
 
-// Rebases inner-node references of a locally built node array.
-void appendNodes(std::vector<gnd::Node4>& dst, const std::vector<gnd::Node4>& src) {
-    uint32_t base = (uint32_t)dst.size();
-    for (gnd::Node4 n : src) {
-        for (int i = 0; i < 4; ++i)
-            if (n.child[i] != gnd::kEmpty && !gnd::isLeaf(n.child[i])) n.child[i] += base;
-        dst.push_back(n);
-    }
-}
-
 }  // namespace
 
 void Scene::build() {
@@ -978,10 +968,10 @@ void Scene::build() {
     int parDepth = meshes.size() == 1 ? 4 : 0;
     if (deviceBlas) {
         // the device builds the mesh trees: keep the original order
-        for (size_t i = 0; i < meshes.size(); ++i) {
+        parallelFor(meshes.size(), [&](size_t i) {
             mb[i].order.resize(meshes[i]->numTris());
             for (size_t t = 0; t < mb[i].order.size(); ++t) mb[i].order[t] = (uint32_t)t;
-        }
+        });
     } else parallelFor(meshes.size(), [&](size_t i) {
         const ShapeObj& m = *meshes[i];
         size_t nt = m.numTris();
@@ -1001,7 +991,7 @@ void Scene::build() {
     size_t np = m_primitives.size();
     std::vector<Bounds> wb(np);
     std::vector<V3> wc(np);
-    for (size_t i = 0; i < np; ++i) {
+    parallelFor(np, [&](size_t i) {
         const PrimitiveObj& pr = *m_primitives[i];
         const Bounds ob = pr.shape->objectBounds();
         wb[i] = ob.transformed(pr.toWorld);
@@ -1010,31 +1000,73 @@ void Scene::build() {
             wb[i].grow(ob.transformed(motionMid(makeMotion(pr.toWorld, pr.toWorldEnd))));
         }
         wc[i] = wb[i].lo * 0.5f + wb[i].hi * 0.5f;
-    }
+    });
     if (np > 0) {
         BinTree tl = buildSAH(wb, wc, 0);
-        fs->tlasRoot = collapseToNode4(tl, 0, wb, fs->nodes);
+        std::vector<gnd::Node4> tlasNodes;
+        fs->tlasRoot = collapseToNode4(tl, 0, wb, tlasNodes);
+        fs->nodes.assign(tlasNodes.begin(), tlasNodes.end());
         fs->tlasList = tl.order;
     }
-    // concatenate the meshes
-    std::vector<uint32_t> blasRoot(meshes.size());
+    // concatenate the meshes: every output offset first, then the meshes (node arrays,
+    // area CDFs) and their triangles (in chunks of kChunk) written on all host cores
+    const size_t nm = meshes.size();
+    std::vector<uint32_t> blasRoot(nm);
+    std::vector<size_t> nodeBase(nm + 1), cdfBase(nm + 1, 0);
+    nodeBase[0] = fs->nodes.size();
+    for (size_t i = 0; i < nm; ++i) {
+        nodeBase[i + 1] = nodeBase[i] + mb[i].nodes.size();
+        cdfBase[i + 1] = cdfBase[i] + meshes[i]->numTris() + 1;
+        blasRoot[i] = mb[i].root == gnd::kEmpty ? gnd::kEmpty : mb[i].root + (uint32_t)nodeBase[i];
+    }
+    fs->nodes.resize(nodeBase[nm]);
     fs->tris.resize(triBase.back());
     fs->attrs.resize(triBase.back());
-    for (size_t i = 0; i < meshes.size(); ++i) {
-        uint32_t base = (uint32_t)fs->nodes.size();
-        appendNodes(fs->nodes, mb[i].nodes);
-        blasRoot[i] = mb[i].root == gnd::kEmpty ? gnd::kEmpty : mb[i].root + base;
+    fs->origToLeaf.resize(triBase.back());
+    fs->cdf.resize(cdfBase[nm]);
+    fs->meshes.resize(nm);
+    parallelFor(nm, [&](size_t i) {
+        const uint32_t base = (uint32_t)nodeBase[i];
+        gnd::Node4* dst = fs->nodes.data() + base;
+        for (gnd::Node4 n : mb[i].nodes) {   // inner-node references rebased
+            for (int c = 0; c < 4; ++c)
+                if (n.child[c] != gnd::kEmpty && !gnd::isLeaf(n.child[c])) n.child[c] += base;
+            *dst++ = n;
+        }
         const ShapeObj& m = *meshes[i];
-        gnd::MeshRec rec{};
-        rec.cdfOffset = (uint32_t)fs->cdf.size();
+        gnd::MeshRec& rec = fs->meshes[i];
+        rec = gnd::MeshRec{};
+        rec.cdfOffset = (uint32_t)cdfBase[i];
         rec.numTris = (uint32_t)m.numTris();
-        rec.origToLeaf = (uint32_t)fs->origToLeaf.size();
-        fs->origToLeaf.resize(fs->origToLeaf.size() + m.numTris());
+        rec.origToLeaf = triBase[i];
+        // area CDF in original triangle order (mesh.cpp:120-145)
+        float* cdf = fs->cdf.data() + cdfBase[i];
+        cdf[0] = 0.0f;
+        float total = 0.0f;
+        for (size_t t = 0; t < m.numTris(); ++t) {
+            V3 e1 = m.positions[3 * t + 1] - m.positions[3 * t];
+            V3 e2 = m.positions[3 * t + 2] - m.positions[3 * t];
+            total += 0.5f * gnd::length(gnd::cross(e1, e2));
+            cdf[t + 1] = total;
+        }
+        if (total > 0.0f)
+            for (size_t t = 1; t <= m.numTris(); ++t) cdf[t] /= total;
+        rec.totalArea = total;
+    });
+    constexpr size_t kChunk = size_t(1) << 16;
+    struct Piece { size_t mesh, lo, hi; };
+    std::vector<Piece> pieces;
+    for (size_t i = 0; i < nm; ++i)
+        for (size_t lo = 0; lo < meshes[i]->numTris(); lo += kChunk)
+            pieces.push_back(Piece{i, lo, std::min(lo + kChunk, meshes[i]->numTris())});
+    parallelFor(pieces.size(), [&](size_t k) {
+        const size_t i = pieces[k].mesh;
+        const ShapeObj& m = *meshes[i];
         bool hasN = !m.normals.empty(), hasUV = !m.uvs.empty();
-        for (size_t s = 0; s < m.numTris(); ++s) {
+        for (size_t s = pieces[k].lo; s < pieces[k].hi; ++s) {
             uint32_t orig = mb[i].order[s];
             uint32_t slot = triBase[i] + (uint32_t)s;
-            fs->origToLeaf[rec.origToLeaf + orig] = slot;
+            fs->origToLeaf[triBase[i] + orig] = slot;
             const V3* P = &m.positions[3 * orig];
             gnd::Tri& t = fs->tris[slot];
             t.v0x = P[0].x; t.v0y = P[0].y; t.v0z = P[0].z; t.prim = orig;
@@ -1054,20 +1086,7 @@ void Scene::build() {
             }
             a.flags = (float)((hasN ? 1 : 0) | (hasUV ? 2 : 0));
         }
-        // area CDF in original triangle order (mesh.cpp:120-145)
-        fs->cdf.push_back(0.0f);
-        float total = 0.0f;
-        for (size_t t = 0; t < m.numTris(); ++t) {
-            V3 e1 = m.positions[3 * t + 1] - m.positions[3 * t];
-            V3 e2 = m.positions[3 * t + 2] - m.positions[3 * t];
-            total += 0.5f * gnd::length(gnd::cross(e1, e2));
-            fs->cdf.push_back(total);
-        }
-        if (total > 0.0f)
-            for (size_t t = 1; t <= m.numTris(); ++t) fs->cdf[rec.cdfOffset + t] /= total;
-        rec.totalArea = total;
-        fs->meshes.push_back(rec);
-    }
+    });
     // emitters in scene-file order (scene.cpp:9-43): area lights of primitives and the
     // standalone point, spot, directional and environment emitters
     std::vector<int32_t> primEmitter(np, -1);

@@ -11,6 +11,8 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "gnd/layout.h"
@@ -365,11 +367,30 @@ protected:
     RenderCallback m_callback;
 };
 
-// Flattened scene: owner of the arrays a gnd_scene_desc points at.
+// Allocator whose construct() without arguments default-initialises: resize() of an
+// array of trivially constructible records reserves it without writing it, so the host
+// threads that fill the array (Scene::build) are the first to touch its pages.
+template <typename T>
+struct UninitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind { using other = UninitAlloc<U>; };
+    UninitAlloc() = default;
+    template <typename U>
+    UninitAlloc(const UninitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible_v<U>) { ::new (static_cast<void*>(p)) U; }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) { ::new (static_cast<void*>(p)) U(std::forward<A>(a)...); }
+};
+template <typename T>
+using FlatArray = std::vector<T, UninitAlloc<T>>;
+
+// Flattened scene: owner of the arrays a gnd_scene_desc points at. The per-triangle
+// arrays are FlatArrays; Scene::build writes every element.
 struct FlatScene {
-    std::vector<gnd::Node4> nodes;
-    std::vector<gnd::Tri> tris;
-    std::vector<gnd::TriAttr> attrs;
+    FlatArray<gnd::Node4> nodes;
+    FlatArray<gnd::Tri> tris;
+    FlatArray<gnd::TriAttr> attrs;
     std::vector<gnd::InstTrav> instT;
     std::vector<gnd::InstShade> instS;
     std::vector<uint32_t> tlasList;
@@ -377,8 +398,8 @@ struct FlatScene {
     std::vector<gnd::Emitter> emitters;
     std::vector<gnd::Medium> media;
     std::vector<gnd::MeshRec> meshes;
-    std::vector<float> cdf;
-    std::vector<uint32_t> origToLeaf;
+    FlatArray<float> cdf;
+    FlatArray<uint32_t> origToLeaf;
     std::vector<gnd::InstMotion> motion;   // per instance when any instance moves, else empty
     std::vector<float> envTexels, envDist;
     TexTables textures;

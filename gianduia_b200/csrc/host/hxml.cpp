@@ -3,9 +3,12 @@
 // t = step * t) and the OBJ reader for meshes (mesh.cpp:148-229).
 #include <atomic>
 #include <cctype>
+#include <charconv>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <filesystem>
+#include <memory>
 #include <fstream>
 #include <mutex>
 #include <sstream>
@@ -349,29 +352,78 @@ std::shared_ptr<GndObject> loadFromXML(const std::string& path, bool deferPrepro
 // mesh.cpp:148-229 for v / vt / vn / f (polygons split as fans). When the file has no
 // normals, smooth normals are generated per original vertex (area-weighted face
 // normals, normalised), as the reference does.
+namespace {
+
+// strtod(p) converted to float, and the end of the number: std::from_chars takes the plain
+// forms; any form it does not parse whole (a sign '+', leading white space other than
+// blanks and tabs, hexadecimal, an out-of-range value) goes to strtod itself, so the
+// values are strtod's in every case. `lineEnd` is the NUL that ends p's line.
+float objFloat(const char* p, const char* lineEnd, const char** end) {
+    const char* q = p;
+    while (*q == ' ' || *q == '\t') ++q;
+    double d;
+    const auto r = std::from_chars(q, lineEnd, d);
+    if (r.ec == std::errc{} && (r.ptr == lineEnd || *r.ptr == ' ' || *r.ptr == '\t' || *r.ptr == '\r')) {
+        *end = r.ptr;
+        return (float)d;
+    }
+    char* e;
+    d = std::strtod(p, &e);
+    *end = e;
+    return (float)d;
+}
+
+// strtol(p, 10) and the end of the number, by the same rule.
+long objIndex(const char* p, const char* lineEnd, const char** end) {
+    long v;
+    const auto r = std::from_chars(p, lineEnd, v);
+    if (r.ec == std::errc{}) {
+        *end = r.ptr;
+        return v;
+    }
+    char* e;
+    v = std::strtol(p, &e, 10);
+    *end = e;
+    return v;
+}
+
+}  // namespace
+
 void loadOBJ(const std::string& path, ShapeObj& mesh) {
-    std::ifstream f(path);
-    if (!f) throw std::runtime_error("Failed to load OBJ: " + path);
+    // the whole file in one read; each line ends in a NUL where its '\n' was
+    std::string text;
+    {
+        std::unique_ptr<FILE, int (*)(FILE*)> f(std::fopen(path.c_str(), "rb"), std::fclose);
+        if (!f) throw std::runtime_error("Failed to load OBJ: " + path);
+        char buf[1 << 16];
+        size_t got;
+        while ((got = std::fread(buf, 1, sizeof(buf), f.get())) > 0) text.append(buf, got);
+        if (std::ferror(f.get())) throw std::runtime_error("Failed to load OBJ: " + path);
+    }
     std::vector<float> V, T, N;
     struct Corner { int v, t, n; };
     std::vector<Corner> corners;
-    std::string line;
     std::vector<Corner> poly;
     auto resolve = [](long idx, size_t count) -> int { return (int)(idx < 0 ? (long)count + idx : idx - 1); };
-    while (std::getline(f, line)) {
-        const char* p = line.c_str();
+    char* const textEnd = text.data() + text.size();
+    for (char* line = text.data(); line < textEnd;) {
+        char* nl = static_cast<char*>(std::memchr(line, '\n', (size_t)(textEnd - line)));
+        char* lineEnd = nl ? nl : textEnd;
+        *lineEnd = '\0';   // textEnd is the string's own terminator
+        const char* p = line;
+        line = lineEnd + 1;
         while (*p == ' ' || *p == '\t') ++p;
         if (p[0] == 'v' && (p[1] == ' ' || p[1] == '\t')) {
-            char* e;
-            float x = (float)std::strtod(p + 2, &e), y = (float)std::strtod(e, &e), z = (float)std::strtod(e, &e);
+            const char* e;
+            float x = objFloat(p + 2, lineEnd, &e), y = objFloat(e, lineEnd, &e), z = objFloat(e, lineEnd, &e);
             V.push_back(x); V.push_back(y); V.push_back(z);
         } else if (p[0] == 'v' && p[1] == 't') {
-            char* e;
-            float u = (float)std::strtod(p + 2, &e), v = (float)std::strtod(e, &e);
+            const char* e;
+            float u = objFloat(p + 2, lineEnd, &e), v = objFloat(e, lineEnd, &e);
             T.push_back(u); T.push_back(v);
         } else if (p[0] == 'v' && p[1] == 'n') {
-            char* e;
-            float x = (float)std::strtod(p + 2, &e), y = (float)std::strtod(e, &e), z = (float)std::strtod(e, &e);
+            const char* e;
+            float x = objFloat(p + 2, lineEnd, &e), y = objFloat(e, lineEnd, &e), z = objFloat(e, lineEnd, &e);
             N.push_back(x); N.push_back(y); N.push_back(z);
         } else if (p[0] == 'f' && (p[1] == ' ' || p[1] == '\t')) {
             poly.clear();
@@ -379,14 +431,14 @@ void loadOBJ(const std::string& path, ShapeObj& mesh) {
             for (;;) {
                 while (*q == ' ' || *q == '\t') ++q;
                 if (!*q || *q == '\r' || *q == '#') break;
-                char* e;
+                const char* e;
                 Corner c{-1, -1, -1};
-                c.v = resolve(std::strtol(q, &e, 10), V.size() / 3);
+                c.v = resolve(objIndex(q, lineEnd, &e), V.size() / 3);
                 q = e;
                 if (*q == '/') {
                     ++q;
-                    if (*q != '/') { c.t = resolve(std::strtol(q, &e, 10), T.size() / 2); q = e; }
-                    if (*q == '/') { ++q; c.n = resolve(std::strtol(q, &e, 10), N.size() / 3); q = e; }
+                    if (*q != '/') { c.t = resolve(objIndex(q, lineEnd, &e), T.size() / 2); q = e; }
+                    if (*q == '/') { ++q; c.n = resolve(objIndex(q, lineEnd, &e), N.size() / 3); q = e; }
                 }
                 if (c.v < 0 || (size_t)c.v >= V.size() / 3) throw std::runtime_error("OBJ: vertex index out of range in " + path);
                 if (c.t >= (int)(T.size() / 2) || c.n >= (int)(N.size() / 3)) throw std::runtime_error("OBJ: attribute index out of range in " + path);

@@ -144,3 +144,62 @@ def test_obj_loader_polygons_and_negative_indices(tmp_path):
     hs = G.HostScene.load_xml(str(tmp_path / "s.xml"))
     assert hs.desc.num_tris == 2
     _check_bvh(hs, 2)
+
+
+def _mesh_scene(tmp_path, names):
+    prims = "".join(
+        f'<primitive><shape type="mesh"><string name="filename" value="{n}"/></shape>'
+        '<emitter type="area"><color name="radiance" value="1 1 1"/></emitter></primitive>' for n in names)
+    (tmp_path / "s.xml").write_text(
+        '<scene><camera type="perspective"/><sampler type="independent"/><integrator type="path_gpu"/>'
+        + prims + '</scene>')
+    return str(tmp_path / "s.xml")
+
+
+def test_obj_loader_number_forms(tmp_path):
+    """Coordinates are strtod's values rounded to float in every written form (a sign,
+    hexadecimal, values below the float range, more digits than a double holds, tabs,
+    CRLF line ends, a comment after a face, no newline at the end)."""
+    vs = [("+1.25", "\t-0.5", "1e-50"), ("1e-40", "0x1.8p1", "2.9999999999999999"),
+          ("1.000000000000000000000001", "-0", "  7"), ("4.9e-324", "1.17549435e-38", "0.1")]
+    text = "".join(f"v {a} {b} {c}\r\n" for a, b, c in vs) + "f +1 2 3 #tri\r\nf\t-1 -2 -3"
+    (tmp_path / "n.obj").write_text(text, newline="")
+
+    def val(s):
+        s = s.strip()
+        return np.float32(float.fromhex(s) if "0x" in s else float(s))
+
+    want = np.array([[val(x) for x in v] for v in vs], np.float32)
+    hs = G.HostScene.load_xml(_mesh_scene(tmp_path, ["n.obj"]), device_blas=True)
+    got = hs.tris().reshape(-1, 3, 4)[:, :, :3]
+    assert got.tobytes() == want[[0, 1, 2, 3, 2, 1]].reshape(2, 3, 3).tobytes()
+
+
+@pytest.mark.parametrize("device_blas", [False, True])
+def test_flatten_many_meshes(tmp_path, device_blas):
+    """Meshes are concatenated in first-use order, each triangle at its mesh's base plus its
+    leaf position; one mesh spans more than one 65,536-triangle piece of the flattening."""
+    rng = np.random.default_rng(5)
+    sizes = [3, 70001, 1, 500]
+    meshes = []
+    for k, n in enumerate(sizes):
+        p = (rng.random((n, 3, 3)) + k).astype(np.float32)
+        meshes.append(p)
+        lines = [f"v {x!r} {y!r} {z!r}" for x, y, z in p.reshape(-1, 3).astype(np.float64).tolist()]
+        lines += [f"f {3 * t + 1} {3 * t + 2} {3 * t + 3}" for t in range(n)]
+        (tmp_path / f"m{k}.obj").write_text("\n".join(lines) + "\n")
+    hs = G.HostScene.load_xml(_mesh_scene(tmp_path, [f"m{k}.obj" for k in range(len(sizes))]),
+                              device_blas=device_blas)
+    tris = hs.tris().reshape(-1, 3, 4)
+    prim = tris[:, 0, 3].copy().view(np.uint32)
+    base = np.concatenate([[0], np.cumsum(sizes)])
+    assert len(tris) == base[-1]
+    for k, p in enumerate(meshes):
+        seg = tris[base[k]:base[k + 1]]
+        order = prim[base[k]:base[k + 1]]
+        assert np.array_equal(np.sort(order), np.arange(sizes[k]))
+        if device_blas:
+            assert np.array_equal(order, np.arange(sizes[k]))
+        assert seg[:, :, :3].tobytes() == p[order].tobytes()
+    if not device_blas:
+        _check_bvh(hs, int(base[-1]))
