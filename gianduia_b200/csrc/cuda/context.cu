@@ -21,12 +21,14 @@ Context::~Context() {
     wave.reset();
     scenes.clear();
     if (stream) cudaStreamSynchronize(stream);
+    if (uploadStream) cudaStreamSynchronize(uploadStream);
     cudaMemPool_t pool = nullptr;
     if (device >= 0 && cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     errWord.release();
     rayScratch.release();
     hitScratch.release();
     if (stream) cudaStreamDestroy(stream);
+    if (uploadStream) cudaStreamDestroy(uploadStream);
 }
 
 void Context::checkKernelErrors(const char* what) {
@@ -168,6 +170,7 @@ gnd_status gnd_gpu_create(int device, gnd_gpu_ctx** out) {
             throw Error(GND_ERR_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100 (this build targets sm_100a)");
         c->numSMs = prop.multiProcessorCount;
         GND_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        GND_CUDA(cudaStreamCreateWithFlags(&c->uploadStream, cudaStreamNonBlocking));
         // scene arrays come from the default memory pool; keep freed memory in the pool
         // (a process-local setting) so that scene uploads reuse it
         cudaMemPool_t pool = nullptr;
@@ -266,34 +269,37 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         }
         validateTextures(d);
         c->bind();
-        std::lock_guard<FairMutex> lk(c->mu);
+        // the copies, the tree build and the validation run on the upload stream without
+        // the context lock (a render may be running); the lock publishes the scene
+        std::lock_guard<std::mutex> ul(c->uploadMu);
+        cudaStream_t st = c->uploadStream;
         auto ds = std::make_unique<DeviceScene>();
         SceneView& v = ds->view;
         PoolBuf rawTris, rawAttrs;   // original order, for the device tree build
         if (!deviceBlas) {
-            v.nodes = upload<Node4>(*ds, c->stream, d->nodes, d->num_nodes);
-            v.tris = upload<Tri>(*ds, c->stream, d->tris, d->num_tris);
-            v.attrs = upload<TriAttr>(*ds, c->stream, d->tri_attrs, d->num_tris);
+            v.nodes = upload<Node4>(*ds, st, d->nodes, d->num_nodes);
+            v.tris = upload<Tri>(*ds, st, d->tris, d->num_tris);
+            v.attrs = upload<TriAttr>(*ds, st, d->tri_attrs, d->num_tris);
         } else {
-            rawTris = PoolBuf(std::max<size_t>((size_t)d->num_tris * sizeof(Tri), 16), c->stream);
-            rawAttrs = PoolBuf(std::max<size_t>((size_t)d->num_tris * sizeof(TriAttr), 16), c->stream);
+            rawTris = PoolBuf(std::max<size_t>((size_t)d->num_tris * sizeof(Tri), 16), st);
+            rawAttrs = PoolBuf(std::max<size_t>((size_t)d->num_tris * sizeof(TriAttr), 16), st);
             if (d->num_tris) {
-                GND_CUDA(cudaMemcpyAsync(rawTris.ptr, d->tris, (size_t)d->num_tris * sizeof(Tri), cudaMemcpyHostToDevice, c->stream));
-                GND_CUDA(cudaMemcpyAsync(rawAttrs.ptr, d->tri_attrs, (size_t)d->num_tris * sizeof(TriAttr), cudaMemcpyHostToDevice, c->stream));
+                GND_CUDA(cudaMemcpyAsync(rawTris.ptr, d->tris, (size_t)d->num_tris * sizeof(Tri), cudaMemcpyHostToDevice, st));
+                GND_CUDA(cudaMemcpyAsync(rawAttrs.ptr, d->tri_attrs, (size_t)d->num_tris * sizeof(TriAttr), cudaMemcpyHostToDevice, st));
             }
         }
-        v.instT = upload<InstTrav>(*ds, c->stream, d->inst_trav, d->num_instances);
-        v.instS = upload<InstShade>(*ds, c->stream, d->inst_shade, d->num_instances);
-        v.tlasList = upload<uint32_t>(*ds, c->stream, d->tlas_list, d->tlas_list_len);
-        v.materials = upload<Material>(*ds, c->stream, d->materials, d->num_materials);
-        v.emitters = upload<Emitter>(*ds, c->stream, d->emitters, d->num_emitters);
-        v.media = upload<Medium>(*ds, c->stream, d->media, d->num_media);
-        v.meshes = upload<MeshRec>(*ds, c->stream, d->meshes, d->num_meshes);
-        v.cdf = upload<float>(*ds, c->stream, d->cdf, d->cdf_len);
-        v.origToLeaf = upload<uint32_t>(*ds, c->stream, d->orig_to_leaf, d->orig_to_leaf_len);
-        v.motion = d->inst_motion ? upload<InstMotion>(*ds, c->stream, d->inst_motion, d->num_instances) : nullptr;
-        v.texNodes = upload<TexNode>(*ds, c->stream, d->tex_nodes, d->num_tex_nodes);
-        v.texels = upload<float>(*ds, c->stream, d->tex_texels, (size_t)d->num_tex_texels * 4);
+        v.instT = upload<InstTrav>(*ds, st, d->inst_trav, d->num_instances);
+        v.instS = upload<InstShade>(*ds, st, d->inst_shade, d->num_instances);
+        v.tlasList = upload<uint32_t>(*ds, st, d->tlas_list, d->tlas_list_len);
+        v.materials = upload<Material>(*ds, st, d->materials, d->num_materials);
+        v.emitters = upload<Emitter>(*ds, st, d->emitters, d->num_emitters);
+        v.media = upload<Medium>(*ds, st, d->media, d->num_media);
+        v.meshes = upload<MeshRec>(*ds, st, d->meshes, d->num_meshes);
+        v.cdf = upload<float>(*ds, st, d->cdf, d->cdf_len);
+        v.origToLeaf = upload<uint32_t>(*ds, st, d->orig_to_leaf, d->orig_to_leaf_len);
+        v.motion = d->inst_motion ? upload<InstMotion>(*ds, st, d->inst_motion, d->num_instances) : nullptr;
+        v.texNodes = upload<TexNode>(*ds, st, d->tex_nodes, d->num_tex_nodes);
+        v.texels = upload<float>(*ds, st, d->tex_texels, (size_t)d->num_tex_texels * 4);
         v.numTexNodes = d->num_tex_nodes;
         // environment map (texels + the sampling tables of distribution.cpp)
         v.env = EnvView{};
@@ -304,8 +310,8 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
             if (d->env_emitter >= d->num_emitters || ems[d->env_emitter].type != kEmitEnv || w <= 0 || h <= 0 ||
                 w * h > ((int64_t)1 << 28) || !d->env_texels || !d->env_dist)
                 throw Error(GND_ERR_INVALID, "bad environment map description");
-            v.env.texels = upload<float>(*ds, c->stream, d->env_texels, (size_t)(w * h * 3));
-            const float* dist = upload<float>(*ds, c->stream, d->env_dist, (size_t)(h + (h + 1) + h * w + h * (w + 1) + h));
+            v.env.texels = upload<float>(*ds, st, d->env_texels, (size_t)(w * h * 3));
+            const float* dist = upload<float>(*ds, st, d->env_dist, (size_t)(h + (h + 1) + h * w + h * (w + 1) + h));
             v.env.margFunc = dist;
             v.env.margCdf = dist + h;
             v.env.condFunc = dist + h + (h + 1);
@@ -357,7 +363,7 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
             mi.origToLeaf = const_cast<uint32_t*>(v.origToLeaf);
             mi.leafMax = c->buildLeafMax;
             mi.numSMs = c->numSMs;
-            MeshTreeOutput mo = buildMeshTrees(mi, c->stream);
+            MeshTreeOutput mo = buildMeshTrees(mi, st);
             nanBounds |= mo.nonFinite;
             ds->numNodes = mo.numNodes;
             ds->buildMs = mo.ms;
@@ -375,17 +381,17 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
         ds->numInstances = d->num_instances;
         ds->numMeshes = d->num_meshes;
         // every node reference in range; bounds fit for the fast slab test
-        PoolBuf vflags(16, c->stream);
-        GND_CUDA(cudaMemsetAsync(vflags.ptr, 0, 16, c->stream));
+        PoolBuf vflags(16, st);
+        GND_CUDA(cudaMemsetAsync(vflags.ptr, 0, 16, st));
         if (ds->numNodes > 0) {
             const unsigned grid = (unsigned)std::min<int64_t>((ds->numNodes + 255) / 256, (int64_t)c->numSMs * 8);
-            kValidateNodes<<<grid, 256, 0, c->stream>>>(v.nodes, ds->numNodes, std::max<int64_t>(d->num_tris, d->tlas_list_len),
+            kValidateNodes<<<grid, 256, 0, st>>>(v.nodes, ds->numNodes, std::max<int64_t>(d->num_tris, d->tlas_list_len),
                                                         vflags.as<uint32_t>());
             GND_CUDA(cudaGetLastError());
         }
         uint32_t vf = 0;
-        GND_CUDA(cudaMemcpyAsync(&vf, vflags.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
-        GND_CUDA(cudaStreamSynchronize(c->stream));
+        GND_CUDA(cudaMemcpyAsync(&vf, vflags.ptr, 4, cudaMemcpyDeviceToHost, st));
+        GND_CUDA(cudaStreamSynchronize(st));
         if (vf & kNodeBadRef) throw Error(GND_ERR_INVALID, "node reference out of range");
         if (vf & kNodeBadLeaf) throw Error(GND_ERR_INVALID, "leaf range out of range");
         nanBounds |= (vf & kNodeSlowBounds) != 0;
@@ -405,19 +411,24 @@ gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctxh, const gnd_scene_desc* d, gnd_
             if (t == kMatIndex) { mask[i] = 1; ds->hasNullMaterials = true; }
         }
         ds->nullMask.alloc(mask.size());
-        GND_CUDA(cudaMemcpyAsync(ds->nullMask.ptr, mask.data(), mask.size(), cudaMemcpyHostToDevice, c->stream));
+        GND_CUDA(cudaMemcpyAsync(ds->nullMask.ptr, mask.data(), mask.size(), cudaMemcpyHostToDevice, st));
         ds->instClass.alloc(cls.size());
-        GND_CUDA(cudaMemcpyAsync(ds->instClass.ptr, cls.data(), cls.size(), cudaMemcpyHostToDevice, c->stream));
+        GND_CUDA(cudaMemcpyAsync(ds->instClass.ptr, cls.data(), cls.size(), cudaMemcpyHostToDevice, st));
         v.instClass = ds->instClass.as<uint8_t>();
         ds->viewDev.alloc(sizeof(SceneView));
-        GND_CUDA(cudaMemcpyAsync(ds->viewDev.ptr, &v, sizeof(SceneView), cudaMemcpyHostToDevice, c->stream));
-        GND_CUDA(cudaStreamSynchronize(c->stream));
+        GND_CUDA(cudaMemcpyAsync(ds->viewDev.ptr, &v, sizeof(SceneView), cudaMemcpyHostToDevice, st));
+        GND_CUDA(cudaStreamSynchronize(st));
         ds->bytes += ds->nullMask.bytes + ds->instClass.bytes + ds->viewDev.bytes;
         ds->width = d->width; ds->height = d->height; ds->spp = d->spp; ds->maxDepth = d->max_depth;
         ds->integrator = d->integrator; ds->filter = d->filter;
         ds->filterRadius[0] = d->filter_radius[0]; ds->filterRadius[1] = d->filter_radius[1];
         ds->filterAlpha = d->filter_alpha;
         ds->numMaterials = d->num_materials;
+        // every copy and kernel above has completed (the synchronize above): from here on
+        // the arrays are released in the order of the context's stream, like the work
+        // that reads them
+        for (PoolBuf& b : ds->bufs) b.stream = c->stream;
+        std::lock_guard<FairMutex> lk(c->mu);
         uint64_t id = c->nextScene++;
         c->scenes[id] = std::move(ds);
         *out = id;
@@ -481,7 +492,7 @@ gnd_status gnd_gpu_set_build_leaf_max(gnd_gpu_ctx* ctxh, int32_t leafMax) {
     return guarded([&]() {
         Context* c = ctxOf(ctxh);
         if (leafMax < 1 || leafMax > kLeafMax) throw Error(GND_ERR_INVALID, "leaf size out of range (1..16)");
-        std::lock_guard<FairMutex> lk(c->mu);
+        std::lock_guard<std::mutex> ul(c->uploadMu);   // the uploads read it
         c->buildLeafMax = leafMax;
     });
 }

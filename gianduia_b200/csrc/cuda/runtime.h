@@ -201,9 +201,14 @@ class Server;
 struct Context {
     int device = 0;
     int numSMs = 148;
-    int buildLeafMax = 4;     // largest leaf of device-built mesh trees
+    int buildLeafMax = 4;     // largest leaf of device-built mesh trees (guarded by uploadMu)
     cudaStream_t stream = nullptr;
     FairMutex mu;   // serialises every use of the context (stream, scenes, engine)
+    // Scene uploads copy, build and validate on their own stream without holding mu, so
+    // that they overlap renders; mu is taken only to publish the finished scene, and
+    // uploadMu serialises the uploads among themselves.
+    cudaStream_t uploadStream = nullptr;
+    std::mutex uploadMu;
     std::map<uint64_t, std::unique_ptr<DeviceScene>> scenes;
     uint64_t nextScene = 1;
     DevBuf errWord;           // device error bitmask written by kernels

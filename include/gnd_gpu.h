@@ -162,7 +162,11 @@ gnd_status gnd_gpu_destroy(gnd_gpu_ctx* ctx);
  * of bvhBuilder.cpp:59-262): a linear BVH over 3D Morton codes of the triangle
  * centroids, leaves chosen by the surface area heuristic, collapsed to the same 4-wide
  * nodes. Closest hits equal those through a host-built tree except between triangles at
- * exactly the same distance. */
+ * exactly the same distance.
+ * An upload copies, builds and validates on a stream of its own and may run on another
+ * host thread while a render or the serving thread uses the context: the transfer
+ * overlaps the render, and only publishing the finished scene waits for the context.
+ * Uploads on one context run one at a time. */
 gnd_status gnd_gpu_scene_upload(gnd_gpu_ctx* ctx, const gnd_scene_desc* desc, gnd_scene_id* out);
 gnd_status gnd_gpu_scene_free(gnd_gpu_ctx* ctx, gnd_scene_id scene);
 /* Largest leaf (1..16 triangles, default 4) of the mesh trees that later uploads build on
