@@ -56,19 +56,49 @@ __device__ __forceinline__ uint32_t warpAppend(uint32_t* counter, bool pred) {
     return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
 }
 
-// Two appends with one atomic: lanes with `a` take consecutive entries of the counter in
-// the low half of `pair`, lanes with `b` of the one in the high half. Every lane of the
-// warp calls it.
-__device__ __forceinline__ void warpAppend2(unsigned long long* pair, bool a, bool b, uint32_t& ia, uint32_t& ib) {
+// Block-aggregated queue operations for the short kernels whose appends and work grabs
+// all reach the same counters at once (kRetire, kClassify): one atomic per counter per
+// block of kAggBlock threads instead of one per warp. Every thread of the block calls
+// them (block-uniform control flow); each starts with a barrier, so the shared scratch
+// of the previous call is free.
+constexpr int kAggBlock = 512;
+constexpr int kAggWarps = kAggBlock / 32;
+
+// Warp counts of `pred` -> this thread's offset among the block's predicated threads
+// (warps in order, lanes in order) and the block total.
+__device__ __forceinline__ uint32_t blockRank(uint32_t mask, uint32_t* sCnt, uint32_t& total) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sCnt[warp] = (uint32_t)__popc(mask);
+    __syncthreads();
+    uint32_t off = 0, tot = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < (uint32_t)kAggWarps; ++w) {
+        const uint32_t c = sCnt[w];
+        off += w < warp ? c : 0u;
+        tot += c;
+    }
+    total = tot;
+    return off + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+
+// Two appends with one atomic: threads with `a` take consecutive entries of the counter
+// in the low half of `pair`, threads with `b` of the one in the high half.
+struct AggScratch {
+    uint32_t a[kAggWarps], b[kAggWarps];
+    unsigned long long base;
+};
+__device__ __forceinline__ void blockAppend2(unsigned long long* pair, bool a, bool b, uint32_t& ia, uint32_t& ib,
+                                             AggScratch& sc) {
     const uint32_t ma = __ballot_sync(0xffffffffu, a), mb = __ballot_sync(0xffffffffu, b);
-    const uint32_t lane = threadIdx.x & 31u;
-    unsigned long long base = 0;
-    if ((ma | mb) && lane == 0)
-        base = atomicAdd(pair, (unsigned long long)__popc(ma) | ((unsigned long long)__popc(mb) << 32));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    const uint32_t lt = (1u << lane) - 1u;
-    ia = (uint32_t)base + (uint32_t)__popc(ma & lt);
-    ib = (uint32_t)(base >> 32) + (uint32_t)__popc(mb & lt);
+    uint32_t ta, tb;
+    const uint32_t ra = blockRank(ma, sc.a, ta);
+    const uint32_t rb = blockRank(mb, sc.b, tb);
+    if (threadIdx.x == 0) sc.base = (ta | tb) ? atomicAdd(pair, (unsigned long long)ta | ((unsigned long long)tb << 32)) : 0ull;
+    __syncthreads();
+    const unsigned long long base = sc.base;
+    ia = (uint32_t)base + ra;
+    ib = (uint32_t)(base >> 32) + rb;
 }
 
 struct KParams {
@@ -897,26 +927,36 @@ __global__ void __launch_bounds__(kBlock) kRayScatter(KParams p) {
 }
 
 
-// Active list -> per-class lists (warp-aggregated appends, one atomic per class per warp).
-__global__ void __launch_bounds__(kBlock) kClassify(KParams p, uint32_t* classLists) {
+// Active list -> per-class lists: per block, the warps' groups of one class take
+// consecutive places (shared-memory counts), then one atomic per class per block.
+__global__ void __launch_bounds__(kAggBlock, 4) kClassify(KParams p, uint32_t* classLists) {
+    __shared__ uint32_t sCount[kShadeClasses], sBase[kShadeClasses];
     const uint32_t n = p.cnt[kQIn];
     const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t base = blockIdx.x * kBlock + (threadIdx.x & ~31u); base < n; base += gridDim.x * kBlock) {
-        const uint32_t i = base + lane;
+    for (uint32_t bb = blockIdx.x * kAggBlock; bb < n; bb += gridDim.x * kAggBlock) {   // block-uniform
+        const uint32_t i = bb + threadIdx.x;
         const bool valid = i < n;
         uint32_t cls = 0xFFFFFFFFu, slot = 0;
         if (valid) {
             slot = p.listIn[i];
             cls = p.hits[slot].pad[0];   // written by the extend store (shadeClass)
         }
+        __syncthreads();   // the previous iteration's reads of sBase are over
+        if (threadIdx.x < (unsigned)kShadeClasses) sCount[threadIdx.x] = 0;
+        __syncthreads();
         const uint32_t grp = __match_any_sync(0xffffffffu, cls);
-        if (valid) {
-            const int leader = __ffs(grp) - 1;
-            uint32_t b = 0;
-            if ((int)lane == leader) b = atomicAdd(&p.cnt[kQClass0 + cls], (uint32_t)__popc(grp));
-            b = __shfl_sync(grp, b, leader);
-            classLists[(size_t)cls * p.capacity + b + (uint32_t)__popc(grp & ((1u << lane) - 1u))] = slot;
+        const int leader = __ffs(grp) - 1;
+        uint32_t off = 0;
+        if (valid && (int)lane == leader) off = atomicAdd(&sCount[cls], (uint32_t)__popc(grp));
+        off = __shfl_sync(0xffffffffu, off, leader);
+        __syncthreads();
+        if (threadIdx.x < (unsigned)kShadeClasses) {
+            const uint32_t c = sCount[threadIdx.x];
+            sBase[threadIdx.x] = c ? atomicAdd(&p.cnt[kQClass0 + threadIdx.x], c) : 0u;
         }
+        __syncthreads();
+        if (valid)
+            classLists[(size_t)cls * p.capacity + sBase[cls] + off + (uint32_t)__popc(grp & ((1u << lane) - 1u))] = slot;
     }
 }
 
@@ -1456,58 +1496,87 @@ __global__ void kFilmFromSamples(JobDev j, uint32_t passes) {
 }
 
 // ---------------------------------------------------------------- retire / refill
-// Lanes in `want` take work items from the active jobs: the warp leader walks the active
-// list from a per-warp round-robin start and takes one contiguous range per job until the
-// warp is served (at most four jobs per grab); lanes left over stay idle this iteration.
-__device__ __forceinline__ bool warpGrab(const KParams& p, bool want, uint32_t& jobOut, uint64_t& itemOut) {
-    const uint32_t full = 0xffffffffu;
-    uint32_t mask = __ballot_sync(full, want);
-    if (!mask) return false;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(mask) - 1;
-    uint32_t sj0 = 0, sj1 = 0, sj2 = 0, sj3 = 0, sc0 = 0, sc1 = 0, sc2 = 0, sc3 = 0;
-    unsigned long long sb0 = 0, sb1 = 0, sb2 = 0, sb3 = 0;
-    if (lane == leader) {
-        const uint32_t na = p.cnt[kQActive];
-        uint32_t remaining = (uint32_t)__popc(mask);
-        const uint32_t start = p.fifo ? 0u : blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5) + p.cnt[kQIter];
+// Threads in `want` take work items from the active jobs: one thread per block walks the
+// active list from a per-block round-robin start (the first job with FIFO admission) and
+// takes one contiguous range per job until the block is served (at most four jobs per
+// grab); threads left over stay idle this iteration. One atomic per job per block.
+struct GrabScratch {
+    uint32_t cnt[kAggWarps];
+    uint32_t job[4], n[4];
+    unsigned long long first[4];
+};
+__device__ __forceinline__ bool blockGrab(const KParams& p, bool want, uint32_t& jobOut, uint64_t& itemOut, GrabScratch& g) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, want);
+    uint32_t total;
+    uint32_t r = blockRank(mask, g.cnt, total);
+    if (threadIdx.x == 0) {
+        uint32_t remaining = total;
         int ns = 0;
-        for (uint32_t t = 0; t < na && remaining > 0 && ns < 4; ++t) {
-            uint32_t jid = p.active[(start + t) % na];
-            unsigned long long end = p.jobs[jid].workEnd;
-            if (*(volatile unsigned long long*)&p.ctl[jid].next >= end) continue;
-            unsigned long long got = atomicAdd(&p.ctl[jid].next, (unsigned long long)remaining);
-            if (got >= end) continue;
-            uint32_t avail = (uint32_t)min((unsigned long long)remaining, end - got);
-            if (ns == 0) { sj0 = jid; sb0 = got; sc0 = avail; }
-            else if (ns == 1) { sj1 = jid; sb1 = got; sc1 = avail; }
-            else if (ns == 2) { sj2 = jid; sb2 = got; sc2 = avail; }
-            else { sj3 = jid; sb3 = got; sc3 = avail; }
-            ++ns;
-            remaining -= avail;
+        if (remaining > 0) {
+            const uint32_t na = p.cnt[kQActive];
+            const uint32_t start = p.fifo ? 0u : blockIdx.x + p.cnt[kQIter];
+            for (uint32_t t = 0; t < na && remaining > 0 && ns < 4; ++t) {
+                const uint32_t jid = p.active[(start + t) % na];
+                const unsigned long long end = p.jobs[jid].workEnd;
+                if (*(volatile unsigned long long*)&p.ctl[jid].next >= end) continue;
+                const unsigned long long got = atomicAdd(&p.ctl[jid].next, (unsigned long long)remaining);
+                if (got >= end) continue;
+                const uint32_t avail = (uint32_t)min((unsigned long long)remaining, end - got);
+                g.job[ns] = jid; g.first[ns] = got; g.n[ns] = avail;
+                ++ns;
+                remaining -= avail;
+            }
         }
+        for (int k = ns; k < 4; ++k) g.n[k] = 0;
     }
-    sj0 = __shfl_sync(full, sj0, leader); sc0 = __shfl_sync(full, sc0, leader); sb0 = __shfl_sync(full, sb0, leader);
-    sj1 = __shfl_sync(full, sj1, leader); sc1 = __shfl_sync(full, sc1, leader); sb1 = __shfl_sync(full, sb1, leader);
-    sj2 = __shfl_sync(full, sj2, leader); sc2 = __shfl_sync(full, sc2, leader); sb2 = __shfl_sync(full, sb2, leader);
-    sj3 = __shfl_sync(full, sj3, leader); sc3 = __shfl_sync(full, sc3, leader); sb3 = __shfl_sync(full, sb3, leader);
+    __syncthreads();
     if (!want) return false;
-    uint32_t r = (uint32_t)__popc(mask & ((1u << lane) - 1u));
-    if (r < sc0) { jobOut = sj0; itemOut = sb0 + r; return true; }
-    r -= sc0;
-    if (r < sc1) { jobOut = sj1; itemOut = sb1 + r; return true; }
-    r -= sc1;
-    if (r < sc2) { jobOut = sj2; itemOut = sb2 + r; return true; }
-    r -= sc2;
-    if (r < sc3) { jobOut = sj3; itemOut = sb3 + r; return true; }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (r < g.n[k]) { jobOut = g.job[k]; itemOut = g.first[k] + r; return true; }
+        r -= g.n[k];
+    }
     return false;
+}
+
+// Per-job retired counts of one block iteration: the warps' groups add into a small
+// shared table (one entry per job met), flushed with one atomic per job; a job that finds
+// the table full adds directly.
+constexpr int kRetireJobSlots = 8;
+struct RetireScratch {
+    uint32_t job[kRetireJobSlots];
+    uint32_t n[kRetireJobSlots];
+};
+__device__ __forceinline__ void blockRetired(const KParams& p, uint32_t jobIdx, RetireScratch& rs) {
+    const uint32_t lane = threadIdx.x & 31u;
+    __syncthreads();   // the previous flush is over
+    if (threadIdx.x < (unsigned)kRetireJobSlots) { rs.job[threadIdx.x] = 0xFFFFFFFFu; rs.n[threadIdx.x] = 0; }
+    __syncthreads();
+    const uint32_t grp = __match_any_sync(0xffffffffu, jobIdx);
+    if (jobIdx != 0xFFFFFFFFu && (int)lane == __ffs(grp) - 1) {
+        bool placed = false;
+        for (int k = 0; k < kRetireJobSlots && !placed; ++k) {
+            const uint32_t old = atomicCAS(&rs.job[k], 0xFFFFFFFFu, jobIdx);
+            if (old == 0xFFFFFFFFu || old == jobIdx) {
+                atomicAdd(&rs.n[k], (uint32_t)__popc(grp));
+                placed = true;
+            }
+        }
+        if (!placed) atomicAdd(&p.ctl[jobIdx].retired, (unsigned long long)__popc(grp));
+    }
+    __syncthreads();
+    if (threadIdx.x < (unsigned)kRetireJobSlots && rs.job[threadIdx.x] != 0xFFFFFFFFu)
+        atomicAdd(&p.ctl[rs.job[threadIdx.x]].retired, (unsigned long long)rs.n[threadIdx.x]);
 }
 
 // Finished paths (done list): film splat and per-job retired count. Finished and idle
 // slots (free list) then take new work items; slots left without work join the next
-// free list. The loop is warp-uniform (all lanes of a warp iterate together).
+// free list. The loop is block-uniform (all threads of a block iterate together).
 template <bool EXT>
-__global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
+__global__ void __launch_bounds__(kAggBlock, 3) kRetire(KParams p) {
+    __shared__ GrabScratch sGrab;
+    __shared__ AggScratch sApp;
+    __shared__ RetireScratch sRet;
     const uint32_t nd = p.cnt[kQDone], nf = p.cnt[kQFree];
     const bool work = p.cnt[kQWork] != 0;
     // with work left, finished and idle slots take work items; without, only finished
@@ -1515,10 +1584,9 @@ __global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
     const uint32_t total = work ? nd + nf : nd;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[2], (unsigned long long)nd);
     if (!work)
-        for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < nf; i += gridDim.x * kBlock) p.freeOut[i] = p.freeIn[i];
-    const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t base = blockIdx.x * kBlock + (threadIdx.x & ~31u); base < total; base += gridDim.x * kBlock) {
-        const uint32_t i = base + lane;
+        for (uint32_t i = blockIdx.x * kAggBlock + threadIdx.x; i < nf; i += gridDim.x * kAggBlock) p.freeOut[i] = p.freeIn[i];
+    for (uint32_t bb = blockIdx.x * kAggBlock; bb < total; bb += gridDim.x * kAggBlock) {
+        const uint32_t i = bb + threadIdx.x;
         const bool valid = i < total;
         const bool isDone = i < nd;
         const uint32_t slot = valid ? (isDone ? p.done[i] : p.freeIn[i - nd]) : 0u;
@@ -1530,13 +1598,11 @@ __global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
             if (jd.samples) sampleRecord<EXT>(jd, ps);
             else filmSplat<EXT>(jd, ps);
         }
-        const uint32_t grp = __match_any_sync(0xffffffffu, jobIdx);
-        if (jobIdx != 0xFFFFFFFFu && (int)lane == __ffs(grp) - 1)
-            atomicAdd(&p.ctl[jobIdx].retired, (unsigned long long)__popc(grp));
+        if (bb < nd) blockRetired(p, jobIdx, sRet);   // block-uniform: done slots come first
         uint32_t gj = 0;
         uint64_t item = 0;
         bool got = false;
-        if (work) got = warpGrab(p, valid, gj, item);   // `work` is uniform over the grid
+        if (work) got = blockGrab(p, valid, gj, item, sGrab);   // `work` is uniform over the grid
         if (got) {
             PathState ps;
             const float t = generatePath<EXT>(p.jobs[gj], gj, item, ps);
@@ -1545,7 +1611,7 @@ __global__ void __launch_bounds__(kBlock) kRetire(KParams p) {
         }
         const bool idle = valid && !got;
         uint32_t k, f;
-        warpAppend2(reinterpret_cast<unsigned long long*>(p.cnt + kQOut), got, idle, k, f);
+        blockAppend2(reinterpret_cast<unsigned long long*>(p.cnt + kQOut), got, idle, k, f, sApp);
         if (got) p.listOut[k] = slot;
         if (idle) p.freeOut[f] = slot;
     }
@@ -2001,7 +2067,7 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
     else launchTraversal<32>(kp, mix, hasNull, count, travGrid, st, ea, eb, 0, tune_.specExtend != 0, motion_, bps);
     if (sort) {
         uint32_t* cls = classes_.as<uint32_t>();
-        kClassify<<<ctx_->numSMs * 16, kBlock, 0, st>>>(kp, cls);   // latency-bound: a full SM of warps
+        kClassify<<<ctx_->numSMs * 4, kAggBlock, 0, st>>>(kp, cls);   // latency-bound: a full SM of warps
         if (mix & 1) {
             if (ext_) launchShade<false, true>(kp, cls, grid, st);
             else launchShade<false, false>(kp, cls, grid, st);
@@ -2033,8 +2099,8 @@ void Wavefront::enqueueIteration(KParams kp, int par, int mix, bool hasNull, int
         else kShadow<true><<<grid, kBlock, 0, st>>>(kp, mix == 3);
     }
     // 12 blocks per SM: its register limit
-    if (ext_) kRetire<true><<<ctx_->numSMs * 12, kBlock, 0, st>>>(kp);
-    else kRetire<false><<<ctx_->numSMs * 12, kBlock, 0, st>>>(kp);
+    if (ext_) kRetire<true><<<ctx_->numSMs * 3, kAggBlock, 0, st>>>(kp);
+    else kRetire<false><<<ctx_->numSMs * 3, kAggBlock, 0, st>>>(kp);
     kEndIter<<<1, 1, 0, st>>>(kp.cnt);
     GND_CUDA(cudaGetLastError());
 }

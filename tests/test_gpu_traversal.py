@@ -136,6 +136,47 @@ def test_analytic_shapes_parity(ctx, tmp_path):
     run_pair(ctx, G.HostScene.load_xml(xml), osc, rays, "analytic")
 
 
+def test_translated_instances_parity(ctx, tmp_path):
+    """Mesh, sphere and cube instances under pure translations (one with a zero
+    component) beside rotated and scaled ones, traced with rays whose origins lie on an
+    integer grid (many zero components, so the transformed origins carry signed zeros) and
+    rays along the axes (infinite inverse directions): the oracle's hits."""
+    scenes.write_cube_obj(str(tmp_path / "cube.obj"))
+    scenes.write_plane_obj(str(tmp_path / "plane.obj"))
+
+    def prim(shape, xf):
+        return "<primitive><transform name=\"toWorld\">%s</transform>%s</primitive>" % (xf, shape)
+
+    mesh = "<shape type=\"mesh\"><string name=\"filename\" value=\"%s\"/></shape>"
+    parts = [prim(mesh % "cube.obj", '<translate x="1.25" y="-0.75" z="0.5"/>'),
+             prim(mesh % "cube.obj", '<translate x="-1.5" y="0" z="-0.25"/>'),
+             prim(mesh % "cube.obj", '<translate x="-0.375" y="-0.625" z="-1.75"/>'),
+             prim(mesh % "plane.obj", '<rotate axis="1 0 0" angle="90"/><translate x="0.125" y="-1.5" z="0.375"/>'),
+             prim(mesh % "cube.obj", '<rotate axis="0 1 1" angle="35"/><scale value="0.35"/><translate x="0.2" y="1.1" z="-1.3"/>'),
+             prim('<shape type="sphere"><float name="radius" value="0.45"/></shape>', '<translate x="-0.6" y="0.7" z="1.2"/>'),
+             prim('<shape type="cube"><vector name="extents" value="0.3, 0.2, 0.4"/></shape>'
+                  '<emitter type="area"><color name="radiance" value="1 1 1"/></emitter>', '<translate x="0.9" y="0.8" z="-0.3"/>')]
+    (tmp_path / "t.xml").write_text(
+        '<scene><camera type="perspective"><transform name="toWorld"><lookat origin="0.3,0.2,5" target="0,0,0" up="0,1,0"/>'
+        '</transform></camera><sampler type="independent"/><integrator type="path_gpu"/>' + "".join(parts) + '</scene>')
+    xml = str(tmp_path / "t.xml")
+    osc = O.Scene.load(xml)
+    rays = _scene_rays(osc, 32, 32, 150000, 14, -2.5, 2.5)
+    rng = np.random.default_rng(15)
+    n = rays.shape[0]
+    # origins on a coarse grid: many components exactly zero
+    grid = rng.random(n) < 0.25
+    rays[grid, :3] = rng.integers(-2, 3, (int(grid.sum()), 3)).astype(np.float32)
+    # some axis-aligned directions (zero components: infinite inverse direction)
+    axis = rng.random(n) < 0.05
+    k = rng.integers(0, 3, int(axis.sum()))
+    d = np.zeros((int(axis.sum()), 3), np.float32)
+    d[np.arange(len(k)), k] = rng.choice([-1.0, 1.0], len(k))
+    rays[axis, 4:7] = d
+    st = run_pair(ctx, G.HostScene.load_xml(xml), osc, rays, "translated")
+    assert st["hits"] > 20000
+
+
 def test_full_size_traversal_parity(ctx):
     """The traversal micro-benchmark's full scene (2^20 triangles); a 2^21-ray sample of
     its 2^24 rays is compared with the oracle, and any-hit is checked against closest-hit
