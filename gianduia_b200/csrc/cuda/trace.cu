@@ -41,7 +41,7 @@ struct BatchSrc {
         if (COUNT) { cnt->nodes = 0; cnt->tris = 0; }
         return true;
     }
-    __device__ void store(uint32_t k, const THit& h) {
+    __device__ void store(uint32_t k, const THit& h, const SceneView&) {
         const uint32_t i = perm ? __ldg(perm + k) : k;
         if (COUNT) {
             nodesOut[i] = cnt->nodes;

@@ -299,9 +299,8 @@ struct Trav {
     int sp;
     bool fast, wfast;   // current / world ray: nodeKeysFast applies (see there)
     uint32_t next;      // entry to visit next without a stack round trip, kEmpty when none
-    uint32_t leaf;      // pending leaf reference, kEmpty when none
-    uint32_t leafK;     // next primitive of the pending leaf
-    THit hit;
+    uint32_t leaf;      // pending primitives (a leaf reference advanced past those done), kEmpty when none
+    THit hit;           // t unused: a hit's distance is bestT (travHit)
 };
 
 // SMEM: entries kept in shared memory (the block's array holds SMEM * BLOCK words); the
@@ -336,7 +335,6 @@ __device__ __forceinline__ void travInit(Trav& t, const SceneView& s, const TRay
     t.bestT = 3.402823466e38f;
     t.curInst = -1;
     t.leaf = kEmpty;
-    t.leafK = 0;
     t.next = kEmpty;
     t.hit.t = INFINITY; t.hit.u = t.hit.v = 0.f; t.hit.inst = -1; t.hit.slot = 0xFFFFFFFFu;
     t.sp = 0;
@@ -433,7 +431,6 @@ __device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<
     }
     if (isLeaf(e)) {
         t.leaf = e;
-        t.leafK = 0;
         return 0;
     }
     const Node4* nd = s.nodes + e;
@@ -483,24 +480,24 @@ __device__ __forceinline__ int travNodeStep(Trav& t, const SceneView& s, TStack<
 template <int BLOCK, bool ANY, bool COUNT, int SMEM, bool MOTION>
 __device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<BLOCK, SMEM>& st, TraceCounters* cnt,
                                             const uint8_t* nullMask) {
-    uint32_t first = leafFirst(t.leaf), count = leafCount(t.leaf);
-    uint32_t k = t.leafK++;
-    if (t.leafK >= count) t.leaf = kEmpty;
+    // the pending leaf's first primitive; the rest stays pending
+    const uint32_t first = leafFirst(t.leaf), count = leafCount(t.leaf);
+    t.leaf = count > 1u ? makeLeaf(first + 1u, count - 1u) : kEmpty;
     if (t.curInst >= 0) {
         float tt, u, v;
         uint32_t prim;
         if (COUNT) cnt->tris++;
-        if (triTest(s.tris + first + k, t.o, t.d, t.tmin, t.tmax, tt, u, v, prim)) {
+        if (triTest(s.tris + first, t.o, t.d, t.tmin, t.tmax, tt, u, v, prim)) {
             t.tmax = tt;
             t.bestT = tt;
-            t.hit.t = tt; t.hit.u = u; t.hit.v = v;
+            t.hit.u = u; t.hit.v = v;
             t.hit.inst = t.curInst;
-            t.hit.slot = first + k;
+            t.hit.slot = first;
             if (ANY) { t.sp = 0; t.leaf = kEmpty; t.next = kEmpty; }
         }
         return 0;
     }
-    uint32_t id = __ldg(s.tlasList + first + k);
+    uint32_t id = __ldg(s.tlasList + first);
     if (nullMask && nullMask[id]) return 0;
     const InstTrav* it = s.instT + id;
     float4 r0 = ldg4(&it->w2o.r[0][0]), r1 = ldg4(&it->w2o.r[1][0]), r2 = ldg4(&it->w2o.r[2][0]);
@@ -527,7 +524,7 @@ __device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<
         if (t.leaf != kEmpty) {
             // the rest of this leaf comes back after the bottom-level tree
             if (t.sp >= kPStackMax) return kTraceStackOverflow;
-            st.put(t.sp++, makeLeaf(first + k + 1, count - k - 1));
+            st.put(t.sp++, t.leaf);
             t.leaf = kEmpty;
         }
         if (t.sp + 1 > kPStackMax) return kTraceStackOverflow;
@@ -547,12 +544,19 @@ __device__ __forceinline__ int travLeafStep(Trav& t, const SceneView& s, TStack<
     if (h && th < t.bestT) {
         t.tmax = th;
         t.bestT = th;
-        t.hit.t = th; t.hit.u = 0.f; t.hit.v = 0.f;
+        t.hit.u = 0.f; t.hit.v = 0.f;
         t.hit.inst = (int)id;
         t.hit.slot = 0xFFFFFFFFu;
         if (ANY) { t.sp = 0; t.leaf = kEmpty; t.next = kEmpty; }
     }
     return 0;
+}
+
+// The hit a finished query reports: every accepted hit sets bestT to its distance.
+__device__ __forceinline__ THit travHit(const Trav& t) {
+    THit h = t.hit;
+    h.t = t.hit.inst >= 0 ? t.bestT : INFINITY;
+    return h;
 }
 
 // Warp-aggregated fetch of the next work index for lanes in `want`.
@@ -572,7 +576,7 @@ __device__ __forceinline__ uint32_t warpFetch(uint32_t* counter, bool want) {
 // is a multiple of 32 and no lane exits early). Src provides:
 //   uint32_t count()                      number of rays
 //   bool load(uint32_t i, TRay&, const SceneView*&, const uint8_t*& nullMask)
-//   void store(uint32_t i, const THit&)   (closest) / store(i, bool) (any)
+//   void store(uint32_t i, const THit&, const SceneView&)   (the query's scene)
 // SLOT_ORDER_ANY: any-hit queries visit hit children in slot order instead of nearest
 // first (faster for the bounded shadow segments of the path tracer; rays to infinity find
 // an occluder sooner nearest first).
@@ -649,7 +653,7 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
             }
         }
         if (active && t.sp == 0 && t.leaf == kEmpty && t.next == kEmpty) {
-            src.store(idx, t.hit);
+            src.store(idx, travHit(t), *sv);
             active = false;
         }
     }

@@ -796,7 +796,6 @@ __global__ void kBeginIter(KParams p) {
     cnt[kQFreeOut] = work ? 0u : cnt[kQFree];
 }
 
-// Closest-hit source/sink over the active list (extend).
 // Shade class of a path after its extend query (see kMatClasses): volpath paths inside a
 // medium go to the medium class, others to their surface's class.
 static_assert(kMatIndex == kMatClasses - 1, "the null-BSDF material type is the last surface class");
@@ -816,7 +815,6 @@ struct ExtendSrc {
     uint32_t slot;
     int32_t medium;
     bool vol;
-    const SceneView* view;
     __device__ uint32_t count() const { return n; }
     __device__ bool load(uint32_t i, TRay& r, const SceneView*& sv, const uint8_t*& nm) {
         slot = p->extList[i];
@@ -824,8 +822,7 @@ struct ExtendSrc {
         float4 a = *reinterpret_cast<const float4*>(&ps->ox);
         float4 b = *reinterpret_cast<const float4*>(&ps->dx);
         uint4 c = *reinterpret_cast<const uint4*>(&ps->bounces);   // bounces, vsBounces, medium, flags
-        const uint32_t job = c.w >> 8;
-        const JobDev& jd = p->jobs[job];
+        const JobDev& jd = p->jobs[c.w >> 8];
         medium = (int32_t)c.z;
         vol = jd.integrator == 1;
         r.o = v3(a.x, a.y, a.z);
@@ -833,15 +830,14 @@ struct ExtendSrc {
         r.tmin = kEpsilon;
         r.tmax = INFINITY;
         r.time = p->slotTime[slot];
-        view = &jd.view;
-        sv = view;
+        sv = &jd.view;
         nm = nullptr;
         return true;
     }
-    __device__ void store(uint32_t, const THit& h) {
+    __device__ void store(uint32_t, const THit& h, const SceneView& sv) {
         HitRec hr;
         hr.t = h.t; hr.u = h.u; hr.v = h.v; hr.inst = h.inst; hr.slot = h.slot;
-        hr.pad[0] = shadeClass(*view, vol, medium, h.inst);
+        hr.pad[0] = shadeClass(sv, vol, medium, h.inst);
         hr.pad[1] = hr.pad[2] = 0;
         p->hits[slot] = hr;
     }
@@ -1203,17 +1199,15 @@ template <bool ANY>
 struct ShadowSrc {
     const KParams* p;
     uint32_t n;
-    uint32_t slot;
-    const uint8_t* nm;
     bool mixed;
-    uint32_t rec;   // the shadow record of the query in flight
+    uint32_t rec;   // the shadow record of the query in flight (its path slot and job are read again at the store)
     __device__ uint32_t count() const { return n; }
     __device__ bool load(uint32_t i, TRay& r, const SceneView*& sv, const uint8_t*& nmOut) {
         rec = p->shadowOrder ? p->shadowOrder[i] : i;
         const ShadowRec* sr = p->shadow + rec;
         float4 a = *reinterpret_cast<const float4*>(&sr->ox);
         float4 b = *reinterpret_cast<const float4*>(&sr->dx);
-        slot = __float_as_uint(b.w);
+        const uint32_t slot = __float_as_uint(b.w);
         r.o = v3(a.x, a.y, a.z);
         r.tmax = a.w;
         r.d = v3(b.x, b.y, b.z);
@@ -1222,16 +1216,16 @@ struct ShadowSrc {
         const JobDev& j = p->jobs[p->paths[slot].flags >> 8];
         if (mixed && j.integrator != 0) return false;
         sv = &j.view;
-        nm = j.nullMask;
         nmOut = nullptr;
         return true;
     }
-    __device__ void store(uint32_t i, const THit& h) {
-        bool clear = h.inst < 0 || (!ANY && nm[h.inst]);
+    __device__ void store(uint32_t i, const THit& h, const SceneView&) {
+        const ShadowRec* sr = p->shadow + rec;
+        const uint32_t slot = sr->slot;
+        PathState* ps = p->paths + slot;
+        bool clear = h.inst < 0 || (!ANY && p->jobs[ps->flags >> 8].nullMask[h.inst]);
         if (clear) {
-            const ShadowRec* sr = p->shadow + rec;
             float4 c = *reinterpret_cast<const float4*>(&sr->cr);
-            PathState* ps = p->paths + slot;
             ps->Lr = ps->Lr + c.x;
             ps->Lg = ps->Lg + c.y;
             ps->Lb = ps->Lb + c.z;
@@ -1244,7 +1238,7 @@ __global__ void __launch_bounds__(kBlock, MINB) kShadowPath(KParams p, bool mixe
     __shared__ uint32_t stack[SMEM * kBlock];
     const uint32_t n = p.cnt[kQShadow];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[1], (unsigned long long)n);
-    ShadowSrc<ANY> src{&p, n, 0, nullptr, mixed};
+    ShadowSrc<ANY> src{&p, n, mixed, 0};
     int err = persistentTrace<kBlock, ANY, false, SMEM, SPEC, MOTION, true>(src, p.cnt + kQFetchB, stack, nullptr,
                                                                             p.shadowLeafBatch);
     if (err) atomicOr(p.errWord, (uint32_t)err);
