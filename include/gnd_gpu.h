@@ -13,7 +13,8 @@
  *
  * Every function returns a gnd_status (0 = success). On failure the message is
  * available from gnd_last_error() (thread-local). No C++ exception crosses the ABI.
- * Calls on one context are serialised internally; contexts are independent.
+ * Calls on one context are serialised internally, except that a scene upload's copies
+ * overlap the other calls (gnd_gpu_scene_upload); contexts are independent.
  */
 #ifndef GND_GPU_H
 #define GND_GPU_H
@@ -427,8 +428,10 @@ gnd_status gnd_gpu_set_tune(gnd_gpu_ctx* ctx, gnd_scene_id scene, const gnd_tune
 /* Chooses the settings for a scene by measurement: coordinate descent from the current
  * settings over every field, each candidate timed on the device with a batched render of
  * `spp` passes (<= 0: 8) at the scene's film size, depth and integrator, until about
- * budget_ms of wall time is spent. Keeps a change only when it is at least 2% faster.
- * Stores the result as the scene's settings; returns it and its Mpaths/s. */
+ * budget_ms of wall time is spent. Keeps a change when it is at least 2% faster, or
+ * when a candidate between 0.3% and 2% faster stays at least 0.5% faster over three
+ * renders alternating with the current settings. Stores the result as the scene's
+ * settings; returns it and its Mpaths/s. */
 gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctx, gnd_scene_id scene, int32_t spp, int32_t budget_ms, gnd_tune* best,
                             double* mpaths_per_s);
 
