@@ -667,6 +667,15 @@ def main():
         other.append(st["ms"])
     other_value = npix * spp / (sum(other) / len(other) / 1000.0) / 1e6 if other else None
 
+    # lanes busy per warp step in the extend traversal's two phases, with the tuned settings
+    # (counting variant, 8 passes)
+    _, pst = ctx.render(sid, spp=8, first_pass=first, profile=2, batched=batched)
+    simt = {"node_phase": pst["extend_nodes"] / (32.0 * max(1, pst["extend_node_warp_steps"])),
+            "leaf_phase": pst["extend_leaf_steps"] / (32.0 * max(1, pst["extend_leaf_warp_steps"])),
+            "node_steps_per_leaf_step": pst["extend_node_warp_steps"] / max(1, pst["extend_leaf_warp_steps"]),
+            "note": "fraction of a warp's 32 lanes busy per step (node visits or leaf steps / 32 x warp steps), "
+                    "counting variant of kExtend, 8 passes with the tuned settings"}
+
     peaks, peak_kind = measured_peaks()
     bytes_per_ray = nodes_per_ray * 128 + tris_per_ray * 48 + 32 + 32
     ext_launches = iters
@@ -697,7 +706,8 @@ def main():
                      "frac": (achieved / peaks["hbm_gbs"]) if achieved else None, "traffic": traffic,
                      "kernel": "kExtend (closest-hit BVH4 traversal)",
                      "bytes_per_ray": bytes_per_ray, "nodes_per_ray": nodes_per_ray, "tris_per_ray": tris_per_ray,
-                     "launches": ext_launches, "ms_total": ext_ms, "peak_kind": peak_kind + " (copy bandwidth)",
+                     "launches": ext_launches, "ms_total": ext_ms, "lanes_busy": simt,
+                     "peak_kind": peak_kind + " (copy bandwidth)",
                      "timed_in": "a separate instrumented render of the same %d passes (CUDA events around each "
                                  "extend launch, graphs off); the headline steps run the CUDA-graph loop" % spp},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": int(scene_bytes),

@@ -562,12 +562,16 @@ class RenderStats(ctypes.Structure):
     _fields_ = [("paths", ctypes.c_int64), ("rays", ctypes.c_int64), ("passes_done", ctypes.c_int32),
                 ("pad", ctypes.c_int32), ("ms", ctypes.c_double), ("extend_rays", ctypes.c_int64),
                 ("shadow_rays", ctypes.c_int64), ("extend_nodes", ctypes.c_int64), ("extend_tris", ctypes.c_int64),
-                ("extend_ms", ctypes.c_double), ("iterations", ctypes.c_int64), ("launches", ctypes.c_int64)]
+                ("extend_ms", ctypes.c_double), ("iterations", ctypes.c_int64), ("launches", ctypes.c_int64),
+                ("extend_node_warp_steps", ctypes.c_int64), ("extend_leaf_steps", ctypes.c_int64),
+                ("extend_leaf_warp_steps", ctypes.c_int64)]
 
     def as_dict(self):
         return dict(paths=self.paths, rays=self.rays, passes=self.passes_done, ms=self.ms, extend_rays=self.extend_rays,
                     shadow_rays=self.shadow_rays, extend_nodes=self.extend_nodes, extend_tris=self.extend_tris,
-                    extend_ms=self.extend_ms, iterations=self.iterations, launches=self.launches)
+                    extend_ms=self.extend_ms, iterations=self.iterations, launches=self.launches,
+                    extend_node_warp_steps=self.extend_node_warp_steps, extend_leaf_steps=self.extend_leaf_steps,
+                    extend_leaf_warp_steps=self.extend_leaf_warp_steps)
 
 
 class Counters(ctypes.Structure):

@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
                 uint32_t* fetch, uint32_t* errWord, unsigned long long* totals, const uint32_t* __restrict__ perm,
                 uint32_t leafBatch) {
     __shared__ uint32_t stack[kSmemStack * kTraceBlock];
-    TraceCounters cnt{0, 0};
+    TraceCounters cnt{0, 0, 0, 0, 0};
     BatchSrc<ANY, COUNT> src{sv, rays, n, hits, occ, nodesOut, trisOut, &cnt, perm};
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&totals[kTraceTotalRays], (unsigned long long)n);

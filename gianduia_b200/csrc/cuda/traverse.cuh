@@ -41,8 +41,13 @@ __device__ __forceinline__ uint4 ldgu4(const void* p) { return __ldg(reinterpret
 __device__ __forceinline__ float lmin(float a, float b) { return a < b ? a : b; }
 __device__ __forceinline__ float lmax(float a, float b) { return a > b ? a : b; }
 
+// Work counters of the counting variants: node visits and triangle tests per lane, and
+// for the phases of the persistent loop (persistentTrace) the warp steps of each phase
+// (counted by lane 0) and the lanes' leaf steps, so that lanes busy per step = lane steps
+// / (32 x warp steps).
 struct TraceCounters {
     uint32_t nodes, tris;
+    uint32_t nodeWarpSteps, leafSteps, leafWarpSteps;
 };
 
 // Moller-Trumbore against the object-space ray (mesh.cpp:259-291). Returns true when the
@@ -635,6 +640,7 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
             if (!__any_sync(0xffffffffu, want)) break;
             if (leafBatch < 32u && (uint32_t)__popc(__ballot_sync(0xffffffffu, active && t.leaf != kEmpty)) >= leafBatch)
                 break;
+            if (COUNT && (threadIdx.x & 31) == 0) cnt->nodeWarpSteps++;
             if (want) {
                 int e = travNodeStep<BLOCK, COUNT, SMEM, !(ANY && SLOT_ORDER_ANY)>(t, *sv, st, cnt);
                 if (e || ++iter > kMaxIterations) {
@@ -647,6 +653,10 @@ __device__ __forceinline__ int persistentTrace(Src& src, uint32_t* fetchCounter,
         for (;;) {
             bool want = active && t.leaf != kEmpty;
             if (!__any_sync(0xffffffffu, want)) break;
+            if (COUNT) {
+                if ((threadIdx.x & 31) == 0) cnt->leafWarpSteps++;
+                if (want) cnt->leafSteps++;
+            }
             if (want) {
                 int e = travLeafStep<BLOCK, ANY, COUNT, SMEM, MOTION>(t, *sv, st, cnt, nm);
                 if (e) { err |= e; t.sp = 0; t.leaf = kEmpty; t.next = kEmpty; }

@@ -851,17 +851,23 @@ __global__ void __launch_bounds__(kBlock, MINB) kExtend(KParams p) {
     __shared__ uint32_t stack[SMEM * kBlock];
     const uint32_t n = p.cnt[kQIn];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.totals[0], (unsigned long long)n);
-    TraceCounters cnt{0, 0};
+    TraceCounters cnt{0, 0, 0, 0, 0};
     ExtendSrc src{&p, n, 0};
     int err = persistentTrace<kBlock, false, COUNT, SMEM, SPEC, MOTION>(src, p.cnt + kQFetchA, stack, &cnt, p.leafBatch);
     if (COUNT) {
-        unsigned long long nn = cnt.nodes, nt = cnt.tris;
+        unsigned long long nn = cnt.nodes, nt = cnt.tris, nw = cnt.nodeWarpSteps, ls = cnt.leafSteps, lw = cnt.leafWarpSteps;
         for (int o = 16; o > 0; o >>= 1) {
             nn += __shfl_down_sync(0xffffffffu, nn, o);
             nt += __shfl_down_sync(0xffffffffu, nt, o);
+            nw += __shfl_down_sync(0xffffffffu, nw, o);
+            ls += __shfl_down_sync(0xffffffffu, ls, o);
+            lw += __shfl_down_sync(0xffffffffu, lw, o);
         }
         if ((threadIdx.x & 31) == 0) {
             atomicAdd(&p.totals[3], nn);
+            atomicAdd(&p.totals[5], nw);
+            atomicAdd(&p.totals[6], ls);
+            atomicAdd(&p.totals[7], lw);
             atomicAdd(&p.totals[4], nt);
         }
     }
@@ -2328,6 +2334,9 @@ Wavefront::Result Wavefront::render(DeviceScene& ds, int W, int H, int spp, int 
     res.shadowRays = (int64_t)tot[1];
     res.extendNodes = (int64_t)tot[3];
     res.extendTris = (int64_t)tot[4];
+    res.extendNodeWarpSteps = (int64_t)tot[5];
+    res.extendLeafSteps = (int64_t)tot[6];
+    res.extendLeafWarpSteps = (int64_t)tot[7];
     res.ms = ms;
     res.launches = (int64_t)(launches_ - launches0);
     return res;
@@ -2372,6 +2381,9 @@ void renderCall(gnd_gpu_ctx* ctxh, gnd_scene_id id, const gnd_render_params* prm
     rs.shadow_rays = r.shadowRays;
     rs.extend_nodes = r.extendNodes;
     rs.extend_tris = r.extendTris;
+    rs.extend_node_warp_steps = r.extendNodeWarpSteps;
+    rs.extend_leaf_steps = r.extendLeafSteps;
+    rs.extend_leaf_warp_steps = r.extendLeafWarpSteps;
     rs.extend_ms = r.extendMs;
     rs.iterations = r.iterations;
     rs.launches = r.launches;

@@ -104,6 +104,7 @@ public:
     ~Wavefront();
     struct Result {
         int64_t paths = 0, rays = 0, extendRays = 0, shadowRays = 0, extendNodes = 0, extendTris = 0, iterations = 0;
+        int64_t extendNodeWarpSteps = 0, extendLeafSteps = 0, extendLeafWarpSteps = 0;
         int64_t launches = 0;         // kernels launched
         int passesDone = 0;
         double ms = 0.0, extendMs = 0.0;

@@ -327,6 +327,13 @@ typedef struct gnd_render_stats {
     double extend_ms;         /* profile bit0: summed device time of the extend launches */
     int64_t iterations;       /* wavefront iterations (bounce steps) */
     int64_t launches;         /* kernels the render launched */
+    /* profile bit1: the extend traversal's phases (a warp alternates inner-node steps and
+     * leaf steps): warp steps of the node phase, lane steps and warp steps of the leaf
+     * phase; lanes busy per step = extend_nodes / (32 x extend_node_warp_steps) and
+     * extend_leaf_steps / (32 x extend_leaf_warp_steps) */
+    int64_t extend_node_warp_steps;
+    int64_t extend_leaf_steps;
+    int64_t extend_leaf_warp_steps;
 } gnd_render_stats;
 
 /* Integrator::render (integrator.h:49-155) for path_gpu / volpath_gpu: renders the

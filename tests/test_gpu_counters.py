@@ -91,4 +91,10 @@ def test_counters_sum_render_stats(ctx, tmp_path):
     assert c["extend_nodes"] == a["extend_nodes"] > 0 and c["extend_tris"] == a["extend_tris"]
     assert c["last"]["paths"] == b["paths"] == 32 * 32 * 2
     assert c["render_ms"] == pytest.approx(a["ms"] + b["ms"])
+    # phase counters of the counted render: a warp step serves 1..32 lanes, and every
+    # triangle test is a leaf step (the others enter instances or test analytic shapes)
+    nw, ls, lw = a["extend_node_warp_steps"], a["extend_leaf_steps"], a["extend_leaf_warp_steps"]
+    assert 0 < nw <= a["extend_nodes"] <= 32 * nw
+    assert 0 < lw <= ls <= 32 * lw and ls >= a["extend_tris"]
+    assert b["extend_node_warp_steps"] == b["extend_leaf_steps"] == 0
     ctx.free_scene(sid)
