@@ -616,6 +616,11 @@ def main():
         if not steps:
             return None
         hscene.pin(True)
+        # untimed warm-up uploads of the freshly page-locked description (the renders are
+        # warm from the device-timed steps)
+        for _ in range(max(1, args.warmup)):
+            s, _ = timed_upload(hscene)
+            ctx.free_scene(s)
         pool = ThreadPoolExecutor(max_workers=1) if overlap else None
         barrier()
         t0 = time.perf_counter()
