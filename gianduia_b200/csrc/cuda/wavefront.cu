@@ -2524,7 +2524,7 @@ gnd_status gnd_gpu_autotune(gnd_gpu_ctx* ctxh, gnd_scene_id id, int32_t spp, int
         };
         const std::vector<Knob> knobs = {
             {&Tune::travBlocks, {8, 9, 10, 6, 4}}, {&Tune::smem, {32, 16}},          {&Tune::sort, {1, 0}},
-            {&Tune::poolLog2, {22, 21, 23, 20}}, {&Tune::roundIters, {8, 16, 4}}, {&Tune::graphs, {1, 0}},
+            {&Tune::poolLog2, {22, 21, 23, 24, 20}}, {&Tune::roundIters, {8, 16, 4}}, {&Tune::graphs, {1, 0}},
             {&Tune::sampleFilm, {1, 0}}, {&Tune::specExtend, {1, 0}}, {&Tune::specShadow, {1, 0}},
             {&Tune::raySort, {1, 3, 0}}, {&Tune::leafBatch, {16, 8, 24, 32}}, {&Tune::shadowLeafBatch, {16, 8, 24, 32}},
         };
