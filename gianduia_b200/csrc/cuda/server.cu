@@ -44,8 +44,13 @@ uint64_t Server::bytesInUseLocked() const {
     return b;
 }
 
+size_t Server::poolSlots() const {
+    return size_t(1) << std::min(std::max(c_->serveTune.poolLog2, 16), 26);
+}
+
 bool Server::fitsLocked(const ServeJob& j) const {
-    const uint64_t pool = c_->wave && c_->wave->capacity() >= kPoolSlots ? 0 : Wavefront::slotBytes() * kPoolSlots;
+    const size_t slots = poolSlots();
+    const uint64_t pool = c_->wave && c_->wave->capacity() >= slots ? 0 : Wavefront::slotBytes() * slots;
     const uint64_t staging = (uint64_t)j.W * j.H * 7 * sizeof(float);
     const uint64_t need = j.filmBytes + staging + pool;
     if (c_->hbmBudget) return bytesInUseLocked() + need <= c_->hbmBudget;
@@ -75,7 +80,7 @@ gnd_job_id Server::submit(const gnd_job_desc& d) {
         if (c_->hbmBudget) {
             uint64_t scenes = 0;
             for (const auto& kv : c_->scenes) scenes += kv.second->bytes;
-            const uint64_t alone = scenes + Wavefront::slotBytes() * kPoolSlots + j->filmBytes + (uint64_t)j->W * j->H * 28;
+            const uint64_t alone = scenes + Wavefront::slotBytes() * poolSlots() + j->filmBytes + (uint64_t)j->W * j->H * 28;
             if (alone > c_->hbmBudget)
                 throw Error(GND_ERR_BUDGET, "job needs " + std::to_string(alone) + " bytes of HBM with its scenes and the path pool; budget " +
                                                 std::to_string(c_->hbmBudget));
@@ -219,7 +224,7 @@ void Server::loop() {
                     admit.push_back(j);
                 }
             }
-            if (!admit.empty() && !wf.busy()) wf.reset(kPoolSlots);
+            if (!admit.empty() && !wf.busy()) wf.reset(poolSlots());
             wf.setFifo(true);
             wf.setTune(c_->serveTune);
             for (ServeJob* j : admit) {

@@ -39,9 +39,11 @@ struct ServeJob {
 
 class Server {
 public:
-    static constexpr size_t kPoolSlots = size_t(1) << 22;   // 4M path slots (~1 GB)
     static constexpr int64_t kStallIters = 20000;           // iterations without a retired sample
 
+    // Path slots of the serving pool: 2^pool_log2 of the serving settings (gnd_gpu_serve_tune;
+    // default 22, 4M slots, about 1 GB). Read with the context mutex held.
+    size_t poolSlots() const;
     explicit Server(Context* c);
     ~Server();
     gnd_job_id submit(const gnd_job_desc& d);

@@ -487,8 +487,9 @@ gnd_status gnd_gpu_set_hbm_budget(gnd_gpu_ctx* ctx, uint64_t bytes);
 enum { GND_SERVE_FIFO = 0, GND_SERVE_SRPT = 1, GND_SERVE_DEADLINE = 2 };
 gnd_status gnd_gpu_serve_policy(gnd_gpu_ctx* ctx, int32_t policy);
 /* Engine settings of the serving thread (gnd_tune; pool_log2 and round_iters are the
- * server's own, and material_sort is always on because jobs of both integrators share
- * launches). Like a scene's settings they change speed, never results. */
+ * server's own: its pool of path slots, default 2^22, takes the new size when no job is
+ * running; material_sort is always on because jobs of both integrators share launches).
+ * Like a scene's settings they change speed, never results. */
 gnd_status gnd_gpu_serve_tune(gnd_gpu_ctx* ctx, const gnd_tune* tune);
 /* Queues a job; returns at once with its id. The scene may not be freed while a job
  * that names it is queued or running (gnd_gpu_scene_free fails with GND_ERR_INVALID). */

@@ -114,3 +114,19 @@ def test_small_job_overtakes_a_large_one(setup, policy):
     assert ss["done_ms"] < sb["done_ms"]
     # the small job does not wait for the big one's samples: it finishes long before
     assert (ss["done_ms"] - ss["submit_ms"]) < 0.5 * (sb["done_ms"] - sb["submit_ms"])
+
+
+def test_serving_pool_size(setup):
+    """The serving pool takes pool_log2 of the serving settings when no job runs; a job
+    served from a 64K-slot pool (many refills per pass) renders what the default pool
+    renders."""
+    ctx, cb, _, _ = setup
+    job = dict(width=64, height=64, spp=4, max_depth=8, integrator=0)
+    ref, _ = ctx.wait(ctx.submit(cb, **job))
+    try:
+        ctx.serve_tune(pool_log2=16)
+        small, st = ctx.wait(ctx.submit(cb, **job))
+        assert st["state"] == "done"
+        same_film(small, ref, "64K-slot serving pool vs the default")
+    finally:
+        ctx.serve_tune()
