@@ -806,6 +806,11 @@ __device__ __forceinline__ uint32_t shadeClass(const SceneView& s, bool vol, int
     const uint32_t c = (vol && medium >= 0) ? (uint32_t)kMediumClass : surfaceClass(s, inst);
     return (vol ? (uint32_t)kClassesPerInt : 0u) + c;
 }
+// Class of a path whose bounce ends it unchanged: a path_gpu ray that escapes a scene
+// without an environment emitter (path.cpp: the escaped ray adds nothing and the path
+// ends). kClassify appends it to the done list directly; the shade kernel would only
+// have stored its state back unchanged.
+constexpr uint32_t kClassDone = kShadeClasses;
 
 // Closest-hit source/sink over the active list (extend). The store also records the
 // path's shade class in the hit record, for kClassify.
@@ -837,7 +842,7 @@ struct ExtendSrc {
     __device__ void store(uint32_t, const THit& h, const SceneView& sv) {
         HitRec hr;
         hr.t = h.t; hr.u = h.u; hr.v = h.v; hr.inst = h.inst; hr.slot = h.slot;
-        hr.pad[0] = shadeClass(sv, vol, medium, h.inst);
+        hr.pad[0] = (h.inst < 0 && !vol && sv.env.emitter < 0) ? kClassDone : shadeClass(sv, vol, medium, h.inst);
         hr.pad[1] = hr.pad[2] = 0;
         p->hits[slot] = hr;
     }
@@ -929,10 +934,12 @@ __global__ void __launch_bounds__(kBlock) kRayScatter(KParams p) {
 }
 
 
-// Active list -> per-class lists: per block, the warps' groups of one class take
-// consecutive places (shared-memory counts), then one atomic per class per block.
+// Active list -> per-class lists (and kClassDone -> the done list): per block, the warps'
+// groups of one class take consecutive places (shared-memory counts), then one atomic per
+// class per block.
 __global__ void __launch_bounds__(kAggBlock, 4) kClassify(KParams p, uint32_t* classLists) {
-    __shared__ uint32_t sCount[kShadeClasses], sBase[kShadeClasses];
+    constexpr int kLists = kShadeClasses + 1;   // the class lists and the done list
+    __shared__ uint32_t sCount[kLists], sBase[kLists];
     const uint32_t n = p.cnt[kQIn];
     const uint32_t lane = threadIdx.x & 31u;
     for (uint32_t bb = blockIdx.x * kAggBlock; bb < n; bb += gridDim.x * kAggBlock) {   // block-uniform
@@ -941,10 +948,10 @@ __global__ void __launch_bounds__(kAggBlock, 4) kClassify(KParams p, uint32_t* c
         uint32_t cls = 0xFFFFFFFFu, slot = 0;
         if (valid) {
             slot = p.listIn[i];
-            cls = p.hits[slot].pad[0];   // written by the extend store (shadeClass)
+            cls = p.hits[slot].pad[0];   // written by the extend store (shadeClass or kClassDone)
         }
         __syncthreads();   // the previous iteration's reads of sBase are over
-        if (threadIdx.x < (unsigned)kShadeClasses) sCount[threadIdx.x] = 0;
+        if (threadIdx.x < (unsigned)kLists) sCount[threadIdx.x] = 0;
         __syncthreads();
         const uint32_t grp = __match_any_sync(0xffffffffu, cls);
         const int leader = __ffs(grp) - 1;
@@ -952,13 +959,17 @@ __global__ void __launch_bounds__(kAggBlock, 4) kClassify(KParams p, uint32_t* c
         if (valid && (int)lane == leader) off = atomicAdd(&sCount[cls], (uint32_t)__popc(grp));
         off = __shfl_sync(0xffffffffu, off, leader);
         __syncthreads();
-        if (threadIdx.x < (unsigned)kShadeClasses) {
+        if (threadIdx.x < (unsigned)kLists) {
             const uint32_t c = sCount[threadIdx.x];
-            sBase[threadIdx.x] = c ? atomicAdd(&p.cnt[kQClass0 + threadIdx.x], c) : 0u;
+            uint32_t* counter = threadIdx.x < (unsigned)kShadeClasses ? &p.cnt[kQClass0 + threadIdx.x] : &p.cnt[kQDone];
+            sBase[threadIdx.x] = c ? atomicAdd(counter, c) : 0u;
         }
         __syncthreads();
-        if (valid)
-            classLists[(size_t)cls * p.capacity + sBase[cls] + off + (uint32_t)__popc(grp & ((1u << lane) - 1u))] = slot;
+        if (valid) {
+            const uint32_t at = sBase[cls] + off + (uint32_t)__popc(grp & ((1u << lane) - 1u));
+            if (cls < (uint32_t)kShadeClasses) classLists[(size_t)cls * p.capacity + at] = slot;
+            else p.done[at] = slot;
+        }
     }
 }
 
