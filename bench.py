@@ -538,8 +538,8 @@ def main():
     tune = ctx.get_tune(sid)
     if not args.no_autotune:
         t = time.time()
-        tune, tune_mp = ctx.autotune(sid, spp=16, budget_ms=12000)
-        log("autotune %.1fs: %s (%.0f Mpaths/s at 16 spp)" % (time.time() - t, tune, tune_mp))
+        tune, tune_mp = ctx.autotune(sid, spp=32, budget_ms=16000)
+        log("autotune %.1fs: %s (%.0f Mpaths/s at 32 spp)" % (time.time() - t, tune, tune_mp))
     # one host film buffer for every render of the run (each render adds its sums into it)
     film = np.zeros((WORKLOAD["height"], WORKLOAD["width"], 7), np.float32)
     for w in range(args.warmup):
